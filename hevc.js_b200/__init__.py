@@ -1,0 +1,360 @@
+"""hevc.js B200 reconstruction back end — Python host mirror of the C ABI.
+
+The product is the C-ABI library ``libhevcgpu.so`` (include/hevcgpu.h): the hevc.js
+decoder's reconstruction path (dequant + inverse transform, intra and inter
+prediction, deblocking, SAO, DPB in HBM) as sm_100a CUDA kernels.  This module binds it
+with ctypes so that Python tests and benchmarks call exactly the entry points a C/C++
+host calls.  It has no compute of its own and no CPU fallback: when the library or a
+CUDA device is missing, ``Context()`` raises.
+
+The stage functions mirror the reference's hot-path functions (privaloops/hevc.js):
+
+  Context.residual_blocks      perform_dequant + perform_transform_inverse +
+                               reconstruct_block  (src/decoding/transform.cpp:293, :374;
+                               src/decoding/coding_tree.cpp:371)
+  Context.inter_pred           perform_inter_prediction (src/decoding/interpolation.cpp:306)
+  Context.intra_recon          perform_intra_prediction (src/decoding/intra_prediction.cpp:428)
+  Context.loop_filter          apply_deblocking + apply_sao (src/filters/deblocking.cpp:357,
+                               src/filters/sao.cpp:20)
+  Context.reconstruct_picture  the per-picture reconstruction of Decoder::decode_picture
+                               (src/decoding/decoder.cpp:52-304) minus parsing
+
+Errors follow the reference C API (src/wasm/hevc_api.h:43-45): a negative status is an
+error; here it is raised as ``HevcGpuError`` carrying the library's message.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import (TU, PU, WP, SAO, Slice, PicParams, PictureSyntax, SynthCfg, SynthPicture,
+                  i420_size, split_i420, as_ptr, ptr_array, md5_planes)
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+SYNTH_SO = os.path.join(PKG, "libhevcsynth.so")
+GPU_SO = os.path.join(PKG, "libhevcgpu.so")
+
+_synth = None
+_gpu = None
+
+
+class HevcGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"hevcgpu error {code}: {msg}")
+        self.code = code
+
+
+# --------------------------------------------------------------------------- synth
+
+def synth_lib():
+    global _synth
+    if _synth is None:
+        if not os.path.exists(SYNTH_SO):
+            from . import build
+            build.build_synth()
+        lib = C.CDLL(SYNTH_SO)
+        lib.hevcsynth_default_cfg.argtypes = [C.POINTER(SynthCfg), C.c_int32, C.c_int32, C.c_uint64]
+        lib.hevcsynth_default_cfg.restype = None
+        lib.hevcsynth_picture.argtypes = [C.POINTER(SynthCfg)]
+        lib.hevcsynth_picture.restype = C.POINTER(SynthPicture)
+        lib.hevcsynth_picture_free.argtypes = [C.POINTER(SynthPicture)]
+        lib.hevcsynth_picture_free.restype = None
+        lib.hevcsynth_content.argtypes = [C.c_int32, C.c_int32, C.c_uint64, C.POINTER(C.c_uint8)]
+        lib.hevcsynth_content.restype = C.c_int
+        lib.hevcsynth_blocks.argtypes = [C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.POINTER(TU),
+                                         C.POINTER(C.c_int16), C.POINTER(C.c_uint8)]
+        lib.hevcsynth_blocks.restype = C.c_int64
+        lib.hevcsynth_bs_histogram.argtypes = [C.POINTER(PictureSyntax), C.POINTER(C.c_int64)]
+        lib.hevcsynth_bs_histogram.restype = C.c_int
+        _synth = lib
+    return _synth
+
+
+def default_cfg(width, height, seed, **kw):
+    cfg = SynthCfg()
+    synth_lib().hevcsynth_default_cfg(C.byref(cfg), width, height, seed)
+    for k, v in kw.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    return cfg
+
+
+class Picture:
+    """One picture of generated syntax (owns the generator's arrays until freed)."""
+
+    def __init__(self, cfg):
+        self._p = synth_lib().hevcsynth_picture(C.byref(cfg))
+        if not self._p:
+            raise ValueError("hevcsynth_picture: bad configuration")
+        self.cfg = cfg
+
+    @property
+    def syn(self):
+        return self._p.contents.syn
+
+    @property
+    def ptr(self):
+        return self._p
+
+    @property
+    def syn_ptr(self):
+        return C.pointer(self._p.contents.syn)
+
+    @property
+    def width(self):
+        return self.syn.params.width
+
+    @property
+    def height(self):
+        return self.syn.params.height
+
+    def tus(self):
+        n = self.syn.num_tus
+        return np.ctypeslib.as_array(C.cast(self.syn.tus, C.POINTER(C.c_uint8)), (n * 16,)).copy() if n else None
+
+    def counts(self):
+        s = self.syn
+        return {"tus": s.num_tus, "coeffs": s.num_coeffs, "pus": s.num_pus, "wp": s.num_wp,
+                "cus": self._p.contents.num_cus}
+
+    def bs_histogram(self):
+        out = (C.c_int64 * 3)()
+        synth_lib().hevcsynth_bs_histogram(self.syn_ptr, out)
+        return list(out)
+
+    def close(self):
+        if self._p:
+            synth_lib().hevcsynth_picture_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def content(width, height, seed):
+    out = np.empty(i420_size(width, height), np.uint8)
+    if synth_lib().hevcsynth_content(width, height, seed, as_ptr(out, C.c_uint8)) != 0:
+        raise ValueError("hevcsynth_content: bad size")
+    return out
+
+
+def blocks(num_tus, seed, qp_min=22, qp_max=37):
+    """Independent residual blocks: (tus array of TU, coeffs int16, pred uint8)."""
+    lib = synth_lib()
+    n = lib.hevcsynth_blocks(num_tus, seed, qp_min, qp_max, None, None, None)
+    if n < 0:
+        raise ValueError("hevcsynth_blocks: bad arguments")
+    tus = (TU * max(1, num_tus))()
+    coeffs = np.zeros(max(1, n), np.int16)
+    pred = np.zeros(max(1, n), np.uint8)
+    lib.hevcsynth_blocks(num_tus, seed, qp_min, qp_max, tus, as_ptr(coeffs, C.c_int16), as_ptr(pred, C.c_uint8))
+    return tus, num_tus, coeffs, pred
+
+
+# --------------------------------------------------------------------------- GPU library
+
+def gpu_lib():
+    """Load libhevcgpu.so; raises if it is missing (there is no fallback)."""
+    global _gpu
+    if _gpu is None:
+        if not os.path.exists(GPU_SO):
+            raise HevcGpuError(abi.HEVCGPU_ECUDA, f"{GPU_SO} is not built (run __graft_entry__.build())")
+        lib = C.CDLL(GPU_SO)
+        P = C.c_void_p
+        u8p = C.POINTER(C.c_uint8)
+        sig = {
+            "hevcgpu_abi_version": ([], C.c_int),
+            "hevcgpu_last_error": ([], C.c_char_p),
+            "hevcgpu_create": ([C.c_int, C.POINTER(P)], C.c_int),
+            "hevcgpu_destroy": ([P], None),
+            "hevcgpu_sync": ([P], C.c_int),
+            "hevcgpu_residual_blocks": ([P, C.POINTER(TU), C.c_int32, C.POINTER(C.c_int16), C.c_uint64, u8p, u8p],
+                                        C.c_int),
+            "hevcgpu_inter_pred": ([P, C.POINTER(PicParams), C.POINTER(PU), C.c_int32, C.POINTER(WP), C.c_int32,
+                                    C.POINTER(u8p), C.c_int32, u8p], C.c_int),
+            "hevcgpu_loop_filter": ([P, C.POINTER(PictureSyntax), u8p, u8p, C.c_int, C.c_int], C.c_int),
+            "hevcgpu_intra_recon": ([P, C.POINTER(PictureSyntax), u8p, u8p], C.c_int),
+            "hevcgpu_reconstruct_picture": ([P, C.POINTER(PictureSyntax), C.POINTER(u8p), C.c_int32, u8p], C.c_int),
+            "hevcgpu_set_budget": ([P, C.c_uint64], C.c_int),
+            "hevcgpu_bytes_in_use": ([P], C.c_uint64),
+            "hevcgpu_stream_open": ([P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(P)], C.c_int),
+            "hevcgpu_stream_close": ([P], None),
+            "hevcgpu_slot_upload": ([P, C.c_int32, u8p], C.c_int),
+            "hevcgpu_slot_download": ([P, C.c_int32, u8p], C.c_int),
+            "hevcgpu_slot_device_ptr": ([P, C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P),
+                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+            "hevcgpu_job_prepare": ([P, C.POINTER(PictureSyntax), C.POINTER(P)], C.c_int),
+            "hevcgpu_job_free": ([P], None),
+            "hevcgpu_job_launch": ([P, C.c_int32], C.c_int),
+            "hevcgpu_batch_launch": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
+            "hevcgpu_stream_sync": ([P], C.c_int),
+            "hevcgpu_cuda_stream": ([P], P),
+            "hevcgpu_launch_count": ([P], C.c_uint64),
+            "hevcgpu_picture_decode": ([P, C.POINTER(PictureSyntax), C.c_int32], C.c_int),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = res
+        _gpu = lib
+    return _gpu
+
+
+def _check(code):
+    if code < 0:
+        msg = gpu_lib().hevcgpu_last_error()
+        raise HevcGpuError(code, msg.decode() if msg else "")
+    return code
+
+
+class Context:
+    """A CUDA context of the back end on one device (hevcgpu_create)."""
+
+    def __init__(self, device=0):
+        self.lib = gpu_lib()
+        h = C.c_void_p()
+        _check(self.lib.hevcgpu_create(device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.hevcgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        _check(self.lib.hevcgpu_sync(self.h))
+
+    @property
+    def launches(self):
+        return int(self.lib.hevcgpu_launch_count(self.h))
+
+    @property
+    def cuda_stream(self):
+        return self.lib.hevcgpu_cuda_stream(self.h)
+
+    # ---- stages on host memory
+    def residual_blocks(self, tus, num_tus, coeffs, pred):
+        out = np.empty_like(pred)
+        _check(self.lib.hevcgpu_residual_blocks(self.h, tus, num_tus, as_ptr(coeffs, C.c_int16), coeffs.size,
+                                                as_ptr(pred, C.c_uint8), as_ptr(out, C.c_uint8)))
+        return out
+
+    def inter_pred(self, pic, refs):
+        p = pic.syn.params
+        out = np.zeros(i420_size(p.width, p.height), np.uint8)
+        _check(self.lib.hevcgpu_inter_pred(self.h, C.byref(p), pic.syn.pus, pic.syn.num_pus, pic.syn.wp,
+                                           pic.syn.num_wp, ptr_array(refs), len(refs), as_ptr(out, C.c_uint8)))
+        return out
+
+    def loop_filter(self, pic, inp, do_deblock=True, do_sao=True):
+        out = np.empty_like(inp)
+        _check(self.lib.hevcgpu_loop_filter(self.h, pic.syn_ptr, as_ptr(inp, C.c_uint8), as_ptr(out, C.c_uint8),
+                                            int(do_deblock), int(do_sao)))
+        return out
+
+    def intra_recon(self, pic, inp):
+        out = np.empty_like(inp)
+        _check(self.lib.hevcgpu_intra_recon(self.h, pic.syn_ptr, as_ptr(inp, C.c_uint8), as_ptr(out, C.c_uint8)))
+        return out
+
+    def reconstruct_picture(self, pic, refs):
+        p = pic.syn.params
+        out = np.zeros(i420_size(p.width, p.height), np.uint8)
+        _check(self.lib.hevcgpu_reconstruct_picture(self.h, pic.syn_ptr, ptr_array(refs), len(refs),
+                                                    as_ptr(out, C.c_uint8)))
+        return out
+
+    # ---- DPB / picture pipeline
+    def set_budget(self, nbytes):
+        _check(self.lib.hevcgpu_set_budget(self.h, nbytes))
+
+    def bytes_in_use(self):
+        return int(self.lib.hevcgpu_bytes_in_use(self.h))
+
+    def open_stream(self, width, height, slots):
+        return Stream(self, width, height, slots)
+
+
+class Stream:
+    """A decode stream: DPB slots in HBM (hevcgpu_stream_open)."""
+
+    def __init__(self, ctx, width, height, slots):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.width, self.height, self.slots = width, height, slots
+        h = C.c_void_p()
+        _check(self.lib.hevcgpu_stream_open(ctx.h, width, height, 8, slots, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.hevcgpu_stream_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, slot, i420):
+        _check(self.lib.hevcgpu_slot_upload(self.h, slot, as_ptr(i420, C.c_uint8)))
+
+    def download(self, slot, out=None):
+        if out is None:
+            out = np.empty(i420_size(self.width, self.height), np.uint8)
+        _check(self.lib.hevcgpu_slot_download(self.h, slot, as_ptr(out, C.c_uint8)))
+        return out
+
+    def prepare(self, pic):
+        return Job(self, pic)
+
+    def decode(self, pic, dst_slot):
+        _check(self.lib.hevcgpu_picture_decode(self.h, pic.syn_ptr, dst_slot))
+
+    def sync(self):
+        _check(self.lib.hevcgpu_stream_sync(self.h))
+
+
+class Job:
+    """A prepared picture (records uploaded once; hevcgpu_job_prepare)."""
+
+    def __init__(self, stream, pic):
+        self.stream = stream
+        self.lib = stream.lib
+        h = C.c_void_p()
+        _check(self.lib.hevcgpu_job_prepare(stream.h, pic.syn_ptr, C.byref(h)))
+        self.h = h
+
+    def launch(self, dst_slot):
+        _check(self.lib.hevcgpu_job_launch(self.h, dst_slot))
+
+    def free(self):
+        if self.h:
+            self.lib.hevcgpu_job_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def batch_launch(jobs, dst_slots):
+    lib = gpu_lib()
+    n = len(jobs)
+    arr = (C.c_void_p * n)(*[j.h for j in jobs])
+    slots = (C.c_int32 * n)(*dst_slots)
+    _check(lib.hevcgpu_batch_launch(arr, slots, n))

@@ -1,0 +1,251 @@
+/*
+ * hevcgpu.h — C ABI of the B200 reconstruction back end for the hevc.js decoder.
+ *
+ * The host decoder (hevc.js src/bitstream, src/syntax, CABAC in src/decoding) keeps
+ * parsing.  Everything it used to do with samples crosses this boundary as plain
+ * records: transform blocks with their coefficient levels, prediction units with
+ * motion vectors, a 4x4 grid of deblocking side information, SAO parameters per CTU.
+ * The GPU side runs dequantisation + inverse transform, intra prediction, motion
+ * compensation with weighted prediction, deblocking and SAO, and keeps the decoded
+ * picture buffer (DPB) in HBM.
+ *
+ * Reference interfaces replaced (paths inside privaloops/hevc.js):
+ *   perform_dequant            src/decoding/transform.cpp:293
+ *   perform_transform_inverse  src/decoding/transform.cpp:374
+ *   reconstruct_block          src/decoding/coding_tree.cpp:371
+ *   perform_intra_prediction   src/decoding/intra_prediction.cpp:428
+ *   perform_inter_prediction   src/decoding/interpolation.cpp:306
+ *   apply_deblocking           src/filters/deblocking.cpp:357
+ *   apply_sao                  src/filters/sao.cpp:20
+ *   Picture / DPB sample store src/common/picture.h:12, src/decoding/dpb.cpp:367
+ *
+ * Conventions.
+ *   - Every function returns HEVCGPU_OK (0) or a negative HEVCGPU_E* code; the text of
+ *     the last error of the calling thread is returned by hevcgpu_last_error().
+ *   - Host sample planes are 8-bit and tightly packed I420: Y (W*H), Cb, Cr ((W/2)*(H/2)
+ *     each), the layout of Picture::write_yuv (src/common/picture.cpp:42) for 8-bit.
+ *   - Only 8-bit 4:2:0 is accepted (HEVCGPU_EUNSUPPORTED otherwise).
+ *   - No function falls back to a CPU implementation: without a usable CUDA device the
+ *     create call fails with HEVCGPU_ECUDA.
+ */
+#ifndef HEVCGPU_H
+#define HEVCGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HEVCGPU_ABI_VERSION 1
+
+/* ---- status codes (negative values map to HEVC_ERROR of src/wasm/hevc_api.h:43) ---- */
+#define HEVCGPU_OK            0
+#define HEVCGPU_EINVAL       -1   /* bad argument or record outside the picture        */
+#define HEVCGPU_ECUDA        -2   /* CUDA runtime error (message has the CUDA string)  */
+#define HEVCGPU_ENOMEM       -3   /* device or pinned host allocation failed / budget */
+#define HEVCGPU_EUNSUPPORTED -4   /* bit depth, chroma format or tool not supported    */
+#define HEVCGPU_ETIMEOUT     -5   /* a bounded device wait gave up (status word set)   */
+#define HEVCGPU_EDEVICE      -6   /* a kernel reported a record it refused (bounds)    */
+
+/* ---- record layouts (all little-endian, naturally aligned, no padding surprises) ---- */
+
+/* Transform block flags. */
+#define HEVC_TU_INTRA   0x01  /* CuPredMode == MODE_INTRA: predicted by intra_mode       */
+#define HEVC_TU_CODED   0x02  /* has coefficient levels at coeff_offset (cbf set)        */
+#define HEVC_TU_TSKIP   0x04  /* transform_skip_flag                                    */
+#define HEVC_TU_BYPASS  0x08  /* cu_transquant_bypass: levels are the residual          */
+
+/* One transform block of one colour component (decode order = z-scan, luma before
+ * chroma, 4x4-luma chroma deferred to blkIdx 3; src/decoding/coding_tree.cpp:1256). */
+typedef struct hevc_tu {
+    uint16_t x, y;          /* top-left in samples of component c_idx                  */
+    uint8_t  log2_size;     /* 2..5                                                    */
+    uint8_t  c_idx;         /* 0 = Y, 1 = Cb, 2 = Cr                                   */
+    uint8_t  qp;            /* qP' = QpY + QpBdOffsetY, or the mapped chroma qP'       */
+    uint8_t  flags;         /* HEVC_TU_*                                               */
+    uint8_t  intra_mode;    /* 0..34, for HEVC_TU_INTRA                                */
+    uint8_t  reserved[3];
+    uint32_t coeff_offset;  /* first int16 of this block's N*N row-major levels       */
+} hevc_tu_t;                /* 16 bytes */
+
+/* One prediction unit (src/decoding/coding_tree.cpp:882-953).  List l is used when
+ * ref_idx[l] >= 0 (predFlagLX); ref_idx indexes the picture's reference list. */
+typedef struct hevc_pu {
+    uint16_t x, y;          /* luma top-left                                           */
+    uint8_t  w, h;          /* luma size, 4..64                                        */
+    int8_t   ref_idx[2];    /* refIdxL0, refIdxL1 (-1: list unused)                    */
+    int16_t  mv[2][2];      /* quarter-pel luma MV: mv[list][0] = x, mv[list][1] = y   */
+    int16_t  wp;            /* -1: default weighted prediction; else row of the WP table */
+    uint16_t reserved;
+} hevc_pu_t;                /* 20 bytes */
+
+/* Explicit weighted prediction parameters of one PU class, already resolved from the
+ * slice's pred_weight_table for its (refIdxL0, refIdxL1): weighted_pred_explicit,
+ * src/decoding/interpolation.cpp:246. */
+typedef struct hevc_wp {
+    int16_t log2wd[2];      /* log2Wd for luma [0] and chroma [1] (denominator + shift1) */
+    int16_t w[2][3];        /* weight [list][component]                                 */
+    int16_t o[2][3];        /* offset [list][component], already << (BitDepth - 8)      */
+} hevc_wp_t;                /* 28 bytes */
+
+/* 4x4-luma-block side information word (deblocking grids of DecodingContext,
+ * src/decoding/coding_tree.h:65-70 and CUInfo :21-30). */
+#define HEVC_BLK_EDGE_V   0x01u   /* edge_flags_v: vertical TU/PU/CU edge at left side  */
+#define HEVC_BLK_EDGE_H   0x02u   /* edge_flags_h: horizontal edge at top side          */
+#define HEVC_BLK_CBF      0x04u   /* cbf_luma of the covering luma TU                   */
+#define HEVC_BLK_INTRA    0x08u   /* CU is intra                                        */
+#define HEVC_BLK_PCM      0x10u   /* CU is PCM                                          */
+#define HEVC_BLK_BYPASS   0x20u   /* cu_transquant_bypass                               */
+#define HEVC_BLK_TU_SHIFT 8       /* bits 8..15: log2 of the covering TU size           */
+#define HEVC_BLK_QP_SHIFT 16      /* bits 16..23: QpY of the CU, two's complement int8  */
+
+/* SAO parameters of one CTU (DecodingContext::SaoParams, coding_tree.h:73-78). */
+typedef struct hevc_sao {
+    uint8_t type[3];        /* 0 off, 1 band offset, 2 edge offset                     */
+    uint8_t band_pos[3];    /* sao_band_position                                       */
+    uint8_t eo_class[3];    /* sao_eo_class                                            */
+    int8_t  offset[3][5];   /* SaoOffsetVal in the reference layout: EO [+,+,0,-,-],   */
+                            /* BO [o0,o1,o2,o3,0] (coding_tree.cpp:146-164)            */
+} hevc_sao_t;               /* 24 bytes */
+
+/* Per-slice filter parameters (SliceHeader fields read by apply_deblocking/apply_sao). */
+typedef struct hevc_slice {
+    int8_t  beta_offset_div2;
+    int8_t  tc_offset_div2;
+    uint8_t deblocking_disabled;      /* slice_deblocking_filter_disabled_flag          */
+    uint8_t lf_across_slices;         /* slice_loop_filter_across_slices_enabled_flag   */
+} hevc_slice_t;
+
+/* Picture-level parameters (SPS/PPS/slice fields the reconstruction reads). */
+typedef struct hevc_pic_params {
+    int32_t width, height;            /* luma samples, multiples of 8                   */
+    int32_t bit_depth;                /* 8                                              */
+    int32_t log2_ctb;                 /* CtbLog2SizeY, 4..6                             */
+    int32_t log2_min_cb;              /* MinCbLog2SizeY                                 */
+    int32_t log2_min_tb;              /* MinTbLog2SizeY (2)                             */
+    int32_t strong_intra_smoothing;   /* strong_intra_smoothing_enabled_flag            */
+    int32_t intra_smoothing_disabled; /* intra_smoothing_disabled_flag                  */
+    int32_t pcm_loop_filter_disabled; /* pcm_loop_filter_disabled_flag                  */
+    int32_t sao_enabled;              /* sample_adaptive_offset_enabled_flag            */
+    int32_t cb_qp_offset, cr_qp_offset;   /* pps_cb_qp_offset, pps_cr_qp_offset         */
+    int32_t tiles_enabled;            /* ctb_tile is meaningful                         */
+    int32_t loop_filter_across_tiles; /* loop_filter_across_tiles_enabled_flag          */
+    int32_t num_ref[2];               /* entries in RefPicList0/1                       */
+    int32_t ref_poc[2][16];           /* POC of each entry (deblocking Bs compares POCs) */
+    int32_t ref_slot[2][16];          /* DPB slot of each entry (picture API)           */
+} hevc_pic_params_t;
+
+/* Everything one picture hands to the GPU at its end (the point where
+ * src/decoding/decoder.cpp:270 calls apply_deblocking today). */
+typedef struct hevc_picture_syntax {
+    hevc_pic_params_t   params;
+    int32_t             num_tus;      /* intra TUs (coded or not) + coded inter TUs     */
+    const hevc_tu_t*    tus;          /* in decode order                                */
+    uint64_t            num_coeffs;
+    const int16_t*      coeffs;
+    int32_t             num_pus;
+    const hevc_pu_t*    pus;
+    int32_t             num_wp;
+    const hevc_wp_t*    wp;
+    const uint32_t*     blk;          /* (width/4)*(height/4) HEVC_BLK_* words          */
+    const hevc_sao_t*   sao;          /* PicSizeInCtbsY entries, raster order           */
+    const uint8_t*      ctb_slice;    /* slice index per CTB (raster), or NULL = all 0  */
+    const uint16_t*     ctb_tile;     /* TileId per CTB (raster), or NULL               */
+    int32_t             num_slices;
+    const hevc_slice_t* slices;
+} hevc_picture_syntax_t;
+
+/* ---- context ---- */
+typedef struct hevcgpu_ctx hevcgpu_ctx_t;
+typedef struct hevcgpu_stream hevcgpu_stream_t;
+typedef struct hevcgpu_job hevcgpu_job_t;
+
+int         hevcgpu_abi_version(void);
+const char* hevcgpu_last_error(void);
+int         hevcgpu_create(int device, hevcgpu_ctx_t** out);
+void        hevcgpu_destroy(hevcgpu_ctx_t* ctx);
+int         hevcgpu_sync(hevcgpu_ctx_t* ctx);
+
+/* ---- stage entry points on host memory (synchronous; copies inside) ---- */
+
+/* Dequant + inverse DST/DCT + add prediction + clip for independent blocks.
+ * Replaces perform_dequant (transform.cpp:293), perform_transform_inverse
+ * (transform.cpp:374) and reconstruct_block (coding_tree.cpp:371).  Block t reads its
+ * N*N levels at coeffs + tus[t].coeff_offset, its N*N prediction samples at
+ * pred + tus[t].coeff_offset and writes N*N samples at out + tus[t].coeff_offset. */
+int hevcgpu_residual_blocks(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int32_t num_tus,
+                            const int16_t* coeffs, uint64_t num_coeffs,
+                            const uint8_t* pred, uint8_t* out);
+
+/* Motion-compensated prediction of every PU into out (I420, params->width x height).
+ * refs[i] is the I420 picture for reference-list slot i (params->ref_slot values
+ * index this array).  Replaces perform_inter_prediction (interpolation.cpp:306) and
+ * the sample store of coding_tree.cpp:892-922. */
+int hevcgpu_inter_pred(hevcgpu_ctx_t* ctx, const hevc_pic_params_t* params,
+                       const hevc_pu_t* pus, int32_t num_pus,
+                       const hevc_wp_t* wp, int32_t num_wp,
+                       const uint8_t* const* refs, int32_t num_refs, uint8_t* out);
+
+/* In-loop filters of one reconstructed picture: deblocking (apply_deblocking,
+ * deblocking.cpp:357) when do_deblock, then SAO (apply_sao, sao.cpp:20) when do_sao.
+ * syn->tus/coeffs are not used; syn->pus provide motion for the Bs derivation. */
+int hevcgpu_loop_filter(hevcgpu_ctx_t* ctx, const hevc_picture_syntax_t* syn,
+                        const uint8_t* in, uint8_t* out, int do_deblock, int do_sao);
+
+/* Intra prediction + residual for the intra TUs of syn over an I420 picture that
+ * already holds every inter sample (in/out may alias).  Replaces
+ * perform_intra_prediction (intra_prediction.cpp:428) in its TU loop. */
+int hevcgpu_intra_recon(hevcgpu_ctx_t* ctx, const hevc_picture_syntax_t* syn,
+                        const uint8_t* in, uint8_t* out);
+
+/* Whole-picture reconstruction (MC, residual, intra wavefront, deblocking, SAO) of one
+ * picture; refs as in hevcgpu_inter_pred. */
+int hevcgpu_reconstruct_picture(hevcgpu_ctx_t* ctx, const hevc_picture_syntax_t* syn,
+                                const uint8_t* const* refs, int32_t num_refs,
+                                uint8_t* out);
+
+/* ---- decoded picture buffer in HBM + picture pipeline ---- */
+
+/* A stream owns num_slots DPB slots of width x height 8-bit 4:2:0 in HBM plus the work
+ * buffers of one picture in flight.  Admission: fails with HEVCGPU_ENOMEM when the
+ * context's HBM budget (hevcgpu_set_budget) would be exceeded. */
+int  hevcgpu_set_budget(hevcgpu_ctx_t* ctx, uint64_t bytes);
+uint64_t hevcgpu_bytes_in_use(hevcgpu_ctx_t* ctx);
+int  hevcgpu_stream_open(hevcgpu_ctx_t* ctx, int32_t width, int32_t height,
+                         int32_t bit_depth, int32_t num_slots, hevcgpu_stream_t** out);
+void hevcgpu_stream_close(hevcgpu_stream_t* st);
+int  hevcgpu_slot_upload(hevcgpu_stream_t* st, int32_t slot, const uint8_t* i420);
+int  hevcgpu_slot_download(hevcgpu_stream_t* st, int32_t slot, uint8_t* i420);
+/* Device address of a slot's Y plane and the row pitches (for zero-copy consumers). */
+int  hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void** cb,
+                             void** cr, int32_t* pitch_y, int32_t* pitch_c);
+
+/* Prepare a picture: host-side packing (bins, per-CTU intra lists) and one upload of
+ * the records into device memory owned by the job.  The job can be launched many
+ * times (benchmarks) and is freed with hevcgpu_job_free. */
+int  hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn,
+                         hevcgpu_job_t** out);
+void hevcgpu_job_free(hevcgpu_job_t* job);
+/* Plain form: one launch per stage for this picture, into DPB slot dst_slot, reading
+ * reference slots from params.ref_slot.  Asynchronous on the stream's CUDA stream. */
+int  hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot);
+/* Batched form: the stages of n pictures (any streams of one context, no picture may
+ * reference another picture of the same batch) run as merged launches. */
+int  hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, int32_t n);
+int  hevcgpu_stream_sync(hevcgpu_stream_t* st);
+/* CUDA stream (cudaStream_t) the context launches on. */
+void* hevcgpu_cuda_stream(hevcgpu_ctx_t* ctx);
+/* Number of kernel launches issued by this context so far. */
+uint64_t hevcgpu_launch_count(hevcgpu_ctx_t* ctx);
+
+/* End-to-end decode-side call: prepare + upload + launch + wait for one picture. */
+int  hevcgpu_picture_decode(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn,
+                            int32_t dst_slot);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HEVCGPU_H */
