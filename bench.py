@@ -1,0 +1,400 @@
+"""Benchmark of the hevc.js B200 reconstruction back end.
+
+Workload (one step): reconstruct B 1920x1080 4:2:0 8-bit pictures — motion
+compensation from two reference pictures held in the HBM DPB, dequant + inverse
+transform, intra wavefront, deblocking, SAO — from seeded synthetic P/B picture syntax
+(CU quadtree split 0.5 to 8x8, 10 % intra CUs, 20 % skip, 50 % bi-prediction, 10 %
+explicit WP, MVs +-256 qpel, QP 22..37, SAO per CTU), one picture per stream, B streams
+merged into shared launches (the batched form).  The plain form (one launch per stage
+per picture) is timed beside it and reported as "plain".  Output is bit-exact against
+the reference (checked by the tests; the bench verifies one picture per stream against
+the oracle before timing).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+
+value      frames/s over the whole job with the records already in HBM (device time, CUDA
+           events on the library's stream, max over ranks).
+e2e        frames/s through the C ABI from host memory: per step each picture's records are
+           packed into pinned memory and copied host->device (hevcgpu_job_prepare), the
+           batch is launched, and every reconstructed picture is copied device->host.
+--impl reference runs privaloops/hevc.js's own reconstruction functions (oracle/_ref,
+           compiled from the reference's sources) on all host cores for the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W_DEFAULT, H_DEFAULT = 1920, 1080
+PICTURE_CFG = dict(p_intra=0.1, p_skip=0.2, p_merge=0.3)
+METRIC = "bit-exact 1080p frames/s on 1 B200, batched/served vs plain GPU; p50/p99 frame ms"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--width", type=int, default=W_DEFAULT)
+    ap.add_argument("--height", type=int, default=H_DEFAULT)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", action="store_true", help="short run for ncu captures")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# --------------------------------------------------------------------------- workload
+
+def make_streams(hb, n, w, h, seed0):
+    """n pictures' syntax and their two reference pictures (content seeds per stream)."""
+    pics, refs = [], []
+    for i in range(n):
+        seed = seed0 + 97 * i
+        pics.append(hb.Picture(hb.default_cfg(w, h, seed, poc=8, **PICTURE_CFG)))
+        refs.append([hb.content(w, h, seed + 1), hb.content(w, h, seed + 2)])
+    return pics, refs
+
+
+def algorithmic_bytes(hb, pic):
+    """Algorithmic HBM bytes per stage of one picture (reads + writes the stage must do)."""
+    import numpy as np
+    s = pic.syn
+    W, H = s.params.width, s.params.height
+    npu, ntu = s.num_pus, s.num_tus
+    pu = np.ctypeslib.as_array(C.cast(s.pus, C.POINTER(C.c_uint8)), (npu * 20,)).view(
+        np.dtype([("x", "<u2"), ("y", "<u2"), ("w", "u1"), ("h", "u1"), ("r", "i1", 2), ("mv", "<i2", 4),
+                  ("wp", "<i2"), ("pad", "<u2")]))
+    pw, ph = pu["w"].astype(np.int64), pu["h"].astype(np.int64)
+    lists = (pu["r"] >= 0).sum(axis=1)
+    mc_read = int((lists * ((pw + 7) * (ph + 7) + 2 * (pw // 2 + 3) * (ph // 2 + 3))).sum())
+    mc_write = int((pw * ph * 3 // 2).sum())
+    tu = np.ctypeslib.as_array(C.cast(s.tus, C.POINTER(C.c_uint8)), (ntu * 16,)).view(
+        np.dtype([("x", "<u2"), ("y", "<u2"), ("l", "u1"), ("c", "u1"), ("qp", "u1"), ("f", "u1"), ("m", "u1"),
+                  ("r", "u1", 3), ("off", "<u4")]))
+    n2 = (1 << tu["l"].astype(np.int64)) ** 2
+    coded = (tu["f"] & 2) != 0
+    intra = (tu["f"] & 1) != 0
+    res = int((n2[coded & ~intra] * 4).sum() + (n2[coded & intra] * 4).sum())
+    intra_b = int((n2[intra] * 1 + n2[intra & coded] * 2).sum())
+    pic_bytes = W * H * 3 // 2
+    grid = (W // 4) * (H // 4) * 4
+    return {"mc": mc_read + mc_write, "residual": res, "intra": intra_b,
+            "deblock": 2 * pic_bytes + 2 * grid + (W // 4) * (H // 4) * 12, "sao": 2 * pic_bytes + grid}
+
+
+# --------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- CPU arms
+
+def cpu_run(checker, pics, refs, n_pictures, threads):
+    """Reconstruct n_pictures (round robin over the generated ones) on host threads."""
+    from concurrent.futures import ThreadPoolExecutor
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda i: checker.reconstruct_picture(pics[i % len(pics)], refs[i % len(pics)]),
+                    range(n_pictures)))
+    return time.perf_counter() - t0
+
+
+def cpu_checker():
+    import oracle
+    if oracle.ref_available():
+        return oracle.ref(), "reference"
+    return oracle.port(), "port"
+
+
+def run_reference(args, hb, rank, world):
+    if rank != 0:
+        return None
+    pics, refs = make_streams(hb, args.batch, args.width, args.height, 1000)
+    checker, kind = cpu_checker()
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_run(checker, pics, refs, args.batch, threads)
+    times = [cpu_run(checker, pics, refs, args.batch, threads) for _ in range(args.steps)]
+    total = sum(times)
+    value = args.batch * args.steps / total
+    line = {"metric": METRIC, "value": round(value, 3), "unit": "frames/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * total / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int16/int32",
+            "data": "synthetic (seeded P/B picture syntax and sinusoid references)", "impl": "reference",
+            "config": {"workload": f"{args.width}x{args.height} 4:2:0 8-bit P/B picture reconstruction "
+                                   f"(MC + residual + intra + deblocking + SAO), {args.batch} pictures per step",
+                       "batch": args.batch, "parallelism": f"{threads} host threads, one picture per thread"},
+            "cpu_baseline": {"value": round(value, 3), "unit": "frames/s", "cores": threads, "kind": kind,
+                             "sample": f"{args.batch} pictures per step x {args.steps} steps"},
+            "e2e": {"value": round(value, 3), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+# --------------------------------------------------------------------------- GPU arm
+
+import ctypes as C  # noqa: E402
+
+
+def run_ours(args, hb, rank, world, local):
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    ctx = hb.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.cuda_stream, device=dev)
+    W, H, B = args.width, args.height, args.batch
+    # replicas: each rank reconstructs its own streams (different seeds), no collective
+    pics, refs = make_streams(hb, B, W, H, 1000 + 100000 * rank)
+    streams, jobs = [], []
+    for i in range(B):
+        st = ctx.open_stream(W, H, 3)
+        st.upload(0, refs[i][0])
+        st.upload(1, refs[i][1])
+        streams.append(st)
+        jobs.append(st.prepare(pics[i]))
+    slots = [2] * B
+
+    # correctness gate before timing: every picture bit-exact against the oracle
+    import oracle
+    hb.batch_launch(jobs, slots)
+    ctx.sync()
+    check = oracle.port()
+    for i in range(B if args.steps > 0 else 1):
+        got = streams[i].download(2)
+        want = check.reconstruct_picture(pics[i], refs[i])
+        if not np.array_equal(got, want):
+            raise SystemExit(f"bench: picture {i} differs from the oracle in {int((got != want).sum())} samples")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        ctx.sync()
+        barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        step_ms = []
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        l0 = ctx.launches
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            evs[0].record(stream)
+            for k in range(steps):
+                fn()
+                evs[k + 1].record(stream)
+            ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+        return max_over_ranks(ms), step_ms, ctx.launches - l0
+
+    if args.profile_only:
+        for _ in range(max(1, args.steps)):
+            hb.batch_launch(jobs, slots)
+        ctx.sync()
+        return None
+
+    with ClockSampler(local) as clocks:
+        batched_ms, step_ms, launches = timed(lambda: hb.batch_launch(jobs, slots), args.steps, args.warmup)
+    plain_steps = max(3, args.steps // 4)
+    plain_ms, _, plain_launches = timed(lambda: [j.launch(2) for j in jobs], plain_steps, args.warmup)
+
+    # stage profile (separate pass; events between stages)
+    ctx.profile(True)
+    prof_steps = max(3, args.steps // 4)
+    for _ in range(prof_steps):
+        hb.batch_launch(jobs, slots)
+    stages = ctx.profile_read()
+    ctx.profile(False)
+
+    # end to end through the C ABI from host memory
+    out_host = [np.empty(hb.i420_size(W, H), np.uint8) for _ in range(B)]
+    h2d_bytes = 0
+
+    def e2e_step():
+        nonlocal h2d_bytes
+        js = [st.prepare(p) for st, p in zip(streams, pics)]
+        h2d_bytes = sum(j.upload_bytes for j in js)
+        hb.batch_launch(js, slots)
+        for i, st in enumerate(streams):
+            st.download(2, out_host[i])
+        for j in js:
+            j.free()
+    e2e_steps = max(3, args.steps // 5)
+    for _ in range(2):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    d2h_bytes = B * hb.i420_size(W, H)
+
+    frames = B * args.steps * world
+    value = frames / (batched_ms / 1000.0)
+    plain_value = B * plain_steps * world / (plain_ms / 1000.0)
+    e2e_value = B * e2e_steps * world / e2e_s
+
+    # roofline of the dominant stage
+    import json as _json
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(_json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    alg = [algorithmic_bytes(hb, p) for p in pics]
+    alg_sum = {k: sum(a[k] for a in alg) for k in alg[0]}
+    stage_ms = {"mc": stages["mc"][0], "residual": stages["residual"][0], "intra": stages["intra"][0],
+                "deblock": stages["deblock_v"][0] + stages["deblock_h"][0], "sao": stages["sao"][0]}
+    per_stage = {}
+    for k, ms in stage_ms.items():
+        per_launch_ms = ms / prof_steps
+        gbs = alg_sum[k] / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
+        per_stage[k] = {"ms_per_step": round(per_launch_ms, 4), "alg_bytes_per_step": alg_sum[k],
+                        "GB/s": round(gbs, 1), "frac_of_hbm": round(gbs / peak, 4)}
+    dom = max(stage_ms, key=lambda k: stage_ms[k])
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        checker, kind = cpu_checker()
+        threads = os.cpu_count() or 1
+        n = max(threads, 2 * B)
+        cpu_run(checker, pics, refs, threads, threads)
+        t = cpu_run(checker, pics, refs, n, threads)
+        cpu = {"value": round(n / t, 3), "unit": "frames/s", "cores": threads, "kind": kind,
+               "sample": f"{n} of the bench's {W}x{H} pictures on {threads} host threads ({t:.1f} s)"}
+
+    clk = clocks.summary()
+    step_sorted = sorted(step_ms)
+    per_frame_ms = [m for m in step_ms]   # each frame completes with its batched step
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(batched_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8/int16/int32", "data": "synthetic (seeded P/B picture "
+        "syntax and sinusoid reference pictures; no public dataset)",
+        "config": {"workload": f"{W}x{H} 4:2:0 8-bit P/B picture reconstruction (MC + residual + intra wavefront + "
+                               f"deblocking + SAO), {B} streams batched per launch",
+                   "global_batch": B * world, "parallelism": f"replicas x{world} (streams sharded, no collective)",
+                   "l2": "inputs larger than L2 (B pictures x 4 HBM buffers)"},
+        "plain": {"value": round(plain_value, 2), "unit": "frames/s", "ms_per_picture": round(plain_ms / plain_steps / B, 4),
+                  "gpu_launches_per_picture": round(plain_launches / plain_steps / B, 1)},
+        "batched_over_plain": round(value / plain_value, 3),
+        "frame_ms": {"p50": round(statistics.median(per_frame_ms), 4),
+                     "p99": round(step_sorted[min(len(step_sorted) - 1, int(0.99 * len(step_sorted)))], 4),
+                     "note": "batched form: every picture of a step completes when its step completes"},
+        "e2e": {"value": round(e2e_value, 2), "unit": "frames/s", "h2d_bytes_per_step": int(h2d_bytes),
+                "d2h_bytes_per_step": int(d2h_bytes)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": per_stage[dom]["GB/s"], "peak": peak,
+                     "unit": "GB/s", "frac": per_stage[dom]["frac_of_hbm"], "traffic": None,
+                     "peak_source": peak_src},
+        "stages": per_stage,
+        "clocks": clk,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    for st in streams:
+        st.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    import __graft_entry__ as ge
+    hb = ge.load_package()
+    if args.impl == "reference":
+        line = run_reference(args, hb, rank, world)
+    else:
+        line = run_ours(args, hb, rank, world, local)
+    if line is not None and rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

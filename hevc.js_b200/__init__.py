@@ -190,12 +190,15 @@ def gpu_lib():
                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
             "hevcgpu_job_prepare": ([P, C.POINTER(PictureSyntax), C.POINTER(P)], C.c_int),
             "hevcgpu_job_free": ([P], None),
+            "hevcgpu_job_upload_bytes": ([P], C.c_uint64),
             "hevcgpu_job_launch": ([P, C.c_int32], C.c_int),
             "hevcgpu_batch_launch": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
             "hevcgpu_stream_sync": ([P], C.c_int),
             "hevcgpu_cuda_stream": ([P], P),
             "hevcgpu_launch_count": ([P], C.c_uint64),
             "hevcgpu_picture_decode": ([P, C.POINTER(PictureSyntax), C.c_int32], C.c_int),
+            "hevcgpu_profile_enable": ([P, C.c_int], C.c_int),
+            "hevcgpu_profile_read": ([P, C.POINTER(C.c_double), C.POINTER(C.c_uint64)], C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(lib, name)
@@ -242,6 +245,17 @@ class Context:
     @property
     def cuda_stream(self):
         return self.lib.hevcgpu_cuda_stream(self.h)
+
+    STAGES = ("motion_grid", "mc", "residual", "intra", "deblock_v", "deblock_h", "sao")
+
+    def profile(self, enable=True):
+        _check(self.lib.hevcgpu_profile_enable(self.h, int(enable)))
+
+    def profile_read(self):
+        ms = (C.c_double * 7)()
+        n = (C.c_uint64 * 7)()
+        _check(self.lib.hevcgpu_profile_read(self.h, ms, n))
+        return {s: (ms[i], int(n[i])) for i, s in enumerate(self.STAGES)}
 
     # ---- stages on host memory
     def residual_blocks(self, tus, num_tus, coeffs, pred):
@@ -339,6 +353,10 @@ class Job:
 
     def launch(self, dst_slot):
         _check(self.lib.hevcgpu_job_launch(self.h, dst_slot))
+
+    @property
+    def upload_bytes(self):
+        return int(self.lib.hevcgpu_job_upload_bytes(self.h))
 
     def free(self):
         if self.h:

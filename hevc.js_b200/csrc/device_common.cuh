@@ -1,0 +1,111 @@
+// device_common.cuh — device-side picture descriptors, tables and helpers shared by the
+// reconstruction kernels.
+#pragma once
+
+#include <cstdint>
+
+#include "hevcgpu.h"
+
+namespace hevcgpu {
+
+// ---------------------------------------------------------------------------------------
+// Per-picture descriptor.  Kernels take an array of these and work items that carry the
+// index of their picture, so one launch can serve one picture (plain form) or many
+// pictures of many streams (batched form).  All three planes of a picture buffer live in
+// one allocation: Cb at y + off_cb, Cr at y + off_cr, with row pitches pitch_y / pitch_c.
+// ---------------------------------------------------------------------------------------
+struct MotionEnt {           // 4x4 motion grid entry (PUMotionInfo, inter_prediction.h:16)
+    int16_t mv[2][2];
+    int8_t  ref[2];          // refIdxLX, -1 when predFlagLX is 0
+    int16_t pad;
+};
+
+struct PicDesc {
+    int32_t width, height;               // luma
+    int32_t pitch_y, pitch_c;
+    int64_t off_cb, off_cr;
+    uint8_t* rec;                        // reconstruction / deblocking buffer
+    uint8_t* dst;                        // DPB slot written by SAO
+    const uint8_t* ref[2][16];           // reference pictures by list entry (Y base)
+    int32_t num_ref[2];
+    int32_t ref_poc[2][16];
+    const hevc_tu_t* tus;
+    const int16_t* coeffs;
+    int16_t* resid;                      // residuals of coded intra TUs (at coeff_offset)
+    const hevc_pu_t* pus;
+    const hevc_wp_t* wp;
+    const uint32_t* blk;                 // (W/4)*(H/4)
+    MotionEnt* mot;                      // (W/4)*(H/4), built on the device from pus
+    const hevc_sao_t* sao;
+    const uint8_t* ctb_slice;            // may be null
+    const uint16_t* ctb_tile;            // may be null
+    const hevc_slice_t* slices;
+    const int32_t* intra_list;           // TU indices of intra TUs grouped by CTU and plane
+    const int32_t* intra_off;            // per CTU: 3 start offsets + next CTU's start
+    int32_t num_pus;
+    int32_t num_slices;
+    int32_t log2_ctb, wctb, hctb;
+    int32_t sao_enabled;
+    int32_t pcm_lf_disabled;
+    int32_t strong_intra;
+    int32_t intra_smoothing_disabled;
+    int32_t cb_qp_offset, cr_qp_offset;
+    int32_t tiles_check;                 // tiles enabled and no filtering across tiles
+    int32_t slice_check;                 // more than one slice in the picture
+};
+
+// Work items ----------------------------------------------------------------------------
+// Residual items are TU indices (int32), intra items CTU raster addresses (int32).
+struct McItem {       // one luma tile (<= 16x16) of one PU, plus its chroma tiles
+    int32_t pu;
+    uint8_t dx, dy;   // offset of the tile in the PU (luma samples)
+    uint8_t w, h;     // tile size (luma samples, multiples of 4)
+};
+
+// A launch covers up to MAX_SEGS pictures.  Segment k owns the blocks
+// [block0, next block0) of an item-list launch, or blockIdx.y == k of a per-picture
+// launch.  The table is a kernel parameter, so a batched launch needs no device-side
+// bookkeeping and is captured by value in a CUDA graph.
+constexpr int MAX_SEGS = 64;
+struct Seg {
+    const void* items;
+    const PicDesc* pic;
+    int32_t n_items;
+    int32_t block0;
+};
+struct SegTable {
+    int32_t n;
+    int32_t pad;
+    Seg s[MAX_SEGS];
+};
+
+__device__ __forceinline__ int find_seg(const SegTable& st, int b) {
+    int k = 0;
+    while (k + 1 < st.n && st.s[k + 1].block0 <= b) k++;
+    return k;
+}
+
+// Residual destinations.
+enum ResMode : int32_t {
+    RES_PACKED = 0,   // pred/out packed per TU at coeff_offset (config-1 form)
+    RES_PICTURE = 1,  // inter TUs: add to rec; intra TUs: int16 residual into resid
+};
+
+// Device status word bits (written with atomicOr; read by the host after a sync).
+enum : uint32_t {
+    ST_BAD_RECORD = 1u,   // a record pointed outside its picture; the item was skipped
+};
+
+__device__ __forceinline__ int clip3(int lo, int hi, int v) { return v < lo ? lo : (v > hi ? hi : v); }
+__device__ __forceinline__ int clip_u8(int v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
+
+// 8-bit z-order address of a 4x4 unit inside a CTU (bit-interleave of 4-bit x, y).
+__device__ __forceinline__ uint32_t zorder16(uint32_t bx, uint32_t by) {
+    bx = (bx | (bx << 2)) & 0x33u;
+    bx = (bx | (bx << 1)) & 0x55u;
+    by = (by | (by << 2)) & 0x33u;
+    by = (by | (by << 1)) & 0x55u;
+    return bx | (by << 1);
+}
+
+}  // namespace hevcgpu

@@ -1,0 +1,1074 @@
+// hevcgpu.cu — host side of the B200 reconstruction back end: context, pooled device
+// memory, DPB slots in HBM, picture jobs (validation, binning, per-CTU intra lists,
+// wavefront diagonals), launch sequencing, and the C ABI of include/hevcgpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "hevcgpu.h"
+#include "kernels.cuh"
+
+using namespace hevcgpu;
+
+// ---------------------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------------------
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (expr);                                                             \
+        if (e_ != cudaSuccess)                                                               \
+            return fail(HEVCGPU_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+struct Layout {  // pitched 8-bit 4:2:0 picture buffer
+    int32_t W = 0, H = 0, pitch_y = 0, pitch_c = 0;
+    int64_t off_cb = 0, off_cr = 0, bytes = 0;
+    void init(int w, int h) {
+        W = w;
+        H = h;
+        pitch_y = (int32_t)align_up(w, 64);
+        pitch_c = (int32_t)align_up(w / 2, 64);
+        off_cb = (int64_t)pitch_y * h;
+        off_cr = off_cb + (int64_t)pitch_c * (h / 2);
+        bytes = align_up(off_cr + (int64_t)pitch_c * (h / 2), 256);
+    }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// context and device memory pool
+// ---------------------------------------------------------------------------------------
+struct hevcgpu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = ~0ull;
+    uint64_t allocated = 0;       // bytes obtained from cudaMalloc (pooled or in use)
+    uint64_t launches = 0;
+    std::multimap<size_t, void*> free_blocks;
+    std::map<void*, size_t> sizes;
+    std::mutex mu;
+    // stage profiling
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    struct Mark { int stage; cudaEvent_t a, b; uint64_t launches; };
+    std::vector<Mark> marks;
+
+    cudaEvent_t next_event() {
+        if (ev_used == ev_pool.size()) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            ev_pool.push_back(e);
+        }
+        return ev_pool[ev_used++];
+    }
+
+    int alloc(void** p, size_t bytes) {
+        bytes = (size_t)align_up((int64_t)std::max<size_t>(bytes, 256), 4096);
+        std::lock_guard<std::mutex> g(mu);
+        auto it = free_blocks.lower_bound(bytes);
+        if (it != free_blocks.end() && it->first <= bytes * 2) {
+            *p = it->second;
+            free_blocks.erase(it);
+            return HEVCGPU_OK;
+        }
+        if (allocated + bytes > budget) {
+            // give pooled blocks back before refusing
+            for (auto& fb : free_blocks) {
+                cudaFree(fb.second);
+                allocated -= fb.first;
+                sizes.erase(fb.second);
+            }
+            free_blocks.clear();
+            if (allocated + bytes > budget)
+                return fail(HEVCGPU_ENOMEM, "HBM budget exceeded: %llu in use + %llu > %llu",
+                            (unsigned long long)allocated, (unsigned long long)bytes, (unsigned long long)budget);
+        }
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(HEVCGPU_ENOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+        }
+        allocated += bytes;
+        sizes[*p] = bytes;
+        return HEVCGPU_OK;
+    }
+    void release(void* p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> g(mu);
+        auto it = sizes.find(p);
+        if (it == sizes.end()) return;
+        free_blocks.emplace(it->second, p);
+    }
+    // pinned host staging pool (record images and picture descriptors)
+    std::multimap<size_t, void*> free_host;
+    std::map<void*, size_t> host_sizes;
+    int alloc_host(void** p, size_t bytes) {
+        bytes = (size_t)align_up((int64_t)std::max<size_t>(bytes, 4096), 65536);
+        std::lock_guard<std::mutex> g(mu);
+        auto it = free_host.lower_bound(bytes);
+        if (it != free_host.end() && it->first <= bytes * 2) {
+            *p = it->second;
+            free_host.erase(it);
+            return HEVCGPU_OK;
+        }
+        cudaError_t e = cudaHostAlloc(p, bytes, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(HEVCGPU_ENOMEM, "cudaHostAlloc(%zu): %s", bytes, cudaGetErrorString(e));
+        }
+        host_sizes[*p] = bytes;
+        return HEVCGPU_OK;
+    }
+    void release_host(void* p) {
+        if (!p) return;
+        std::lock_guard<std::mutex> g(mu);
+        auto it = host_sizes.find(p);
+        if (it != host_sizes.end()) free_host.emplace(it->second, p);
+    }
+    ~hevcgpu_ctx() {
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        for (auto& h : host_sizes) cudaFreeHost(h.first);
+        for (auto& s : sizes) cudaFree(s.first);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+struct DevBuf {  // pooled device buffer
+    hevcgpu_ctx* ctx = nullptr;
+    void* p = nullptr;
+    size_t n = 0;
+    int get(hevcgpu_ctx* c, size_t bytes) {
+        if (p && n >= bytes) return HEVCGPU_OK;
+        put();
+        ctx = c;
+        int rc = c->alloc(&p, bytes);
+        if (rc == HEVCGPU_OK) n = bytes;
+        return rc;
+    }
+    void put() {
+        if (p && ctx) ctx->release(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { put(); }
+};
+
+struct HostBuf {  // pooled pinned host buffer
+    hevcgpu_ctx* ctx = nullptr;
+    void* p = nullptr;
+    size_t n = 0;
+    int get(hevcgpu_ctx* c, size_t bytes) {
+        if (p && n >= bytes) return HEVCGPU_OK;
+        put();
+        ctx = c;
+        int rc = c->alloc_host(&p, bytes);
+        if (rc == HEVCGPU_OK) n = bytes;
+        return rc;
+    }
+    void put() {
+        if (p && ctx) ctx->release_host(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~HostBuf() { put(); }
+};
+
+}  // namespace
+
+struct hevcgpu_stream {
+    hevcgpu_ctx* ctx = nullptr;
+    Layout lay;
+    std::vector<DevBuf> slots;
+};
+
+// ---------------------------------------------------------------------------------------
+// jobs: one picture's records, prepared and uploaded
+// ---------------------------------------------------------------------------------------
+struct hevcgpu_job {
+    hevcgpu_ctx* ctx = nullptr;
+    hevcgpu_stream* st = nullptr;  // may be null for stage entry points
+    Layout lay;
+    DevBuf recs;      // all record arrays + work lists, one upload
+    DevBuf rec;       // reconstruction / deblocking buffer (pitched picture)
+    DevBuf scratch;   // resid (int16) + motion grid
+    DevBuf desc;      // PicDesc
+    HostBuf pin;      // pinned staging: the record image, then the PicDesc
+    size_t desc_off = 0;
+    cudaEvent_t desc_copied = nullptr;  // the last PicDesc upload has read the staging copy
+    PicDesc host_desc{};
+    int32_t n_res[4] = {0, 0, 0, 0};
+    const int32_t* d_res[4] = {nullptr, nullptr, nullptr, nullptr};
+    int32_t n_mc = 0;
+    const McItem* d_mc = nullptr;
+    std::vector<int32_t> diag_off;      // per diagonal: start in d_ctus (size D+1)
+    const int32_t* d_ctus = nullptr;
+    int32_t n_pus = 0;
+    int has_intra = 0;
+    int32_t dst_slot = -2;              // slot currently written into host_desc / desc
+    uint64_t upload_bytes = 0;          // host -> device bytes of the prepare call
+    hevc_pic_params_t params{};
+    ~hevcgpu_job() {
+        // buffers go back to the pools only after every queued use of them has run
+        if (ctx) cudaStreamSynchronize(ctx->stream);
+        if (desc_copied) cudaEventDestroy(desc_copied);
+    }
+};
+
+namespace {
+
+// Host image of a job's device records: offsets into one buffer.  A first pass with
+// out == nullptr only measures; the second pass writes into pinned staging memory.
+struct Packer {
+    uint8_t* out = nullptr;
+    size_t size = 0;
+    size_t add(const void* src, size_t bytes, size_t align = 256) {
+        size_t off = (size_t)align_up((int64_t)size, (int64_t)align);
+        size = off + bytes;
+        if (out && bytes && src) std::memcpy(out + off, src, bytes);
+        return off;
+    }
+};
+
+int validate(const hevc_picture_syntax_t* s, bool need_tus, bool need_pus, bool need_filters) {
+    if (!s) return fail(HEVCGPU_EINVAL, "null picture syntax");
+    const hevc_pic_params_t& p = s->params;
+    if (p.bit_depth != 8) return fail(HEVCGPU_EUNSUPPORTED, "bit depth %d (only 8 is supported)", p.bit_depth);
+    if (p.width <= 0 || p.height <= 0 || (p.width & 7) || (p.height & 7) || p.width > 8192 || p.height > 8192)
+        return fail(HEVCGPU_EINVAL, "picture size %dx%d (multiples of 8 up to 8192)", p.width, p.height);
+    if (p.log2_ctb < 4 || p.log2_ctb > 6) return fail(HEVCGPU_EUNSUPPORTED, "log2_ctb %d", p.log2_ctb);
+    if (p.log2_min_tb != 2) return fail(HEVCGPU_EUNSUPPORTED, "log2_min_tb %d (4x4 minimum TB)", p.log2_min_tb);
+    for (int l = 0; l < 2; l++)
+        if (p.num_ref[l] < 0 || p.num_ref[l] > 16) return fail(HEVCGPU_EINVAL, "num_ref[%d] = %d", l, p.num_ref[l]);
+    const int W = p.width, H = p.height;
+    if (need_tus) {
+        if (s->num_tus < 0 || (s->num_tus && !s->tus)) return fail(HEVCGPU_EINVAL, "bad TU array");
+        for (int i = 0; i < s->num_tus; i++) {
+            const hevc_tu_t& t = s->tus[i];
+            int n = 1 << t.log2_size, sub = t.c_idx ? 2 : 1;
+            if (t.log2_size < 2 || t.log2_size > 5 || t.c_idx > 2 || (t.x % n) || (t.y % n) ||
+                t.x + n > W / sub || t.y + n > H / sub)
+                return fail(HEVCGPU_EINVAL, "TU %d at (%d,%d) size %d comp %d is outside the picture or unaligned", i,
+                            t.x, t.y, n, t.c_idx);
+            if ((t.flags & HEVC_TU_INTRA) && t.intra_mode > 34)
+                return fail(HEVCGPU_EINVAL, "TU %d intra mode %d", i, t.intra_mode);
+            if (t.flags & HEVC_TU_CODED) {
+                if ((t.coeff_offset & 15) || (uint64_t)t.coeff_offset + (uint64_t)n * n > s->num_coeffs)
+                    return fail(HEVCGPU_EINVAL, "TU %d coeff_offset %u (multiple of 16, inside the pool)", i,
+                                t.coeff_offset);
+                if (t.qp > 51 + 48) return fail(HEVCGPU_EINVAL, "TU %d qp %d", i, t.qp);
+            }
+        }
+    }
+    if (need_pus) {
+        if (s->num_pus < 0 || (s->num_pus && !s->pus)) return fail(HEVCGPU_EINVAL, "bad PU array");
+        for (int i = 0; i < s->num_pus; i++) {
+            const hevc_pu_t& u = s->pus[i];
+            if (u.w < 4 || u.h < 4 || u.w > 64 || u.h > 64 || (u.w & 3) || (u.h & 3) || (u.x & 3) || (u.y & 3) ||
+                u.x + u.w > W || u.y + u.h > H)
+                return fail(HEVCGPU_EINVAL, "PU %d (%d,%d %dx%d) outside the picture", i, u.x, u.y, u.w, u.h);
+            if (u.ref_idx[0] < 0 && u.ref_idx[1] < 0) return fail(HEVCGPU_EINVAL, "PU %d uses no list", i);
+            for (int l = 0; l < 2; l++)
+                if (u.ref_idx[l] >= p.num_ref[l]) return fail(HEVCGPU_EINVAL, "PU %d refIdxL%d %d", i, l, u.ref_idx[l]);
+            if (u.wp >= s->num_wp) return fail(HEVCGPU_EINVAL, "PU %d WP row %d", i, u.wp);
+        }
+        for (int i = 0; i < s->num_wp; i++)
+            for (int c = 0; c < 2; c++)
+                if (s->wp[i].log2wd[c] < 1 || s->wp[i].log2wd[c] > 20)
+                    return fail(HEVCGPU_EINVAL, "WP row %d log2wd %d", i, s->wp[i].log2wd[c]);
+    }
+    if (need_filters) {
+        if (!s->blk) return fail(HEVCGPU_EINVAL, "missing 4x4 side-information grid");
+        if (!s->sao && p.sao_enabled) return fail(HEVCGPU_EINVAL, "missing SAO parameters");
+        if (s->num_slices < 1 || !s->slices) return fail(HEVCGPU_EINVAL, "missing slice parameters");
+        int ctb = 1 << p.log2_ctb;
+        int nctb = ((W + ctb - 1) / ctb) * ((H + ctb - 1) / ctb);
+        if (s->ctb_slice)
+            for (int a = 0; a < nctb; a++)
+                if (s->ctb_slice[a] >= s->num_slices) return fail(HEVCGPU_EINVAL, "CTB %d slice index", a);
+        if (s->sao)
+            for (int a = 0; a < nctb; a++)
+                for (int c = 0; c < 3; c++)
+                    if (s->sao[a].type[c] > 2 || s->sao[a].eo_class[c] > 3 || s->sao[a].band_pos[c] > 31)
+                        return fail(HEVCGPU_EINVAL, "CTB %d SAO parameters", a);
+    }
+    return HEVCGPU_OK;
+}
+
+enum StageMask : int {
+    ST_MC = 1,
+    ST_RESID = 2,
+    ST_INTRA = 4,
+    ST_DEBLOCK = 8,
+    ST_SAO = 16,
+    ST_ALL = 31,
+};
+
+// Build the host image, upload it and fill host_desc (except dst/ref pointers).
+int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
+    hevcgpu_ctx* ctx = j->ctx;
+    const hevc_pic_params_t& p = s->params;
+    j->params = p;
+    j->lay.init(p.width, p.height);
+    const int W = p.width, H = p.height, gw = W / 4, gh = H / 4;
+    const int ctb = 1 << p.log2_ctb;
+    const int wctb = (W + ctb - 1) / ctb, hctb = (H + ctb - 1) / ctb, nctb = wctb * hctb;
+
+    // residual bins (coded TUs by size), intra lists
+    std::vector<int32_t> bins[4];
+    std::vector<std::vector<int32_t>> per_ctu((size_t)nctb * 3);
+    for (int i = 0; i < s->num_tus; i++) {
+        const hevc_tu_t& t = s->tus[i];
+        bool intra = t.flags & HEVC_TU_INTRA;
+        if ((t.flags & HEVC_TU_CODED) && (stages & (intra ? ST_INTRA : ST_RESID))) bins[t.log2_size - 2].push_back(i);
+        if (intra && (stages & ST_INTRA)) {
+            int sub = t.c_idx ? 2 : 1;
+            int a = (t.y * sub / ctb) * wctb + (t.x * sub / ctb);
+            per_ctu[(size_t)a * 3 + t.c_idx].push_back(i);
+        }
+    }
+    std::vector<int32_t> intra_list, intra_off((size_t)nctb * 3 + 1, 0);
+    for (size_t k = 0; k < per_ctu.size(); k++) {
+        intra_off[k] = (int32_t)intra_list.size();
+        intra_list.insert(intra_list.end(), per_ctu[k].begin(), per_ctu[k].end());
+    }
+    intra_off[per_ctu.size()] = (int32_t)intra_list.size();
+    j->has_intra = !intra_list.empty();
+    // wavefront diagonals: CTU (rx, ry) on diagonal rx + 2*ry
+    int ndiag = wctb + 2 * (hctb - 1);
+    std::vector<int32_t> ctus;
+    j->diag_off.assign((size_t)ndiag + 1, 0);
+    for (int d = 0; d < ndiag; d++) {
+        j->diag_off[(size_t)d] = (int32_t)ctus.size();
+        for (int ry = 0; ry < hctb; ry++) {
+            int rx = d - 2 * ry;
+            if (rx < 0 || rx >= wctb) continue;
+            int a = ry * wctb + rx;
+            if (intra_off[(size_t)a * 3 + 3] > intra_off[(size_t)a * 3]) ctus.push_back(a);
+        }
+    }
+    j->diag_off[(size_t)ndiag] = (int32_t)ctus.size();
+    // MC tiles
+    std::vector<McItem> mc;
+    if (stages & ST_MC)
+        for (int i = 0; i < s->num_pus; i++) {
+            const hevc_pu_t& u = s->pus[i];
+            for (int dy = 0; dy < u.h; dy += 16)
+                for (int dx = 0; dx < u.w; dx += 16) {
+                    McItem m;
+                    m.pu = i;
+                    m.dx = (uint8_t)dx;
+                    m.dy = (uint8_t)dy;
+                    m.w = (uint8_t)std::min(16, u.w - dx);
+                    m.h = (uint8_t)std::min(16, u.h - dy);
+                    mc.push_back(m);
+                }
+        }
+    j->n_pus = s->num_pus;
+
+    size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc, o_il, o_io, o_ctus;
+    hevc_slice_t dflt{0, 0, 0, 1};
+    auto pack = [&](Packer& pk) {
+        o_tus = pk.add(s->tus, sizeof(hevc_tu_t) * (size_t)std::max(0, s->num_tus));
+        o_coef = pk.add(s->coeffs, sizeof(int16_t) * (size_t)s->num_coeffs);
+        o_pus = pk.add(s->pus, sizeof(hevc_pu_t) * (size_t)std::max(0, s->num_pus));
+        o_wp = pk.add(s->wp, sizeof(hevc_wp_t) * (size_t)std::max(0, s->num_wp));
+        o_blk = pk.add(s->blk, s->blk ? sizeof(uint32_t) * (size_t)gw * gh : 0);
+        o_sao = pk.add(s->sao, s->sao ? sizeof(hevc_sao_t) * (size_t)nctb : 0);
+        o_sl = pk.add(s->ctb_slice, s->ctb_slice ? (size_t)nctb : 0);
+        o_ti = pk.add(s->ctb_tile, s->ctb_tile ? sizeof(uint16_t) * (size_t)nctb : 0);
+        o_slices = s->num_slices > 0 && s->slices ? pk.add(s->slices, sizeof(hevc_slice_t) * (size_t)s->num_slices)
+                                                  : pk.add(&dflt, sizeof(dflt));
+        for (int k = 0; k < 4; k++) o_res[k] = pk.add(bins[k].data(), sizeof(int32_t) * bins[k].size());
+        o_mc = pk.add(mc.data(), sizeof(McItem) * mc.size());
+        o_il = pk.add(intra_list.data(), sizeof(int32_t) * intra_list.size());
+        o_io = pk.add(intra_off.data(), sizeof(int32_t) * intra_off.size());
+        o_ctus = pk.add(ctus.data(), sizeof(int32_t) * ctus.size());
+    };
+    Packer measure;
+    pack(measure);
+    const size_t img = std::max<size_t>(measure.size, 256);
+    j->desc_off = (size_t)align_up((int64_t)img, 256);
+    int rc = j->recs.get(ctx, img);
+    if (rc) return rc;
+    if ((rc = j->pin.get(ctx, j->desc_off + sizeof(PicDesc)))) return rc;
+    Packer write;
+    write.out = static_cast<uint8_t*>(j->pin.p);
+    pack(write);
+    CUDA_TRY(cudaMemcpyAsync(j->recs.p, j->pin.p, img, cudaMemcpyHostToDevice, ctx->stream));
+    j->upload_bytes = img + sizeof(PicDesc);
+    uint8_t* base = static_cast<uint8_t*>(j->recs.p);
+
+    size_t resid_bytes = j->has_intra ? sizeof(int16_t) * (size_t)align_up((int64_t)s->num_coeffs, 8) : 0;
+    size_t mot_bytes = (stages & ST_DEBLOCK) ? sizeof(MotionEnt) * (size_t)gw * gh : 0;
+    rc = j->scratch.get(ctx, std::max<size_t>(resid_bytes + mot_bytes, 256));
+    if (rc) return rc;
+    rc = j->desc.get(ctx, sizeof(PicDesc));
+    if (rc) return rc;
+
+    PicDesc& D = j->host_desc;
+    std::memset(&D, 0, sizeof(D));
+    D.width = W;
+    D.height = H;
+    D.pitch_y = j->lay.pitch_y;
+    D.pitch_c = j->lay.pitch_c;
+    D.off_cb = j->lay.off_cb;
+    D.off_cr = j->lay.off_cr;
+    for (int l = 0; l < 2; l++) {
+        D.num_ref[l] = p.num_ref[l];
+        for (int i = 0; i < 16; i++) D.ref_poc[l][i] = p.ref_poc[l][i];
+    }
+    D.tus = reinterpret_cast<const hevc_tu_t*>(base + o_tus);
+    D.coeffs = reinterpret_cast<const int16_t*>(base + o_coef);
+    D.resid = resid_bytes ? static_cast<int16_t*>(j->scratch.p) : nullptr;
+    D.pus = reinterpret_cast<const hevc_pu_t*>(base + o_pus);
+    D.wp = reinterpret_cast<const hevc_wp_t*>(base + o_wp);
+    D.blk = s->blk ? reinterpret_cast<const uint32_t*>(base + o_blk) : nullptr;
+    D.mot = mot_bytes ? reinterpret_cast<MotionEnt*>(static_cast<uint8_t*>(j->scratch.p) + resid_bytes) : nullptr;
+    D.sao = s->sao ? reinterpret_cast<const hevc_sao_t*>(base + o_sao) : nullptr;
+    D.ctb_slice = s->ctb_slice ? base + o_sl : nullptr;
+    D.ctb_tile = (s->ctb_tile && p.tiles_enabled) ? reinterpret_cast<const uint16_t*>(base + o_ti) : nullptr;
+    D.slices = reinterpret_cast<const hevc_slice_t*>(base + o_slices);
+    D.intra_list = reinterpret_cast<const int32_t*>(base + o_il);
+    D.intra_off = reinterpret_cast<const int32_t*>(base + o_io);
+    D.num_pus = s->num_pus;
+    D.num_slices = std::max(1, (int)s->num_slices);
+    D.log2_ctb = p.log2_ctb;
+    D.wctb = wctb;
+    D.hctb = hctb;
+    D.sao_enabled = p.sao_enabled && s->sao ? 1 : 0;
+    D.pcm_lf_disabled = p.pcm_loop_filter_disabled;
+    D.strong_intra = p.strong_intra_smoothing;
+    D.intra_smoothing_disabled = p.intra_smoothing_disabled;
+    D.cb_qp_offset = p.cb_qp_offset;
+    D.cr_qp_offset = p.cr_qp_offset;
+    D.tiles_check = (p.tiles_enabled && !p.loop_filter_across_tiles && s->ctb_tile) ? 1 : 0;
+    bool multi = false;
+    if (s->ctb_slice)
+        for (int a = 1; a < nctb && !multi; a++) multi = s->ctb_slice[a] != s->ctb_slice[0];
+    D.slice_check = multi ? 1 : 0;
+    for (int k = 0; k < 4; k++) {
+        j->n_res[k] = (int32_t)bins[k].size();
+        j->d_res[k] = reinterpret_cast<const int32_t*>(base + o_res[k]);
+    }
+    j->n_mc = (int32_t)mc.size();
+    j->d_mc = reinterpret_cast<const McItem*>(base + o_mc);
+    j->d_ctus = reinterpret_cast<const int32_t*>(base + o_ctus);
+    return HEVCGPU_OK;
+}
+
+// Point the job at its output and reference pictures and upload the descriptor.
+int job_bind(hevcgpu_job* j, uint8_t* rec, uint8_t* dst, const uint8_t* const refs[2][16]) {
+    PicDesc& D = j->host_desc;
+    D.rec = rec;
+    D.dst = dst;
+    for (int l = 0; l < 2; l++)
+        for (int i = 0; i < 16; i++) D.ref[l][i] = refs ? refs[l][i] : nullptr;
+    // the pinned staging copy may be rewritten only after its previous upload ran
+    if (j->desc_copied) {
+        CUDA_TRY(cudaEventSynchronize(j->desc_copied));
+    } else {
+        CUDA_TRY(cudaEventCreateWithFlags(&j->desc_copied, cudaEventDisableTiming));
+    }
+    uint8_t* stage = static_cast<uint8_t*>(j->pin.p) + j->desc_off;
+    std::memcpy(stage, &D, sizeof(PicDesc));
+    CUDA_TRY(cudaMemcpyAsync(j->desc.p, stage, sizeof(PicDesc), cudaMemcpyHostToDevice, j->ctx->stream));
+    CUDA_TRY(cudaEventRecord(j->desc_copied, j->ctx->stream));
+    return HEVCGPU_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// launch sequencing over a batch of jobs
+// ---------------------------------------------------------------------------------------
+struct Launcher {
+    hevcgpu_ctx* ctx;
+    cudaStream_t s;
+
+    template <typename K, typename... A>
+    int go(K kernel, dim3 grid, dim3 block, A... args) {
+        if (grid.x == 0 || grid.y == 0 || grid.z == 0) return HEVCGPU_OK;
+        kernel<<<grid, block, 0, s>>>(args...);
+        ctx->launches++;
+        CUDA_TRY(cudaGetLastError());
+        return HEVCGPU_OK;
+    }
+
+    // item-list launch over jobs[0..n): items_of(j) -> (ptr, count); per_block items per CTA
+    template <typename K, typename F, typename... A>
+    int items(K kernel, hevcgpu_job* const* jobs, int n, int per_block, int threads, F items_of, A... extra) {
+        for (int b0 = 0; b0 < n; b0 += MAX_SEGS) {
+            SegTable t;
+            std::memset(&t, 0, sizeof(t));
+            int blocks = 0;
+            for (int k = b0; k < std::min(n, b0 + MAX_SEGS); k++) {
+                const void* ptr;
+                int cnt;
+                items_of(jobs[k], ptr, cnt);
+                if (cnt <= 0) continue;
+                Seg& sg = t.s[t.n++];
+                sg.items = ptr;
+                sg.pic = static_cast<const PicDesc*>(jobs[k]->desc.p);
+                sg.n_items = cnt;
+                sg.block0 = blocks;
+                blocks += (cnt + per_block - 1) / per_block;
+            }
+            if (t.n == 0) continue;
+            int rc = go(kernel, dim3(blocks), dim3(threads), t, extra...);
+            if (rc) return rc;
+        }
+        return HEVCGPU_OK;
+    }
+
+    // per-picture launch: grid.y = picture; grid.x from blocks_of(job)
+    template <typename K, typename F>
+    int pictures(K kernel, hevcgpu_job* const* jobs, int n, int threads, int z, F blocks_of) {
+        for (int b0 = 0; b0 < n; b0 += MAX_SEGS) {
+            SegTable t;
+            std::memset(&t, 0, sizeof(t));
+            int bx = 0;
+            for (int k = b0; k < std::min(n, b0 + MAX_SEGS); k++) {
+                Seg& sg = t.s[t.n++];
+                sg.pic = static_cast<const PicDesc*>(jobs[k]->desc.p);
+                bx = std::max(bx, blocks_of(jobs[k]));
+            }
+            int rc = go(kernel, dim3(bx, t.n, z), dim3(threads), t);
+            if (rc) return rc;
+        }
+        return HEVCGPU_OK;
+    }
+};
+
+// Brackets one stage with profiling events when profiling is on.
+struct StageMark {
+    hevcgpu_ctx* ctx;
+    int stage;
+    cudaEvent_t a = nullptr;
+    uint64_t l0 = 0;
+    StageMark(hevcgpu_ctx* c, int s) : ctx(c), stage(s) {
+        if (!ctx->profiling) return;
+        a = ctx->next_event();
+        l0 = ctx->launches;
+        if (a) cudaEventRecord(a, ctx->stream);
+    }
+    ~StageMark() {
+        if (!ctx->profiling || !a) return;
+        cudaEvent_t b = ctx->next_event();
+        if (!b) return;
+        cudaEventRecord(b, ctx->stream);
+        ctx->marks.push_back({stage, a, b, ctx->launches - l0});
+    }
+};
+
+int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, int res_mode) {
+    Launcher L{ctx, ctx->stream};
+    int rc;
+    if (stages & ST_DEBLOCK) {
+        StageMark m(ctx, 0);
+        rc = L.pictures(k_motion_grid, jobs, n, 256, 1, [](hevcgpu_job* j) { return (j->n_pus * 32 + 255) / 256; });
+        if (rc) return rc;
+    }
+    if (stages & ST_MC) {
+        StageMark m(ctx, 1);
+        rc = L.items(k_mc, jobs, n, MC_WARPS, 32 * MC_WARPS, [](hevcgpu_job* j, const void*& p, int& c) {
+            p = j->d_mc;
+            c = j->n_mc;
+        });
+        if (rc) return rc;
+    }
+    if (stages & (ST_RESID | ST_INTRA)) {
+        StageMark m(ctx, 2);
+        void (*kr[4])(const SegTable, int) = {k_residual<2>, k_residual<3>, k_residual<4>, k_residual<5>};
+        for (int k = 0; k < 4; k++) {
+            rc = L.items(kr[k], jobs, n, 128 >> (k + 2), 128,
+                         [k](hevcgpu_job* j, const void*& p, int& c) {
+                             p = j->d_res[k];
+                             c = j->n_res[k];
+                         },
+                         res_mode);
+            if (rc) return rc;
+        }
+    }
+    if (stages & ST_INTRA) {
+        StageMark m(ctx, 3);
+        size_t nd = 0;
+        for (int k = 0; k < n; k++) nd = std::max(nd, jobs[k]->diag_off.size());
+        for (size_t d = 0; d + 1 < nd; d++) {
+            rc = L.items(k_intra_ctu, jobs, n, 1, 96, [d](hevcgpu_job* j, const void*& p, int& c) {
+                if (d + 1 >= j->diag_off.size()) { p = nullptr; c = 0; return; }
+                p = j->d_ctus + j->diag_off[d];
+                c = j->diag_off[d + 1] - j->diag_off[d];
+            });
+            if (rc) return rc;
+        }
+    }
+    if (stages & ST_DEBLOCK) {
+        {
+            StageMark m(ctx, 4);
+            rc = L.pictures(k_deblock<true>, jobs, n, 256, 1, [](hevcgpu_job* j) {
+                int segs = ((j->params.width + 7) / 8) * (j->params.height / 4);
+                return (segs + 255) / 256;
+            });
+            if (rc) return rc;
+        }
+        StageMark m(ctx, 5);
+        rc = L.pictures(k_deblock<false>, jobs, n, 256, 1, [](hevcgpu_job* j) {
+            int segs = (j->params.width / 4) * ((j->params.height + 7) / 8);
+            return (segs + 255) / 256;
+        });
+        if (rc) return rc;
+    }
+    if (stages & ST_SAO) {
+        StageMark m(ctx, 6);
+        rc = L.pictures(k_sao, jobs, n, 256, 3, [](hevcgpu_job* j) {
+            int groups = (j->params.width / 4) * j->params.height;
+            return (groups + 255) / 256;
+        });
+        if (rc) return rc;
+    }
+    return HEVCGPU_OK;
+}
+
+int upload_i420(hevcgpu_ctx* ctx, const Layout& L, uint8_t* dev, const uint8_t* host) {
+    const int W = L.W, H = L.H, cw = W / 2, ch = H / 2;
+    CUDA_TRY(cudaMemcpy2DAsync(dev, L.pitch_y, host, W, W, H, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpy2DAsync(dev + L.off_cb, L.pitch_c, host + (size_t)W * H, cw, cw, ch, cudaMemcpyHostToDevice,
+                               ctx->stream));
+    CUDA_TRY(cudaMemcpy2DAsync(dev + L.off_cr, L.pitch_c, host + (size_t)W * H + (size_t)cw * ch, cw, cw, ch,
+                               cudaMemcpyHostToDevice, ctx->stream));
+    return HEVCGPU_OK;
+}
+
+int download_i420(hevcgpu_ctx* ctx, const Layout& L, const uint8_t* dev, uint8_t* host) {
+    const int W = L.W, H = L.H, cw = W / 2, ch = H / 2;
+    CUDA_TRY(cudaMemcpy2DAsync(host, W, dev, L.pitch_y, W, H, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaMemcpy2DAsync(host + (size_t)W * H, cw, dev + L.off_cb, L.pitch_c, cw, ch, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+    CUDA_TRY(cudaMemcpy2DAsync(host + (size_t)W * H + (size_t)cw * ch, cw, dev + L.off_cr, L.pitch_c, cw, ch,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+    return HEVCGPU_OK;
+}
+
+int check_ctx(hevcgpu_ctx* ctx) {
+    if (!ctx) return fail(HEVCGPU_EINVAL, "null context");
+    CUDA_TRY(cudaSetDevice(ctx->device));
+    return HEVCGPU_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------
+extern "C" {
+
+int hevcgpu_abi_version(void) { return HEVCGPU_ABI_VERSION; }
+const char* hevcgpu_last_error(void) { return g_err.c_str(); }
+
+int hevcgpu_create(int device, hevcgpu_ctx_t** out) {
+    if (!out) return fail(HEVCGPU_EINVAL, "null out");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= device || device < 0)
+        return fail(HEVCGPU_ECUDA, "no CUDA device %d (%s)", device, e != cudaSuccess ? cudaGetErrorString(e) : "count");
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return fail(HEVCGPU_EUNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a", device,
+                    prop.major, prop.minor);
+    CUDA_TRY(cudaSetDevice(device));
+    auto* c = new (std::nothrow) hevcgpu_ctx();
+    if (!c) return fail(HEVCGPU_ENOMEM, "host allocation");
+    c->device = device;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(HEVCGPU_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return HEVCGPU_OK;
+}
+
+void hevcgpu_destroy(hevcgpu_ctx_t* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+}
+
+int hevcgpu_sync(hevcgpu_ctx_t* ctx) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return HEVCGPU_OK;
+}
+
+void* hevcgpu_cuda_stream(hevcgpu_ctx_t* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+uint64_t hevcgpu_launch_count(hevcgpu_ctx_t* ctx) { return ctx ? ctx->launches : 0; }
+
+int hevcgpu_set_budget(hevcgpu_ctx_t* ctx, uint64_t bytes) {
+    if (!ctx) return fail(HEVCGPU_EINVAL, "null context");
+    ctx->budget = bytes ? bytes : ~0ull;
+    return HEVCGPU_OK;
+}
+uint64_t hevcgpu_bytes_in_use(hevcgpu_ctx_t* ctx) { return ctx ? ctx->allocated : 0; }
+
+// ---- stage entry points -------------------------------------------------------------
+
+int hevcgpu_residual_blocks(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int32_t num_tus, const int16_t* coeffs,
+                            uint64_t num_coeffs, const uint8_t* pred, uint8_t* out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (num_tus < 0 || (num_tus && (!tus || !coeffs || !pred || !out)))
+        return fail(HEVCGPU_EINVAL, "null arrays");
+    if (num_tus == 0) return HEVCGPU_OK;
+    for (int i = 0; i < num_tus; i++) {
+        const hevc_tu_t& t = tus[i];
+        int n = 1 << t.log2_size;
+        if (t.log2_size < 2 || t.log2_size > 5 || t.c_idx > 2 || (t.coeff_offset & 15) ||
+            (uint64_t)t.coeff_offset + (uint64_t)n * n > num_coeffs || t.qp > 99)
+            return fail(HEVCGPU_EINVAL, "block %d: size %d, coeff_offset %u (multiple of 16 inside the pool)", i, n,
+                        t.coeff_offset);
+    }
+    hevcgpu_job j;
+    j.ctx = ctx;
+    std::vector<int32_t> bins[4];
+    for (int i = 0; i < num_tus; i++) bins[tus[i].log2_size - 2].push_back(i);
+    size_t o_tus, o_coef, o_pred, o_out, o_res[4];
+    auto pack = [&](Packer& pk) {
+        o_tus = pk.add(tus, sizeof(hevc_tu_t) * (size_t)num_tus);
+        o_coef = pk.add(coeffs, sizeof(int16_t) * (size_t)num_coeffs);
+        o_pred = pk.add(pred, (size_t)num_coeffs);
+        o_out = pk.add(nullptr, (size_t)num_coeffs);
+        for (int k = 0; k < 4; k++) o_res[k] = pk.add(bins[k].data(), sizeof(int32_t) * bins[k].size());
+    };
+    Packer measure;
+    pack(measure);
+    const size_t img = measure.size;
+    j.desc_off = (size_t)align_up((int64_t)img, 256);
+    if ((rc = j.recs.get(ctx, img)) || (rc = j.desc.get(ctx, sizeof(PicDesc))) ||
+        (rc = j.pin.get(ctx, j.desc_off + sizeof(PicDesc))))
+        return rc;
+    Packer write;
+    write.out = static_cast<uint8_t*>(j.pin.p);
+    pack(write);
+    uint8_t* base = static_cast<uint8_t*>(j.recs.p);
+    PicDesc& D = j.host_desc;
+    std::memset(&D, 0, sizeof(D));
+    D.tus = reinterpret_cast<const hevc_tu_t*>(base + o_tus);
+    D.coeffs = reinterpret_cast<const int16_t*>(base + o_coef);
+    D.rec = base + o_pred;
+    D.dst = base + o_out;
+    for (int k = 0; k < 4; k++) {
+        j.n_res[k] = (int32_t)bins[k].size();
+        j.d_res[k] = reinterpret_cast<const int32_t*>(base + o_res[k]);
+    }
+    CUDA_TRY(cudaMemcpyAsync(j.recs.p, j.pin.p, img, cudaMemcpyHostToDevice, ctx->stream));
+    std::memcpy(static_cast<uint8_t*>(j.pin.p) + j.desc_off, &D, sizeof(D));
+    CUDA_TRY(cudaMemcpyAsync(j.desc.p, static_cast<uint8_t*>(j.pin.p) + j.desc_off, sizeof(D),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    hevcgpu_job* jp = &j;
+    if ((rc = run_stages(ctx, &jp, 1, ST_RESID, RES_PACKED))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(out, base + o_out, (size_t)num_coeffs, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return HEVCGPU_OK;
+}
+
+namespace {
+
+// Shared body of the picture-level stage entry points on host memory.
+int run_host_picture(hevcgpu_ctx* ctx, const hevc_picture_syntax_t* syn, int stages, const uint8_t* in,
+                     const uint8_t* const* refs, int num_refs, uint8_t* out) {
+    hevcgpu_job j;
+    j.ctx = ctx;
+    int rc = job_build(&j, syn, stages);
+    if (rc) return rc;
+    const Layout& L = j.lay;
+    std::vector<DevBuf> ref_bufs((size_t)std::max(0, num_refs));
+    const uint8_t* ref_ptrs[2][16] = {};
+    for (int l = 0; l < 2; l++)
+        for (int i = 0; i < syn->params.num_ref[l]; i++) {
+            int slot = syn->params.ref_slot[l][i];
+            if (!(stages & ST_MC)) continue;
+            if (slot < 0 || slot >= num_refs || !refs || !refs[slot])
+                return fail(HEVCGPU_EINVAL, "reference list %d entry %d names slot %d (have %d)", l, i, slot, num_refs);
+            DevBuf& b = ref_bufs[(size_t)slot];
+            if (!b.p) {
+                if ((rc = b.get(ctx, (size_t)L.bytes))) return rc;
+                if ((rc = upload_i420(ctx, L, static_cast<uint8_t*>(b.p), refs[slot]))) return rc;
+            }
+            ref_ptrs[l][i] = static_cast<const uint8_t*>(b.p);
+        }
+    DevBuf dst;
+    if ((rc = j.rec.get(ctx, (size_t)L.bytes)) || (rc = dst.get(ctx, (size_t)L.bytes))) return rc;
+    if (in) {
+        if ((rc = upload_i420(ctx, L, static_cast<uint8_t*>(j.rec.p), in))) return rc;
+    } else {
+        CUDA_TRY(cudaMemsetAsync(j.rec.p, 0, (size_t)L.bytes, ctx->stream));
+    }
+    if ((rc = job_bind(&j, static_cast<uint8_t*>(j.rec.p), static_cast<uint8_t*>(dst.p), ref_ptrs))) return rc;
+    hevcgpu_job* jp = &j;
+    if ((rc = run_stages(ctx, &jp, 1, stages, RES_PICTURE))) return rc;
+    const uint8_t* result = (stages & ST_SAO) ? static_cast<uint8_t*>(dst.p) : static_cast<uint8_t*>(j.rec.p);
+    if ((rc = download_i420(ctx, L, result, out))) return rc;
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return HEVCGPU_OK;
+}
+
+}  // namespace
+
+int hevcgpu_inter_pred(hevcgpu_ctx_t* ctx, const hevc_pic_params_t* params, const hevc_pu_t* pus, int32_t num_pus,
+                       const hevc_wp_t* wp, int32_t num_wp, const uint8_t* const* refs, int32_t num_refs,
+                       uint8_t* out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!params || !out) return fail(HEVCGPU_EINVAL, "null arguments");
+    hevc_picture_syntax_t s;
+    std::memset(&s, 0, sizeof(s));
+    s.params = *params;
+    s.num_pus = num_pus;
+    s.pus = pus;
+    s.num_wp = num_wp;
+    s.wp = wp;
+    if ((rc = validate(&s, false, true, false))) return rc;
+    return run_host_picture(ctx, &s, ST_MC, nullptr, refs, num_refs, out);
+}
+
+int hevcgpu_loop_filter(hevcgpu_ctx_t* ctx, const hevc_picture_syntax_t* syn, const uint8_t* in, uint8_t* out,
+                        int do_deblock, int do_sao) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!in || !out) return fail(HEVCGPU_EINVAL, "null planes");
+    if ((rc = validate(syn, false, true, true))) return rc;
+    int stages = (do_deblock ? ST_DEBLOCK : 0) | ST_SAO;
+    hevc_picture_syntax_t s = *syn;
+    if (!do_sao) s.params.sao_enabled = 0;  // the SAO pass then only copies
+    return run_host_picture(ctx, &s, stages, in, nullptr, 0, out);
+}
+
+int hevcgpu_intra_recon(hevcgpu_ctx_t* ctx, const hevc_picture_syntax_t* syn, const uint8_t* in, uint8_t* out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!in || !out) return fail(HEVCGPU_EINVAL, "null planes");
+    if ((rc = validate(syn, true, false, false))) return rc;
+    return run_host_picture(ctx, syn, ST_INTRA, in, nullptr, 0, out);
+}
+
+int hevcgpu_reconstruct_picture(hevcgpu_ctx_t* ctx, const hevc_picture_syntax_t* syn, const uint8_t* const* refs,
+                                int32_t num_refs, uint8_t* out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out) return fail(HEVCGPU_EINVAL, "null output");
+    if ((rc = validate(syn, true, true, true))) return rc;
+    return run_host_picture(ctx, syn, ST_ALL, nullptr, refs, num_refs, out);
+}
+
+// ---- DPB / picture pipeline ----------------------------------------------------------
+
+int hevcgpu_stream_open(hevcgpu_ctx_t* ctx, int32_t width, int32_t height, int32_t bit_depth, int32_t num_slots,
+                        hevcgpu_stream_t** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out) return fail(HEVCGPU_EINVAL, "null out");
+    *out = nullptr;
+    if (bit_depth != 8) return fail(HEVCGPU_EUNSUPPORTED, "bit depth %d", bit_depth);
+    if (width <= 0 || height <= 0 || (width & 7) || (height & 7) || num_slots <= 0 || num_slots > 64)
+        return fail(HEVCGPU_EINVAL, "stream %dx%d with %d slots", width, height, num_slots);
+    auto* st = new (std::nothrow) hevcgpu_stream();
+    if (!st) return fail(HEVCGPU_ENOMEM, "host allocation");
+    st->ctx = ctx;
+    st->lay.init(width, height);
+    st->slots.resize((size_t)num_slots);
+    for (auto& b : st->slots) {
+        if ((rc = b.get(ctx, (size_t)st->lay.bytes))) {
+            delete st;
+            return rc;
+        }
+    }
+    *out = st;
+    return HEVCGPU_OK;
+}
+
+void hevcgpu_stream_close(hevcgpu_stream_t* st) {
+    if (!st) return;
+    cudaStreamSynchronize(st->ctx->stream);
+    delete st;
+}
+
+int hevcgpu_slot_upload(hevcgpu_stream_t* st, int32_t slot, const uint8_t* i420) {
+    if (!st || !i420 || slot < 0 || slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);
+    int rc = upload_i420(st->ctx, st->lay, static_cast<uint8_t*>(st->slots[(size_t)slot].p), i420);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(st->ctx->stream));
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_slot_download(hevcgpu_stream_t* st, int32_t slot, uint8_t* i420) {
+    if (!st || !i420 || slot < 0 || slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);
+    int rc = download_i420(st->ctx, st->lay, static_cast<uint8_t*>(st->slots[(size_t)slot].p), i420);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(st->ctx->stream));
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void** cb, void** cr, int32_t* pitch_y,
+                            int32_t* pitch_c) {
+    if (!st || slot < 0 || slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);
+    uint8_t* b = static_cast<uint8_t*>(st->slots[(size_t)slot].p);
+    if (y) *y = b;
+    if (cb) *cb = b + st->lay.off_cb;
+    if (cr) *cr = b + st->lay.off_cr;
+    if (pitch_y) *pitch_y = st->lay.pitch_y;
+    if (pitch_c) *pitch_c = st->lay.pitch_c;
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, hevcgpu_job_t** out) {
+    if (!st || !out) return fail(HEVCGPU_EINVAL, "null arguments");
+    *out = nullptr;
+    int rc = check_ctx(st->ctx);
+    if (rc) return rc;
+    if ((rc = validate(syn, true, true, true))) return rc;
+    if (syn->params.width != st->lay.W || syn->params.height != st->lay.H)
+        return fail(HEVCGPU_EINVAL, "picture %dx%d on a %dx%d stream", syn->params.width, syn->params.height,
+                    st->lay.W, st->lay.H);
+    for (int l = 0; l < 2; l++)
+        for (int i = 0; i < syn->params.num_ref[l]; i++) {
+            int s = syn->params.ref_slot[l][i];
+            if (s < 0 || s >= (int)st->slots.size())
+                return fail(HEVCGPU_EINVAL, "reference list %d entry %d names slot %d", l, i, s);
+        }
+    auto* j = new (std::nothrow) hevcgpu_job();
+    if (!j) return fail(HEVCGPU_ENOMEM, "host allocation");
+    j->ctx = st->ctx;
+    j->st = st;
+    if ((rc = job_build(j, syn, ST_ALL)) || (rc = j->rec.get(st->ctx, (size_t)j->lay.bytes))) {
+        delete j;
+        return rc;
+    }
+    *out = j;
+    return HEVCGPU_OK;
+}
+
+uint64_t hevcgpu_job_upload_bytes(hevcgpu_job_t* job) { return job ? job->upload_bytes : 0; }
+
+void hevcgpu_job_free(hevcgpu_job_t* job) {
+    if (!job) return;
+    cudaStreamSynchronize(job->ctx->stream);
+    delete job;
+}
+
+namespace {
+int job_target(hevcgpu_job* j, int32_t dst_slot) {
+    hevcgpu_stream* st = j->st;
+    if (!st) return fail(HEVCGPU_EINVAL, "job has no stream");
+    if (dst_slot < 0 || dst_slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", dst_slot);
+    for (int l = 0; l < 2; l++)
+        for (int i = 0; i < j->params.num_ref[l]; i++)
+            if (j->params.ref_slot[l][i] == dst_slot)
+                return fail(HEVCGPU_EINVAL, "slot %d is both a reference and the destination", dst_slot);
+    if (j->dst_slot == dst_slot) return HEVCGPU_OK;
+    const uint8_t* refs[2][16] = {};
+    for (int l = 0; l < 2; l++)
+        for (int i = 0; i < j->params.num_ref[l]; i++)
+            refs[l][i] = static_cast<const uint8_t*>(st->slots[(size_t)j->params.ref_slot[l][i]].p);
+    int rc = job_bind(j, static_cast<uint8_t*>(j->rec.p), static_cast<uint8_t*>(st->slots[(size_t)dst_slot].p), refs);
+    if (rc) return rc;
+    j->dst_slot = dst_slot;
+    return HEVCGPU_OK;
+}
+}  // namespace
+
+int hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot) {
+    if (!job) return fail(HEVCGPU_EINVAL, "null job");
+    int rc = job_target(job, dst_slot);
+    if (rc) return rc;
+    hevcgpu_job* jp = job;
+    return run_stages(job->ctx, &jp, 1, ST_ALL, RES_PICTURE);
+}
+
+int hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, int32_t n) {
+    if (!jobs || !dst_slots || n <= 0) return fail(HEVCGPU_EINVAL, "empty batch");
+    hevcgpu_ctx* ctx = jobs[0]->ctx;
+    for (int k = 0; k < n; k++) {
+        if (!jobs[k] || jobs[k]->ctx != ctx) return fail(HEVCGPU_EINVAL, "batch mixes contexts");
+        int rc = job_target(jobs[k], dst_slots[k]);
+        if (rc) return rc;
+    }
+    return run_stages(ctx, jobs, n, ST_ALL, RES_PICTURE);
+}
+
+int hevcgpu_stream_sync(hevcgpu_stream_t* st) {
+    if (!st) return fail(HEVCGPU_EINVAL, "null stream");
+    CUDA_TRY(cudaStreamSynchronize(st->ctx->stream));
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_profile_enable(hevcgpu_ctx_t* ctx, int enable) {
+    if (!ctx) return fail(HEVCGPU_EINVAL, "null context");
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    ctx->profiling = enable != 0;
+    ctx->marks.clear();
+    ctx->ev_used = 0;
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_profile_read(hevcgpu_ctx_t* ctx, double* ms, uint64_t* launches) {
+    if (!ctx) return fail(HEVCGPU_EINVAL, "null context");
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < HEVCGPU_NUM_STAGES; k++) {
+        if (ms) ms[k] = 0;
+        if (launches) launches[k] = 0;
+    }
+    for (auto& m : ctx->marks) {
+        float t = 0;
+        CUDA_TRY(cudaEventElapsedTime(&t, m.a, m.b));
+        if (ms) ms[m.stage] += t;
+        if (launches) launches[m.stage] += m.launches;
+    }
+    ctx->marks.clear();
+    ctx->ev_used = 0;
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_picture_decode(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, int32_t dst_slot) {
+    hevcgpu_job_t* j = nullptr;
+    int rc = hevcgpu_job_prepare(st, syn, &j);
+    if (rc) return rc;
+    rc = hevcgpu_job_launch(j, dst_slot);
+    if (rc == HEVCGPU_OK) {
+        cudaError_t e = cudaStreamSynchronize(st->ctx->stream);
+        if (e != cudaSuccess) rc = fail(HEVCGPU_ECUDA, "picture decode: %s", cudaGetErrorString(e));
+    }
+    hevcgpu_job_free(j);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,928 @@
+// kernels.cuh — the reconstruction kernels (sm_100a).
+//
+//   k_residual<LOG2>  dequant + inverse DST/DCT + add-and-clip of coded TUs
+//                     (transform.cpp:293-394, coding_tree.cpp:371-396)
+//   k_mc              8-tap/4-tap interpolation + default/explicit weighting
+//                     (interpolation.cpp:45-411)
+//   k_intra_ctu       intra prediction of the intra TUs of one CTU per CTA, CTUs of one
+//                     wavefront diagonal per launch (intra_prediction.cpp:44-481)
+//   k_motion_grid     4x4 motion grid of the PUs (store_pu_motion's grid)
+//   k_deblock<V>      Bs + decisions + luma/chroma filters of one edge direction
+//                     (deblocking.cpp:50-614)
+//   k_sao             band/edge offset from the deblocked picture into the DPB slot
+//                     (sao.cpp:20-243)
+#pragma once
+
+#include "device_common.cuh"
+
+namespace hevcgpu {
+
+// ======================================================================================
+// Inverse transform.  The N-point inverse DCT is computed by the even/odd recursion of
+// the HEVC basis: out[k] = E[k] + O[k], out[N-1-k] = E[k] - O[k], with E the N/2-point
+// inverse of the even inputs and O[k] the odd-input dot products.  The basis entries
+// are integer cosines of pi*i*(2k+1)/64 (H.265 eq. 8-315); cos_mag lists the 33
+// magnitudes for angles 0..pi/2 and every coefficient below is a compile-time constant.
+// Integer sums are exact, so any summation order reproduces the reference's butterflies.
+// ======================================================================================
+__host__ __device__ constexpr int cos_mag(int m) {
+    constexpr int t[33] = {64, 90, 90, 90, 89, 88, 87, 85, 83, 82, 80, 78, 75, 73, 70, 67, 64,
+                           61, 57, 54, 50, 46, 43, 38, 36, 31, 25, 22, 18, 13, 9,  4,  0};
+    return t[m];
+}
+__host__ __device__ constexpr int cos_entry(int m) {
+    return (m & 127) <= 32 ? cos_mag(m & 127)
+           : (m & 127) <= 64 ? -cos_mag(64 - (m & 127))
+           : (m & 127) <= 96 ? -cos_mag((m & 127) - 64)
+                             : cos_mag(128 - (m & 127));
+}
+// weight of input n in output k of the N-point inverse DCT
+template <int N>
+__host__ __device__ constexpr int dct_w(int n, int k) { return cos_entry(n * (32 / N) * (2 * k + 1)); }
+
+template <int N>
+__device__ __forceinline__ void idct_1d(const int* src, int* dst) {
+    if constexpr (N == 2) {
+        dst[0] = 64 * src[0] + 64 * src[1];
+        dst[1] = 64 * src[0] - 64 * src[1];
+    } else {
+        int ev[N / 2], E[N / 2];
+#pragma unroll
+        for (int n = 0; n < N / 2; n++) ev[n] = src[2 * n];
+        idct_1d<N / 2>(ev, E);
+#pragma unroll
+        for (int k = 0; k < N / 2; k++) {
+            int o = 0;
+#pragma unroll
+            for (int n = 0; n < N / 2; n++) o += dct_w<N>(2 * n + 1, k) * src[2 * n + 1];
+            dst[k] = E[k] + o;
+            dst[N - 1 - k] = E[k] - o;
+        }
+    }
+}
+
+// DST-VII 4x4 (transform.cpp:22-43): out[k] = sum_n D[n][k] * src[n]
+__device__ __forceinline__ void idst4_1d(const int* s, int* d) {
+    d[0] = 29 * s[0] + 74 * s[1] + 84 * s[2] + 55 * s[3];
+    d[1] = 55 * s[0] + 74 * s[1] - 29 * s[2] - 84 * s[3];
+    d[2] = 74 * s[0] - 74 * s[2] + 74 * s[3];
+    d[3] = 84 * s[0] - 74 * s[1] + 55 * s[2] - 29 * s[3];
+}
+
+template <int N>
+__device__ __forceinline__ void inv_1d(const int* s, int* d, bool dst4) {
+    if constexpr (N == 4) {
+        if (dst4) { idst4_1d(s, d); return; }
+    }
+    idct_1d<N>(s, d);
+}
+
+// Flat-scaling dequantisation of one level (transform.cpp:360-365): int64 product,
+// rounding shift, narrowing to int (modulo 2^32), int16 clip.
+__device__ __forceinline__ int16_t dequant1(int c, int scale, int qp_per, int bd_shift) {
+    if (c == 0) return 0;
+    long long v = (long long)(c * 16 * scale);
+    v = v * (1ll << qp_per) + (1ll << (bd_shift - 1));
+    v >>= bd_shift;
+    return (int16_t)clip3(-32768, 32767, (int)(unsigned)(unsigned long long)v);
+}
+
+__constant__ int c_level_scale[6] = {40, 45, 51, 57, 64, 72};
+
+// Residual kernel: N threads per TU (thread j owns column j in the first pass and row j
+// in the second), 128 threads per CTA.  Coefficients are staged through shared memory;
+// the intermediate has a padded row pitch (N + 2 int16) so that row reads by different
+// threads hit distinct banks.
+template <int LOG2>
+__global__ void __launch_bounds__(128) k_residual(const __grid_constant__ SegTable st, int mode) {
+    constexpr int N = 1 << LOG2;
+    constexpr int TUS = 128 / N;
+    constexpr int TP = N + 2;
+    __shared__ __align__(16) int16_t s_coef[TUS][N * N];
+    __shared__ int16_t s_tmp[TUS][N * TP];
+
+    const int slot = threadIdx.x / N;
+    const int j = threadIdx.x % N;
+    const Seg& sg = st.s[find_seg(st, blockIdx.x)];
+    const int item = (blockIdx.x - sg.block0) * TUS + slot;
+    const bool live = item < sg.n_items;
+    const PicDesc& P = *sg.pic;
+    hevc_tu_t t = live ? P.tus[static_cast<const int32_t*>(sg.items)[item]] : hevc_tu_t{};
+    const bool bypass = t.flags & HEVC_TU_BYPASS;
+    const bool tskip = (t.flags & HEVC_TU_TSKIP) && !bypass;
+    const bool dst4 = (LOG2 == 2) && (t.flags & HEVC_TU_INTRA) && t.c_idx == 0;
+
+    // load row j of the levels and dequantise it
+    if (live) {
+        const int16_t* src = P.coeffs + t.coeff_offset + j * N;
+        int16_t v[N];
+        if constexpr (N >= 8) {
+#pragma unroll
+            for (int q = 0; q < N / 8; q++) {
+                int4 w = reinterpret_cast<const int4*>(src)[q];
+                *reinterpret_cast<int4*>(&v[q * 8]) = w;
+            }
+        } else {
+            int2 w = *reinterpret_cast<const int2*>(src);
+            *reinterpret_cast<int2*>(&v[0]) = w;
+        }
+        if (!bypass) {
+            int scale = c_level_scale[t.qp % 6], qp_per = t.qp / 6, bd_shift = 8 + LOG2 - 5;
+#pragma unroll
+            for (int i = 0; i < N; i++) v[i] = dequant1(v[i], scale, qp_per, bd_shift);
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) s_coef[slot][j * N + i] = v[i];
+    }
+    __syncthreads();
+
+    // first pass: column j, shift 7, int16 clip
+    if (live && !tskip && !bypass) {
+        int s[N], d[N];
+#pragma unroll
+        for (int n = 0; n < N; n++) s[n] = s_coef[slot][n * N + j];
+        inv_1d<N>(s, d, dst4);
+#pragma unroll
+        for (int k = 0; k < N; k++) s_tmp[slot][k * TP + j] = (int16_t)clip3(-32768, 32767, (d[k] + 64) >> 7);
+    }
+    __syncthreads();
+    if (!live) return;
+
+    // second pass: row j, shift 12 (20 - BitDepth), int16 clip
+    int r[N];
+    if (bypass) {
+#pragma unroll
+        for (int k = 0; k < N; k++) r[k] = s_coef[slot][j * N + k];
+    } else if (tskip) {
+#pragma unroll
+        for (int k = 0; k < N; k++) r[k] = (s_coef[slot][j * N + k] + 64) >> 7;
+    } else {
+        int s[N], d[N];
+#pragma unroll
+        for (int n = 0; n < N; n++) s[n] = s_tmp[slot][j * TP + n];
+        inv_1d<N>(s, d, dst4);
+#pragma unroll
+        for (int k = 0; k < N; k++) r[k] = clip3(-32768, 32767, (d[k] + 2048) >> 12);
+    }
+
+    if (mode == RES_PICTURE && (t.flags & HEVC_TU_INTRA)) {
+        // residual of an intra TU: the wavefront adds it to its prediction
+        int16_t* dst = P.resid + t.coeff_offset + j * N;
+#pragma unroll
+        for (int k = 0; k < N; k++) dst[k] = (int16_t)r[k];
+        return;
+    }
+    const uint8_t* pred;
+    uint8_t* out;
+    if (mode == RES_PACKED) {
+        pred = P.rec + t.coeff_offset + j * N;
+        out = P.dst + t.coeff_offset + j * N;
+    } else {
+        int pitch = t.c_idx ? P.pitch_c : P.pitch_y;
+        int64_t base = t.c_idx == 0 ? 0 : (t.c_idx == 1 ? P.off_cb : P.off_cr);
+        out = P.rec + base + (int64_t)(t.y + j) * pitch + t.x;
+        pred = out;
+    }
+    // add the prediction row and clip (reconstruct_block)
+    if constexpr (N >= 16) {
+#pragma unroll
+        for (int q = 0; q < N / 16; q++) {
+            uint4 pv = reinterpret_cast<const uint4*>(pred)[q];
+            const uint8_t* pb = reinterpret_cast<const uint8_t*>(&pv);
+            uint4 ov;
+            uint8_t* ob = reinterpret_cast<uint8_t*>(&ov);
+#pragma unroll
+            for (int i = 0; i < 16; i++) ob[i] = (uint8_t)clip_u8(pb[i] + r[q * 16 + i]);
+            reinterpret_cast<uint4*>(out)[q] = ov;
+        }
+    } else if constexpr (N == 8) {
+        uint2 pv = *reinterpret_cast<const uint2*>(pred);
+        const uint8_t* pb = reinterpret_cast<const uint8_t*>(&pv);
+        uint2 ov;
+        uint8_t* ob = reinterpret_cast<uint8_t*>(&ov);
+#pragma unroll
+        for (int i = 0; i < 8; i++) ob[i] = (uint8_t)clip_u8(pb[i] + r[i]);
+        *reinterpret_cast<uint2*>(out) = ov;
+    } else {
+        uint32_t pv = *reinterpret_cast<const uint32_t*>(pred);
+        uint32_t ov = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) ov |= (uint32_t)clip_u8((int)((pv >> (8 * i)) & 0xFF) + r[i]) << (8 * i);
+        *reinterpret_cast<uint32_t*>(out) = ov;
+    }
+}
+
+// ======================================================================================
+// Motion compensation.  One warp per McItem: a luma tile of at most 16x16 of one PU and
+// its two 4:2:0 chroma tiles.  Per list the (w+7)x(h+7) luma and (w/2+3)x(h/2+3) chroma
+// reference windows are staged in shared memory with edge-clamped coordinates (the
+// reference's refClamp), filtered horizontally into an int16 intermediate and then
+// vertically; the final weighting writes 8-bit samples into the reconstruction buffer.
+// ======================================================================================
+__constant__ int8_t c_luma_taps[4][8] = {{0, 0, 0, 64, 0, 0, 0, 0},
+                                         {-1, 4, -10, 58, 17, -5, 1, 0},
+                                         {-1, 4, -11, 40, 40, -11, 4, -1},
+                                         {0, 1, -5, 17, 58, -10, 4, -1}};
+__constant__ int8_t c_chroma_taps[8][4] = {{0, 64, 0, 0},    {-2, 58, 10, -2}, {-4, 54, 16, -2},
+                                           {-6, 46, 28, -4}, {-4, 36, 36, -4}, {-4, 28, 46, -6},
+                                           {-2, 16, 54, -4}, {-2, 10, 58, -2}};
+
+constexpr int MC_WARPS = 8;
+constexpr int MC_WIN = 24 * 23;   // luma window, pitch 24
+constexpr int MC_TMP = 23 * 16;   // luma intermediate
+
+struct McSmem {
+    uint8_t win[MC_WIN];
+    int16_t tmp[MC_TMP];
+    uint8_t cwin[2][12 * 11];
+    int16_t ctmp[11 * 8];
+};
+
+// One component, one list: NT-tap prediction of a bw x bh block at (xi, yi) integer
+// position with fractions (fx, fy) into per-lane registers pred[k] for the elements
+// e = lane + 32k (row-major in the block).
+template <int NT, int MAXE>
+__device__ __forceinline__ void mc_block(const uint8_t* __restrict__ plane, int pitch, int pw, int ph, int xi,
+                                         int yi, int fx, int fy, int bw, int bh, uint8_t* win, int wpitch,
+                                         int16_t* tmp, int lane, int (&pred)[MAXE]) {
+    constexpr int HALF = NT / 2 - 1;
+    const int ww = bw + NT - 1, wh = bh + NT - 1;
+    const int x0 = xi - HALF, y0 = yi - HALF;
+    const bool interior = x0 >= 0 && y0 >= 0 && x0 + ww <= pw && y0 + wh <= ph;
+    for (int e = lane; e < ww * wh; e += 32) {
+        int r = e / ww, c = e - r * ww;
+        int yy = y0 + r, xx = x0 + c;
+        if (!interior) {
+            yy = clip3(0, ph - 1, yy);
+            xx = clip3(0, pw - 1, xx);
+        }
+        win[r * wpitch + c] = __ldg(plane + (int64_t)yy * pitch + xx);
+    }
+    __syncwarp();
+    const int8_t* th = NT == 8 ? c_luma_taps[fx] : c_chroma_taps[fx];
+    const int8_t* tv = NT == 8 ? c_luma_taps[fy] : c_chroma_taps[fy];
+    if (fx == 0 && fy == 0) {
+#pragma unroll
+        for (int k = 0; k < MAXE; k++) {
+            int e = lane + 32 * k;
+            if (e < bw * bh) {
+                int r = e / bw, c = e - r * bw;
+                pred[k] = (int16_t)(win[(r + HALF) * wpitch + c + HALF] << 6);
+            }
+        }
+    } else if (fy == 0) {
+#pragma unroll
+        for (int k = 0; k < MAXE; k++) {
+            int e = lane + 32 * k;
+            if (e < bw * bh) {
+                int r = e / bw, c = e - r * bw;
+                const uint8_t* w = win + (r + HALF) * wpitch + c;
+                int s = 0;
+#pragma unroll
+                for (int q = 0; q < NT; q++) s += th[q] * w[q];
+                pred[k] = (int16_t)s;
+            }
+        }
+    } else if (fx == 0) {
+#pragma unroll
+        for (int k = 0; k < MAXE; k++) {
+            int e = lane + 32 * k;
+            if (e < bw * bh) {
+                int r = e / bw, c = e - r * bw;
+                const uint8_t* w = win + r * wpitch + c + HALF;
+                int s = 0;
+#pragma unroll
+                for (int q = 0; q < NT; q++) s += tv[q] * w[q * wpitch];
+                pred[k] = (int16_t)s;
+            }
+        }
+    } else {
+        for (int e = lane; e < wh * bw; e += 32) {
+            int r = e / bw, c = e - r * bw;
+            const uint8_t* w = win + r * wpitch + c;
+            int s = 0;
+#pragma unroll
+            for (int q = 0; q < NT; q++) s += th[q] * w[q];
+            tmp[r * bw + c] = (int16_t)s;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < MAXE; k++) {
+            int e = lane + 32 * k;
+            if (e < bw * bh) {
+                int r = e / bw, c = e - r * bw;
+                int s = 0;
+#pragma unroll
+                for (int q = 0; q < NT; q++) s += tv[q] * tmp[(r + q) * bw + c];
+                pred[k] = (int16_t)(s >> 6);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+template <int MAXE>
+__device__ __forceinline__ void mc_weight_store(const int (&p0)[MAXE], const int (&p1)[MAXE], bool u0, bool u1,
+                                                const hevc_wp_t* wp, int ci, uint8_t* dst, int pitch, int bw,
+                                                int bh, int lane) {
+#pragma unroll
+    for (int k = 0; k < MAXE; k++) {
+        int e = lane + 32 * k;
+        if (e >= bw * bh) continue;
+        int r = e / bw, c = e - r * bw;
+        int v;
+        if (!wp) {
+            v = (u0 && u1) ? (p0[k] + p1[k] + 64) >> 7 : ((u0 ? p0[k] : p1[k]) + 32) >> 6;
+        } else {
+            int lw = wp->log2wd[ci ? 1 : 0];
+            if (u0 && u1)
+                v = (p0[k] * wp->w[0][ci] + p1[k] * wp->w[1][ci] + ((wp->o[0][ci] + wp->o[1][ci] + 1) << lw)) >>
+                    (lw + 1);
+            else {
+                int l = u0 ? 0 : 1;
+                v = (((u0 ? p0[k] : p1[k]) * wp->w[l][ci] + (1 << (lw - 1))) >> lw) + wp->o[l][ci];
+            }
+        }
+        dst[(int64_t)r * pitch + c] = (uint8_t)clip_u8(v);
+    }
+}
+
+__global__ void __launch_bounds__(32 * MC_WARPS) k_mc(const __grid_constant__ SegTable st) {
+    __shared__ __align__(16) McSmem sm[MC_WARPS];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const Seg& sg = st.s[find_seg(st, blockIdx.x)];
+    const int item = (blockIdx.x - sg.block0) * MC_WARPS + warp;
+    if (item >= sg.n_items) return;
+    const McItem it = static_cast<const McItem*>(sg.items)[item];
+    const PicDesc& P = *sg.pic;
+    const hevc_pu_t pu = P.pus[it.pu];
+    McSmem& S = sm[warp];
+    const int tx = pu.x + it.dx, ty = pu.y + it.dy, bw = it.w, bh = it.h;
+    const bool use[2] = {pu.ref_idx[0] >= 0, pu.ref_idx[1] >= 0};
+    const hevc_wp_t* wp = pu.wp >= 0 ? &P.wp[pu.wp] : nullptr;
+    const int W = P.width, H = P.height;
+
+    // luma
+    {
+        int pl[2][8];
+#pragma unroll
+        for (int l = 0; l < 2; l++) {
+            if (!use[l]) continue;
+            const uint8_t* ref = P.ref[l][pu.ref_idx[l]];
+            int mvx = pu.mv[l][0], mvy = pu.mv[l][1];
+            mc_block<8, 8>(ref, P.pitch_y, W, H, tx + (mvx >> 2), ty + (mvy >> 2), mvx & 3, mvy & 3, bw, bh, S.win,
+                           24, S.tmp, lane, pl[l]);
+        }
+        mc_weight_store<8>(pl[0], pl[1], use[0], use[1], wp, 0, P.rec + (int64_t)ty * P.pitch_y + tx, P.pitch_y, bw,
+                           bh, lane);
+    }
+    // chroma (4:2:0)
+    const int cw = bw / 2, ch = bh / 2, cx = tx / 2, cy = ty / 2;
+#pragma unroll
+    for (int ci = 1; ci <= 2; ci++) {
+        int pl[2][2];
+        int64_t off = ci == 1 ? P.off_cb : P.off_cr;
+#pragma unroll
+        for (int l = 0; l < 2; l++) {
+            if (!use[l]) continue;
+            const uint8_t* ref = P.ref[l][pu.ref_idx[l]] + off;
+            int mvx = pu.mv[l][0], mvy = pu.mv[l][1];
+            mc_block<4, 2>(ref, P.pitch_c, W / 2, H / 2, cx + (mvx >> 3), cy + (mvy >> 3), mvx & 7, mvy & 7, cw, ch,
+                           S.cwin[ci - 1], 12, S.ctmp, lane, pl[l]);
+        }
+        mc_weight_store<2>(pl[0], pl[1], use[0], use[1], wp, ci, P.rec + off + (int64_t)cy * P.pitch_c + cx,
+                           P.pitch_c, cw, ch, lane);
+    }
+}
+
+// ======================================================================================
+// Intra prediction, one CTA per CTU, one warp per colour plane.  The warp copies the CTU
+// and its top/left neighbourhood into shared memory, then walks its plane's intra TUs
+// in decode order: reference samples with availability and substitution, optional
+// [1 2 1] or bilinear smoothing, planar/DC/angular prediction, + residual, clip; each
+// result is written to shared memory (for the next TU) and to the picture.
+// ======================================================================================
+constexpr int IT_LW = 129, IT_LH = 65;  // luma tile: cols -1..127, rows -1..63
+constexpr int IT_CW = 65, IT_CH = 33;   // chroma tile
+__constant__ int8_t c_intra_angle[35] = {0,   0,   32,  26,  21,  17,  13,  9,  5,  2,  0,  -2,
+                                         -5,  -9,  -13, -17, -21, -26, -32, -26, -21, -17, -13, -9,
+                                         -5,  -2,  0,   2,   5,   9,   13,  17,  21,  26,  32};
+__constant__ int16_t c_inv_angle[35] = {0,    0,    256, 315, 390, 482,  630,  910,  1638, 4096, 0,   4096,
+                                        1638, 910,  630, 482, 390, 315,  256,  315,  390,  482,  630, 910,
+                                        1638, 4096, 0,   4096, 1638, 910, 630, 482,  390,  315,  256};
+
+struct IntraWarpSmem {
+    int16_t s[129];   // substituted reference samples (bottom-left .. corner .. top-right)
+    int16_t f[129];   // filtered copy
+    int16_t raw[129];
+};
+
+__global__ void __launch_bounds__(96) k_intra_ctu(const __grid_constant__ SegTable st) {
+    __shared__ uint8_t t_luma[IT_LH * IT_LW];
+    __shared__ uint8_t t_chroma[2][IT_CH * IT_CW];
+    __shared__ IntraWarpSmem ws[3];
+    const int ci = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const Seg& sg = st.s[find_seg(st, blockIdx.x)];
+    const int item = blockIdx.x - sg.block0;
+    if (item >= sg.n_items) return;
+    struct { int ctu; } it = {static_cast<const int32_t*>(sg.items)[item]};
+    const PicDesc& P = *sg.pic;
+    const int beg = P.intra_off[it.ctu * 3 + ci], end = P.intra_off[it.ctu * 3 + ci + 1];
+    if (beg >= end) return;
+
+    const int sub = ci ? 2 : 1;
+    const int ctb = 1 << P.log2_ctb, ctbc = ctb / sub;
+    const int rx = it.ctu % P.wctb, ry = it.ctu / P.wctb;
+    const int pw = P.width / sub, ph = P.height / sub;
+    const int cx0 = rx * ctbc, cy0 = ry * ctbc;      // CTU origin, plane coordinates
+    const int ox = rx * ctb, oy = ry * ctb;          // CTU origin, luma
+    const int tw = ci ? IT_CW : IT_LW;               // tile pitch; tile (0,0) = (cx0-1, cy0-1)
+    uint8_t* tile = ci ? t_chroma[ci - 1] : t_luma;
+    const int pitch = ci ? P.pitch_c : P.pitch_y;
+    uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));
+    const int cur_slice = P.ctb_slice ? P.ctb_slice[it.ctu] : 0;
+    const int cur_tile = P.ctb_tile ? P.ctb_tile[it.ctu] : 0;
+
+    // stage the neighbourhood: row -1 (cols -1 .. 2*ctbc-1), col -1 (rows 0..ctbc-1), interior
+    {
+        const int row_n = 2 * ctbc + 1;
+        for (int e = lane; e < row_n; e += 32) {
+            int x = cx0 - 1 + e, y = cy0 - 1;
+            if (x >= 0 && y >= 0 && x < pw) tile[e] = plane[(int64_t)y * pitch + x];
+        }
+        for (int e = lane; e < ctbc; e += 32) {
+            int x = cx0 - 1, y = cy0 + e;
+            if (x >= 0 && y < ph) tile[(e + 1) * tw] = plane[(int64_t)y * pitch + x];
+        }
+        for (int e = lane; e < ctbc * ctbc / 4; e += 32) {
+            int r = e / (ctbc / 4), c4 = (e % (ctbc / 4)) * 4;
+            int x = cx0 + c4, y = cy0 + r;
+            if (y < ph && x < pw) {
+                uint32_t v = *reinterpret_cast<const uint32_t*>(plane + (int64_t)y * pitch + x);
+                uint8_t* d = tile + (r + 1) * tw + c4 + 1;
+                d[0] = v & 0xFF; d[1] = (v >> 8) & 0xFF; d[2] = (v >> 16) & 0xFF; d[3] = v >> 24;
+            }
+        }
+    }
+    __syncwarp();
+
+    IntraWarpSmem& W = ws[ci];
+    const int cur_addr = it.ctu;
+    for (int li = beg; li < end; li++) {
+        const hevc_tu_t t = P.tus[P.intra_list[li]];
+        const int n = 1 << t.log2_size, log2 = t.log2_size;
+        const int xc = t.x, yc = t.y;
+        const uint32_t cur_z = zorder16((uint32_t)((xc * sub - ox) >> 2), (uint32_t)((yc * sub - oy) >> 2));
+        const int total = 4 * n + 1;
+
+        // 1. reference samples and their availability (build_reference_samples)
+        uint32_t mask[5];
+#pragma unroll
+        for (int r = 0; r < 5; r++) {
+            int i = lane + 32 * r;
+            bool ok = false;
+            int val = 0;
+            if (i < total) {
+                int px, py;
+                if (i < 2 * n) { px = xc - 1; py = yc + 2 * n - 1 - i; }
+                else if (i == 2 * n) { px = xc - 1; py = yc - 1; }
+                else { px = xc + (i - 2 * n - 1); py = yc - 1; }
+                if (px >= 0 && py >= 0 && px < pw && py < ph) {
+                    int ncx = px / ctbc, ncy = py / ctbc;
+                    if (ncx != rx || ncy != ry) {
+                        int a = ncy * P.wctb + ncx;
+                        ok = a < cur_addr && (P.ctb_slice ? P.ctb_slice[a] : 0) == cur_slice &&
+                             (P.ctb_tile ? P.ctb_tile[a] : 0) == cur_tile;
+                    } else {
+                        ok = zorder16((uint32_t)((px * sub - ox) >> 2), (uint32_t)((py * sub - oy) >> 2)) < cur_z;
+                    }
+                    if (ok) val = tile[(py - cy0 + 1) * tw + (px - cx0 + 1)];
+                }
+                W.raw[i] = (int16_t)val;
+            }
+            mask[r] = __ballot_sync(0xffffffffu, ok);
+        }
+        __syncwarp();
+        // 2. substitution: nearest available below, else the first available
+        int first = -1;
+#pragma unroll
+        for (int r = 0; r < 5; r++)
+            if (first < 0 && mask[r]) first = 32 * r + __ffs(mask[r]) - 1;
+#pragma unroll
+        for (int r = 0; r < 5; r++) {
+            int i = lane + 32 * r;
+            if (i >= total) continue;
+            int v;
+            if (first < 0) v = 128;
+            else if ((mask[r] >> lane) & 1u) v = W.raw[i];
+            else {
+                int j = -1;
+                uint32_t m = lane ? (mask[r] & ((1u << lane) - 1u)) : 0u;
+                if (m) j = 32 * r + 31 - __clz(m);
+                for (int q = r - 1; q >= 0 && j < 0; q--)
+                    if (mask[q]) j = 32 * q + 31 - __clz(mask[q]);
+                v = W.raw[j < 0 ? first : j];
+            }
+            W.s[i] = (int16_t)v;
+        }
+        __syncwarp();
+        // 3. smoothing of luma references (intra_prediction.cpp:217-257, :443-471)
+        const int mode = t.intra_mode;
+        const int16_t* R = W.s;
+        if (ci == 0 && !P.intra_smoothing_disabled && mode != 1 && n != 4) {
+            int d = min(abs(mode - 26), abs(mode - 10));
+            int thr = n == 8 ? 7 : (n == 16 ? 1 : 0);
+            if (d > thr) {
+                bool bil = false;
+                if (P.strong_intra && n == 32) {
+                    int c = W.s[2 * n];
+                    bil = abs(c + W.s[4 * n] - 2 * W.s[3 * n]) < 8 && abs(c + W.s[0] - 2 * W.s[n]) < 8;
+                }
+#pragma unroll
+                for (int r = 0; r < 5; r++) {
+                    int i = lane + 32 * r;
+                    if (i >= total) continue;
+                    int v;
+                    if (i == 0 || i == 4 * n) v = W.s[i];
+                    else if (bil) {
+                        if (i == 2 * n) v = W.s[i];
+                        else if (i > 2 * n) { int k = i - 2 * n; v = ((2 * n - k) * W.s[2 * n] + k * W.s[4 * n] + n) >> (log2 + 1); }
+                        else { int k = 2 * n - i; v = ((2 * n - k) * W.s[2 * n] + k * W.s[0] + n) >> (log2 + 1); }
+                    } else {
+                        v = (W.s[i - 1] + 2 * W.s[i] + W.s[i + 1] + 2) >> 2;
+                    }
+                    W.f[i] = (int16_t)v;
+                }
+                __syncwarp();
+                R = W.f;
+            }
+        }
+        // 4. prediction + residual (top[k] = R[2n + k], left[k] = R[2n - k])
+        const int16_t* res = (t.flags & HEVC_TU_CODED) ? P.resid + t.coeff_offset : nullptr;
+        const int ang = c_intra_angle[mode];
+        const int inv = c_inv_angle[mode];
+        int dc = 0;
+        if (mode == 1) {
+            int s = 0;
+            for (int i = lane; i < n; i += 32) s += R[2 * n + 1 + i] + R[2 * n - 1 - i];
+            s = __reduce_add_sync(0xffffffffu, s);
+            dc = (s + n) >> (log2 + 1);
+        }
+        for (int e = lane; e < n * n; e += 32) {
+            int y = e >> log2, x = e & (n - 1);
+            int p;
+            if (mode == 0) {
+                p = ((n - 1 - x) * R[2 * n - 1 - y] + (x + 1) * R[3 * n + 1] + (n - 1 - y) * R[2 * n + 1 + x] +
+                     (y + 1) * R[n - 1] + n) >> (log2 + 1);
+            } else if (mode == 1) {
+                p = dc;
+                if (ci == 0 && n < 32) {
+                    if (x == 0 && y == 0) p = (R[2 * n + 1] + R[2 * n - 1] + 2 * dc + 2) >> 2;
+                    else if (y == 0) p = (R[2 * n + 1 + x] + 3 * dc + 2) >> 2;
+                    else if (x == 0) p = (R[2 * n - 1 - y] + 3 * dc + 2) >> 2;
+                }
+            } else {
+                const bool vert = mode >= 18;
+                const int pos = vert ? y : x, ln = vert ? x : y;
+                const int idx = ((pos + 1) * ang) >> 5, fr = ((pos + 1) * ang) & 31;
+                const int ri = ln + 1 + idx;
+                // main reference (top for vertical, left for horizontal); negative indices
+                // project onto the side reference through invAngle (:346-368)
+                auto ref_at = [&](int q) -> int {
+                    if (q >= 0) return vert ? R[2 * n + q] : R[2 * n - q];
+                    int si = min(2 * n, ((-q) * inv + 128) >> 8);
+                    return vert ? R[2 * n - si] : R[2 * n + si];
+                };
+                p = fr ? ((32 - fr) * ref_at(ri) + fr * ref_at(ri + 1) + 16) >> 5 : ref_at(ri);
+                if (ci == 0 && n < 32) {
+                    if (mode == 26 && x == 0) p = clip_u8(p + ((R[2 * n - 1 - y] - R[2 * n]) >> 1));
+                    else if (mode == 10 && y == 0) p = clip_u8(p + ((R[2 * n + 1 + x] - R[2 * n]) >> 1));
+                }
+            }
+            int v = clip_u8(p + (res ? res[e] : 0));
+            int lx = xc - cx0, ly = yc - cy0;
+            tile[(ly + y + 1) * tw + lx + x + 1] = (uint8_t)v;
+            if (xc + x < pw && yc + y < ph) plane[(int64_t)(yc + y) * pitch + xc + x] = (uint8_t)v;
+        }
+        __syncwarp();
+    }
+}
+
+// ======================================================================================
+// Motion grid: one warp per PU writes its 4x4 entries (used by the Bs derivation).
+// ======================================================================================
+__global__ void k_motion_grid(const __grid_constant__ SegTable st) {
+    const PicDesc& P = *st.s[blockIdx.y].pic;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x % 32;
+    if (warp >= P.num_pus) return;
+    const hevc_pu_t pu = P.pus[warp];
+    MotionEnt m;
+    m.mv[0][0] = pu.mv[0][0]; m.mv[0][1] = pu.mv[0][1];
+    m.mv[1][0] = pu.mv[1][0]; m.mv[1][1] = pu.mv[1][1];
+    m.ref[0] = pu.ref_idx[0]; m.ref[1] = pu.ref_idx[1];
+    m.pad = 0;
+    const int bw = pu.w / 4, n = bw * (pu.h / 4), gw = P.width / 4;
+    for (int e = lane; e < n; e += 32) {
+        int gy = pu.y / 4 + e / bw, gx = pu.x / 4 + e % bw;
+        P.mot[(int64_t)gy * gw + gx] = m;
+    }
+}
+
+// ======================================================================================
+// Deblocking.  One thread per 4-sample edge segment on the 8x8 grid; all segments of
+// one direction are independent (each filters at most 3 samples either side and its
+// decisions read 4, so neighbouring 8-spaced edges never touch the same samples), so
+// the vertical pass and then the horizontal pass are each one launch.
+// ======================================================================================
+__constant__ uint8_t c_beta[52] = {0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  6,  7,
+                                   8,  9,  10, 11, 12, 13, 14, 15, 16, 17, 18, 20, 22, 24, 26, 28, 30, 32,
+                                   34, 36, 38, 40, 42, 44, 46, 48, 50, 52, 54, 56, 58, 60, 62, 64};
+__constant__ uint8_t c_tc[54] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1,  1,  1,  1,  1,  1,  1,  1,  1,
+                                 2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 5, 5, 6, 6, 7, 8, 9, 10, 11, 13, 14, 16, 18, 20, 22, 24};
+__constant__ uint8_t c_qpc[58] = {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11, 12, 13, 14, 15, 16, 17, 18, 19,
+                                  20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 29, 30, 31, 32, 33, 33, 34, 34, 35, 35,
+                                  36, 36, 37, 37, 38, 39, 40, 41, 42, 43, 44, 45, 46, 47, 48, 49, 50, 51};
+
+__device__ __forceinline__ int ref_poc_of(const PicDesc& P, const MotionEnt& m, int l) {
+    int r = m.ref[l];
+    return (r < 0 || r >= P.num_ref[l]) ? -999999 : P.ref_poc[l][r];
+}
+__device__ __forceinline__ bool mv_far(const int16_t* a, const int16_t* b) {
+    return abs(a[0] - b[0]) >= 4 || abs(a[1] - b[1]) >= 4;
+}
+
+// derive_bs (deblocking.cpp:125-247)
+__device__ int derive_bs(const PicDesc& P, int gw, uint32_t bp, uint32_t bq, int xp, int yp, int xq, int yq) {
+    if ((bp | bq) & HEVC_BLK_INTRA) return 2;
+    int tp = 1 << ((bp >> HEVC_BLK_TU_SHIFT) & 0xFF), tq = 1 << ((bq >> HEVC_BLK_TU_SHIFT) & 0xFF);
+    bool tu_edge = (xp != xq) ? ((xq % tq == 0) || ((xp + 1) % tp == 0 && xp + 1 == xq))
+                              : ((yq % tq == 0) || ((yp + 1) % tp == 0 && yp + 1 == yq));
+    if (tu_edge && ((bp | bq) & HEVC_BLK_CBF)) return 1;
+    const MotionEnt mp = P.mot[(int64_t)(yp >> 2) * gw + (xp >> 2)];
+    const MotionEnt mq = P.mot[(int64_t)(yq >> 2) * gw + (xq >> 2)];
+    int np = (mp.ref[0] >= 0) + (mp.ref[1] >= 0), nq = (mq.ref[0] >= 0) + (mq.ref[1] >= 0);
+    if (np != nq) return 1;
+    if (np == 1) {
+        int lp = mp.ref[0] >= 0 ? 0 : 1, lq = mq.ref[0] >= 0 ? 0 : 1;
+        if (ref_poc_of(P, mp, lp) != ref_poc_of(P, mq, lq)) return 1;
+        return mv_far(mp.mv[lp], mq.mv[lq]) ? 1 : 0;
+    }
+    if (np == 2) {
+        int p0 = ref_poc_of(P, mp, 0), p1 = ref_poc_of(P, mp, 1), q0 = ref_poc_of(P, mq, 0), q1 = ref_poc_of(P, mq, 1);
+        bool same = p0 == q0 && p1 == q1, swp = p0 == q1 && p1 == q0;
+        if (!same && !swp) return 1;
+        bool o1 = !mv_far(mp.mv[0], mq.mv[0]) && !mv_far(mp.mv[1], mq.mv[1]);
+        bool o2 = !mv_far(mp.mv[0], mq.mv[1]) && !mv_far(mp.mv[1], mq.mv[0]);
+        if (same && !swp) return o1 ? 0 : 1;
+        if (!same && swp) return o2 ? 0 : 1;
+        return (o1 || o2) ? 0 : 1;
+    }
+    return 0;
+}
+
+__device__ __forceinline__ const hevc_slice_t& slice_at(const PicDesc& P, int addr) {
+    int s = P.ctb_slice ? P.ctb_slice[addr] : 0;
+    return P.slices[s < P.num_slices ? s : 0];
+}
+
+// Filter one 4-sample luma segment held as p[line][i] (i = distance - 1 from the edge on
+// the P side) and q[line][i]; returns the sample counts to write (per side, in
+// nP/nQ) via the arrays themselves.
+__device__ __forceinline__ void luma_segment(int (&p)[4][4], int (&q)[4][4], int beta, int tc, bool noP, bool noQ,
+                                             int (&np)[4], int (&nq)[4]) {
+    int dp0 = abs(p[0][2] - 2 * p[0][1] + p[0][0]), dp3 = abs(p[3][2] - 2 * p[3][1] + p[3][0]);
+    int dq0 = abs(q[0][2] - 2 * q[0][1] + q[0][0]), dq3 = abs(q[3][2] - 2 * q[3][1] + q[3][0]);
+    int dpq0 = dp0 + dq0, dpq3 = dp3 + dq3, dp = dp0 + dp3, dq = dq0 + dq3;
+#pragma unroll
+    for (int k = 0; k < 4; k++) np[k] = nq[k] = 0;
+    if (dpq0 + dpq3 >= beta) return;
+    bool strong = true;
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+        int k = kk * 3, dpq = kk ? dpq3 : dpq0;
+        if (!(2 * dpq < (beta >> 2) && abs(p[k][3] - p[k][0]) + abs(q[k][0] - q[k][3]) < (beta >> 3) &&
+              abs(p[k][0] - q[k][0]) < ((5 * tc + 1) >> 1)))
+            strong = false;
+    }
+    int thr = (beta + (beta >> 1)) >> 3;
+    bool dEp = dp < thr, dEq = dq < thr;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        int P0 = p[k][0], P1 = p[k][1], P2 = p[k][2], P3 = p[k][3];
+        int Q0 = q[k][0], Q1 = q[k][1], Q2 = q[k][2], Q3 = q[k][3];
+        if (strong) {
+            int t2 = 2 * tc;
+            p[k][0] = clip3(P0 - t2, P0 + t2, (P2 + 2 * P1 + 2 * P0 + 2 * Q0 + Q1 + 4) >> 3);
+            p[k][1] = clip3(P1 - t2, P1 + t2, (P2 + P1 + P0 + Q0 + 2) >> 2);
+            p[k][2] = clip3(P2 - t2, P2 + t2, (2 * P3 + 3 * P2 + P1 + P0 + Q0 + 4) >> 3);
+            q[k][0] = clip3(Q0 - t2, Q0 + t2, (P1 + 2 * P0 + 2 * Q0 + 2 * Q1 + Q2 + 4) >> 3);
+            q[k][1] = clip3(Q1 - t2, Q1 + t2, (P0 + Q0 + Q1 + Q2 + 2) >> 2);
+            q[k][2] = clip3(Q2 - t2, Q2 + t2, (P0 + Q0 + Q1 + 3 * Q2 + 2 * Q3 + 4) >> 3);
+            np[k] = nq[k] = 3;
+        } else {
+            int delta = (9 * (Q0 - P0) - 3 * (Q1 - P1) + 8) >> 4;
+            if (abs(delta) < tc * 10) {
+                delta = clip3(-tc, tc, delta);
+                p[k][0] = clip_u8(P0 + delta);
+                q[k][0] = clip_u8(Q0 - delta);
+                if (dEp) p[k][1] = clip_u8(P1 + clip3(-(tc >> 1), tc >> 1, (((P2 + P0 + 1) >> 1) - P1 + delta) >> 1));
+                if (dEq) q[k][1] = clip_u8(Q1 + clip3(-(tc >> 1), tc >> 1, (((Q2 + Q0 + 1) >> 1) - Q1 - delta) >> 1));
+                np[k] = dEp + 1;
+                nq[k] = dEq + 1;
+            }
+        }
+        if (noP) np[k] = 0;
+        if (noQ) nq[k] = 0;
+    }
+}
+
+template <bool VERT>
+__global__ void __launch_bounds__(256) k_deblock(const __grid_constant__ SegTable st) {
+    const PicDesc& P = *st.s[blockIdx.y].pic;
+    const int W = P.width, H = P.height, gw = W >> 2;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    // VERT: segments at x = 8i, y = 4j.  !VERT: x = 4i, y = 8j.
+    const int nx = VERT ? (W + 7) >> 3 : W >> 2;
+    const int x = VERT ? (tid % nx) * 8 : (tid % nx) * 4;
+    const int y = VERT ? (tid / nx) * 4 : (tid / nx) * 8;
+    if (y >= H || x >= W) return;
+    if (VERT ? x == 0 : y == 0) return;
+    const uint32_t bq = P.blk[(int64_t)(y >> 2) * gw + (x >> 2)];
+    if (!(bq & (VERT ? HEVC_BLK_EDGE_V : HEVC_BLK_EDGE_H))) return;
+    const int ctb = 1 << P.log2_ctb;
+    const int aq = (y >> P.log2_ctb) * P.wctb + (x >> P.log2_ctb);
+    const hevc_slice_t& sq = slice_at(P, aq);
+    if (sq.deblocking_disabled) return;
+    const int xp = VERT ? x - 1 : x, yp = VERT ? y : y - 1;
+    if (P.tiles_check || P.slice_check) {
+        const int ap = (yp >> P.log2_ctb) * P.wctb + (xp >> P.log2_ctb);
+        if (P.tiles_check && P.ctb_tile && P.ctb_tile[aq] != P.ctb_tile[ap]) return;
+        if (P.slice_check && P.ctb_slice && P.ctb_slice[aq] != P.ctb_slice[ap] && !sq.lf_across_slices) return;
+    }
+    (void)ctb;
+    const uint32_t bp = P.blk[(int64_t)(yp >> 2) * gw + (xp >> 2)];
+    const int bs = derive_bs(P, gw, bp, bq, xp, yp, x, y);
+    if (bs == 0) return;
+    const int qpP = (int8_t)(bp >> HEVC_BLK_QP_SHIFT), qpQ = (int8_t)(bq >> HEVC_BLK_QP_SHIFT);
+    const bool noP = (P.pcm_lf_disabled && (bp & HEVC_BLK_PCM)) || (bp & HEVC_BLK_BYPASS);
+    const bool noQ = (P.pcm_lf_disabled && (bq & HEVC_BLK_PCM)) || (bq & HEVC_BLK_BYPASS);
+    const int qpl = (qpQ + qpP + 1) >> 1;
+    const int beta = c_beta[clip3(0, 51, qpl + 2 * sq.beta_offset_div2)];
+    const int tc = c_tc[clip3(0, 53, qpl + 2 * (bs - 1) + 2 * sq.tc_offset_div2)];
+
+    // ---- luma: load the 8x4 (or 4x8) neighbourhood as 32-bit words
+    uint8_t* Y = P.rec;
+    int p[4][4], q[4][4];
+    uint32_t wv[8];
+    if (VERT) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint8_t* row = Y + (int64_t)(y + k) * P.pitch_y + x;
+            wv[2 * k] = *reinterpret_cast<const uint32_t*>(row - 4);
+            wv[2 * k + 1] = *reinterpret_cast<const uint32_t*>(row);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                p[k][i] = (wv[2 * k] >> (8 * (3 - i))) & 0xFF;
+                q[k][i] = (wv[2 * k + 1] >> (8 * i)) & 0xFF;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            wv[3 - i] = *reinterpret_cast<const uint32_t*>(Y + (int64_t)(y - 1 - i) * P.pitch_y + x);
+            wv[4 + i] = *reinterpret_cast<const uint32_t*>(Y + (int64_t)(y + i) * P.pitch_y + x);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                p[k][i] = (wv[3 - i] >> (8 * k)) & 0xFF;
+                q[k][i] = (wv[4 + i] >> (8 * k)) & 0xFF;
+            }
+    }
+    int np[4], nq[4];
+    luma_segment(p, q, beta, tc, noP, noQ, np, nq);
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) any |= (np[k] | nq[k]) != 0;
+    if (any) {
+        if (VERT) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                uint32_t a = wv[2 * k], b = wv[2 * k + 1];
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    if (i < np[k]) a = (a & ~(0xFFu << (8 * (3 - i)))) | ((uint32_t)p[k][i] << (8 * (3 - i)));
+                    if (i < nq[k]) b = (b & ~(0xFFu << (8 * i))) | ((uint32_t)q[k][i] << (8 * i));
+                }
+                uint8_t* row = Y + (int64_t)(y + k) * P.pitch_y + x;
+                *reinterpret_cast<uint32_t*>(row - 4) = a;
+                *reinterpret_cast<uint32_t*>(row) = b;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                uint32_t a = wv[3 - i], b = wv[4 + i];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (i < np[k]) a = (a & ~(0xFFu << (8 * k))) | ((uint32_t)p[k][i] << (8 * k));
+                    if (i < nq[k]) b = (b & ~(0xFFu << (8 * k))) | ((uint32_t)q[k][i] << (8 * k));
+                }
+                *reinterpret_cast<uint32_t*>(Y + (int64_t)(y - 1 - i) * P.pitch_y + x) = a;
+                *reinterpret_cast<uint32_t*>(Y + (int64_t)(y + i) * P.pitch_y + x) = b;
+            }
+        }
+    }
+
+    // ---- chroma: Bs 2 on the 8-sample chroma grid (deblocking.cpp:538-609)
+    if (bs == 2 && (((VERT ? x : y) >> 1) & 7) == 0) {
+        const int cx = x >> 1, cy = y >> 1;
+#pragma unroll
+        for (int ci = 1; ci <= 2; ci++) {
+            const int off = ci == 1 ? P.cb_qp_offset : P.cr_qp_offset;
+            const int qpc = c_qpc[clip3(0, 57, ((qpQ + qpP + 1) >> 1) + off)];
+            const int tcc = c_tc[clip3(0, 53, qpc + 2 + 2 * sq.tc_offset_div2)];
+            uint8_t* Cp = P.rec + (ci == 1 ? P.off_cb : P.off_cr);
+            const int pc = P.pitch_c;
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                uint8_t* s0 = VERT ? Cp + (int64_t)(cy + k) * pc + cx : Cp + (int64_t)cy * pc + cx + k;
+                const int st = VERT ? 1 : pc;
+                int p0 = s0[-st], p1 = s0[-2 * st], q0 = s0[0], q1 = s0[st];
+                int delta = clip3(-tcc, tcc, ((((q0 - p0) * 4) + p1 - q1 + 4) >> 3));
+                if (!noP) s0[-st] = (uint8_t)clip_u8(p0 + delta);
+                if (!noQ) s0[0] = (uint8_t)clip_u8(q0 - delta);
+            }
+        }
+    }
+}
+
+// ======================================================================================
+// SAO: one thread per 4 horizontal samples of one plane, reading the deblocked picture
+// (rec) and writing the DPB slot (dst); samples without SAO are copied.
+// ======================================================================================
+__global__ void __launch_bounds__(256) k_sao(const __grid_constant__ SegTable st) {
+    const PicDesc& P = *st.s[blockIdx.y].pic;
+    const int ci = blockIdx.z;
+    const int sub = ci ? 2 : 1;
+    const int pw = P.width / sub, ph = P.height / sub;
+    const int groups = pw >> 2;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = tid / groups, x = (tid % groups) * 4;
+    if (y >= ph) return;
+    const int pitch = ci ? P.pitch_c : P.pitch_y;
+    const int64_t base = ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr);
+    const uint8_t* S = P.rec + base;
+    uint8_t* D = P.dst + base;
+    const uint32_t c4 = *reinterpret_cast<const uint32_t*>(S + (int64_t)y * pitch + x);
+    uint32_t out = c4;
+    const int ctbc = (1 << P.log2_ctb) / sub;
+    const int addr = (y / ctbc) * P.wctb + x / ctbc;
+    const hevc_sao_t& sp = P.sao[addr];
+    const int type = P.sao_enabled ? sp.type[ci] : 0;
+    if (type != 0) {
+        const int gw = P.width >> 2;
+        const bool check_slices = P.slice_check || P.tiles_check;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int xs = x + i;
+            const uint32_t b = P.blk[(int64_t)((y * sub) >> 2) * gw + ((xs * sub) >> 2)];
+            if ((P.pcm_lf_disabled && (b & HEVC_BLK_PCM)) || (b & HEVC_BLK_BYPASS)) continue;
+            const int c = (c4 >> (8 * i)) & 0xFF;
+            int v;
+            if (type == 2) {
+                const int cl = sp.eo_class[ci];
+                const int dx0 = cl == 1 ? 0 : (cl == 3 ? 1 : -1), dy0 = cl == 0 ? 0 : -1;
+                const int dx1 = -dx0, dy1 = -dy0;
+                const int ax = xs + dx0, ay = y + dy0, bx = xs + dx1, by = y + dy1;
+                if (ax < 0 || ay < 0 || ax >= pw || ay >= ph || bx < 0 || by < 0 || bx >= pw || by >= ph) continue;
+                if (check_slices) {
+                    bool skip = false;
+                    const int cur = ((y * sub) >> P.log2_ctb) * P.wctb + ((xs * sub) >> P.log2_ctb);
+                    for (int nk = 0; nk < 2 && !skip; nk++) {
+                        int nx = nk ? bx : ax, ny = nk ? by : ay;
+                        int na = ((ny * sub) >> P.log2_ctb) * P.wctb + ((nx * sub) >> P.log2_ctb);
+                        int sc = P.ctb_slice ? P.ctb_slice[cur] : 0, sn = P.ctb_slice ? P.ctb_slice[na] : 0;
+                        if (sc != sn) {
+                            int owner = sn < sc ? cur : na;
+                            if (!slice_at(P, owner).lf_across_slices) skip = true;
+                        }
+                        if (!skip && P.tiles_check && P.ctb_tile && P.ctb_tile[cur] != P.ctb_tile[na]) skip = true;
+                    }
+                    if (skip) continue;
+                }
+                const int a = S[(int64_t)ay * pitch + ax], bb = S[(int64_t)by * pitch + bx];
+                const int e = 2 + (c < a ? -1 : (c > a ? 1 : 0)) + (c < bb ? -1 : (c > bb ? 1 : 0));
+                v = c + sp.offset[ci][e];
+            } else {
+                const int k = (c >> 3) - sp.band_pos[ci];
+                if (k < 0 || k >= 4) continue;
+                v = c + sp.offset[ci][k];
+            }
+            out = (out & ~(0xFFu << (8 * i))) | ((uint32_t)clip_u8(v) << (8 * i));
+        }
+    }
+    *reinterpret_cast<uint32_t*>(D + (int64_t)y * pitch + x) = out;
+}
+
+}  // namespace hevcgpu

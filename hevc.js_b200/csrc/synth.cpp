@@ -468,11 +468,24 @@ int hevcsynth_content(int32_t width, int32_t height, uint64_t seed, uint8_t* out
             ph[k] = r.unit() * two_pi;
             amp[k] = 6.0 + r.unit() * 18.0;
         }
-        std::vector<double> row(8);
+        // sin(a + b) = sin a cos b + cos a sin b with a = fx*x (per column) and
+        // b = fy*y + phase (per row): two tables per sinusoid instead of a sin per sample
+        std::vector<double> sx((size_t)8 * w), cx((size_t)8 * w), sy((size_t)8 * h), cy((size_t)8 * h);
+        for (int k = 0; k < 8; k++) {
+            for (int x = 0; x < w; x++) {
+                sx[(size_t)k * w + x] = amp[k] * std::sin(fx[k] * x);
+                cx[(size_t)k * w + x] = amp[k] * std::cos(fx[k] * x);
+            }
+            for (int y = 0; y < h; y++) {
+                sy[(size_t)k * h + y] = std::sin(fy[k] * y + ph[k]);
+                cy[(size_t)k * h + y] = std::cos(fy[k] * y + ph[k]);
+            }
+        }
         for (int y = 0; y < h; y++)
             for (int x = 0; x < w; x++) {
                 double v = 128.0;
-                for (int k = 0; k < 8; k++) v += amp[k] * std::sin(fx[k] * x + fy[k] * y + ph[k]);
+                for (int k = 0; k < 8; k++)
+                    v += sx[(size_t)k * w + x] * cy[(size_t)k * h + y] + cx[(size_t)k * w + x] * sy[(size_t)k * h + y];
                 int s = (int)std::lround(v) + r.range(-8, 8);
                 plane[(size_t)y * w + x] = (uint8_t)std::min(255, std::max(0, s));
             }

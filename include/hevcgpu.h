@@ -228,6 +228,8 @@ int  hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void*
 int  hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn,
                          hevcgpu_job_t** out);
 void hevcgpu_job_free(hevcgpu_job_t* job);
+/* Bytes the prepare call copied host -> device for this job (records + work lists). */
+uint64_t hevcgpu_job_upload_bytes(hevcgpu_job_t* job);
 /* Plain form: one launch per stage for this picture, into DPB slot dst_slot, reading
  * reference slots from params.ref_slot.  Asynchronous on the stream's CUDA stream. */
 int  hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot);
@@ -239,6 +241,16 @@ int  hevcgpu_stream_sync(hevcgpu_stream_t* st);
 void* hevcgpu_cuda_stream(hevcgpu_ctx_t* ctx);
 /* Number of kernel launches issued by this context so far. */
 uint64_t hevcgpu_launch_count(hevcgpu_ctx_t* ctx);
+
+/* Stage profiling: when enabled, CUDA events are recorded on the context's stream around
+ * each reconstruction stage of every later launch.  hevcgpu_profile_read waits for the
+ * stream and returns, per stage, the summed device milliseconds and the number of kernel
+ * launches since the previous read.  Stages: 0 motion grid, 1 motion compensation,
+ * 2 residual, 3 intra wavefront, 4 deblocking (vertical edges), 5 deblocking
+ * (horizontal edges), 6 SAO. */
+#define HEVCGPU_NUM_STAGES 7
+int hevcgpu_profile_enable(hevcgpu_ctx_t* ctx, int enable);
+int hevcgpu_profile_read(hevcgpu_ctx_t* ctx, double* ms, uint64_t* launches);
 
 /* End-to-end decode-side call: prepare + upload + launch + wait for one picture. */
 int  hevcgpu_picture_decode(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn,

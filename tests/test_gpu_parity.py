@@ -1,0 +1,135 @@
+"""GPU parity: every stage of the CUDA back end, called through the C ABI, is bit-exact
+against the oracle and against the reference's golden digests."""
+import numpy as np
+import pytest
+
+import cases
+from test_oracle import _edit_blocks, with_filter_edits
+
+pytestmark = pytest.mark.gpu
+
+
+def _diff(a, b):
+    return int((a != b).sum())
+
+
+@pytest.mark.parametrize("name", list(cases.CASES))
+def test_gpu_matches_reference_digests(hb, gpu_ctx, port, golden, name):
+    case = cases.CASES[name]
+    inp = cases.build_inputs(hb, case)
+    got = cases.run_case(gpu_ctx, case, inp)
+    want = cases.run_case(port, case, inp)
+    assert _diff(got, want) == 0
+    assert cases.digest(hb, case, got) == golden[name]["md5"]
+
+
+@pytest.mark.parametrize("seed,opts", [(21, dict(tskip=True)), (22, dict(big=True, qp=(40, 51))),
+                                       (23, dict(big=True, qp=(0, 10))), (24, dict(qp=(0, 51)))])
+def test_gpu_blocks_edge_levels(hb, gpu_ctx, port, seed, opts):
+    tus, n, coeffs, pred = _edit_blocks(hb, 600, seed, **opts)
+    assert _diff(gpu_ctx.residual_blocks(tus, n, coeffs, pred), port.residual_blocks(tus, n, coeffs, pred)) == 0
+
+
+def test_gpu_blocks_empty(hb, gpu_ctx):
+    tus, n, coeffs, pred = hb.blocks(0, 1)
+    assert gpu_ctx.residual_blocks(tus, 0, coeffs, pred).size == pred.size
+
+
+@pytest.mark.parametrize("seed,w,h,kw", [(31, 176, 144, dict(p_intra=0.3)), (32, 64, 64, dict(slice_type=2)),
+                                         (33, 136, 72, dict(p_intra=0.2, p_skip=0.5, p_merge=0.6)),
+                                         (34, 256, 192, dict(p_intra=0.7, p_intra_nxn=1.0)),
+                                         (35, 320, 128, dict(p_wp=0.6, mv_range=4096)),
+                                         (36, 3840, 2160, dict(p_intra=0.1)),
+                                         (37, 1280, 720, dict(slice_type=2, strong_intra_smoothing=0))])
+def test_gpu_pictures(hb, gpu_ctx, port, seed, w, h, kw):
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+    refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
+    assert _diff(gpu_ctx.reconstruct_picture(pic, refs), port.reconstruct_picture(pic, refs)) == 0
+
+
+@pytest.mark.parametrize("seed,w,h", [(41, 320, 192), (42, 200, 136), (43, 1920, 1080)])
+def test_gpu_filters_with_slices_pcm_bypass(hb, gpu_ctx, port, seed, w, h):
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **cases.FILTERS))
+    keep = with_filter_edits(hb, pic, seed)
+    src = hb.content(w, h, seed)
+    for db, sao in [(True, True), (True, False), (False, True)]:
+        assert _diff(gpu_ctx.loop_filter(pic, src, db, sao), port.loop_filter(pic, src, db, sao)) == 0, (db, sao)
+    del keep
+
+
+def test_dpb_jobs_plain_and_batched(hb, gpu_ctx, port):
+    """Pictures of three streams of different sizes through the DPB API: plain launches
+    and one batched launch give the oracle's pictures, and relaunching a prepared job
+    reproduces the same output."""
+    specs = [(416, 240, 51), (1920, 1080, 52), (208, 120, 53)]
+    streams, jobs, want, pics = [], [], [], []
+    for (w, h, seed) in specs:
+        st = gpu_ctx.open_stream(w, h, 3)
+        refs = [hb.content(w, h, seed + 1), hb.content(w, h, seed + 2)]
+        st.upload(0, refs[0])
+        st.upload(1, refs[1])
+        pic = hb.Picture(hb.default_cfg(w, h, seed, **cases.PICTURE))
+        pics.append(pic)
+        want.append(port.reconstruct_picture(pic, refs))
+        streams.append(st)
+        jobs.append(st.prepare(pic))
+    for st, job, wnt in zip(streams, jobs, want):
+        job.launch(2)
+        st.sync()
+        assert _diff(st.download(2), wnt) == 0
+        job.launch(2)
+        st.sync()
+        assert _diff(st.download(2), wnt) == 0
+    # batched: clear the destinations first
+    for st in streams:
+        st.upload(2, np.zeros(hb.i420_size(st.width, st.height), np.uint8))
+    hb.batch_launch(jobs, [2, 2, 2])
+    gpu_ctx.sync()
+    for st, wnt in zip(streams, want):
+        assert _diff(st.download(2), wnt) == 0
+
+
+def test_picture_decode_end_to_end(hb, gpu_ctx, port):
+    w, h = 640, 360
+    st = gpu_ctx.open_stream(w, h, 3)
+    refs = [hb.content(w, h, 71), hb.content(w, h, 72)]
+    st.upload(0, refs[0])
+    st.upload(1, refs[1])
+    pic = hb.Picture(hb.default_cfg(w, h, 70, **cases.PICTURE))
+    st.decode(pic, 2)
+    assert _diff(st.download(2), port.reconstruct_picture(pic, refs)) == 0
+
+
+def test_invalid_records_are_refused(hb, gpu_ctx):
+    w, h = 128, 64
+    pic = hb.Picture(hb.default_cfg(w, h, 5, **cases.PICTURE))
+    refs = [hb.content(w, h, 1), hb.content(w, h, 2)]
+    s = pic.syn
+    t0 = s.tus[0]
+    old = (t0.x, t0.coeff_offset)
+    s.tus[0].x = 4000
+    with pytest.raises(hb.HevcGpuError) as e:
+        gpu_ctx.reconstruct_picture(pic, refs)
+    assert e.value.code == hb.abi.HEVCGPU_EINVAL
+    s.tus[0].x = old[0]
+    s.pus[0].ref_idx[0] = 9
+    with pytest.raises(hb.HevcGpuError):
+        gpu_ctx.reconstruct_picture(pic, refs)
+    st = gpu_ctx.open_stream(w, h, 2)
+    with pytest.raises(hb.HevcGpuError):
+        st.upload(5, refs[0])
+    with pytest.raises(hb.HevcGpuError):
+        gpu_ctx.open_stream(100, 60, 2)   # not a multiple of 8
+
+
+def test_budget_admission(hb, gpu_ctx):
+    from hevc_b200 import HevcGpuError
+    ctx = hb.Context(0)
+    ctx.set_budget(8 << 20)
+    with pytest.raises(HevcGpuError) as e:
+        ctx.open_stream(1920, 1080, 4)   # 4 x 3.1 MB > 8 MB
+    assert e.value.code == hb.abi.HEVCGPU_ENOMEM
+    st = ctx.open_stream(416, 240, 2)
+    assert ctx.bytes_in_use() <= 8 << 20
+    st.close()
+    ctx.close()
