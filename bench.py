@@ -90,7 +90,7 @@ def algorithmic_bytes(hb, pic):
     coded = (tu["f"] & 2) != 0
     intra = (tu["f"] & 1) != 0
     res = int((n2[coded & ~intra] * 4).sum() + (n2[coded & intra] * 4).sum())
-    intra_b = int((n2[intra] * 1 + n2[intra & coded] * 2).sum())
+    intra_b = int((n2 * intra).sum() + (2 * n2 * (intra & coded)).sum())
     pic_bytes = W * H * 3 // 2
     grid = (W // 4) * (H // 4) * 4
     return {"mc": mc_read + mc_write, "residual": res, "intra": intra_b,
@@ -341,8 +341,9 @@ def run_ours(args, hb, rank, world, local):
     if rank == 0 and not args.no_cpu_baseline:
         checker, kind = cpu_checker()
         threads = os.cpu_count() or 1
-        n = max(threads, 2 * B)
-        cpu_run(checker, pics, refs, threads, threads)
+        # bounded sample: about 10 s of wall time on all host threads
+        t_probe = cpu_run(checker, pics, refs, threads, threads)
+        n = threads * max(1, int(10.0 / max(t_probe, 1e-3)))
         t = cpu_run(checker, pics, refs, n, threads)
         cpu = {"value": round(n / t, 3), "unit": "frames/s", "cores": threads, "kind": kind,
                "sample": f"{n} of the bench's {W}x{H} pictures on {threads} host threads ({t:.1f} s)"}

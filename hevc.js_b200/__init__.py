@@ -24,6 +24,7 @@ error; here it is raised as ``HevcGpuError`` carrying the library's message.
 """
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -220,12 +221,20 @@ class Context:
 
     def __init__(self, device=0):
         self.lib = gpu_lib()
+        self._children = weakref.WeakSet()   # streams and jobs: closed before the context
         h = C.c_void_p()
         _check(self.lib.hevcgpu_create(device, C.byref(h)))
         self.h = h
 
     def close(self):
         if self.h:
+            kids = list(self._children)
+            for k in kids:
+                if isinstance(k, Job):
+                    k.free()
+            for k in kids:
+                if isinstance(k, Stream):
+                    k.close()
             self.lib.hevcgpu_destroy(self.h)
             self.h = None
 
@@ -310,11 +319,12 @@ class Stream:
         h = C.c_void_p()
         _check(self.lib.hevcgpu_stream_open(ctx.h, width, height, 8, slots, C.byref(h)))
         self.h = h
+        ctx._children.add(self)
 
     def close(self):
-        if self.h:
+        if self.h and self.ctx.h:
             self.lib.hevcgpu_stream_close(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -350,6 +360,7 @@ class Job:
         h = C.c_void_p()
         _check(self.lib.hevcgpu_job_prepare(stream.h, pic.syn_ptr, C.byref(h)))
         self.h = h
+        stream.ctx._children.add(self)
 
     def launch(self, dst_slot):
         _check(self.lib.hevcgpu_job_launch(self.h, dst_slot))
@@ -359,9 +370,9 @@ class Job:
         return int(self.lib.hevcgpu_job_upload_bytes(self.h))
 
     def free(self):
-        if self.h:
+        if self.h and self.stream.h and self.stream.ctx.h:
             self.lib.hevcgpu_job_free(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

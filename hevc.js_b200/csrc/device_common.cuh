@@ -40,8 +40,15 @@ struct PicDesc {
     const uint8_t* ctb_slice;            // may be null
     const uint16_t* ctb_tile;            // may be null
     const hevc_slice_t* slices;
-    const int32_t* intra_list;           // TU indices of intra TUs grouped by CTU and plane
-    const int32_t* intra_off;            // per CTU: 3 start offsets + next CTU's start
+    // intra dataflow: intra TUs in decode order and the DAG of which TU reads samples
+    // another one writes (built on the host from the reference-sample positions)
+    const int32_t* intra_list;           // TU index of each intra TU
+    const int32_t* dep_off;              // dependents of intra TU i: dep_list[dep_off[i]..[i+1])
+    const int32_t* dep_list;
+    const int32_t* init_count;           // number of intra TUs each one waits for
+    int32_t* count;                      // working copy, re-armed before every launch
+    const int32_t* ready;                // intra TUs that wait for none
+    int32_t n_intra, n_ready;
     int32_t num_pus;
     int32_t num_slices;
     int32_t log2_ctb, wctb, hctb;
@@ -52,6 +59,7 @@ struct PicDesc {
     int32_t cb_qp_offset, cr_qp_offset;
     int32_t tiles_check;                 // tiles enabled and no filtering across tiles
     int32_t slice_check;                 // more than one slice in the picture
+    int32_t pcm_bypass_any;              // some CU is PCM or transquant-bypass
 };
 
 // Work items ----------------------------------------------------------------------------
@@ -72,6 +80,7 @@ struct Seg {
     const PicDesc* pic;
     int32_t n_items;
     int32_t block0;
+    int32_t aux0, aux1;   // per-launch extras (intra arming: queue offsets)
 };
 struct SegTable {
     int32_t n;
@@ -94,6 +103,15 @@ enum ResMode : int32_t {
 // Device status word bits (written with atomicOr; read by the host after a sync).
 enum : uint32_t {
     ST_BAD_RECORD = 1u,   // a record pointed outside its picture; the item was skipped
+    ST_TIMEOUT = 2u,      // a bounded wait gave up; the kernel returned early
+};
+
+// Shared state of one intra dataflow launch (see intra.cuh).
+struct FlowState {
+    int32_t head;         // next queue slot to claim
+    int32_t tail;         // next queue slot to publish
+    uint32_t status;      // ST_* bits
+    int32_t pad;
 };
 
 __device__ __forceinline__ int clip3(int lo, int hi, int v) { return v < lo ? lo : (v > hi ? hi : v); }

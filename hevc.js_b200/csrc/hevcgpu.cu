@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "hevcgpu.h"
+#include "intra.cuh"
 #include "kernels.cuh"
 
 using namespace hevcgpu;
@@ -151,7 +152,39 @@ struct hevcgpu_ctx {
         auto it = host_sizes.find(p);
         if (it != host_sizes.end()) free_host.emplace(it->second, p);
     }
+    // intra dataflow: FlowState followed by the sticky status word, and the TU queue
+    void* flow = nullptr;
+    void* queue = nullptr;
+    size_t queue_bytes = 0;
+    int sm_count = 148;
+    int ensure_queue(size_t bytes) {
+        if (bytes <= queue_bytes) return HEVCGPU_OK;
+        cudaStreamSynchronize(stream);  // the old queue may still be in use
+        if (queue) cudaFree(queue);
+        queue = nullptr;
+        queue_bytes = 0;
+        bytes = (size_t)align_up((int64_t)bytes * 2, 1 << 16);
+        if (cudaMalloc(&queue, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(HEVCGPU_ENOMEM, "intra queue of %zu bytes", bytes);
+        }
+        queue_bytes = bytes;
+        return HEVCGPU_OK;
+    }
+    // Reads and clears the sticky device status; maps it to a return code.
+    int take_status() {
+        uint32_t st = 0;
+        uint32_t* sticky = reinterpret_cast<uint32_t*>(static_cast<FlowState*>(flow) + 1);
+        if (cudaMemcpy(&st, sticky, sizeof(st), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return fail(HEVCGPU_ECUDA, "reading the device status: %s", cudaGetErrorString(cudaGetLastError()));
+        if (!st) return HEVCGPU_OK;
+        cudaMemset(sticky, 0, sizeof(uint32_t));
+        if (st & ST_TIMEOUT) return fail(HEVCGPU_ETIMEOUT, "a bounded device wait gave up (status 0x%x)", st);
+        return fail(HEVCGPU_EDEVICE, "a kernel refused a record (status 0x%x)", st);
+    }
     ~hevcgpu_ctx() {
+        if (queue) cudaFree(queue);
+        if (flow) cudaFree(flow);
         for (auto e : ev_pool) cudaEventDestroy(e);
         for (auto& h : host_sizes) cudaFreeHost(h.first);
         for (auto& s : sizes) cudaFree(s.first);
@@ -228,8 +261,7 @@ struct hevcgpu_job {
     const int32_t* d_res[4] = {nullptr, nullptr, nullptr, nullptr};
     int32_t n_mc = 0;
     const McItem* d_mc = nullptr;
-    std::vector<int32_t> diag_off;      // per diagonal: start in d_ctus (size D+1)
-    const int32_t* d_ctus = nullptr;
+    int32_t n_intra = 0, n_ready = 0;   // intra TUs, and those without dependencies
     int32_t n_pus = 0;
     int has_intra = 0;
     int32_t dst_slot = -2;              // slot currently written into host_desc / desc
@@ -341,40 +373,68 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     const int ctb = 1 << p.log2_ctb;
     const int wctb = (W + ctb - 1) / ctb, hctb = (H + ctb - 1) / ctb, nctb = wctb * hctb;
 
-    // residual bins (coded TUs by size), intra lists
+    // residual bins (coded TUs by size) and the intra TUs in decode order
     std::vector<int32_t> bins[4];
-    std::vector<std::vector<int32_t>> per_ctu((size_t)nctb * 3);
+    std::vector<int32_t> intra_list;
     for (int i = 0; i < s->num_tus; i++) {
         const hevc_tu_t& t = s->tus[i];
         bool intra = t.flags & HEVC_TU_INTRA;
         if ((t.flags & HEVC_TU_CODED) && (stages & (intra ? ST_INTRA : ST_RESID))) bins[t.log2_size - 2].push_back(i);
-        if (intra && (stages & ST_INTRA)) {
-            int sub = t.c_idx ? 2 : 1;
-            int a = (t.y * sub / ctb) * wctb + (t.x * sub / ctb);
-            per_ctu[(size_t)a * 3 + t.c_idx].push_back(i);
-        }
+        if (intra && (stages & ST_INTRA)) intra_list.push_back(i);
     }
-    std::vector<int32_t> intra_list, intra_off((size_t)nctb * 3 + 1, 0);
-    for (size_t k = 0; k < per_ctu.size(); k++) {
-        intra_off[k] = (int32_t)intra_list.size();
-        intra_list.insert(intra_list.end(), per_ctu[k].begin(), per_ctu[k].end());
-    }
-    intra_off[per_ctu.size()] = (int32_t)intra_list.size();
     j->has_intra = !intra_list.empty();
-    // wavefront diagonals: CTU (rx, ry) on diagonal rx + 2*ry
-    int ndiag = wctb + 2 * (hctb - 1);
-    std::vector<int32_t> ctus;
-    j->diag_off.assign((size_t)ndiag + 1, 0);
-    for (int d = 0; d < ndiag; d++) {
-        j->diag_off[(size_t)d] = (int32_t)ctus.size();
-        for (int ry = 0; ry < hctb; ry++) {
-            int rx = d - 2 * ry;
-            if (rx < 0 || rx >= wctb) continue;
-            int a = ry * wctb + rx;
-            if (intra_off[(size_t)a * 3 + 3] > intra_off[(size_t)a * 3]) ctus.push_back(a);
+    // Intra dependency DAG.  Per plane, an owner map at 4-sample granularity records the
+    // latest intra TU written there; intra TU B depends on every earlier intra TU that
+    // owns a unit of B's reference row (x-1 .. x+2N-1 at y-1) or column (y .. y+2N-1 at
+    // x-1).  Units whose samples are unavailable to B (later CTBs, other slices) can only
+    // add edges the prediction does not need, which costs parallelism, never exactness.
+    const int n_intra = (int)intra_list.size();
+    std::vector<int32_t> dep_off((size_t)n_intra + 1, 0), dep_list, init_count((size_t)n_intra, 0), ready;
+    if (n_intra) {
+        std::vector<std::pair<int32_t, int32_t>> edges;  // (src, dst)
+        std::vector<int32_t> owner[3];
+        int uw[3], uh[3];
+        for (int c = 0; c < 3; c++) {
+            uw[c] = (c ? W / 2 : W) / 4;
+            uh[c] = (c ? H / 2 : H) / 4;
+            owner[c].assign((size_t)uw[c] * uh[c], -1);
         }
+        std::vector<int32_t> srcs;
+        for (int b = 0; b < n_intra; b++) {
+            const hevc_tu_t& t = s->tus[intra_list[(size_t)b]];
+            const int c = t.c_idx, n = 1 << t.log2_size;
+            std::vector<int32_t>& own = owner[c];
+            srcs.clear();
+            if (t.y > 0) {
+                const int uy = (t.y - 1) / 4;
+                const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(uw[c] - 1, (t.x + 2 * n - 1) / 4);
+                for (int ux = ux0; ux <= ux1; ux++) srcs.push_back(own[(size_t)uy * uw[c] + ux]);
+            }
+            if (t.x > 0) {
+                const int ux = (t.x - 1) / 4;
+                const int uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
+                for (int uy = uy0; uy <= uy1; uy++) srcs.push_back(own[(size_t)uy * uw[c] + ux]);
+            }
+            std::sort(srcs.begin(), srcs.end());
+            srcs.erase(std::unique(srcs.begin(), srcs.end()), srcs.end());
+            for (int32_t a : srcs)
+                if (a >= 0) {
+                    edges.emplace_back(a, b);
+                    init_count[(size_t)b]++;
+                }
+            for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++)
+                for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) own[(size_t)uy * uw[c] + ux] = b;
+        }
+        for (auto& e : edges) dep_off[(size_t)e.first + 1]++;
+        for (int b = 0; b < n_intra; b++) dep_off[(size_t)b + 1] += dep_off[(size_t)b];
+        dep_list.resize(edges.size());
+        std::vector<int32_t> fill(dep_off.begin(), dep_off.end() - 1);
+        for (auto& e : edges) dep_list[(size_t)fill[(size_t)e.first]++] = e.second;
+        for (int b = 0; b < n_intra; b++)
+            if (init_count[(size_t)b] == 0) ready.push_back(b);
     }
-    j->diag_off[(size_t)ndiag] = (int32_t)ctus.size();
+    j->n_intra = n_intra;
+    j->n_ready = (int32_t)ready.size();
     // MC tiles
     std::vector<McItem> mc;
     if (stages & ST_MC)
@@ -393,7 +453,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         }
     j->n_pus = s->num_pus;
 
-    size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc, o_il, o_io, o_ctus;
+    size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc, o_il, o_do, o_dl, o_ic,
+        o_rd;
     hevc_slice_t dflt{0, 0, 0, 1};
     auto pack = [&](Packer& pk) {
         o_tus = pk.add(s->tus, sizeof(hevc_tu_t) * (size_t)std::max(0, s->num_tus));
@@ -409,8 +470,10 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         for (int k = 0; k < 4; k++) o_res[k] = pk.add(bins[k].data(), sizeof(int32_t) * bins[k].size());
         o_mc = pk.add(mc.data(), sizeof(McItem) * mc.size());
         o_il = pk.add(intra_list.data(), sizeof(int32_t) * intra_list.size());
-        o_io = pk.add(intra_off.data(), sizeof(int32_t) * intra_off.size());
-        o_ctus = pk.add(ctus.data(), sizeof(int32_t) * ctus.size());
+        o_do = pk.add(dep_off.data(), sizeof(int32_t) * dep_off.size());
+        o_dl = pk.add(dep_list.data(), sizeof(int32_t) * dep_list.size());
+        o_ic = pk.add(init_count.data(), sizeof(int32_t) * init_count.size());
+        o_rd = pk.add(ready.data(), sizeof(int32_t) * ready.size());
     };
     Packer measure;
     pack(measure);
@@ -426,9 +489,10 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     j->upload_bytes = img + sizeof(PicDesc);
     uint8_t* base = static_cast<uint8_t*>(j->recs.p);
 
-    size_t resid_bytes = j->has_intra ? sizeof(int16_t) * (size_t)align_up((int64_t)s->num_coeffs, 8) : 0;
-    size_t mot_bytes = (stages & ST_DEBLOCK) ? sizeof(MotionEnt) * (size_t)gw * gh : 0;
-    rc = j->scratch.get(ctx, std::max<size_t>(resid_bytes + mot_bytes, 256));
+    size_t resid_bytes = j->has_intra ? sizeof(int16_t) * (size_t)align_up((int64_t)s->num_coeffs, 128) : 0;
+    size_t mot_bytes = (stages & ST_DEBLOCK) ? sizeof(MotionEnt) * (size_t)align_up((int64_t)gw * gh, 32) : 0;
+    size_t count_bytes = sizeof(int32_t) * (size_t)n_intra;
+    rc = j->scratch.get(ctx, std::max<size_t>(resid_bytes + mot_bytes + count_bytes, 256));
     if (rc) return rc;
     rc = j->desc.get(ctx, sizeof(PicDesc));
     if (rc) return rc;
@@ -457,7 +521,13 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     D.ctb_tile = (s->ctb_tile && p.tiles_enabled) ? reinterpret_cast<const uint16_t*>(base + o_ti) : nullptr;
     D.slices = reinterpret_cast<const hevc_slice_t*>(base + o_slices);
     D.intra_list = reinterpret_cast<const int32_t*>(base + o_il);
-    D.intra_off = reinterpret_cast<const int32_t*>(base + o_io);
+    D.dep_off = reinterpret_cast<const int32_t*>(base + o_do);
+    D.dep_list = reinterpret_cast<const int32_t*>(base + o_dl);
+    D.init_count = reinterpret_cast<const int32_t*>(base + o_ic);
+    D.ready = reinterpret_cast<const int32_t*>(base + o_rd);
+    D.count = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(j->scratch.p) + resid_bytes + mot_bytes);
+    D.n_intra = n_intra;
+    D.n_ready = (int32_t)ready.size();
     D.num_pus = s->num_pus;
     D.num_slices = std::max(1, (int)s->num_slices);
     D.log2_ctb = p.log2_ctb;
@@ -474,13 +544,17 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     if (s->ctb_slice)
         for (int a = 1; a < nctb && !multi; a++) multi = s->ctb_slice[a] != s->ctb_slice[0];
     D.slice_check = multi ? 1 : 0;
+    bool pcm_bypass = false;
+    if (s->blk)
+        for (size_t i = 0; i < (size_t)gw * gh && !pcm_bypass; i++)
+            pcm_bypass = (s->blk[i] & (HEVC_BLK_PCM | HEVC_BLK_BYPASS)) != 0;
+    D.pcm_bypass_any = pcm_bypass ? 1 : 0;
     for (int k = 0; k < 4; k++) {
         j->n_res[k] = (int32_t)bins[k].size();
         j->d_res[k] = reinterpret_cast<const int32_t*>(base + o_res[k]);
     }
     j->n_mc = (int32_t)mc.size();
     j->d_mc = reinterpret_cast<const McItem*>(base + o_mc);
-    j->d_ctus = reinterpret_cast<const int32_t*>(base + o_ctus);
     return HEVCGPU_OK;
 }
 
@@ -617,14 +691,32 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
     }
     if (stages & ST_INTRA) {
         StageMark m(ctx, 3);
-        size_t nd = 0;
-        for (int k = 0; k < n; k++) nd = std::max(nd, jobs[k]->diag_off.size());
-        for (size_t d = 0; d + 1 < nd; d++) {
-            rc = L.items(k_intra_ctu, jobs, n, 1, 96, [d](hevcgpu_job* j, const void*& p, int& c) {
-                if (d + 1 >= j->diag_off.size()) { p = nullptr; c = 0; return; }
-                p = j->d_ctus + j->diag_off[d];
-                c = j->diag_off[d + 1] - j->diag_off[d];
-            });
+        // one arm + one persistent dataflow launch per group of up to MAX_SEGS pictures
+        int k = 0;
+        while (k < n) {
+            SegTable t;
+            std::memset(&t, 0, sizeof(t));
+            int total = 0, n_ready = 0, max_intra = 0;
+            for (; k < n && t.n < MAX_SEGS; k++) {
+                hevcgpu_job* j = jobs[k];
+                if (j->n_intra == 0) continue;
+                Seg& sg = t.s[t.n++];
+                sg.pic = static_cast<const PicDesc*>(j->desc.p);
+                sg.aux0 = n_ready;
+                sg.aux1 = total;
+                total += j->n_intra;
+                n_ready += j->n_ready;
+                max_intra = std::max(max_intra, j->n_intra);
+            }
+            if (t.n == 0) continue;
+            if ((rc = ctx->ensure_queue(sizeof(int32_t) * (size_t)total))) return rc;
+            FlowState* fs = static_cast<FlowState*>(ctx->flow);
+            uint32_t* sticky = reinterpret_cast<uint32_t*>(fs + 1);
+            int32_t* queue = static_cast<int32_t*>(ctx->queue);
+            rc = L.go(k_intra_arm, dim3((max_intra + 255) / 256, t.n), dim3(256), t, fs, queue, n_ready);
+            if (rc) return rc;
+            int ctas = std::min((total + IF_WARPS - 1) / IF_WARPS, ctx->sm_count * 4);
+            rc = L.go(k_intra_flow, dim3(ctas), dim3(32 * IF_WARPS), t, fs, queue, total, sticky);
             if (rc) return rc;
         }
     }
@@ -707,10 +799,13 @@ int hevcgpu_create(int device, hevcgpu_ctx_t** out) {
     auto* c = new (std::nothrow) hevcgpu_ctx();
     if (!c) return fail(HEVCGPU_ENOMEM, "host allocation");
     c->device = device;
+    c->sm_count = prop.multiProcessorCount;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->flow, sizeof(FlowState) + 16);
+    if (e == cudaSuccess) e = cudaMemset(c->flow, 0, sizeof(FlowState) + 16);
     if (e != cudaSuccess) {
         delete c;
-        return fail(HEVCGPU_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+        return fail(HEVCGPU_ECUDA, "context set-up: %s", cudaGetErrorString(e));
     }
     *out = c;
     return HEVCGPU_OK;
@@ -727,7 +822,7 @@ int hevcgpu_sync(hevcgpu_ctx_t* ctx) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return HEVCGPU_OK;
+    return ctx->take_status();
 }
 
 void* hevcgpu_cuda_stream(hevcgpu_ctx_t* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
@@ -839,7 +934,7 @@ int run_host_picture(hevcgpu_ctx* ctx, const hevc_picture_syntax_t* syn, int sta
     const uint8_t* result = (stages & ST_SAO) ? static_cast<uint8_t*>(dst.p) : static_cast<uint8_t*>(j.rec.p);
     if ((rc = download_i420(ctx, L, result, out))) return rc;
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return HEVCGPU_OK;
+    return ctx->take_status();
 }
 
 }  // namespace
@@ -1028,7 +1123,7 @@ int hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, i
 int hevcgpu_stream_sync(hevcgpu_stream_t* st) {
     if (!st) return fail(HEVCGPU_EINVAL, "null stream");
     CUDA_TRY(cudaStreamSynchronize(st->ctx->stream));
-    return HEVCGPU_OK;
+    return st->ctx->take_status();
 }
 
 int hevcgpu_profile_enable(hevcgpu_ctx_t* ctx, int enable) {
@@ -1065,7 +1160,8 @@ int hevcgpu_picture_decode(hevcgpu_stream_t* st, const hevc_picture_syntax_t* sy
     rc = hevcgpu_job_launch(j, dst_slot);
     if (rc == HEVCGPU_OK) {
         cudaError_t e = cudaStreamSynchronize(st->ctx->stream);
-        if (e != cudaSuccess) rc = fail(HEVCGPU_ECUDA, "picture decode: %s", cudaGetErrorString(e));
+        rc = e != cudaSuccess ? fail(HEVCGPU_ECUDA, "picture decode: %s", cudaGetErrorString(e))
+                              : st->ctx->take_status();
     }
     hevcgpu_job_free(j);
     return rc;

@@ -4,8 +4,7 @@
 //                     (transform.cpp:293-394, coding_tree.cpp:371-396)
 //   k_mc              8-tap/4-tap interpolation + default/explicit weighting
 //                     (interpolation.cpp:45-411)
-//   k_intra_ctu       intra prediction of the intra TUs of one CTU per CTA, CTUs of one
-//                     wavefront diagonal per launch (intra_prediction.cpp:44-481)
+//   (intra prediction: intra.cuh)
 //   k_motion_grid     4x4 motion grid of the PUs (store_pu_motion's grid)
 //   k_deblock<V>      Bs + decisions + luma/chroma filters of one edge direction
 //                     (deblocking.cpp:50-614)
@@ -246,17 +245,37 @@ __device__ __forceinline__ void mc_block(const uint8_t* __restrict__ plane, int 
                                          int yi, int fx, int fy, int bw, int bh, uint8_t* win, int wpitch,
                                          int16_t* tmp, int lane, int (&pred)[MAXE]) {
     constexpr int HALF = NT / 2 - 1;
+    constexpr int WMAX = NT == 8 ? 23 * 23 : 11 * 11;  // largest window (16x16 / 8x8 block)
+    constexpr int ITER = (WMAX + 31) / 32;
     const int ww = bw + NT - 1, wh = bh + NT - 1;
     const int x0 = xi - HALF, y0 = yi - HALF;
     const bool interior = x0 >= 0 && y0 >= 0 && x0 + ww <= pw && y0 + wh <= ph;
-    for (int e = lane; e < ww * wh; e += 32) {
-        int r = e / ww, c = e - r * ww;
-        int yy = y0 + r, xx = x0 + c;
-        if (!interior) {
-            yy = clip3(0, ph - 1, yy);
-            xx = clip3(0, pw - 1, xx);
+    // all loads of this lane first (they are in flight together), then the stores
+    uint8_t v[ITER];
+    {
+        int r = lane / ww, c = lane - r * ww;
+#pragma unroll
+        for (int k = 0; k < ITER; k++) {
+            if (lane + 32 * k < ww * wh) {
+                int yy = y0 + r, xx = x0 + c;
+                if (!interior) {
+                    yy = clip3(0, ph - 1, yy);
+                    xx = clip3(0, pw - 1, xx);
+                }
+                v[k] = __ldg(plane + (int64_t)yy * pitch + xx);
+            }
+            c += 32;
+            while (c >= ww) { c -= ww; r++; }
         }
-        win[r * wpitch + c] = __ldg(plane + (int64_t)yy * pitch + xx);
+    }
+    {
+        int r = lane / ww, c = lane - r * ww;
+#pragma unroll
+        for (int k = 0; k < ITER; k++) {
+            if (lane + 32 * k < ww * wh) win[r * wpitch + c] = v[k];
+            c += 32;
+            while (c >= ww) { c -= ww; r++; }
+        }
     }
     __syncwarp();
     const int8_t* th = NT == 8 ? c_luma_taps[fx] : c_chroma_taps[fx];
@@ -392,219 +411,6 @@ __global__ void __launch_bounds__(32 * MC_WARPS) k_mc(const __grid_constant__ Se
         }
         mc_weight_store<2>(pl[0], pl[1], use[0], use[1], wp, ci, P.rec + off + (int64_t)cy * P.pitch_c + cx,
                            P.pitch_c, cw, ch, lane);
-    }
-}
-
-// ======================================================================================
-// Intra prediction, one CTA per CTU, one warp per colour plane.  The warp copies the CTU
-// and its top/left neighbourhood into shared memory, then walks its plane's intra TUs
-// in decode order: reference samples with availability and substitution, optional
-// [1 2 1] or bilinear smoothing, planar/DC/angular prediction, + residual, clip; each
-// result is written to shared memory (for the next TU) and to the picture.
-// ======================================================================================
-constexpr int IT_LW = 129, IT_LH = 65;  // luma tile: cols -1..127, rows -1..63
-constexpr int IT_CW = 65, IT_CH = 33;   // chroma tile
-__constant__ int8_t c_intra_angle[35] = {0,   0,   32,  26,  21,  17,  13,  9,  5,  2,  0,  -2,
-                                         -5,  -9,  -13, -17, -21, -26, -32, -26, -21, -17, -13, -9,
-                                         -5,  -2,  0,   2,   5,   9,   13,  17,  21,  26,  32};
-__constant__ int16_t c_inv_angle[35] = {0,    0,    256, 315, 390, 482,  630,  910,  1638, 4096, 0,   4096,
-                                        1638, 910,  630, 482, 390, 315,  256,  315,  390,  482,  630, 910,
-                                        1638, 4096, 0,   4096, 1638, 910, 630, 482,  390,  315,  256};
-
-struct IntraWarpSmem {
-    int16_t s[129];   // substituted reference samples (bottom-left .. corner .. top-right)
-    int16_t f[129];   // filtered copy
-    int16_t raw[129];
-};
-
-__global__ void __launch_bounds__(96) k_intra_ctu(const __grid_constant__ SegTable st) {
-    __shared__ uint8_t t_luma[IT_LH * IT_LW];
-    __shared__ uint8_t t_chroma[2][IT_CH * IT_CW];
-    __shared__ IntraWarpSmem ws[3];
-    const int ci = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const Seg& sg = st.s[find_seg(st, blockIdx.x)];
-    const int item = blockIdx.x - sg.block0;
-    if (item >= sg.n_items) return;
-    struct { int ctu; } it = {static_cast<const int32_t*>(sg.items)[item]};
-    const PicDesc& P = *sg.pic;
-    const int beg = P.intra_off[it.ctu * 3 + ci], end = P.intra_off[it.ctu * 3 + ci + 1];
-    if (beg >= end) return;
-
-    const int sub = ci ? 2 : 1;
-    const int ctb = 1 << P.log2_ctb, ctbc = ctb / sub;
-    const int rx = it.ctu % P.wctb, ry = it.ctu / P.wctb;
-    const int pw = P.width / sub, ph = P.height / sub;
-    const int cx0 = rx * ctbc, cy0 = ry * ctbc;      // CTU origin, plane coordinates
-    const int ox = rx * ctb, oy = ry * ctb;          // CTU origin, luma
-    const int tw = ci ? IT_CW : IT_LW;               // tile pitch; tile (0,0) = (cx0-1, cy0-1)
-    uint8_t* tile = ci ? t_chroma[ci - 1] : t_luma;
-    const int pitch = ci ? P.pitch_c : P.pitch_y;
-    uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));
-    const int cur_slice = P.ctb_slice ? P.ctb_slice[it.ctu] : 0;
-    const int cur_tile = P.ctb_tile ? P.ctb_tile[it.ctu] : 0;
-
-    // stage the neighbourhood: row -1 (cols -1 .. 2*ctbc-1), col -1 (rows 0..ctbc-1), interior
-    {
-        const int row_n = 2 * ctbc + 1;
-        for (int e = lane; e < row_n; e += 32) {
-            int x = cx0 - 1 + e, y = cy0 - 1;
-            if (x >= 0 && y >= 0 && x < pw) tile[e] = plane[(int64_t)y * pitch + x];
-        }
-        for (int e = lane; e < ctbc; e += 32) {
-            int x = cx0 - 1, y = cy0 + e;
-            if (x >= 0 && y < ph) tile[(e + 1) * tw] = plane[(int64_t)y * pitch + x];
-        }
-        for (int e = lane; e < ctbc * ctbc / 4; e += 32) {
-            int r = e / (ctbc / 4), c4 = (e % (ctbc / 4)) * 4;
-            int x = cx0 + c4, y = cy0 + r;
-            if (y < ph && x < pw) {
-                uint32_t v = *reinterpret_cast<const uint32_t*>(plane + (int64_t)y * pitch + x);
-                uint8_t* d = tile + (r + 1) * tw + c4 + 1;
-                d[0] = v & 0xFF; d[1] = (v >> 8) & 0xFF; d[2] = (v >> 16) & 0xFF; d[3] = v >> 24;
-            }
-        }
-    }
-    __syncwarp();
-
-    IntraWarpSmem& W = ws[ci];
-    const int cur_addr = it.ctu;
-    for (int li = beg; li < end; li++) {
-        const hevc_tu_t t = P.tus[P.intra_list[li]];
-        const int n = 1 << t.log2_size, log2 = t.log2_size;
-        const int xc = t.x, yc = t.y;
-        const uint32_t cur_z = zorder16((uint32_t)((xc * sub - ox) >> 2), (uint32_t)((yc * sub - oy) >> 2));
-        const int total = 4 * n + 1;
-
-        // 1. reference samples and their availability (build_reference_samples)
-        uint32_t mask[5];
-#pragma unroll
-        for (int r = 0; r < 5; r++) {
-            int i = lane + 32 * r;
-            bool ok = false;
-            int val = 0;
-            if (i < total) {
-                int px, py;
-                if (i < 2 * n) { px = xc - 1; py = yc + 2 * n - 1 - i; }
-                else if (i == 2 * n) { px = xc - 1; py = yc - 1; }
-                else { px = xc + (i - 2 * n - 1); py = yc - 1; }
-                if (px >= 0 && py >= 0 && px < pw && py < ph) {
-                    int ncx = px / ctbc, ncy = py / ctbc;
-                    if (ncx != rx || ncy != ry) {
-                        int a = ncy * P.wctb + ncx;
-                        ok = a < cur_addr && (P.ctb_slice ? P.ctb_slice[a] : 0) == cur_slice &&
-                             (P.ctb_tile ? P.ctb_tile[a] : 0) == cur_tile;
-                    } else {
-                        ok = zorder16((uint32_t)((px * sub - ox) >> 2), (uint32_t)((py * sub - oy) >> 2)) < cur_z;
-                    }
-                    if (ok) val = tile[(py - cy0 + 1) * tw + (px - cx0 + 1)];
-                }
-                W.raw[i] = (int16_t)val;
-            }
-            mask[r] = __ballot_sync(0xffffffffu, ok);
-        }
-        __syncwarp();
-        // 2. substitution: nearest available below, else the first available
-        int first = -1;
-#pragma unroll
-        for (int r = 0; r < 5; r++)
-            if (first < 0 && mask[r]) first = 32 * r + __ffs(mask[r]) - 1;
-#pragma unroll
-        for (int r = 0; r < 5; r++) {
-            int i = lane + 32 * r;
-            if (i >= total) continue;
-            int v;
-            if (first < 0) v = 128;
-            else if ((mask[r] >> lane) & 1u) v = W.raw[i];
-            else {
-                int j = -1;
-                uint32_t m = lane ? (mask[r] & ((1u << lane) - 1u)) : 0u;
-                if (m) j = 32 * r + 31 - __clz(m);
-                for (int q = r - 1; q >= 0 && j < 0; q--)
-                    if (mask[q]) j = 32 * q + 31 - __clz(mask[q]);
-                v = W.raw[j < 0 ? first : j];
-            }
-            W.s[i] = (int16_t)v;
-        }
-        __syncwarp();
-        // 3. smoothing of luma references (intra_prediction.cpp:217-257, :443-471)
-        const int mode = t.intra_mode;
-        const int16_t* R = W.s;
-        if (ci == 0 && !P.intra_smoothing_disabled && mode != 1 && n != 4) {
-            int d = min(abs(mode - 26), abs(mode - 10));
-            int thr = n == 8 ? 7 : (n == 16 ? 1 : 0);
-            if (d > thr) {
-                bool bil = false;
-                if (P.strong_intra && n == 32) {
-                    int c = W.s[2 * n];
-                    bil = abs(c + W.s[4 * n] - 2 * W.s[3 * n]) < 8 && abs(c + W.s[0] - 2 * W.s[n]) < 8;
-                }
-#pragma unroll
-                for (int r = 0; r < 5; r++) {
-                    int i = lane + 32 * r;
-                    if (i >= total) continue;
-                    int v;
-                    if (i == 0 || i == 4 * n) v = W.s[i];
-                    else if (bil) {
-                        if (i == 2 * n) v = W.s[i];
-                        else if (i > 2 * n) { int k = i - 2 * n; v = ((2 * n - k) * W.s[2 * n] + k * W.s[4 * n] + n) >> (log2 + 1); }
-                        else { int k = 2 * n - i; v = ((2 * n - k) * W.s[2 * n] + k * W.s[0] + n) >> (log2 + 1); }
-                    } else {
-                        v = (W.s[i - 1] + 2 * W.s[i] + W.s[i + 1] + 2) >> 2;
-                    }
-                    W.f[i] = (int16_t)v;
-                }
-                __syncwarp();
-                R = W.f;
-            }
-        }
-        // 4. prediction + residual (top[k] = R[2n + k], left[k] = R[2n - k])
-        const int16_t* res = (t.flags & HEVC_TU_CODED) ? P.resid + t.coeff_offset : nullptr;
-        const int ang = c_intra_angle[mode];
-        const int inv = c_inv_angle[mode];
-        int dc = 0;
-        if (mode == 1) {
-            int s = 0;
-            for (int i = lane; i < n; i += 32) s += R[2 * n + 1 + i] + R[2 * n - 1 - i];
-            s = __reduce_add_sync(0xffffffffu, s);
-            dc = (s + n) >> (log2 + 1);
-        }
-        for (int e = lane; e < n * n; e += 32) {
-            int y = e >> log2, x = e & (n - 1);
-            int p;
-            if (mode == 0) {
-                p = ((n - 1 - x) * R[2 * n - 1 - y] + (x + 1) * R[3 * n + 1] + (n - 1 - y) * R[2 * n + 1 + x] +
-                     (y + 1) * R[n - 1] + n) >> (log2 + 1);
-            } else if (mode == 1) {
-                p = dc;
-                if (ci == 0 && n < 32) {
-                    if (x == 0 && y == 0) p = (R[2 * n + 1] + R[2 * n - 1] + 2 * dc + 2) >> 2;
-                    else if (y == 0) p = (R[2 * n + 1 + x] + 3 * dc + 2) >> 2;
-                    else if (x == 0) p = (R[2 * n - 1 - y] + 3 * dc + 2) >> 2;
-                }
-            } else {
-                const bool vert = mode >= 18;
-                const int pos = vert ? y : x, ln = vert ? x : y;
-                const int idx = ((pos + 1) * ang) >> 5, fr = ((pos + 1) * ang) & 31;
-                const int ri = ln + 1 + idx;
-                // main reference (top for vertical, left for horizontal); negative indices
-                // project onto the side reference through invAngle (:346-368)
-                auto ref_at = [&](int q) -> int {
-                    if (q >= 0) return vert ? R[2 * n + q] : R[2 * n - q];
-                    int si = min(2 * n, ((-q) * inv + 128) >> 8);
-                    return vert ? R[2 * n - si] : R[2 * n + si];
-                };
-                p = fr ? ((32 - fr) * ref_at(ri) + fr * ref_at(ri + 1) + 16) >> 5 : ref_at(ri);
-                if (ci == 0 && n < 32) {
-                    if (mode == 26 && x == 0) p = clip_u8(p + ((R[2 * n - 1 - y] - R[2 * n]) >> 1));
-                    else if (mode == 10 && y == 0) p = clip_u8(p + ((R[2 * n + 1 + x] - R[2 * n]) >> 1));
-                }
-            }
-            int v = clip_u8(p + (res ? res[e] : 0));
-            int lx = xc - cx0, ly = yc - cy0;
-            tile[(ly + y + 1) * tw + lx + x + 1] = (uint8_t)v;
-            if (xc + x < pw && yc + y < ph) plane[(int64_t)(yc + y) * pitch + xc + x] = (uint8_t)v;
-        }
-        __syncwarp();
     }
 }
 
@@ -874,7 +680,7 @@ __global__ void __launch_bounds__(256) k_sao(const __grid_constant__ SegTable st
     const int64_t base = ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr);
     const uint8_t* S = P.rec + base;
     uint8_t* D = P.dst + base;
-    const uint32_t c4 = *reinterpret_cast<const uint32_t*>(S + (int64_t)y * pitch + x);
+    const uint32_t c4 = __ldg(reinterpret_cast<const uint32_t*>(S + (int64_t)y * pitch + x));
     uint32_t out = c4;
     const int ctbc = (1 << P.log2_ctb) / sub;
     const int addr = (y / ctbc) * P.wctb + x / ctbc;
@@ -883,17 +689,38 @@ __global__ void __launch_bounds__(256) k_sao(const __grid_constant__ SegTable st
     if (type != 0) {
         const int gw = P.width >> 2;
         const bool check_slices = P.slice_check || P.tiles_check;
+        // edge offset: the words left of, at and right of the group in the rows the
+        // class needs (neighbours outside the picture are never read)
+        const int cl = sp.eo_class[ci];
+        const int dx0 = cl == 1 ? 0 : (cl == 3 ? 1 : -1), dy0 = cl == 0 ? 0 : -1;
+        const int dx1 = -dx0, dy1 = -dy0;
+        // per neighbour row k: samples x-1 .. x+4 packed into bytes 0..5 of nw[k]
+        uint64_t nw[2] = {0, 0};
+        if (type == 2) {
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int yy = y + (k ? dy1 : dy0);
+                if (yy < 0 || yy >= ph) continue;
+                const uint32_t* row = reinterpret_cast<const uint32_t*>(S + (int64_t)yy * pitch + x);
+                const uint32_t mid = yy == y ? c4 : __ldg(row);
+                const uint32_t lo = x >= 4 ? __ldg(row - 1) : 0u;
+                const uint32_t hi = x + 4 < pw ? __ldg(row + 1) : 0u;
+                nw[k] = (uint64_t)(lo >> 24) | ((uint64_t)mid << 8) | ((uint64_t)(hi & 0xFFu) << 40);
+            }
+        }
+        auto nbyte = [&](int k, int off) -> int {  // sample at x + off (off in -1..4) of row k
+            return (int)((nw[k] >> (8 * (off + 1))) & 0xFFu);
+        };
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const int xs = x + i;
-            const uint32_t b = P.blk[(int64_t)((y * sub) >> 2) * gw + ((xs * sub) >> 2)];
-            if ((P.pcm_lf_disabled && (b & HEVC_BLK_PCM)) || (b & HEVC_BLK_BYPASS)) continue;
+            if (P.pcm_bypass_any) {
+                const uint32_t b = P.blk[(int64_t)((y * sub) >> 2) * gw + ((xs * sub) >> 2)];
+                if ((P.pcm_lf_disabled && (b & HEVC_BLK_PCM)) || (b & HEVC_BLK_BYPASS)) continue;
+            }
             const int c = (c4 >> (8 * i)) & 0xFF;
             int v;
             if (type == 2) {
-                const int cl = sp.eo_class[ci];
-                const int dx0 = cl == 1 ? 0 : (cl == 3 ? 1 : -1), dy0 = cl == 0 ? 0 : -1;
-                const int dx1 = -dx0, dy1 = -dy0;
                 const int ax = xs + dx0, ay = y + dy0, bx = xs + dx1, by = y + dy1;
                 if (ax < 0 || ay < 0 || ax >= pw || ay >= ph || bx < 0 || by < 0 || bx >= pw || by >= ph) continue;
                 if (check_slices) {
@@ -911,7 +738,7 @@ __global__ void __launch_bounds__(256) k_sao(const __grid_constant__ SegTable st
                     }
                     if (skip) continue;
                 }
-                const int a = S[(int64_t)ay * pitch + ax], bb = S[(int64_t)by * pitch + bx];
+                const int a = nbyte(0, i + dx0), bb = nbyte(1, i + dx1);
                 const int e = 2 + (c < a ? -1 : (c > a ? 1 : 0)) + (c < bb ? -1 : (c > bb ? 1 : 0));
                 v = c + sp.offset[ci][e];
             } else {
