@@ -40,15 +40,16 @@ struct PicDesc {
     const uint8_t* ctb_slice;            // may be null
     const uint16_t* ctb_tile;            // may be null
     const hevc_slice_t* slices;
-    // intra dataflow: intra TUs in decode order and the DAG of which TU reads samples
-    // another one writes (built on the host from the reference-sample positions)
-    const int32_t* intra_list;           // TU index of each intra TU
-    const int32_t* dep_off;              // dependents of intra TU i: dep_list[dep_off[i]..[i+1])
-    const int32_t* dep_list;
-    const int32_t* init_count;           // number of intra TUs each one waits for
-    int32_t* count;                      // working copy, re-armed before every launch
-    const int32_t* ready;                // intra TUs that wait for none
-    int32_t n_intra, n_ready;
+    // intra CTU tasks (intra.cuh): the CTUs that hold intra TUs, raster order, and their
+    // TUs ordered by level of the CTU-local dependency DAG
+    const int32_t* ictu_addr;            // raster address of intra CTU k
+    const int32_t* ictu_deps;            // 4 per intra CTU: intra CTUs it reads from, or -1
+    const int32_t* ictu_tu_off;          // TUs of intra CTU k: itu[ictu_tu_off[k] .. [k+1])
+    const int32_t* itu;                  // TU index
+    const int32_t* itu_level_end;        // first entry of the next level of the same CTU
+    const int32_t* itu_res_off;          // residual offset inside the CTU's staged residuals
+    int32_t* ictu_done;                  // per intra CTU: epoch of its last completion
+    int32_t n_ictu;
     int32_t num_pus;
     int32_t num_slices;
     int32_t log2_ctb, wctb, hctb;

@@ -152,25 +152,9 @@ struct hevcgpu_ctx {
         auto it = host_sizes.find(p);
         if (it != host_sizes.end()) free_host.emplace(it->second, p);
     }
-    // intra dataflow: FlowState followed by the sticky status word, and the TU queue
+    // intra wavefront: FlowState (row ticket) followed by the sticky status word
     void* flow = nullptr;
-    void* queue = nullptr;
-    size_t queue_bytes = 0;
     int sm_count = 148;
-    int ensure_queue(size_t bytes) {
-        if (bytes <= queue_bytes) return HEVCGPU_OK;
-        cudaStreamSynchronize(stream);  // the old queue may still be in use
-        if (queue) cudaFree(queue);
-        queue = nullptr;
-        queue_bytes = 0;
-        bytes = (size_t)align_up((int64_t)bytes * 2, 1 << 16);
-        if (cudaMalloc(&queue, bytes) != cudaSuccess) {
-            cudaGetLastError();
-            return fail(HEVCGPU_ENOMEM, "intra queue of %zu bytes", bytes);
-        }
-        queue_bytes = bytes;
-        return HEVCGPU_OK;
-    }
     // Reads and clears the sticky device status; maps it to a return code.
     int take_status() {
         uint32_t st = 0;
@@ -183,7 +167,6 @@ struct hevcgpu_ctx {
         return fail(HEVCGPU_EDEVICE, "a kernel refused a record (status 0x%x)", st);
     }
     ~hevcgpu_ctx() {
-        if (queue) cudaFree(queue);
         if (flow) cudaFree(flow);
         for (auto e : ev_pool) cudaEventDestroy(e);
         for (auto& h : host_sizes) cudaFreeHost(h.first);
@@ -261,7 +244,8 @@ struct hevcgpu_job {
     const int32_t* d_res[4] = {nullptr, nullptr, nullptr, nullptr};
     int32_t n_mc = 0;
     const McItem* d_mc = nullptr;
-    int32_t n_intra = 0, n_ready = 0;   // intra TUs, and those without dependencies
+    int32_t n_ictu = 0;                 // CTUs that hold intra TUs
+    int32_t epoch = 0;                  // intra launches of this job so far
     int32_t n_pus = 0;
     int has_intra = 0;
     int32_t dst_slot = -2;              // slot currently written into host_desc / desc
@@ -383,15 +367,17 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         if (intra && (stages & ST_INTRA)) intra_list.push_back(i);
     }
     j->has_intra = !intra_list.empty();
-    // Intra dependency DAG.  Per plane, an owner map at 4-sample granularity records the
-    // latest intra TU written there; intra TU B depends on every earlier intra TU that
-    // owns a unit of B's reference row (x-1 .. x+2N-1 at y-1) or column (y .. y+2N-1 at
-    // x-1).  Units whose samples are unavailable to B (later CTBs, other slices) can only
-    // add edges the prediction does not need, which costs parallelism, never exactness.
+    // Intra schedule.  Per plane an owner map at 4-sample granularity records the latest
+    // intra TU written there; intra TU B reads the units of its reference row
+    // (x-1 .. x+2N-1 at y-1) and column (y .. y+2N-1 at x-1).  An owner in B's CTU puts B
+    // one level above it in the CTU-local DAG; an owner in another CTU makes B's CTU wait
+    // for that CTU.  A unit whose samples B may not use (availability) can only add an
+    // unneeded level or wait, never change a sample.
     const int n_intra = (int)intra_list.size();
-    std::vector<int32_t> dep_off((size_t)n_intra + 1, 0), dep_list, init_count((size_t)n_intra, 0), ready;
+    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, itu, itu_level_end, itu_res_off;
     if (n_intra) {
-        std::vector<std::pair<int32_t, int32_t>> edges;  // (src, dst)
+        std::vector<int32_t> level((size_t)n_intra, 0), ctu_of((size_t)n_intra, 0);
+        std::vector<std::vector<int32_t>> ctu_deps((size_t)nctb);  // by CTU address
         std::vector<int32_t> owner[3];
         int uw[3], uh[3];
         for (int c = 0; c < 3; c++) {
@@ -399,42 +385,88 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             uh[c] = (c ? H / 2 : H) / 4;
             owner[c].assign((size_t)uw[c] * uh[c], -1);
         }
-        std::vector<int32_t> srcs;
         for (int b = 0; b < n_intra; b++) {
             const hevc_tu_t& t = s->tus[intra_list[(size_t)b]];
-            const int c = t.c_idx, n = 1 << t.log2_size;
+            const int c = t.c_idx, n = 1 << t.log2_size, sub = c ? 2 : 1;
+            const int a = ((t.y * sub) >> p.log2_ctb) * wctb + ((t.x * sub) >> p.log2_ctb);
+            ctu_of[(size_t)b] = a;
             std::vector<int32_t>& own = owner[c];
-            srcs.clear();
+            int lv = 0;
+            auto dep = [&](int ux, int uy) {
+                const int o = own[(size_t)uy * uw[c] + ux];
+                if (o < 0) return;
+                const int oa = ctu_of[(size_t)o];
+                if (oa == a) {
+                    lv = std::max(lv, level[(size_t)o] + 1);
+                } else {
+                    std::vector<int32_t>& dl = ctu_deps[(size_t)a];
+                    if (std::find(dl.begin(), dl.end(), oa) == dl.end()) dl.push_back(oa);
+                }
+            };
             if (t.y > 0) {
                 const int uy = (t.y - 1) / 4;
                 const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(uw[c] - 1, (t.x + 2 * n - 1) / 4);
-                for (int ux = ux0; ux <= ux1; ux++) srcs.push_back(own[(size_t)uy * uw[c] + ux]);
+                for (int ux = ux0; ux <= ux1; ux++) dep(ux, uy);
             }
             if (t.x > 0) {
                 const int ux = (t.x - 1) / 4;
                 const int uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
-                for (int uy = uy0; uy <= uy1; uy++) srcs.push_back(own[(size_t)uy * uw[c] + ux]);
+                for (int uy = uy0; uy <= uy1; uy++) dep(ux, uy);
             }
-            std::sort(srcs.begin(), srcs.end());
-            srcs.erase(std::unique(srcs.begin(), srcs.end()), srcs.end());
-            for (int32_t a : srcs)
-                if (a >= 0) {
-                    edges.emplace_back(a, b);
-                    init_count[(size_t)b]++;
-                }
+            level[(size_t)b] = lv;
             for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++)
                 for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) own[(size_t)uy * uw[c] + ux] = b;
         }
-        for (auto& e : edges) dep_off[(size_t)e.first + 1]++;
-        for (int b = 0; b < n_intra; b++) dep_off[(size_t)b + 1] += dep_off[(size_t)b];
-        dep_list.resize(edges.size());
-        std::vector<int32_t> fill(dep_off.begin(), dep_off.end() - 1);
-        for (auto& e : edges) dep_list[(size_t)fill[(size_t)e.first]++] = e.second;
-        for (int b = 0; b < n_intra; b++)
-            if (init_count[(size_t)b] == 0) ready.push_back(b);
+        // order by (CTU raster address, level, decode order)
+        std::vector<int32_t> order((size_t)n_intra);
+        for (int b = 0; b < n_intra; b++) order[(size_t)b] = b;
+        std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+            if (ctu_of[(size_t)x] != ctu_of[(size_t)y]) return ctu_of[(size_t)x] < ctu_of[(size_t)y];
+            return level[(size_t)x] < level[(size_t)y];
+        });
+        itu.resize((size_t)n_intra);
+        itu_level_end.resize((size_t)n_intra);
+        for (int i = 0; i < n_intra; i++) {
+            const int b = order[(size_t)i];
+            itu[(size_t)i] = intra_list[(size_t)b];
+            if (i == 0 || ctu_of[(size_t)b] != ctu_of[(size_t)order[(size_t)i - 1]]) {
+                ictu_addr.push_back(ctu_of[(size_t)b]);
+                ictu_tu_off.push_back(i);
+            }
+        }
+        ictu_tu_off.push_back(n_intra);
+        for (int i = n_intra - 1; i >= 0; i--) {
+            const int b = order[(size_t)i];
+            const bool last = i == n_intra - 1 || ctu_of[(size_t)order[(size_t)i + 1]] != ctu_of[(size_t)b] ||
+                              level[(size_t)order[(size_t)i + 1]] != level[(size_t)b];
+            itu_level_end[(size_t)i] = last ? i + 1 : itu_level_end[(size_t)i + 1];
+        }
+        // residual offsets inside each CTU's staged residuals (coded TUs, in itu order)
+        itu_res_off.assign((size_t)n_intra, -1);
+        const int nic = (int)ictu_addr.size();
+        for (int k = 0; k < nic; k++) {
+            int acc = 0;
+            for (int i = ictu_tu_off[(size_t)k]; i < ictu_tu_off[(size_t)k + 1]; i++) {
+                const hevc_tu_t& t = s->tus[itu[(size_t)i]];
+                if (!(t.flags & HEVC_TU_CODED)) continue;
+                itu_res_off[(size_t)i] = acc;
+                acc += 1 << (2 * t.log2_size);
+            }
+            if (acc > IC_MAX_RES || ictu_tu_off[(size_t)k + 1] - ictu_tu_off[(size_t)k] > IC_MAX_TUS)
+                return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", ictu_addr[(size_t)k]);
+        }
+        // dependencies by intra-CTU index (earlier CTUs in raster order: at most left,
+        // above-left, above and above-right)
+        std::vector<int32_t> index_of((size_t)nctb, -1);
+        for (int k = 0; k < nic; k++) index_of[(size_t)ictu_addr[(size_t)k]] = k;
+        ictu_deps.assign((size_t)nic * 4, -1);
+        for (int k = 0; k < nic; k++) {
+            const std::vector<int32_t>& dl = ctu_deps[(size_t)ictu_addr[(size_t)k]];
+            if (dl.size() > 4) return fail(HEVCGPU_EINVAL, "CTU %d depends on %zu CTUs", ictu_addr[(size_t)k], dl.size());
+            for (size_t q = 0; q < dl.size(); q++) ictu_deps[(size_t)k * 4 + q] = index_of[(size_t)dl[q]];
+        }
     }
-    j->n_intra = n_intra;
-    j->n_ready = (int32_t)ready.size();
+    j->n_ictu = (int32_t)ictu_addr.size();
     // MC tiles
     std::vector<McItem> mc;
     if (stages & ST_MC)
@@ -453,8 +485,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         }
     j->n_pus = s->num_pus;
 
-    size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc, o_il, o_do, o_dl, o_ic,
-        o_rd;
+    size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc, o_ia, o_idp, o_ito,
+        o_itu, o_ile, o_iro;
     hevc_slice_t dflt{0, 0, 0, 1};
     auto pack = [&](Packer& pk) {
         o_tus = pk.add(s->tus, sizeof(hevc_tu_t) * (size_t)std::max(0, s->num_tus));
@@ -469,11 +501,12 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
                                                   : pk.add(&dflt, sizeof(dflt));
         for (int k = 0; k < 4; k++) o_res[k] = pk.add(bins[k].data(), sizeof(int32_t) * bins[k].size());
         o_mc = pk.add(mc.data(), sizeof(McItem) * mc.size());
-        o_il = pk.add(intra_list.data(), sizeof(int32_t) * intra_list.size());
-        o_do = pk.add(dep_off.data(), sizeof(int32_t) * dep_off.size());
-        o_dl = pk.add(dep_list.data(), sizeof(int32_t) * dep_list.size());
-        o_ic = pk.add(init_count.data(), sizeof(int32_t) * init_count.size());
-        o_rd = pk.add(ready.data(), sizeof(int32_t) * ready.size());
+        o_ia = pk.add(ictu_addr.data(), sizeof(int32_t) * ictu_addr.size());
+        o_idp = pk.add(ictu_deps.data(), sizeof(int32_t) * ictu_deps.size());
+        o_ito = pk.add(ictu_tu_off.data(), sizeof(int32_t) * ictu_tu_off.size());
+        o_itu = pk.add(itu.data(), sizeof(int32_t) * itu.size());
+        o_ile = pk.add(itu_level_end.data(), sizeof(int32_t) * itu_level_end.size());
+        o_iro = pk.add(itu_res_off.data(), sizeof(int32_t) * itu_res_off.size());
     };
     Packer measure;
     pack(measure);
@@ -491,8 +524,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
 
     size_t resid_bytes = j->has_intra ? sizeof(int16_t) * (size_t)align_up((int64_t)s->num_coeffs, 128) : 0;
     size_t mot_bytes = (stages & ST_DEBLOCK) ? sizeof(MotionEnt) * (size_t)align_up((int64_t)gw * gh, 32) : 0;
-    size_t count_bytes = sizeof(int32_t) * (size_t)n_intra;
-    rc = j->scratch.get(ctx, std::max<size_t>(resid_bytes + mot_bytes + count_bytes, 256));
+    size_t done_bytes = sizeof(int32_t) * ictu_addr.size();
+    rc = j->scratch.get(ctx, std::max<size_t>(resid_bytes + mot_bytes + done_bytes, 256));
     if (rc) return rc;
     rc = j->desc.get(ctx, sizeof(PicDesc));
     if (rc) return rc;
@@ -520,14 +553,16 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     D.ctb_slice = s->ctb_slice ? base + o_sl : nullptr;
     D.ctb_tile = (s->ctb_tile && p.tiles_enabled) ? reinterpret_cast<const uint16_t*>(base + o_ti) : nullptr;
     D.slices = reinterpret_cast<const hevc_slice_t*>(base + o_slices);
-    D.intra_list = reinterpret_cast<const int32_t*>(base + o_il);
-    D.dep_off = reinterpret_cast<const int32_t*>(base + o_do);
-    D.dep_list = reinterpret_cast<const int32_t*>(base + o_dl);
-    D.init_count = reinterpret_cast<const int32_t*>(base + o_ic);
-    D.ready = reinterpret_cast<const int32_t*>(base + o_rd);
-    D.count = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(j->scratch.p) + resid_bytes + mot_bytes);
-    D.n_intra = n_intra;
-    D.n_ready = (int32_t)ready.size();
+    D.ictu_addr = reinterpret_cast<const int32_t*>(base + o_ia);
+    D.ictu_deps = reinterpret_cast<const int32_t*>(base + o_idp);
+    D.ictu_tu_off = reinterpret_cast<const int32_t*>(base + o_ito);
+    D.itu = reinterpret_cast<const int32_t*>(base + o_itu);
+    D.itu_level_end = reinterpret_cast<const int32_t*>(base + o_ile);
+    D.itu_res_off = reinterpret_cast<const int32_t*>(base + o_iro);
+    D.ictu_done = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(j->scratch.p) + resid_bytes + mot_bytes);
+    D.n_ictu = (int32_t)ictu_addr.size();
+    // completion flags start below every epoch a launch can use
+    if (done_bytes) CUDA_TRY(cudaMemsetAsync(D.ictu_done, 0, done_bytes, ctx->stream));
     D.num_pus = s->num_pus;
     D.num_slices = std::max(1, (int)s->num_slices);
     D.log2_ctb = p.log2_ctb;
@@ -691,32 +726,27 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
     }
     if (stages & ST_INTRA) {
         StageMark m(ctx, 3);
-        // one arm + one persistent dataflow launch per group of up to MAX_SEGS pictures
+        // one launch per group of up to MAX_SEGS pictures: CTAs take intra CTUs by ticket
+        // in (picture, raster) order; aux0 = intra CTUs of earlier pictures, aux1 = epoch
         int k = 0;
         while (k < n) {
             SegTable t;
             std::memset(&t, 0, sizeof(t));
-            int total = 0, n_ready = 0, max_intra = 0;
+            int total = 0;
             for (; k < n && t.n < MAX_SEGS; k++) {
                 hevcgpu_job* j = jobs[k];
-                if (j->n_intra == 0) continue;
+                if (j->n_ictu == 0) continue;
                 Seg& sg = t.s[t.n++];
                 sg.pic = static_cast<const PicDesc*>(j->desc.p);
-                sg.aux0 = n_ready;
-                sg.aux1 = total;
-                total += j->n_intra;
-                n_ready += j->n_ready;
-                max_intra = std::max(max_intra, j->n_intra);
+                sg.aux0 = total;
+                sg.aux1 = ++j->epoch;
+                total += j->n_ictu;
             }
             if (t.n == 0) continue;
-            if ((rc = ctx->ensure_queue(sizeof(int32_t) * (size_t)total))) return rc;
             FlowState* fs = static_cast<FlowState*>(ctx->flow);
             uint32_t* sticky = reinterpret_cast<uint32_t*>(fs + 1);
-            int32_t* queue = static_cast<int32_t*>(ctx->queue);
-            rc = L.go(k_intra_arm, dim3((max_intra + 255) / 256, t.n), dim3(256), t, fs, queue, n_ready);
-            if (rc) return rc;
-            int ctas = std::min((total + IF_WARPS - 1) / IF_WARPS, ctx->sm_count * 4);
-            rc = L.go(k_intra_flow, dim3(ctas), dim3(32 * IF_WARPS), t, fs, queue, total, sticky);
+            CUDA_TRY(cudaMemsetAsync(&fs->head, 0, sizeof(int32_t), ctx->stream));
+            rc = L.go(k_intra_ctus, dim3(total), dim3(IC_THREADS), t, &fs->head, total, sticky);
             if (rc) return rc;
         }
     }
@@ -1111,9 +1141,15 @@ int hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot) {
 
 int hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, int32_t n) {
     if (!jobs || !dst_slots || n <= 0) return fail(HEVCGPU_EINVAL, "empty batch");
+    if (!jobs[0]) return fail(HEVCGPU_EINVAL, "null job");
     hevcgpu_ctx* ctx = jobs[0]->ctx;
     for (int k = 0; k < n; k++) {
         if (!jobs[k] || jobs[k]->ctx != ctx) return fail(HEVCGPU_EINVAL, "batch mixes contexts");
+        for (int q = 0; q < k; q++) {
+            if (jobs[q] == jobs[k]) return fail(HEVCGPU_EINVAL, "job %d appears twice in the batch", k);
+            if (jobs[q]->st == jobs[k]->st && dst_slots[q] == dst_slots[k])
+                return fail(HEVCGPU_EINVAL, "two pictures of the batch write slot %d of one stream", dst_slots[k]);
+        }
         int rc = job_target(jobs[k], dst_slots[k]);
         if (rc) return rc;
     }

@@ -40,22 +40,32 @@ struct IntraWarpSmem {
     int16_t f[129];    // after smoothing
 };
 
+// Shared-memory copy of one plane around the CTU being reconstructed: sample (x, y) of
+// the plane is at t[(y - y0) * pitch + (x - x0)].
+struct CtuTile {
+    uint8_t* t;
+    int pitch, x0, y0;
+};
+
+// Neighbour CTBs an intra TU may read from, as bits of a mask: they must precede the
+// current CTB in raster order and share its slice and tile (intra_prediction.cpp:108-124).
+enum : uint32_t { NB_LEFT = 1u, NB_ABOVE_LEFT = 2u, NB_ABOVE = 4u, NB_ABOVE_RIGHT = 8u };
+
 // Predict + reconstruct one intra TU with one warp (perform_intra_prediction,
 // intra_prediction.cpp:428-481, then reconstruct_block's add and clip).  Reference
-// samples are read through L2 (ld.global.cg): other warps of this launch wrote them.
-__device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W) {
+// samples come from the CTU tile; results go to the tile (for later TUs) and the picture.
+// res is the TU's residual (null when it has none).
+__device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W, const CtuTile& tile,
+                         uint32_t nb_mask, const int16_t* res) {
     const int ci = t.c_idx, sub = ci ? 2 : 1;
     const int n = 1 << t.log2_size, log2 = t.log2_size;
     const int xc = t.x, yc = t.y;
     const int ctb = 1 << P.log2_ctb, ctbc = ctb / sub;
     const int rx = xc / ctbc, ry = yc / ctbc;
-    const int cur_addr = ry * P.wctb + rx;
     const int pw = P.width / sub, ph = P.height / sub;
     const int ox = rx * ctb, oy = ry * ctb;
     const int pitch = ci ? P.pitch_c : P.pitch_y;
     uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));
-    const int cur_slice = P.ctb_slice ? P.ctb_slice[cur_addr] : 0;
-    const int cur_tile = P.ctb_tile ? P.ctb_tile[cur_addr] : 0;
     const uint32_t cur_z = zorder16((uint32_t)((xc * sub - ox) >> 2), (uint32_t)((yc * sub - oy) >> 2));
     const int total = 4 * n + 1;
 
@@ -76,13 +86,17 @@ __device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWa
             if (px >= 0 && py >= 0 && px < pw && py < ph) {
                 const int ncx = px / ctbc, ncy = py / ctbc;
                 if (ncx != rx || ncy != ry) {
-                    const int a = ncy * P.wctb + ncx;
-                    ok = a < cur_addr && (P.ctb_slice ? P.ctb_slice[a] : 0) == cur_slice &&
-                         (P.ctb_tile ? P.ctb_tile[a] : 0) == cur_tile;
+                    // reference positions reach one CTB left, one CTB right (top row) and
+                    // one CTB row up or down; later CTBs are never available
+                    uint32_t bit = 0u;
+                    if (ncy == ry) bit = ncx == rx - 1 ? NB_LEFT : 0u;
+                    else if (ncy == ry - 1)
+                        bit = ncx == rx - 1 ? NB_ABOVE_LEFT : (ncx == rx ? NB_ABOVE : (ncx == rx + 1 ? NB_ABOVE_RIGHT : 0u));
+                    ok = (nb_mask & bit) != 0;
                 } else {
                     ok = zorder16((uint32_t)((px * sub - ox) >> 2), (uint32_t)((py * sub - oy) >> 2)) < cur_z;
                 }
-                if (ok) val = __ldcg(plane + (int64_t)py * pitch + px);
+                if (ok) val = tile.t[(py - tile.y0) * tile.pitch + (px - tile.x0)];
             }
             W.raw[i] = (int16_t)val;
         }
@@ -146,7 +160,6 @@ __device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWa
         }
     }
     // 4. prediction (top[k] = R[2n + k], left[k] = R[2n - k]) + residual, clip, store
-    const int16_t* res = (t.flags & HEVC_TU_CODED) ? P.resid + t.coeff_offset : nullptr;
     const int ang = c_intra_angle[mode];
     const int inv = c_inv_angle[mode];
     int dc = 0;
@@ -187,80 +200,147 @@ __device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWa
                 else if (mode == 10 && y == 0) p = clip_u8(p + ((R[2 * n + 1 + x] - R[2 * n]) >> 1));
             }
         }
-        plane[(int64_t)(yc + y) * pitch + xc + x] = (uint8_t)clip_u8(p + (res ? res[e] : 0));
+        const uint8_t v = (uint8_t)clip_u8(p + (res ? res[e] : 0));
+        tile.t[(yc + y - tile.y0) * tile.pitch + (xc + x - tile.x0)] = v;
+        plane[(int64_t)(yc + y) * pitch + xc + x] = v;
     }
 }
 
-constexpr int IF_WARPS = 8;
-constexpr long long SPIN_LIMIT = 1ll << 23;  // polls of ~128 ns: about a second
+// ---------------------------------------------------------------------------------------
+// CTU tasks.  One CTA per CTU that holds intra TUs.  CTAs take CTUs by ticket in raster
+// order, picture after picture; a CTU waits (bounded) for the at most four earlier intra
+// CTUs whose intra samples it reads (left, above-left, above, above-right, found on the
+// host), so every wait is for a CTA that already runs.  The CTA then stages the CTU and
+// its neighbourhood, its TU records and their residuals in shared memory, runs the TUs
+// level by level of the CTU-local dependency DAG (one warp per TU, a barrier between
+// levels) and publishes its completion with the launch's epoch.
+// ---------------------------------------------------------------------------------------
+constexpr int IC_WARPS = 4;
+constexpr int IC_THREADS = 32 * IC_WARPS;
+constexpr int IC_MARGIN = 16;                        // bytes left of the CTU (column -1 last)
+constexpr int IC_LP = IC_MARGIN + 128, IC_LH = 65;   // luma tile pitch, rows -1 .. 63
+constexpr int IC_CP = IC_MARGIN + 64, IC_CH = 33;    // chroma tile
+constexpr int IC_MAX_TUS = 256 + 2 * 64;             // 4x4 TUs of a 64x64 CTU, all planes
+constexpr int IC_MAX_RES = 64 * 64 + 2 * 32 * 32;    // residual samples of a 64x64 CTU
+constexpr long long SPIN_LIMIT = 1ll << 24;          // polls of ~64 ns: about a second
 
-__device__ __forceinline__ int32_t encode_item(int seg, int idx) { return (seg << 24) | idx; }
-
-// Re-arm the counters of every picture and seed the queue: picture k's ready TUs go to
-// slots [aux0, aux0 + n_ready), its other slots [n_ready_total + aux1 - aux0, ...) are
-// cleared to -1 (aux0 = ready TUs of earlier pictures, aux1 = intra TUs of earlier ones).
-__global__ void k_intra_arm(const __grid_constant__ SegTable st, FlowState* fs, int32_t* queue, int n_ready_total) {
-    const Seg& sg = st.s[blockIdx.y];
-    const PicDesc& P = *sg.pic;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
-        fs->head = 0;
-        fs->tail = n_ready_total;
-        fs->status = 0;
+// Copy plane c around CTU (rx, ry) into its tile with 16-byte L2 loads: row -1 from
+// column -16 to 2*ctbc-1, rows 0..ctbc-1 from column -16 to ctbc-1.
+__device__ __forceinline__ void stage_tile(const PicDesc& P, int c, int rx, int ry, uint8_t* tile, int tid) {
+    const int sub = c ? 2 : 1, ctbc = (1 << P.log2_ctb) / sub;
+    const int pw = P.width / sub, ph = P.height / sub, pitch = c ? P.pitch_c : P.pitch_y;
+    const uint8_t* plane = P.rec + (c == 0 ? 0 : (c == 1 ? P.off_cb : P.off_cr));
+    const int tp = c ? IC_CP : IC_LP;
+    const int x0 = rx * ctbc - IC_MARGIN, y0 = ry * ctbc - 1;
+    const int top_chunks = (IC_MARGIN + 2 * ctbc + 15) / 16, row_chunks = (IC_MARGIN + ctbc + 15) / 16;
+    const int n = top_chunks + ctbc * row_chunks;
+    for (int e = tid; e < n; e += IC_THREADS) {
+        int r, q;
+        if (e < top_chunks) { r = 0; q = e; }
+        else { r = 1 + (e - top_chunks) / row_chunks; q = (e - top_chunks) % row_chunks; }
+        const int y = y0 + r, x = x0 + 16 * q;
+        if (y < 0 || y >= ph || x < 0 || x >= pw) continue;
+        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(plane + (int64_t)y * pitch + x));
+        *reinterpret_cast<uint4*>(tile + r * tp + 16 * q) = v;
     }
-    if (i >= P.n_intra) return;
-    P.count[i] = P.init_count[i];
-    if (i < P.n_ready) queue[sg.aux0 + i] = encode_item(blockIdx.y, P.ready[i]);
-    else queue[n_ready_total + sg.aux1 - sg.aux0 + (i - P.n_ready)] = -1;
 }
 
-__global__ void __launch_bounds__(32 * IF_WARPS) k_intra_flow(const __grid_constant__ SegTable st, FlowState* fs,
-                                                              int32_t* queue, int total, uint32_t* sticky) {
-    __shared__ IntraWarpSmem ws[IF_WARPS];
-    const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
-    IntraWarpSmem& W = ws[warp];
-    cuda::atomic_ref<int32_t, cuda::thread_scope_device> head(fs->head), tail(fs->tail);
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> status(fs->status);
-    while (true) {
-        int slot = 0, item = -1;
-        if (lane == 0) {
-            slot = head.fetch_add(1, cuda::memory_order_relaxed);
-            if (slot < total) {
-                cuda::atomic_ref<int32_t, cuda::thread_scope_device> q(queue[slot]);
-                long long polls = 0;
-                while ((item = q.load(cuda::memory_order_acquire)) < 0) {
-                    if (status.load(cuda::memory_order_relaxed) != 0u || ++polls > SPIN_LIMIT) {
-                        status.fetch_or(ST_TIMEOUT, cuda::memory_order_relaxed);
-                        atomicOr(sticky, ST_TIMEOUT);
-                        item = -1;
-                        break;
-                    }
-                    __nanosleep(128);
+__global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant__ SegTable st, int32_t* ticket,
+                                                           int total, uint32_t* sticky) {
+    __shared__ __align__(16) uint8_t t_luma[IC_LH * IC_LP];
+    __shared__ __align__(16) uint8_t t_chroma[2][IC_CH * IC_CP];
+    __shared__ __align__(16) hevc_tu_t s_tu[IC_MAX_TUS];
+    __shared__ __align__(16) int16_t s_res[IC_MAX_RES];
+    __shared__ IntraWarpSmem ws[IC_WARPS];
+    __shared__ int s_ticket, s_abort;
+    __shared__ uint32_t s_nb;
+    const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
+    if (tid == 0) {
+        s_ticket = atomicAdd(ticket, 1);
+        s_abort = 0;
+    }
+    __syncthreads();
+    const int t = s_ticket;
+    if (t >= total) return;
+    int k = 0;
+    while (k + 1 < st.n && st.s[k + 1].aux0 <= t) k++;
+    const PicDesc& P = *st.s[k].pic;
+    const int epoch = st.s[k].aux1;
+    const int idx = t - st.s[k].aux0;
+    const int a = P.ictu_addr[idx], rx = a % P.wctb, ry = a / P.wctb;
+
+    // wait for the intra CTUs this one reads from (one thread per dependency)
+    if (tid < 4) {
+        const int d = P.ictu_deps[4 * idx + tid];
+        if (d >= 0) {
+            cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[d]);
+            long long polls = 0;
+            while (done.load(cuda::memory_order_acquire) != epoch) {
+                if (++polls > SPIN_LIMIT) {
+                    atomicOr(sticky, ST_TIMEOUT);
+                    s_abort = 1;
+                    break;
                 }
+                __nanosleep(32);
             }
         }
-        slot = __shfl_sync(0xffffffffu, slot, 0);
-        item = __shfl_sync(0xffffffffu, item, 0);
-        if (slot >= total || item < 0) return;
-        const int seg = item >> 24, idx = item & 0xFFFFFF;
-        const PicDesc& P = *st.s[seg].pic;
-        const hevc_tu_t t = P.tus[P.intra_list[idx]];
-        intra_tu(P, t, lane, W);
-        // make this TU's samples visible before its dependents can be claimed
-        __threadfence();
-        __syncwarp();
-        if (lane == 0) {
-            for (int k = P.dep_off[idx]; k < P.dep_off[idx + 1]; k++) {
-                const int d = P.dep_list[k];
-                cuda::atomic_ref<int32_t, cuda::thread_scope_device> cnt(P.count[d]);
-                if (cnt.fetch_sub(1, cuda::memory_order_acq_rel) == 1) {
-                    const int s2 = tail.fetch_add(1, cuda::memory_order_relaxed);
-                    cuda::atomic_ref<int32_t, cuda::thread_scope_device> q(queue[s2]);
-                    q.store(encode_item(seg, d), cuda::memory_order_release);
-                }
-            }
+    }
+    if (tid == 4) {  // which neighbour CTBs share this CTB's slice and tile
+        const int sl = P.ctb_slice ? P.ctb_slice[a] : 0, ti = P.ctb_tile ? P.ctb_tile[a] : 0;
+        auto same = [&](int nx, int ny) {
+            if (nx < 0 || ny < 0 || nx >= P.wctb) return false;
+            const int b = ny * P.wctb + nx;
+            return (P.ctb_slice ? P.ctb_slice[b] : 0) == sl && (P.ctb_tile ? P.ctb_tile[b] : 0) == ti;
+        };
+        s_nb = (same(rx - 1, ry) ? NB_LEFT : 0u) | (same(rx - 1, ry - 1) ? NB_ABOVE_LEFT : 0u) |
+               (same(rx, ry - 1) ? NB_ABOVE : 0u) | (same(rx + 1, ry - 1) ? NB_ABOVE_RIGHT : 0u);
+    }
+    __syncthreads();
+    if (s_abort) return;
+
+    // stage the neighbourhood and the TU records
+    const int off = P.ictu_tu_off[idx], n_tu = P.ictu_tu_off[idx + 1] - off;
+    for (int i = tid; i < n_tu; i += IC_THREADS) s_tu[i] = P.tus[P.itu[off + i]];
+    stage_tile(P, 0, rx, ry, t_luma, tid);
+    stage_tile(P, 1, rx, ry, t_chroma[0], tid);
+    stage_tile(P, 2, rx, ry, t_chroma[1], tid);
+    __syncthreads();
+    // residuals of the coded TUs, packed in TU order (one warp per TU, 16-byte chunks)
+    for (int i = warp; i < n_tu; i += IC_WARPS) {
+        const hevc_tu_t& tu = s_tu[i];
+        if (!(tu.flags & HEVC_TU_CODED)) continue;
+        const int chunks = (1 << (2 * tu.log2_size)) / 8;
+        const uint4* src = reinterpret_cast<const uint4*>(P.resid + tu.coeff_offset);
+        uint4* dst = reinterpret_cast<uint4*>(s_res + P.itu_res_off[off + i]);
+        for (int c = lane; c < chunks; c += 32) dst[c] = __ldcg(src + c);
+    }
+    __syncthreads();
+
+    const int ctbl = 1 << P.log2_ctb;
+    const uint32_t nb = s_nb;
+    int pos = 0;
+    while (pos < n_tu) {
+        const int lvl_end = P.itu_level_end[off + pos] - off;
+        for (int i = pos + warp; i < lvl_end; i += IC_WARPS) {
+            const hevc_tu_t& tu = s_tu[i];
+            const int ctbc = tu.c_idx ? ctbl / 2 : ctbl;
+            CtuTile tile;
+            tile.t = tu.c_idx == 0 ? t_luma : t_chroma[tu.c_idx - 1];
+            tile.pitch = tu.c_idx ? IC_CP : IC_LP;
+            tile.x0 = rx * ctbc - IC_MARGIN;
+            tile.y0 = ry * ctbc - 1;
+            const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + P.itu_res_off[off + i] : nullptr;
+            intra_tu(P, tu, lane, ws[warp], tile, nb, res);
         }
-        __syncwarp();
+        __syncthreads();
+        pos = lvl_end;
+    }
+    // publish: every thread's picture writes are visible before the flag moves
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[idx]);
+        done.store(epoch, cuda::memory_order_release);
     }
 }
 
