@@ -64,12 +64,7 @@ struct PicDesc {
 };
 
 // Work items ----------------------------------------------------------------------------
-// Residual items are TU indices (int32), intra items CTU raster addresses (int32).
-struct McItem {       // one luma tile (<= 16x16) of one PU, plus its chroma tiles
-    int32_t pu;
-    uint8_t dx, dy;   // offset of the tile in the PU (luma samples)
-    uint8_t w, h;     // tile size (luma samples, multiples of 4)
-};
+// Residual items are TU indices (int32); motion-compensation items are McStrip (mc.cuh).
 
 // A launch covers up to MAX_SEGS pictures.  Segment k owns the blocks
 // [block0, next block0) of an item-list launch, or blockIdx.y == k of a per-picture

@@ -16,6 +16,7 @@
 
 #include "hevcgpu.h"
 #include "intra.cuh"
+#include "mc.cuh"
 #include "kernels.cuh"
 
 using namespace hevcgpu;
@@ -243,7 +244,7 @@ struct hevcgpu_job {
     int32_t n_res[4] = {0, 0, 0, 0};
     const int32_t* d_res[4] = {nullptr, nullptr, nullptr, nullptr};
     int32_t n_mc = 0;
-    const McItem* d_mc = nullptr;
+    const McStrip* d_mc = nullptr;
     int32_t n_ictu = 0;                 // CTUs that hold intra TUs
     int32_t epoch = 0;                  // intra launches of this job so far
     int32_t n_pus = 0;
@@ -467,22 +468,29 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         }
     }
     j->n_ictu = (int32_t)ictu_addr.size();
-    // MC tiles
-    std::vector<McItem> mc;
-    if (stages & ST_MC)
-        for (int i = 0; i < s->num_pus; i++) {
-            const hevc_pu_t& u = s->pus[i];
-            for (int dy = 0; dy < u.h; dy += 16)
-                for (int dx = 0; dx < u.w; dx += 16) {
-                    McItem m;
-                    m.pu = i;
-                    m.dx = (uint8_t)dx;
-                    m.dy = (uint8_t)dy;
-                    m.w = (uint8_t)std::min(16, u.w - dx);
-                    m.h = (uint8_t)std::min(16, u.h - dy);
-                    mc.push_back(m);
-                }
-        }
+    // MC strips: 4 columns x up to 16 rows, luma then chroma (Cb and Cr together), and
+    // bi- before uni-predicted PUs, so that the threads of a warp follow the same path
+    std::vector<McStrip> mc;
+    if (stages & ST_MC) {
+        for (int c = 0; c < 2; c++)
+            for (int pass = 0; pass < 2; pass++)
+            for (int i = 0; i < s->num_pus; i++) {
+                const hevc_pu_t& u = s->pus[i];
+                const bool bi = u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0;
+                if (bi != (pass == 0)) continue;
+                const int w = c ? u.w / 2 : u.w, h = c ? u.h / 2 : u.h;
+                for (int sy = 0; sy < h; sy += 16)
+                    for (int sx = 0; sx < w; sx += 4) {
+                        McStrip m;
+                        m.pu = i;
+                        m.sx = (uint8_t)sx;
+                        m.sy = (uint8_t)sy;
+                        m.h = (uint8_t)std::min(16, h - sy);
+                        m.chroma = (uint8_t)c;
+                        mc.push_back(m);
+                    }
+            }
+    }
     j->n_pus = s->num_pus;
 
     size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc, o_ia, o_idp, o_ito,
@@ -500,7 +508,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         o_slices = s->num_slices > 0 && s->slices ? pk.add(s->slices, sizeof(hevc_slice_t) * (size_t)s->num_slices)
                                                   : pk.add(&dflt, sizeof(dflt));
         for (int k = 0; k < 4; k++) o_res[k] = pk.add(bins[k].data(), sizeof(int32_t) * bins[k].size());
-        o_mc = pk.add(mc.data(), sizeof(McItem) * mc.size());
+        o_mc = pk.add(mc.data(), sizeof(McStrip) * mc.size());
         o_ia = pk.add(ictu_addr.data(), sizeof(int32_t) * ictu_addr.size());
         o_idp = pk.add(ictu_deps.data(), sizeof(int32_t) * ictu_deps.size());
         o_ito = pk.add(ictu_tu_off.data(), sizeof(int32_t) * ictu_tu_off.size());
@@ -589,7 +597,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         j->d_res[k] = reinterpret_cast<const int32_t*>(base + o_res[k]);
     }
     j->n_mc = (int32_t)mc.size();
-    j->d_mc = reinterpret_cast<const McItem*>(base + o_mc);
+    j->d_mc = reinterpret_cast<const McStrip*>(base + o_mc);
     return HEVCGPU_OK;
 }
 
@@ -705,7 +713,7 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
     }
     if (stages & ST_MC) {
         StageMark m(ctx, 1);
-        rc = L.items(k_mc, jobs, n, MC_WARPS, 32 * MC_WARPS, [](hevcgpu_job* j, const void*& p, int& c) {
+        rc = L.items(k_mc, jobs, n, MC_THREADS, MC_THREADS, [](hevcgpu_job* j, const void*& p, int& c) {
             p = j->d_mc;
             c = j->n_mc;
         });

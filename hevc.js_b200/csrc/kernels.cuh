@@ -2,9 +2,7 @@
 //
 //   k_residual<LOG2>  dequant + inverse DST/DCT + add-and-clip of coded TUs
 //                     (transform.cpp:293-394, coding_tree.cpp:371-396)
-//   k_mc              8-tap/4-tap interpolation + default/explicit weighting
-//                     (interpolation.cpp:45-411)
-//   (intra prediction: intra.cuh)
+//   (motion compensation: mc.cuh; intra prediction: intra.cuh)
 //   k_motion_grid     4x4 motion grid of the PUs (store_pu_motion's grid)
 //   k_deblock<V>      Bs + decisions + luma/chroma filters of one edge direction
 //                     (deblocking.cpp:50-614)
@@ -208,209 +206,6 @@ __global__ void __launch_bounds__(128) k_residual(const __grid_constant__ SegTab
 #pragma unroll
         for (int i = 0; i < 4; i++) ov |= (uint32_t)clip_u8((int)((pv >> (8 * i)) & 0xFF) + r[i]) << (8 * i);
         *reinterpret_cast<uint32_t*>(out) = ov;
-    }
-}
-
-// ======================================================================================
-// Motion compensation.  One warp per McItem: a luma tile of at most 16x16 of one PU and
-// its two 4:2:0 chroma tiles.  Per list the (w+7)x(h+7) luma and (w/2+3)x(h/2+3) chroma
-// reference windows are staged in shared memory with edge-clamped coordinates (the
-// reference's refClamp), filtered horizontally into an int16 intermediate and then
-// vertically; the final weighting writes 8-bit samples into the reconstruction buffer.
-// ======================================================================================
-__constant__ int8_t c_luma_taps[4][8] = {{0, 0, 0, 64, 0, 0, 0, 0},
-                                         {-1, 4, -10, 58, 17, -5, 1, 0},
-                                         {-1, 4, -11, 40, 40, -11, 4, -1},
-                                         {0, 1, -5, 17, 58, -10, 4, -1}};
-__constant__ int8_t c_chroma_taps[8][4] = {{0, 64, 0, 0},    {-2, 58, 10, -2}, {-4, 54, 16, -2},
-                                           {-6, 46, 28, -4}, {-4, 36, 36, -4}, {-4, 28, 46, -6},
-                                           {-2, 16, 54, -4}, {-2, 10, 58, -2}};
-
-constexpr int MC_WARPS = 8;
-constexpr int MC_WIN = 24 * 23;   // luma window, pitch 24
-constexpr int MC_TMP = 23 * 16;   // luma intermediate
-
-struct McSmem {
-    uint8_t win[MC_WIN];
-    int16_t tmp[MC_TMP];
-    uint8_t cwin[2][12 * 11];
-    int16_t ctmp[11 * 8];
-};
-
-// One component, one list: NT-tap prediction of a bw x bh block at (xi, yi) integer
-// position with fractions (fx, fy) into per-lane registers pred[k] for the elements
-// e = lane + 32k (row-major in the block).
-template <int NT, int MAXE>
-__device__ __forceinline__ void mc_block(const uint8_t* __restrict__ plane, int pitch, int pw, int ph, int xi,
-                                         int yi, int fx, int fy, int bw, int bh, uint8_t* win, int wpitch,
-                                         int16_t* tmp, int lane, int (&pred)[MAXE]) {
-    constexpr int HALF = NT / 2 - 1;
-    constexpr int WMAX = NT == 8 ? 23 * 23 : 11 * 11;  // largest window (16x16 / 8x8 block)
-    constexpr int ITER = (WMAX + 31) / 32;
-    const int ww = bw + NT - 1, wh = bh + NT - 1;
-    const int x0 = xi - HALF, y0 = yi - HALF;
-    const bool interior = x0 >= 0 && y0 >= 0 && x0 + ww <= pw && y0 + wh <= ph;
-    // all loads of this lane first (they are in flight together), then the stores
-    uint8_t v[ITER];
-    {
-        int r = lane / ww, c = lane - r * ww;
-#pragma unroll
-        for (int k = 0; k < ITER; k++) {
-            if (lane + 32 * k < ww * wh) {
-                int yy = y0 + r, xx = x0 + c;
-                if (!interior) {
-                    yy = clip3(0, ph - 1, yy);
-                    xx = clip3(0, pw - 1, xx);
-                }
-                v[k] = __ldg(plane + (int64_t)yy * pitch + xx);
-            }
-            c += 32;
-            while (c >= ww) { c -= ww; r++; }
-        }
-    }
-    {
-        int r = lane / ww, c = lane - r * ww;
-#pragma unroll
-        for (int k = 0; k < ITER; k++) {
-            if (lane + 32 * k < ww * wh) win[r * wpitch + c] = v[k];
-            c += 32;
-            while (c >= ww) { c -= ww; r++; }
-        }
-    }
-    __syncwarp();
-    const int8_t* th = NT == 8 ? c_luma_taps[fx] : c_chroma_taps[fx];
-    const int8_t* tv = NT == 8 ? c_luma_taps[fy] : c_chroma_taps[fy];
-    if (fx == 0 && fy == 0) {
-#pragma unroll
-        for (int k = 0; k < MAXE; k++) {
-            int e = lane + 32 * k;
-            if (e < bw * bh) {
-                int r = e / bw, c = e - r * bw;
-                pred[k] = (int16_t)(win[(r + HALF) * wpitch + c + HALF] << 6);
-            }
-        }
-    } else if (fy == 0) {
-#pragma unroll
-        for (int k = 0; k < MAXE; k++) {
-            int e = lane + 32 * k;
-            if (e < bw * bh) {
-                int r = e / bw, c = e - r * bw;
-                const uint8_t* w = win + (r + HALF) * wpitch + c;
-                int s = 0;
-#pragma unroll
-                for (int q = 0; q < NT; q++) s += th[q] * w[q];
-                pred[k] = (int16_t)s;
-            }
-        }
-    } else if (fx == 0) {
-#pragma unroll
-        for (int k = 0; k < MAXE; k++) {
-            int e = lane + 32 * k;
-            if (e < bw * bh) {
-                int r = e / bw, c = e - r * bw;
-                const uint8_t* w = win + r * wpitch + c + HALF;
-                int s = 0;
-#pragma unroll
-                for (int q = 0; q < NT; q++) s += tv[q] * w[q * wpitch];
-                pred[k] = (int16_t)s;
-            }
-        }
-    } else {
-        for (int e = lane; e < wh * bw; e += 32) {
-            int r = e / bw, c = e - r * bw;
-            const uint8_t* w = win + r * wpitch + c;
-            int s = 0;
-#pragma unroll
-            for (int q = 0; q < NT; q++) s += th[q] * w[q];
-            tmp[r * bw + c] = (int16_t)s;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int k = 0; k < MAXE; k++) {
-            int e = lane + 32 * k;
-            if (e < bw * bh) {
-                int r = e / bw, c = e - r * bw;
-                int s = 0;
-#pragma unroll
-                for (int q = 0; q < NT; q++) s += tv[q] * tmp[(r + q) * bw + c];
-                pred[k] = (int16_t)(s >> 6);
-            }
-        }
-    }
-    __syncwarp();
-}
-
-template <int MAXE>
-__device__ __forceinline__ void mc_weight_store(const int (&p0)[MAXE], const int (&p1)[MAXE], bool u0, bool u1,
-                                                const hevc_wp_t* wp, int ci, uint8_t* dst, int pitch, int bw,
-                                                int bh, int lane) {
-#pragma unroll
-    for (int k = 0; k < MAXE; k++) {
-        int e = lane + 32 * k;
-        if (e >= bw * bh) continue;
-        int r = e / bw, c = e - r * bw;
-        int v;
-        if (!wp) {
-            v = (u0 && u1) ? (p0[k] + p1[k] + 64) >> 7 : ((u0 ? p0[k] : p1[k]) + 32) >> 6;
-        } else {
-            int lw = wp->log2wd[ci ? 1 : 0];
-            if (u0 && u1)
-                v = (p0[k] * wp->w[0][ci] + p1[k] * wp->w[1][ci] + ((wp->o[0][ci] + wp->o[1][ci] + 1) << lw)) >>
-                    (lw + 1);
-            else {
-                int l = u0 ? 0 : 1;
-                v = (((u0 ? p0[k] : p1[k]) * wp->w[l][ci] + (1 << (lw - 1))) >> lw) + wp->o[l][ci];
-            }
-        }
-        dst[(int64_t)r * pitch + c] = (uint8_t)clip_u8(v);
-    }
-}
-
-__global__ void __launch_bounds__(32 * MC_WARPS) k_mc(const __grid_constant__ SegTable st) {
-    __shared__ __align__(16) McSmem sm[MC_WARPS];
-    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const Seg& sg = st.s[find_seg(st, blockIdx.x)];
-    const int item = (blockIdx.x - sg.block0) * MC_WARPS + warp;
-    if (item >= sg.n_items) return;
-    const McItem it = static_cast<const McItem*>(sg.items)[item];
-    const PicDesc& P = *sg.pic;
-    const hevc_pu_t pu = P.pus[it.pu];
-    McSmem& S = sm[warp];
-    const int tx = pu.x + it.dx, ty = pu.y + it.dy, bw = it.w, bh = it.h;
-    const bool use[2] = {pu.ref_idx[0] >= 0, pu.ref_idx[1] >= 0};
-    const hevc_wp_t* wp = pu.wp >= 0 ? &P.wp[pu.wp] : nullptr;
-    const int W = P.width, H = P.height;
-
-    // luma
-    {
-        int pl[2][8];
-#pragma unroll
-        for (int l = 0; l < 2; l++) {
-            if (!use[l]) continue;
-            const uint8_t* ref = P.ref[l][pu.ref_idx[l]];
-            int mvx = pu.mv[l][0], mvy = pu.mv[l][1];
-            mc_block<8, 8>(ref, P.pitch_y, W, H, tx + (mvx >> 2), ty + (mvy >> 2), mvx & 3, mvy & 3, bw, bh, S.win,
-                           24, S.tmp, lane, pl[l]);
-        }
-        mc_weight_store<8>(pl[0], pl[1], use[0], use[1], wp, 0, P.rec + (int64_t)ty * P.pitch_y + tx, P.pitch_y, bw,
-                           bh, lane);
-    }
-    // chroma (4:2:0)
-    const int cw = bw / 2, ch = bh / 2, cx = tx / 2, cy = ty / 2;
-#pragma unroll
-    for (int ci = 1; ci <= 2; ci++) {
-        int pl[2][2];
-        int64_t off = ci == 1 ? P.off_cb : P.off_cr;
-#pragma unroll
-        for (int l = 0; l < 2; l++) {
-            if (!use[l]) continue;
-            const uint8_t* ref = P.ref[l][pu.ref_idx[l]] + off;
-            int mvx = pu.mv[l][0], mvy = pu.mv[l][1];
-            mc_block<4, 2>(ref, P.pitch_c, W / 2, H / 2, cx + (mvx >> 3), cy + (mvy >> 3), mvx & 7, mvy & 7, cw, ch,
-                           S.cwin[ci - 1], 12, S.ctmp, lane, pl[l]);
-        }
-        mc_weight_store<2>(pl[0], pl[1], use[0], use[1], wp, ci, P.rec + off + (int64_t)cy * P.pitch_c + cx,
-                           P.pitch_c, cw, ch, lane);
     }
 }
 
