@@ -243,8 +243,8 @@ struct hevcgpu_job {
     PicDesc host_desc{};
     int32_t n_res[4] = {0, 0, 0, 0};
     const int32_t* d_res[4] = {nullptr, nullptr, nullptr, nullptr};
-    int32_t n_mc = 0;
-    const McStrip* d_mc = nullptr;
+    int32_t n_mc[2] = {0, 0};            // luma strips, chroma strips
+    const McStrip* d_mc[2] = {nullptr, nullptr};
     int32_t n_ictu = 0;                 // CTUs that hold intra TUs
     int32_t epoch = 0;                  // intra launches of this job so far
     int32_t n_pus = 0;
@@ -468,16 +468,16 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         }
     }
     j->n_ictu = (int32_t)ictu_addr.size();
-    // MC strips: 4 columns x up to 16 rows, luma then chroma (Cb and Cr together), and
-    // bi- before uni-predicted PUs, so that the threads of a warp follow the same path
-    std::vector<McStrip> mc;
+    // MC strips: 4 columns x up to 16 rows; luma and chroma (Cb and Cr together) are two
+    // lists.  Each list is ordered bi- before uni-predicted PUs, then by strip height, so
+    // that the threads of a warp take the same path for the same number of rows.
+    std::vector<McStrip> mc[2];
     if (stages & ST_MC) {
-        for (int c = 0; c < 2; c++)
-            for (int pass = 0; pass < 2; pass++)
+        for (int c = 0; c < 2; c++) {
+            std::vector<std::pair<int, McStrip>> keyed;
             for (int i = 0; i < s->num_pus; i++) {
                 const hevc_pu_t& u = s->pus[i];
                 const bool bi = u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0;
-                if (bi != (pass == 0)) continue;
                 const int w = c ? u.w / 2 : u.w, h = c ? u.h / 2 : u.h;
                 for (int sy = 0; sy < h; sy += 16)
                     for (int sx = 0; sx < w; sx += 4) {
@@ -486,14 +486,19 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
                         m.sx = (uint8_t)sx;
                         m.sy = (uint8_t)sy;
                         m.h = (uint8_t)std::min(16, h - sy);
-                        m.chroma = (uint8_t)c;
-                        mc.push_back(m);
+                        m.pad = 0;
+                        keyed.emplace_back((bi ? 0 : 32) + (16 - m.h), m);
                     }
             }
+            std::stable_sort(keyed.begin(), keyed.end(),
+                             [](const std::pair<int, McStrip>& a, const std::pair<int, McStrip>& b) { return a.first < b.first; });
+            mc[c].reserve(keyed.size());
+            for (auto& kv : keyed) mc[c].push_back(kv.second);
+        }
     }
     j->n_pus = s->num_pus;
 
-    size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc, o_ia, o_idp, o_ito,
+    size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc[2], o_ia, o_idp, o_ito,
         o_itu, o_ile, o_iro;
     hevc_slice_t dflt{0, 0, 0, 1};
     auto pack = [&](Packer& pk) {
@@ -508,7 +513,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         o_slices = s->num_slices > 0 && s->slices ? pk.add(s->slices, sizeof(hevc_slice_t) * (size_t)s->num_slices)
                                                   : pk.add(&dflt, sizeof(dflt));
         for (int k = 0; k < 4; k++) o_res[k] = pk.add(bins[k].data(), sizeof(int32_t) * bins[k].size());
-        o_mc = pk.add(mc.data(), sizeof(McStrip) * mc.size());
+        for (int c = 0; c < 2; c++) o_mc[c] = pk.add(mc[c].data(), sizeof(McStrip) * mc[c].size());
         o_ia = pk.add(ictu_addr.data(), sizeof(int32_t) * ictu_addr.size());
         o_idp = pk.add(ictu_deps.data(), sizeof(int32_t) * ictu_deps.size());
         o_ito = pk.add(ictu_tu_off.data(), sizeof(int32_t) * ictu_tu_off.size());
@@ -596,8 +601,10 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         j->n_res[k] = (int32_t)bins[k].size();
         j->d_res[k] = reinterpret_cast<const int32_t*>(base + o_res[k]);
     }
-    j->n_mc = (int32_t)mc.size();
-    j->d_mc = reinterpret_cast<const McStrip*>(base + o_mc);
+    for (int c = 0; c < 2; c++) {
+        j->n_mc[c] = (int32_t)mc[c].size();
+        j->d_mc[c] = reinterpret_cast<const McStrip*>(base + o_mc[c]);
+    }
     return HEVCGPU_OK;
 }
 
@@ -713,9 +720,14 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
     }
     if (stages & ST_MC) {
         StageMark m(ctx, 1);
-        rc = L.items(k_mc, jobs, n, MC_THREADS, MC_THREADS, [](hevcgpu_job* j, const void*& p, int& c) {
-            p = j->d_mc;
-            c = j->n_mc;
+        rc = L.items(k_mc<false>, jobs, n, MC_THREADS, MC_THREADS, [](hevcgpu_job* j, const void*& p, int& c) {
+            p = j->d_mc[0];
+            c = j->n_mc[0];
+        });
+        if (rc) return rc;
+        rc = L.items(k_mc<true>, jobs, n, MC_THREADS, MC_THREADS, [](hevcgpu_job* j, const void*& p, int& c) {
+            p = j->d_mc[1];
+            c = j->n_mc[1];
         });
         if (rc) return rc;
     }

@@ -48,7 +48,7 @@ struct McStrip {
     int32_t pu;
     uint8_t sx, sy;   // strip offset inside the PU, in samples of its component
     uint8_t h;        // rows (1..16)
-    uint8_t chroma;   // 0: luma, 1: Cb and Cr
+    uint8_t pad;
 };
 constexpr int MC_THREADS = 128;
 
@@ -155,12 +155,13 @@ __device__ __forceinline__ int hi16(uint32_t v) { return (int)(int16_t)(v >> 16)
 // One strip of one component: the lists run one after the other; a bi-predicted strip
 // keeps its list-0 predictions in shared memory (s_pred[row][thread], int16 x 4) until the
 // list-1 pass combines them.  Chroma strips may be 2 wide at the end of a 2/6-wide PU.
+template <bool CHROMA>
 __device__ __forceinline__ void mc_strip(const PicDesc& P, const hevc_pu_t& pu, const McStrip& s, uint2 (*s_pred)[MC_THREADS]) {
     const bool use0 = pu.ref_idx[0] >= 0, use1 = pu.ref_idx[1] >= 0, bi = use0 && use1;
     const hevc_wp_t* wp = pu.wp >= 0 ? &P.wp[pu.wp] : nullptr;
     const int tid = threadIdx.x;
-    const bool chroma = s.chroma != 0;
-    const int sub = chroma ? 2 : 1;
+    constexpr bool chroma = CHROMA;
+    constexpr int sub = chroma ? 2 : 1;
     const int x = pu.x / sub + s.sx, y = pu.y / sub + s.sy, h = s.h;
     const int width = min(4, pu.w / sub - s.sx);
     const int pw = P.width / sub, ph = P.height / sub, pitch = chroma ? P.pitch_c : P.pitch_y;
@@ -187,14 +188,14 @@ __device__ __forceinline__ void mc_strip(const PicDesc& P, const hevc_pu_t& pu, 
                 uint32_t b = 0;
 #pragma unroll
                 for (int j = 0; j < 4; j++) b |= (uint32_t)weigh(q[j], p[j], use0, use1, wp, ci) << (8 * j);
-                if (!chroma) {
+                if constexpr (!chroma) {
                     *reinterpret_cast<uint32_t*>(o) = b;   // luma strips are 4 wide and 4-aligned
                 } else {
                     *reinterpret_cast<uint16_t*>(o) = (uint16_t)b;
                     if (width == 4) *reinterpret_cast<uint16_t*>(o + 2) = (uint16_t)(b >> 16);
                 }
             };
-            if (!chroma)
+            if constexpr (!chroma)
                 filter_strip<8>(ref, pitch, pw, ph, x + (mvx >> 2), y + (mvy >> 2), mvx & 3, mvy & 3, h, emit);
             else
                 filter_strip<4>(ref, pitch, pw, ph, x + (mvx >> 3), y + (mvy >> 3), mvx & 7, mvy & 7, h, emit);
@@ -202,7 +203,9 @@ __device__ __forceinline__ void mc_strip(const PicDesc& P, const hevc_pu_t& pu, 
     }
 }
 
-__global__ void __launch_bounds__(MC_THREADS) k_mc(const __grid_constant__ SegTable st) {
+// Luma strips and chroma strips are separate launches (separate item lists).
+template <bool CHROMA>
+__global__ void __launch_bounds__(MC_THREADS, 6) k_mc(const __grid_constant__ SegTable st) {
     __shared__ uint2 s_pred[16][MC_THREADS];
     const Seg& sg = st.s[find_seg(st, blockIdx.x)];
     const int item = (blockIdx.x - sg.block0) * MC_THREADS + threadIdx.x;
@@ -210,7 +213,7 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc(const __grid_constant__ SegTa
     const McStrip s = static_cast<const McStrip*>(sg.items)[item];
     const PicDesc& P = *sg.pic;
     const hevc_pu_t pu = P.pus[s.pu];
-    mc_strip(P, pu, s, s_pred);
+    mc_strip<CHROMA>(P, pu, s, s_pred);
 }
 
 }  // namespace hevcgpu
