@@ -789,7 +789,7 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
     if (stages & ST_SAO) {
         StageMark m(ctx, 6);
         rc = L.pictures(k_sao, jobs, n, 256, 3, [](hevcgpu_job* j) {
-            int groups = (j->params.width / 4) * j->params.height;
+            int groups = ((j->params.width + SAO_G - 1) / SAO_G) * j->params.height;  // luma: the most
             return (groups + 255) / 256;
         });
         if (rc) return rc;

@@ -1,24 +1,17 @@
-// intra.cuh — intra prediction as a dataflow over transform units.
+// intra.cuh — intra prediction (perform_intra_prediction, intra_prediction.cpp:428-481,
+// with build_reference_samples :44-211, filtering :217-257, planar/DC/angular :263-422).
 //
-// Every intra TU reads reference samples left of and above it (build_reference_samples,
-// intra_prediction.cpp:44-211).  The host lists, for each intra TU, the earlier intra TUs
-// that own any of those samples (the only samples that are not final when this kernel
-// starts: MC and the inter residuals ran before).  That DAG replaces the CTU wavefront:
-//
-//   k_intra_arm   re-arms the dependency counters and seeds a device queue with the TUs
-//                 that wait for nothing;
-//   k_intra_flow  persistent warps claim queue slots in order, wait (bounded) until their
-//                 slot is published, predict the TU (reference samples, substitution,
-//                 smoothing, planar/DC/angular, + residual, clip) straight into the
-//                 picture, then count down their dependents and publish those that became
-//                 ready.
-//
-// Progress is guaranteed without co-residency: a warp only waits for slot t after slots
-// 0..t-1 were claimed by warps that are already running, and once those TUs are done some
-// remaining TU has all its dependencies met (the graph is acyclic), so slot t gets
-// published.  Every wait is bounded anyway: after SPIN_LIMIT polls the warp sets
-// ST_TIMEOUT (in the launch state, which stops the other warps, and in the context's
-// sticky status word that the host turns into HEVCGPU_ETIMEOUT) and returns.
+// Every intra TU reads reference samples left of and above it.  Those samples are final
+// when this stage runs, except where an earlier intra TU writes them (MC and the inter
+// residuals ran before).  The host turns that into two levels of schedule:
+//   - per CTU, a level for each intra TU in the DAG of the CTU's own intra TUs;
+//   - per CTU, the at most four earlier CTUs (left, above-left, above, above-right) whose
+//     intra TUs own samples it reads.
+// k_intra_ctus runs one CTA per CTU with intra TUs: it waits (bounded) for those CTUs,
+// stages the CTU, its neighbourhood, its TU records and residuals in shared memory, and
+// runs the TUs level by level, one warp per TU.  Every wait gives up after SPIN_LIMIT
+// polls, sets ST_TIMEOUT in the context's sticky status word (the host turns it into
+// HEVCGPU_ETIMEOUT) and returns.
 #pragma once
 
 #include <cuda/atomic>
@@ -51,30 +44,32 @@ struct CtuTile {
 // current CTB in raster order and share its slice and tile (intra_prediction.cpp:108-124).
 enum : uint32_t { NB_LEFT = 1u, NB_ABOVE_LEFT = 2u, NB_ABOVE = 4u, NB_ABOVE_RIGHT = 8u };
 
-// Predict + reconstruct one intra TU with one warp (perform_intra_prediction,
-// intra_prediction.cpp:428-481, then reconstruct_block's add and clip).  Reference
-// samples come from the CTU tile; results go to the tile (for later TUs) and the picture.
-// res is the TU's residual (null when it has none).
-__device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W, const CtuTile& tile,
-                         uint32_t nb_mask, const int16_t* res) {
-    const int ci = t.c_idx, sub = ci ? 2 : 1;
-    const int n = 1 << t.log2_size, log2 = t.log2_size;
+// Predict + reconstruct one intra TU of size 1 << LOG2 in plane CI (0 luma, 1/2 chroma)
+// with one warp (perform_intra_prediction, then reconstruct_block's add and clip).
+// Reference samples come from the CTU tile; results go to the tile (for later TUs) and
+// the picture.  res is the TU's residual (null when it has none).
+template <int LOG2, bool CHROMA>
+__device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W,
+                                         const CtuTile& tile, uint32_t nb_mask, const int16_t* res) {
+    constexpr int n = 1 << LOG2, sub = CHROMA ? 2 : 1;
+    constexpr int total = 4 * n + 1, R = (total + 31) / 32;  // reference samples, lane rounds
+    const int ci = t.c_idx;
     const int xc = t.x, yc = t.y;
-    const int ctb = 1 << P.log2_ctb, ctbc = ctb / sub;
-    const int rx = xc / ctbc, ry = yc / ctbc;
+    const int log2c = P.log2_ctb - (CHROMA ? 1 : 0);          // CTB size in this plane
+    const int rx = xc >> log2c, ry = yc >> log2c;
     const int pw = P.width / sub, ph = P.height / sub;
-    const int ox = rx * ctb, oy = ry * ctb;
-    const int pitch = ci ? P.pitch_c : P.pitch_y;
+    const int ox = rx << P.log2_ctb, oy = ry << P.log2_ctb;   // CTB origin in luma samples
+    const int pitch = CHROMA ? P.pitch_c : P.pitch_y;
     uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));
     const uint32_t cur_z = zorder16((uint32_t)((xc * sub - ox) >> 2), (uint32_t)((yc * sub - oy) >> 2));
-    const int total = 4 * n + 1;
 
     // 1. reference samples and their availability: in the picture, and either in an
     //    earlier CTB of the same slice and tile, or in this CTB at a lower z-scan address
-    //    of the 4x4 luma unit (intra_prediction.cpp:102-133)
-    uint32_t mask[5];
+    //    of the 4x4 luma unit (intra_prediction.cpp:102-133).  Index i runs from the
+    //    bottom-left sample (0) through the corner (2n) to the top-right one (4n).
+    uint32_t mask[R];
 #pragma unroll
-    for (int r = 0; r < 5; r++) {
+    for (int r = 0; r < R; r++) {
         const int i = lane + 32 * r;
         bool ok = false;
         int val = 0;
@@ -84,7 +79,7 @@ __device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWa
             else if (i == 2 * n) { px = xc - 1; py = yc - 1; }
             else { px = xc + (i - 2 * n - 1); py = yc - 1; }
             if (px >= 0 && py >= 0 && px < pw && py < ph) {
-                const int ncx = px / ctbc, ncy = py / ctbc;
+                const int ncx = px >> log2c, ncy = py >> log2c;
                 if (ncx != rx || ncy != ry) {
                     // reference positions reach one CTB left, one CTB right (top row) and
                     // one CTB row up or down; later CTBs are never available
@@ -107,10 +102,10 @@ __device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWa
     //    below it in the array, or the first available one; none available -> 128
     int first = -1;
 #pragma unroll
-    for (int r = 0; r < 5; r++)
+    for (int r = 0; r < R; r++)
         if (first < 0 && mask[r]) first = 32 * r + __ffs(mask[r]) - 1;
 #pragma unroll
-    for (int r = 0; r < 5; r++) {
+    for (int r = 0; r < R; r++) {
         const int i = lane + 32 * r;
         if (i >= total) continue;
         int v;
@@ -120,8 +115,9 @@ __device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWa
             int j = -1;
             const uint32_t m = lane ? (mask[r] & ((1u << lane) - 1u)) : 0u;
             if (m) j = 32 * r + 31 - __clz(m);
-            for (int q = r - 1; q >= 0 && j < 0; q--)
-                if (mask[q]) j = 32 * q + 31 - __clz(mask[q]);
+#pragma unroll
+            for (int q = r - 1; q >= 0; q--)
+                if (j < 0 && mask[q]) j = 32 * q + 31 - __clz(mask[q]);
             v = W.raw[j < 0 ? first : j];
         }
         W.s[i] = (int16_t)v;
@@ -130,57 +126,63 @@ __device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWa
     // 3. smoothing of luma references (:217-257, :443-471): [1 2 1] over the linear array
     //    (which also gives the corner filter), or the bilinear strong smoothing of 32x32
     const int mode = t.intra_mode;
-    const int16_t* R = W.s;
-    if (ci == 0 && !P.intra_smoothing_disabled && mode != 1 && n != 4) {
+    const int16_t* R_ = W.s;
+    if constexpr (!CHROMA && n != 4) {
+        constexpr int thr = n == 8 ? 7 : (n == 16 ? 1 : 0);
         const int d = min(abs(mode - 26), abs(mode - 10));
-        const int thr = n == 8 ? 7 : (n == 16 ? 1 : 0);
-        if (d > thr) {
+        if (!P.intra_smoothing_disabled && mode != 1 && d > thr) {
             bool bil = false;
-            if (P.strong_intra && n == 32) {
-                const int c = W.s[2 * n];
-                bil = abs(c + W.s[4 * n] - 2 * W.s[3 * n]) < 8 && abs(c + W.s[0] - 2 * W.s[n]) < 8;
+            if constexpr (n == 32) {
+                if (P.strong_intra) {
+                    const int c = W.s[2 * n];
+                    bil = abs(c + W.s[4 * n] - 2 * W.s[3 * n]) < 8 && abs(c + W.s[0] - 2 * W.s[n]) < 8;
+                }
             }
 #pragma unroll
-            for (int r = 0; r < 5; r++) {
+            for (int r = 0; r < R; r++) {
                 const int i = lane + 32 * r;
                 if (i >= total) continue;
                 int v;
                 if (i == 0 || i == 4 * n) v = W.s[i];
                 else if (bil) {
                     if (i == 2 * n) v = W.s[i];
-                    else if (i > 2 * n) { int k = i - 2 * n; v = ((2 * n - k) * W.s[2 * n] + k * W.s[4 * n] + n) >> (log2 + 1); }
-                    else { int k = 2 * n - i; v = ((2 * n - k) * W.s[2 * n] + k * W.s[0] + n) >> (log2 + 1); }
+                    else if (i > 2 * n) { const int k = i - 2 * n; v = ((2 * n - k) * W.s[2 * n] + k * W.s[4 * n] + n) >> (LOG2 + 1); }
+                    else { const int k = 2 * n - i; v = ((2 * n - k) * W.s[2 * n] + k * W.s[0] + n) >> (LOG2 + 1); }
                 } else {
                     v = (W.s[i - 1] + 2 * W.s[i] + W.s[i + 1] + 2) >> 2;
                 }
                 W.f[i] = (int16_t)v;
             }
             __syncwarp();
-            R = W.f;
+            R_ = W.f;
         }
     }
-    // 4. prediction (top[k] = R[2n + k], left[k] = R[2n - k]) + residual, clip, store
+    // 4. prediction (top[k] = R_[2n + k], left[k] = R_[2n - k]) + residual, clip, store
     const int ang = c_intra_angle[mode];
     const int inv = c_inv_angle[mode];
     int dc = 0;
     if (mode == 1) {  // predict_dc :295-317
         int s = 0;
-        for (int i = lane; i < n; i += 32) s += R[2 * n + 1 + i] + R[2 * n - 1 - i];
+        for (int i = lane; i < n; i += 32) s += R_[2 * n + 1 + i] + R_[2 * n - 1 - i];
         s = __reduce_add_sync(0xffffffffu, s);
-        dc = (s + n) >> (log2 + 1);
+        dc = (s + n) >> (LOG2 + 1);
     }
-    for (int e = lane; e < n * n; e += 32) {
-        const int y = e >> log2, x = e & (n - 1);
+    constexpr int PER_LANE = (n * n + 31) / 32;
+#pragma unroll
+    for (int q = 0; q < PER_LANE; q++) {
+        const int e = lane + 32 * q;
+        if (e >= n * n) break;
+        const int y = e >> LOG2, x = e & (n - 1);
         int p;
         if (mode == 0) {  // predict_planar :263-289
-            p = ((n - 1 - x) * R[2 * n - 1 - y] + (x + 1) * R[3 * n + 1] + (n - 1 - y) * R[2 * n + 1 + x] +
-                 (y + 1) * R[n - 1] + n) >> (log2 + 1);
+            p = ((n - 1 - x) * R_[2 * n - 1 - y] + (x + 1) * R_[3 * n + 1] + (n - 1 - y) * R_[2 * n + 1 + x] +
+                 (y + 1) * R_[n - 1] + n) >> (LOG2 + 1);
         } else if (mode == 1) {
             p = dc;
-            if (ci == 0 && n < 32) {
-                if (x == 0 && y == 0) p = (R[2 * n + 1] + R[2 * n - 1] + 2 * dc + 2) >> 2;
-                else if (y == 0) p = (R[2 * n + 1 + x] + 3 * dc + 2) >> 2;
-                else if (x == 0) p = (R[2 * n - 1 - y] + 3 * dc + 2) >> 2;
+            if (!CHROMA && n < 32) {
+                if (x == 0 && y == 0) p = (R_[2 * n + 1] + R_[2 * n - 1] + 2 * dc + 2) >> 2;
+                else if (y == 0) p = (R_[2 * n + 1 + x] + 3 * dc + 2) >> 2;
+                else if (x == 0) p = (R_[2 * n - 1 - y] + 3 * dc + 2) >> 2;
             }
         } else {  // predict_angular :323-422
             const bool vert = mode >= 18;
@@ -190,19 +192,39 @@ __device__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWa
             // main reference (top for vertical, left for horizontal); negative indices
             // project onto the side reference through invAngle (:346-368)
             auto ref_at = [&](int q) -> int {
-                if (q >= 0) return vert ? R[2 * n + q] : R[2 * n - q];
+                if (q >= 0) return vert ? R_[2 * n + q] : R_[2 * n - q];
                 const int si = min(2 * n, ((-q) * inv + 128) >> 8);
-                return vert ? R[2 * n - si] : R[2 * n + si];
+                return vert ? R_[2 * n - si] : R_[2 * n + si];
             };
             p = fr ? ((32 - fr) * ref_at(ri) + fr * ref_at(ri + 1) + 16) >> 5 : ref_at(ri);
-            if (ci == 0 && n < 32) {
-                if (mode == 26 && x == 0) p = clip_u8(p + ((R[2 * n - 1 - y] - R[2 * n]) >> 1));
-                else if (mode == 10 && y == 0) p = clip_u8(p + ((R[2 * n + 1 + x] - R[2 * n]) >> 1));
+            if (!CHROMA && n < 32) {
+                if (mode == 26 && x == 0) p = clip_u8(p + ((R_[2 * n - 1 - y] - R_[2 * n]) >> 1));
+                else if (mode == 10 && y == 0) p = clip_u8(p + ((R_[2 * n + 1 + x] - R_[2 * n]) >> 1));
             }
         }
         const uint8_t v = (uint8_t)clip_u8(p + (res ? res[e] : 0));
         tile.t[(yc + y - tile.y0) * tile.pitch + (xc + x - tile.x0)] = v;
         plane[(int64_t)(yc + y) * pitch + xc + x] = v;
+    }
+}
+
+// Size/plane dispatch of intra_tu.
+__device__ __forceinline__ void intra_tu_any(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W,
+                                             const CtuTile& tile, uint32_t nb_mask, const int16_t* res) {
+    if (t.c_idx == 0) {
+        switch (t.log2_size) {
+            case 2: intra_tu<2, false>(P, t, lane, W, tile, nb_mask, res); break;
+            case 3: intra_tu<3, false>(P, t, lane, W, tile, nb_mask, res); break;
+            case 4: intra_tu<4, false>(P, t, lane, W, tile, nb_mask, res); break;
+            default: intra_tu<5, false>(P, t, lane, W, tile, nb_mask, res); break;
+        }
+    } else {
+        switch (t.log2_size) {
+            case 2: intra_tu<2, true>(P, t, lane, W, tile, nb_mask, res); break;
+            case 3: intra_tu<3, true>(P, t, lane, W, tile, nb_mask, res); break;
+            case 4: intra_tu<4, true>(P, t, lane, W, tile, nb_mask, res); break;
+            default: intra_tu<5, true>(P, t, lane, W, tile, nb_mask, res); break;
+        }
     }
 }
 
@@ -330,7 +352,7 @@ __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant
             tile.x0 = rx * ctbc - IC_MARGIN;
             tile.y0 = ry * ctbc - 1;
             const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + P.itu_res_off[off + i] : nullptr;
-            intra_tu(P, tu, lane, ws[warp], tile, nb, res);
+            intra_tu_any(P, tu, lane, ws[warp], tile, nb, res);
         }
         __syncthreads();
         pos = lvl_end;

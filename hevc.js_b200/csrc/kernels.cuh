@@ -459,92 +459,110 @@ __global__ void __launch_bounds__(256) k_deblock(const __grid_constant__ SegTabl
 }
 
 // ======================================================================================
-// SAO: one thread per 4 horizontal samples of one plane, reading the deblocked picture
-// (rec) and writing the DPB slot (dst); samples without SAO are copied.
+// SAO: one thread per 8 horizontal samples of one plane (a group never straddles a CTB:
+// CTBs are at least 8 samples wide in every plane), reading the deblocked picture (rec)
+// with 8-byte loads and writing the DPB slot (dst); groups without SAO are copied.
 // ======================================================================================
+constexpr int SAO_G = 8;
+
+__device__ __forceinline__ int sign3(int d) { return (d > 0) - (d < 0); }
+
 __global__ void __launch_bounds__(256) k_sao(const __grid_constant__ SegTable st) {
     const PicDesc& P = *st.s[blockIdx.y].pic;
     const int ci = blockIdx.z;
     const int sub = ci ? 2 : 1;
     const int pw = P.width / sub, ph = P.height / sub;
-    const int groups = pw >> 2;
+    const int groups = (pw + SAO_G - 1) / SAO_G;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = tid / groups, x = (tid % groups) * 4;
+    const int y = tid / groups, x = (tid % groups) * SAO_G;
     if (y >= ph) return;
+    const int n = min(SAO_G, pw - x);  // 8, or 4 at the end of a row
     const int pitch = ci ? P.pitch_c : P.pitch_y;
     const int64_t base = ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr);
     const uint8_t* S = P.rec + base;
     uint8_t* D = P.dst + base;
-    const uint32_t c4 = __ldg(reinterpret_cast<const uint32_t*>(S + (int64_t)y * pitch + x));
-    uint32_t out = c4;
-    const int ctbc = (1 << P.log2_ctb) / sub;
-    const int addr = (y / ctbc) * P.wctb + x / ctbc;
-    const hevc_sao_t& sp = P.sao[addr];
-    const int type = P.sao_enabled ? sp.type[ci] : 0;
+    const int64_t at = (int64_t)y * pitch + x;
+    // x is a multiple of 8 and pitches of 64: 8-byte aligned (a 4-byte tail reads 4 more
+    // bytes of the row padding, which are not used)
+    const uint2 c8 = __ldg(reinterpret_cast<const uint2*>(S + at));
+    const int log2c = P.log2_ctb - (sub - 1);
+    const int addr = (y >> log2c) * P.wctb + (x >> log2c);
+    const int type = P.sao_enabled ? P.sao[addr].type[ci] : 0;
+    uint32_t o[2] = {c8.x, c8.y};
     if (type != 0) {
-        const int gw = P.width >> 2;
-        const bool check_slices = P.slice_check || P.tiles_check;
-        // edge offset: the words left of, at and right of the group in the rows the
-        // class needs (neighbours outside the picture are never read)
-        const int cl = sp.eo_class[ci];
+        const hevc_sao_t& sp = P.sao[addr];
+        // the five offsets as bytes of one word pair (index k -> byte k), sign-extended on use
+        uint64_t offs = 0;
+#pragma unroll
+        for (int k = 0; k < 5; k++) offs |= (uint64_t)(uint8_t)sp.offset[ci][k] << (8 * k);
+        auto off = [&](int k) { return (int)(int8_t)(offs >> (8 * k)); };
+        const int cl = sp.eo_class[ci], band = sp.band_pos[ci];
         const int dx0 = cl == 1 ? 0 : (cl == 3 ? 1 : -1), dy0 = cl == 0 ? 0 : -1;
         const int dx1 = -dx0, dy1 = -dy0;
-        // per neighbour row k: samples x-1 .. x+4 packed into bytes 0..5 of nw[k]
-        uint64_t nw[2] = {0, 0};
+        // edge offset: samples x-1 .. x+8 of the two neighbour rows, byte i+1 of nb[k]
+        uint32_t nb[2][3] = {{0, 0, 0}, {0, 0, 0}};
+        bool row_ok[2] = {false, false};
         if (type == 2) {
 #pragma unroll
             for (int k = 0; k < 2; k++) {
                 const int yy = y + (k ? dy1 : dy0);
-                if (yy < 0 || yy >= ph) continue;
-                const uint32_t* row = reinterpret_cast<const uint32_t*>(S + (int64_t)yy * pitch + x);
-                const uint32_t mid = yy == y ? c4 : __ldg(row);
-                const uint32_t lo = x >= 4 ? __ldg(row - 1) : 0u;
-                const uint32_t hi = x + 4 < pw ? __ldg(row + 1) : 0u;
-                nw[k] = (uint64_t)(lo >> 24) | ((uint64_t)mid << 8) | ((uint64_t)(hi & 0xFFu) << 40);
+                row_ok[k] = yy >= 0 && yy < ph;
+                if (!row_ok[k]) continue;
+                const uint8_t* row = S + (int64_t)yy * pitch + x;
+                const uint2 m = yy == y ? c8 : __ldg(reinterpret_cast<const uint2*>(row));
+                const uint32_t lo = x >= 4 ? __ldg(reinterpret_cast<const uint32_t*>(row) - 1) : 0u;
+                const uint32_t hi = x + 8 < pw ? __ldg(reinterpret_cast<const uint32_t*>(row) + 2) : 0u;
+                nb[k][0] = (lo >> 24) | (m.x << 8);
+                nb[k][1] = (m.x >> 24) | (m.y << 8);
+                nb[k][2] = (m.y >> 24) | ((hi & 0xFFu) << 8);
             }
         }
-        auto nbyte = [&](int k, int off) -> int {  // sample at x + off (off in -1..4) of row k
-            return (int)((nw[k] >> (8 * (off + 1))) & 0xFFu);
-        };
+        const int gw = P.width >> 2;
+        const bool check_slices = P.slice_check || P.tiles_check;
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
+        for (int i = 0; i < SAO_G; i++) {
+            if (i >= n) break;
             const int xs = x + i;
             if (P.pcm_bypass_any) {
                 const uint32_t b = P.blk[(int64_t)((y * sub) >> 2) * gw + ((xs * sub) >> 2)];
                 if ((P.pcm_lf_disabled && (b & HEVC_BLK_PCM)) || (b & HEVC_BLK_BYPASS)) continue;
             }
-            const int c = (c4 >> (8 * i)) & 0xFF;
+            const int c = (o[i >> 2] >> (8 * (i & 3))) & 0xFF;
             int v;
             if (type == 2) {
-                const int ax = xs + dx0, ay = y + dy0, bx = xs + dx1, by = y + dy1;
-                if (ax < 0 || ay < 0 || ax >= pw || ay >= ph || bx < 0 || by < 0 || bx >= pw || by >= ph) continue;
+                const int ax = xs + dx0, bx = xs + dx1;
+                if (!row_ok[0] || !row_ok[1] || ax < 0 || ax >= pw || bx < 0 || bx >= pw) continue;
                 if (check_slices) {
                     bool skip = false;
+                    const int ay = y + dy0, by = y + dy1;
                     const int cur = ((y * sub) >> P.log2_ctb) * P.wctb + ((xs * sub) >> P.log2_ctb);
                     for (int nk = 0; nk < 2 && !skip; nk++) {
-                        int nx = nk ? bx : ax, ny = nk ? by : ay;
-                        int na = ((ny * sub) >> P.log2_ctb) * P.wctb + ((nx * sub) >> P.log2_ctb);
-                        int sc = P.ctb_slice ? P.ctb_slice[cur] : 0, sn = P.ctb_slice ? P.ctb_slice[na] : 0;
-                        if (sc != sn) {
-                            int owner = sn < sc ? cur : na;
-                            if (!slice_at(P, owner).lf_across_slices) skip = true;
-                        }
+                        const int nx = nk ? bx : ax, ny = nk ? by : ay;
+                        const int na = ((ny * sub) >> P.log2_ctb) * P.wctb + ((nx * sub) >> P.log2_ctb);
+                        const int sc = P.ctb_slice ? P.ctb_slice[cur] : 0, sn = P.ctb_slice ? P.ctb_slice[na] : 0;
+                        if (sc != sn && !slice_at(P, sn < sc ? cur : na).lf_across_slices) skip = true;
                         if (!skip && P.tiles_check && P.ctb_tile && P.ctb_tile[cur] != P.ctb_tile[na]) skip = true;
                     }
                     if (skip) continue;
                 }
-                const int a = nbyte(0, i + dx0), bb = nbyte(1, i + dx1);
-                const int e = 2 + (c < a ? -1 : (c > a ? 1 : 0)) + (c < bb ? -1 : (c > bb ? 1 : 0));
-                v = c + sp.offset[ci][e];
+                // neighbour at column offset d (-1..1) of sample i: byte i + d + 1 of row k
+                auto nbyte = [&](int k, int q) {
+                    const uint32_t w = q < 4 ? nb[k][0] : (q < 8 ? nb[k][1] : nb[k][2]);
+                    return (int)((w >> (8 * (q & 3))) & 0xFFu);
+                };
+                const int a = nbyte(0, i + dx0 + 1), bb = nbyte(1, i + dx1 + 1);
+                const int e = 2 + sign3(c - a) + sign3(c - bb);
+                v = c + off(e);
             } else {
-                const int k = (c >> 3) - sp.band_pos[ci];
+                const int k = (c >> 3) - band;  // no wrap-around (sao.cpp:229-230)
                 if (k < 0 || k >= 4) continue;
-                v = c + sp.offset[ci][k];
+                v = c + off(k);
             }
-            out = (out & ~(0xFFu << (8 * i))) | ((uint32_t)clip_u8(v) << (8 * i));
+            o[i >> 2] = (o[i >> 2] & ~(0xFFu << (8 * (i & 3)))) | ((uint32_t)clip_u8(v) << (8 * (i & 3)));
         }
     }
-    *reinterpret_cast<uint32_t*>(D + (int64_t)y * pitch + x) = out;
+    if (n == SAO_G) *reinterpret_cast<uint2*>(D + at) = make_uint2(o[0], o[1]);
+    else *reinterpret_cast<uint32_t*>(D + at) = o[0];
 }
 
 }  // namespace hevcgpu
