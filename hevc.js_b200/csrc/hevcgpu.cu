@@ -946,6 +946,133 @@ int hevcgpu_residual_blocks(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int32_t nu
     return HEVCGPU_OK;
 }
 
+}  // extern "C"
+
+// ---- residual blocks without allocation ----------------------------------------------
+// hevcgpu_residual_blocks_static runs k_residual (RES_PACKED) on caller-owned device
+// buffers for callers that must not allocate while decoding: a serving process that
+// sized its device memory once at start-up, and decode threads on which cudaMalloc /
+// cudaFree would synchronise the device and stall the other streams' work.  Its scratch
+// (picture descriptor, TU records, per-size lists of TU indices) is the fixed array
+// below: one copy per device, since a __device__ variable exists in each device's
+// instance of the module.  Every call writes all the scratch it reads, so nothing there
+// has to start at zero.
+namespace {
+
+constexpr size_t STATIC_DESC_BYTES = 1024;
+static_assert(sizeof(PicDesc) <= STATIC_DESC_BYTES, "descriptor slot of the static scratch");
+static_assert(sizeof(hevc_tu_t) == 16, "TU record size");
+constexpr size_t STATIC_TUS_OFF = STATIC_DESC_BYTES;
+constexpr size_t STATIC_LISTS_OFF = STATIC_TUS_OFF + (size_t)HEVCGPU_STATIC_MAX_TUS * sizeof(hevc_tu_t);
+constexpr size_t STATIC_SCRATCH_BYTES = STATIC_LISTS_OFF + (size_t)HEVCGPU_STATIC_MAX_TUS * sizeof(int32_t);
+
+static __device__ __align__(256) uint8_t g_static_scratch[STATIC_SCRATCH_BYTES];
+
+// Host side: the per-size lists are built in a static array, and one lock serialises
+// whole calls, since every call on a device shares the one scratch array.
+constexpr int STATIC_MAX_DEVICES = 64;
+std::mutex g_static_mu;
+uint8_t* g_static_dev[STATIC_MAX_DEVICES];  // scratch address per device, set by the first call
+int32_t g_static_lists[HEVCGPU_STATIC_MAX_TUS];
+
+// The buffer must be device (or managed) memory of this device.
+int check_device_buffer(const void* p, int device, const char* what) {
+    if (reinterpret_cast<uintptr_t>(p) & 15) return fail(HEVCGPU_EINVAL, "%s is not 16-byte aligned", what);
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HEVCGPU_EINVAL, "%s: %s", what, cudaGetErrorString(e));
+    }
+    if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != device)
+        return fail(HEVCGPU_EINVAL, "%s is not device memory of device %d", what, device);
+    return HEVCGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hevcgpu_residual_blocks_static(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int32_t num_tus,
+                                   const int16_t* d_coeffs, uint64_t num_coeffs, const uint8_t* d_pred,
+                                   uint8_t* d_out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (num_tus < 0 || (num_tus && !tus)) return fail(HEVCGPU_EINVAL, "null arrays");
+    if (num_tus > HEVCGPU_STATIC_MAX_TUS)
+        return fail(HEVCGPU_EINVAL, "%d blocks: the static scratch holds at most %d", num_tus,
+                    HEVCGPU_STATIC_MAX_TUS);
+    if (ctx->device < 0 || ctx->device >= STATIC_MAX_DEVICES)
+        return fail(HEVCGPU_EUNSUPPORTED, "device %d: static scratch is kept for devices 0..%d", ctx->device,
+                    STATIC_MAX_DEVICES - 1);
+    if (num_tus == 0) return HEVCGPU_OK;
+    if ((rc = check_device_buffer(d_coeffs, ctx->device, "levels")) ||
+        (rc = check_device_buffer(d_pred, ctx->device, "prediction")) ||
+        (rc = check_device_buffer(d_out, ctx->device, "output")))
+        return rc;
+    for (int i = 0; i < num_tus; i++) {
+        const hevc_tu_t& t = tus[i];
+        int n = 1 << t.log2_size;
+        if (t.log2_size < 2 || t.log2_size > 5 || t.c_idx > 2 || (t.coeff_offset & 15) ||
+            (uint64_t)t.coeff_offset + (uint64_t)n * n > num_coeffs || t.qp > 99)
+            return fail(HEVCGPU_EINVAL, "block %d: size %d, coeff_offset %u (multiple of 16 inside the pool)", i, n,
+                        t.coeff_offset);
+    }
+
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    uint8_t*& base = g_static_dev[ctx->device];
+    if (!base) {
+        // first call on this device (its device is current): look up the scratch address
+        void* p = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_static_scratch));
+        base = static_cast<uint8_t*>(p);
+    }
+
+    // per-size lists of TU indices, back to back in g_static_lists
+    int32_t count[4] = {0, 0, 0, 0}, start[4];
+    for (int i = 0; i < num_tus; i++) count[tus[i].log2_size - 2]++;
+    start[0] = 0;
+    for (int k = 1; k < 4; k++) start[k] = start[k - 1] + count[k - 1];
+    int32_t fill[4] = {start[0], start[1], start[2], start[3]};
+    for (int i = 0; i < num_tus; i++) g_static_lists[fill[tus[i].log2_size - 2]++] = i;
+
+    PicDesc D;
+    std::memset(&D, 0, sizeof(D));
+    D.tus = reinterpret_cast<const hevc_tu_t*>(base + STATIC_TUS_OFF);
+    D.coeffs = d_coeffs;
+    D.rec = const_cast<uint8_t*>(d_pred);  // RES_PACKED reads the prediction through rec
+    D.dst = d_out;
+    // pageable sources: each copy has consumed its host buffer when the call returns
+    CUDA_TRY(cudaMemcpyAsync(base, &D, sizeof(D), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(base + STATIC_TUS_OFF, tus, sizeof(hevc_tu_t) * (size_t)num_tus,
+                             cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(base + STATIC_LISTS_OFF, g_static_lists, sizeof(int32_t) * (size_t)num_tus,
+                             cudaMemcpyHostToDevice, ctx->stream));
+
+    Launcher L{ctx, ctx->stream};
+    void (*kr[4])(const SegTable, int) = {k_residual<2>, k_residual<3>, k_residual<4>, k_residual<5>};
+    for (int k = 0; k < 4; k++) {
+        if (count[k] == 0) continue;
+        const int per_block = 128 >> (k + 2);
+        SegTable t;
+        std::memset(&t, 0, sizeof(t));
+        t.n = 1;
+        t.s[0].items = base + STATIC_LISTS_OFF + sizeof(int32_t) * (size_t)start[k];
+        t.s[0].pic = reinterpret_cast<const PicDesc*>(base);
+        t.s[0].n_items = count[k];
+        t.s[0].block0 = 0;
+        if ((rc = L.go(kr[k], dim3((count[k] + per_block - 1) / per_block), dim3(128), t, (int)RES_PACKED)))
+            return rc;
+    }
+    // the lock is held until the kernels are done with the scratch
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return HEVCGPU_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
 namespace {
 
 // Shared body of the picture-level stage entry points on host memory.
