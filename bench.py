@@ -100,33 +100,86 @@ def algorithmic_bytes(hb, pic):
 # --------------------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled through NVML every 5 ms during the timed
+    region (the device is found by its PCI bus id, so CUDA_VISIBLE_DEVICES remapping
+    does not matter).  Falls back to `nvidia-smi -lms 200` when NVML is unavailable."""
 
-    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown," \
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
-             "clocks_event_reasons.sw_power_cap"
+    PERIOD_S = 0.005
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
 
-    def __init__(self, index):
-        self.index = index
+    def __init__(self, local):
+        self.local = local
+        self.samples = []          # (sm_mhz, max_mhz, reasons bitmask)
+        self.stop = threading.Event()
+        self.nvml = None
         self.proc = None
-        self.lines = []
+        self.source = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+        p = torch.cuda.get_device_properties(self.local)
+        pynvml.nvmlInit()
+        bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _sample_nvml(self):
+        nv, h = self.nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.samples.append((float(sm), float(mx), int(rs)))
+
+    def _loop(self):
+        while not self.stop.wait(self.PERIOD_S):
+            try:
+                self._sample_nvml()
+            except Exception:
+                return
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+            self.nvml = self._handle()
+            self._sample_nvml()
+            self.source = "nvml 5 ms"
+            self.t = threading.Thread(target=self._loop, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
+        try:
+            fields = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+                      "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                      "clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.local}", f"--query-gpu={fields}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.source = "nvidia-smi 200 ms"
+            self.t = threading.Thread(target=self._read_smi, daemon=True)
             self.t.start()
         except OSError:
             self.proc = None
         return self
 
-    def _read(self):
+    def _read_smi(self):
+        bits = [0x8, 0x40, 0x20, 0x4]
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            parts = [p.strip() for p in line.split(",")]
+            try:
+                rs = sum(b for b, v in zip(bits, parts[2:6]) if v.lower().startswith("active"))
+                self.samples.append((float(parts[0]), float(parts[1]), rs))
+            except (ValueError, IndexError):
+                continue
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml:
+            try:
+                self._sample_nvml()
+            except Exception:
+                pass
+            self.t.join(timeout=1)
         if self.proc:
             self.proc.terminate()
             try:
@@ -135,24 +188,12 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[3:7]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": self.source}
+        reasons = sorted(n for n, b in self.REASONS.items() if any(s[2] & b for s in self.samples))
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples), "reasons": reasons,
+                "samples": len(self.samples), "source": self.source}
 
 
 # --------------------------------------------------------------------------- CPU arms
@@ -297,11 +338,10 @@ def run_ours(args, hb, rank, world, local):
 
     def e2e_step():
         nonlocal h2d_bytes
-        js = [st.prepare(p) for st, p in zip(streams, pics)]
+        js = hb.prepare_batch(streams, pics)
         h2d_bytes = sum(j.upload_bytes for j in js)
         hb.batch_launch(js, slots)
-        for i, st in enumerate(streams):
-            st.download(2, out_host[i])
+        hb.download_batch(streams, slots, out_host)
         for j in js:
             j.free()
     e2e_steps = max(3, args.steps // 5)

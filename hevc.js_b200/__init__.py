@@ -195,6 +195,8 @@ def gpu_lib():
             "hevcgpu_job_launch": ([P, C.c_int32], C.c_int),
             "hevcgpu_batch_launch": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
             "hevcgpu_stream_sync": ([P], C.c_int),
+            "hevcgpu_jobs_prepare": ([C.POINTER(P), C.POINTER(P), C.c_int32, C.POINTER(P)], C.c_int),
+            "hevcgpu_slots_download": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32, C.POINTER(P)], C.c_int),
             "hevcgpu_cuda_stream": ([P], P),
             "hevcgpu_launch_count": ([P], C.c_uint64),
             "hevcgpu_picture_decode": ([P, C.POINTER(PictureSyntax), C.c_int32], C.c_int),
@@ -354,12 +356,13 @@ class Stream:
 class Job:
     """A prepared picture (records uploaded once; hevcgpu_job_prepare)."""
 
-    def __init__(self, stream, pic):
+    def __init__(self, stream, pic, handle=None):
         self.stream = stream
         self.lib = stream.lib
-        h = C.c_void_p()
-        _check(self.lib.hevcgpu_job_prepare(stream.h, pic.syn_ptr, C.byref(h)))
-        self.h = h
+        if handle is None:
+            handle = C.c_void_p()
+            _check(self.lib.hevcgpu_job_prepare(stream.h, pic.syn_ptr, C.byref(handle)))
+        self.h = handle
         stream.ctx._children.add(self)
 
     def launch(self, dst_slot):
@@ -387,3 +390,28 @@ def batch_launch(jobs, dst_slots):
     arr = (C.c_void_p * n)(*[j.h for j in jobs])
     slots = (C.c_int32 * n)(*dst_slots)
     _check(lib.hevcgpu_batch_launch(arr, slots, n))
+
+
+def prepare_batch(streams, pics):
+    """Jobs for pics[i] on streams[i], built on the context's host workers
+    (hevcgpu_jobs_prepare)."""
+    lib = gpu_lib()
+    n = len(pics)
+    sts = (C.c_void_p * n)(*[st.h for st in streams])
+    syns = (C.c_void_p * n)(*[C.cast(p.syn_ptr, C.c_void_p) for p in pics])
+    out = (C.c_void_p * n)()
+    _check(lib.hevcgpu_jobs_prepare(sts, syns, n, out))
+    return [Job(st, None, C.c_void_p(h)) for st, h in zip(streams, out)]
+
+
+def download_batch(streams, slots, outs=None):
+    """Slot slots[i] of streams[i] into I420 host buffers (hevcgpu_slots_download)."""
+    lib = gpu_lib()
+    n = len(streams)
+    if outs is None:
+        outs = [np.empty(i420_size(st.width, st.height), np.uint8) for st in streams]
+    sts = (C.c_void_p * n)(*[st.h for st in streams])
+    sl = (C.c_int32 * n)(*slots)
+    ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+    _check(lib.hevcgpu_slots_download(sts, sl, n, ptrs))
+    return outs

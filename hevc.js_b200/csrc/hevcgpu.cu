@@ -4,14 +4,18 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "hevcgpu.h"
@@ -58,6 +62,90 @@ struct Layout {  // pitched 8-bit 4:2:0 picture buffer
         off_cr = off_cb + (int64_t)pitch_c * (h / 2);
         bytes = align_up(off_cr + (int64_t)pitch_c * (h / 2), 256);
     }
+};
+
+// Persistent host workers.  run(n, f) calls f(i) for every i < n, spread over the
+// workers and the calling thread, and returns when all calls are done.  One run at a
+// time per pool (the caller holds run_mu).  Workers make the context's device current
+// once at start.
+class HostPool {
+  public:
+    ~HostPool() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : threads_) t.join();
+    }
+    // Starts the workers on first use; false if no thread could be started.
+    void ensure(int device) {
+        std::lock_guard<std::mutex> g(m_);
+        if (started_) return;
+        started_ = true;
+        unsigned hw = std::thread::hardware_concurrency();
+        int workers = (int)std::min<unsigned>(hw ? hw : 1, 64) - 1;
+        for (int i = 0; i < workers; i++) {
+            try {
+                threads_.emplace_back([this, device] { loop(device); });
+            } catch (...) {
+                break;
+            }
+        }
+    }
+    void run(int n, const std::function<void(int)>& f) {
+        if (n <= 0) return;
+        std::unique_lock<std::mutex> lk(m_);
+        task_ = &f;
+        n_ = n;
+        next_.store(0);
+        done_ = 0;
+        gen_++;
+        lk.unlock();
+        cv_.notify_all();
+        int finished = drain(f);
+        lk.lock();
+        done_ += finished;
+        done_cv_.wait(lk, [&] { return done_ == n_ && busy_ == 0; });
+        task_ = nullptr;
+    }
+    std::mutex run_mu;
+
+  private:
+    int drain(const std::function<void(int)>& f) {
+        int finished = 0;
+        for (int i = next_.fetch_add(1); i < n_; i = next_.fetch_add(1)) {
+            f(i);
+            finished++;
+        }
+        return finished;
+    }
+    void loop(int device) {
+        cudaSetDevice(device);
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> lk(m_);
+        for (;;) {
+            cv_.wait(lk, [&] { return stop_ || (gen_ != seen && task_); });
+            if (stop_) return;
+            seen = gen_;
+            const std::function<void(int)>* f = task_;
+            busy_++;
+            lk.unlock();
+            int finished = drain(*f);
+            lk.lock();
+            busy_--;
+            done_ += finished;
+            if (done_ == n_ && busy_ == 0) done_cv_.notify_all();
+        }
+    }
+    std::vector<std::thread> threads_;
+    std::mutex m_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(int)>* task_ = nullptr;
+    std::atomic<int> next_{0};
+    int n_ = 0, done_ = 0, busy_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false, started_ = false;
 };
 
 }  // namespace
@@ -153,6 +241,9 @@ struct hevcgpu_ctx {
         auto it = host_sizes.find(p);
         if (it != host_sizes.end()) free_host.emplace(it->second, p);
     }
+    // host worker pool for the batched host-side calls (job preparation, downloads)
+    HostPool pool;
+    std::vector<cudaEvent_t> dl_events;  // per-picture completion of batched downloads
     // intra wavefront: FlowState (row ticket) followed by the sticky status word
     void* flow = nullptr;
     int sm_count = 148;
@@ -170,6 +261,7 @@ struct hevcgpu_ctx {
     ~hevcgpu_ctx() {
         if (flow) cudaFree(flow);
         for (auto e : ev_pool) cudaEventDestroy(e);
+        for (auto e : dl_events) cudaEventDestroy(e);
         for (auto& h : host_sizes) cudaFreeHost(h.first);
         for (auto& s : sizes) cudaFree(s.first);
         if (stream) cudaStreamDestroy(stream);
@@ -473,27 +565,32 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     // that the threads of a warp take the same path for the same number of rows.
     std::vector<McStrip> mc[2];
     if (stages & ST_MC) {
+        // counting sort on the key (bi ? 0 : 16) + (16 - strip height), stable in PU order
         for (int c = 0; c < 2; c++) {
-            std::vector<std::pair<int, McStrip>> keyed;
-            for (int i = 0; i < s->num_pus; i++) {
-                const hevc_pu_t& u = s->pus[i];
-                const bool bi = u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0;
-                const int w = c ? u.w / 2 : u.w, h = c ? u.h / 2 : u.h;
-                for (int sy = 0; sy < h; sy += 16)
-                    for (int sx = 0; sx < w; sx += 4) {
-                        McStrip m;
-                        m.pu = i;
-                        m.sx = (uint8_t)sx;
-                        m.sy = (uint8_t)sy;
-                        m.h = (uint8_t)std::min(16, h - sy);
-                        m.pad = 0;
-                        keyed.emplace_back((bi ? 0 : 32) + (16 - m.h), m);
+            int32_t cnt[33] = {};
+            auto each_strip = [&](auto&& emit) {
+                for (int i = 0; i < s->num_pus; i++) {
+                    const hevc_pu_t& u = s->pus[i];
+                    const int key0 = (u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0) ? 0 : 16;
+                    const int w = c ? u.w / 2 : u.w, h = c ? u.h / 2 : u.h;
+                    for (int sy = 0; sy < h; sy += 16) {
+                        const int sh = std::min(16, h - sy);
+                        for (int sx = 0; sx < w; sx += 4) emit(key0 + 16 - sh, i, sx, sy, sh);
                     }
-            }
-            std::stable_sort(keyed.begin(), keyed.end(),
-                             [](const std::pair<int, McStrip>& a, const std::pair<int, McStrip>& b) { return a.first < b.first; });
-            mc[c].reserve(keyed.size());
-            for (auto& kv : keyed) mc[c].push_back(kv.second);
+                }
+            };
+            each_strip([&](int key, int, int, int, int) { cnt[key + 1]++; });
+            for (int k = 1; k <= 32; k++) cnt[k] += cnt[k - 1];
+            mc[c].resize((size_t)cnt[32]);
+            McStrip* out = mc[c].data();
+            each_strip([&](int key, int i, int sx, int sy, int sh) {
+                McStrip& m = out[cnt[key]++];
+                m.pu = i;
+                m.sx = (uint8_t)sx;
+                m.sy = (uint8_t)sy;
+                m.h = (uint8_t)sh;
+                m.pad = 0;
+            });
         }
     }
     j->n_pus = s->num_pus;
@@ -1301,6 +1398,91 @@ int hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, i
         if (rc) return rc;
     }
     return run_stages(ctx, jobs, n, ST_ALL, RES_PICTURE);
+}
+
+int hevcgpu_jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns, int32_t n,
+                         hevcgpu_job_t** out) {
+    if (n < 0 || (n && (!sts || !syns || !out))) return fail(HEVCGPU_EINVAL, "null arrays");
+    if (n == 0) return HEVCGPU_OK;
+    for (int i = 0; i < n; i++) {
+        out[i] = nullptr;
+        if (!sts[i] || !syns[i]) return fail(HEVCGPU_EINVAL, "picture %d: null stream or syntax", i);
+        if (sts[i]->ctx != sts[0]->ctx) return fail(HEVCGPU_EINVAL, "picture %d: streams of two contexts", i);
+    }
+    hevcgpu_ctx* ctx = sts[0]->ctx;
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    std::vector<int> rcs((size_t)n, 0);
+    std::vector<std::string> msgs((size_t)n);
+    {
+        std::lock_guard<std::mutex> g(ctx->pool.run_mu);
+        ctx->pool.ensure(ctx->device);
+        ctx->pool.run(n, [&](int i) {
+            rcs[(size_t)i] = hevcgpu_job_prepare(sts[i], syns[i], &out[i]);
+            if (rcs[(size_t)i]) msgs[(size_t)i] = g_err;
+        });
+    }
+    for (int i = 0; i < n; i++) {
+        if (!rcs[(size_t)i]) continue;
+        for (int k = 0; k < n; k++) {
+            hevcgpu_job_free(out[k]);
+            out[k] = nullptr;
+        }
+        return fail(rcs[(size_t)i], "picture %d: %s", i, msgs[(size_t)i].c_str());
+    }
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n, uint8_t* const* outs) {
+    if (n < 0 || (n && (!sts || !slots || !outs))) return fail(HEVCGPU_EINVAL, "null arrays");
+    if (n == 0) return HEVCGPU_OK;
+    for (int i = 0; i < n; i++) {
+        if (!sts[i] || !outs[i]) return fail(HEVCGPU_EINVAL, "picture %d: null stream or buffer", i);
+        if (sts[i]->ctx != sts[0]->ctx) return fail(HEVCGPU_EINVAL, "picture %d: streams of two contexts", i);
+        if (slots[i] < 0 || slots[i] >= (int)sts[i]->slots.size())
+            return fail(HEVCGPU_EINVAL, "picture %d: bad slot %d", i, slots[i]);
+    }
+    hevcgpu_ctx* ctx = sts[0]->ctx;
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(ctx->pool.run_mu);
+    ctx->pool.ensure(ctx->device);
+    while ((int)ctx->dl_events.size() < n) {
+        cudaEvent_t e;
+        CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->dl_events.push_back(e);
+    }
+    // Pageable buffers go through pinned staging, which the workers copy out as soon as
+    // each picture's copies have landed; pinned (registered) buffers take the DMA directly.
+    std::vector<HostBuf> stage((size_t)n);
+    for (int i = 0; i < n; i++) {
+        const Layout& L = sts[i]->lay;
+        const size_t bytes = (size_t)L.W * L.H * 3 / 2;
+        cudaPointerAttributes a;
+        const bool pinned = cudaPointerGetAttributes(&a, outs[i]) == cudaSuccess && a.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        uint8_t* dst = outs[i];
+        if (!pinned) {
+            if ((rc = stage[(size_t)i].get(ctx, bytes))) return rc;
+            dst = static_cast<uint8_t*>(stage[(size_t)i].p);
+        }
+        if ((rc = download_i420(ctx, L, static_cast<uint8_t*>(sts[i]->slots[(size_t)slots[i]].p), dst))) return rc;
+        CUDA_TRY(cudaEventRecord(ctx->dl_events[(size_t)i], ctx->stream));
+    }
+    std::vector<int> rcs((size_t)n, 0);
+    ctx->pool.run(n, [&](int i) {
+        if (cudaEventSynchronize(ctx->dl_events[(size_t)i]) != cudaSuccess) {
+            rcs[(size_t)i] = HEVCGPU_ECUDA;
+            return;
+        }
+        if (stage[(size_t)i].p) {
+            const Layout& L = sts[i]->lay;
+            std::memcpy(outs[i], stage[(size_t)i].p, (size_t)L.W * L.H * 3 / 2);
+        }
+    });
+    for (int i = 0; i < n; i++)
+        if (rcs[(size_t)i]) return fail(HEVCGPU_ECUDA, "picture %d: download: %s", i, cudaGetErrorString(cudaGetLastError()));
+    return HEVCGPU_OK;
 }
 
 int hevcgpu_stream_sync(hevcgpu_stream_t* st) {

@@ -237,6 +237,25 @@ int  hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot);
  * reference another picture of the same batch) run as merged launches. */
 int  hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, int32_t n);
 int  hevcgpu_stream_sync(hevcgpu_stream_t* st);
+
+/* Batched host-side calls for a decoder that finishes several pictures at once (one per
+ * stream).  The work is spread over the context's host worker threads (one per
+ * hardware thread, started on first use).
+ *
+ * hevcgpu_jobs_prepare: hevcgpu_job_prepare of syns[i] on sts[i] for i < n (streams of
+ * one context).  On failure no job is returned (every out[i] is null) and the message
+ * names the first failing picture.
+ * hevcgpu_slots_download: slot slots[i] of sts[i] into the I420 host buffer outs[i].
+ * Pageable buffers are filled from pinned staging as each picture's copy lands; pinned
+ * buffers (cudaHostAlloc / cudaHostRegister) receive the copy directly.  Returns when
+ * every buffer is written.  Together with hevcgpu_batch_launch these serve, for a batch,
+ * what the reference's frame output hands to its caller per picture
+ * (Decoder::output_pictures, decoding/decoder.cpp:320; hevc_decoder_get_frame,
+ * wasm/hevc_api.cpp:49), as packed I420 host frames. */
+int  hevcgpu_jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns,
+                          int32_t n, hevcgpu_job_t** out);
+int  hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n,
+                            uint8_t* const* outs);
 /* CUDA stream (cudaStream_t) the context launches on. */
 void* hevcgpu_cuda_stream(hevcgpu_ctx_t* ctx);
 /* Number of kernel launches issued by this context so far. */

@@ -89,6 +89,43 @@ def test_dpb_jobs_plain_and_batched(hb, gpu_ctx, port):
         assert _diff(st.download(2), wnt) == 0
 
 
+def test_batched_prepare_and_download(hb, gpu_ctx, port):
+    """hevcgpu_jobs_prepare + hevcgpu_batch_launch + hevcgpu_slots_download over streams
+    of mixed sizes give the oracle's pictures into pageable and pinned host buffers; a
+    failing picture makes the whole preparation fail with no job returned."""
+    import torch
+    specs = [(416, 240, 81), (1280, 720, 82), (208, 120, 83), (640, 360, 84), (1920, 1080, 85)]
+    streams, pics, want = [], [], []
+    for (w, h, seed) in specs:
+        st = gpu_ctx.open_stream(w, h, 3)
+        refs = [hb.content(w, h, seed + 1), hb.content(w, h, seed + 2)]
+        st.upload(0, refs[0])
+        st.upload(1, refs[1])
+        pic = hb.Picture(hb.default_cfg(w, h, seed, **cases.PICTURE))
+        streams.append(st)
+        pics.append(pic)
+        want.append(port.reconstruct_picture(pic, refs))
+    for rep in range(2):
+        jobs = hb.prepare_batch(streams, pics)
+        hb.batch_launch(jobs, [2] * len(jobs))
+        if rep == 0:
+            outs = hb.download_batch(streams, [2] * len(streams))
+        else:   # pinned destinations take the copy directly
+            outs = [torch.empty(hb.i420_size(st.width, st.height), dtype=torch.uint8).pin_memory().numpy()
+                    for st in streams]
+            hb.download_batch(streams, [2] * len(streams), outs)
+        for got, wnt in zip(outs, want):
+            assert _diff(got, wnt) == 0
+        for j in jobs:
+            j.free()
+    bad = hb.Picture(hb.default_cfg(208, 120, 86, **cases.PICTURE))
+    bad.syn.tus[0].x = 4000
+    with pytest.raises(hb.HevcGpuError) as e:
+        hb.prepare_batch([streams[2], streams[0]], [bad, pics[0]])
+    assert e.value.code == hb.abi.HEVCGPU_EINVAL
+    assert "picture 0" in str(e.value)
+
+
 def test_picture_decode_end_to_end(hb, gpu_ctx, port):
     w, h = 640, 360
     st = gpu_ctx.open_stream(w, h, 3)
