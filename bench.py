@@ -14,9 +14,14 @@ the oracle before timing).
 
 value      frames/s over the whole job with the records already in HBM (device time, CUDA
            events on the library's stream, max over ranks).
-e2e        frames/s through the C ABI from host memory: per step each picture's records are
-           packed into pinned memory and copied host->device (hevcgpu_job_prepare), the
-           batch is launched, and every reconstructed picture is copied device->host.
+e2e        frames/s through the C ABI from host memory: per step the pictures' records are
+           packed into pinned memory on the library's host workers and copied host->device
+           (hevcgpu_jobs_prepare), the batch is launched (hevcgpu_batch_launch), and every
+           reconstructed picture is copied device->host into pageable host buffers
+           (hevcgpu_slots_download).
+stages     per-stage device times from CUDA events recorded around each stage on the
+           library's stream, in a separate pass of the same batched step (the timed region
+           itself carries no extra events).
 --impl reference runs privaloops/hevc.js's own reconstruction functions (oracle/_ref,
            compiled from the reference's sources) on all host cores for the same workload.
 """
@@ -376,6 +381,11 @@ def run_ours(args, hb, rank, world, local):
         per_stage[k] = {"ms_per_step": round(per_launch_ms, 4), "alg_bytes_per_step": alg_sum[k],
                         "GB/s": round(gbs, 1), "frac_of_hbm": round(gbs / peak, 4)}
     dom = max(stage_ms, key=lambda k: stage_ms[k])
+    # DRAM bytes (read + write) per launch of each stage's kernels, from one ncu capture of
+    # this workload at 16 pictures per launch (profiles/kernels_pb16_1080p.md); scaled by
+    # the pictures per launch when --batch differs (the traffic grows with the pictures).
+    ncu_dram_16 = {"mc": 130.38e6, "residual": 170.48e6, "intra": 54.13e6, "deblock": 123.83e6, "sao": 66.84e6}
+    traffic = ncu_dram_16[dom] * B / 16.0 if W == W_DEFAULT and H == H_DEFAULT else None
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -410,7 +420,9 @@ def run_ours(args, hb, rank, world, local):
                 "d2h_bytes_per_step": int(d2h_bytes)},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": per_stage[dom]["GB/s"], "peak": peak,
-                     "unit": "GB/s", "frac": per_stage[dom]["frac_of_hbm"], "traffic": None,
+                     "unit": "GB/s", "frac": per_stage[dom]["frac_of_hbm"],
+                     "traffic": None if traffic is None else int(traffic),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture",
                      "peak_source": peak_src},
         "stages": per_stage,
         "clocks": clk,
