@@ -20,7 +20,7 @@ SYNTH_SO = os.path.join(PKG, "libhevcsynth.so")
 GPU_SO = os.path.join(PKG, "libhevcgpu.so")
 
 GPU_SOURCES = ["hevcgpu.cu"]
-GPU_DEPS = ["hevcgpu.cu", "kernels.cuh", "device_common.cuh", "../../include/hevcgpu.h"]
+GPU_DEPS = ["hevcgpu.cu", "kernels.cuh", "mc.cuh", "intra.cuh", "device_common.cuh", "../../include/hevcgpu.h"]
 
 
 def _newer(target, deps):

@@ -885,9 +885,10 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
     }
     if (stages & ST_SAO) {
         StageMark m(ctx, 6);
-        rc = L.pictures(k_sao, jobs, n, 256, 3, [](hevcgpu_job* j) {
-            int groups = ((j->params.width + SAO_G - 1) / SAO_G) * j->params.height;  // luma: the most
-            return (groups + 255) / 256;
+        // one CTA per CTB; z = 0 luma, z = 1 both chroma planes
+        rc = L.pictures(k_sao, jobs, n, 256, 2, [](hevcgpu_job* j) {
+            const int ctb = 1 << j->params.log2_ctb;
+            return ((j->params.width + ctb - 1) / ctb) * ((j->params.height + ctb - 1) / ctb);
         });
         if (rc) return rc;
     }

@@ -463,106 +463,190 @@ __global__ void __launch_bounds__(256) k_deblock(const __grid_constant__ SegTabl
 // CTBs are at least 8 samples wide in every plane), reading the deblocked picture (rec)
 // with 8-byte loads and writing the DPB slot (dst); groups without SAO are copied.
 // ======================================================================================
-constexpr int SAO_G = 8;
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+    uint32_t d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(sel));
+    return d;
+}
 
-__device__ __forceinline__ int sign3(int d) { return (d > 0) - (d < 0); }
+// Bytes x+d .. x+d+7 of a row from its words at x-4, x, x+4, x+8 (d in -1..1).
+__device__ __forceinline__ void shifted_pair(uint32_t wm, uint32_t w0, uint32_t w1, uint32_t w2, int d,
+                                             uint32_t& s0, uint32_t& s1) {
+    if (d > 0) {
+        s0 = __funnelshift_r(w0, w1, 8);
+        s1 = __funnelshift_r(w1, w2, 8);
+    } else {
+        s0 = __funnelshift_rc(wm, w0, 32 + 8 * d);
+        s1 = __funnelshift_rc(w0, w1, 32 + 8 * d);
+    }
+}
 
+// SAO arithmetic on 16-bit lanes: two samples per 32-bit word, biased so that no lane
+// borrows from its neighbour.  For a word of 4 samples c (and neighbours a, b), the even
+// samples go to lanes as lo16(c0) | c2 << 16 and the odd ones as c1 | c3 << 16.
+__device__ __forceinline__ uint32_t lanes_even(uint32_t w) { return prmt(w, 0u, 0x4240u); }
+__device__ __forceinline__ uint32_t lanes_odd(uint32_t w) { return prmt(w, 0u, 0x4341u); }
+// Offset-table selector for two lanes holding indices 0..5: nibbles [i0, 5, i1, 5] pick
+// table byte i and the zero byte 5 as the lane's upper half.
+__device__ __forceinline__ uint32_t lane_sel(uint32_t idx) { return prmt(idx + 0x00500050u, 0u, 0x4420u); }
+// c + table offset (bytes of the table are offset + 8), clipped to 0..255, in lanes biased
+// by 256; the low byte of each lane is the result.
+__device__ __forceinline__ uint32_t lane_apply(uint32_t c, uint32_t tlo, uint32_t thi, uint32_t idx) {
+    const uint32_t r = c + prmt(tlo, thi, lane_sel(idx)) + 0x00F800F8u;
+    return __vmins2(__vmaxs2(r, 0x01000100u), 0x01FF01FFu);
+}
+// Edge index 2 + sign(c - a) + sign(c - b) per lane.
+__device__ __forceinline__ uint32_t lane_edge(uint32_t c, uint32_t a, uint32_t b) {
+    const uint32_t sa = __vmins2(__vmaxs2(c + 0x01000100u - a, 0x00FF00FFu), 0x01010101u);
+    const uint32_t sb = __vmins2(__vmaxs2(c + 0x01000100u - b, 0x00FF00FFu), 0x01010101u);
+    return sa + sb - 0x01FE01FEu;
+}
+// Band index (c >> 3) - band_position per lane, or 4 outside the four bands (no
+// wrap-around, sao.cpp:229-230): (c >> 3) + 256 - pos keeps lanes apart, its low byte is
+// the difference mod 256, and an unsigned min with 4 maps everything else to 4.
+__device__ __forceinline__ uint32_t lane_band(uint32_t c, uint32_t k256) {
+    return __vminu2(((c >> 3) + k256) & 0x00FF00FFu, 0x00040004u);
+}
+__device__ __forceinline__ uint32_t lanes_join(uint32_t even, uint32_t odd) { return prmt(even, odd, 0x6240u); }
+
+// SAO of one CTB and plane per group of threads (apply_sao, sao.cpp:20-243): grid
+// (CTB, picture, z) with z = 0 for luma (256 threads) and z = 1 for both chroma planes
+// (128 threads each).  A thread takes 8 samples of a row, rows strided over the CTB.  The
+// CTB's parameters are read once; samples are classified and offset branch-free on
+// 16-bit lanes (edge offset: signs by clamping biased differences; band offset: band
+// index by an unsigned min), the offset picked with one prmt from the five offset bytes.
+// Samples the reference leaves unchanged — neighbour outside the picture, across a slice
+// or tile boundary that filtering may not cross, PCM with pcm_loop_filter_disabled,
+// transquant bypass — get their deblocked value back.  Reads the deblocked buffer (rec),
+// writes the DPB slot (dst), so no full-picture copy is made.
 __global__ void __launch_bounds__(256) k_sao(const __grid_constant__ SegTable st) {
     const PicDesc& P = *st.s[blockIdx.y].pic;
-    const int ci = blockIdx.z;
+    const int ctb = blockIdx.x;
+    if (ctb >= P.wctb * P.hctb) return;
+    const int ci = blockIdx.z == 0 ? 0 : 1 + (threadIdx.x >> 7);
+    const int T = blockIdx.z == 0 ? 256 : 128;
+    const int t = blockIdx.z == 0 ? threadIdx.x : (threadIdx.x & 127);
     const int sub = ci ? 2 : 1;
+    const int log2c = P.log2_ctb - (sub - 1);
+    const int cs = 1 << log2c;
     const int pw = P.width / sub, ph = P.height / sub;
-    const int groups = (pw + SAO_G - 1) / SAO_G;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = tid / groups, x = (tid % groups) * SAO_G;
-    if (y >= ph) return;
-    const int n = min(SAO_G, pw - x);  // 8, or 4 at the end of a row
+    const int cx = (ctb % P.wctb) << log2c, cy = (ctb / P.wctb) << log2c;
+    const int G = cs >> 3;                 // 8-sample groups per CTB row (2..8)
+    const int x = cx + (t % G) * 8;
+    const int rstep = T / G;
     const int pitch = ci ? P.pitch_c : P.pitch_y;
     const int64_t base = ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr);
     const uint8_t* S = P.rec + base;
     uint8_t* D = P.dst + base;
-    const int64_t at = (int64_t)y * pitch + x;
-    // x is a multiple of 8 and pitches of 64: 8-byte aligned (a 4-byte tail reads 4 more
-    // bytes of the row padding, which are not used)
-    const uint2 c8 = __ldg(reinterpret_cast<const uint2*>(S + at));
-    const int log2c = P.log2_ctb - (sub - 1);
-    const int addr = (y >> log2c) * P.wctb + (x >> log2c);
-    const int type = P.sao_enabled ? P.sao[addr].type[ci] : 0;
-    uint32_t o[2] = {c8.x, c8.y};
-    if (type != 0) {
-        const hevc_sao_t& sp = P.sao[addr];
-        // the five offsets as bytes of one word pair (index k -> byte k), sign-extended on use
-        uint64_t offs = 0;
-#pragma unroll
-        for (int k = 0; k < 5; k++) offs |= (uint64_t)(uint8_t)sp.offset[ci][k] << (8 * k);
-        auto off = [&](int k) { return (int)(int8_t)(offs >> (8 * k)); };
-        const int cl = sp.eo_class[ci], band = sp.band_pos[ci];
-        const int dx0 = cl == 1 ? 0 : (cl == 3 ? 1 : -1), dy0 = cl == 0 ? 0 : -1;
-        const int dx1 = -dx0, dy1 = -dy0;
-        // edge offset: samples x-1 .. x+8 of the two neighbour rows, byte i+1 of nb[k]
-        uint32_t nb[2][3] = {{0, 0, 0}, {0, 0, 0}};
-        bool row_ok[2] = {false, false};
-        if (type == 2) {
-#pragma unroll
-            for (int k = 0; k < 2; k++) {
-                const int yy = y + (k ? dy1 : dy0);
-                row_ok[k] = yy >= 0 && yy < ph;
-                if (!row_ok[k]) continue;
-                const uint8_t* row = S + (int64_t)yy * pitch + x;
-                const uint2 m = yy == y ? c8 : __ldg(reinterpret_cast<const uint2*>(row));
-                const uint32_t lo = x >= 4 ? __ldg(reinterpret_cast<const uint32_t*>(row) - 1) : 0u;
-                const uint32_t hi = x + 8 < pw ? __ldg(reinterpret_cast<const uint32_t*>(row) + 2) : 0u;
-                nb[k][0] = (lo >> 24) | (m.x << 8);
-                nb[k][1] = (m.x >> 24) | (m.y << 8);
-                nb[k][2] = (m.y >> 24) | ((hi & 0xFFu) << 8);
-            }
+    if (x >= pw) return;
+    const int n = min(8, pw - x);          // 8, or 4 at the end of a row
+    const int ymax = min(cy + cs, ph);
+
+    const int type = P.sao_enabled ? P.sao[ctb].type[ci] : 0;
+    if (type == 0) {
+        for (int y = cy + t / G; y < ymax; y += rstep) {
+            const int64_t at = (int64_t)y * pitch + x;
+            const uint2 c8 = __ldg(reinterpret_cast<const uint2*>(S + at));
+            if (n == 8) *reinterpret_cast<uint2*>(D + at) = c8;
+            else *reinterpret_cast<uint32_t*>(D + at) = c8.x;
         }
-        const int gw = P.width >> 2;
-        const bool check_slices = P.slice_check || P.tiles_check;
+        return;
+    }
+    const hevc_sao_t& sp = P.sao[ctb];
+    // offset table: byte k = offset k + 8 (k = 0..4), byte 5 = 0 (the lanes' upper halves)
+    uint32_t tlo = 0;
 #pragma unroll
-        for (int i = 0; i < SAO_G; i++) {
-            if (i >= n) break;
-            const int xs = x + i;
-            if (P.pcm_bypass_any) {
-                const uint32_t b = P.blk[(int64_t)((y * sub) >> 2) * gw + ((xs * sub) >> 2)];
-                if ((P.pcm_lf_disabled && (b & HEVC_BLK_PCM)) || (b & HEVC_BLK_BYPASS)) continue;
+    for (int k = 0; k < 4; k++) tlo |= (uint32_t)(uint8_t)(sp.offset[ci][k] + 8) << (8 * k);
+    const uint32_t thi = type == 2 ? (uint32_t)(uint8_t)(sp.offset[ci][4] + 8) : 8u;
+    const int cl = sp.eo_class[ci];
+    const int dx = type == 2 ? (cl == 1 ? 0 : (cl == 3 ? 1 : -1)) : 0;   // a at (x+dx, y+dy), b opposite
+    const int dy = type == 2 ? (cl == 0 ? 0 : -1) : 0;
+    const uint32_t k256 = (uint32_t)(256 - sp.band_pos[ci]) * 0x00010001u;
+    const bool check_slices = type == 2 && (P.slice_check || P.tiles_check);
+
+    for (int y = cy + t / G; y < ymax; y += rstep) {
+        const int64_t at = (int64_t)y * pitch + x;
+        const uint2 c8 = __ldg(reinterpret_cast<const uint2*>(S + at));
+        uint32_t o0 = c8.x, o1 = c8.y;
+        bool apply = true;
+        if (type == 2) {
+            apply = y + dy >= 0 && y - dy < ph;
+            if (apply) {
+                uint32_t nw[2][2];
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    const int yy = y + (k ? -dy : dy);
+                    const uint8_t* row = S + (int64_t)yy * pitch + x;
+                    const uint2 m = yy == y ? c8 : __ldg(reinterpret_cast<const uint2*>(row));
+                    const uint32_t wm = x >= 4 ? __ldg(reinterpret_cast<const uint32_t*>(row) - 1) : 0u;
+                    const uint32_t w2 = x + 8 < pw ? __ldg(reinterpret_cast<const uint32_t*>(row) + 2) : 0u;
+                    shifted_pair(wm, m.x, m.y, w2, k ? -dx : dx, nw[k][0], nw[k][1]);
+                }
+                o0 = lanes_join(lane_apply(lanes_even(c8.x), tlo, thi,
+                                           lane_edge(lanes_even(c8.x), lanes_even(nw[0][0]), lanes_even(nw[1][0]))),
+                                lane_apply(lanes_odd(c8.x), tlo, thi,
+                                           lane_edge(lanes_odd(c8.x), lanes_odd(nw[0][0]), lanes_odd(nw[1][0]))));
+                o1 = lanes_join(lane_apply(lanes_even(c8.y), tlo, thi,
+                                           lane_edge(lanes_even(c8.y), lanes_even(nw[0][1]), lanes_even(nw[1][1]))),
+                                lane_apply(lanes_odd(c8.y), tlo, thi,
+                                           lane_edge(lanes_odd(c8.y), lanes_odd(nw[0][1]), lanes_odd(nw[1][1]))));
             }
-            const int c = (o[i >> 2] >> (8 * (i & 3))) & 0xFF;
-            int v;
-            if (type == 2) {
-                const int ax = xs + dx0, bx = xs + dx1;
-                if (!row_ok[0] || !row_ok[1] || ax < 0 || ax >= pw || bx < 0 || bx >= pw) continue;
-                if (check_slices) {
-                    bool skip = false;
-                    const int ay = y + dy0, by = y + dy1;
+        } else {
+            o0 = lanes_join(lane_apply(lanes_even(c8.x), tlo, thi, lane_band(lanes_even(c8.x), k256)),
+                            lane_apply(lanes_odd(c8.x), tlo, thi, lane_band(lanes_odd(c8.x), k256)));
+            o1 = lanes_join(lane_apply(lanes_even(c8.y), tlo, thi, lane_band(lanes_even(c8.y), k256)),
+                            lane_apply(lanes_odd(c8.y), tlo, thi, lane_band(lanes_odd(c8.y), k256)));
+        }
+        if (apply) {
+            // samples that keep their deblocked value
+            uint32_t keep = 0;
+            if (dx != 0) {
+                if (x == 0) keep |= 1u;
+                if (x + n >= pw) keep |= 1u << (n - 1);
+            }
+            if (P.pcm_bypass_any || check_slices) {
+                const int gw = P.width >> 2;
+                for (int i = 0; i < n; i++) {
+                    const int xs = x + i;
+                    if (P.pcm_bypass_any) {
+                        const uint32_t b = P.blk[(int64_t)((y * sub) >> 2) * gw + ((xs * sub) >> 2)];
+                        if ((P.pcm_lf_disabled && (b & HEVC_BLK_PCM)) || (b & HEVC_BLK_BYPASS)) {
+                            keep |= 1u << i;
+                            continue;
+                        }
+                    }
+                    if (!check_slices) continue;
                     const int cur = ((y * sub) >> P.log2_ctb) * P.wctb + ((xs * sub) >> P.log2_ctb);
-                    for (int nk = 0; nk < 2 && !skip; nk++) {
-                        const int nx = nk ? bx : ax, ny = nk ? by : ay;
+                    for (int nk = 0; nk < 2; nk++) {
+                        const int nx = xs + (nk ? -dx : dx), ny = y + (nk ? -dy : dy);
+                        if (nx < 0 || nx >= pw) continue;   // kept above
                         const int na = ((ny * sub) >> P.log2_ctb) * P.wctb + ((nx * sub) >> P.log2_ctb);
                         const int sc = P.ctb_slice ? P.ctb_slice[cur] : 0, sn = P.ctb_slice ? P.ctb_slice[na] : 0;
-                        if (sc != sn && !slice_at(P, sn < sc ? cur : na).lf_across_slices) skip = true;
-                        if (!skip && P.tiles_check && P.ctb_tile && P.ctb_tile[cur] != P.ctb_tile[na]) skip = true;
+                        if ((sc != sn && !slice_at(P, sn < sc ? cur : na).lf_across_slices) ||
+                            (P.tiles_check && P.ctb_tile && P.ctb_tile[cur] != P.ctb_tile[na])) {
+                            keep |= 1u << i;
+                            break;
+                        }
                     }
-                    if (skip) continue;
                 }
-                // neighbour at column offset d (-1..1) of sample i: byte i + d + 1 of row k
-                auto nbyte = [&](int k, int q) {
-                    const uint32_t w = q < 4 ? nb[k][0] : (q < 8 ? nb[k][1] : nb[k][2]);
-                    return (int)((w >> (8 * (q & 3))) & 0xFFu);
-                };
-                const int a = nbyte(0, i + dx0 + 1), bb = nbyte(1, i + dx1 + 1);
-                const int e = 2 + sign3(c - a) + sign3(c - bb);
-                v = c + off(e);
-            } else {
-                const int k = (c >> 3) - band;  // no wrap-around (sao.cpp:229-230)
-                if (k < 0 || k >= 4) continue;
-                v = c + off(k);
             }
-            o[i >> 2] = (o[i >> 2] & ~(0xFFu << (8 * (i & 3)))) | ((uint32_t)clip_u8(v) << (8 * (i & 3)));
+            if (keep) {
+                uint32_t m0 = 0, m1 = 0;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    m0 |= ((keep >> i) & 1u) * (0xFFu << (8 * i));
+                    m1 |= ((keep >> (i + 4)) & 1u) * (0xFFu << (8 * i));
+                }
+                o0 = (c8.x & m0) | (o0 & ~m0);
+                o1 = (c8.y & m1) | (o1 & ~m1);
+            }
+        } else {
+            o0 = c8.x;
+            o1 = c8.y;
         }
+        if (n == 8) *reinterpret_cast<uint2*>(D + at) = make_uint2(o0, o1);
+        else *reinterpret_cast<uint32_t*>(D + at) = o0;
     }
-    if (n == SAO_G) *reinterpret_cast<uint2*>(D + at) = make_uint2(o[0], o[1]);
-    else *reinterpret_cast<uint32_t*>(D + at) = o[0];
 }
 
 }  // namespace hevcgpu
