@@ -64,7 +64,7 @@ struct PicDesc {
 };
 
 // Work items ----------------------------------------------------------------------------
-// Residual items are TU indices (int32); motion-compensation items are McStrip (mc.cuh).
+// Residual items are TU indices (int32); motion-compensation items are McBlock (mc.cuh).
 
 // A launch covers up to MAX_SEGS pictures.  Segment k owns the blocks
 // [block0, next block0) of an item-list launch, or blockIdx.y == k of a per-picture

@@ -335,8 +335,8 @@ struct hevcgpu_job {
     PicDesc host_desc{};
     int32_t n_res[4] = {0, 0, 0, 0};
     const int32_t* d_res[4] = {nullptr, nullptr, nullptr, nullptr};
-    int32_t n_mc[2] = {0, 0};            // luma strips, chroma strips
-    const McStrip* d_mc[2] = {nullptr, nullptr};
+    int32_t n_mc[2] = {0, 0};            // luma blocks, chroma blocks
+    const McBlock* d_mc[2] = {nullptr, nullptr};
     int32_t n_ictu = 0;                 // CTUs that hold intra TUs
     int32_t epoch = 0;                  // intra launches of this job so far
     int32_t n_pus = 0;
@@ -560,36 +560,40 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         }
     }
     j->n_ictu = (int32_t)ictu_addr.size();
-    // MC strips: 4 columns x up to 16 rows; luma and chroma (Cb and Cr together) are two
-    // lists.  Each list is ordered bi- before uni-predicted PUs, then by strip height, so
-    // that the threads of a warp take the same path for the same number of rows.
-    std::vector<McStrip> mc[2];
+    // MC blocks: up to 16 x 16 luma / 8 x 8 chroma of one PU, one warp each; luma and
+    // chroma (Cb and Cr together) are two lists, each ordered bi- before uni-predicted
+    // PUs, then by block area (larger first), so that the warps of a CTA finish together.
+    std::vector<McBlock> mc[2];
     if (stages & ST_MC) {
-        // counting sort on the key (bi ? 0 : 16) + (16 - strip height), stable in PU order
+        // counting sort on the key (bi ? 0 : 32) + (31 - (area - 1) / 8), stable in PU order
         for (int c = 0; c < 2; c++) {
-            int32_t cnt[33] = {};
-            auto each_strip = [&](auto&& emit) {
+            const int B = c ? MC_BLOCK_CHROMA : MC_BLOCK_LUMA, area_shift = c ? 1 : 3;
+            int32_t cnt[65] = {};
+            auto each_block = [&](auto&& emit) {
                 for (int i = 0; i < s->num_pus; i++) {
                     const hevc_pu_t& u = s->pus[i];
-                    const int key0 = (u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0) ? 0 : 16;
+                    const int key0 = (u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0) ? 0 : 32;
                     const int w = c ? u.w / 2 : u.w, h = c ? u.h / 2 : u.h;
-                    for (int sy = 0; sy < h; sy += 16) {
-                        const int sh = std::min(16, h - sy);
-                        for (int sx = 0; sx < w; sx += 4) emit(key0 + 16 - sh, i, sx, sy, sh);
+                    for (int by = 0; by < h; by += B) {
+                        const int bh = std::min(B, h - by);
+                        for (int bx = 0; bx < w; bx += B) {
+                            const int bw = std::min(B, w - bx);
+                            emit(key0 + 31 - std::min(31, (bw * bh - 1) >> area_shift), i, bx, by, bw, bh);
+                        }
                     }
                 }
             };
-            each_strip([&](int key, int, int, int, int) { cnt[key + 1]++; });
-            for (int k = 1; k <= 32; k++) cnt[k] += cnt[k - 1];
-            mc[c].resize((size_t)cnt[32]);
-            McStrip* out = mc[c].data();
-            each_strip([&](int key, int i, int sx, int sy, int sh) {
-                McStrip& m = out[cnt[key]++];
+            each_block([&](int key, int, int, int, int, int) { cnt[key + 1]++; });
+            for (int k = 1; k <= 64; k++) cnt[k] += cnt[k - 1];
+            mc[c].resize((size_t)cnt[64]);
+            McBlock* out = mc[c].data();
+            each_block([&](int key, int i, int bx, int by, int bw, int bh) {
+                McBlock& m = out[cnt[key]++];
                 m.pu = i;
-                m.sx = (uint8_t)sx;
-                m.sy = (uint8_t)sy;
-                m.h = (uint8_t)sh;
-                m.pad = 0;
+                m.bx = (uint8_t)bx;
+                m.by = (uint8_t)by;
+                m.bw = (uint8_t)bw;
+                m.bh = (uint8_t)bh;
             });
         }
     }
@@ -610,7 +614,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         o_slices = s->num_slices > 0 && s->slices ? pk.add(s->slices, sizeof(hevc_slice_t) * (size_t)s->num_slices)
                                                   : pk.add(&dflt, sizeof(dflt));
         for (int k = 0; k < 4; k++) o_res[k] = pk.add(bins[k].data(), sizeof(int32_t) * bins[k].size());
-        for (int c = 0; c < 2; c++) o_mc[c] = pk.add(mc[c].data(), sizeof(McStrip) * mc[c].size());
+        for (int c = 0; c < 2; c++) o_mc[c] = pk.add(mc[c].data(), sizeof(McBlock) * mc[c].size());
         o_ia = pk.add(ictu_addr.data(), sizeof(int32_t) * ictu_addr.size());
         o_idp = pk.add(ictu_deps.data(), sizeof(int32_t) * ictu_deps.size());
         o_ito = pk.add(ictu_tu_off.data(), sizeof(int32_t) * ictu_tu_off.size());
@@ -700,7 +704,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     }
     for (int c = 0; c < 2; c++) {
         j->n_mc[c] = (int32_t)mc[c].size();
-        j->d_mc[c] = reinterpret_cast<const McStrip*>(base + o_mc[c]);
+        j->d_mc[c] = reinterpret_cast<const McBlock*>(base + o_mc[c]);
     }
     return HEVCGPU_OK;
 }
@@ -817,12 +821,12 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
     }
     if (stages & ST_MC) {
         StageMark m(ctx, 1);
-        rc = L.items(k_mc<false>, jobs, n, MC_THREADS, MC_THREADS, [](hevcgpu_job* j, const void*& p, int& c) {
+        rc = L.items(k_mc<false>, jobs, n, MC_WARPS, MC_WARPS * 32, [](hevcgpu_job* j, const void*& p, int& c) {
             p = j->d_mc[0];
             c = j->n_mc[0];
         });
         if (rc) return rc;
-        rc = L.items(k_mc<true>, jobs, n, MC_THREADS, MC_THREADS, [](hevcgpu_job* j, const void*& p, int& c) {
+        rc = L.items(k_mc<true>, jobs, n, MC_WARPS, MC_WARPS * 32, [](hevcgpu_job* j, const void*& p, int& c) {
             p = j->d_mc[1];
             c = j->n_mc[1];
         });
