@@ -20,6 +20,14 @@ struct MotionEnt {           // 4x4 motion grid entry (PUMotionInfo, inter_predi
     int16_t pad;
 };
 
+// One level of an intra CTU task: req[d] > 0 means "dependency slot d must have completed
+// req[d] levels before this level runs" (only where the requirement rises); bit 15 of
+// req[0] (INTRA_LEVEL_PUBLISH) means other CTUs wait for this level's completion.
+struct IntraLevel {
+    uint16_t req[4];
+};
+constexpr uint16_t INTRA_LEVEL_PUBLISH = 0x8000u;
+
 struct PicDesc {
     int32_t width, height;               // luma
     int32_t pitch_y, pitch_c;
@@ -48,7 +56,9 @@ struct PicDesc {
     const int32_t* itu;                  // TU index
     const int32_t* itu_level_end;        // first entry of the next level of the same CTU
     const int32_t* itu_res_off;          // residual offset inside the CTU's staged residuals
-    int32_t* ictu_done;                  // per intra CTU: epoch of its last completion
+    const int32_t* ictu_lvl_off;         // levels of intra CTU k: ictu_lvl[ictu_lvl_off[k] ..]
+    const IntraLevel* ictu_lvl;
+    int32_t* ictu_done;                  // per intra CTU: (epoch << 16) | levels completed
     int32_t n_ictu;
     int32_t num_pus;
     int32_t num_slices;

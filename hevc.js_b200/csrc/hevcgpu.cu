@@ -467,10 +467,16 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     // for that CTU.  A unit whose samples B may not use (availability) can only add an
     // unneeded level or wait, never change a sample.
     const int n_intra = (int)intra_list.size();
-    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, itu, itu_level_end, itu_res_off;
+    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, itu, itu_level_end, itu_res_off, ictu_lvl_off;
+    std::vector<IntraLevel> ictu_lvl;
     if (n_intra) {
         std::vector<int32_t> level((size_t)n_intra, 0), ctu_of((size_t)n_intra, 0);
         std::vector<std::vector<int32_t>> ctu_deps((size_t)nctb);  // by CTU address
+        // cross-CTU requirements: (CTU, level, dependency CTU address, levels it must have done)
+        struct Req { int32_t a, lv, dep, need; };
+        std::vector<Req> reqs;
+        std::vector<std::pair<int32_t, int32_t>> pending;           // (dep CTU, need) of one TU
+        std::vector<std::vector<uint8_t>> publish((size_t)nctb);     // by CTU address and level
         std::vector<int32_t> owner[3];
         int uw[3], uh[3];
         for (int c = 0; c < 3; c++) {
@@ -494,6 +500,10 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
                 } else {
                     std::vector<int32_t>& dl = ctu_deps[(size_t)a];
                     if (std::find(dl.begin(), dl.end(), oa) == dl.end()) dl.push_back(oa);
+                    pending.emplace_back(oa, level[(size_t)o] + 1);
+                    std::vector<uint8_t>& pb = publish[(size_t)oa];
+                    if (pb.size() <= (size_t)level[(size_t)o]) pb.resize((size_t)level[(size_t)o] + 1, 0);
+                    pb[(size_t)level[(size_t)o]] = 1;
                 }
             };
             if (t.y > 0) {
@@ -507,6 +517,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
                 for (int uy = uy0; uy <= uy1; uy++) dep(ux, uy);
             }
             level[(size_t)b] = lv;
+            for (const auto& pd : pending) reqs.push_back({a, lv, pd.first, pd.second});
+            pending.clear();
             for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++)
                 for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) own[(size_t)uy * uw[c] + ux] = b;
         }
@@ -558,6 +570,36 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             if (dl.size() > 4) return fail(HEVCGPU_EINVAL, "CTU %d depends on %zu CTUs", ictu_addr[(size_t)k], dl.size());
             for (size_t q = 0; q < dl.size(); q++) ictu_deps[(size_t)k * 4 + q] = index_of[(size_t)dl[q]];
         }
+        // per CTU level: the levels each dependency slot must have completed before it runs
+        // (only where the requirement rises) and whether dependents wait for its completion
+        ictu_lvl_off.resize((size_t)nic + 1);
+        std::vector<int32_t> nlev((size_t)nic, 0);
+        for (int k = 0; k < nic; k++) {
+            const int last = ictu_tu_off[(size_t)k + 1] - 1;
+            nlev[(size_t)k] = level[(size_t)order[(size_t)last]] + 1;
+            ictu_lvl_off[(size_t)k] = k ? ictu_lvl_off[(size_t)k - 1] + nlev[(size_t)k - 1] : 0;
+        }
+        ictu_lvl_off[(size_t)nic] = nic ? ictu_lvl_off[(size_t)nic - 1] + nlev[(size_t)nic - 1] : 0;
+        ictu_lvl.assign((size_t)ictu_lvl_off[(size_t)nic], IntraLevel{{0, 0, 0, 0}});
+        for (const Req& r : reqs) {
+            const int k = index_of[(size_t)r.a];
+            const std::vector<int32_t>& dl = ctu_deps[(size_t)r.a];
+            const int slot = (int)(std::find(dl.begin(), dl.end(), r.dep) - dl.begin());
+            uint16_t& q = ictu_lvl[(size_t)(ictu_lvl_off[(size_t)k] + r.lv)].req[slot];
+            q = (uint16_t)std::max<int>(q, r.need);
+        }
+        for (int k = 0; k < nic; k++) {
+            uint16_t seen[4] = {0, 0, 0, 0};
+            const std::vector<uint8_t>& pb = publish[(size_t)ictu_addr[(size_t)k]];
+            for (int L = 0; L < nlev[(size_t)k]; L++) {
+                IntraLevel& e = ictu_lvl[(size_t)(ictu_lvl_off[(size_t)k] + L)];
+                for (int q = 0; q < 4; q++) {
+                    if (e.req[q] > seen[q]) seen[q] = e.req[q];
+                    else e.req[q] = 0;   // already satisfied by an earlier check
+                }
+                if ((size_t)L < pb.size() && pb[(size_t)L]) e.req[0] |= INTRA_LEVEL_PUBLISH;
+            }
+        }
     }
     j->n_ictu = (int32_t)ictu_addr.size();
     // MC blocks: up to 16 x 16 luma / 8 x 8 chroma of one PU, one warp each; luma and
@@ -600,7 +642,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     j->n_pus = s->num_pus;
 
     size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc[2], o_ia, o_idp, o_ito,
-        o_itu, o_ile, o_iro;
+        o_itu, o_ile, o_iro, o_ilo, o_ilv;
     hevc_slice_t dflt{0, 0, 0, 1};
     auto pack = [&](Packer& pk) {
         o_tus = pk.add(s->tus, sizeof(hevc_tu_t) * (size_t)std::max(0, s->num_tus));
@@ -621,6 +663,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         o_itu = pk.add(itu.data(), sizeof(int32_t) * itu.size());
         o_ile = pk.add(itu_level_end.data(), sizeof(int32_t) * itu_level_end.size());
         o_iro = pk.add(itu_res_off.data(), sizeof(int32_t) * itu_res_off.size());
+        o_ilo = pk.add(ictu_lvl_off.data(), sizeof(int32_t) * ictu_lvl_off.size());
+        o_ilv = pk.add(ictu_lvl.data(), sizeof(IntraLevel) * ictu_lvl.size());
     };
     Packer measure;
     pack(measure);
@@ -673,6 +717,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     D.itu = reinterpret_cast<const int32_t*>(base + o_itu);
     D.itu_level_end = reinterpret_cast<const int32_t*>(base + o_ile);
     D.itu_res_off = reinterpret_cast<const int32_t*>(base + o_iro);
+    D.ictu_lvl_off = reinterpret_cast<const int32_t*>(base + o_ilo);
+    D.ictu_lvl = reinterpret_cast<const IntraLevel*>(base + o_ilv);
     D.ictu_done = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(j->scratch.p) + resid_bytes + mot_bytes);
     D.n_ictu = (int32_t)ictu_addr.size();
     // completion flags start below every epoch a launch can use
@@ -860,6 +906,13 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
                 Seg& sg = t.s[t.n++];
                 sg.pic = static_cast<const PicDesc*>(j->desc.p);
                 sg.aux0 = total;
+                // completion words are (epoch << 16) | levels; restart the epochs from zero
+                // flags before they would reach the sign bit
+                if (j->epoch >= 32767) {
+                    CUDA_TRY(cudaMemsetAsync(j->host_desc.ictu_done, 0, sizeof(int32_t) * (size_t)j->n_ictu,
+                                             ctx->stream));
+                    j->epoch = 0;
+                }
                 sg.aux1 = ++j->epoch;
                 total += j->n_ictu;
             }

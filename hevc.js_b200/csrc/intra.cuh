@@ -230,12 +230,15 @@ __device__ __forceinline__ void intra_tu_any(const PicDesc& P, const hevc_tu_t& 
 
 // ---------------------------------------------------------------------------------------
 // CTU tasks.  One CTA per CTU that holds intra TUs.  CTAs take CTUs by ticket in raster
-// order, picture after picture; a CTU waits (bounded) for the at most four earlier intra
-// CTUs whose intra samples it reads (left, above-left, above, above-right, found on the
-// host), so every wait is for a CTA that already runs.  The CTA then stages the CTU and
-// its neighbourhood, its TU records and their residuals in shared memory, runs the TUs
-// level by level of the CTU-local dependency DAG (one warp per TU, a barrier between
-// levels) and publishes its completion with the launch's epoch.
+// order, picture after picture.  The CTA stages the CTU and its neighbourhood, its TU
+// records and their residuals in shared memory, then runs the TUs level by level of the
+// CTU-local dependency DAG (one warp per TU, a barrier between levels).  Dependencies on
+// the at most four earlier intra CTUs whose intra samples it reads (left, above-left,
+// above, above-right, found on the host) are per level: before a level the CTA waits
+// (bounded) until each such CTU has completed the levels that own those samples, so a
+// CTU starts while its neighbours are still running and the critical path is the TU
+// dependency chain, not a chain of whole CTUs.  Every wait is for a CTU with an earlier
+// ticket, which already holds a running CTA.
 // ---------------------------------------------------------------------------------------
 constexpr int IC_WARPS = 4;
 constexpr int IC_THREADS = 32 * IC_WARPS;
@@ -267,6 +270,24 @@ __device__ __forceinline__ void stage_tile(const PicDesc& P, int c, int rx, int 
     }
 }
 
+// Re-copy the parts of the tile that other CTUs write: row -1 and the IC_MARGIN columns
+// left of the CTU (the first chunk of each row).
+__device__ __forceinline__ void stage_margin(const PicDesc& P, int c, int rx, int ry, uint8_t* tile, int tid) {
+    const int sub = c ? 2 : 1, ctbc = (1 << P.log2_ctb) / sub;
+    const int pw = P.width / sub, ph = P.height / sub, pitch = c ? P.pitch_c : P.pitch_y;
+    const uint8_t* plane = P.rec + (c == 0 ? 0 : (c == 1 ? P.off_cb : P.off_cr));
+    const int tp = c ? IC_CP : IC_LP;
+    const int x0 = rx * ctbc - IC_MARGIN, y0 = ry * ctbc - 1;
+    const int top_chunks = (IC_MARGIN + 2 * ctbc + 15) / 16;
+    for (int e = tid; e < top_chunks + ctbc; e += IC_THREADS) {
+        const int r = e < top_chunks ? 0 : 1 + (e - top_chunks), q = e < top_chunks ? e : 0;
+        const int y = y0 + r, x = x0 + 16 * q;
+        if (y < 0 || y >= ph || x < 0 || x >= pw) continue;
+        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(plane + (int64_t)y * pitch + x));
+        *reinterpret_cast<uint4*>(tile + r * tp + 16 * q) = v;
+    }
+}
+
 __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant__ SegTable st, int32_t* ticket,
                                                            int total, uint32_t* sticky) {
     __shared__ __align__(16) uint8_t t_luma[IC_LH * IC_LP];
@@ -291,22 +312,6 @@ __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant
     const int idx = t - st.s[k].aux0;
     const int a = P.ictu_addr[idx], rx = a % P.wctb, ry = a / P.wctb;
 
-    // wait for the intra CTUs this one reads from (one thread per dependency)
-    if (tid < 4) {
-        const int d = P.ictu_deps[4 * idx + tid];
-        if (d >= 0) {
-            cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[d]);
-            long long polls = 0;
-            while (done.load(cuda::memory_order_acquire) != epoch) {
-                if (++polls > SPIN_LIMIT) {
-                    atomicOr(sticky, ST_TIMEOUT);
-                    s_abort = 1;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-    }
     if (tid == 4) {  // which neighbour CTBs share this CTB's slice and tile
         const int sl = P.ctb_slice ? P.ctb_slice[a] : 0, ti = P.ctb_tile ? P.ctb_tile[a] : 0;
         auto same = [&](int nx, int ny) {
@@ -317,8 +322,6 @@ __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant
         s_nb = (same(rx - 1, ry) ? NB_LEFT : 0u) | (same(rx - 1, ry - 1) ? NB_ABOVE_LEFT : 0u) |
                (same(rx, ry - 1) ? NB_ABOVE : 0u) | (same(rx + 1, ry - 1) ? NB_ABOVE_RIGHT : 0u);
     }
-    __syncthreads();
-    if (s_abort) return;
 
     // stage the neighbourhood and the TU records
     const int off = P.ictu_tu_off[idx], n_tu = P.ictu_tu_off[idx + 1] - off;
@@ -340,8 +343,41 @@ __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant
 
     const int ctbl = 1 << P.log2_ctb;
     const uint32_t nb = s_nb;
+    // Levels of the CTU-local DAG.  Before a level, threads 0-3 wait (bounded) until their
+    // dependency CTU has completed the levels this level needs; after a level that other
+    // CTUs need, the CTU publishes (epoch << 16) | levels completed.
+    const uint2* lvl = reinterpret_cast<const uint2*>(P.ictu_lvl + P.ictu_lvl_off[idx]);
+    const int dep = tid < 4 ? P.ictu_deps[4 * idx + tid] : -1;
+    const int32_t stamp = epoch << 16;
     int pos = 0;
-    while (pos < n_tu) {
+    for (int L = 0; pos < n_tu; L++) {
+        const uint2 info = __ldg(lvl + L);
+        const uint32_t req01 = info.x & 0xFFFF7FFFu;      // req[0] without the publish bit, req[1]
+        if (req01 | info.y) {
+            if (dep >= 0) {
+                const uint32_t w = tid < 2 ? req01 : info.y;
+                const int need = (int)((w >> (16 * (tid & 1))) & 0xFFFFu);
+                if (need) {
+                    cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[dep]);
+                    long long polls = 0;
+                    while (done.load(cuda::memory_order_acquire) < (stamp | need)) {
+                        if (++polls > SPIN_LIMIT) {
+                            atomicOr(sticky, ST_TIMEOUT);
+                            s_abort = 1;
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+            }
+            __syncthreads();
+            if (s_abort) return;
+            // the neighbourhood now holds the samples this level reads
+            stage_margin(P, 0, rx, ry, t_luma, tid);
+            stage_margin(P, 1, rx, ry, t_chroma[0], tid);
+            stage_margin(P, 2, rx, ry, t_chroma[1], tid);
+            __syncthreads();
+        }
         const int lvl_end = P.itu_level_end[off + pos] - off;
         for (int i = pos + warp; i < lvl_end; i += IC_WARPS) {
             const hevc_tu_t& tu = s_tu[i];
@@ -355,14 +391,16 @@ __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant
             intra_tu_any(P, tu, lane, ws[warp], tile, nb, res);
         }
         __syncthreads();
+        if (info.x & INTRA_LEVEL_PUBLISH) {
+            // every thread's picture writes are visible before the word moves
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) {
+                cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[idx]);
+                done.store(stamp | (L + 1), cuda::memory_order_release);
+            }
+        }
         pos = lvl_end;
-    }
-    // publish: every thread's picture writes are visible before the flag moves
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-        cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[idx]);
-        done.store(epoch, cuda::memory_order_release);
     }
 }
 
