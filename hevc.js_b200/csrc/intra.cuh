@@ -31,6 +31,7 @@ struct IntraWarpSmem {
     int16_t raw[129];  // reference samples as read (0 where unavailable)
     int16_t s[129];    // after substitution: bottom-left .. corner (index 2n) .. top-right
     int16_t f[129];    // after smoothing
+    int16_t m[130];    // angular main reference m[q + n], q = -n .. 2n (+1 padding entry)
 };
 
 // Shared-memory copy of one plane around the CTU being reconstructed: sample (x, y) of
@@ -157,9 +158,29 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
             R_ = W.f;
         }
     }
-    // 4. prediction (top[k] = R_[2n + k], left[k] = R_[2n - k]) + residual, clip, store
+    // 4. prediction (top[k] = R_[2n + k], left[k] = R_[2n - k]) + residual, clip, store.
+    //    Each lane takes groups of 4 samples of a row; its column x0 = 4 * (lane % (n / 4))
+    //    is the same for all its groups, so column terms are computed once.
+    constexpr int GPR = n / 4, NG = n * n / 4, G_PER_LANE = (NG + 31) / 32;
     const int ang = c_intra_angle[mode];
-    const int inv = c_inv_angle[mode];
+    const bool vert = mode >= 18;
+    if (mode >= 2) {
+        // main reference with the side reference projected through invAngle (:346-368):
+        // m[q + n] = top[q] (vertical) / left[q] (horizontal) for q >= 0, the other side's
+        // sample min(2n, (-q * invAngle + 128) >> 8) for q < 0
+        const int inv = c_inv_angle[mode];
+        for (int q = lane - n; q <= 2 * n + 1; q += 32) {
+            int v = 0;
+            if (q > 2 * n) v = 0;   // padding entry, read but never weighted
+            else if (q >= 0) v = vert ? R_[2 * n + q] : R_[2 * n - q];
+            else {
+                const int si = min(2 * n, ((-q) * inv + 128) >> 8);
+                v = vert ? R_[2 * n - si] : R_[2 * n + si];
+            }
+            W.m[q + n] = (int16_t)v;
+        }
+        __syncwarp();
+    }
     int dc = 0;
     if (mode == 1) {  // predict_dc :295-317
         int s = 0;
@@ -167,44 +188,73 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
         s = __reduce_add_sync(0xffffffffu, s);
         dc = (s + n) >> (LOG2 + 1);
     }
-    constexpr int PER_LANE = (n * n + 31) / 32;
+    const int x0 = 4 * (lane % GPR);
+    const int corner = R_[2 * n], tr = R_[3 * n + 1], bl = R_[n - 1];
+    int ctop[4], cidx[4], cfr[4];
 #pragma unroll
-    for (int q = 0; q < PER_LANE; q++) {
-        const int e = lane + 32 * q;
-        if (e >= n * n) break;
-        const int y = e >> LOG2, x = e & (n - 1);
-        int p;
+    for (int j = 0; j < 4; j++) {
+        const int x = x0 + j;
+        ctop[j] = R_[2 * n + 1 + x];
+        cidx[j] = ((x + 1) * ang) >> 5;
+        cfr[j] = ((x + 1) * ang) & 31;
+    }
+#pragma unroll
+    for (int q = 0; q < G_PER_LANE; q++) {
+        const int g = lane + 32 * q;
+        if (g >= NG) break;
+        const int y = g / GPR;
+        const int left = R_[2 * n - 1 - y];
+        int p[4];
         if (mode == 0) {  // predict_planar :263-289
-            p = ((n - 1 - x) * R_[2 * n - 1 - y] + (x + 1) * R_[3 * n + 1] + (n - 1 - y) * R_[2 * n + 1 + x] +
-                 (y + 1) * R_[n - 1] + n) >> (LOG2 + 1);
-        } else if (mode == 1) {
-            p = dc;
-            if (!CHROMA && n < 32) {
-                if (x == 0 && y == 0) p = (R_[2 * n + 1] + R_[2 * n - 1] + 2 * dc + 2) >> 2;
-                else if (y == 0) p = (R_[2 * n + 1 + x] + 3 * dc + 2) >> 2;
-                else if (x == 0) p = (R_[2 * n - 1 - y] + 3 * dc + 2) >> 2;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int x = x0 + j;
+                p[j] = ((n - 1 - x) * left + (x + 1) * tr + (n - 1 - y) * ctop[j] + (y + 1) * bl + n) >> (LOG2 + 1);
             }
-        } else {  // predict_angular :323-422
-            const bool vert = mode >= 18;
-            const int pos = vert ? y : x, ln = vert ? x : y;
-            const int idx = ((pos + 1) * ang) >> 5, fr = ((pos + 1) * ang) & 31;
-            const int ri = ln + 1 + idx;
-            // main reference (top for vertical, left for horizontal); negative indices
-            // project onto the side reference through invAngle (:346-368)
-            auto ref_at = [&](int q) -> int {
-                if (q >= 0) return vert ? R_[2 * n + q] : R_[2 * n - q];
-                const int si = min(2 * n, ((-q) * inv + 128) >> 8);
-                return vert ? R_[2 * n - si] : R_[2 * n + si];
-            };
-            p = fr ? ((32 - fr) * ref_at(ri) + fr * ref_at(ri + 1) + 16) >> 5 : ref_at(ri);
+        } else if (mode == 1) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) p[j] = dc;
             if (!CHROMA && n < 32) {
-                if (mode == 26 && x == 0) p = clip_u8(p + ((R_[2 * n - 1 - y] - R_[2 * n]) >> 1));
-                else if (mode == 10 && y == 0) p = clip_u8(p + ((R_[2 * n + 1 + x] - R_[2 * n]) >> 1));
+                if (y == 0) {
+#pragma unroll
+                    for (int j = 0; j < 4; j++) p[j] = (ctop[j] + 3 * dc + 2) >> 2;
+                }
+                if (x0 == 0) p[0] = y == 0 ? (ctop[0] + left + 2 * dc + 2) >> 2 : (left + 3 * dc + 2) >> 2;
+            }
+        } else if (vert) {  // predict_angular :323-422, main reference on top
+            const int idx = ((y + 1) * ang) >> 5, fr = ((y + 1) * ang) & 31;
+            const int16_t* m = W.m + n + x0 + 1 + idx;
+            int r[5];
+#pragma unroll
+            for (int j = 0; j < 5; j++) r[j] = m[j];
+#pragma unroll
+            for (int j = 0; j < 4; j++) p[j] = fr ? ((32 - fr) * r[j] + fr * r[j + 1] + 16) >> 5 : r[j];
+            if (!CHROMA && n < 32 && mode == 26 && x0 == 0) p[0] = clip_u8(p[0] + ((left - corner) >> 1));
+        } else {  // main reference on the left
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int16_t* m = W.m + n + y + 1 + cidx[j];
+                p[j] = cfr[j] ? ((32 - cfr[j]) * m[0] + cfr[j] * m[1] + 16) >> 5 : m[0];
+            }
+            if (!CHROMA && n < 32 && mode == 10 && y == 0) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) p[j] = clip_u8(p[j] + ((ctop[j] - corner) >> 1));
             }
         }
-        const uint8_t v = (uint8_t)clip_u8(p + (res ? res[e] : 0));
-        tile.t[(yc + y - tile.y0) * tile.pitch + (xc + x - tile.x0)] = v;
-        plane[(int64_t)(yc + y) * pitch + xc + x] = v;
+        // residual (four int16 in one 8-byte load), clip, one word to the tile and the picture
+        int rv[4] = {0, 0, 0, 0};
+        if (res) {
+            const int2 rw = *reinterpret_cast<const int2*>(res + y * n + x0);
+            rv[0] = (int)(int16_t)(rw.x & 0xFFFF);
+            rv[1] = rw.x >> 16;
+            rv[2] = (int)(int16_t)(rw.y & 0xFFFF);
+            rv[3] = rw.y >> 16;
+        }
+        uint32_t w = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) w |= (uint32_t)clip_u8(p[j] + rv[j]) << (8 * j);
+        *reinterpret_cast<uint32_t*>(tile.t + (yc + y - tile.y0) * tile.pitch + (xc + x0 - tile.x0)) = w;
+        *reinterpret_cast<uint32_t*>(plane + (int64_t)(yc + y) * pitch + xc + x0) = w;
     }
 }
 
