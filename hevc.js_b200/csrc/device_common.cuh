@@ -53,9 +53,10 @@ struct PicDesc {
     const int32_t* ictu_addr;            // raster address of intra CTU k
     const int32_t* ictu_deps;            // 4 per intra CTU: intra CTUs it reads from, or -1
     const int32_t* ictu_tu_off;          // TUs of intra CTU k: itu[ictu_tu_off[k] .. [k+1])
-    const int32_t* itu;                  // TU index
+    const hevc_tu_t* itu_rec;            // TU records in task order
     const int32_t* itu_level_end;        // first entry of the next level of the same CTU
-    const int32_t* itu_res_off;          // residual offset inside the CTU's staged residuals
+    const int4* itu_res;                 // per task entry: residual source offset (-1: none),
+                                         // offset in the CTU's staged residuals, 16-byte chunks
     const int32_t* ictu_lvl_off;         // levels of intra CTU k: ictu_lvl[ictu_lvl_off[k] ..]
     const IntraLevel* ictu_lvl;
     int32_t* ictu_done;                  // per intra CTU: (epoch << 16) | levels completed

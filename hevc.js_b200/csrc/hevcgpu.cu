@@ -244,8 +244,11 @@ struct hevcgpu_ctx {
     // host worker pool for the batched host-side calls (job preparation, downloads)
     HostPool pool;
     std::vector<cudaEvent_t> dl_events;  // per-picture completion of batched downloads
-    // intra wavefront: FlowState (row ticket) followed by the sticky status word
+    // intra CTU tasks: FlowState, the sticky status word (16 bytes on), and one ticket
+    // counter per picture of a launch (32 bytes on)
     void* flow = nullptr;
+    static constexpr size_t FLOW_BYTES = sizeof(FlowState) + 16 + sizeof(int32_t) * MAX_SEGS;
+    int32_t* tickets() { return reinterpret_cast<int32_t*>(static_cast<uint8_t*>(flow) + sizeof(FlowState) + 16); }
     int sm_count = 148;
     // Reads and clears the sticky device status; maps it to a return code.
     int take_status() {
@@ -467,7 +470,9 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     // for that CTU.  A unit whose samples B may not use (availability) can only add an
     // unneeded level or wait, never change a sample.
     const int n_intra = (int)intra_list.size();
-    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, itu, itu_level_end, itu_res_off, ictu_lvl_off;
+    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, itu, itu_level_end, ictu_lvl_off;
+    std::vector<hevc_tu_t> itu_rec;     // intra TU records in task order
+    std::vector<int4> itu_res;          // per task entry: residual source, staged offset, 16-byte chunks
     std::vector<IntraLevel> ictu_lvl;
     if (n_intra) {
         std::vector<int32_t> level((size_t)n_intra, 0), ctu_of((size_t)n_intra, 0);
@@ -547,15 +552,18 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             itu_level_end[(size_t)i] = last ? i + 1 : itu_level_end[(size_t)i + 1];
         }
         // residual offsets inside each CTU's staged residuals (coded TUs, in itu order)
-        itu_res_off.assign((size_t)n_intra, -1);
+        itu_res.assign((size_t)n_intra, make_int4(-1, 0, 0, 0));
+        itu_rec.resize((size_t)n_intra);
         const int nic = (int)ictu_addr.size();
         for (int k = 0; k < nic; k++) {
             int acc = 0;
             for (int i = ictu_tu_off[(size_t)k]; i < ictu_tu_off[(size_t)k + 1]; i++) {
                 const hevc_tu_t& t = s->tus[itu[(size_t)i]];
+                itu_rec[(size_t)i] = t;
                 if (!(t.flags & HEVC_TU_CODED)) continue;
-                itu_res_off[(size_t)i] = acc;
-                acc += 1 << (2 * t.log2_size);
+                const int nn = 1 << (2 * t.log2_size);
+                itu_res[(size_t)i] = make_int4((int)t.coeff_offset, acc, nn / 8, 0);
+                acc += nn;
             }
             if (acc > IC_MAX_RES || ictu_tu_off[(size_t)k + 1] - ictu_tu_off[(size_t)k] > IC_MAX_TUS)
                 return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", ictu_addr[(size_t)k]);
@@ -660,9 +668,9 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         o_ia = pk.add(ictu_addr.data(), sizeof(int32_t) * ictu_addr.size());
         o_idp = pk.add(ictu_deps.data(), sizeof(int32_t) * ictu_deps.size());
         o_ito = pk.add(ictu_tu_off.data(), sizeof(int32_t) * ictu_tu_off.size());
-        o_itu = pk.add(itu.data(), sizeof(int32_t) * itu.size());
+        o_itu = pk.add(itu_rec.data(), sizeof(hevc_tu_t) * itu_rec.size());
         o_ile = pk.add(itu_level_end.data(), sizeof(int32_t) * itu_level_end.size());
-        o_iro = pk.add(itu_res_off.data(), sizeof(int32_t) * itu_res_off.size());
+        o_iro = pk.add(itu_res.data(), sizeof(int4) * itu_res.size());
         o_ilo = pk.add(ictu_lvl_off.data(), sizeof(int32_t) * ictu_lvl_off.size());
         o_ilv = pk.add(ictu_lvl.data(), sizeof(IntraLevel) * ictu_lvl.size());
     };
@@ -714,9 +722,9 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     D.ictu_addr = reinterpret_cast<const int32_t*>(base + o_ia);
     D.ictu_deps = reinterpret_cast<const int32_t*>(base + o_idp);
     D.ictu_tu_off = reinterpret_cast<const int32_t*>(base + o_ito);
-    D.itu = reinterpret_cast<const int32_t*>(base + o_itu);
+    D.itu_rec = reinterpret_cast<const hevc_tu_t*>(base + o_itu);
     D.itu_level_end = reinterpret_cast<const int32_t*>(base + o_ile);
-    D.itu_res_off = reinterpret_cast<const int32_t*>(base + o_iro);
+    D.itu_res = reinterpret_cast<const int4*>(base + o_iro);
     D.ictu_lvl_off = reinterpret_cast<const int32_t*>(base + o_ilo);
     D.ictu_lvl = reinterpret_cast<const IntraLevel*>(base + o_ilv);
     D.ictu_done = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(j->scratch.p) + resid_bytes + mot_bytes);
@@ -919,8 +927,9 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
             if (t.n == 0) continue;
             FlowState* fs = static_cast<FlowState*>(ctx->flow);
             uint32_t* sticky = reinterpret_cast<uint32_t*>(fs + 1);
-            CUDA_TRY(cudaMemsetAsync(&fs->head, 0, sizeof(int32_t), ctx->stream));
-            rc = L.go(k_intra_ctus, dim3(total), dim3(IC_THREADS), t, &fs->head, total, sticky);
+            int32_t* tickets = ctx->tickets();
+            CUDA_TRY(cudaMemsetAsync(tickets, 0, sizeof(int32_t) * (size_t)t.n, ctx->stream));
+            rc = L.go(k_intra_ctus, dim3(total), dim3(IC_THREADS), t, tickets, total, sticky);
             if (rc) return rc;
         }
     }
@@ -1006,8 +1015,8 @@ int hevcgpu_create(int device, hevcgpu_ctx_t** out) {
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&c->flow, sizeof(FlowState) + 16);
-    if (e == cudaSuccess) e = cudaMemset(c->flow, 0, sizeof(FlowState) + 16);
+    if (e == cudaSuccess) e = cudaMalloc(&c->flow, hevcgpu_ctx::FLOW_BYTES);
+    if (e == cudaSuccess) e = cudaMemset(c->flow, 0, hevcgpu_ctx::FLOW_BYTES);
     if (e != cudaSuccess) {
         delete c;
         return fail(HEVCGPU_ECUDA, "context set-up: %s", cudaGetErrorString(e));

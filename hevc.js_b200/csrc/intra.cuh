@@ -7,11 +7,12 @@
 //   - per CTU, a level for each intra TU in the DAG of the CTU's own intra TUs;
 //   - per CTU, the at most four earlier CTUs (left, above-left, above, above-right) whose
 //     intra TUs own samples it reads.
-// k_intra_ctus runs one CTA per CTU with intra TUs: it waits (bounded) for those CTUs,
-// stages the CTU, its neighbourhood, its TU records and residuals in shared memory, and
-// runs the TUs level by level, one warp per TU.  Every wait gives up after SPIN_LIMIT
-// polls, sets ST_TIMEOUT in the context's sticky status word (the host turns it into
-// HEVCGPU_ETIMEOUT) and returns.
+// k_intra_ctus runs one CTA per CTU with intra TUs: it stages the CTU, its TU records and
+// residuals in shared memory, and runs the TUs level by level, one warp per TU; before a
+// level that reads samples of those CTUs it waits (bounded) until they have completed
+// the levels that write them, and reads such samples from the picture through L2.
+// Every wait gives up after SPIN_LIMIT polls, sets ST_TIMEOUT in the context's sticky
+// status word (the host turns it into HEVCGPU_ETIMEOUT) and returns.
 #pragma once
 
 #include <cuda/atomic>
@@ -81,7 +82,8 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
             else { px = xc + (i - 2 * n - 1); py = yc - 1; }
             if (px >= 0 && py >= 0 && px < pw && py < ph) {
                 const int ncx = px >> log2c, ncy = py >> log2c;
-                if (ncx != rx || ncy != ry) {
+                const bool outside = ncx != rx || ncy != ry;
+                if (outside) {
                     // reference positions reach one CTB left, one CTB right (top row) and
                     // one CTB row up or down; later CTBs are never available
                     uint32_t bit = 0u;
@@ -92,7 +94,12 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
                 } else {
                     ok = zorder16((uint32_t)((px * sub - ox) >> 2), (uint32_t)((py * sub - oy) >> 2)) < cur_z;
                 }
-                if (ok) val = tile.t[(py - tile.y0) * tile.pitch + (px - tile.x0)];
+                if (ok) {
+                    // samples of other CTUs come from the picture through L2 (those CTUs
+                    // published them before this level), this CTU's from the tile
+                    val = outside ? __ldcg(plane + (int64_t)py * pitch + px)
+                                  : tile.t[(py - tile.y0) * tile.pitch + (px - tile.x0)];
+                }
             }
             W.raw[i] = (int16_t)val;
         }
@@ -280,7 +287,7 @@ __device__ __forceinline__ void intra_tu_any(const PicDesc& P, const hevc_tu_t& 
 
 // ---------------------------------------------------------------------------------------
 // CTU tasks.  One CTA per CTU that holds intra TUs.  CTAs take CTUs by ticket in raster
-// order, picture after picture.  The CTA stages the CTU and its neighbourhood, its TU
+// order per picture, the pictures of a launch side by side.  The CTA stages the CTU and its neighbourhood, its TU
 // records and their residuals in shared memory, then runs the TUs level by level of the
 // CTU-local dependency DAG (one warp per TU, a barrier between levels).  Dependencies on
 // the at most four earlier intra CTUs whose intra samples it reads (left, above-left,
@@ -292,74 +299,81 @@ __device__ __forceinline__ void intra_tu_any(const PicDesc& P, const hevc_tu_t& 
 // ---------------------------------------------------------------------------------------
 constexpr int IC_WARPS = 4;
 constexpr int IC_THREADS = 32 * IC_WARPS;
-constexpr int IC_MARGIN = 16;                        // bytes left of the CTU (column -1 last)
-constexpr int IC_LP = IC_MARGIN + 128, IC_LH = 65;   // luma tile pitch, rows -1 .. 63
-constexpr int IC_CP = IC_MARGIN + 64, IC_CH = 33;    // chroma tile
+constexpr int IC_LP = 64, IC_LH = 64;                // luma tile (the CTU): pitch, rows
+constexpr int IC_CP = 32, IC_CH = 32;                // chroma tiles
 constexpr int IC_MAX_TUS = 256 + 2 * 64;             // 4x4 TUs of a 64x64 CTU, all planes
 constexpr int IC_MAX_RES = 64 * 64 + 2 * 32 * 32;    // residual samples of a 64x64 CTU
 constexpr long long SPIN_LIMIT = 1ll << 24;          // polls of ~64 ns: about a second
 
-// Copy plane c around CTU (rx, ry) into its tile with 16-byte L2 loads: row -1 from
-// column -16 to 2*ctbc-1, rows 0..ctbc-1 from column -16 to ctbc-1.
+// 16-byte asynchronous global -> shared copy (through L2 only, so that samples other
+// CTUs wrote are seen), and the wait for all of a thread's copies.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Copy plane c of CTU (rx, ry) into its tile with 16-byte copies (issued, not waited
+// for).  Only the CTU itself: reference samples of other CTUs are read from the picture.
 __device__ __forceinline__ void stage_tile(const PicDesc& P, int c, int rx, int ry, uint8_t* tile, int tid) {
     const int sub = c ? 2 : 1, ctbc = (1 << P.log2_ctb) / sub;
     const int pw = P.width / sub, ph = P.height / sub, pitch = c ? P.pitch_c : P.pitch_y;
     const uint8_t* plane = P.rec + (c == 0 ? 0 : (c == 1 ? P.off_cb : P.off_cr));
     const int tp = c ? IC_CP : IC_LP;
-    const int x0 = rx * ctbc - IC_MARGIN, y0 = ry * ctbc - 1;
-    const int top_chunks = (IC_MARGIN + 2 * ctbc + 15) / 16, row_chunks = (IC_MARGIN + ctbc + 15) / 16;
-    const int n = top_chunks + ctbc * row_chunks;
-    for (int e = tid; e < n; e += IC_THREADS) {
-        int r, q;
-        if (e < top_chunks) { r = 0; q = e; }
-        else { r = 1 + (e - top_chunks) / row_chunks; q = (e - top_chunks) % row_chunks; }
-        const int y = y0 + r, x = x0 + 16 * q;
-        if (y < 0 || y >= ph || x < 0 || x >= pw) continue;
-        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(plane + (int64_t)y * pitch + x));
-        *reinterpret_cast<uint4*>(tile + r * tp + 16 * q) = v;
+    const int x0 = rx * ctbc, y0 = ry * ctbc;
+    if (ctbc >= 16) {
+        const int row_chunks = ctbc / 16;
+        for (int e = tid; e < ctbc * row_chunks; e += IC_THREADS) {
+            const int r = e / row_chunks, q = e % row_chunks;
+            const int y = y0 + r, x = x0 + 16 * q;
+            if (y >= ph || x >= pw) continue;
+            cp_async16(tile + r * tp + 16 * q, plane + (int64_t)y * pitch + x);
+        }
+    } else {  // 8-sample chroma CTBs (16x16 CTUs): words
+        for (int e = tid; e < ctbc * 2; e += IC_THREADS) {
+            const int r = e / 2, q = e % 2;
+            const int y = y0 + r, x = x0 + 4 * q;
+            if (y >= ph || x >= pw) continue;
+            *reinterpret_cast<uint32_t*>(tile + r * tp + 4 * q) =
+                __ldcg(reinterpret_cast<const uint32_t*>(plane + (int64_t)y * pitch + x));
+        }
     }
 }
 
-// Re-copy the parts of the tile that other CTUs write: row -1 and the IC_MARGIN columns
-// left of the CTU (the first chunk of each row).
-__device__ __forceinline__ void stage_margin(const PicDesc& P, int c, int rx, int ry, uint8_t* tile, int tid) {
-    const int sub = c ? 2 : 1, ctbc = (1 << P.log2_ctb) / sub;
-    const int pw = P.width / sub, ph = P.height / sub, pitch = c ? P.pitch_c : P.pitch_y;
-    const uint8_t* plane = P.rec + (c == 0 ? 0 : (c == 1 ? P.off_cb : P.off_cr));
-    const int tp = c ? IC_CP : IC_LP;
-    const int x0 = rx * ctbc - IC_MARGIN, y0 = ry * ctbc - 1;
-    const int top_chunks = (IC_MARGIN + 2 * ctbc + 15) / 16;
-    for (int e = tid; e < top_chunks + ctbc; e += IC_THREADS) {
-        const int r = e < top_chunks ? 0 : 1 + (e - top_chunks), q = e < top_chunks ? e : 0;
-        const int y = y0 + r, x = x0 + 16 * q;
-        if (y < 0 || y >= ph || x < 0 || x >= pw) continue;
-        const uint4 v = __ldcg(reinterpret_cast<const uint4*>(plane + (int64_t)y * pitch + x));
-        *reinterpret_cast<uint4*>(tile + r * tp + 16 * q) = v;
-    }
-}
-
-__global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant__ SegTable st, int32_t* ticket,
+__global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant__ SegTable st, int32_t* tickets,
                                                            int total, uint32_t* sticky) {
     __shared__ __align__(16) uint8_t t_luma[IC_LH * IC_LP];
     __shared__ __align__(16) uint8_t t_chroma[2][IC_CH * IC_CP];
     __shared__ __align__(16) hevc_tu_t s_tu[IC_MAX_TUS];
     __shared__ __align__(16) int16_t s_res[IC_MAX_RES];
     __shared__ IntraWarpSmem ws[IC_WARPS];
-    __shared__ int s_ticket, s_abort;
+    __shared__ int s_ticket, s_pic, s_abort;
     __shared__ uint32_t s_nb;
     const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
     if (tid == 0) {
-        s_ticket = atomicAdd(ticket, 1);
+        // Each picture hands out its CTUs by ticket in raster order.  CTAs start at picture
+        // blockIdx.x % n, so the pictures of a launch progress side by side; a picture whose
+        // tickets are used up passes the CTA on.  There are as many CTAs as CTUs, so every
+        // CTA finds one.
+        int k = blockIdx.x % st.n, got = -1;
+        for (int tries = 0; tries < st.n && got < 0; tries++) {
+            const int n_k = (k + 1 < st.n ? st.s[k + 1].aux0 : total) - st.s[k].aux0;
+            const int v = atomicAdd(&tickets[k], 1);
+            if (v < n_k) got = v;
+            else k = k + 1 == st.n ? 0 : k + 1;
+        }
+        s_ticket = got;
+        s_pic = k;
         s_abort = 0;
     }
     __syncthreads();
-    const int t = s_ticket;
-    if (t >= total) return;
-    int k = 0;
-    while (k + 1 < st.n && st.s[k + 1].aux0 <= t) k++;
+    if (s_ticket < 0) return;
+    const int k = s_pic;
     const PicDesc& P = *st.s[k].pic;
     const int epoch = st.s[k].aux1;
-    const int idx = t - st.s[k].aux0;
+    const int idx = s_ticket;
     const int a = P.ictu_addr[idx], rx = a % P.wctb, ry = a / P.wctb;
 
     if (tid == 4) {  // which neighbour CTBs share this CTB's slice and tile
@@ -375,20 +389,17 @@ __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant
 
     // stage the neighbourhood and the TU records
     const int off = P.ictu_tu_off[idx], n_tu = P.ictu_tu_off[idx + 1] - off;
-    for (int i = tid; i < n_tu; i += IC_THREADS) s_tu[i] = P.tus[P.itu[off + i]];
+    // one round of asynchronous copies: TU records, the three tiles, the residuals of the
+    // coded TUs (packed in task order, one thread per TU)
+    for (int i = tid; i < n_tu; i += IC_THREADS) cp_async16(&s_tu[i], &P.itu_rec[off + i]);
     stage_tile(P, 0, rx, ry, t_luma, tid);
     stage_tile(P, 1, rx, ry, t_chroma[0], tid);
     stage_tile(P, 2, rx, ry, t_chroma[1], tid);
-    __syncthreads();
-    // residuals of the coded TUs, packed in TU order (one warp per TU, 16-byte chunks)
-    for (int i = warp; i < n_tu; i += IC_WARPS) {
-        const hevc_tu_t& tu = s_tu[i];
-        if (!(tu.flags & HEVC_TU_CODED)) continue;
-        const int chunks = (1 << (2 * tu.log2_size)) / 8;
-        const uint4* src = reinterpret_cast<const uint4*>(P.resid + tu.coeff_offset);
-        uint4* dst = reinterpret_cast<uint4*>(s_res + P.itu_res_off[off + i]);
-        for (int c = lane; c < chunks; c += 32) dst[c] = __ldcg(src + c);
+    for (int i = tid; i < n_tu; i += IC_THREADS) {
+        const int4 r = __ldg(&P.itu_res[off + i]);
+        for (int c = 0; c < r.z; c++) cp_async16(s_res + r.y + 8 * c, P.resid + r.x + 8 * c);
     }
+    cp_async_wait_all();
     __syncthreads();
 
     const int ctbl = 1 << P.log2_ctb;
@@ -422,11 +433,6 @@ __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant
             }
             __syncthreads();
             if (s_abort) return;
-            // the neighbourhood now holds the samples this level reads
-            stage_margin(P, 0, rx, ry, t_luma, tid);
-            stage_margin(P, 1, rx, ry, t_chroma[0], tid);
-            stage_margin(P, 2, rx, ry, t_chroma[1], tid);
-            __syncthreads();
         }
         const int lvl_end = P.itu_level_end[off + pos] - off;
         for (int i = pos + warp; i < lvl_end; i += IC_WARPS) {
@@ -435,20 +441,17 @@ __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant
             CtuTile tile;
             tile.t = tu.c_idx == 0 ? t_luma : t_chroma[tu.c_idx - 1];
             tile.pitch = tu.c_idx ? IC_CP : IC_LP;
-            tile.x0 = rx * ctbc - IC_MARGIN;
-            tile.y0 = ry * ctbc - 1;
-            const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + P.itu_res_off[off + i] : nullptr;
+            tile.x0 = rx * ctbc;
+            tile.y0 = ry * ctbc;
+            const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + __ldg(&P.itu_res[off + i].y) : nullptr;
             intra_tu_any(P, tu, lane, ws[warp], tile, nb, res);
         }
         __syncthreads();
-        if (info.x & INTRA_LEVEL_PUBLISH) {
-            // every thread's picture writes are visible before the word moves
+        if ((info.x & INTRA_LEVEL_PUBLISH) && tid == 0) {
+            // after the barrier, one fence orders the CTA's picture writes before the word
             __threadfence();
-            __syncthreads();
-            if (tid == 0) {
-                cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[idx]);
-                done.store(stamp | (L + 1), cuda::memory_order_release);
-            }
+            cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[idx]);
+            done.store(stamp | (L + 1), cuda::memory_order_release);
         }
         pos = lvl_end;
     }
