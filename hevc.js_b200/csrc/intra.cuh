@@ -342,7 +342,7 @@ __device__ __forceinline__ void stage_tile(const PicDesc& P, int c, int rx, int 
     }
 }
 
-__global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant__ SegTable st, int32_t* tickets,
+__global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_constant__ SegTable st, int32_t* tickets,
                                                            int total, uint32_t* sticky) {
     __shared__ __align__(16) uint8_t t_luma[IC_LH * IC_LP];
     __shared__ __align__(16) uint8_t t_chroma[2][IC_CH * IC_CP];
@@ -448,8 +448,8 @@ __global__ void __launch_bounds__(IC_THREADS) k_intra_ctus(const __grid_constant
         }
         __syncthreads();
         if ((info.x & INTRA_LEVEL_PUBLISH) && tid == 0) {
-            // after the barrier, one fence orders the CTA's picture writes before the word
-            __threadfence();
+            // after the barrier, the release store orders the CTA's picture writes before
+            // the word (the barrier makes them prior to thread 0's release)
             cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[idx]);
             done.store(stamp | (L + 1), cuda::memory_order_release);
         }
