@@ -63,6 +63,34 @@ def dist_env():
     return rank, world, local
 
 
+# --------------------------------------------------------------------------- replicas
+# With N > 1 ranks (one process per GPU under torchrun) every rank reconstructs its own
+# streams: the work shards by stream with no data-path collective.  These helpers are the
+# host side of that: the per-rank content seed, the max over ranks of a time, and the
+# whole-job rate.
+
+def rank_seed0(rank):
+    """First content seed of a rank's streams; ranks never share a stream."""
+    return 1000 + 100000 * rank
+
+
+def max_over_ranks(x, world, device):
+    """Max of a per-rank float over all ranks (all_reduce MAX on device: a CUDA device
+    under NCCL, the CPU under gloo)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, seconds):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return units_per_rank * world / seconds
+
+
 # --------------------------------------------------------------------------- workload
 
 def make_streams(hb, n, w, h, seed0):
@@ -262,7 +290,7 @@ def run_ours(args, hb, rank, world, local):
     stream = torch.cuda.ExternalStream(ctx.cuda_stream, device=dev)
     W, H, B = args.width, args.height, args.batch
     # replicas: each rank reconstructs its own streams (different seeds), no collective
-    pics, refs = make_streams(hb, B, W, H, 1000 + 100000 * rank)
+    pics, refs = make_streams(hb, B, W, H, rank_seed0(rank))
     streams, jobs = [], []
     for i in range(B):
         st = ctx.open_stream(W, H, 3)
@@ -287,12 +315,8 @@ def run_ours(args, hb, rank, world, local):
         if world > 1:
             torch.distributed.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    def rank_max(x):
+        return max_over_ranks(x, world, dev)
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -316,7 +340,7 @@ def run_ours(args, hb, rank, world, local):
         barrier()
         ms = ev0.elapsed_time(ev1)
         step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
-        return max_over_ranks(ms), step_ms, ctx.launches - l0
+        return rank_max(ms), step_ms, ctx.launches - l0
 
     if args.profile_only:
         for _ in range(max(1, args.steps)):
@@ -356,13 +380,12 @@ def run_ours(args, hb, rank, world, local):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_step()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_s = rank_max(time.perf_counter() - t0)
     d2h_bytes = B * hb.i420_size(W, H)
 
-    frames = B * args.steps * world
-    value = frames / (batched_ms / 1000.0)
-    plain_value = B * plain_steps * world / (plain_ms / 1000.0)
-    e2e_value = B * e2e_steps * world / e2e_s
+    value = job_rate(B * args.steps, world, batched_ms / 1000.0)
+    plain_value = job_rate(B * plain_steps, world, plain_ms / 1000.0)
+    e2e_value = job_rate(B * e2e_steps, world, e2e_s)
 
     # roofline of the dominant stage
     import json as _json
