@@ -196,6 +196,11 @@ def gpu_lib():
             "hevcgpu_batch_launch": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
             "hevcgpu_stream_sync": ([P], C.c_int),
             "hevcgpu_jobs_prepare": ([C.POINTER(P), C.POINTER(P), C.c_int32, C.POINTER(P)], C.c_int),
+            "hevcgpu_lane_open": ([P, C.POINTER(P)], C.c_int),
+            "hevcgpu_lane_close": ([P], None),
+            "hevcgpu_lane_batch_launch": ([P, C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
+            "hevcgpu_lane_sync": ([P], C.c_int),
+            "hevcgpu_lane_cuda_stream": ([P], P),
             "hevcgpu_slots_download": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32, C.POINTER(P)], C.c_int),
             "hevcgpu_cuda_stream": ([P], P),
             "hevcgpu_launch_count": ([P], C.c_uint64),
@@ -223,7 +228,7 @@ class Context:
 
     def __init__(self, device=0):
         self.lib = gpu_lib()
-        self._children = weakref.WeakSet()   # streams and jobs: closed before the context
+        self._children = weakref.WeakSet()   # streams, lanes and jobs: closed before the context
         h = C.c_void_p()
         _check(self.lib.hevcgpu_create(device, C.byref(h)))
         self.h = h
@@ -235,7 +240,7 @@ class Context:
                 if isinstance(k, Job):
                     k.free()
             for k in kids:
-                if isinstance(k, Stream):
+                if isinstance(k, (Stream, Lane)):
                     k.close()
             self.lib.hevcgpu_destroy(self.h)
             self.h = None
@@ -390,6 +395,43 @@ def batch_launch(jobs, dst_slots):
     arr = (C.c_void_p * n)(*[j.h for j in jobs])
     slots = (C.c_int32 * n)(*dst_slots)
     _check(lib.hevcgpu_batch_launch(arr, slots, n))
+
+
+class Lane:
+    """A launch queue of a context that runs side by side with the others
+    (hevcgpu_lane_open): batches on different lanes overlap on the device."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = C.c_void_p()
+        _check(self.lib.hevcgpu_lane_open(ctx.h, C.byref(h)))
+        self.h = h
+        ctx._children.add(self)
+
+    def batch_launch(self, jobs, dst_slots):
+        n = len(jobs)
+        arr = (C.c_void_p * n)(*[j.h for j in jobs])
+        slots = (C.c_int32 * n)(*dst_slots)
+        _check(self.lib.hevcgpu_lane_batch_launch(self.h, arr, slots, n))
+
+    def sync(self):
+        _check(self.lib.hevcgpu_lane_sync(self.h))
+
+    @property
+    def cuda_stream(self):
+        return self.lib.hevcgpu_lane_cuda_stream(self.h)
+
+    def close(self):
+        if self.h and self.ctx.h:
+            self.lib.hevcgpu_lane_close(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def prepare_batch(streams, pics):

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -250,10 +251,14 @@ struct hevcgpu_ctx {
     static constexpr size_t FLOW_BYTES = sizeof(FlowState) + 16 + sizeof(int32_t) * MAX_SEGS;
     int32_t* tickets() { return reinterpret_cast<int32_t*>(static_cast<uint8_t*>(flow) + sizeof(FlowState) + 16); }
     int sm_count = 148;
-    // Reads and clears the sticky device status; maps it to a return code.
-    int take_status() {
+    cudaEvent_t done = nullptr;   // recorded after each launch on the context's own stream
+    std::mutex jobs_mu;
+    std::set<hevcgpu_job*> live_jobs;   // jobs of the DPB API, for lanes that close
+    // Reads and clears the sticky device status of a flow area; maps it to a return code.
+    int take_status() { return take_status_of(flow); }
+    static int take_status_of(void* flow_area) {
         uint32_t st = 0;
-        uint32_t* sticky = reinterpret_cast<uint32_t*>(static_cast<FlowState*>(flow) + 1);
+        uint32_t* sticky = reinterpret_cast<uint32_t*>(static_cast<FlowState*>(flow_area) + 1);
         if (cudaMemcpy(&st, sticky, sizeof(st), cudaMemcpyDeviceToHost) != cudaSuccess)
             return fail(HEVCGPU_ECUDA, "reading the device status: %s", cudaGetErrorString(cudaGetLastError()));
         if (!st) return HEVCGPU_OK;
@@ -263,6 +268,7 @@ struct hevcgpu_ctx {
     }
     ~hevcgpu_ctx() {
         if (flow) cudaFree(flow);
+        if (done) cudaEventDestroy(done);
         for (auto e : ev_pool) cudaEventDestroy(e);
         for (auto e : dl_events) cudaEventDestroy(e);
         for (auto& h : host_sizes) cudaFreeHost(h.first);
@@ -315,6 +321,21 @@ struct HostBuf {  // pooled pinned host buffer
 
 }  // namespace
 
+struct hevcgpu_lane {
+    hevcgpu_ctx* ctx = nullptr;
+    cudaStream_t stream = nullptr;
+    void* flow = nullptr;              // FlowState, status word, per-picture tickets
+    cudaEvent_t done = nullptr;        // recorded after each batch of the lane
+    cudaEvent_t ctx_ready = nullptr;   // the context stream's work before a batch
+    ~hevcgpu_lane() {
+        if (stream) cudaStreamSynchronize(stream);
+        if (flow) cudaFree(flow);
+        if (done) cudaEventDestroy(done);
+        if (ctx_ready) cudaEventDestroy(ctx_ready);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
 struct hevcgpu_stream {
     hevcgpu_ctx* ctx = nullptr;
     Layout lay;
@@ -345,11 +366,19 @@ struct hevcgpu_job {
     int32_t n_pus = 0;
     int has_intra = 0;
     int32_t dst_slot = -2;              // slot currently written into host_desc / desc
+    cudaStream_t last_stream = nullptr; // stream of the job's last launch (null: the context's)
+    cudaEvent_t last_done = nullptr;    // recorded after that launch
+    bool registered = false;            // in ctx->live_jobs
     uint64_t upload_bytes = 0;          // host -> device bytes of the prepare call
     hevc_pic_params_t params{};
     ~hevcgpu_job() {
         // buffers go back to the pools only after every queued use of them has run
         if (ctx) cudaStreamSynchronize(ctx->stream);
+        if (last_stream) cudaStreamSynchronize(last_stream);
+        if (registered) {
+            std::lock_guard<std::mutex> g(ctx->jobs_mu);
+            ctx->live_jobs.erase(this);
+        }
         if (desc_copied) cudaEventDestroy(desc_copied);
     }
 };
@@ -764,7 +793,9 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
 }
 
 // Point the job at its output and reference pictures and upload the descriptor.
-int job_bind(hevcgpu_job* j, uint8_t* rec, uint8_t* dst, const uint8_t* const refs[2][16]) {
+int job_bind(hevcgpu_job* j, uint8_t* rec, uint8_t* dst, const uint8_t* const refs[2][16],
+             cudaStream_t stream = nullptr) {
+    if (!stream) stream = j->ctx->stream;
     PicDesc& D = j->host_desc;
     D.rec = rec;
     D.dst = dst;
@@ -778,8 +809,8 @@ int job_bind(hevcgpu_job* j, uint8_t* rec, uint8_t* dst, const uint8_t* const re
     }
     uint8_t* stage = static_cast<uint8_t*>(j->pin.p) + j->desc_off;
     std::memcpy(stage, &D, sizeof(PicDesc));
-    CUDA_TRY(cudaMemcpyAsync(j->desc.p, stage, sizeof(PicDesc), cudaMemcpyHostToDevice, j->ctx->stream));
-    CUDA_TRY(cudaEventRecord(j->desc_copied, j->ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(j->desc.p, stage, sizeof(PicDesc), cudaMemcpyHostToDevice, stream));
+    CUDA_TRY(cudaEventRecord(j->desc_copied, stream));
     return HEVCGPU_OK;
 }
 
@@ -847,34 +878,43 @@ struct Launcher {
 // Brackets one stage with profiling events when profiling is on.
 struct StageMark {
     hevcgpu_ctx* ctx;
+    cudaStream_t stream;
     int stage;
     cudaEvent_t a = nullptr;
     uint64_t l0 = 0;
-    StageMark(hevcgpu_ctx* c, int s) : ctx(c), stage(s) {
+    StageMark(hevcgpu_ctx* c, cudaStream_t st, int s) : ctx(c), stream(st), stage(s) {
         if (!ctx->profiling) return;
         a = ctx->next_event();
         l0 = ctx->launches;
-        if (a) cudaEventRecord(a, ctx->stream);
+        if (a) cudaEventRecord(a, stream);
     }
     ~StageMark() {
         if (!ctx->profiling || !a) return;
         cudaEvent_t b = ctx->next_event();
         if (!b) return;
-        cudaEventRecord(b, ctx->stream);
+        cudaEventRecord(b, stream);
         ctx->marks.push_back({stage, a, b, ctx->launches - l0});
     }
 };
 
-int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, int res_mode) {
-    Launcher L{ctx, ctx->stream};
+// Where a batch runs: a CUDA stream and the flow area of its intra tasks (FlowState,
+// status word, per-picture tickets).  The context's own, or a lane's.
+struct Exec {
+    cudaStream_t stream;
+    void* flow;
+    int32_t* tickets() const { return reinterpret_cast<int32_t*>(static_cast<uint8_t*>(flow) + sizeof(FlowState) + 16); }
+};
+
+int run_stages(hevcgpu_ctx* ctx, const Exec& ex, hevcgpu_job* const* jobs, int n, int stages, int res_mode) {
+    Launcher L{ctx, ex.stream};
     int rc;
     if (stages & ST_DEBLOCK) {
-        StageMark m(ctx, 0);
+        StageMark m(ctx, ex.stream, 0);
         rc = L.pictures(k_motion_grid, jobs, n, 256, 1, [](hevcgpu_job* j) { return (j->n_pus * 32 + 255) / 256; });
         if (rc) return rc;
     }
     if (stages & ST_MC) {
-        StageMark m(ctx, 1);
+        StageMark m(ctx, ex.stream, 1);
         rc = L.items(k_mc<false>, jobs, n, MC_WARPS, MC_WARPS * 32, [](hevcgpu_job* j, const void*& p, int& c) {
             p = j->d_mc[0];
             c = j->n_mc[0];
@@ -887,7 +927,7 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
         if (rc) return rc;
     }
     if (stages & (ST_RESID | ST_INTRA)) {
-        StageMark m(ctx, 2);
+        StageMark m(ctx, ex.stream, 2);
         void (*kr[4])(const SegTable, int) = {k_residual<2>, k_residual<3>, k_residual<4>, k_residual<5>};
         for (int k = 0; k < 4; k++) {
             rc = L.items(kr[k], jobs, n, 128 >> (k + 2), 128,
@@ -900,7 +940,7 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
         }
     }
     if (stages & ST_INTRA) {
-        StageMark m(ctx, 3);
+        StageMark m(ctx, ex.stream, 3);
         // one launch per group of up to MAX_SEGS pictures: CTAs take intra CTUs by ticket
         // in (picture, raster) order; aux0 = intra CTUs of earlier pictures, aux1 = epoch
         int k = 0;
@@ -918,31 +958,31 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
                 // flags before they would reach the sign bit
                 if (j->epoch >= 32767) {
                     CUDA_TRY(cudaMemsetAsync(j->host_desc.ictu_done, 0, sizeof(int32_t) * (size_t)j->n_ictu,
-                                             ctx->stream));
+                                             ex.stream));
                     j->epoch = 0;
                 }
                 sg.aux1 = ++j->epoch;
                 total += j->n_ictu;
             }
             if (t.n == 0) continue;
-            FlowState* fs = static_cast<FlowState*>(ctx->flow);
+            FlowState* fs = static_cast<FlowState*>(ex.flow);
             uint32_t* sticky = reinterpret_cast<uint32_t*>(fs + 1);
-            int32_t* tickets = ctx->tickets();
-            CUDA_TRY(cudaMemsetAsync(tickets, 0, sizeof(int32_t) * (size_t)t.n, ctx->stream));
+            int32_t* tickets = ex.tickets();
+            CUDA_TRY(cudaMemsetAsync(tickets, 0, sizeof(int32_t) * (size_t)t.n, ex.stream));
             rc = L.go(k_intra_ctus, dim3(total), dim3(IC_THREADS), t, tickets, total, sticky);
             if (rc) return rc;
         }
     }
     if (stages & ST_DEBLOCK) {
         {
-            StageMark m(ctx, 4);
+            StageMark m(ctx, ex.stream, 4);
             rc = L.pictures(k_deblock<true>, jobs, n, 256, 1, [](hevcgpu_job* j) {
                 int segs = ((j->params.width + 7) / 8) * (j->params.height / 4);
                 return (segs + 255) / 256;
             });
             if (rc) return rc;
         }
-        StageMark m(ctx, 5);
+        StageMark m(ctx, ex.stream, 5);
         rc = L.pictures(k_deblock<false>, jobs, n, 256, 1, [](hevcgpu_job* j) {
             int segs = (j->params.width / 4) * ((j->params.height + 7) / 8);
             return (segs + 255) / 256;
@@ -950,7 +990,7 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
         if (rc) return rc;
     }
     if (stages & ST_SAO) {
-        StageMark m(ctx, 6);
+        StageMark m(ctx, ex.stream, 6);
         // one CTA per CTB; z = 0 luma, z = 1 both chroma planes
         rc = L.pictures(k_sao, jobs, n, 256, 2, [](hevcgpu_job* j) {
             const int ctb = 1 << j->params.log2_ctb;
@@ -959,6 +999,10 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
         if (rc) return rc;
     }
     return HEVCGPU_OK;
+}
+
+int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, int res_mode) {
+    return run_stages(ctx, Exec{ctx->stream, ctx->flow}, jobs, n, stages, res_mode);
 }
 
 int upload_i420(hevcgpu_ctx* ctx, const Layout& L, uint8_t* dev, const uint8_t* host) {
@@ -1017,6 +1061,7 @@ int hevcgpu_create(int device, hevcgpu_ctx_t** out) {
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->flow, hevcgpu_ctx::FLOW_BYTES);
     if (e == cudaSuccess) e = cudaMemset(c->flow, 0, hevcgpu_ctx::FLOW_BYTES);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         delete c;
         return fail(HEVCGPU_ECUDA, "context set-up: %s", cudaGetErrorString(e));
@@ -1409,6 +1454,11 @@ int hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, 
         delete j;
         return rc;
     }
+    {
+        std::lock_guard<std::mutex> g(st->ctx->jobs_mu);
+        st->ctx->live_jobs.insert(j);
+        j->registered = true;
+    }
     *out = j;
     return HEVCGPU_OK;
 }
@@ -1418,11 +1468,38 @@ uint64_t hevcgpu_job_upload_bytes(hevcgpu_job_t* job) { return job ? job->upload
 void hevcgpu_job_free(hevcgpu_job_t* job) {
     if (!job) return;
     cudaStreamSynchronize(job->ctx->stream);
+    if (job->last_stream) cudaStreamSynchronize(job->last_stream);
     delete job;
 }
 
 namespace {
-int job_target(hevcgpu_job* j, int32_t dst_slot) {
+// Jobs last launched on another stream: make `stream` wait for those launches (their
+// descriptors and scratch are reused).
+int order_jobs(hevcgpu_job* const* jobs, int n, cudaStream_t stream) {
+    cudaEvent_t waited[8];
+    int nw = 0;
+    for (int k = 0; k < n; k++) {
+        hevcgpu_job* j = jobs[k];
+        if (!j->last_done || j->last_stream == stream) continue;
+        bool seen = false;
+        for (int q = 0; q < nw && !seen; q++) seen = waited[q] == j->last_done;
+        if (seen) continue;
+        CUDA_TRY(cudaStreamWaitEvent(stream, j->last_done, 0));
+        if (nw < 8) waited[nw++] = j->last_done;
+    }
+    return HEVCGPU_OK;
+}
+// After a launch on `stream`: record its completion event and remember it in the jobs.
+int mark_jobs(hevcgpu_job* const* jobs, int n, cudaStream_t stream, cudaEvent_t done) {
+    CUDA_TRY(cudaEventRecord(done, stream));
+    for (int k = 0; k < n; k++) {
+        jobs[k]->last_stream = stream;
+        jobs[k]->last_done = done;
+    }
+    return HEVCGPU_OK;
+}
+
+int job_target(hevcgpu_job* j, int32_t dst_slot, cudaStream_t stream = nullptr) {
     hevcgpu_stream* st = j->st;
     if (!st) return fail(HEVCGPU_EINVAL, "job has no stream");
     if (dst_slot < 0 || dst_slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", dst_slot);
@@ -1435,22 +1512,17 @@ int job_target(hevcgpu_job* j, int32_t dst_slot) {
     for (int l = 0; l < 2; l++)
         for (int i = 0; i < j->params.num_ref[l]; i++)
             refs[l][i] = static_cast<const uint8_t*>(st->slots[(size_t)j->params.ref_slot[l][i]].p);
-    int rc = job_bind(j, static_cast<uint8_t*>(j->rec.p), static_cast<uint8_t*>(st->slots[(size_t)dst_slot].p), refs);
+    int rc = job_bind(j, static_cast<uint8_t*>(j->rec.p), static_cast<uint8_t*>(st->slots[(size_t)dst_slot].p), refs,
+                      stream);
     if (rc) return rc;
     j->dst_slot = dst_slot;
     return HEVCGPU_OK;
 }
 }  // namespace
 
-int hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot) {
-    if (!job) return fail(HEVCGPU_EINVAL, "null job");
-    int rc = job_target(job, dst_slot);
-    if (rc) return rc;
-    hevcgpu_job* jp = job;
-    return run_stages(job->ctx, &jp, 1, ST_ALL, RES_PICTURE);
-}
-
-int hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, int32_t n) {
+namespace {
+// Checks of a batch: one context, no job twice, no two pictures into one slot of a stream.
+int check_batch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, int32_t n, hevcgpu_ctx** ctx_out) {
     if (!jobs || !dst_slots || n <= 0) return fail(HEVCGPU_EINVAL, "empty batch");
     if (!jobs[0]) return fail(HEVCGPU_EINVAL, "null job");
     hevcgpu_ctx* ctx = jobs[0]->ctx;
@@ -1461,11 +1533,96 @@ int hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, i
             if (jobs[q]->st == jobs[k]->st && dst_slots[q] == dst_slots[k])
                 return fail(HEVCGPU_EINVAL, "two pictures of the batch write slot %d of one stream", dst_slots[k]);
         }
-        int rc = job_target(jobs[k], dst_slots[k]);
-        if (rc) return rc;
     }
-    return run_stages(ctx, jobs, n, ST_ALL, RES_PICTURE);
+    *ctx_out = ctx;
+    return HEVCGPU_OK;
 }
+
+// A batch on an execution stream: order after the jobs' launches elsewhere, point the
+// jobs at their slots, run the stages, record completion.
+int launch_batch(hevcgpu_ctx* ctx, const Exec& ex, cudaEvent_t done, hevcgpu_job* const* jobs,
+                 const int32_t* dst_slots, int n) {
+    int rc = order_jobs(jobs, n, ex.stream);
+    if (rc) return rc;
+    for (int k = 0; k < n; k++)
+        if ((rc = job_target(jobs[k], dst_slots[k], ex.stream))) return rc;
+    if ((rc = run_stages(ctx, ex, jobs, n, ST_ALL, RES_PICTURE))) return rc;
+    return mark_jobs(jobs, n, ex.stream, done);
+}
+}  // namespace
+
+int hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot) {
+    if (!job) return fail(HEVCGPU_EINVAL, "null job");
+    hevcgpu_job* jp = job;
+    return launch_batch(job->ctx, Exec{job->ctx->stream, job->ctx->flow}, job->ctx->done, &jp, &dst_slot, 1);
+}
+
+int hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, int32_t n) {
+    hevcgpu_ctx* ctx = nullptr;
+    int rc = check_batch(jobs, dst_slots, n, &ctx);
+    if (rc) return rc;
+    return launch_batch(ctx, Exec{ctx->stream, ctx->flow}, ctx->done, jobs, dst_slots, n);
+}
+
+// ---- lanes ---------------------------------------------------------------------------
+
+int hevcgpu_lane_open(hevcgpu_ctx_t* ctx, hevcgpu_lane_t** out) {
+    if (!out) return fail(HEVCGPU_EINVAL, "null out");
+    *out = nullptr;
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    auto* ln = new (std::nothrow) hevcgpu_lane();
+    if (!ln) return fail(HEVCGPU_ENOMEM, "host allocation");
+    ln->ctx = ctx;
+    cudaError_t e = cudaStreamCreateWithFlags(&ln->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&ln->flow, hevcgpu_ctx::FLOW_BYTES);
+    if (e == cudaSuccess) e = cudaMemset(ln->flow, 0, hevcgpu_ctx::FLOW_BYTES);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ln->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ln->ctx_ready, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete ln;
+        return fail(HEVCGPU_ECUDA, "lane set-up: %s", cudaGetErrorString(e));
+    }
+    *out = ln;
+    return HEVCGPU_OK;
+}
+
+void hevcgpu_lane_close(hevcgpu_lane_t* lane) {
+    if (!lane) return;
+    cudaSetDevice(lane->ctx->device);
+    cudaStreamSynchronize(lane->stream);
+    {   // jobs last launched on this lane forget it: its work is done
+        std::lock_guard<std::mutex> g(lane->ctx->jobs_mu);
+        for (hevcgpu_job* j : lane->ctx->live_jobs)
+            if (j->last_stream == lane->stream) {
+                j->last_stream = nullptr;
+                j->last_done = nullptr;
+            }
+    }
+    delete lane;
+}
+
+int hevcgpu_lane_batch_launch(hevcgpu_lane_t* lane, hevcgpu_job_t* const* jobs, const int32_t* dst_slots,
+                              int32_t n) {
+    if (!lane) return fail(HEVCGPU_EINVAL, "null lane");
+    hevcgpu_ctx* ctx = nullptr;
+    int rc = check_batch(jobs, dst_slots, n, &ctx);
+    if (rc) return rc;
+    if (ctx != lane->ctx) return fail(HEVCGPU_EINVAL, "jobs of another context");
+    // the jobs' record uploads and the slots' uploads ran on the context's stream
+    CUDA_TRY(cudaEventRecord(lane->ctx_ready, ctx->stream));
+    CUDA_TRY(cudaStreamWaitEvent(lane->stream, lane->ctx_ready, 0));
+    return launch_batch(ctx, Exec{lane->stream, lane->flow}, lane->done, jobs, dst_slots, n);
+}
+
+int hevcgpu_lane_sync(hevcgpu_lane_t* lane) {
+    if (!lane) return fail(HEVCGPU_EINVAL, "null lane");
+    CUDA_TRY(cudaStreamSynchronize(lane->stream));
+    return hevcgpu_ctx::take_status_of(lane->flow);
+}
+
+void* hevcgpu_lane_cuda_stream(hevcgpu_lane_t* lane) { return lane ? (void*)lane->stream : nullptr; }
 
 int hevcgpu_jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns, int32_t n,
                          hevcgpu_job_t** out) {

@@ -238,6 +238,27 @@ int  hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot);
 int  hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, int32_t n);
 int  hevcgpu_stream_sync(hevcgpu_stream_t* st);
 
+/* Lanes: launch queues of one context that run side by side on the device.  A lane has
+ * its own CUDA stream and its own intra-task state, so batches launched on different
+ * lanes overlap (one batch's latency-bound intra waves share the SMs with another's MC
+ * and filters) - the device side of continuous batching.  No counterpart in the
+ * reference, whose decoder reconstructs one picture at a time (decoder.cpp:52-304).
+ * Ordering: a lane batch starts after everything queued so far on the context's stream
+ * (record uploads, slot uploads), and a job launched on a lane other than its last one
+ * waits for that launch.  A picture that references a slot written by a batch of another
+ * lane must be launched after hevcgpu_lane_sync of that lane (or on the same lane); the
+ * context's own slot downloads likewise follow hevcgpu_lane_sync.  A lane is used from
+ * one host thread at a time. */
+typedef struct hevcgpu_lane hevcgpu_lane_t;
+int   hevcgpu_lane_open(hevcgpu_ctx_t* ctx, hevcgpu_lane_t** out);
+void  hevcgpu_lane_close(hevcgpu_lane_t* lane);
+int   hevcgpu_lane_batch_launch(hevcgpu_lane_t* lane, hevcgpu_job_t* const* jobs,
+                                const int32_t* dst_slots, int32_t n);
+/* Waits for the lane and returns its device status (HEVCGPU_ETIMEOUT / EDEVICE). */
+int   hevcgpu_lane_sync(hevcgpu_lane_t* lane);
+/* CUDA stream (cudaStream_t) of the lane. */
+void* hevcgpu_lane_cuda_stream(hevcgpu_lane_t* lane);
+
 /* Batched host-side calls for a decoder that finishes several pictures at once (one per
  * stream).  The work is spread over the context's host worker threads (one per
  * hardware thread, started on first use).

@@ -126,6 +126,47 @@ def test_batched_prepare_and_download(hb, gpu_ctx, port):
     assert "picture 0" in str(e.value)
 
 
+def test_lanes_alone_and_in_the_mix(hb, gpu_ctx, port):
+    """Pictures of mixed sizes give the same bytes decoded alone (plain launch on the
+    context) and decoded in overlapping batches on two lanes, round after round, and a
+    job moved from one lane to the other reproduces them again."""
+    specs = [(416, 240, 91, cases.PICTURE), (1280, 720, 92, cases.PICTURE), (1920, 1080, 93, cases.PICTURE),
+             (640, 360, 94, dict(slice_type=2)), (208, 120, 95, cases.INTRA_HEAVY), (1920, 1080, 96, cases.PICTURE)]
+    streams, jobs, alone = [], [], []
+    for (w, h, seed, kw) in specs:
+        st = gpu_ctx.open_stream(w, h, 3)
+        refs = [hb.content(w, h, seed + 1), hb.content(w, h, seed + 2)]
+        st.upload(0, refs[0])
+        st.upload(1, refs[1])
+        pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+        job = st.prepare(pic)
+        job.launch(2)
+        st.sync()
+        got = st.download(2)
+        assert _diff(got, port.reconstruct_picture(pic, refs)) == 0
+        streams.append(st)
+        jobs.append(job)
+        alone.append(got)
+    lanes = [hb.Lane(gpu_ctx), hb.Lane(gpu_ctx)]
+    groups = [[0, 2, 4], [1, 3, 5]]
+    for st in streams:
+        st.upload(2, np.zeros(hb.i420_size(st.width, st.height), np.uint8))
+    for _ in range(3):
+        for lane, g in zip(lanes, groups):
+            lane.batch_launch([jobs[i] for i in g], [2] * len(g))
+    for lane in lanes:
+        lane.sync()
+    for st, want in zip(streams, alone):
+        assert _diff(st.download(2), want) == 0
+    # job 0 last ran on lane 0; run it on lane 1 into a cleared slot
+    streams[0].upload(2, np.zeros(hb.i420_size(streams[0].width, streams[0].height), np.uint8))
+    lanes[1].batch_launch([jobs[0]], [2])
+    lanes[1].sync()
+    assert _diff(streams[0].download(2), alone[0]) == 0
+    for lane in lanes:
+        lane.close()
+
+
 def test_picture_decode_end_to_end(hb, gpu_ctx, port):
     w, h = 640, 360
     st = gpu_ctx.open_stream(w, h, 3)
