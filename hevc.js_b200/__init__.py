@@ -201,6 +201,8 @@ def gpu_lib():
             "hevcgpu_lane_batch_launch": ([P, C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
             "hevcgpu_lane_sync": ([P], C.c_int),
             "hevcgpu_lane_cuda_stream": ([P], P),
+            "hevcgpu_lane_slots_download": ([P, C.POINTER(P), C.POINTER(C.c_int32), C.c_int32, C.POINTER(P)],
+                                            C.c_int),
             "hevcgpu_slots_download": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32, C.POINTER(P)], C.c_int),
             "hevcgpu_cuda_stream": ([P], P),
             "hevcgpu_launch_count": ([P], C.c_uint64),
@@ -417,6 +419,15 @@ class Lane:
 
     def sync(self):
         _check(self.lib.hevcgpu_lane_sync(self.h))
+
+    def download_batch(self, streams, slots, outs):
+        """Slots of streams into host buffers, the copies ordered after this lane's batches."""
+        n = len(streams)
+        sts = (C.c_void_p * n)(*[st.h for st in streams])
+        sl = (C.c_int32 * n)(*slots)
+        ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        _check(self.lib.hevcgpu_lane_slots_download(self.h, sts, sl, n, ptrs))
+        return outs
 
     @property
     def cuda_stream(self):

@@ -1015,13 +1015,15 @@ int upload_i420(hevcgpu_ctx* ctx, const Layout& L, uint8_t* dev, const uint8_t* 
     return HEVCGPU_OK;
 }
 
-int download_i420(hevcgpu_ctx* ctx, const Layout& L, const uint8_t* dev, uint8_t* host) {
+int download_i420(hevcgpu_ctx* ctx, const Layout& L, const uint8_t* dev, uint8_t* host,
+                  cudaStream_t stream = nullptr) {
     const int W = L.W, H = L.H, cw = W / 2, ch = H / 2;
-    CUDA_TRY(cudaMemcpy2DAsync(host, W, dev, L.pitch_y, W, H, cudaMemcpyDeviceToHost, ctx->stream));
+    if (!stream) stream = ctx->stream;
+    CUDA_TRY(cudaMemcpy2DAsync(host, W, dev, L.pitch_y, W, H, cudaMemcpyDeviceToHost, stream));
     CUDA_TRY(cudaMemcpy2DAsync(host + (size_t)W * H, cw, dev + L.off_cb, L.pitch_c, cw, ch, cudaMemcpyDeviceToHost,
-                               ctx->stream));
+                               stream));
     CUDA_TRY(cudaMemcpy2DAsync(host + (size_t)W * H + (size_t)cw * ch, cw, dev + L.off_cr, L.pitch_c, cw, ch,
-                               cudaMemcpyDeviceToHost, ctx->stream));
+                               cudaMemcpyDeviceToHost, stream));
     return HEVCGPU_OK;
 }
 
@@ -1657,7 +1659,12 @@ int hevcgpu_jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax
     return HEVCGPU_OK;
 }
 
-int hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n, uint8_t* const* outs) {
+}  // extern "C"
+
+namespace {
+// Batched download with the device->host copies on `stream` (null: the context's).
+int slots_download_on(hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n, uint8_t* const* outs,
+                      cudaStream_t stream) {
     if (n < 0 || (n && (!sts || !slots || !outs))) return fail(HEVCGPU_EINVAL, "null arrays");
     if (n == 0) return HEVCGPU_OK;
     for (int i = 0; i < n; i++) {
@@ -1690,8 +1697,9 @@ int hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, i
             if ((rc = stage[(size_t)i].get(ctx, bytes))) return rc;
             dst = static_cast<uint8_t*>(stage[(size_t)i].p);
         }
-        if ((rc = download_i420(ctx, L, static_cast<uint8_t*>(sts[i]->slots[(size_t)slots[i]].p), dst))) return rc;
-        CUDA_TRY(cudaEventRecord(ctx->dl_events[(size_t)i], ctx->stream));
+        if ((rc = download_i420(ctx, L, static_cast<uint8_t*>(sts[i]->slots[(size_t)slots[i]].p), dst, stream)))
+            return rc;
+        CUDA_TRY(cudaEventRecord(ctx->dl_events[(size_t)i], stream ? stream : ctx->stream));
     }
     std::vector<int> rcs((size_t)n, 0);
     ctx->pool.run(n, [&](int i) {
@@ -1707,6 +1715,24 @@ int hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, i
     for (int i = 0; i < n; i++)
         if (rcs[(size_t)i]) return fail(HEVCGPU_ECUDA, "picture %d: download: %s", i, cudaGetErrorString(cudaGetLastError()));
     return HEVCGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n, uint8_t* const* outs) {
+    return slots_download_on(sts, slots, n, outs, nullptr);
+}
+
+int hevcgpu_lane_slots_download(hevcgpu_lane_t* lane, hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n,
+                                uint8_t* const* outs) {
+    if (!lane) return fail(HEVCGPU_EINVAL, "null lane");
+    for (int i = 0; i < n; i++)
+        if (sts && sts[i] && sts[i]->ctx != lane->ctx) return fail(HEVCGPU_EINVAL, "picture %d: stream of another context", i);
+    int rc = slots_download_on(sts, slots, n, outs, lane->stream);
+    if (rc) return rc;
+    return hevcgpu_ctx::take_status_of(lane->flow);
 }
 
 int hevcgpu_stream_sync(hevcgpu_stream_t* st) {

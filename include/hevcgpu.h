@@ -258,6 +258,11 @@ int   hevcgpu_lane_batch_launch(hevcgpu_lane_t* lane, hevcgpu_job_t* const* jobs
 int   hevcgpu_lane_sync(hevcgpu_lane_t* lane);
 /* CUDA stream (cudaStream_t) of the lane. */
 void* hevcgpu_lane_cuda_stream(hevcgpu_lane_t* lane);
+/* hevcgpu_slots_download with the copies queued on the lane, after its batches: the
+ * pictures of a lane batch can be read back without waiting for the other lanes.
+ * Returns the lane's device status, like hevcgpu_lane_sync. */
+int   hevcgpu_lane_slots_download(hevcgpu_lane_t* lane, hevcgpu_stream_t* const* sts,
+                                  const int32_t* slots, int32_t n, uint8_t* const* outs);
 
 /* Batched host-side calls for a decoder that finishes several pictures at once (one per
  * stream).  The work is spread over the context's host worker threads (one per

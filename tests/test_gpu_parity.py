@@ -163,6 +163,14 @@ def test_lanes_alone_and_in_the_mix(hb, gpu_ctx, port):
     lanes[1].batch_launch([jobs[0]], [2])
     lanes[1].sync()
     assert _diff(streams[0].download(2), alone[0]) == 0
+    # a lane's download is ordered after its own batches, without a sync first
+    for st in streams:
+        st.upload(2, np.zeros(hb.i420_size(st.width, st.height), np.uint8))
+    lanes[0].batch_launch([jobs[i] for i in groups[0]], [2] * 3)
+    outs = [np.empty(hb.i420_size(streams[i].width, streams[i].height), np.uint8) for i in groups[0]]
+    lanes[0].download_batch([streams[i] for i in groups[0]], [2] * 3, outs)
+    for i, got in zip(groups[0], outs):
+        assert _diff(got, alone[i]) == 0
     for lane in lanes:
         lane.close()
 
