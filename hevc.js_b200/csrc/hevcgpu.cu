@@ -251,7 +251,12 @@ struct hevcgpu_ctx {
     static constexpr size_t FLOW_BYTES = sizeof(FlowState) + 16 + sizeof(int32_t) * MAX_SEGS;
     int32_t* tickets() { return reinterpret_cast<int32_t*>(static_cast<uint8_t*>(flow) + sizeof(FlowState) + 16); }
     int sm_count = 148;
-    cudaEvent_t done = nullptr;   // recorded after each launch on the context's own stream
+    // completion events of the batches on the context's own stream, used in turn: a job
+    // waits for its own batch's event (re-recorded only EVENT_RING batches later)
+    static constexpr int EVENT_RING = 16;
+    cudaEvent_t done[EVENT_RING] = {};
+    int done_next = 0;
+    cudaEvent_t next_done() { cudaEvent_t e = done[done_next]; done_next = (done_next + 1) % EVENT_RING; return e; }
     std::mutex jobs_mu;
     std::set<hevcgpu_job*> live_jobs;   // jobs of the DPB API, for lanes that close
     // Reads and clears the sticky device status of a flow area; maps it to a return code.
@@ -268,7 +273,8 @@ struct hevcgpu_ctx {
     }
     ~hevcgpu_ctx() {
         if (flow) cudaFree(flow);
-        if (done) cudaEventDestroy(done);
+        for (auto e : done)
+            if (e) cudaEventDestroy(e);
         for (auto e : ev_pool) cudaEventDestroy(e);
         for (auto e : dl_events) cudaEventDestroy(e);
         for (auto& h : host_sizes) cudaFreeHost(h.first);
@@ -325,12 +331,19 @@ struct hevcgpu_lane {
     hevcgpu_ctx* ctx = nullptr;
     cudaStream_t stream = nullptr;
     void* flow = nullptr;              // FlowState, status word, per-picture tickets
-    cudaEvent_t done = nullptr;        // recorded after each batch of the lane
+    cudaEvent_t done[hevcgpu_ctx::EVENT_RING] = {};   // batch completion events, used in turn
+    int done_next = 0;
     cudaEvent_t ctx_ready = nullptr;   // the context stream's work before a batch
+    cudaEvent_t next_done() {
+        cudaEvent_t e = done[done_next];
+        done_next = (done_next + 1) % hevcgpu_ctx::EVENT_RING;
+        return e;
+    }
     ~hevcgpu_lane() {
         if (stream) cudaStreamSynchronize(stream);
         if (flow) cudaFree(flow);
-        if (done) cudaEventDestroy(done);
+        for (auto e : done)
+            if (e) cudaEventDestroy(e);
         if (ctx_ready) cudaEventDestroy(ctx_ready);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -374,7 +387,8 @@ struct hevcgpu_job {
     ~hevcgpu_job() {
         // buffers go back to the pools only after every queued use of them has run
         if (ctx) cudaStreamSynchronize(ctx->stream);
-        if (last_stream) cudaStreamSynchronize(last_stream);
+        if (last_done) cudaEventSynchronize(last_done);   // the job's last batch, not later ones
+        else if (last_stream) cudaStreamSynchronize(last_stream);
         if (registered) {
             std::lock_guard<std::mutex> g(ctx->jobs_mu);
             ctx->live_jobs.erase(this);
@@ -1063,7 +1077,8 @@ int hevcgpu_create(int device, hevcgpu_ctx_t** out) {
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&c->flow, hevcgpu_ctx::FLOW_BYTES);
     if (e == cudaSuccess) e = cudaMemset(c->flow, 0, hevcgpu_ctx::FLOW_BYTES);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
+    for (int k = 0; k < hevcgpu_ctx::EVENT_RING && e == cudaSuccess; k++)
+        e = cudaEventCreateWithFlags(&c->done[k], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         delete c;
         return fail(HEVCGPU_ECUDA, "context set-up: %s", cudaGetErrorString(e));
@@ -1556,14 +1571,14 @@ int launch_batch(hevcgpu_ctx* ctx, const Exec& ex, cudaEvent_t done, hevcgpu_job
 int hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot) {
     if (!job) return fail(HEVCGPU_EINVAL, "null job");
     hevcgpu_job* jp = job;
-    return launch_batch(job->ctx, Exec{job->ctx->stream, job->ctx->flow}, job->ctx->done, &jp, &dst_slot, 1);
+    return launch_batch(job->ctx, Exec{job->ctx->stream, job->ctx->flow}, job->ctx->next_done(), &jp, &dst_slot, 1);
 }
 
 int hevcgpu_batch_launch(hevcgpu_job_t* const* jobs, const int32_t* dst_slots, int32_t n) {
     hevcgpu_ctx* ctx = nullptr;
     int rc = check_batch(jobs, dst_slots, n, &ctx);
     if (rc) return rc;
-    return launch_batch(ctx, Exec{ctx->stream, ctx->flow}, ctx->done, jobs, dst_slots, n);
+    return launch_batch(ctx, Exec{ctx->stream, ctx->flow}, ctx->next_done(), jobs, dst_slots, n);
 }
 
 // ---- lanes ---------------------------------------------------------------------------
@@ -1579,7 +1594,8 @@ int hevcgpu_lane_open(hevcgpu_ctx_t* ctx, hevcgpu_lane_t** out) {
     cudaError_t e = cudaStreamCreateWithFlags(&ln->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&ln->flow, hevcgpu_ctx::FLOW_BYTES);
     if (e == cudaSuccess) e = cudaMemset(ln->flow, 0, hevcgpu_ctx::FLOW_BYTES);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ln->done, cudaEventDisableTiming);
+    for (int k = 0; k < hevcgpu_ctx::EVENT_RING && e == cudaSuccess; k++)
+        e = cudaEventCreateWithFlags(&ln->done[k], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ln->ctx_ready, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1615,7 +1631,7 @@ int hevcgpu_lane_batch_launch(hevcgpu_lane_t* lane, hevcgpu_job_t* const* jobs, 
     // the jobs' record uploads and the slots' uploads ran on the context's stream
     CUDA_TRY(cudaEventRecord(lane->ctx_ready, ctx->stream));
     CUDA_TRY(cudaStreamWaitEvent(lane->stream, lane->ctx_ready, 0));
-    return launch_batch(ctx, Exec{lane->stream, lane->flow}, lane->done, jobs, dst_slots, n);
+    return launch_batch(ctx, Exec{lane->stream, lane->flow}, lane->next_done(), jobs, dst_slots, n);
 }
 
 int hevcgpu_lane_sync(hevcgpu_lane_t* lane) {
