@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="short run for ncu captures")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving (Poisson) measurement")
+    ap.add_argument("--serve-seconds", type=float, default=6.0)
     return ap.parse_args()
 
 
@@ -526,6 +528,28 @@ def run_ours(args, hb, rank, world, local):
     }
     if cpu:
         line["cpu_baseline"] = cpu
+    if not args.no_serving and rank == 0 and W == W_DEFAULT and H == H_DEFAULT:
+        # the serving workload: 64 streams of mixed resolutions, Poisson segment arrivals
+        from hevc_b200 import serve
+        sctx = hb.Context(local)   # a serving process owns its context
+        pool = serve.PicturePool(hb, [(416, 240), (1280, 720), (1920, 1080), (3840, 2160)])
+        # an unmeasured 2 s run first: the first use of a context's pools and launch paths
+        # in a process costs once what a long-running server pays at start-up
+        serve.run_poisson(hb, sctx, seconds=2.0, n_streams=64, seed=5, lanes=4, pool=pool)
+        res = serve.run_poisson(hb, sctx, seconds=args.serve_seconds, n_streams=64, seed=4, lanes=4, pool=pool)
+        sctx.close()
+        line["serving"] = {
+            "workload": "64 live streams, 416x240 / 1280x720 / 1920x1080 / 3840x2160 in ratio 4:3:2:1, "
+                        "30 or 60 fps, 2-second segments (I picture, then P/B) arriving as a Poisson process "
+                        f"(seed 4) for {args.serve_seconds:g} s; 4 lanes, continuous batching",
+            "frames": res["frames"], "frames_per_s": round(res["frames_per_s"], 1),
+            "p50_ms": round(res["p50_ms"], 2), "p99_ms": round(res["p99_ms"], 2), "max_ms": round(res["max_ms"], 2),
+            "steady_p50_ms": round(res["steady_p50_ms"], 2), "steady_p99_ms": round(res["steady_p99_ms"], 2),
+            "steady": "frames released after the first 2 s, when every stream's first segment (and its "
+                      "I picture) has arrived",
+            "latency": "device completion of the picture's batch minus the picture's live release time "
+                       "(segment start + i / fps); records prepared on host workers, CABAC not included; "
+                       "measured after an unmeasured 2 s warm-up run on the same context"}
     for ln in lanes:
         ln.close()
     for st in streams:

@@ -499,6 +499,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     // residual bins (coded TUs by size) and the intra TUs in decode order
     std::vector<int32_t> bins[4];
     std::vector<int32_t> intra_list;
+    for (auto& v : bins) v.reserve((size_t)s->num_tus / 2);
+    intra_list.reserve((size_t)s->num_tus);
     for (int i = 0; i < s->num_tus; i++) {
         const hevc_tu_t& t = s->tus[i];
         bool intra = t.flags & HEVC_TU_INTRA;
@@ -519,12 +521,14 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     std::vector<IntraLevel> ictu_lvl;
     if (n_intra) {
         std::vector<int32_t> level((size_t)n_intra, 0), ctu_of((size_t)n_intra, 0);
-        std::vector<std::vector<int32_t>> ctu_deps((size_t)nctb);  // by CTU address
+        std::vector<int32_t> dep_list((size_t)nctb * 4, -1), dep_n((size_t)nctb, 0);   // by CTU address
+        std::vector<std::vector<int32_t>> ctu_deps((size_t)nctb);
         // cross-CTU requirements: (CTU, level, dependency CTU address, levels it must have done)
         struct Req { int32_t a, lv, dep, need; };
         std::vector<Req> reqs;
         std::vector<std::pair<int32_t, int32_t>> pending;           // (dep CTU, need) of one TU
         std::vector<std::vector<uint8_t>> publish((size_t)nctb);     // by CTU address and level
+        // owner maps: (CTU address << 16) | level of the latest intra TU per 4x4 unit, -1 none
         std::vector<int32_t> owner[3];
         int uw[3], uh[3];
         for (int c = 0; c < 3; c++) {
@@ -537,46 +541,76 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             const int c = t.c_idx, n = 1 << t.log2_size, sub = c ? 2 : 1;
             const int a = ((t.y * sub) >> p.log2_ctb) * wctb + ((t.x * sub) >> p.log2_ctb);
             ctu_of[(size_t)b] = a;
-            std::vector<int32_t>& own = owner[c];
+            int32_t* own = owner[c].data();
+            const int row = uw[c];
             int lv = 0;
-            auto dep = [&](int ux, int uy) {
-                const int o = own[(size_t)uy * uw[c] + ux];
+            auto dep = [&](int32_t o) {
                 if (o < 0) return;
-                const int oa = ctu_of[(size_t)o];
+                const int oa = o >> 16, ol = o & 0xFFFF;
                 if (oa == a) {
-                    lv = std::max(lv, level[(size_t)o] + 1);
-                } else {
-                    std::vector<int32_t>& dl = ctu_deps[(size_t)a];
-                    if (std::find(dl.begin(), dl.end(), oa) == dl.end()) dl.push_back(oa);
-                    pending.emplace_back(oa, level[(size_t)o] + 1);
-                    std::vector<uint8_t>& pb = publish[(size_t)oa];
-                    if (pb.size() <= (size_t)level[(size_t)o]) pb.resize((size_t)level[(size_t)o] + 1, 0);
-                    pb[(size_t)level[(size_t)o]] = 1;
+                    lv = std::max(lv, ol + 1);
+                    return;
                 }
+                int32_t* dl = &dep_list[(size_t)a * 4];
+                int& dn = dep_n[(size_t)a];
+                bool have = false;
+                for (int q = 0; q < dn; q++) have |= dl[q] == oa;
+                if (!have) {
+                    if (dn < 4) dl[dn] = oa;
+                    dn++;
+                }
+                pending.emplace_back(oa, ol + 1);
+                std::vector<uint8_t>& pb = publish[(size_t)oa];
+                if (pb.size() <= (size_t)ol) pb.resize((size_t)ol + 1, 0);
+                pb[(size_t)ol] = 1;
             };
             if (t.y > 0) {
-                const int uy = (t.y - 1) / 4;
-                const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(uw[c] - 1, (t.x + 2 * n - 1) / 4);
-                for (int ux = ux0; ux <= ux1; ux++) dep(ux, uy);
+                const int32_t* r = own + (size_t)((t.y - 1) / 4) * row;
+                const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(row - 1, (t.x + 2 * n - 1) / 4);
+                for (int ux = ux0; ux <= ux1; ux++) dep(r[ux]);
             }
             if (t.x > 0) {
                 const int ux = (t.x - 1) / 4;
                 const int uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
-                for (int uy = uy0; uy <= uy1; uy++) dep(ux, uy);
+                for (int uy = uy0; uy <= uy1; uy++) dep(own[(size_t)uy * row + ux]);
             }
+            if (lv > 0xFFFF) return fail(HEVCGPU_EINVAL, "intra dependency chain too deep in CTU %d", a);
             level[(size_t)b] = lv;
             for (const auto& pd : pending) reqs.push_back({a, lv, pd.first, pd.second});
             pending.clear();
-            for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++)
-                for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) own[(size_t)uy * uw[c] + ux] = b;
+            const int32_t mark = (a << 16) | lv;
+            for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++) {
+                int32_t* r = own + (size_t)uy * row;
+                for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) r[ux] = mark;
+            }
         }
-        // order by (CTU raster address, level, decode order)
+        for (int a = 0; a < nctb; a++) {
+            if (dep_n[(size_t)a] > 4) return fail(HEVCGPU_EINVAL, "CTU %d depends on %d CTUs", a, dep_n[(size_t)a]);
+            ctu_deps[(size_t)a].assign(&dep_list[(size_t)a * 4], &dep_list[(size_t)a * 4] + dep_n[(size_t)a]);
+        }
+        // order by (CTU raster address, level, decode order): the TUs come CTU by CTU in
+        // decode order, so a counting sort by level within each CTU's run keeps it stable
         std::vector<int32_t> order((size_t)n_intra);
-        for (int b = 0; b < n_intra; b++) order[(size_t)b] = b;
-        std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
-            if (ctu_of[(size_t)x] != ctu_of[(size_t)y]) return ctu_of[(size_t)x] < ctu_of[(size_t)y];
-            return level[(size_t)x] < level[(size_t)y];
-        });
+        bool grouped = true;
+        for (int b = 1; b < n_intra && grouped; b++) grouped = ctu_of[(size_t)b] >= ctu_of[(size_t)b - 1];
+        if (grouped) {
+            std::vector<int32_t> cnt;
+            for (int r0 = 0; r0 < n_intra;) {
+                int r1 = r0, maxl = 0;
+                while (r1 < n_intra && ctu_of[(size_t)r1] == ctu_of[(size_t)r0]) maxl = std::max(maxl, level[(size_t)r1++]);
+                cnt.assign((size_t)maxl + 2, 0);
+                for (int b = r0; b < r1; b++) cnt[(size_t)level[(size_t)b] + 1]++;
+                for (int l = 1; l <= maxl + 1; l++) cnt[(size_t)l] += cnt[(size_t)l - 1];
+                for (int b = r0; b < r1; b++) order[(size_t)(r0 + cnt[(size_t)level[(size_t)b]]++)] = b;
+                r0 = r1;
+            }
+        } else {
+            for (int b = 0; b < n_intra; b++) order[(size_t)b] = b;
+            std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+                if (ctu_of[(size_t)x] != ctu_of[(size_t)y]) return ctu_of[(size_t)x] < ctu_of[(size_t)y];
+                return level[(size_t)x] < level[(size_t)y];
+            });
+        }
         itu.resize((size_t)n_intra);
         itu_level_end.resize((size_t)n_intra);
         for (int i = 0; i < n_intra; i++) {

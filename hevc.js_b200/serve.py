@@ -4,7 +4,8 @@ The request loop of a decoding service built on the C-ABI.  Streams of different
 resolutions are admitted while their DPB slots and work buffers fit the context's HBM
 budget; each admitted stream's DPB stays resident and the stream is pinned to one lane
 (hevcgpu_lane_*), whose CUDA stream keeps its pictures in order.  Segments of pictures
-arrive over time; a picture is *released* at its live time (segment arrival + i / fps).
+arrive over time; a picture is *released* at its live time (segment start + i / fps, a
+segment starting at its arrival or when the stream's previous segment ends).
 Whenever a lane has room, the loop takes every stream of that lane whose next picture is
 released, prepares their records in one batched call on the host workers
 (hevcgpu_jobs_prepare) and launches them as one batch: pictures of many streams and
@@ -20,7 +21,9 @@ after it, two reference pictures in a three-slot DPB ring); CABAC parsing is not
 of this path and is not timed.
 """
 import collections
+import concurrent.futures
 import heapq
+import os
 import random
 
 import numpy as np
@@ -69,14 +72,16 @@ class PicturePool:
 
 
 class _Stream:
-    __slots__ = ("sid", "w", "h", "fps", "st", "lane", "queue", "n", "variant", "inflight")
+    __slots__ = ("sid", "w", "h", "fps", "st", "lane", "queue", "n", "n_queued", "variant", "inflight", "release_end")
 
     def __init__(self, sid, w, h, fps, st, lane, variant):
         self.sid, self.w, self.h, self.fps, self.st, self.lane = sid, w, h, fps, st, lane
-        self.queue = collections.deque()   # (n within segment, release time)
+        self.queue = collections.deque()   # [index in segment, release time, index in stream, prepared job]
         self.n = 0                          # pictures launched so far
+        self.n_queued = 0                   # pictures queued so far
         self.variant = variant
         self.inflight = 0
+        self.release_end = 0.0              # end of the release schedule of the queued segments
 
 
 class Server:
@@ -85,15 +90,26 @@ class Server:
     admit() opens a stream when its DPB and work buffers fit the budget (else False:
     the caller retries after streams close); add_segment() queues a segment's pictures
     with their release times; poll(now) launches and retires batches and returns the
-    latencies (seconds) of the pictures completed since the last call."""
+    latencies (seconds) of the pictures completed since the last call.
 
-    def __init__(self, hb, ctx, pool, lanes=2, max_batch=64, depth=2, budget_bytes=None, content_seed=7):
+    A picture's records are prepared (hevcgpu_job_prepare, on a pool of host threads) as
+    soon as its segment is queued, up to `lookahead` pictures ahead per stream: preparing
+    needs only the syntax, not the previous pictures, so launching never waits for it
+    unless the preparation is slower than the stream."""
+
+    def __init__(self, hb, ctx, pool, lanes=2, max_batch=64, depth=2, budget_bytes=None, content_seed=7,
+                 lookahead=4, prep_threads=None, min_batch=1, max_wait=0.0):
         import torch
         self.hb, self.ctx, self.pool = hb, ctx, pool
+        self.lookahead = lookahead
+        self.prep = concurrent.futures.ThreadPoolExecutor(max_workers=prep_threads or os.cpu_count() or 4)
         self.torch = torch
         self.lanes = [hb.Lane(ctx) for _ in range(lanes)]
         self.lane_cuda = [torch.cuda.ExternalStream(ln.cuda_stream) for ln in self.lanes]
         self.max_batch, self.depth = max_batch, depth
+        # a lane launches when min_batch pictures are ready or the oldest ready one has
+        # waited max_wait seconds since its release
+        self.min_batch, self.max_wait = min_batch, max_wait
         self.budget = budget_bytes
         if budget_bytes:
             ctx.set_budget(budget_bytes)
@@ -102,19 +118,23 @@ class Server:
         self.by_lane = [[] for _ in range(lanes)]
         self.inflight = [collections.deque() for _ in range(lanes)]
         self.frames_done = 0
+        self.batches = []   # (lane, pictures, launch time, completion time) of finished batches
+        self.records = []   # (release time, latency, stream id) of finished pictures
         # device clock -> host clock: a base event recorded when the loop starts
         self.base_ev = None
         self.base_host = None
 
     # ---- clock
-    def start_clock(self, now):
+    def start_clock(self, clock):
+        """Tie the device clock to the host clock `clock()`; returns the host time."""
         torch = self.torch
         torch.cuda.synchronize()
         self.ctx.sync()
         self.base_ev = torch.cuda.Event(enable_timing=True)
         self.base_ev.record(self.lane_cuda[0])
         self.base_ev.synchronize()
-        self.base_host = now
+        self.base_host = clock()
+        return self.base_host
 
     def _device_time(self, ev):
         return self.base_host + self.base_ev.elapsed_time(ev) / 1000.0
@@ -151,9 +171,36 @@ class Server:
         s.st.close()
 
     def add_segment(self, sid, arrival, n_pictures):
+        """Queue a segment.  A stream's segments follow each other in media time: frame i
+        is released at start + i / fps, where start is the segment's arrival, or the end
+        of the previous segment's frames if that is later (the segment arrived early and
+        waits in the buffer)."""
         s = self.streams[sid]
+        start = max(arrival, s.release_end)
         for i in range(n_pictures):
-            s.queue.append((i, arrival + i / s.fps))
+            s.queue.append([i, start + i / s.fps, s.n_queued, None])
+            s.n_queued += 1
+        s.release_end = start + n_pictures / s.fps
+        self._feed(s)
+
+    def _feed(self, s):
+        """Start the preparation of the stream's next `lookahead` queued pictures."""
+        for e in list(s.queue)[: self.lookahead]:
+            if e[3] is None:
+                pic = self.pool.picture(s.w, s.h, e[0], e[2], s.variant)
+                e[3] = self.prep.submit(self.hb.Job, s.st, pic)
+
+    def warm(self):
+        """Fill the context's device and pinned pools before serving: prepare the first
+        `lookahead` pictures of every stream (its I picture and P/B pictures) at once and
+        free them, so that the buffers the steady state needs are already allocated."""
+        futs = []
+        for s in self.streams.values():
+            for n in range(self.lookahead):
+                futs.append(self.prep.submit(self.hb.Job, s.st, self.pool.picture(s.w, s.h, n, n, s.variant)))
+        jobs = [f.result() for f in futs]
+        for j in jobs:
+            j.free()
 
     def pending(self):
         return sum(len(s.queue) for s in self.streams.values()) + sum(len(q) for q in self.inflight)
@@ -163,10 +210,12 @@ class Server:
         done = []
         for k, q in enumerate(self.inflight):
             while q and q[0][0].query():
-                ev, jobs, streams, releases = q.popleft()
+                ev, jobs, streams, releases, t_launch = q.popleft()
                 t_done = self._device_time(ev)
+                self.batches.append((k, len(jobs), t_launch, t_done))
                 for s, rel in zip(streams, releases):
                     done.append(t_done - rel)
+                    self.records.append((rel, t_done - rel, s.sid))
                     s.inflight -= 1
                 for j in jobs:
                     j.free()
@@ -174,26 +223,28 @@ class Server:
         for k, lane in enumerate(self.lanes):
             if len(self.inflight[k]) >= self.depth:
                 continue
-            ready = [s for s in self.by_lane[k] if s.queue and s.queue[0][1] <= now]
+            ready = [s for s in self.by_lane[k]
+                     if s.queue and s.queue[0][1] <= now and s.queue[0][3] is not None and s.queue[0][3].done()]
             if not ready:
                 continue
             ready.sort(key=lambda s: s.queue[0][1])   # oldest release first
+            if len(ready) < self.min_batch and now - ready[0].queue[0][1] < self.max_wait:
+                continue
             ready = ready[: self.max_batch]
-            pics, sts, slots, releases = [], [], [], []
+            jobs, slots, releases = [], [], []
             for s in ready:   # picture n of a stream writes slot n % SLOTS
-                i, rel = s.queue.popleft()
-                pics.append(self.pool.picture(s.w, s.h, i, s.n, s.variant))
-                sts.append(s.st)
-                slots.append(s.n % SLOTS)
+                i, rel, n, fut = s.queue.popleft()
+                jobs.append(fut.result())
+                slots.append(n % SLOTS)
                 releases.append(rel)
-            jobs = self.hb.prepare_batch(sts, pics)
+                self._feed(s)
             lane.batch_launch(jobs, slots)
             ev = self.torch.cuda.Event(enable_timing=True)
             ev.record(self.lane_cuda[k])
             for s in ready:
                 s.n += 1
                 s.inflight += 1
-            self.inflight[k].append((ev, jobs, ready, releases))
+            self.inflight[k].append((ev, jobs, ready, releases, now))
         return done
 
     def drain(self):
@@ -202,37 +253,43 @@ class Server:
 
     def close(self):
         self.drain()
+        self.prep.shutdown(wait=True)
+        for s in self.streams.values():   # prepared, never launched
+            for e in s.queue:
+                if e[3] is not None:
+                    e[3].result().free()
         for sid in list(self.streams):
             self.close_stream(sid)
         for ln in self.lanes:
             ln.close()
 
 
-def run_poisson(hb, ctx, seconds=5.0, n_streams=64, seed=4, lanes=2, max_batch=64, pool=None,
+def run_poisson(hb, ctx, seconds=5.0, n_streams=64, seed=4, lanes=4, max_batch=64, pool=None,
                 resolutions=((416, 240), (1280, 720), (1920, 1080), (3840, 2160)), ratio=(4, 3, 2, 1),
-                segment_s=2.0, clock=None):
-    """Serve n_streams for `seconds` of wall time: resolutions in `ratio`, 30 or 60 fps,
-    2-second segments arriving as a Poisson process per stream (mean gap = segment length,
-    so each stream offers real-time load).  Returns latencies and throughput."""
+                segment_s=2.0, clock=None, min_batch=8, max_wait=0.004):
+    """Serve n_streams whose segments arrive for `seconds` of wall time (the run ends when
+    every queued frame is decoded): resolutions in `ratio`, 30 or 60 fps, 2-second
+    segments arriving as a Poisson process per stream (mean gap = segment length, so each
+    stream offers real-time load).  Returns per-frame latency percentiles (device
+    completion minus release) and the frames/s served."""
     import time
     clock = clock or time.perf_counter
     rng = random.Random(seed)
     if pool is None:
         pool = PicturePool(hb, resolutions)
-    srv = Server(hb, ctx, pool, lanes=lanes, max_batch=max_batch)
+    srv = Server(hb, ctx, pool, lanes=lanes, max_batch=max_batch, min_batch=min_batch, max_wait=max_wait)
     mix = [r for r, k in zip(resolutions, ratio) for _ in range(k)]
     specs = []
     for sid in range(n_streams):
         w, h = mix[sid % len(mix)]
         fps = rng.choice((30, 60))
         specs.append((sid, w, h, fps))
-    t0 = clock()
-    srv.start_clock(t0)
-    arrivals = []   # (time, sid)
-    for sid, w, h, fps in specs:
-        if not srv.admit(sid, w, h, fps, variant=sid):
-            continue
-        heapq.heappush(arrivals, (t0 + rng.expovariate(1.0 / segment_s) * 0.5, sid))
+    admitted = [sid for sid, w, h, fps in specs if srv.admit(sid, w, h, fps, variant=sid)]
+    srv.warm()
+    t0 = srv.start_clock(clock)   # streams are open and their DPBs resident before the clock starts
+    arrivals = []   # (time, sid): each stream's first segment within the first segment length
+    for sid in admitted:
+        heapq.heappush(arrivals, (t0 + rng.uniform(0.0, segment_s), sid))
     lat = []
     offered = 0
     t_end = t0 + seconds
@@ -249,9 +306,14 @@ def run_poisson(hb, ctx, seconds=5.0, n_streams=64, seed=4, lanes=2, max_batch=6
         if now >= t_end and srv.pending() == 0:
             break
     t_stop = clock()
+    records = np.array([(r[0], r[1]) for r in srv.records]) if srv.records else np.zeros((0, 2))
     srv.close()
     lat_ms = np.array(lat) * 1000.0
-    return {"streams": len(specs), "frames": int(len(lat)), "offered_frames": offered,
-            "frames_per_s": len(lat) / (t_stop - t0), "p50_ms": float(np.percentile(lat_ms, 50)) if len(lat) else None,
-            "p99_ms": float(np.percentile(lat_ms, 99)) if len(lat) else None,
-            "max_ms": float(lat_ms.max()) if len(lat) else None, "wall_s": t_stop - t0}
+    # steady state: frames released after every stream's first segment has started (the
+    # first segments, each opening with an I picture, all arrive within segment_s)
+    steady = records[records[:, 0] >= t0 + segment_s, 1] * 1000.0 if len(records) else np.zeros(0)
+    pct = lambda v, q: float(np.percentile(v, q)) if len(v) else None
+    return {"streams": len(admitted), "frames": int(len(lat)), "offered_frames": offered,
+            "frames_per_s": len(lat) / (t_stop - t0), "p50_ms": pct(lat_ms, 50), "p99_ms": pct(lat_ms, 99),
+            "max_ms": float(lat_ms.max()) if len(lat) else None, "steady_frames": int(len(steady)),
+            "steady_p50_ms": pct(steady, 50), "steady_p99_ms": pct(steady, 99), "wall_s": t_stop - t0}

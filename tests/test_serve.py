@@ -11,7 +11,7 @@ def test_served_streams_match_streams_decoded_alone(hb, gpu_ctx):
     res = [(208, 120), (416, 240), (320, 176)]
     pool = serve.PicturePool(hb, res, variants=2)
     srv = serve.Server(hb, gpu_ctx, pool, lanes=2, max_batch=8)
-    srv.start_clock(0.0)
+    srv.start_clock(lambda: 0.0)
     specs = [(0, 208, 120), (1, 416, 240), (2, 320, 176), (3, 208, 120), (4, 416, 240)]
     segments = {sid: [7] for sid, _, _ in specs}
     segments[0] = [4, 5]          # two segments: a second I picture mid-stream
