@@ -75,7 +75,7 @@ struct PicDesc {
 };
 
 // Work items ----------------------------------------------------------------------------
-// Residual items are TU indices (int32); motion-compensation items are McBlock (mc.cuh).
+// Residual items are TU indices (int32); motion-compensation items are packed strips (mc_item, mc.cuh).
 
 // A launch covers up to MAX_SEGS pictures.  Segment k owns the blocks
 // [block0, next block0) of an item-list launch, or blockIdx.y == k of a per-picture

@@ -372,8 +372,8 @@ struct hevcgpu_job {
     PicDesc host_desc{};
     int32_t n_res[4] = {0, 0, 0, 0};
     const int32_t* d_res[4] = {nullptr, nullptr, nullptr, nullptr};
-    int32_t n_mc[2] = {0, 0};            // luma blocks, chroma blocks
-    const McBlock* d_mc[2] = {nullptr, nullptr};
+    int32_t n_mc[2] = {0, 0};            // luma strips, chroma strips (mc.cuh items)
+    const uint32_t* d_mc[2] = {nullptr, nullptr};
     int32_t n_ictu = 0;                 // CTUs that hold intra TUs
     int32_t epoch = 0;                  // intra launches of this job so far
     int32_t n_pus = 0;
@@ -444,6 +444,7 @@ int validate(const hevc_picture_syntax_t* s, bool need_tus, bool need_pus, bool 
     }
     if (need_pus) {
         if (s->num_pus < 0 || (s->num_pus && !s->pus)) return fail(HEVCGPU_EINVAL, "bad PU array");
+        if (s->num_pus > MC_MAX_PUS) return fail(HEVCGPU_EINVAL, "%d PUs, at most %d", s->num_pus, MC_MAX_PUS);
         for (int i = 0; i < s->num_pus; i++) {
             const hevc_pu_t& u = s->pus[i];
             if (u.w < 4 || u.h < 4 || u.w > 64 || u.h > 64 || (u.w & 3) || (u.h & 3) || (u.x & 3) || (u.y & 3) ||
@@ -687,41 +688,51 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         }
     }
     j->n_ictu = (int32_t)ictu_addr.size();
-    // MC blocks: up to 16 x 16 luma / 8 x 8 chroma of one PU, one warp each; luma and
-    // chroma (Cb and Cr together) are two lists, each ordered bi- before uni-predicted
-    // PUs, then by block area (larger first), so that the warps of a CTA finish together.
-    std::vector<McBlock> mc[2];
+    // MC strips: 4 columns x up to 16 rows of one PU in one plane, one thread each; luma
+    // and chroma (Cb and Cr strips) are two lists, each ordered by class: bi-predicted
+    // first, then windows inside the picture first, then taller first, so that the
+    // threads of a warp share their path and row count; PU order inside a class.
+    std::vector<uint32_t> mc[2];
     if (stages & ST_MC) {
-        // counting sort on the key (bi ? 0 : 32) + (31 - (area - 1) / 8), stable in PU order
         for (int c = 0; c < 2; c++) {
-            const int B = c ? MC_BLOCK_CHROMA : MC_BLOCK_LUMA, area_shift = c ? 1 : 3;
-            int32_t cnt[65] = {};
-            auto each_block = [&](auto&& emit) {
+            const bool chroma = c == 1;
+            const int sub = chroma ? 2 : 1, pw = W / sub, ph = H / sub;
+            const int pitch = chroma ? j->lay.pitch_c : j->lay.pitch_y;
+            const int nrow = chroma ? 8 : 4;   // row classes: rows / 2 (chroma) or rows / 4 (luma)
+            const int ncls = 4 * nrow;
+            int32_t cnt[33] = {};
+            auto each_strip = [&](auto&& emit) {
                 for (int i = 0; i < s->num_pus; i++) {
                     const hevc_pu_t& u = s->pus[i];
-                    const int key0 = (u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0) ? 0 : 32;
-                    const int w = c ? u.w / 2 : u.w, h = c ? u.h / 2 : u.h;
-                    for (int by = 0; by < h; by += B) {
-                        const int bh = std::min(B, h - by);
-                        for (int bx = 0; bx < w; bx += B) {
-                            const int bw = std::min(B, w - bx);
-                            emit(key0 + 31 - std::min(31, (bw * bh - 1) >> area_shift), i, bx, by, bw, bh);
-                        }
+                    const bool bi = u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0;
+                    const int w = u.w / sub, h = u.h / sub, x = u.x / sub, y = u.y / sub;
+                    // list windows at the PU's top-left, extended over the PU: a strip is
+                    // inside when every list's window of the whole PU is
+                    bool inside = true;
+                    for (int l = 0; l < 2; l++) {
+                        if (u.ref_idx[l] < 0) continue;
+                        const int mvx = u.mv[l][0], mvy = u.mv[l][1];
+                        const int x0 = x + (chroma ? (mvx >> 3) : (mvx >> 2)) - (chroma ? 1 : 3);
+                        const int y0 = y + (chroma ? (mvy >> 3) : (mvy >> 2)) - (chroma ? 1 : 3);
+                        inside = inside && (chroma ? mc_inside<true>(x0, y0, h, pw, ph, pitch) &&
+                                                         mc_inside<true>(x0 + ((w - 1) & ~3), y0, h, pw, ph, pitch)
+                                                   : mc_inside<false>(x0, y0, h, pw, ph, pitch) &&
+                                                         mc_inside<false>(x0 + ((w - 1) & ~3), y0, h, pw, ph, pitch));
+                    }
+                    const int key0 = (bi ? 0 : 2 * nrow) + (inside ? 0 : nrow);
+                    for (int sy = 0; sy < h; sy += MC_STRIP_ROWS) {
+                        const int rows = std::min(MC_STRIP_ROWS, h - sy);
+                        const int key = key0 + nrow - (chroma ? rows / 2 : rows / 4);
+                        for (int pl = 0; pl < (chroma ? 2 : 1); pl++)
+                            for (int sx = 0; sx < w; sx += 4) emit(key, mc_item(i, sx, sy, rows, chroma, pl));
                     }
                 }
             };
-            each_block([&](int key, int, int, int, int, int) { cnt[key + 1]++; });
-            for (int k = 1; k <= 64; k++) cnt[k] += cnt[k - 1];
-            mc[c].resize((size_t)cnt[64]);
-            McBlock* out = mc[c].data();
-            each_block([&](int key, int i, int bx, int by, int bw, int bh) {
-                McBlock& m = out[cnt[key]++];
-                m.pu = i;
-                m.bx = (uint8_t)bx;
-                m.by = (uint8_t)by;
-                m.bw = (uint8_t)bw;
-                m.bh = (uint8_t)bh;
-            });
+            each_strip([&](int key, uint32_t) { cnt[key + 1]++; });
+            for (int k = 1; k <= ncls; k++) cnt[k] += cnt[k - 1];
+            mc[c].resize((size_t)cnt[ncls]);
+            uint32_t* out = mc[c].data();
+            each_strip([&](int key, uint32_t item) { out[cnt[key]++] = item; });
         }
     }
     j->n_pus = s->num_pus;
@@ -741,7 +752,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         o_slices = s->num_slices > 0 && s->slices ? pk.add(s->slices, sizeof(hevc_slice_t) * (size_t)s->num_slices)
                                                   : pk.add(&dflt, sizeof(dflt));
         for (int k = 0; k < 4; k++) o_res[k] = pk.add(bins[k].data(), sizeof(int32_t) * bins[k].size());
-        for (int c = 0; c < 2; c++) o_mc[c] = pk.add(mc[c].data(), sizeof(McBlock) * mc[c].size());
+        for (int c = 0; c < 2; c++) o_mc[c] = pk.add(mc[c].data(), sizeof(uint32_t) * mc[c].size());
         o_ia = pk.add(ictu_addr.data(), sizeof(int32_t) * ictu_addr.size());
         o_idp = pk.add(ictu_deps.data(), sizeof(int32_t) * ictu_deps.size());
         o_ito = pk.add(ictu_tu_off.data(), sizeof(int32_t) * ictu_tu_off.size());
@@ -835,7 +846,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     }
     for (int c = 0; c < 2; c++) {
         j->n_mc[c] = (int32_t)mc[c].size();
-        j->d_mc[c] = reinterpret_cast<const McBlock*>(base + o_mc[c]);
+        j->d_mc[c] = reinterpret_cast<const uint32_t*>(base + o_mc[c]);
     }
     return HEVCGPU_OK;
 }
@@ -963,12 +974,12 @@ int run_stages(hevcgpu_ctx* ctx, const Exec& ex, hevcgpu_job* const* jobs, int n
     }
     if (stages & ST_MC) {
         StageMark m(ctx, ex.stream, 1);
-        rc = L.items(k_mc<false>, jobs, n, MC_WARPS, MC_WARPS * 32, [](hevcgpu_job* j, const void*& p, int& c) {
+        rc = L.items(k_mc<false>, jobs, n, MC_THREADS, MC_THREADS, [](hevcgpu_job* j, const void*& p, int& c) {
             p = j->d_mc[0];
             c = j->n_mc[0];
         });
         if (rc) return rc;
-        rc = L.items(k_mc<true>, jobs, n, MC_WARPS, MC_WARPS * 32, [](hevcgpu_job* j, const void*& p, int& c) {
+        rc = L.items(k_mc<true>, jobs, n, MC_THREADS, MC_THREADS, [](hevcgpu_job* j, const void*& p, int& c) {
             p = j->d_mc[1];
             c = j->n_mc[1];
         });
