@@ -20,13 +20,21 @@ struct MotionEnt {           // 4x4 motion grid entry (PUMotionInfo, inter_predi
     int16_t pad;
 };
 
-// One level of an intra CTU task: req[d] > 0 means "dependency slot d must have completed
-// req[d] levels before this level runs" (only where the requirement rises); bit 15 of
-// req[0] (INTRA_LEVEL_PUBLISH) means other CTUs wait for this level's completion.
+// One level of an intra CTU task, packed in 8 bytes (staged into shared memory):
+// req(d) > 0 means "dependency slot d must have completed req(d) levels before this level
+// runs" (only where the requirement rises); publish means other CTUs wait for this level's
+// completion; end is the first task entry of the next level, counted from the CTU's first.
+// Fields of 10 bits: x = req(0) | req(1) << 10 | req(2) << 20 | publish << 31,
+// y = req(3) | end << 10.
 struct IntraLevel {
-    uint16_t req[4];
+    uint32_t x, y;
 };
-constexpr uint16_t INTRA_LEVEL_PUBLISH = 0x8000u;
+constexpr uint32_t INTRA_LEVEL_PUBLISH = 0x80000000u;
+constexpr int INTRA_FIELD_MAX = 1023;
+__host__ __device__ __forceinline__ int intra_req(const IntraLevel& e, int d) {
+    return (int)((d < 3 ? e.x >> (10 * d) : e.y) & 0x3FFu);
+}
+__host__ __device__ __forceinline__ int intra_end(const IntraLevel& e) { return (int)((e.y >> 10) & 0x3FFu); }
 
 struct PicDesc {
     int32_t width, height;               // luma
@@ -53,8 +61,8 @@ struct PicDesc {
     const int32_t* ictu_addr;            // raster address of intra CTU k
     const int32_t* ictu_deps;            // 4 per intra CTU: intra CTUs it reads from, or -1
     const int32_t* ictu_tu_off;          // TUs of intra CTU k: itu[ictu_tu_off[k] .. [k+1])
-    const hevc_tu_t* itu_rec;            // TU records in task order
-    const int32_t* itu_level_end;        // first entry of the next level of the same CTU
+    const hevc_tu_t* itu_rec;            // TU records in task order; coeff_offset holds the
+                                         // offset of the TU's residual in the CTU's staged ones
     const int4* itu_res;                 // per task entry: residual source offset (-1: none),
                                          // offset in the CTU's staged residuals, 16-byte chunks
     const int32_t* ictu_lvl_off;         // levels of intra CTU k: ictu_lvl[ictu_lvl_off[k] ..]

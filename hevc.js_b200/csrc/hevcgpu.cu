@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <condition_variable>
 #include <cstdarg>
@@ -516,7 +517,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     // for that CTU.  A unit whose samples B may not use (availability) can only add an
     // unneeded level or wait, never change a sample.
     const int n_intra = (int)intra_list.size();
-    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, itu, itu_level_end, ictu_lvl_off;
+    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, itu, ictu_lvl_off;
     std::vector<hevc_tu_t> itu_rec;     // intra TU records in task order
     std::vector<int4> itu_res;          // per task entry: residual source, staged offset, 16-byte chunks
     std::vector<IntraLevel> ictu_lvl;
@@ -613,7 +614,6 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             });
         }
         itu.resize((size_t)n_intra);
-        itu_level_end.resize((size_t)n_intra);
         for (int i = 0; i < n_intra; i++) {
             const int b = order[(size_t)i];
             itu[(size_t)i] = intra_list[(size_t)b];
@@ -623,13 +623,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             }
         }
         ictu_tu_off.push_back(n_intra);
-        for (int i = n_intra - 1; i >= 0; i--) {
-            const int b = order[(size_t)i];
-            const bool last = i == n_intra - 1 || ctu_of[(size_t)order[(size_t)i + 1]] != ctu_of[(size_t)b] ||
-                              level[(size_t)order[(size_t)i + 1]] != level[(size_t)b];
-            itu_level_end[(size_t)i] = last ? i + 1 : itu_level_end[(size_t)i + 1];
-        }
-        // residual offsets inside each CTU's staged residuals (coded TUs, in itu order)
+        // residual offsets inside each CTU's staged residuals (coded TUs, in itu order); the
+        // task-order record carries its TU's offset there in coeff_offset
         itu_res.assign((size_t)n_intra, make_int4(-1, 0, 0, 0));
         itu_rec.resize((size_t)n_intra);
         const int nic = (int)ictu_addr.size();
@@ -637,10 +632,13 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             int acc = 0;
             for (int i = ictu_tu_off[(size_t)k]; i < ictu_tu_off[(size_t)k + 1]; i++) {
                 const hevc_tu_t& t = s->tus[itu[(size_t)i]];
-                itu_rec[(size_t)i] = t;
+                hevc_tu_t& r = itu_rec[(size_t)i];
+                r = t;
+                r.coeff_offset = 0;
                 if (!(t.flags & HEVC_TU_CODED)) continue;
                 const int nn = 1 << (2 * t.log2_size);
                 itu_res[(size_t)i] = make_int4((int)t.coeff_offset, acc, nn / 8, 0);
+                r.coeff_offset = (uint32_t)acc;
                 acc += nn;
             }
             if (acc > IC_MAX_RES || ictu_tu_off[(size_t)k + 1] - ictu_tu_off[(size_t)k] > IC_MAX_TUS)
@@ -666,24 +664,36 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             ictu_lvl_off[(size_t)k] = k ? ictu_lvl_off[(size_t)k - 1] + nlev[(size_t)k - 1] : 0;
         }
         ictu_lvl_off[(size_t)nic] = nic ? ictu_lvl_off[(size_t)nic - 1] + nlev[(size_t)nic - 1] : 0;
-        ictu_lvl.assign((size_t)ictu_lvl_off[(size_t)nic], IntraLevel{{0, 0, 0, 0}});
+        const size_t nlv = (size_t)ictu_lvl_off[(size_t)nic];
+        std::vector<std::array<uint16_t, 4>> req(nlv, std::array<uint16_t, 4>{0, 0, 0, 0});
         for (const Req& r : reqs) {
             const int k = index_of[(size_t)r.a];
             const std::vector<int32_t>& dl = ctu_deps[(size_t)r.a];
             const int slot = (int)(std::find(dl.begin(), dl.end(), r.dep) - dl.begin());
-            uint16_t& q = ictu_lvl[(size_t)(ictu_lvl_off[(size_t)k] + r.lv)].req[slot];
+            uint16_t& q = req[(size_t)(ictu_lvl_off[(size_t)k] + r.lv)][(size_t)slot];
             q = (uint16_t)std::max<int>(q, r.need);
         }
+        // one padding entry: the kernel stages levels in 16-byte pairs from an even entry
+        ictu_lvl.assign(nlv + 1, IntraLevel{0u, 0u});
         for (int k = 0; k < nic; k++) {
             uint16_t seen[4] = {0, 0, 0, 0};
             const std::vector<uint8_t>& pb = publish[(size_t)ictu_addr[(size_t)k]];
+            const int t0 = ictu_tu_off[(size_t)k], t1 = ictu_tu_off[(size_t)k + 1];
+            int i = t0;
             for (int L = 0; L < nlev[(size_t)k]; L++) {
-                IntraLevel& e = ictu_lvl[(size_t)(ictu_lvl_off[(size_t)k] + L)];
+                std::array<uint16_t, 4>& rq = req[(size_t)(ictu_lvl_off[(size_t)k] + L)];
                 for (int q = 0; q < 4; q++) {
-                    if (e.req[q] > seen[q]) seen[q] = e.req[q];
-                    else e.req[q] = 0;   // already satisfied by an earlier check
+                    if (rq[(size_t)q] > seen[q]) seen[q] = rq[(size_t)q];
+                    else rq[(size_t)q] = 0;   // already satisfied by an earlier check
                 }
-                if ((size_t)L < pb.size() && pb[(size_t)L]) e.req[0] |= INTRA_LEVEL_PUBLISH;
+                while (i < t1 && level[(size_t)order[(size_t)i]] == L) i++;
+                if (i - t0 > INTRA_FIELD_MAX || rq[0] > INTRA_FIELD_MAX || rq[1] > INTRA_FIELD_MAX ||
+                    rq[2] > INTRA_FIELD_MAX || rq[3] > INTRA_FIELD_MAX)
+                    return fail(HEVCGPU_EINVAL, "CTU %d intra schedule out of range", ictu_addr[(size_t)k]);
+                IntraLevel& e = ictu_lvl[(size_t)(ictu_lvl_off[(size_t)k] + L)];
+                e.x = (uint32_t)rq[0] | ((uint32_t)rq[1] << 10) | ((uint32_t)rq[2] << 20);
+                e.y = (uint32_t)rq[3] | ((uint32_t)(i - t0) << 10);
+                if ((size_t)L < pb.size() && pb[(size_t)L]) e.x |= INTRA_LEVEL_PUBLISH;
             }
         }
     }
@@ -738,7 +748,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     j->n_pus = s->num_pus;
 
     size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc[2], o_ia, o_idp, o_ito,
-        o_itu, o_ile, o_iro, o_ilo, o_ilv;
+        o_itu, o_iro, o_ilo, o_ilv;
     hevc_slice_t dflt{0, 0, 0, 1};
     auto pack = [&](Packer& pk) {
         o_tus = pk.add(s->tus, sizeof(hevc_tu_t) * (size_t)std::max(0, s->num_tus));
@@ -757,7 +767,6 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         o_idp = pk.add(ictu_deps.data(), sizeof(int32_t) * ictu_deps.size());
         o_ito = pk.add(ictu_tu_off.data(), sizeof(int32_t) * ictu_tu_off.size());
         o_itu = pk.add(itu_rec.data(), sizeof(hevc_tu_t) * itu_rec.size());
-        o_ile = pk.add(itu_level_end.data(), sizeof(int32_t) * itu_level_end.size());
         o_iro = pk.add(itu_res.data(), sizeof(int4) * itu_res.size());
         o_ilo = pk.add(ictu_lvl_off.data(), sizeof(int32_t) * ictu_lvl_off.size());
         o_ilv = pk.add(ictu_lvl.data(), sizeof(IntraLevel) * ictu_lvl.size());
@@ -811,7 +820,6 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     D.ictu_deps = reinterpret_cast<const int32_t*>(base + o_idp);
     D.ictu_tu_off = reinterpret_cast<const int32_t*>(base + o_ito);
     D.itu_rec = reinterpret_cast<const hevc_tu_t*>(base + o_itu);
-    D.itu_level_end = reinterpret_cast<const int32_t*>(base + o_ile);
     D.itu_res = reinterpret_cast<const int4*>(base + o_iro);
     D.ictu_lvl_off = reinterpret_cast<const int32_t*>(base + o_ilo);
     D.ictu_lvl = reinterpret_cast<const IntraLevel*>(base + o_ilv);

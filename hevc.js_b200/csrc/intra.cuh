@@ -29,9 +29,7 @@ __constant__ int16_t c_inv_angle[35] = {0,    0,    256, 315, 390, 482,  630,  9
                                         1638, 4096, 0,   4096, 1638, 910, 630, 482,  390,  315,  256};
 
 struct IntraWarpSmem {
-    int16_t raw[129];  // reference samples as read (0 where unavailable)
-    int16_t s[129];    // after substitution: bottom-left .. corner (index 2n) .. top-right
-    int16_t f[129];    // after smoothing
+    int16_t s[129];    // final references: bottom-left .. corner (index 2n) .. top-right
     int16_t m[130];    // angular main reference m[q + n], q = -n .. 2n (+1 padding entry)
 };
 
@@ -70,11 +68,12 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
     //    of the 4x4 luma unit (intra_prediction.cpp:102-133).  Index i runs from the
     //    bottom-left sample (0) through the corner (2n) to the top-right one (4n).
     uint32_t mask[R];
+    int val[R];
 #pragma unroll
     for (int r = 0; r < R; r++) {
         const int i = lane + 32 * r;
         bool ok = false;
-        int val = 0;
+        int v = 0;
         if (i < total) {
             int px, py;
             if (i < 2 * n) { px = xc - 1; py = yc + 2 * n - 1 - i; }
@@ -97,97 +96,129 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
                 if (ok) {
                     // samples of other CTUs come from the picture through L2 (those CTUs
                     // published them before this level), this CTU's from the tile
-                    val = outside ? __ldcg(plane + (int64_t)py * pitch + px)
-                                  : tile.t[(py - tile.y0) * tile.pitch + (px - tile.x0)];
+                    v = outside ? __ldcg(plane + (int64_t)py * pitch + px)
+                                : tile.t[(py - tile.y0) * tile.pitch + (px - tile.x0)];
                 }
             }
-            W.raw[i] = (int16_t)val;
         }
+        val[r] = v;
         mask[r] = __ballot_sync(0xffffffffu, ok);
     }
-    __syncwarp();
+    // Phases 2-4 keep the reference array in registers, element i in lane i % 32 of round
+    // i / 32, and move elements between lanes with shuffles: fetch(a, j) gives every lane
+    // element j of its own choosing, fetch_at(a, J) element J (the same in all lanes).
+    auto fetch = [&](const int (&a)[R], int j) {
+        int v = 0;
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            const int tq = __shfl_sync(0xffffffffu, a[q], j & 31);
+            if ((j >> 5) == q) v = tq;
+        }
+        return v;
+    };
+    auto fetch_at = [&](const int (&a)[R], int J) { return __shfl_sync(0xffffffffu, a[J >> 5], J & 31); };
+
     // 2. substitution (:177-197): an unavailable sample takes the nearest available one
     //    below it in the array, or the first available one; none available -> 128
+    constexpr uint32_t LAST_LANES = (total & 31) ? ((1u << (total & 31)) - 1u) : 0xffffffffu;
+    bool all = true;
     int first = -1;
 #pragma unroll
-    for (int r = 0; r < R; r++)
-        if (first < 0 && mask[r]) first = 32 * r + __ffs(mask[r]) - 1;
-#pragma unroll
     for (int r = 0; r < R; r++) {
-        const int i = lane + 32 * r;
-        if (i >= total) continue;
-        int v;
-        if (first < 0) v = 128;
-        else if ((mask[r] >> lane) & 1u) v = W.raw[i];
-        else {
-            int j = -1;
-            const uint32_t m = lane ? (mask[r] & ((1u << lane) - 1u)) : 0u;
-            if (m) j = 32 * r + 31 - __clz(m);
+        all = all && mask[r] == (r == R - 1 ? LAST_LANES : 0xffffffffu);
+        if (first < 0 && mask[r]) first = 32 * r + __ffs(mask[r]) - 1;
+    }
+    int s[R];
+    if (all) {
+#pragma unroll
+        for (int r = 0; r < R; r++) s[r] = val[r];
+    } else if (first < 0) {
+#pragma unroll
+        for (int r = 0; r < R; r++) s[r] = 128;
+    } else {
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const uint32_t below = mask[r] & ((1u << lane) - 1u);
+            int j = below ? 32 * r + 31 - __clz(below) : -1;
 #pragma unroll
             for (int q = r - 1; q >= 0; q--)
                 if (j < 0 && mask[q]) j = 32 * q + 31 - __clz(mask[q]);
-            v = W.raw[j < 0 ? first : j];
+            if ((mask[r] >> lane) & 1u) j = lane + 32 * r;
+            else if (j < 0) j = first;
+            s[r] = fetch(val, j);
         }
-        W.s[i] = (int16_t)v;
     }
-    __syncwarp();
     // 3. smoothing of luma references (:217-257, :443-471): [1 2 1] over the linear array
     //    (which also gives the corner filter), or the bilinear strong smoothing of 32x32
     const int mode = t.intra_mode;
-    const int16_t* R_ = W.s;
+    int f[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) f[r] = s[r];
     if constexpr (!CHROMA && n != 4) {
         constexpr int thr = n == 8 ? 7 : (n == 16 ? 1 : 0);
         const int d = min(abs(mode - 26), abs(mode - 10));
         if (!P.intra_smoothing_disabled && mode != 1 && d > thr) {
+            const int c = fetch_at(s, 2 * n), e_top = fetch_at(s, 4 * n), e_left = fetch_at(s, 0);
             bool bil = false;
             if constexpr (n == 32) {
-                if (P.strong_intra) {
-                    const int c = W.s[2 * n];
-                    bil = abs(c + W.s[4 * n] - 2 * W.s[3 * n]) < 8 && abs(c + W.s[0] - 2 * W.s[n]) < 8;
-                }
+                if (P.strong_intra)
+                    bil = abs(c + e_top - 2 * fetch_at(s, 3 * n)) < 8 && abs(c + e_left - 2 * fetch_at(s, n)) < 8;
             }
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const int i = lane + 32 * r;
-                if (i >= total) continue;
-                int v;
-                if (i == 0 || i == 4 * n) v = W.s[i];
-                else if (bil) {
-                    if (i == 2 * n) v = W.s[i];
-                    else if (i > 2 * n) { const int k = i - 2 * n; v = ((2 * n - k) * W.s[2 * n] + k * W.s[4 * n] + n) >> (LOG2 + 1); }
-                    else { const int k = 2 * n - i; v = ((2 * n - k) * W.s[2 * n] + k * W.s[0] + n) >> (LOG2 + 1); }
-                } else {
-                    v = (W.s[i - 1] + 2 * W.s[i] + W.s[i + 1] + 2) >> 2;
+                int prev = __shfl_up_sync(0xffffffffu, s[r], 1), next = __shfl_down_sync(0xffffffffu, s[r], 1);
+                if (r > 0) {
+                    const int pl = __shfl_sync(0xffffffffu, s[r > 0 ? r - 1 : 0], 31);
+                    if (lane == 0) prev = pl;
                 }
-                W.f[i] = (int16_t)v;
+                if (r + 1 < R) {
+                    const int nf = __shfl_sync(0xffffffffu, s[r + 1 < R ? r + 1 : r], 0);
+                    if (lane == 31) next = nf;
+                }
+                if (i == 0 || i >= 4 * n) f[r] = s[r];
+                else if (bil) {
+                    if (i == 2 * n) f[r] = s[r];
+                    else if (i > 2 * n) { const int k = i - 2 * n; f[r] = ((2 * n - k) * c + k * e_top + n) >> (LOG2 + 1); }
+                    else { const int k = 2 * n - i; f[r] = ((2 * n - k) * c + k * e_left + n) >> (LOG2 + 1); }
+                } else {
+                    f[r] = (prev + 2 * s[r] + next + 2) >> 2;
+                }
             }
-            __syncwarp();
-            R_ = W.f;
         }
     }
-    // 4. prediction (top[k] = R_[2n + k], left[k] = R_[2n - k]) + residual, clip, store.
-    //    Each lane takes groups of 4 samples of a row; its column x0 = 4 * (lane % (n / 4))
-    //    is the same for all its groups, so column terms are computed once.
-    constexpr int GPR = n / 4, NG = n * n / 4, G_PER_LANE = (NG + 31) / 32;
+    // 4. the final references to shared memory (top[k] = R_[2n + k], left[k] = R_[2n - k])
+    //    and, for the angular modes, the main reference with the side reference projected
+    //    through invAngle (:346-368): m[q + n] = top[q] (vertical) / left[q] (horizontal)
+    //    for q >= 0, the other side's sample min(2n, (-q * invAngle + 128) >> 8) for q < 0
+    const int16_t* R_ = W.s;
+#pragma unroll
+    for (int r = 0; r < R; r++)
+        if (lane + 32 * r < total) W.s[lane + 32 * r] = (int16_t)f[r];
     const int ang = c_intra_angle[mode];
     const bool vert = mode >= 18;
     if (mode >= 2) {
-        // main reference with the side reference projected through invAngle (:346-368):
-        // m[q + n] = top[q] (vertical) / left[q] (horizontal) for q >= 0, the other side's
-        // sample min(2n, (-q * invAngle + 128) >> 8) for q < 0
         const int inv = c_inv_angle[mode];
-        for (int q = lane - n; q <= 2 * n + 1; q += 32) {
-            int v = 0;
-            if (q > 2 * n) v = 0;   // padding entry, read but never weighted
-            else if (q >= 0) v = vert ? R_[2 * n + q] : R_[2 * n - q];
+        constexpr int ME = 3 * n + 2;   // entries q = -n .. 2n + 1 (the last one padding, never weighted)
+#pragma unroll
+        for (int k = 0; k < (ME + 31) / 32; k++) {
+            const int e = lane + 32 * k, q = e - n;
+            int src;
+            if (q > 2 * n) src = -1;
+            else if (q >= 0) src = vert ? 2 * n + q : 2 * n - q;
             else {
                 const int si = min(2 * n, ((-q) * inv + 128) >> 8);
-                v = vert ? R_[2 * n - si] : R_[2 * n + si];
+                src = vert ? 2 * n - si : 2 * n + si;
             }
-            W.m[q + n] = (int16_t)v;
+            const int v = fetch(f, src < 0 ? 0 : src);
+            if (e < ME) W.m[e] = (int16_t)(src < 0 ? 0 : v);
         }
-        __syncwarp();
     }
+    __syncwarp();
+    // 5. prediction + residual, clip, store.  Each lane takes groups of 4 samples of a row;
+    //    its column x0 = 4 * (lane % (n / 4)) is the same for all its groups, so column
+    //    terms are computed once.
+    constexpr int GPR = n / 4, NG = n * n / 4, G_PER_LANE = (NG + 31) / 32;
     int dc = 0;
     if (mode == 1) {  // predict_dc :295-317
         int s = 0;
@@ -299,6 +330,7 @@ __device__ __forceinline__ void intra_tu_any(const PicDesc& P, const hevc_tu_t& 
 // ---------------------------------------------------------------------------------------
 constexpr int IC_WARPS = 4;
 constexpr int IC_THREADS = 32 * IC_WARPS;
+constexpr int IC_PUBLISHER = 32 * (IC_WARPS - 1);    // lane 0 of the last warp
 constexpr int IC_LP = 64, IC_LH = 64;                // luma tile (the CTU): pitch, rows
 constexpr int IC_CP = 32, IC_CH = 32;                // chroma tiles
 constexpr int IC_MAX_TUS = 256 + 2 * 64;             // 4x4 TUs of a 64x64 CTU, all planes
@@ -349,7 +381,9 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
     __shared__ __align__(16) hevc_tu_t s_tu[IC_MAX_TUS];
     __shared__ __align__(16) int16_t s_res[IC_MAX_RES];
     __shared__ IntraWarpSmem ws[IC_WARPS];
+    __shared__ __align__(16) IntraLevel s_lvl[IC_MAX_TUS + 2];   // the CTU's levels (from an even entry)
     __shared__ int s_ticket, s_pic, s_abort;
+    __shared__ int s_seen[4];   // levels each dependency CTU was seen to have completed
     __shared__ uint32_t s_nb;
     const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
     if (tid == 0) {
@@ -389,9 +423,14 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
 
     // stage the neighbourhood and the TU records
     const int off = P.ictu_tu_off[idx], n_tu = P.ictu_tu_off[idx + 1] - off;
-    // one round of asynchronous copies: TU records, the three tiles, the residuals of the
-    // coded TUs (packed in task order, one thread per TU)
+    const int lvl0 = P.ictu_lvl_off[idx], n_lvl = P.ictu_lvl_off[idx + 1] - lvl0;
+    if (tid < 4) s_seen[tid] = 0;
+    // one round of asynchronous copies: TU records, levels (two per 16-byte copy, from the
+    // even entry at or below the first), the three tiles, the residuals of the coded TUs
+    // (packed in task order, one thread per TU)
     for (int i = tid; i < n_tu; i += IC_THREADS) cp_async16(&s_tu[i], &P.itu_rec[off + i]);
+    for (int i = tid; 2 * i < n_lvl + (lvl0 & 1); i += IC_THREADS)
+        cp_async16(&s_lvl[2 * i], &P.ictu_lvl[(lvl0 & ~1) + 2 * i]);
     stage_tile(P, 0, rx, ry, t_luma, tid);
     stage_tile(P, 1, rx, ry, t_chroma[0], tid);
     stage_tile(P, 2, rx, ry, t_chroma[1], tid);
@@ -404,24 +443,30 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
 
     const int ctbl = 1 << P.log2_ctb;
     const uint32_t nb = s_nb;
-    // Levels of the CTU-local DAG.  Before a level, threads 0-3 wait (bounded) until their
-    // dependency CTU has completed the levels this level needs; after a level that other
-    // CTUs need, the CTU publishes (epoch << 16) | levels completed.
-    const uint2* lvl = reinterpret_cast<const uint2*>(P.ictu_lvl + P.ictu_lvl_off[idx]);
+    // Levels of the CTU-local DAG.  Before a level whose requirement on a dependency CTU
+    // exceeds what was last seen of it, threads 0-3 wait (bounded) until their dependency
+    // CTU has completed the levels this level needs, then the CTA meets at a barrier; a
+    // requirement already seen met needs neither (the barrier that ended the level where it
+    // was seen orders it for every thread).  After a level that other CTUs need, the CTU
+    // publishes (epoch << 16) | levels completed.
+    const IntraLevel* lvl = s_lvl + (lvl0 & 1);
     const int dep = tid < 4 ? P.ictu_deps[4 * idx + tid] : -1;
     const int32_t stamp = epoch << 16;
     int pos = 0;
     for (int L = 0; pos < n_tu; L++) {
-        const uint2 info = __ldg(lvl + L);
-        const uint32_t req01 = info.x & 0xFFFF7FFFu;      // req[0] without the publish bit, req[1]
-        if (req01 | info.y) {
+        const IntraLevel info = lvl[L];
+        bool wait = false;
+#pragma unroll
+        for (int d = 0; d < 4; d++) wait = wait || intra_req(info, d) > s_seen[d];
+        if (wait) {
+            int seen = -1;   // levels the dependency was seen to have completed, when polled
             if (dep >= 0) {
-                const uint32_t w = tid < 2 ? req01 : info.y;
-                const int need = (int)((w >> (16 * (tid & 1))) & 0xFFFFu);
-                if (need) {
+                const int need = intra_req(info, tid);
+                if (need > s_seen[tid]) {
                     cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[dep]);
                     long long polls = 0;
-                    while (done.load(cuda::memory_order_acquire) < (stamp | need)) {
+                    int v;
+                    while ((v = done.load(cuda::memory_order_acquire)) < (stamp | need)) {
                         if (++polls > SPIN_LIMIT) {
                             atomicOr(sticky, ST_TIMEOUT);
                             s_abort = 1;
@@ -429,12 +474,15 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
                         }
                         __nanosleep(32);
                     }
+                    seen = v - stamp;   // same epoch: levels completed (>= need)
                 }
             }
             __syncthreads();
             if (s_abort) return;
+            // after the barrier, so that no thread still reads s_seen for this level's test
+            if (seen >= 0) s_seen[tid] = seen;
         }
-        const int lvl_end = P.itu_level_end[off + pos] - off;
+        const int lvl_end = intra_end(info);
         for (int i = pos + warp; i < lvl_end; i += IC_WARPS) {
             const hevc_tu_t& tu = s_tu[i];
             const int ctbc = tu.c_idx ? ctbl / 2 : ctbl;
@@ -443,13 +491,16 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
             tile.pitch = tu.c_idx ? IC_CP : IC_LP;
             tile.x0 = rx * ctbc;
             tile.y0 = ry * ctbc;
-            const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + __ldg(&P.itu_res[off + i].y) : nullptr;
+            const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + tu.coeff_offset : nullptr;
             intra_tu_any(P, tu, lane, ws[warp], tile, nb, res);
         }
         __syncthreads();
-        if ((info.x & INTRA_LEVEL_PUBLISH) && tid == 0) {
+        if ((info.x & INTRA_LEVEL_PUBLISH) && tid == IC_PUBLISHER) {
             // after the barrier, the release store orders the CTA's picture writes before
-            // the word (the barrier makes them prior to thread 0's release)
+            // the word (the barrier makes them prior to this thread's release).  The last
+            // warp publishes: TUs go to warps from warp 0 up, so it is the warp most often
+            // idle in the next level, and the release's wait for the stores overlaps the
+            // other warps' next TUs.
             cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[idx]);
             done.store(stamp | (L + 1), cuda::memory_order_release);
         }
