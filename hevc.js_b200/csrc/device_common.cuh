@@ -19,6 +19,7 @@ struct MotionEnt {           // 4x4 motion grid entry (PUMotionInfo, inter_predi
     int8_t  ref[2];          // refIdxLX, -1 when predFlagLX is 0
     int16_t pad;
 };
+static_assert(sizeof(MotionEnt) == 12, "MotionEnt is written as three words by the MC kernel");
 
 // One level of an intra CTU task, packed in 8 bytes (staged into shared memory):
 // req(d) > 0 means "dependency slot d must have completed req(d) levels before this level

@@ -975,7 +975,7 @@ struct Exec {
 int run_stages(hevcgpu_ctx* ctx, const Exec& ex, hevcgpu_job* const* jobs, int n, int stages, int res_mode) {
     Launcher L{ctx, ex.stream};
     int rc;
-    if (stages & ST_DEBLOCK) {
+    if ((stages & ST_DEBLOCK) && !(stages & ST_MC)) {   // with MC, its luma strips write the grid
         StageMark m(ctx, ex.stream, 0);
         rc = L.pictures(k_motion_grid, jobs, n, 256, 1, [](hevcgpu_job* j) { return (j->n_pus * 32 + 255) / 256; });
         if (rc) return rc;

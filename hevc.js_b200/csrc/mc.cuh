@@ -282,6 +282,22 @@ __global__ void __launch_bounds__(MC_THREADS, HEVCGPU_MC_MIN_CTAS) k_mc(const __
     const McWeights wt = mc_weights(pu.wp >= 0 ? &P.wp[pu.wp] : nullptr, bi, use0, ci);
     uint8_t* const out = P.rec + poff + (int64_t)y * pitch + x;
     const int wlast = bi ? wt.w1 : wt.w0;   // weight of the last pass's list
+    if constexpr (!CHROMA) {
+        // the strip's 4x4 units of the motion grid (the Bs derivation's PU motion), as the
+        // three words of a MotionEnt: mv[0], mv[1], ref_idx[0..1] (padding zero)
+        if (P.mot) {
+            const uint32_t m0 = (uint32_t)(uint16_t)pu.mv[0][0] | ((uint32_t)(uint16_t)pu.mv[0][1] << 16);
+            const uint32_t m1 = (uint32_t)(uint16_t)pu.mv[1][0] | ((uint32_t)(uint16_t)pu.mv[1][1] << 16);
+            const uint32_t m2 = (uint32_t)(uint8_t)pu.ref_idx[0] | ((uint32_t)(uint8_t)pu.ref_idx[1] << 8);
+            const int gw = P.width / 4;
+            uint32_t* g = reinterpret_cast<uint32_t*>(P.mot + (int64_t)(y >> 2) * gw + (x >> 2));
+            for (int k = 0; k < rows / 4; k++, g += 3 * gw) {
+                g[0] = m0;
+                g[1] = m1;
+                g[2] = m2;
+            }
+        }
+    }
 
 #pragma unroll 1
     for (int q = 0; q < (bi ? 2 : 1); q++) {
