@@ -245,40 +245,58 @@ __constant__ uint8_t c_qpc[58] = {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11
                                   36, 36, 37, 37, 38, 39, 40, 41, 42, 43, 44, 45, 46, 47, 48, 49, 50, 51};
 
 __device__ __forceinline__ int ref_poc_of(const PicDesc& P, const MotionEnt& m, int l) {
-    int r = m.ref[l];
+    const int r = l ? m.ref[1] : m.ref[0];
     return (r < 0 || r >= P.num_ref[l]) ? -999999 : P.ref_poc[l][r];
 }
-__device__ __forceinline__ bool mv_far(const int16_t* a, const int16_t* b) {
-    return abs(a[0] - b[0]) >= 4 || abs(a[1] - b[1]) >= 4;
+// |MV difference| >= 4 in either component, for list la of a and list lb of b (lists picked
+// by value, so that the entries stay in registers)
+__device__ __forceinline__ bool mv_far(const MotionEnt& a, int la, const MotionEnt& b, int lb) {
+    const int ax = la ? a.mv[1][0] : a.mv[0][0], ay = la ? a.mv[1][1] : a.mv[0][1];
+    const int bx = lb ? b.mv[1][0] : b.mv[0][0], by = lb ? b.mv[1][1] : b.mv[0][1];
+    return abs(ax - bx) >= 4 || abs(ay - by) >= 4;
 }
 
-// derive_bs (deblocking.cpp:125-247)
-__device__ int derive_bs(const PicDesc& P, int gw, uint32_t bp, uint32_t bq, int xp, int yp, int xq, int yq) {
+// derive_bs (deblocking.cpp:125-247), on the grid words and motion entries of the two sides
+__device__ __forceinline__ int derive_bs(const PicDesc& P, uint32_t bp, uint32_t bq, const MotionEnt& mp,
+                                         const MotionEnt& mq, int xp, int yp, int xq, int yq) {
     if ((bp | bq) & HEVC_BLK_INTRA) return 2;
     int tp = 1 << ((bp >> HEVC_BLK_TU_SHIFT) & 0xFF), tq = 1 << ((bq >> HEVC_BLK_TU_SHIFT) & 0xFF);
     bool tu_edge = (xp != xq) ? ((xq % tq == 0) || ((xp + 1) % tp == 0 && xp + 1 == xq))
                               : ((yq % tq == 0) || ((yp + 1) % tp == 0 && yp + 1 == yq));
     if (tu_edge && ((bp | bq) & HEVC_BLK_CBF)) return 1;
-    const MotionEnt mp = P.mot[(int64_t)(yp >> 2) * gw + (xp >> 2)];
-    const MotionEnt mq = P.mot[(int64_t)(yq >> 2) * gw + (xq >> 2)];
     int np = (mp.ref[0] >= 0) + (mp.ref[1] >= 0), nq = (mq.ref[0] >= 0) + (mq.ref[1] >= 0);
     if (np != nq) return 1;
     if (np == 1) {
         int lp = mp.ref[0] >= 0 ? 0 : 1, lq = mq.ref[0] >= 0 ? 0 : 1;
         if (ref_poc_of(P, mp, lp) != ref_poc_of(P, mq, lq)) return 1;
-        return mv_far(mp.mv[lp], mq.mv[lq]) ? 1 : 0;
+        return mv_far(mp, lp, mq, lq) ? 1 : 0;
     }
     if (np == 2) {
         int p0 = ref_poc_of(P, mp, 0), p1 = ref_poc_of(P, mp, 1), q0 = ref_poc_of(P, mq, 0), q1 = ref_poc_of(P, mq, 1);
         bool same = p0 == q0 && p1 == q1, swp = p0 == q1 && p1 == q0;
         if (!same && !swp) return 1;
-        bool o1 = !mv_far(mp.mv[0], mq.mv[0]) && !mv_far(mp.mv[1], mq.mv[1]);
-        bool o2 = !mv_far(mp.mv[0], mq.mv[1]) && !mv_far(mp.mv[1], mq.mv[0]);
+        bool o1 = !mv_far(mp, 0, mq, 0) && !mv_far(mp, 1, mq, 1);
+        bool o2 = !mv_far(mp, 0, mq, 1) && !mv_far(mp, 1, mq, 0);
         if (same && !swp) return o1 ? 0 : 1;
         if (!same && swp) return o2 ? 0 : 1;
         return (o1 || o2) ? 0 : 1;
     }
     return 0;
+}
+
+// Motion entry from its three words (the grid is 12-byte entries, 4-byte aligned).
+__device__ __forceinline__ MotionEnt load_motion(const MotionEnt* g) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(g);
+    const uint32_t a = w[0], b = w[1], c = w[2];
+    MotionEnt m;
+    m.mv[0][0] = (int16_t)(a & 0xFFFF);
+    m.mv[0][1] = (int16_t)(a >> 16);
+    m.mv[1][0] = (int16_t)(b & 0xFFFF);
+    m.mv[1][1] = (int16_t)(b >> 16);
+    m.ref[0] = (int8_t)(c & 0xFF);
+    m.ref[1] = (int8_t)((c >> 8) & 0xFF);
+    m.pad = 0;
+    return m;
 }
 
 __device__ __forceinline__ const hevc_slice_t& slice_at(const PicDesc& P, int addr) {
@@ -338,7 +356,7 @@ __device__ __forceinline__ void luma_segment(int (&p)[4][4], int (&q)[4][4], int
 }
 
 template <bool VERT>
-__global__ void __launch_bounds__(256) k_deblock(const __grid_constant__ SegTable st) {
+__global__ void __launch_bounds__(256, 3) k_deblock(const __grid_constant__ SegTable st) {
     const PicDesc& P = *st.s[blockIdx.y].pic;
     const int W = P.width, H = P.height, gw = W >> 2;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -348,21 +366,68 @@ __global__ void __launch_bounds__(256) k_deblock(const __grid_constant__ SegTabl
     const int y = VERT ? (tid / nx) * 4 : (tid / nx) * 8;
     if (y >= H || x >= W) return;
     if (VERT ? x == 0 : y == 0) return;
+    const int xp = VERT ? x - 1 : x, yp = VERT ? y : y - 1;
+    // Every load the segment may need is issued here, before any decision, so that the
+    // segment waits for memory once: the grid words and motion entries of both sides, the
+    // luma neighbourhood, and on the chroma grid the chroma neighbourhood.
     const uint32_t bq = P.blk[(int64_t)(y >> 2) * gw + (x >> 2)];
+    const uint32_t bp = P.blk[(int64_t)(yp >> 2) * gw + (xp >> 2)];
+    MotionEnt mp{}, mq{};
+    if (P.mot) {
+        mp = load_motion(P.mot + (int64_t)(yp >> 2) * gw + (xp >> 2));
+        mq = load_motion(P.mot + (int64_t)(y >> 2) * gw + (x >> 2));
+    }
+    uint8_t* Y = P.rec;
+    uint32_t wv[8];
+    if (VERT) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint8_t* row = Y + (int64_t)(y + k) * P.pitch_y + x;
+            wv[2 * k] = *reinterpret_cast<const uint32_t*>(row - 4);
+            wv[2 * k + 1] = *reinterpret_cast<const uint32_t*>(row);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            wv[3 - i] = *reinterpret_cast<const uint32_t*>(Y + (int64_t)(y - 1 - i) * P.pitch_y + x);
+            wv[4 + i] = *reinterpret_cast<const uint32_t*>(Y + (int64_t)(y + i) * P.pitch_y + x);
+        }
+    }
+    // chroma (4:2:0): the segment's half on the 8-sample chroma grid, two lines of p1 p0 q0 q1
+    // per plane; vertical edges as the words at cx - 4 and cx, horizontal ones as the words
+    // of rows cy - 2 .. cy + 1 at the 4-aligned column holding cx .. cx + 1
+    const bool cgrid = (((VERT ? x : y) >> 1) & 7) == 0;
+    const int cx = x >> 1, cy = y >> 1, pc = P.pitch_c;
+    uint32_t cw[2][4];
+    if (cgrid) {
+#pragma unroll
+        for (int ci = 0; ci < 2; ci++) {
+            const uint8_t* Cp = P.rec + (ci == 0 ? P.off_cb : P.off_cr);
+            if (VERT) {
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    const uint8_t* row = Cp + (int64_t)(cy + k) * pc + cx;
+                    cw[ci][2 * k] = *reinterpret_cast<const uint32_t*>(row - 4);
+                    cw[ci][2 * k + 1] = *reinterpret_cast<const uint32_t*>(row);
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+                    cw[ci][r] = *reinterpret_cast<const uint32_t*>(Cp + (int64_t)(cy - 2 + r) * pc + (cx & ~3));
+            }
+        }
+    }
+
     if (!(bq & (VERT ? HEVC_BLK_EDGE_V : HEVC_BLK_EDGE_H))) return;
-    const int ctb = 1 << P.log2_ctb;
     const int aq = (y >> P.log2_ctb) * P.wctb + (x >> P.log2_ctb);
     const hevc_slice_t& sq = slice_at(P, aq);
     if (sq.deblocking_disabled) return;
-    const int xp = VERT ? x - 1 : x, yp = VERT ? y : y - 1;
     if (P.tiles_check || P.slice_check) {
         const int ap = (yp >> P.log2_ctb) * P.wctb + (xp >> P.log2_ctb);
         if (P.tiles_check && P.ctb_tile && P.ctb_tile[aq] != P.ctb_tile[ap]) return;
         if (P.slice_check && P.ctb_slice && P.ctb_slice[aq] != P.ctb_slice[ap] && !sq.lf_across_slices) return;
     }
-    (void)ctb;
-    const uint32_t bp = P.blk[(int64_t)(yp >> 2) * gw + (xp >> 2)];
-    const int bs = derive_bs(P, gw, bp, bq, xp, yp, x, y);
+    const int bs = derive_bs(P, bp, bq, mp, mq, xp, yp, x, y);
     if (bs == 0) return;
     const int qpP = (int8_t)(bp >> HEVC_BLK_QP_SHIFT), qpQ = (int8_t)(bq >> HEVC_BLK_QP_SHIFT);
     const bool noP = (P.pcm_lf_disabled && (bp & HEVC_BLK_PCM)) || (bp & HEVC_BLK_BYPASS);
@@ -371,16 +436,11 @@ __global__ void __launch_bounds__(256) k_deblock(const __grid_constant__ SegTabl
     const int beta = c_beta[clip3(0, 51, qpl + 2 * sq.beta_offset_div2)];
     const int tc = c_tc[clip3(0, 53, qpl + 2 * (bs - 1) + 2 * sq.tc_offset_div2)];
 
-    // ---- luma: load the 8x4 (or 4x8) neighbourhood as 32-bit words
-    uint8_t* Y = P.rec;
+    // ---- luma: the 8x4 (or 4x8) neighbourhood from its words
     int p[4][4], q[4][4];
-    uint32_t wv[8];
     if (VERT) {
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            const uint8_t* row = Y + (int64_t)(y + k) * P.pitch_y + x;
-            wv[2 * k] = *reinterpret_cast<const uint32_t*>(row - 4);
-            wv[2 * k + 1] = *reinterpret_cast<const uint32_t*>(row);
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 p[k][i] = (wv[2 * k] >> (8 * (3 - i))) & 0xFF;
@@ -388,11 +448,6 @@ __global__ void __launch_bounds__(256) k_deblock(const __grid_constant__ SegTabl
             }
         }
     } else {
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            wv[3 - i] = *reinterpret_cast<const uint32_t*>(Y + (int64_t)(y - 1 - i) * P.pitch_y + x);
-            wv[4 + i] = *reinterpret_cast<const uint32_t*>(Y + (int64_t)(y + i) * P.pitch_y + x);
-        }
 #pragma unroll
         for (int k = 0; k < 4; k++)
 #pragma unroll
@@ -436,22 +491,33 @@ __global__ void __launch_bounds__(256) k_deblock(const __grid_constant__ SegTabl
     }
 
     // ---- chroma: Bs 2 on the 8-sample chroma grid (deblocking.cpp:538-609)
-    if (bs == 2 && (((VERT ? x : y) >> 1) & 7) == 0) {
-        const int cx = x >> 1, cy = y >> 1;
+    if (bs == 2 && cgrid) {
 #pragma unroll
-        for (int ci = 1; ci <= 2; ci++) {
-            const int off = ci == 1 ? P.cb_qp_offset : P.cr_qp_offset;
+        for (int ci = 0; ci < 2; ci++) {
+            const int off = ci == 0 ? P.cb_qp_offset : P.cr_qp_offset;
             const int qpc = c_qpc[clip3(0, 57, ((qpQ + qpP + 1) >> 1) + off)];
             const int tcc = c_tc[clip3(0, 53, qpc + 2 + 2 * sq.tc_offset_div2)];
-            uint8_t* Cp = P.rec + (ci == 1 ? P.off_cb : P.off_cr);
-            const int pc = P.pitch_c;
+            uint8_t* Cp = P.rec + (ci == 0 ? P.off_cb : P.off_cr);
 #pragma unroll
             for (int k = 0; k < 2; k++) {
+                // p1 p0 | q0 q1 of line k
+                int p0, p1, q0, q1;
+                if (VERT) {
+                    p1 = (cw[ci][2 * k] >> 16) & 0xFF;
+                    p0 = cw[ci][2 * k] >> 24;
+                    q0 = cw[ci][2 * k + 1] & 0xFF;
+                    q1 = (cw[ci][2 * k + 1] >> 8) & 0xFF;
+                } else {
+                    const int sh = 8 * ((cx & 3) + k);
+                    p1 = (cw[ci][0] >> sh) & 0xFF;
+                    p0 = (cw[ci][1] >> sh) & 0xFF;
+                    q0 = (cw[ci][2] >> sh) & 0xFF;
+                    q1 = (cw[ci][3] >> sh) & 0xFF;
+                }
+                const int delta = clip3(-tcc, tcc, ((((q0 - p0) * 4) + p1 - q1 + 4) >> 3));
                 uint8_t* s0 = VERT ? Cp + (int64_t)(cy + k) * pc + cx : Cp + (int64_t)cy * pc + cx + k;
-                const int st = VERT ? 1 : pc;
-                int p0 = s0[-st], p1 = s0[-2 * st], q0 = s0[0], q1 = s0[st];
-                int delta = clip3(-tcc, tcc, ((((q0 - p0) * 4) + p1 - q1 + 4) >> 3));
-                if (!noP) s0[-st] = (uint8_t)clip_u8(p0 + delta);
+                const int stp = VERT ? 1 : pc;
+                if (!noP) s0[-stp] = (uint8_t)clip_u8(p0 + delta);
                 if (!noQ) s0[0] = (uint8_t)clip_u8(q0 - delta);
             }
         }
