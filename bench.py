@@ -478,7 +478,7 @@ def run_ours(args, hb, rank, world, local):
     # DRAM bytes (read + write) per launch of each stage's kernels, from one ncu capture of
     # this workload at 16 pictures per launch (profiles/kernels_pb16_1080p.md); scaled by
     # the pictures per launch when --batch differs (the traffic grows with the pictures).
-    ncu_dram_16 = {"mc": 125.48e6, "residual": 171.37e6, "intra": 50.88e6, "deblock": 123.92e6, "sao": 68.25e6}
+    ncu_dram_16 = {"mc": 146.71e6, "residual": 170.51e6, "intra": 50.43e6, "deblock": 160.87e6, "sao": 68.79e6}
     traffic = ncu_dram_16[dom] * B / 16.0 if W == W_DEFAULT and H == H_DEFAULT else None
 
     cpu = None
