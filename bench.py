@@ -21,8 +21,9 @@ e2e        frames/s through the C ABI from host memory: per step the pictures' r
            packed into pinned memory on the library's host workers and copied host->device
            (hevcgpu_jobs_prepare), the batch is launched on a lane, and every reconstructed
            picture is copied device->host into pinned host frame buffers
-           (hevcgpu_lane_slots_download); consecutive steps alternate lanes, so step k's
-           host preparation overlaps step k-1 on the device.
+           (hevcgpu_lane_slots_download_async, waited for with hevcgpu_lane_wait before the
+           buffers are reused two steps later and at the end); consecutive steps alternate
+           lanes, so step k's host preparation overlaps step k-1 on the device and its copies.
 stages     per-stage device times from CUDA events recorded around each stage on the
            library's stream, in a separate pass of the same batched step (the timed region
            itself carries no extra events).
@@ -418,9 +419,10 @@ def run_ours(args, hb, rank, world, local):
 
     # end to end through the C ABI from host memory, pipelined over the two lanes: step k
     # prepares its B pictures on the host workers (records packed into pinned memory and
-    # copied host->device: hevcgpu_jobs_prepare), launches them on lane k % 2, and then
-    # reads step k-1's pictures back into pinned host frame buffers on that step's lane
-    # (hevcgpu_lane_slots_download) while step k runs on the device
+    # copied host->device: hevcgpu_jobs_prepare), launches them on lane k % 2 and queues the
+    # copies of its frames into pinned host frame buffers behind them
+    # (hevcgpu_lane_slots_download_async); the frames of step k are waited for
+    # (hevcgpu_lane_wait) when their buffers come round again at step k + 2, and at the end
     frame_bytes = hb.i420_size(W, H)
     out_host = [[torch.empty(frame_bytes, dtype=torch.uint8).pin_memory().numpy() for _ in range(B)]
                 for _ in range(2)]
@@ -428,22 +430,23 @@ def run_ours(args, hb, rank, world, local):
 
     def e2e_run(steps):
         nonlocal h2d_bytes
-        pending = None
+        tickets, held = [None, None], [[], []]
         for k in range(steps):
             i = k % 2
+            if tickets[i] is not None:
+                lanes[i].wait(tickets[i])
+                for j in held[i]:
+                    j.free()
             js = hb.prepare_batch(grp_streams[i], grp_pics[i])
             h2d_bytes = sum(j.upload_bytes for j in js)
             lanes[i].batch_launch(js, slots)
-            if pending is not None:
-                pi, pjs = pending
-                lanes[pi].download_batch(grp_streams[pi], slots, out_host[pi])
-                for j in pjs:
+            tickets[i] = lanes[i].download_batch_async(grp_streams[i], slots, out_host[i])
+            held[i] = js
+        for i in range(2):
+            if tickets[i] is not None:
+                lanes[i].wait(tickets[i])
+                for j in held[i]:
                     j.free()
-            pending = (i, js)
-        pi, pjs = pending
-        lanes[pi].download_batch(grp_streams[pi], slots, out_host[pi])
-        for j in pjs:
-            j.free()
 
     e2e_steps = max(4, args.steps // 5)
     e2e_run(2)

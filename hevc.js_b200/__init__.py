@@ -203,6 +203,9 @@ def gpu_lib():
             "hevcgpu_lane_cuda_stream": ([P], P),
             "hevcgpu_lane_slots_download": ([P, C.POINTER(P), C.POINTER(C.c_int32), C.c_int32, C.POINTER(P)],
                                             C.c_int),
+            "hevcgpu_lane_slots_download_async": ([P, C.POINTER(P), C.POINTER(C.c_int32), C.c_int32,
+                                                   C.POINTER(P), C.POINTER(C.c_uint64)], C.c_int),
+            "hevcgpu_lane_wait": ([P, C.c_uint64], C.c_int),
             "hevcgpu_slots_download": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32, C.POINTER(P)], C.c_int),
             "hevcgpu_cuda_stream": ([P], P),
             "hevcgpu_launch_count": ([P], C.c_uint64),
@@ -428,6 +431,21 @@ class Lane:
         ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
         _check(self.lib.hevcgpu_lane_slots_download(self.h, sts, sl, n, ptrs))
         return outs
+
+    def download_batch_async(self, streams, slots, outs):
+        """The same copies into page-locked host buffers, queued without waiting; returns
+        the ticket to pass to wait() before reading the buffers."""
+        n = len(streams)
+        sts = (C.c_void_p * n)(*[st.h for st in streams])
+        sl = (C.c_int32 * n)(*slots)
+        ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        ticket = C.c_uint64()
+        _check(self.lib.hevcgpu_lane_slots_download_async(self.h, sts, sl, n, ptrs, C.byref(ticket)))
+        return ticket.value
+
+    def wait(self, ticket):
+        """Returns once the download with this ticket has landed."""
+        _check(self.lib.hevcgpu_lane_wait(self.h, ticket))
 
     @property
     def cuda_stream(self):

@@ -335,6 +335,11 @@ struct hevcgpu_lane {
     cudaEvent_t done[hevcgpu_ctx::EVENT_RING] = {};   // batch completion events, used in turn
     int done_next = 0;
     cudaEvent_t ctx_ready = nullptr;   // the context stream's work before a batch
+    // Asynchronous downloads: download k (k = 1, 2, ...) records dl_done[k % EVENT_RING]
+    // after its copies; a later download reuses the slot, whose event then completes later,
+    // so waiting on it still waits for download k.
+    cudaEvent_t dl_done[hevcgpu_ctx::EVENT_RING] = {};
+    uint64_t dl_seq = 0;
     cudaEvent_t next_done() {
         cudaEvent_t e = done[done_next];
         done_next = (done_next + 1) % hevcgpu_ctx::EVENT_RING;
@@ -344,6 +349,8 @@ struct hevcgpu_lane {
         if (stream) cudaStreamSynchronize(stream);
         if (flow) cudaFree(flow);
         for (auto e : done)
+            if (e) cudaEventDestroy(e);
+        for (auto e : dl_done)
             if (e) cudaEventDestroy(e);
         if (ctx_ready) cudaEventDestroy(ctx_ready);
         if (stream) cudaStreamDestroy(stream);
@@ -1801,6 +1808,44 @@ int hevcgpu_lane_slots_download(hevcgpu_lane_t* lane, hevcgpu_stream_t* const* s
         if (sts && sts[i] && sts[i]->ctx != lane->ctx) return fail(HEVCGPU_EINVAL, "picture %d: stream of another context", i);
     int rc = slots_download_on(sts, slots, n, outs, lane->stream);
     if (rc) return rc;
+    return hevcgpu_ctx::take_status_of(lane->flow);
+}
+
+int hevcgpu_lane_slots_download_async(hevcgpu_lane_t* lane, hevcgpu_stream_t* const* sts, const int32_t* slots,
+                                      int32_t n, uint8_t* const* outs, uint64_t* ticket) {
+    if (!lane || !ticket) return fail(HEVCGPU_EINVAL, "null lane or ticket");
+    *ticket = 0;
+    if (n < 0 || (n && (!sts || !slots || !outs))) return fail(HEVCGPU_EINVAL, "null arrays");
+    for (int i = 0; i < n; i++) {
+        if (!sts[i] || !outs[i]) return fail(HEVCGPU_EINVAL, "picture %d: null stream or buffer", i);
+        if (sts[i]->ctx != lane->ctx) return fail(HEVCGPU_EINVAL, "picture %d: stream of another context", i);
+        if (slots[i] < 0 || slots[i] >= (int)sts[i]->slots.size())
+            return fail(HEVCGPU_EINVAL, "picture %d: bad slot %d", i, slots[i]);
+        cudaPointerAttributes a;
+        const bool pinned = cudaPointerGetAttributes(&a, outs[i]) == cudaSuccess && a.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (!pinned) return fail(HEVCGPU_EINVAL, "picture %d: destination is not page-locked host memory", i);
+    }
+    int rc = check_ctx(lane->ctx);
+    if (rc) return rc;
+    for (int i = 0; i < n; i++)
+        if ((rc = download_i420(lane->ctx, sts[i]->lay, static_cast<uint8_t*>(sts[i]->slots[(size_t)slots[i]].p),
+                                outs[i], lane->stream)))
+            return rc;
+    const uint64_t t = lane->dl_seq + 1;
+    cudaEvent_t& e = lane->dl_done[t % hevcgpu_ctx::EVENT_RING];
+    if (!e) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(e, lane->stream));
+    lane->dl_seq = t;
+    *ticket = t;
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_lane_wait(hevcgpu_lane_t* lane, uint64_t ticket) {
+    if (!lane) return fail(HEVCGPU_EINVAL, "null lane");
+    if (ticket == 0 || ticket > lane->dl_seq) return fail(HEVCGPU_EINVAL, "unknown download ticket %llu",
+                                                          (unsigned long long)ticket);
+    CUDA_TRY(cudaEventSynchronize(lane->dl_done[ticket % hevcgpu_ctx::EVENT_RING]));
     return hevcgpu_ctx::take_status_of(lane->flow);
 }
 

@@ -263,6 +263,19 @@ void* hevcgpu_lane_cuda_stream(hevcgpu_lane_t* lane);
  * Returns the lane's device status, like hevcgpu_lane_sync. */
 int   hevcgpu_lane_slots_download(hevcgpu_lane_t* lane, hevcgpu_stream_t* const* sts,
                                   const int32_t* slots, int32_t n, uint8_t* const* outs);
+/* The same copies, queued on the lane after its batches, without waiting: every
+ * destination must be page-locked host memory (cudaHostAlloc / cudaHostRegister), which
+ * the copies write directly.  *ticket identifies the download; the frames are complete
+ * once hevcgpu_lane_wait(lane, ticket) has returned (or after hevcgpu_lane_sync).  A
+ * decoder pipeline overlaps the copies of one batch with the preparation of the next
+ * (the reference hands each frame out synchronously: hevc_decoder_get_frame,
+ * wasm/hevc_api.h:63). */
+int   hevcgpu_lane_slots_download_async(hevcgpu_lane_t* lane, hevcgpu_stream_t* const* sts,
+                                        const int32_t* slots, int32_t n, uint8_t* const* outs,
+                                        uint64_t* ticket);
+/* Waits until the download with this ticket has landed; returns the lane's device status,
+ * like hevcgpu_lane_sync. */
+int   hevcgpu_lane_wait(hevcgpu_lane_t* lane, uint64_t ticket);
 
 /* Batched host-side calls for a decoder that finishes several pictures at once (one per
  * stream).  The work is spread over the context's host worker threads (one per

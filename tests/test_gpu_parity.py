@@ -171,6 +171,25 @@ def test_lanes_alone_and_in_the_mix(hb, gpu_ctx, port):
     lanes[0].download_batch([streams[i] for i in groups[0]], [2] * 3, outs)
     for i, got in zip(groups[0], outs):
         assert _diff(got, alone[i]) == 0
+    # asynchronous downloads into pinned buffers: queued behind the lane's batch, complete
+    # after the wait on their ticket, two in flight on the two lanes at once
+    import torch
+    for st in streams:
+        st.upload(2, np.zeros(hb.i420_size(st.width, st.height), np.uint8))
+    pinned = [torch.empty(hb.i420_size(st.width, st.height), dtype=torch.uint8).pin_memory().numpy()
+              for st in streams]
+    tickets = []
+    for lane, g in zip(lanes, groups):
+        lane.batch_launch([jobs[i] for i in g], [2] * len(g))
+        tickets.append(lane.download_batch_async([streams[i] for i in g], [2] * len(g), [pinned[i] for i in g]))
+    for lane, t in zip(lanes, tickets):
+        lane.wait(t)
+    for got, want in zip(pinned, alone):
+        assert _diff(got, want) == 0
+    # a pageable destination is refused: the asynchronous copies write their destinations directly
+    with pytest.raises(hb.HevcGpuError) as e:
+        lanes[0].download_batch_async([streams[0]], [2], [np.empty_like(alone[0])])
+    assert e.value.code == hb.abi.HEVCGPU_EINVAL
     for lane in lanes:
         lane.close()
 
