@@ -125,8 +125,43 @@ class Picture:
         synth_lib().hevcsynth_bs_histogram(self.syn_ptr, out)
         return list(out)
 
+    # the large record arrays: (field, bytes)
+    def _large_arrays(self):
+        s = self.syn
+        grid = (s.params.width // 4) * (s.params.height // 4) * 4 if s.blk else 0
+        return [("tus", 16 * s.num_tus), ("coeffs", 2 * s.num_coeffs), ("pus", 20 * s.num_pus), ("blk", grid)]
+
+    def pin(self):
+        """Moves the large record arrays (TUs, coefficient levels, PUs, 4x4 grid) into
+        page-locked memory from hevcgpu_host_alloc, as a recorder that writes its records
+        there would: the library uploads them from where they lie, with no staging copy.
+        The generator's own arrays are put back before they are freed."""
+        if getattr(self, "_pinned", None):
+            return self
+        lib = gpu_lib()
+        s = self.syn
+        pinned = []
+        for field, nbytes in self._large_arrays():
+            if nbytes <= 0:
+                continue
+            src = getattr(s, field)
+            p = C.c_void_p()
+            _check(lib.hevcgpu_host_alloc(nbytes, C.byref(p)))
+            C.memmove(p, C.cast(src, C.c_void_p), nbytes)
+            pinned.append((field, C.cast(src, C.c_void_p).value, type(src), p))
+            setattr(s, field, C.cast(p, type(src)))
+        self._pinned = pinned
+        return self
+
+    def _unpin(self):
+        for field, orig, ptype, p in getattr(self, "_pinned", None) or []:
+            setattr(self.syn, field, C.cast(C.c_void_p(orig), ptype))
+            gpu_lib().hevcgpu_host_free(p)
+        self._pinned = None
+
     def close(self):
         if self._p:
+            self._unpin()
             synth_lib().hevcsynth_picture_free(self._p)
             self._p = None
 
@@ -192,6 +227,8 @@ def gpu_lib():
             "hevcgpu_job_prepare": ([P, C.POINTER(PictureSyntax), C.POINTER(P)], C.c_int),
             "hevcgpu_job_free": ([P], None),
             "hevcgpu_job_upload_bytes": ([P], C.c_uint64),
+            "hevcgpu_host_alloc": ([C.c_size_t, C.POINTER(P)], C.c_int),
+            "hevcgpu_host_free": ([P], C.c_int),
             "hevcgpu_job_launch": ([P, C.c_int32], C.c_int),
             "hevcgpu_batch_launch": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
             "hevcgpu_stream_sync": ([P], C.c_int),

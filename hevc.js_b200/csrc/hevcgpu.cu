@@ -377,6 +377,7 @@ struct hevcgpu_job {
     HostBuf pin;      // pinned staging: the record image, then the PicDesc
     size_t desc_off = 0;
     cudaEvent_t desc_copied = nullptr;  // the last PicDesc upload has read the staging copy
+    cudaEvent_t direct_read = nullptr;  // the uploads straight from the caller's arrays are done
     PicDesc host_desc{};
     int32_t n_res[4] = {0, 0, 0, 0};
     const int32_t* d_res[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -402,23 +403,45 @@ struct hevcgpu_job {
             ctx->live_jobs.erase(this);
         }
         if (desc_copied) cudaEventDestroy(desc_copied);
+        if (direct_read) cudaEventDestroy(direct_read);
     }
 };
 
 namespace {
 
 // Host image of a job's device records: offsets into one buffer.  A first pass with
-// out == nullptr only measures; the second pass writes into pinned staging memory.
+// out == nullptr only measures; the second pass writes into pinned staging memory.  An
+// array added as direct (it lies in page-locked memory) keeps its place in the image but
+// is not copied: it is uploaded from where it lies (the regions are listed in direct).
+struct DirectRegion {
+    size_t off;
+    const void* src;
+    size_t bytes;
+};
 struct Packer {
     uint8_t* out = nullptr;
     size_t size = 0;
-    size_t add(const void* src, size_t bytes, size_t align = 256) {
-        size_t off = (size_t)align_up((int64_t)size, (int64_t)align);
+    std::vector<DirectRegion>* direct = nullptr;
+    size_t add(const void* src, size_t bytes, bool is_direct = false) {
+        size_t off = (size_t)align_up((int64_t)size, 256);
         size = off + bytes;
-        if (out && bytes && src) std::memcpy(out + off, src, bytes);
+        if (is_direct) {
+            if (direct && bytes) direct->push_back({off, src, bytes});
+        } else if (out && bytes && src) {
+            std::memcpy(out + off, src, bytes);
+        }
         return off;
     }
 };
+
+// True when p points into page-locked host memory (cudaHostAlloc or registered).
+bool page_locked(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    const bool ok = cudaPointerGetAttributes(&a, p) == cudaSuccess && a.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return ok;
+}
 
 int validate(const hevc_picture_syntax_t* s, bool need_tus, bool need_pus, bool need_filters) {
     if (!s) return fail(HEVCGPU_EINVAL, "null picture syntax");
@@ -757,12 +780,11 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc[2], o_ia, o_idp, o_ito,
         o_itu, o_iro, o_ilo, o_ilv;
     hevc_slice_t dflt{0, 0, 0, 1};
+    // the large caller arrays go last; those in page-locked memory are uploaded directly
+    const bool d_tus = page_locked(s->tus), d_coef = page_locked(s->coeffs), d_pus = page_locked(s->pus),
+               d_blk = page_locked(s->blk);
     auto pack = [&](Packer& pk) {
-        o_tus = pk.add(s->tus, sizeof(hevc_tu_t) * (size_t)std::max(0, s->num_tus));
-        o_coef = pk.add(s->coeffs, sizeof(int16_t) * (size_t)s->num_coeffs);
-        o_pus = pk.add(s->pus, sizeof(hevc_pu_t) * (size_t)std::max(0, s->num_pus));
         o_wp = pk.add(s->wp, sizeof(hevc_wp_t) * (size_t)std::max(0, s->num_wp));
-        o_blk = pk.add(s->blk, s->blk ? sizeof(uint32_t) * (size_t)gw * gh : 0);
         o_sao = pk.add(s->sao, s->sao ? sizeof(hevc_sao_t) * (size_t)nctb : 0);
         o_sl = pk.add(s->ctb_slice, s->ctb_slice ? (size_t)nctb : 0);
         o_ti = pk.add(s->ctb_tile, s->ctb_tile ? sizeof(uint16_t) * (size_t)nctb : 0);
@@ -777,6 +799,10 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         o_iro = pk.add(itu_res.data(), sizeof(int4) * itu_res.size());
         o_ilo = pk.add(ictu_lvl_off.data(), sizeof(int32_t) * ictu_lvl_off.size());
         o_ilv = pk.add(ictu_lvl.data(), sizeof(IntraLevel) * ictu_lvl.size());
+        o_pus = pk.add(s->pus, sizeof(hevc_pu_t) * (size_t)std::max(0, s->num_pus), d_pus);
+        o_blk = pk.add(s->blk, s->blk ? sizeof(uint32_t) * (size_t)gw * gh : 0, d_blk);
+        o_tus = pk.add(s->tus, sizeof(hevc_tu_t) * (size_t)std::max(0, s->num_tus), d_tus);
+        o_coef = pk.add(s->coeffs, sizeof(int16_t) * (size_t)s->num_coeffs, d_coef);
     };
     Packer measure;
     pack(measure);
@@ -785,10 +811,28 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     int rc = j->recs.get(ctx, img);
     if (rc) return rc;
     if ((rc = j->pin.get(ctx, j->desc_off + sizeof(PicDesc)))) return rc;
+    std::vector<DirectRegion> direct;
     Packer write;
     write.out = static_cast<uint8_t*>(j->pin.p);
+    write.direct = &direct;
     pack(write);
-    CUDA_TRY(cudaMemcpyAsync(j->recs.p, j->pin.p, img, cudaMemcpyHostToDevice, ctx->stream));
+    // staged runs between the direct regions, and the direct regions from the caller's memory
+    size_t pos = 0;
+    for (const DirectRegion& d : direct) {
+        if (d.off > pos)
+            CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->recs.p) + pos, static_cast<uint8_t*>(j->pin.p) + pos,
+                                     d.off - pos, cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->recs.p) + d.off, d.src, d.bytes, cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        pos = d.off + d.bytes;
+    }
+    if (img > pos)
+        CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->recs.p) + pos, static_cast<uint8_t*>(j->pin.p) + pos,
+                                 img - pos, cudaMemcpyHostToDevice, ctx->stream));
+    if (!direct.empty()) {
+        if (!j->direct_read) CUDA_TRY(cudaEventCreateWithFlags(&j->direct_read, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventRecord(j->direct_read, ctx->stream));
+    }
     j->upload_bytes = img + sizeof(PicDesc);
     uint8_t* base = static_cast<uint8_t*>(j->recs.p);
 
@@ -863,6 +907,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         j->n_mc[c] = (int32_t)mc[c].size();
         j->d_mc[c] = reinterpret_cast<const uint32_t*>(base + o_mc[c]);
     }
+    // the caller may change its arrays once this returns: the direct uploads must have read them
+    if (!direct.empty()) CUDA_TRY(cudaEventSynchronize(j->direct_read));
     return HEVCGPU_OK;
 }
 
@@ -1541,6 +1587,24 @@ int hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, 
 }
 
 uint64_t hevcgpu_job_upload_bytes(hevcgpu_job_t* job) { return job ? job->upload_bytes : 0; }
+
+int hevcgpu_host_alloc(size_t bytes, void** out) {
+    if (!out) return fail(HEVCGPU_EINVAL, "null out");
+    *out = nullptr;
+    if (bytes == 0) return fail(HEVCGPU_EINVAL, "zero bytes");
+    if (cudaHostAlloc(out, bytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return fail(HEVCGPU_ENOMEM, "cudaHostAlloc of %zu bytes failed", bytes);
+    }
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_host_free(void* p) {
+    if (!p) return HEVCGPU_OK;
+    CUDA_TRY(cudaFreeHost(p));
+    return HEVCGPU_OK;
+}
 
 void hevcgpu_job_free(hevcgpu_job_t* job) {
     if (!job) return;

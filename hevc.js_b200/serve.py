@@ -41,7 +41,9 @@ class PicturePool:
     """Generated syntax per resolution: one I picture and `variants` P/B pictures, each
     P/B one in SLOTS copies whose reference slots match picture index n % SLOTS."""
 
-    def __init__(self, hb, resolutions, variants=2, seed=4, p_cfg=None):
+    def __init__(self, hb, resolutions, variants=2, seed=4, p_cfg=None, pin=False):
+        """pin: keep the pictures' large record arrays in page-locked memory (uploaded
+        without a staging copy)."""
         self.hb = hb
         self.pool = {}
         p_cfg = p_cfg or dict(p_intra=0.1, p_skip=0.2, p_merge=0.3)
@@ -60,6 +62,9 @@ class PicturePool:
                         prm.ref_slot[1][i] = l1[i]
                     by_phase.append(pic)
                 pb.append(by_phase)
+            if pin:
+                for pic in [intra] + [q for ph in pb for q in ph]:
+                    pic.pin()
             self.pool[(w, h)] = (intra, pb)
 
     def picture(self, w, h, i, n, variant):

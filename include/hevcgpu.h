@@ -224,12 +224,21 @@ int  hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void*
 
 /* Prepare a picture: host-side packing (bins, per-CTU intra lists) and one upload of
  * the records into device memory owned by the job.  The job can be launched many
- * times (benchmarks) and is freed with hevcgpu_job_free. */
+ * times (benchmarks) and is freed with hevcgpu_job_free.  The large record arrays (TUs,
+ * coefficient levels, PUs, 4x4 grid) are packed into pinned staging and uploaded from
+ * there; an array that already lies in page-locked memory is uploaded from where it
+ * lies, with no staging copy. */
 int  hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn,
                          hevcgpu_job_t** out);
 void hevcgpu_job_free(hevcgpu_job_t* job);
 /* Bytes the prepare call copied host -> device for this job (records + work lists). */
 uint64_t hevcgpu_job_upload_bytes(hevcgpu_job_t* job);
+/* Page-locked host memory for a recorder's record arrays (the per-picture data the
+ * reference keeps in DecodingContext, decoding/coding_tree.h:60-78, recorded as TU, PU and
+ * grid arrays): arrays in it are uploaded without a staging copy.  Any CUDA device of the
+ * process may be current. */
+int  hevcgpu_host_alloc(size_t bytes, void** out);
+int  hevcgpu_host_free(void* p);
 /* Plain form: one launch per stage for this picture, into DPB slot dst_slot, reading
  * reference slots from params.ref_slot.  Asynchronous on the stream's CUDA stream. */
 int  hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot);

@@ -105,10 +105,15 @@ def test_batched_prepare_and_download(hb, gpu_ctx, port):
         streams.append(st)
         pics.append(pic)
         want.append(port.reconstruct_picture(pic, refs))
-    for rep in range(2):
+    for rep in range(3):
+        if rep == 2:   # records in page-locked memory: uploaded without the staging copy
+            for pic in pics[::2]:
+                pic.pin()
+            for st in streams:
+                st.upload(2, np.zeros(hb.i420_size(st.width, st.height), np.uint8))
         jobs = hb.prepare_batch(streams, pics)
         hb.batch_launch(jobs, [2] * len(jobs))
-        if rep == 0:
+        if rep != 1:
             outs = hb.download_batch(streams, [2] * len(streams))
         else:   # pinned destinations take the copy directly
             outs = [torch.empty(hb.i420_size(st.width, st.height), dtype=torch.uint8).pin_memory().numpy()
