@@ -443,6 +443,38 @@ bool page_locked(const void* p) {
     return ok;
 }
 
+// Branch-free screens of the TU and PU arrays: true when every record passes the checks
+// of validate(); validate() walks the records one by one (to name the first bad one) only
+// when a screen fails.
+bool tus_pass(const hevc_picture_syntax_t* s, int W, int H) {
+    uint32_t bad = 0;
+    const uint32_t ncoef = (uint32_t)s->num_coeffs;
+    for (int i = 0; i < s->num_tus; i++) {
+        const hevc_tu_t& t = s->tus[i];
+        const uint32_t lg = t.log2_size & 7u, n = 1u << lg;
+        const uint32_t pw = t.c_idx ? (uint32_t)W / 2 : (uint32_t)W, ph = t.c_idx ? (uint32_t)H / 2 : (uint32_t)H;
+        bad |= (uint32_t)(t.log2_size - 2u > 3u) | (uint32_t)(t.c_idx > 2) | (uint32_t)(((t.x | t.y) & (n - 1)) != 0) |
+               (uint32_t)(t.x + n > pw) | (uint32_t)(t.y + n > ph) |
+               (uint32_t)((t.flags & HEVC_TU_INTRA) && t.intra_mode > 34);
+        const uint64_t end = (uint64_t)t.coeff_offset + (uint64_t)n * n;
+        bad |= (uint32_t)((t.flags & HEVC_TU_CODED) && ((t.coeff_offset & 15) | (uint32_t)(end > ncoef) |
+                                                        (uint32_t)(t.qp > 51 + 48)));
+    }
+    return bad == 0;
+}
+bool pus_pass(const hevc_picture_syntax_t* s, int W, int H) {
+    uint32_t bad = 0;
+    const int n0 = s->params.num_ref[0], n1 = s->params.num_ref[1];
+    for (int i = 0; i < s->num_pus; i++) {
+        const hevc_pu_t& u = s->pus[i];
+        bad |= (uint32_t)(u.w - 4u > 60u) | (uint32_t)(u.h - 4u > 60u) | ((u.w | u.h | u.x | u.y) & 3u) |
+               (uint32_t)(u.x + u.w > W) | (uint32_t)(u.y + u.h > H) |
+               (uint32_t)(u.ref_idx[0] < 0 && u.ref_idx[1] < 0) | (uint32_t)(u.ref_idx[0] >= n0) |
+               (uint32_t)(u.ref_idx[1] >= n1) | (uint32_t)(u.wp >= s->num_wp);
+    }
+    return bad == 0;
+}
+
 int validate(const hevc_picture_syntax_t* s, bool need_tus, bool need_pus, bool need_filters) {
     if (!s) return fail(HEVCGPU_EINVAL, "null picture syntax");
     const hevc_pic_params_t& p = s->params;
@@ -456,7 +488,7 @@ int validate(const hevc_picture_syntax_t* s, bool need_tus, bool need_pus, bool 
     const int W = p.width, H = p.height;
     if (need_tus) {
         if (s->num_tus < 0 || (s->num_tus && !s->tus)) return fail(HEVCGPU_EINVAL, "bad TU array");
-        for (int i = 0; i < s->num_tus; i++) {
+        for (int i = tus_pass(s, W, H) ? s->num_tus : 0; i < s->num_tus; i++) {
             const hevc_tu_t& t = s->tus[i];
             int n = 1 << t.log2_size, sub = t.c_idx ? 2 : 1;
             if (t.log2_size < 2 || t.log2_size > 5 || t.c_idx > 2 || (t.x % n) || (t.y % n) ||
@@ -476,7 +508,7 @@ int validate(const hevc_picture_syntax_t* s, bool need_tus, bool need_pus, bool 
     if (need_pus) {
         if (s->num_pus < 0 || (s->num_pus && !s->pus)) return fail(HEVCGPU_EINVAL, "bad PU array");
         if (s->num_pus > MC_MAX_PUS) return fail(HEVCGPU_EINVAL, "%d PUs, at most %d", s->num_pus, MC_MAX_PUS);
-        for (int i = 0; i < s->num_pus; i++) {
+        for (int i = pus_pass(s, W, H) ? s->num_pus : 0; i < s->num_pus; i++) {
             const hevc_pu_t& u = s->pus[i];
             if (u.w < 4 || u.h < 4 || u.w > 64 || u.h > 64 || (u.w & 3) || (u.h & 3) || (u.x & 3) || (u.y & 3) ||
                 u.x + u.w > W || u.y + u.h > H)
@@ -731,48 +763,66 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     // MC strips: 4 columns x up to 16 rows of one PU in one plane, one thread each; luma
     // and chroma (Cb and Cr strips) are two lists, each ordered by class: bi-predicted
     // first, then windows inside the picture first, then taller first, so that the
-    // threads of a warp share their path and row count; PU order inside a class.
+    // threads of a warp share their path and row count; PU order inside a class.  One pass
+    // finds each PU's class word in both planes and counts its strips per class by row
+    // band; a second pass writes the items of each row band.
     std::vector<uint32_t> mc[2];
     if (stages & ST_MC) {
+        const int n_pu = s->num_pus, pitch_y = j->lay.pitch_y, pitch_c = j->lay.pitch_c;
+        int32_t cnt[2][33] = {};
+        std::vector<uint8_t> cls((size_t)n_pu * 2);   // per PU and plane: (bi ? 0 : 2) + (inside ? 0 : 1)
+        for (int i = 0; i < n_pu; i++) {
+            const hevc_pu_t& u = s->pus[i];
+            const bool bi = u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0;
+            const int wl = u.w, hl = u.h, wc = u.w / 2, hc = u.h / 2;
+            // list windows at the PU's top-left, extended over the PU: its strips are
+            // inside when every list's window of the whole PU is
+            bool in_l = true, in_c = true;
+            for (int l = 0; l < 2; l++) {
+                if (u.ref_idx[l] < 0) continue;
+                const int mvx = u.mv[l][0], mvy = u.mv[l][1];
+                const int x0 = u.x + (mvx >> 2) - 3, y0 = u.y + (mvy >> 2) - 3;
+                in_l = in_l && mc_inside<false>(x0, y0, hl, W, H, pitch_y) &&
+                       mc_inside<false>(x0 + ((wl - 1) & ~3), y0, hl, W, H, pitch_y);
+                const int cx0 = u.x / 2 + (mvx >> 3) - 1, cy0 = u.y / 2 + (mvy >> 3) - 1;
+                in_c = in_c && mc_inside<true>(cx0, cy0, hc, W / 2, H / 2, pitch_c) &&
+                       mc_inside<true>(cx0 + ((wc - 1) & ~3), cy0, hc, W / 2, H / 2, pitch_c);
+            }
+            const int kl = (bi ? 0 : 2) + (in_l ? 0 : 1), kc = (bi ? 0 : 2) + (in_c ? 0 : 1);
+            cls[2 * (size_t)i] = (uint8_t)kl;
+            cls[2 * (size_t)i + 1] = (uint8_t)kc;
+            // class = kind * (row classes) + (row classes) - rows / (rows per class)
+            const int nl = wl / 4, nc = 2 * ((wc + 3) / 4);
+            for (int sy = 0; sy < hl; sy += MC_STRIP_ROWS)
+                cnt[0][kl * 4 + 4 - std::min(MC_STRIP_ROWS, hl - sy) / 4 + 1] += nl;
+            for (int sy = 0; sy < hc; sy += MC_STRIP_ROWS)
+                cnt[1][kc * 8 + 8 - std::min(MC_STRIP_ROWS, hc - sy) / 2 + 1] += nc;
+        }
         for (int c = 0; c < 2; c++) {
-            const bool chroma = c == 1;
-            const int sub = chroma ? 2 : 1, pw = W / sub, ph = H / sub;
-            const int pitch = chroma ? j->lay.pitch_c : j->lay.pitch_y;
-            const int nrow = chroma ? 8 : 4;   // row classes: rows / 2 (chroma) or rows / 4 (luma)
-            const int ncls = 4 * nrow;
-            int32_t cnt[33] = {};
-            auto each_strip = [&](auto&& emit) {
-                for (int i = 0; i < s->num_pus; i++) {
-                    const hevc_pu_t& u = s->pus[i];
-                    const bool bi = u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0;
-                    const int w = u.w / sub, h = u.h / sub, x = u.x / sub, y = u.y / sub;
-                    // list windows at the PU's top-left, extended over the PU: a strip is
-                    // inside when every list's window of the whole PU is
-                    bool inside = true;
-                    for (int l = 0; l < 2; l++) {
-                        if (u.ref_idx[l] < 0) continue;
-                        const int mvx = u.mv[l][0], mvy = u.mv[l][1];
-                        const int x0 = x + (chroma ? (mvx >> 3) : (mvx >> 2)) - (chroma ? 1 : 3);
-                        const int y0 = y + (chroma ? (mvy >> 3) : (mvy >> 2)) - (chroma ? 1 : 3);
-                        inside = inside && (chroma ? mc_inside<true>(x0, y0, h, pw, ph, pitch) &&
-                                                         mc_inside<true>(x0 + ((w - 1) & ~3), y0, h, pw, ph, pitch)
-                                                   : mc_inside<false>(x0, y0, h, pw, ph, pitch) &&
-                                                         mc_inside<false>(x0 + ((w - 1) & ~3), y0, h, pw, ph, pitch));
-                    }
-                    const int key0 = (bi ? 0 : 2 * nrow) + (inside ? 0 : nrow);
-                    for (int sy = 0; sy < h; sy += MC_STRIP_ROWS) {
-                        const int rows = std::min(MC_STRIP_ROWS, h - sy);
-                        const int key = key0 + nrow - (chroma ? rows / 2 : rows / 4);
-                        for (int pl = 0; pl < (chroma ? 2 : 1); pl++)
-                            for (int sx = 0; sx < w; sx += 4) emit(key, mc_item(i, sx, sy, rows, chroma, pl));
-                    }
+            const int ncls = c ? 32 : 16;
+            for (int k = 1; k <= ncls; k++) cnt[c][k] += cnt[c][k - 1];
+            mc[c].resize((size_t)cnt[c][ncls]);
+        }
+        uint32_t* out_l = mc[0].data();
+        uint32_t* out_c = mc[1].data();
+        for (int i = 0; i < n_pu; i++) {
+            const hevc_pu_t& u = s->pus[i];
+            const int kl = cls[2 * (size_t)i], kc = cls[2 * (size_t)i + 1];
+            for (int sy = 0; sy < u.h; sy += MC_STRIP_ROWS) {
+                const int rows = std::min(MC_STRIP_ROWS, u.h - sy);
+                int32_t& pos = cnt[0][kl * 4 + 4 - rows / 4];
+                uint32_t item = mc_item(i, 0, sy, rows, false, 0);
+                for (int sx = 0; sx < u.w; sx += 4, item += 1u << 20) out_l[pos++] = item;
+            }
+            const int wc = u.w / 2, hc = u.h / 2;
+            for (int sy = 0; sy < hc; sy += MC_STRIP_ROWS) {
+                const int rows = std::min(MC_STRIP_ROWS, hc - sy);
+                int32_t& pos = cnt[1][kc * 8 + 8 - rows / 2];
+                for (int pl = 0; pl < 2; pl++) {
+                    uint32_t item = mc_item(i, 0, sy, rows, true, pl);
+                    for (int sx = 0; sx < wc; sx += 4, item += 1u << 20) out_c[pos++] = item;
                 }
-            };
-            each_strip([&](int key, uint32_t) { cnt[key + 1]++; });
-            for (int k = 1; k <= ncls; k++) cnt[k] += cnt[k - 1];
-            mc[c].resize((size_t)cnt[ncls]);
-            uint32_t* out = mc[c].data();
-            each_strip([&](int key, uint32_t item) { out[cnt[key]++] = item; });
+            }
         }
     }
     j->n_pus = s->num_pus;
