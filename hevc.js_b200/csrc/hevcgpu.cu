@@ -370,7 +370,9 @@ struct hevcgpu_job {
     hevcgpu_ctx* ctx = nullptr;
     hevcgpu_stream* st = nullptr;  // may be null for stage entry points
     Layout lay;
-    DevBuf recs;      // all record arrays + work lists, one upload
+    DevBuf recs;      // the small record arrays + work lists, one upload
+    DevBuf big;       // the caller's large arrays: PUs, 4x4 grid, TUs, coefficient levels
+    HostBuf pin_big;  // pinned staging for those of them not in page-locked memory
     DevBuf rec;       // reconstruction / deblocking buffer (pitched picture)
     DevBuf scratch;   // resid (int16) + motion grid
     DevBuf desc;      // PicDesc
@@ -410,26 +412,14 @@ struct hevcgpu_job {
 namespace {
 
 // Host image of a job's device records: offsets into one buffer.  A first pass with
-// out == nullptr only measures; the second pass writes into pinned staging memory.  An
-// array added as direct (it lies in page-locked memory) keeps its place in the image but
-// is not copied: it is uploaded from where it lies (the regions are listed in direct).
-struct DirectRegion {
-    size_t off;
-    const void* src;
-    size_t bytes;
-};
+// out == nullptr only measures; the second pass writes into pinned staging memory.
 struct Packer {
     uint8_t* out = nullptr;
     size_t size = 0;
-    std::vector<DirectRegion>* direct = nullptr;
-    size_t add(const void* src, size_t bytes, bool is_direct = false) {
+    size_t add(const void* src, size_t bytes) {
         size_t off = (size_t)align_up((int64_t)size, 256);
         size = off + bytes;
-        if (is_direct) {
-            if (direct && bytes) direct->push_back({off, src, bytes});
-        } else if (out && bytes && src) {
-            std::memcpy(out + off, src, bytes);
-        }
+        if (out && bytes && src) std::memcpy(out + off, src, bytes);
         return off;
     }
 };
@@ -559,6 +549,48 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     const int W = p.width, H = p.height, gw = W / 4, gh = H / 4;
     const int ctb = 1 << p.log2_ctb;
     const int wctb = (W + ctb - 1) / ctb, hctb = (H + ctb - 1) / ctb, nctb = wctb * hctb;
+
+    // The caller's large arrays (PUs, 4x4 grid, TUs, coefficient levels) have their own
+    // device buffer and are uploaded first, so that the transfer overlaps the building of
+    // the work lists below: straight from where they lie when they are in page-locked
+    // memory, else through pinned staging.
+    struct BigArray {
+        const void* src;
+        size_t bytes, off;
+        bool direct;
+    };
+    BigArray big[4] = {{s->pus, sizeof(hevc_pu_t) * (size_t)std::max(0, s->num_pus), 0, false},
+                       {s->blk, s->blk ? sizeof(uint32_t) * (size_t)gw * gh : 0, 0, false},
+                       {s->tus, sizeof(hevc_tu_t) * (size_t)std::max(0, s->num_tus), 0, false},
+                       {s->coeffs, sizeof(int16_t) * (size_t)s->num_coeffs, 0, false}};
+    size_t big_bytes = 0;
+    bool any_direct = false, any_staged = false;
+    for (BigArray& b : big) {
+        if (!b.src) b.bytes = 0;
+        b.off = (size_t)align_up((int64_t)big_bytes, 256);
+        big_bytes = b.off + b.bytes;
+        b.direct = b.bytes && page_locked(b.src);
+        any_direct |= b.direct;
+        any_staged |= b.bytes && !b.direct;
+    }
+    big_bytes = std::max<size_t>(big_bytes, 256);
+    int rc = j->big.get(ctx, big_bytes);
+    if (rc) return rc;
+    if (any_staged && (rc = j->pin_big.get(ctx, big_bytes))) return rc;
+    for (const BigArray& b : big) {
+        if (!b.bytes) continue;
+        const void* from = b.src;
+        if (!b.direct) {
+            std::memcpy(static_cast<uint8_t*>(j->pin_big.p) + b.off, b.src, b.bytes);
+            from = static_cast<uint8_t*>(j->pin_big.p) + b.off;
+        }
+        CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->big.p) + b.off, from, b.bytes, cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    }
+    if (any_direct) {   // the caller's arrays must have been read before this call returns
+        if (!j->direct_read) CUDA_TRY(cudaEventCreateWithFlags(&j->direct_read, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventRecord(j->direct_read, ctx->stream));
+    }
 
     // residual bins (coded TUs by size) and the intra TUs in decode order
     std::vector<int32_t> bins[4];
@@ -827,12 +859,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     }
     j->n_pus = s->num_pus;
 
-    size_t o_tus, o_coef, o_pus, o_wp, o_blk, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc[2], o_ia, o_idp, o_ito,
-        o_itu, o_iro, o_ilo, o_ilv;
+    size_t o_wp, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc[2], o_ia, o_idp, o_ito, o_itu, o_iro, o_ilo, o_ilv;
     hevc_slice_t dflt{0, 0, 0, 1};
-    // the large caller arrays go last; those in page-locked memory are uploaded directly
-    const bool d_tus = page_locked(s->tus), d_coef = page_locked(s->coeffs), d_pus = page_locked(s->pus),
-               d_blk = page_locked(s->blk);
     auto pack = [&](Packer& pk) {
         o_wp = pk.add(s->wp, sizeof(hevc_wp_t) * (size_t)std::max(0, s->num_wp));
         o_sao = pk.add(s->sao, s->sao ? sizeof(hevc_sao_t) * (size_t)nctb : 0);
@@ -849,41 +877,19 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         o_iro = pk.add(itu_res.data(), sizeof(int4) * itu_res.size());
         o_ilo = pk.add(ictu_lvl_off.data(), sizeof(int32_t) * ictu_lvl_off.size());
         o_ilv = pk.add(ictu_lvl.data(), sizeof(IntraLevel) * ictu_lvl.size());
-        o_pus = pk.add(s->pus, sizeof(hevc_pu_t) * (size_t)std::max(0, s->num_pus), d_pus);
-        o_blk = pk.add(s->blk, s->blk ? sizeof(uint32_t) * (size_t)gw * gh : 0, d_blk);
-        o_tus = pk.add(s->tus, sizeof(hevc_tu_t) * (size_t)std::max(0, s->num_tus), d_tus);
-        o_coef = pk.add(s->coeffs, sizeof(int16_t) * (size_t)s->num_coeffs, d_coef);
     };
     Packer measure;
     pack(measure);
     const size_t img = std::max<size_t>(measure.size, 256);
     j->desc_off = (size_t)align_up((int64_t)img, 256);
-    int rc = j->recs.get(ctx, img);
-    if (rc) return rc;
+    if ((rc = j->recs.get(ctx, img))) return rc;
     if ((rc = j->pin.get(ctx, j->desc_off + sizeof(PicDesc)))) return rc;
-    std::vector<DirectRegion> direct;
     Packer write;
     write.out = static_cast<uint8_t*>(j->pin.p);
-    write.direct = &direct;
     pack(write);
-    // staged runs between the direct regions, and the direct regions from the caller's memory
-    size_t pos = 0;
-    for (const DirectRegion& d : direct) {
-        if (d.off > pos)
-            CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->recs.p) + pos, static_cast<uint8_t*>(j->pin.p) + pos,
-                                     d.off - pos, cudaMemcpyHostToDevice, ctx->stream));
-        CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->recs.p) + d.off, d.src, d.bytes, cudaMemcpyHostToDevice,
-                                 ctx->stream));
-        pos = d.off + d.bytes;
-    }
-    if (img > pos)
-        CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->recs.p) + pos, static_cast<uint8_t*>(j->pin.p) + pos,
-                                 img - pos, cudaMemcpyHostToDevice, ctx->stream));
-    if (!direct.empty()) {
-        if (!j->direct_read) CUDA_TRY(cudaEventCreateWithFlags(&j->direct_read, cudaEventDisableTiming));
-        CUDA_TRY(cudaEventRecord(j->direct_read, ctx->stream));
-    }
-    j->upload_bytes = img + sizeof(PicDesc);
+    CUDA_TRY(cudaMemcpyAsync(j->recs.p, j->pin.p, img, cudaMemcpyHostToDevice, ctx->stream));
+    j->upload_bytes = big_bytes + img + sizeof(PicDesc);
+    uint8_t* big_base = static_cast<uint8_t*>(j->big.p);
     uint8_t* base = static_cast<uint8_t*>(j->recs.p);
 
     size_t resid_bytes = j->has_intra ? sizeof(int16_t) * (size_t)align_up((int64_t)s->num_coeffs, 128) : 0;
@@ -906,12 +912,12 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         D.num_ref[l] = p.num_ref[l];
         for (int i = 0; i < 16; i++) D.ref_poc[l][i] = p.ref_poc[l][i];
     }
-    D.tus = reinterpret_cast<const hevc_tu_t*>(base + o_tus);
-    D.coeffs = reinterpret_cast<const int16_t*>(base + o_coef);
+    D.tus = reinterpret_cast<const hevc_tu_t*>(big_base + big[2].off);
+    D.coeffs = reinterpret_cast<const int16_t*>(big_base + big[3].off);
     D.resid = resid_bytes ? static_cast<int16_t*>(j->scratch.p) : nullptr;
-    D.pus = reinterpret_cast<const hevc_pu_t*>(base + o_pus);
+    D.pus = reinterpret_cast<const hevc_pu_t*>(big_base + big[0].off);
     D.wp = reinterpret_cast<const hevc_wp_t*>(base + o_wp);
-    D.blk = s->blk ? reinterpret_cast<const uint32_t*>(base + o_blk) : nullptr;
+    D.blk = s->blk ? reinterpret_cast<const uint32_t*>(big_base + big[1].off) : nullptr;
     D.mot = mot_bytes ? reinterpret_cast<MotionEnt*>(static_cast<uint8_t*>(j->scratch.p) + resid_bytes) : nullptr;
     D.sao = s->sao ? reinterpret_cast<const hevc_sao_t*>(base + o_sao) : nullptr;
     D.ctb_slice = s->ctb_slice ? base + o_sl : nullptr;
@@ -958,7 +964,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         j->d_mc[c] = reinterpret_cast<const uint32_t*>(base + o_mc[c]);
     }
     // the caller may change its arrays once this returns: the direct uploads must have read them
-    if (!direct.empty()) CUDA_TRY(cudaEventSynchronize(j->direct_read));
+    if (any_direct) CUDA_TRY(cudaEventSynchronize(j->direct_read));
     return HEVCGPU_OK;
 }
 
