@@ -541,7 +541,20 @@ enum StageMask : int {
 };
 
 // Build the host image, upload it and fill host_desc (except dst/ref pointers).
+// Work vectors of job_build, kept per host thread (the context's workers live as long as
+// the context), so that their memory is reused from one picture to the next: no allocation
+// and no first-touch page faults per picture.
+struct BuildScratch {
+    std::vector<int32_t> bins[4], intra_list, itu, level, ctu_of, order, owner[3];
+    std::vector<hevc_tu_t> itu_rec;
+    std::vector<int4> itu_res;
+    std::vector<uint32_t> mc[2];
+    std::vector<uint8_t> mc_cls;
+};
+thread_local BuildScratch t_build;
+
 int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
+    BuildScratch& BS = t_build;
     hevcgpu_ctx* ctx = j->ctx;
     const hevc_pic_params_t& p = s->params;
     j->params = p;
@@ -593,8 +606,10 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     }
 
     // residual bins (coded TUs by size) and the intra TUs in decode order
-    std::vector<int32_t> bins[4];
-    std::vector<int32_t> intra_list;
+    auto& bins = BS.bins;
+    auto& intra_list = BS.intra_list;
+    for (auto& v : bins) v.clear();
+    intra_list.clear();
     for (auto& v : bins) v.reserve((size_t)s->num_tus / 2);
     intra_list.reserve((size_t)s->num_tus);
     for (int i = 0; i < s->num_tus; i++) {
@@ -611,12 +626,19 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     // for that CTU.  A unit whose samples B may not use (availability) can only add an
     // unneeded level or wait, never change a sample.
     const int n_intra = (int)intra_list.size();
-    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, itu, ictu_lvl_off;
-    std::vector<hevc_tu_t> itu_rec;     // intra TU records in task order
-    std::vector<int4> itu_res;          // per task entry: residual source, staged offset, 16-byte chunks
+    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, ictu_lvl_off;
+    auto& itu = BS.itu;
+    auto& itu_rec = BS.itu_rec;         // intra TU records in task order
+    auto& itu_res = BS.itu_res;         // per task entry: residual source, staged offset, 16-byte chunks
+    itu.clear();
+    itu_rec.clear();
+    itu_res.clear();
     std::vector<IntraLevel> ictu_lvl;
     if (n_intra) {
-        std::vector<int32_t> level((size_t)n_intra, 0), ctu_of((size_t)n_intra, 0);
+        auto& level = BS.level;
+        auto& ctu_of = BS.ctu_of;
+        level.assign((size_t)n_intra, 0);
+        ctu_of.assign((size_t)n_intra, 0);
         std::vector<int32_t> dep_list((size_t)nctb * 4, -1), dep_n((size_t)nctb, 0);   // by CTU address
         std::vector<std::vector<int32_t>> ctu_deps((size_t)nctb);
         // cross-CTU requirements: (CTU, level, dependency CTU address, levels it must have done)
@@ -625,7 +647,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         std::vector<std::pair<int32_t, int32_t>> pending;           // (dep CTU, need) of one TU
         std::vector<std::vector<uint8_t>> publish((size_t)nctb);     // by CTU address and level
         // owner maps: (CTU address << 16) | level of the latest intra TU per 4x4 unit, -1 none
-        std::vector<int32_t> owner[3];
+        auto& owner = BS.owner;
         int uw[3], uh[3];
         for (int c = 0; c < 3; c++) {
             uw[c] = (c ? W / 2 : W) / 4;
@@ -686,7 +708,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         }
         // order by (CTU raster address, level, decode order): the TUs come CTU by CTU in
         // decode order, so a counting sort by level within each CTU's run keeps it stable
-        std::vector<int32_t> order((size_t)n_intra);
+        auto& order = BS.order;
+        order.resize((size_t)n_intra);
         bool grouped = true;
         for (int b = 1; b < n_intra && grouped; b++) grouped = ctu_of[(size_t)b] >= ctu_of[(size_t)b - 1];
         if (grouped) {
@@ -798,11 +821,14 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     // threads of a warp share their path and row count; PU order inside a class.  One pass
     // finds each PU's class word in both planes and counts its strips per class by row
     // band; a second pass writes the items of each row band.
-    std::vector<uint32_t> mc[2];
+    auto& mc = BS.mc;
+    mc[0].clear();
+    mc[1].clear();
     if (stages & ST_MC) {
         const int n_pu = s->num_pus, pitch_y = j->lay.pitch_y, pitch_c = j->lay.pitch_c;
         int32_t cnt[2][33] = {};
-        std::vector<uint8_t> cls((size_t)n_pu * 2);   // per PU and plane: (bi ? 0 : 2) + (inside ? 0 : 1)
+        auto& cls = BS.mc_cls;   // per PU and plane: (bi ? 0 : 2) + (inside ? 0 : 1)
+        cls.resize((size_t)n_pu * 2);
         for (int i = 0; i < n_pu; i++) {
             const hevc_pu_t& u = s->pus[i];
             const bool bi = u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0;
