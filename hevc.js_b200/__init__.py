@@ -125,38 +125,51 @@ class Picture:
         synth_lib().hevcsynth_bs_histogram(self.syn_ptr, out)
         return list(out)
 
-    # the large record arrays: (field, bytes)
+    # the large record arrays: (field, bytes), in the order and 256-byte alignment of the
+    # device buffer that job preparation uploads them into
     def _large_arrays(self):
         s = self.syn
         grid = (s.params.width // 4) * (s.params.height // 4) * 4 if s.blk else 0
-        return [("tus", 16 * s.num_tus), ("coeffs", 2 * s.num_coeffs), ("pus", 20 * s.num_pus), ("blk", grid)]
+        return [("pus", 20 * s.num_pus), ("blk", grid), ("tus", 16 * s.num_tus), ("coeffs", 2 * s.num_coeffs)]
 
     def pin(self):
-        """Moves the large record arrays (TUs, coefficient levels, PUs, 4x4 grid) into
-        page-locked memory from hevcgpu_host_alloc, as a recorder that writes its records
-        there would: the library uploads them from where they lie, with no staging copy.
-        The generator's own arrays are put back before they are freed."""
+        """Moves the large record arrays (PUs, 4x4 grid, TUs, coefficient levels) into one
+        block of page-locked memory from hevcgpu_host_alloc, laid out as the device buffer
+        they go to (each at a 256-byte aligned offset, in that order), as a recorder that
+        writes its records there would: the library uploads them from there in one copy, with
+        no staging.  The generator's own arrays are put back before they are freed."""
         if getattr(self, "_pinned", None):
             return self
         lib = gpu_lib()
         s = self.syn
-        pinned = []
+        layout, end = [], 0
         for field, nbytes in self._large_arrays():
-            if nbytes <= 0:
+            if nbytes <= 0 or not getattr(s, field):
                 continue
+            off = (end + 255) // 256 * 256
+            layout.append((field, nbytes, off))
+            end = off + nbytes
+        if not layout:
+            return self
+        block = C.c_void_p()
+        _check(lib.hevcgpu_host_alloc(end, C.byref(block)))
+        moved = []
+        for field, nbytes, off in layout:
             src = getattr(s, field)
-            p = C.c_void_p()
-            _check(lib.hevcgpu_host_alloc(nbytes, C.byref(p)))
-            C.memmove(p, C.cast(src, C.c_void_p), nbytes)
-            pinned.append((field, C.cast(src, C.c_void_p).value, type(src), p))
-            setattr(s, field, C.cast(p, type(src)))
-        self._pinned = pinned
+            dst = block.value + off
+            C.memmove(dst, C.cast(src, C.c_void_p), nbytes)
+            moved.append((field, C.cast(src, C.c_void_p).value, type(src)))
+            setattr(s, field, C.cast(C.c_void_p(dst), type(src)))
+        self._pinned = (block, moved)
         return self
 
     def _unpin(self):
-        for field, orig, ptype, p in getattr(self, "_pinned", None) or []:
-            setattr(self.syn, field, C.cast(C.c_void_p(orig), ptype))
-            gpu_lib().hevcgpu_host_free(p)
+        pinned = getattr(self, "_pinned", None)
+        if pinned:
+            block, moved = pinned
+            for field, orig, ptype in moved:
+                setattr(self.syn, field, C.cast(C.c_void_p(orig), ptype))
+            gpu_lib().hevcgpu_host_free(block)
         self._pinned = None
 
     def close(self):

@@ -396,10 +396,13 @@ struct hevcgpu_job {
     uint64_t upload_bytes = 0;          // host -> device bytes of the prepare call
     hevc_pic_params_t params{};
     ~hevcgpu_job() {
-        // buffers go back to the pools only after every queued use of them has run
-        if (ctx) cudaStreamSynchronize(ctx->stream);
+        // buffers go back to the pools only after every queued use of them has run: a job's
+        // uploads all precede its launches (the launching stream waits for the context
+        // stream, and descriptor copies go on the launching stream), so the completion of its
+        // last batch covers them; a job never launched waits for the context stream
         if (last_done) cudaEventSynchronize(last_done);   // the job's last batch, not later ones
         else if (last_stream) cudaStreamSynchronize(last_stream);
+        else if (ctx) cudaStreamSynchronize(ctx->stream);
         if (registered) {
             std::lock_guard<std::mutex> g(ctx->jobs_mu);
             ctx->live_jobs.erase(this);
@@ -546,6 +549,10 @@ enum StageMask : int {
 // and no first-touch page faults per picture.
 struct BuildScratch {
     std::vector<int32_t> bins[4], intra_list, itu, level, ctu_of, order, owner[3];
+    // an owner map entry is valid when its stamp is this picture's generation, so the maps
+    // need no clearing between pictures
+    std::vector<uint32_t> owner_gen[3];
+    uint32_t gen = 0;
     std::vector<hevc_tu_t> itu_rec;
     std::vector<int4> itu_res;
     std::vector<uint32_t> mc[2];
@@ -590,15 +597,37 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     int rc = j->big.get(ctx, big_bytes);
     if (rc) return rc;
     if (any_staged && (rc = j->pin_big.get(ctx, big_bytes))) return rc;
+    // Page-locked arrays that sit in one block in this same layout (each at its offset from
+    // one base, as a recorder that lays them out so puts them) go up in one copy: the gaps
+    // between them are under 256 bytes, so every byte copied lies on a page that holds array
+    // data.
+    const uint8_t* host0 = nullptr;
+    size_t first = 0, used = 0;
+    bool one_block = any_direct && !any_staged;
     for (const BigArray& b : big) {
         if (!b.bytes) continue;
-        const void* from = b.src;
-        if (!b.direct) {
-            std::memcpy(static_cast<uint8_t*>(j->pin_big.p) + b.off, b.src, b.bytes);
-            from = static_cast<uint8_t*>(j->pin_big.p) + b.off;
+        const uint8_t* h = static_cast<const uint8_t*>(b.src) - b.off;
+        if (!host0) {
+            host0 = h;
+            first = b.off;
         }
-        CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->big.p) + b.off, from, b.bytes, cudaMemcpyHostToDevice,
-                                 ctx->stream));
+        one_block = one_block && h == host0;
+        used = b.off + b.bytes;
+    }
+    if (one_block && host0) {
+        CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->big.p) + first, host0 + first, used - first,
+                                 cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        for (const BigArray& b : big) {
+            if (!b.bytes) continue;
+            const void* from = b.src;
+            if (!b.direct) {
+                std::memcpy(static_cast<uint8_t*>(j->pin_big.p) + b.off, b.src, b.bytes);
+                from = static_cast<uint8_t*>(j->pin_big.p) + b.off;
+            }
+            CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->big.p) + b.off, from, b.bytes, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+        }
     }
     if (any_direct) {   // the caller's arrays must have been read before this call returns
         if (!j->direct_read) CUDA_TRY(cudaEventCreateWithFlags(&j->direct_read, cudaEventDisableTiming));
@@ -646,13 +675,23 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         std::vector<Req> reqs;
         std::vector<std::pair<int32_t, int32_t>> pending;           // (dep CTU, need) of one TU
         std::vector<std::vector<uint8_t>> publish((size_t)nctb);     // by CTU address and level
-        // owner maps: (CTU address << 16) | level of the latest intra TU per 4x4 unit, -1 none
+        // owner maps: (CTU address << 16) | level of the latest intra TU per 4x4 unit, valid
+        // where the unit's stamp is this picture's generation (else no owner)
         auto& owner = BS.owner;
         int uw[3], uh[3];
+        if (++BS.gen == 0) {   // wrapped: every old stamp must differ from the new generation
+            for (auto& g : BS.owner_gen) std::fill(g.begin(), g.end(), 0u);
+            BS.gen = 1;
+        }
+        const uint32_t gen = BS.gen;
         for (int c = 0; c < 3; c++) {
             uw[c] = (c ? W / 2 : W) / 4;
             uh[c] = (c ? H / 2 : H) / 4;
-            owner[c].assign((size_t)uw[c] * uh[c], -1);
+            const size_t nu = (size_t)uw[c] * uh[c];
+            if (owner[c].size() < nu) {
+                owner[c].resize(nu);
+                BS.owner_gen[c].resize(nu, 0u);
+            }
         }
         for (int b = 0; b < n_intra; b++) {
             const hevc_tu_t& t = s->tus[intra_list[(size_t)b]];
@@ -660,7 +699,9 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             const int a = ((t.y * sub) >> p.log2_ctb) * wctb + ((t.x * sub) >> p.log2_ctb);
             ctu_of[(size_t)b] = a;
             int32_t* own = owner[c].data();
+            uint32_t* own_gen = BS.owner_gen[c].data();
             const int row = uw[c];
+            auto owner_at = [&](size_t u) { return own_gen[u] == gen ? own[u] : -1; };
             int lv = 0;
             auto dep = [&](int32_t o) {
                 if (o < 0) return;
@@ -683,14 +724,14 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
                 pb[(size_t)ol] = 1;
             };
             if (t.y > 0) {
-                const int32_t* r = own + (size_t)((t.y - 1) / 4) * row;
+                const size_t r = (size_t)((t.y - 1) / 4) * row;
                 const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(row - 1, (t.x + 2 * n - 1) / 4);
-                for (int ux = ux0; ux <= ux1; ux++) dep(r[ux]);
+                for (int ux = ux0; ux <= ux1; ux++) dep(owner_at(r + ux));
             }
             if (t.x > 0) {
                 const int ux = (t.x - 1) / 4;
                 const int uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
-                for (int uy = uy0; uy <= uy1; uy++) dep(own[(size_t)uy * row + ux]);
+                for (int uy = uy0; uy <= uy1; uy++) dep(owner_at((size_t)uy * row + ux));
             }
             if (lv > 0xFFFF) return fail(HEVCGPU_EINVAL, "intra dependency chain too deep in CTU %d", a);
             level[(size_t)b] = lv;
@@ -698,8 +739,11 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             pending.clear();
             const int32_t mark = (a << 16) | lv;
             for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++) {
-                int32_t* r = own + (size_t)uy * row;
-                for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) r[ux] = mark;
+                const size_t r = (size_t)uy * row;
+                for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) {
+                    own[r + ux] = mark;
+                    own_gen[r + ux] = gen;
+                }
             }
         }
         for (int a = 0; a < nctb; a++) {
@@ -1690,9 +1734,7 @@ int hevcgpu_host_free(void* p) {
 
 void hevcgpu_job_free(hevcgpu_job_t* job) {
     if (!job) return;
-    cudaStreamSynchronize(job->ctx->stream);
-    if (job->last_stream) cudaStreamSynchronize(job->last_stream);
-    delete job;
+    delete job;   // waits for the job's own last use (see ~hevcgpu_job)
 }
 
 namespace {
