@@ -555,6 +555,14 @@ struct BuildScratch {
     uint32_t gen = 0;
     std::vector<hevc_tu_t> itu_rec;
     std::vector<int4> itu_res;
+    // intra schedule
+    struct Req { int32_t a, lv, dep, need; };
+    std::vector<Req> reqs;
+    std::vector<int32_t> dep_list, dep_n, index_of, nlev, cnt;
+    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, ictu_lvl_off;
+    std::vector<IntraLevel> ictu_lvl;
+    std::vector<std::array<uint16_t, 4>> req;
+    std::vector<uint8_t> publish;
     std::vector<uint32_t> mc[2];
     std::vector<uint8_t> mc_cls;
 };
@@ -655,26 +663,36 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     // for that CTU.  A unit whose samples B may not use (availability) can only add an
     // unneeded level or wait, never change a sample.
     const int n_intra = (int)intra_list.size();
-    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, ictu_lvl_off;
+    auto& ictu_addr = BS.ictu_addr;
+    auto& ictu_deps = BS.ictu_deps;
+    auto& ictu_tu_off = BS.ictu_tu_off;
+    auto& ictu_lvl_off = BS.ictu_lvl_off;
+    auto& ictu_lvl = BS.ictu_lvl;
     auto& itu = BS.itu;
     auto& itu_rec = BS.itu_rec;         // intra TU records in task order
     auto& itu_res = BS.itu_res;         // per task entry: residual source, staged offset, 16-byte chunks
+    ictu_addr.clear();
+    ictu_deps.clear();
+    ictu_tu_off.clear();
+    ictu_lvl_off.clear();
+    ictu_lvl.clear();
     itu.clear();
     itu_rec.clear();
     itu_res.clear();
-    std::vector<IntraLevel> ictu_lvl;
     if (n_intra) {
         auto& level = BS.level;
         auto& ctu_of = BS.ctu_of;
-        level.assign((size_t)n_intra, 0);
-        ctu_of.assign((size_t)n_intra, 0);
-        std::vector<int32_t> dep_list((size_t)nctb * 4, -1), dep_n((size_t)nctb, 0);   // by CTU address
-        std::vector<std::vector<int32_t>> ctu_deps((size_t)nctb);
-        // cross-CTU requirements: (CTU, level, dependency CTU address, levels it must have done)
-        struct Req { int32_t a, lv, dep, need; };
-        std::vector<Req> reqs;
-        std::vector<std::pair<int32_t, int32_t>> pending;           // (dep CTU, need) of one TU
-        std::vector<std::vector<uint8_t>> publish((size_t)nctb);     // by CTU address and level
+        level.resize((size_t)n_intra);
+        ctu_of.resize((size_t)n_intra);
+        // up to 4 dependency CTU addresses per CTU address (dep_n counts past 4 to report)
+        auto& dep_list = BS.dep_list;
+        auto& dep_n = BS.dep_n;
+        dep_list.assign((size_t)nctb * 4, -1);
+        dep_n.assign((size_t)nctb, 0);
+        // cross-CTU requirements: (CTU, level, dependency CTU address, levels it must have
+        // done); the dependency publishes after level need - 1
+        auto& reqs = BS.reqs;
+        reqs.clear();
         // owner maps: (CTU address << 16) | level of the latest intra TU per 4x4 unit, valid
         // where the unit's stamp is this picture's generation (else no owner)
         auto& owner = BS.owner;
@@ -701,42 +719,41 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
             int32_t* own = owner[c].data();
             uint32_t* own_gen = BS.owner_gen[c].data();
             const int row = uw[c];
-            auto owner_at = [&](size_t u) { return own_gen[u] == gen ? own[u] : -1; };
+            const size_t r0 = reqs.size();
             int lv = 0;
-            auto dep = [&](int32_t o) {
-                if (o < 0) return;
+            int32_t last = -1;   // a run of units with one owner adds what its first unit added
+            auto dep = [&](size_t u) {
+                const int32_t o = own_gen[u] == gen ? own[u] : -1;
+                if (o < 0 || o == last) return;
+                last = o;
                 const int oa = o >> 16, ol = o & 0xFFFF;
                 if (oa == a) {
                     lv = std::max(lv, ol + 1);
                     return;
                 }
                 int32_t* dl = &dep_list[(size_t)a * 4];
-                int& dn = dep_n[(size_t)a];
+                int32_t& dn = dep_n[(size_t)a];
                 bool have = false;
-                for (int q = 0; q < dn; q++) have |= dl[q] == oa;
+                for (int q = 0; q < std::min<int32_t>(dn, 4); q++) have |= dl[q] == oa;
                 if (!have) {
                     if (dn < 4) dl[dn] = oa;
                     dn++;
                 }
-                pending.emplace_back(oa, ol + 1);
-                std::vector<uint8_t>& pb = publish[(size_t)oa];
-                if (pb.size() <= (size_t)ol) pb.resize((size_t)ol + 1, 0);
-                pb[(size_t)ol] = 1;
+                reqs.push_back({a, 0, oa, ol + 1});
             };
             if (t.y > 0) {
                 const size_t r = (size_t)((t.y - 1) / 4) * row;
                 const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(row - 1, (t.x + 2 * n - 1) / 4);
-                for (int ux = ux0; ux <= ux1; ux++) dep(owner_at(r + ux));
+                for (int ux = ux0; ux <= ux1; ux++) dep(r + ux);
             }
             if (t.x > 0) {
                 const int ux = (t.x - 1) / 4;
                 const int uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
-                for (int uy = uy0; uy <= uy1; uy++) dep(owner_at((size_t)uy * row + ux));
+                for (int uy = uy0; uy <= uy1; uy++) dep((size_t)uy * row + ux);
             }
             if (lv > 0xFFFF) return fail(HEVCGPU_EINVAL, "intra dependency chain too deep in CTU %d", a);
             level[(size_t)b] = lv;
-            for (const auto& pd : pending) reqs.push_back({a, lv, pd.first, pd.second});
-            pending.clear();
+            for (size_t q = r0; q < reqs.size(); q++) reqs[q].lv = lv;
             const int32_t mark = (a << 16) | lv;
             for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++) {
                 const size_t r = (size_t)uy * row;
@@ -746,10 +763,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
                 }
             }
         }
-        for (int a = 0; a < nctb; a++) {
+        for (int a = 0; a < nctb; a++)
             if (dep_n[(size_t)a] > 4) return fail(HEVCGPU_EINVAL, "CTU %d depends on %d CTUs", a, dep_n[(size_t)a]);
-            ctu_deps[(size_t)a].assign(&dep_list[(size_t)a * 4], &dep_list[(size_t)a * 4] + dep_n[(size_t)a]);
-        }
         // order by (CTU raster address, level, decode order): the TUs come CTU by CTU in
         // decode order, so a counting sort by level within each CTU's run keeps it stable
         auto& order = BS.order;
@@ -757,7 +772,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         bool grouped = true;
         for (int b = 1; b < n_intra && grouped; b++) grouped = ctu_of[(size_t)b] >= ctu_of[(size_t)b - 1];
         if (grouped) {
-            std::vector<int32_t> cnt;
+            auto& cnt = BS.cnt;
             for (int r0 = 0; r0 < n_intra;) {
                 int r1 = r0, maxl = 0;
                 while (r1 < n_intra && ctu_of[(size_t)r1] == ctu_of[(size_t)r0]) maxl = std::max(maxl, level[(size_t)r1++]);
@@ -807,18 +822,19 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         }
         // dependencies by intra-CTU index (earlier CTUs in raster order: at most left,
         // above-left, above and above-right)
-        std::vector<int32_t> index_of((size_t)nctb, -1);
+        auto& index_of = BS.index_of;
+        index_of.assign((size_t)nctb, -1);
         for (int k = 0; k < nic; k++) index_of[(size_t)ictu_addr[(size_t)k]] = k;
         ictu_deps.assign((size_t)nic * 4, -1);
         for (int k = 0; k < nic; k++) {
-            const std::vector<int32_t>& dl = ctu_deps[(size_t)ictu_addr[(size_t)k]];
-            if (dl.size() > 4) return fail(HEVCGPU_EINVAL, "CTU %d depends on %zu CTUs", ictu_addr[(size_t)k], dl.size());
-            for (size_t q = 0; q < dl.size(); q++) ictu_deps[(size_t)k * 4 + q] = index_of[(size_t)dl[q]];
+            const size_t a = (size_t)ictu_addr[(size_t)k];
+            for (int q = 0; q < dep_n[a]; q++) ictu_deps[(size_t)k * 4 + q] = index_of[(size_t)dep_list[a * 4 + q]];
         }
         // per CTU level: the levels each dependency slot must have completed before it runs
         // (only where the requirement rises) and whether dependents wait for its completion
         ictu_lvl_off.resize((size_t)nic + 1);
-        std::vector<int32_t> nlev((size_t)nic, 0);
+        auto& nlev = BS.nlev;
+        nlev.resize((size_t)nic);
         for (int k = 0; k < nic; k++) {
             const int last = ictu_tu_off[(size_t)k + 1] - 1;
             nlev[(size_t)k] = level[(size_t)order[(size_t)last]] + 1;
@@ -826,23 +842,27 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         }
         ictu_lvl_off[(size_t)nic] = nic ? ictu_lvl_off[(size_t)nic - 1] + nlev[(size_t)nic - 1] : 0;
         const size_t nlv = (size_t)ictu_lvl_off[(size_t)nic];
-        std::vector<std::array<uint16_t, 4>> req(nlv, std::array<uint16_t, 4>{0, 0, 0, 0});
-        for (const Req& r : reqs) {
+        auto& req = BS.req;
+        req.assign(nlv, std::array<uint16_t, 4>{0, 0, 0, 0});
+        auto& publish = BS.publish;   // by level entry: dependents wait for that level
+        publish.assign(nlv, 0);
+        for (const BuildScratch::Req& r : reqs) {
             const int k = index_of[(size_t)r.a];
-            const std::vector<int32_t>& dl = ctu_deps[(size_t)r.a];
-            const int slot = (int)(std::find(dl.begin(), dl.end(), r.dep) - dl.begin());
+            const int32_t* dl = &dep_list[(size_t)r.a * 4];
+            const int slot = (int)(std::find(dl, dl + dep_n[(size_t)r.a], r.dep) - dl);
             uint16_t& q = req[(size_t)(ictu_lvl_off[(size_t)k] + r.lv)][(size_t)slot];
             q = (uint16_t)std::max<int>(q, r.need);
+            publish[(size_t)(ictu_lvl_off[(size_t)index_of[(size_t)r.dep]] + r.need - 1)] = 1;
         }
         // one padding entry: the kernel stages levels in 16-byte pairs from an even entry
         ictu_lvl.assign(nlv + 1, IntraLevel{0u, 0u});
         for (int k = 0; k < nic; k++) {
             uint16_t seen[4] = {0, 0, 0, 0};
-            const std::vector<uint8_t>& pb = publish[(size_t)ictu_addr[(size_t)k]];
             const int t0 = ictu_tu_off[(size_t)k], t1 = ictu_tu_off[(size_t)k + 1];
             int i = t0;
             for (int L = 0; L < nlev[(size_t)k]; L++) {
-                std::array<uint16_t, 4>& rq = req[(size_t)(ictu_lvl_off[(size_t)k] + L)];
+                const size_t e_at = (size_t)(ictu_lvl_off[(size_t)k] + L);
+                std::array<uint16_t, 4>& rq = req[e_at];
                 for (int q = 0; q < 4; q++) {
                     if (rq[(size_t)q] > seen[q]) seen[q] = rq[(size_t)q];
                     else rq[(size_t)q] = 0;   // already satisfied by an earlier check
@@ -851,10 +871,10 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
                 if (i - t0 > INTRA_FIELD_MAX || rq[0] > INTRA_FIELD_MAX || rq[1] > INTRA_FIELD_MAX ||
                     rq[2] > INTRA_FIELD_MAX || rq[3] > INTRA_FIELD_MAX)
                     return fail(HEVCGPU_EINVAL, "CTU %d intra schedule out of range", ictu_addr[(size_t)k]);
-                IntraLevel& e = ictu_lvl[(size_t)(ictu_lvl_off[(size_t)k] + L)];
+                IntraLevel& e = ictu_lvl[e_at];
                 e.x = (uint32_t)rq[0] | ((uint32_t)rq[1] << 10) | ((uint32_t)rq[2] << 20);
                 e.y = (uint32_t)rq[3] | ((uint32_t)(i - t0) << 10);
-                if ((size_t)L < pb.size() && pb[(size_t)L]) e.x |= INTRA_LEVEL_PUBLISH;
+                if (publish[e_at]) e.x |= INTRA_LEVEL_PUBLISH;
             }
         }
     }
