@@ -29,7 +29,7 @@ import weakref
 import numpy as np
 
 from . import abi
-from .abi import (TU, PU, WP, SAO, Slice, PicParams, PictureSyntax, SynthCfg, SynthPicture,
+from .abi import (TU, PU, WP, SAO, Slice, Scaling, PicParams, PictureSyntax, SynthCfg, SynthPicture,
                   i420_size, split_i420, as_ptr, ptr_array, md5_planes)
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -66,6 +66,8 @@ def synth_lib():
         lib.hevcsynth_blocks.argtypes = [C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.POINTER(TU),
                                          C.POINTER(C.c_int16), C.POINTER(C.c_uint8)]
         lib.hevcsynth_blocks.restype = C.c_int64
+        lib.hevcsynth_scaling.argtypes = [C.c_uint64, C.POINTER(Scaling)]
+        lib.hevcsynth_scaling.restype = C.c_int
         lib.hevcsynth_bs_histogram.argtypes = [C.POINTER(PictureSyntax), C.POINTER(C.c_int64)]
         lib.hevcsynth_bs_histogram.restype = C.c_int
         _synth = lib
@@ -205,6 +207,14 @@ def blocks(num_tus, seed, qp_min=22, qp_max=37):
     return tus, num_tus, coeffs, pred
 
 
+def scaling(seed):
+    """Scaling lists (hevc_scaling_t) drawn by the generator from seed."""
+    sl = Scaling()
+    if synth_lib().hevcsynth_scaling(seed, C.byref(sl)) != 0:
+        raise ValueError("hevcsynth_scaling failed")
+    return sl
+
+
 # --------------------------------------------------------------------------- GPU library
 
 def gpu_lib():
@@ -224,6 +234,8 @@ def gpu_lib():
             "hevcgpu_sync": ([P], C.c_int),
             "hevcgpu_residual_blocks": ([P, C.POINTER(TU), C.c_int32, C.POINTER(C.c_int16), C.c_uint64, u8p, u8p],
                                         C.c_int),
+            "hevcgpu_residual_blocks_scaled": ([P, C.POINTER(Scaling), C.POINTER(TU), C.c_int32,
+                                                C.POINTER(C.c_int16), C.c_uint64, u8p, u8p], C.c_int),
             "hevcgpu_inter_pred": ([P, C.POINTER(PicParams), C.POINTER(PU), C.c_int32, C.POINTER(WP), C.c_int32,
                                     C.POINTER(u8p), C.c_int32, u8p], C.c_int),
             "hevcgpu_loop_filter": ([P, C.POINTER(PictureSyntax), u8p, u8p, C.c_int, C.c_int], C.c_int),
@@ -329,10 +341,12 @@ class Context:
         return {s: (ms[i], int(n[i])) for i, s in enumerate(self.STAGES)}
 
     # ---- stages on host memory
-    def residual_blocks(self, tus, num_tus, coeffs, pred):
+    def residual_blocks(self, tus, num_tus, coeffs, pred, scaling=None):
+        """scaling: an abi.Scaling (scaling_list_enabled_flag = 1) or None (flat)."""
         out = np.empty_like(pred)
-        _check(self.lib.hevcgpu_residual_blocks(self.h, tus, num_tus, as_ptr(coeffs, C.c_int16), coeffs.size,
-                                                as_ptr(pred, C.c_uint8), as_ptr(out, C.c_uint8)))
+        _check(self.lib.hevcgpu_residual_blocks_scaled(
+            self.h, C.byref(scaling) if scaling is not None else None, tus, num_tus, as_ptr(coeffs, C.c_int16),
+            coeffs.size, as_ptr(pred, C.c_uint8), as_ptr(out, C.c_uint8)))
         return out
 
     def inter_pred(self, pic, refs):

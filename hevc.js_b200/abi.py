@@ -57,6 +57,10 @@ class Slice(C.Structure):
                 ("deblocking_disabled", C.c_uint8), ("lf_across_slices", C.c_uint8)]
 
 
+class Scaling(C.Structure):
+    _fields_ = [("list", ((C.c_uint8 * 64) * 6) * 4), ("dc", (C.c_uint8 * 6) * 2), ("reserved", C.c_uint8 * 4)]
+
+
 class PicParams(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("bit_depth", C.c_int32),
                 ("log2_ctb", C.c_int32), ("log2_min_cb", C.c_int32), ("log2_min_tb", C.c_int32),
@@ -78,7 +82,8 @@ class PictureSyntax(C.Structure):
                 ("sao", C.POINTER(SAO)),
                 ("ctb_slice", C.POINTER(C.c_uint8)),
                 ("ctb_tile", C.POINTER(C.c_uint16)),
-                ("num_slices", C.c_int32), ("slices", C.POINTER(Slice))]
+                ("num_slices", C.c_int32), ("slices", C.POINTER(Slice)),
+                ("scaling", C.POINTER(Scaling))]
 
 
 class SynthCfg(C.Structure):
@@ -91,7 +96,7 @@ class SynthCfg(C.Structure):
                 ("num_refs", C.c_int32), ("slice_type", C.c_int32), ("poc", C.c_int32),
                 ("strong_intra_smoothing", C.c_int32), ("cb_qp_offset", C.c_int32),
                 ("cr_qp_offset", C.c_int32), ("beta_offset_div2", C.c_int32),
-                ("tc_offset_div2", C.c_int32)]
+                ("tc_offset_div2", C.c_int32), ("scaling_lists", C.c_int32)]
 
 
 class SynthCU(C.Structure):
@@ -107,12 +112,12 @@ class SynthPicture(C.Structure):
 
 
 RECORD_SIZES = {"hevc_tu_t": 16, "hevc_pu_t": 20, "hevc_wp_t": 28, "hevc_sao_t": 24,
-                "hevc_slice_t": 4}
+                "hevc_slice_t": 4, "hevc_scaling_t": 1552}
 
 
 def check_layouts():
     got = {"hevc_tu_t": C.sizeof(TU), "hevc_pu_t": C.sizeof(PU), "hevc_wp_t": C.sizeof(WP),
-           "hevc_sao_t": C.sizeof(SAO), "hevc_slice_t": C.sizeof(Slice)}
+           "hevc_sao_t": C.sizeof(SAO), "hevc_slice_t": C.sizeof(Slice), "hevc_scaling_t": C.sizeof(Scaling)}
     if got != RECORD_SIZES:
         raise AssertionError(f"record layout mismatch: {got} != {RECORD_SIZES}")
 

@@ -57,6 +57,7 @@ struct PicDesc {
     const uint8_t* ctb_slice;            // may be null
     const uint16_t* ctb_tile;            // may be null
     const hevc_slice_t* slices;
+    const hevc_scaling_t* scaling;       // scaling lists, or null for flat scaling
     // intra CTU tasks (intra.cuh): the CTUs that hold intra TUs, raster order, and their
     // TUs ordered by level of the CTU-local dependency DAG
     const int32_t* ictu_addr;            // raster address of intra CTU k

@@ -950,8 +950,11 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     j->n_pus = s->num_pus;
 
     size_t o_wp, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc[2], o_ia, o_idp, o_ito, o_itu, o_iro, o_ilo, o_ilv;
+    size_t o_scal = 0;
     hevc_slice_t dflt{0, 0, 0, 1};
+    const bool scaled = s->scaling && (stages & (ST_RESID | ST_INTRA));
     auto pack = [&](Packer& pk) {
+        if (scaled) o_scal = pk.add(s->scaling, sizeof(hevc_scaling_t));
         o_wp = pk.add(s->wp, sizeof(hevc_wp_t) * (size_t)std::max(0, s->num_wp));
         o_sao = pk.add(s->sao, s->sao ? sizeof(hevc_sao_t) * (size_t)nctb : 0);
         o_sl = pk.add(s->ctb_slice, s->ctb_slice ? (size_t)nctb : 0);
@@ -1013,6 +1016,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
     D.ctb_slice = s->ctb_slice ? base + o_sl : nullptr;
     D.ctb_tile = (s->ctb_tile && p.tiles_enabled) ? reinterpret_cast<const uint16_t*>(base + o_ti) : nullptr;
     D.slices = reinterpret_cast<const hevc_slice_t*>(base + o_slices);
+    D.scaling = scaled ? reinterpret_cast<const hevc_scaling_t*>(base + o_scal) : nullptr;
     D.ictu_addr = reinterpret_cast<const int32_t*>(base + o_ia);
     D.ictu_deps = reinterpret_cast<const int32_t*>(base + o_idp);
     D.ictu_tu_off = reinterpret_cast<const int32_t*>(base + o_ito);
@@ -1367,6 +1371,12 @@ uint64_t hevcgpu_bytes_in_use(hevcgpu_ctx_t* ctx) { return ctx ? ctx->allocated 
 
 int hevcgpu_residual_blocks(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int32_t num_tus, const int16_t* coeffs,
                             uint64_t num_coeffs, const uint8_t* pred, uint8_t* out) {
+    return hevcgpu_residual_blocks_scaled(ctx, nullptr, tus, num_tus, coeffs, num_coeffs, pred, out);
+}
+
+int hevcgpu_residual_blocks_scaled(hevcgpu_ctx_t* ctx, const hevc_scaling_t* scaling, const hevc_tu_t* tus,
+                                   int32_t num_tus, const int16_t* coeffs, uint64_t num_coeffs,
+                                   const uint8_t* pred, uint8_t* out) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (num_tus < 0 || (num_tus && (!tus || !coeffs || !pred || !out)))
@@ -1384,8 +1394,9 @@ int hevcgpu_residual_blocks(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int32_t nu
     j.ctx = ctx;
     std::vector<int32_t> bins[4];
     for (int i = 0; i < num_tus; i++) bins[tus[i].log2_size - 2].push_back(i);
-    size_t o_tus, o_coef, o_pred, o_out, o_res[4];
+    size_t o_tus, o_coef, o_pred, o_out, o_res[4], o_scal = 0;
     auto pack = [&](Packer& pk) {
+        if (scaling) o_scal = pk.add(scaling, sizeof(hevc_scaling_t));
         o_tus = pk.add(tus, sizeof(hevc_tu_t) * (size_t)num_tus);
         o_coef = pk.add(coeffs, sizeof(int16_t) * (size_t)num_coeffs);
         o_pred = pk.add(pred, (size_t)num_coeffs);
@@ -1409,6 +1420,7 @@ int hevcgpu_residual_blocks(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int32_t nu
     D.coeffs = reinterpret_cast<const int16_t*>(base + o_coef);
     D.rec = base + o_pred;
     D.dst = base + o_out;
+    D.scaling = scaling ? reinterpret_cast<const hevc_scaling_t*>(base + o_scal) : nullptr;
     for (int k = 0; k < 4; k++) {
         j.n_res[k] = (int32_t)bins[k].size();
         j.d_res[k] = reinterpret_cast<const int32_t*>(base + o_res[k]);

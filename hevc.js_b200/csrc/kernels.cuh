@@ -74,14 +74,47 @@ __device__ __forceinline__ void inv_1d(const int* s, int* d, bool dst4) {
     idct_1d<N>(s, d);
 }
 
-// Flat-scaling dequantisation of one level (transform.cpp:360-365): int64 product,
-// rounding shift, narrowing to int (modulo 2^32), int16 clip.
-__device__ __forceinline__ int16_t dequant1(int c, int scale, int qp_per, int bd_shift) {
+// Dequantisation of one level (transform.cpp:360-365) with ms = m * levelScale[qP % 6]:
+// the product, the shift by qP / 6 and the rounding shift in int64, narrowing to int
+// (modulo 2^32), int16 clip.  |c * ms| <= 32768 * 255 * 72 fits an int.
+__device__ __forceinline__ int16_t dequant1(int c, int ms, int qp_per, int bd_shift) {
     if (c == 0) return 0;
-    long long v = (long long)(c * 16 * scale);
+    long long v = (long long)(c * ms);
     v = v * (1ll << qp_per) + (1ll << (bd_shift - 1));
     v >>= bd_shift;
     return (int16_t)clip3(-32768, 32767, (int)(unsigned)(unsigned long long)v);
+}
+
+// Scaling factors m of row j of an N x N block (transform.cpp:320-358): matrixId is the
+// plane plus 3 for a non-intra CU below 32x32, 0 or 3 at 32x32; a 4x4 block reads its
+// list at j*4 + i, larger ones the 8x8 list at (j/r)*8 + i/r (r = N/8), and 16x16 and
+// 32x32 blocks take the DC value (0 read as 16) at (0,0).  The lists sit 16-byte aligned,
+// so a row is one 4- or 8-byte load.
+template <int LOG2>
+__device__ __forceinline__ void scaling_row(const hevc_scaling_t* S, int c_idx, bool intra, int j,
+                                            int (&m)[1 << LOG2]) {
+    constexpr int N = 1 << LOG2, SIZE_ID = LOG2 - 2;
+    const int matrix = (SIZE_ID < 3 ? c_idx : 0) + (intra ? 0 : 3);
+    const uint8_t* list = S->list[SIZE_ID][matrix];
+    if constexpr (LOG2 == 2) {
+        const uint32_t w = *reinterpret_cast<const uint32_t*>(list + 4 * j);
+#pragma unroll
+        for (int i = 0; i < 4; i++) m[i] = (w >> (8 * i)) & 255;
+    } else {
+        constexpr int R = N / 8;
+        const uint2 w = *reinterpret_cast<const uint2*>(list + 8 * (j / R));
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            const int k = i / R;
+            m[i] = ((k < 4 ? w.x : w.y) >> (8 * (k & 3))) & 255;
+        }
+        if constexpr (LOG2 >= 4) {
+            if (j == 0) {
+                const int dc = S->dc[SIZE_ID - 2][matrix];
+                m[0] = dc ? dc : 16;
+            }
+        }
+    }
 }
 
 __constant__ int c_level_scale[6] = {40, 45, 51, 57, 64, 72};
@@ -124,9 +157,16 @@ __global__ void __launch_bounds__(128) k_residual(const __grid_constant__ SegTab
             *reinterpret_cast<int2*>(&v[0]) = w;
         }
         if (!bypass) {
-            int scale = c_level_scale[t.qp % 6], qp_per = t.qp / 6, bd_shift = 8 + LOG2 - 5;
+            const int scale = c_level_scale[t.qp % 6], qp_per = t.qp / 6, bd_shift = 8 + LOG2 - 5;
+            if (P.scaling) {
+                int m[N];
+                scaling_row<LOG2>(P.scaling, t.c_idx, t.flags & HEVC_TU_INTRA, j, m);
 #pragma unroll
-            for (int i = 0; i < N; i++) v[i] = dequant1(v[i], scale, qp_per, bd_shift);
+                for (int i = 0; i < N; i++) v[i] = dequant1(v[i], m[i] * scale, qp_per, bd_shift);
+            } else {
+#pragma unroll
+                for (int i = 0; i < N; i++) v[i] = dequant1(v[i], 16 * scale, qp_per, bd_shift);
+            }
         }
 #pragma unroll
         for (int i = 0; i < N; i++) s_coef[slot][j * N + i] = v[i];

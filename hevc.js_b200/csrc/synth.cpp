@@ -62,8 +62,23 @@ void draw_levels(Rng& r, int n, int16_t* dst) {
         }
 }
 
+void draw_scaling(Rng& r, hevc_scaling_t* s) {
+    std::memset(s, 0, sizeof(*s));
+    for (int sz = 0; sz < 4; sz++)
+        for (int m = 0; m < 6; m++) {
+            const int n = sz == 0 ? 4 : 8, kind = r.range(0, 2), k = r.range(0, 12);
+            for (int v = 0; v < n; v++)
+                for (int u = 0; u < n; u++)
+                    s->list[sz][m][v * n + u] =
+                        (uint8_t)(kind == 0 ? 16 : kind == 1 ? 16 + k * (u + v) : r.range(0, 255));
+        }
+    for (int i = 0; i < 2; i++)
+        for (int m = 0; m < 6; m++) s->dc[i][m] = (uint8_t)(r.bern(0.25) ? 0 : r.range(0, 255));
+}
+
 struct Picture {
     hevcsynth_picture_t pub{};
+    hevc_scaling_t scaling{};
     std::vector<hevc_tu_t> tus;
     std::vector<int16_t> coeffs;
     std::vector<hevc_pu_t> pus;
@@ -399,6 +414,12 @@ struct Gen {
         syn.ctb_tile = nullptr;
         syn.num_slices = 1;
         syn.slices = P.slices.data();
+        syn.scaling = nullptr;
+        if (c.scaling_lists) {   // own stream of draws: the rest of the picture is unchanged
+            Rng rs(c.seed ^ 0x5CA1E11575ull);
+            draw_scaling(rs, &P.scaling);
+            syn.scaling = &P.scaling;
+        }
         P.pub.num_cus = (int32_t)P.cus.size();
         P.pub.cus = P.cus.data();
         P.pub.impl = &P;
@@ -491,6 +512,13 @@ int hevcsynth_content(int32_t width, int32_t height, uint64_t seed, uint8_t* out
             }
         plane += (size_t)w * h;
     }
+    return 0;
+}
+
+int hevcsynth_scaling(uint64_t seed, hevc_scaling_t* out) {
+    if (!out) return -1;
+    Rng r(seed);
+    draw_scaling(r, out);
     return 0;
 }
 

@@ -43,6 +43,7 @@ typedef struct hevcsynth_cfg {
     int32_t  strong_intra_smoothing;
     int32_t  cb_qp_offset, cr_qp_offset;
     int32_t  beta_offset_div2, tc_offset_div2;
+    int32_t  scaling_lists;      /* attach scaling lists drawn by hevcsynth_scaling     */
 } hevcsynth_cfg_t;
 
 /* One coding unit (synth-only: used by the reference harness to replay decode order). */
@@ -82,6 +83,11 @@ int hevcsynth_content(int32_t width, int32_t height, uint64_t seed, uint8_t* out
  * Call with NULL arrays to size them first. */
 int64_t hevcsynth_blocks(int32_t num_tus, uint64_t seed, int32_t qp_min, int32_t qp_max,
                          hevc_tu_t* tus, int16_t* coeffs, uint8_t* pred);
+
+/* Scaling lists for the dequantisation checks: per (sizeId, matrixId) a flat list of 16,
+ * a ramp 16 + k*(u+v) (k uniform 0..12) or bytes uniform in 0..255 (a parsed list can
+ * hold any byte, 0 included); DC values uniform in 0..255, 0 with probability 1/4. */
+int hevcsynth_scaling(uint64_t seed, hevc_scaling_t* out);
 
 /* Histogram of the boundary strengths that the deblocking filter will derive for a
  * picture (edges on the 8x8 grid, per 4-sample segment, picture-edge and disabled

@@ -22,6 +22,7 @@ of this path and is not timed.
 """
 import collections
 import concurrent.futures
+import gc
 import heapq
 import os
 import random
@@ -291,26 +292,36 @@ def run_poisson(hb, ctx, seconds=5.0, n_streams=64, seed=4, lanes=4, max_batch=6
         specs.append((sid, w, h, fps))
     admitted = [sid for sid, w, h, fps in specs if srv.admit(sid, w, h, fps, variant=sid)]
     srv.warm()
-    t0 = srv.start_clock(clock)   # streams are open and their DPBs resident before the clock starts
-    arrivals = []   # (time, sid): each stream's first segment within the first segment length
-    for sid in admitted:
-        heapq.heappush(arrivals, (t0 + rng.uniform(0.0, segment_s), sid))
-    lat = []
-    offered = 0
-    t_end = t0 + seconds
-    while True:
-        now = clock()
-        while arrivals and arrivals[0][0] <= now and arrivals[0][0] < t_end:
-            t, sid = heapq.heappop(arrivals)
-            s = srv.streams[sid]
-            n = int(round(segment_s * s.fps))
-            srv.add_segment(sid, t, n)
-            offered += n
-            heapq.heappush(arrivals, (t + rng.expovariate(1.0 / segment_s), sid))
-        lat.extend(srv.poll(now))
-        if now >= t_end and srv.pending() == 0:
-            break
-    t_stop = clock()
+    # the loop allocates no cycles; a cyclic collection pass over the whole process's
+    # objects would stall it (for a long-running process holding many objects, by
+    # hundreds of ms), so collect once now and keep the collector off while serving
+    gc.collect()
+    gc_was_on = gc.isenabled()
+    gc.disable()
+    try:
+        t0 = srv.start_clock(clock)   # streams are open and their DPBs resident before the clock starts
+        arrivals = []   # (time, sid): each stream's first segment within the first segment length
+        for sid in admitted:
+            heapq.heappush(arrivals, (t0 + rng.uniform(0.0, segment_s), sid))
+        lat = []
+        offered = 0
+        t_end = t0 + seconds
+        while True:
+            now = clock()
+            while arrivals and arrivals[0][0] <= now and arrivals[0][0] < t_end:
+                t, sid = heapq.heappop(arrivals)
+                s = srv.streams[sid]
+                n = int(round(segment_s * s.fps))
+                srv.add_segment(sid, t, n)
+                offered += n
+                heapq.heappush(arrivals, (t + rng.expovariate(1.0 / segment_s), sid))
+            lat.extend(srv.poll(now))
+            if now >= t_end and srv.pending() == 0:
+                break
+        t_stop = clock()
+    finally:
+        if gc_was_on:
+            gc.enable()
     records = np.array([(r[0], r[1]) for r in srv.records]) if srv.records else np.zeros((0, 2))
     srv.close()
     lat_ms = np.array(lat) * 1000.0

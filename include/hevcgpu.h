@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define HEVCGPU_ABI_VERSION 1
+#define HEVCGPU_ABI_VERSION 2
 
 /* ---- status codes (negative values map to HEVC_ERROR of src/wasm/hevc_api.h:43) ---- */
 #define HEVCGPU_OK            0
@@ -118,6 +118,19 @@ typedef struct hevc_slice {
     uint8_t lf_across_slices;         /* slice_loop_filter_across_slices_enabled_flag   */
 } hevc_slice_t;
 
+/* Scaling lists of the active parameter set: ScalingListData (src/syntax/sps.h:15-31),
+ * i.e. pps.scaling_list_data when pps_scaling_list_data_present_flag, else
+ * sps.scaling_list_data, exactly as the parser stores them (set_defaults and parse,
+ * src/syntax/sps.cpp:41-113).  perform_dequant (src/decoding/transform.cpp:320-358) reads
+ * list[sizeId][matrixId] at y*4+x for 4x4 blocks and at (y/r)*8 + x/r (r = N/8) above,
+ * with dc[sizeId-2][matrixId] (0 read as 16) at (0,0) of 16x16 and 32x32 blocks;
+ * matrixId = c_idx + 3 * !intra below 32x32 and 3 * !intra at 32x32. */
+typedef struct hevc_scaling {
+    uint8_t list[4][6][64];   /* ScalingListData::scaling_list                        */
+    uint8_t dc[2][6];         /* ScalingListData::scaling_list_dc                     */
+    uint8_t reserved[4];
+} hevc_scaling_t;             /* 1552 bytes */
+
 /* Picture-level parameters (SPS/PPS/slice fields the reconstruction reads). */
 typedef struct hevc_pic_params {
     int32_t width, height;            /* luma samples, multiples of 8                   */
@@ -155,6 +168,7 @@ typedef struct hevc_picture_syntax {
     const uint16_t*     ctb_tile;     /* TileId per CTB (raster), or NULL               */
     int32_t             num_slices;
     const hevc_slice_t* slices;
+    const hevc_scaling_t* scaling;    /* NULL: flat scaling (scaling_list_enabled_flag = 0) */
 } hevc_picture_syntax_t;
 
 /* ---- context ---- */
@@ -178,6 +192,14 @@ int         hevcgpu_sync(hevcgpu_ctx_t* ctx);
 int hevcgpu_residual_blocks(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int32_t num_tus,
                             const int16_t* coeffs, uint64_t num_coeffs,
                             const uint8_t* pred, uint8_t* out);
+
+/* The same with scaling lists (sps.scaling_list_enabled_flag = 1): each block dequantises
+ * with the matrix of its size, plane and HEVC_TU_INTRA flag (CuPredMode of the CU at the
+ * block, transform.cpp:330-336).  scaling NULL is flat, as hevcgpu_residual_blocks. */
+int hevcgpu_residual_blocks_scaled(hevcgpu_ctx_t* ctx, const hevc_scaling_t* scaling,
+                                   const hevc_tu_t* tus, int32_t num_tus,
+                                   const int16_t* coeffs, uint64_t num_coeffs,
+                                   const uint8_t* pred, uint8_t* out);
 
 /* Motion-compensated prediction of every PU into out (I420, params->width x height).
  * refs[i] is the I420 picture for reference-list slot i (params->ref_slot values

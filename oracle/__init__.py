@@ -38,6 +38,8 @@ def _bind(lib, prefix, syn_t):
     u8p = C.POINTER(C.c_uint8)
     sig = {
         "residual_blocks": ([C.POINTER(abi.TU), C.c_int32, C.POINTER(C.c_int16), u8p, u8p], C.c_int),
+        "residual_blocks_scaled": ([C.POINTER(abi.Scaling), C.POINTER(abi.TU), C.c_int32, C.POINTER(C.c_int16),
+                                    u8p, u8p], C.c_int),
         "inter_pred": ([C.POINTER(abi.PicParams), C.POINTER(abi.PU), C.c_int32, C.POINTER(abi.WP), C.c_int32,
                         C.POINTER(u8p), C.c_int32, u8p], C.c_int),
         "loop_filter": ([C.POINTER(abi.PictureSyntax), u8p, u8p, C.c_int, C.c_int], C.c_int),
@@ -88,12 +90,13 @@ class Checker:
     def _f(self, name):
         return getattr(self.lib, self.prefix + name)
 
-    def residual_blocks(self, tus, num_tus, coeffs, pred):
+    def residual_blocks(self, tus, num_tus, coeffs, pred, scaling=None):
         import numpy as np
         from hevc_b200.abi import as_ptr
         out = np.empty_like(pred)
-        rc = self._f("residual_blocks")(tus, num_tus, as_ptr(coeffs, C.c_int16), as_ptr(pred, C.c_uint8),
-                                        as_ptr(out, C.c_uint8))
+        sl = C.byref(scaling) if scaling is not None else None
+        rc = self._f("residual_blocks_scaled")(sl, tus, num_tus, as_ptr(coeffs, C.c_int16), as_ptr(pred, C.c_uint8),
+                                               as_ptr(out, C.c_uint8))
         assert rc == 0
         return out
 

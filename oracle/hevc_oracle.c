@@ -61,10 +61,35 @@ static void basis(int n_pts, int dst, int out[32][32]) {
             out[n][k] = dst ? kDst[n][k] : cos_entry(n * (32 / n_pts) * (2 * k + 1));
 }
 
-/* Dequantisation with flat scaling: perform_dequant, transform.cpp:293-368.
- * The reference forms the product in int64, shifts, then narrows to int before the
- * int16 clip (static_cast<int> at :365); the narrowing is modulo 2^32 here too. */
-static void dequant(const int16_t* c, int n, int qp, int bit_depth, int16_t* d) {
+/* Scaling factor m of coefficient (x, y): perform_dequant, transform.cpp:320-358.
+ * Flat 16 without lists.  sizeId = log2 - 2; matrixId = plane + 3 for a non-intra CU
+ * below 32x32, 0 / 3 (intra / not) at 32x32 (:330-336).  4x4 reads list[0][matrixId]
+ * at y*4 + x; larger sizes read list[sizeId][matrixId % 6] at (y/r)*8 + x/r, r = N/8,
+ * capped at 63 (:343-347), and 16x16 / 32x32 take dc[sizeId-2][matrixId % 6] at (0,0),
+ * where a 0 reads as 16 (:350-353). */
+static int scale_factor(const hevc_scaling_t* sl, int log2, int c_idx, int intra, int x, int y) {
+    if (!sl) return 16;
+    int n = 1 << log2, size_id = log2 - 2, matrix;
+    if (size_id < 3) matrix = c_idx + (intra ? 0 : 3);
+    else matrix = intra ? 0 : 3;
+    if (size_id == 0) return sl->list[0][matrix][y * n + x];
+    int ratio = n / 8 < 1 ? 1 : n / 8;
+    int idx = (y / ratio) * 8 + (x / ratio);
+    if (idx > 63) idx = 63;
+    int m = sl->list[size_id][matrix % 6][idx];
+    if ((size_id == 2 || size_id == 3) && x == 0 && y == 0) {
+        m = sl->dc[size_id - 2][matrix % 6];
+        if (m == 0) m = 16;
+    }
+    return m;
+}
+
+/* Dequantisation: perform_dequant, transform.cpp:293-368.  The reference forms the
+ * product in int64, shifts, then narrows to int before the int16 clip
+ * (static_cast<int> at :365); the narrowing is modulo 2^32 here too (it bites only
+ * with scaling factors above 16). */
+static void dequant(const int16_t* c, int n, int qp, int bit_depth, const hevc_scaling_t* sl, int c_idx,
+                    int intra, int16_t* d) {
     static const int level_scale[6] = {40, 45, 51, 57, 64, 72};
     int log2 = n == 4 ? 2 : n == 8 ? 3 : n == 16 ? 4 : 5;
     int bd_shift = bit_depth + log2 - 5;
@@ -72,7 +97,7 @@ static void dequant(const int16_t* c, int n, int qp, int bit_depth, int16_t* d) 
     int64_t scale = level_scale[qp % 6];
     for (int i = 0; i < n * n; i++) {
         if (c[i] == 0) { d[i] = 0; continue; }
-        int64_t v = (int64_t)c[i] * 16 * scale;
+        int64_t v = (int64_t)c[i] * scale_factor(sl, log2, c_idx, intra, i % n, i / n) * scale;
         v = v * ((int64_t)1 << (qp / 6)) + add;
         v >>= bd_shift;
         int32_t narrowed = (int32_t)(uint32_t)(uint64_t)v;
@@ -112,23 +137,24 @@ static void inverse_transform(const int16_t* d, int n, int flags, int c_idx, int
 
 /* Residual of one TU (levels -> residual), including the transquant-bypass copy of
  * coding_tree.cpp:1302-1304. */
-static void tu_residual(const hevc_tu_t* t, const int16_t* levels, int bit_depth, int16_t* res) {
+static void tu_residual(const hevc_tu_t* t, const int16_t* levels, int bit_depth, const hevc_scaling_t* sl,
+                        int16_t* res) {
     int n = 1 << t->log2_size;
     if (!(t->flags & HEVC_TU_CODED)) { memset(res, 0, sizeof(int16_t) * n * n); return; }
     if (t->flags & HEVC_TU_BYPASS) { memcpy(res, levels, sizeof(int16_t) * n * n); return; }
     int16_t d[32 * 32];
-    dequant(levels, n, t->qp, bit_depth, d);
+    dequant(levels, n, t->qp, bit_depth, sl, t->c_idx, (t->flags & HEVC_TU_INTRA) != 0, d);
     inverse_transform(d, n, t->flags, t->c_idx, bit_depth, res);
 }
 
-int oracle_residual_blocks(const hevc_tu_t* tus, int32_t num_tus, const int16_t* coeffs,
-                           const uint8_t* pred, uint8_t* out) {
+int oracle_residual_blocks_scaled(const hevc_scaling_t* sl, const hevc_tu_t* tus, int32_t num_tus,
+                                  const int16_t* coeffs, const uint8_t* pred, uint8_t* out) {
     int16_t res[32 * 32];
     for (int t = 0; t < num_tus; t++) {
         const hevc_tu_t* tu = &tus[t];
         if (tu->log2_size < 2 || tu->log2_size > 5) return -1;
         int n = 1 << tu->log2_size;
-        tu_residual(tu, coeffs + tu->coeff_offset, 8, res);
+        tu_residual(tu, coeffs + tu->coeff_offset, 8, sl, res);
         /* reconstruct_block, coding_tree.cpp:371-396 */
         for (int i = 0; i < n * n; i++) {
             int v = pred[tu->coeff_offset + i] + res[i];
@@ -136,6 +162,11 @@ int oracle_residual_blocks(const hevc_tu_t* tus, int32_t num_tus, const int16_t*
         }
     }
     return 0;
+}
+
+int oracle_residual_blocks(const hevc_tu_t* tus, int32_t num_tus, const int16_t* coeffs,
+                           const uint8_t* pred, uint8_t* out) {
+    return oracle_residual_blocks_scaled(NULL, tus, num_tus, coeffs, pred, out);
 }
 
 /* ------------------------------------------------------------------------------------
@@ -443,7 +474,7 @@ static void inter_residuals(const hevc_picture_syntax_t* syn, planes_t* pic) {
         const hevc_tu_t* t = &syn->tus[i];
         if ((t->flags & HEVC_TU_INTRA) || !(t->flags & HEVC_TU_CODED)) continue;
         int n = 1 << t->log2_size, ci = t->c_idx;
-        tu_residual(t, syn->coeffs + t->coeff_offset, 8, res);
+        tu_residual(t, syn->coeffs + t->coeff_offset, 8, syn->scaling, res);
         for (int y = 0; y < n; y++)
             for (int x = 0; x < n; x++) {
                 if (t->x + x >= pic->w[ci] || t->y + y >= pic->h[ci]) continue;
@@ -466,7 +497,7 @@ static void intra_pass(const hevc_picture_syntax_t* syn, planes_t* pic) {
         if (!(t->flags & HEVC_TU_INTRA)) continue;
         const int16_t* r = NULL;
         if (t->flags & HEVC_TU_CODED) {
-            tu_residual(t, syn->coeffs + t->coeff_offset, 8, res);
+            tu_residual(t, syn->coeffs + t->coeff_offset, 8, syn->scaling, res);
             r = res;
         }
         intra_tu(&e, t, r, pic);

@@ -81,6 +81,18 @@ void init_sps(SPS& s, int W, int H, int log2_ctb, int log2_min_cb, int strong, i
     s.derive();
 }
 
+// Scaling lists: the SPS carries them (scaling_list_enabled_flag with the SPS's own
+// ScalingListData; the PPS has none), as the parser leaves them (sps.cpp:400-410).
+void set_scaling(SPS& s, const hevc_scaling_t* sl) {
+    s.scaling_list_enabled_flag = sl != nullptr;
+    if (!sl) return;
+    for (int sz = 0; sz < 4; sz++)
+        for (int m = 0; m < 6; m++)
+            std::memcpy(s.scaling_list_data.scaling_list[(size_t)sz][(size_t)m].data(), sl->list[sz][m], 64);
+    for (int i = 0; i < 2; i++)
+        for (int m = 0; m < 6; m++) s.scaling_list_data.scaling_list_dc[(size_t)i][(size_t)m] = sl->dc[i][m];
+}
+
 void load_picture(Picture& pic, int W, int H, const uint8_t* i420) {
     pic.allocate(W, H, ChromaFormat::YUV420, 8, 8);
     if (!i420) return;
@@ -109,6 +121,7 @@ void setup(Env& e, const hevc_picture_syntax_t& syn, const uint8_t* in, const ui
     e.H = p.height;
     init_sps(e.sps, p.width, p.height, p.log2_ctb, p.log2_min_cb, p.strong_intra_smoothing,
              p.intra_smoothing_disabled, p.pcm_loop_filter_disabled, p.sao_enabled);
+    set_scaling(e.sps, syn.scaling);
     e.pps.pps_cb_qp_offset = p.cb_qp_offset;
     e.pps.pps_cr_qp_offset = p.cr_qp_offset;
     e.pps.loop_filter_across_tiles_enabled_flag = p.loop_filter_across_tiles != 0;
@@ -325,15 +338,22 @@ void tu_recon(Env& e, const hevc_tu_t& t, const int16_t* coeffs) {
 
 extern "C" {
 
-int ref_residual_blocks(const hevc_tu_t* tus, int32_t num_tus, const int16_t* coeffs, const uint8_t* pred,
-                        uint8_t* out) {
+// Independent blocks at (0,0) of a one-CU grid whose prediction mode follows each
+// block's HEVC_TU_INTRA flag (perform_dequant reads it through cu_at with scaling lists).
+int ref_residual_blocks_scaled(const hevc_scaling_t* sl, const hevc_tu_t* tus, int32_t num_tus,
+                               const int16_t* coeffs, const uint8_t* pred, uint8_t* out) {
     Env e;
     init_sps(e.sps, 64, 64, 6, 3, 0, 0, 0, 0);
+    set_scaling(e.sps, sl);
+    e.cu_info.assign(1, CUInfo{});
     e.ctx.sps = &e.sps;
     e.ctx.pps = &e.pps;
+    e.ctx.cu_info = e.cu_info.data();
+    e.ctx.cu_info_stride = 1;
     for (int i = 0; i < num_tus; i++) {
         const hevc_tu_t& t = tus[i];
         int n = 1 << t.log2_size;
+        e.cu_info[0].pred_mode = (t.flags & HEVC_TU_INTRA) ? PredMode::MODE_INTRA : PredMode::MODE_INTER;
         int16_t scaled[32 * 32] = {}, residual[32 * 32] = {};
         perform_dequant(e.ctx, 0, 0, t.log2_size, t.c_idx, t.qp, coeffs + t.coeff_offset, scaled);
         perform_transform_inverse(t.log2_size, t.c_idx, (t.flags & HEVC_TU_INTRA) != 0,
@@ -344,6 +364,11 @@ int ref_residual_blocks(const hevc_tu_t* tus, int32_t num_tus, const int16_t* co
         }
     }
     return 0;
+}
+
+int ref_residual_blocks(const hevc_tu_t* tus, int32_t num_tus, const int16_t* coeffs, const uint8_t* pred,
+                        uint8_t* out) {
+    return ref_residual_blocks_scaled(nullptr, tus, num_tus, coeffs, pred, out);
 }
 
 int ref_inter_pred(const hevc_pic_params_t* pp, const hevc_pu_t* pus, int32_t num_pus, const hevc_wp_t* wp,

@@ -32,7 +32,26 @@ CASES = {
     "picture_intra_352x288_s6": dict(kind="picture", w=352, h=288, seed=6, cfg=ALL_INTRA, refs=(61, 62)),
     "picture_64x64_s10": dict(kind="picture", w=64, h=64, seed=10, cfg=PICTURE, refs=(101, 102)),
     "picture_72x40_s12": dict(kind="picture", w=72, h=40, seed=12, cfg=dict(PICTURE, p_intra=0.4), refs=(121, 122)),
+    # scaling lists (scaling_list_enabled_flag): blocks of every matrix, and whole pictures
+    "blocks_scaled_2048_s13": dict(kind="blocks", n=2048, seed=13, scaling=113, mix=True),
+    "picture_scaled_416x240_s14": dict(kind="picture", w=416, h=240, seed=14,
+                                       cfg=dict(PICTURE, p_intra=0.3, scaling_lists=1), refs=(141, 142)),
+    "picture_scaled_1080p_s15": dict(kind="picture", w=1920, h=1080, seed=15, cfg=dict(PICTURE, scaling_lists=1),
+                                     refs=(151, 152)),
 }
+
+
+def mix_blocks(hb, tus, n, seed, qp=(0, 51)):
+    """Spread blocks over every scaling matrix: intra or not, any plane below 32x32, QP
+    uniform in qp (None: kept)."""
+    rng = np.random.default_rng(seed)
+    for i in range(n):
+        if rng.random() < 0.5:
+            tus[i].flags ^= hb.abi.HEVC_TU_INTRA
+        if tus[i].log2_size < 5:
+            tus[i].c_idx = int(rng.integers(0, 3))
+        if qp is not None:
+            tus[i].qp = int(rng.integers(qp[0], qp[1] + 1))
 
 
 def build_inputs(hb, case):
@@ -40,7 +59,10 @@ def build_inputs(hb, case):
     k = case["kind"]
     if k == "blocks":
         tus, n, coeffs, pred = hb.blocks(case["n"], case["seed"])
-        return dict(tus=tus, n=n, coeffs=coeffs, pred=pred)
+        if case.get("mix"):
+            mix_blocks(hb, tus, n, case["seed"])
+        sl = hb.scaling(case["scaling"]) if "scaling" in case else None
+        return dict(tus=tus, n=n, coeffs=coeffs, pred=pred, scaling=sl)
     cfg = hb.default_cfg(case["w"], case["h"], case["seed"], **case["cfg"])
     pic = hb.Picture(cfg)
     out = dict(pic=pic)
@@ -55,7 +77,7 @@ def run_case(checker, case, inp):
     """Run a case through any object with the stage entry points (GPU context or oracle)."""
     k = case["kind"]
     if k == "blocks":
-        return checker.residual_blocks(inp["tus"], inp["n"], inp["coeffs"], inp["pred"])
+        return checker.residual_blocks(inp["tus"], inp["n"], inp["coeffs"], inp["pred"], inp["scaling"])
     if k == "inter":
         return checker.inter_pred(inp["pic"], inp["refs"])
     if k == "filters":

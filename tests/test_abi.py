@@ -64,7 +64,7 @@ int main(void) {
 
 def test_abi_version(lib):
     lib.hevcgpu_abi_version.restype = C.c_int
-    assert lib.hevcgpu_abi_version() == 1
+    assert lib.hevcgpu_abi_version() == 2
 
 
 def test_create_fails_loudly_without_gpu(hb):

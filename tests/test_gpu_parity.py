@@ -30,6 +30,17 @@ def test_gpu_blocks_edge_levels(hb, gpu_ctx, port, seed, opts):
     assert _diff(gpu_ctx.residual_blocks(tus, n, coeffs, pred), port.residual_blocks(tus, n, coeffs, pred)) == 0
 
 
+@pytest.mark.parametrize("seed,opts", [(25, dict()), (26, dict(big=True)), (27, dict(tskip=True, big=True)),
+                                       (28, dict(big=True, qp=(45, 51)))])
+def test_gpu_blocks_scaled(hb, gpu_ctx, port, seed, opts):
+    tus, n, coeffs, pred = _edit_blocks(hb, 800, seed, **opts)
+    cases.mix_blocks(hb, tus, n, seed, qp=None if "qp" in opts else (0, 51))
+    sl = hb.scaling(seed)
+    got = gpu_ctx.residual_blocks(tus, n, coeffs, pred, sl)
+    assert _diff(got, port.residual_blocks(tus, n, coeffs, pred, sl)) == 0
+    assert _diff(gpu_ctx.residual_blocks(tus, n, coeffs, pred), port.residual_blocks(tus, n, coeffs, pred)) == 0
+
+
 def test_gpu_blocks_empty(hb, gpu_ctx):
     tus, n, coeffs, pred = hb.blocks(0, 1)
     assert gpu_ctx.residual_blocks(tus, 0, coeffs, pred).size == pred.size
@@ -40,7 +51,9 @@ def test_gpu_blocks_empty(hb, gpu_ctx):
                                          (34, 256, 192, dict(p_intra=0.7, p_intra_nxn=1.0)),
                                          (35, 320, 128, dict(p_wp=0.6, mv_range=4096)),
                                          (36, 3840, 2160, dict(p_intra=0.1)),
-                                         (37, 1280, 720, dict(slice_type=2, strong_intra_smoothing=0))])
+                                         (37, 1280, 720, dict(slice_type=2, strong_intra_smoothing=0)),
+                                         (38, 640, 360, dict(p_intra=0.4, scaling_lists=1)),
+                                         (39, 1280, 720, dict(slice_type=2, scaling_lists=1))])
 def test_gpu_pictures(hb, gpu_ctx, port, seed, w, h, kw):
     pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
     refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]

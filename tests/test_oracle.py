@@ -58,6 +58,28 @@ def test_port_matches_reference_blocks(hb, port, seed, opts):
     assert np.array_equal(port.residual_blocks(tus, n, coeffs, pred), ref.residual_blocks(tus, n, coeffs, pred))
 
 
+@pytest.mark.parametrize("seed,opts", [(25, dict()), (26, dict(big=True)), (27, dict(tskip=True, big=True))])
+def test_port_matches_reference_scaled_blocks(hb, port, seed, opts):
+    # scaling lists with factors up to 255: with levels near the int16 limits the
+    # reference's int64 product overflows int before its clip, which the port narrows alike
+    ref = _ref()
+    tus, n, coeffs, pred = _edit_blocks(hb, 800, seed, **opts)
+    cases.mix_blocks(hb, tus, n, seed)
+    sl = hb.scaling(seed)
+    got = port.residual_blocks(tus, n, coeffs, pred, sl)
+    assert np.array_equal(got, ref.residual_blocks(tus, n, coeffs, pred, sl))
+    assert not np.array_equal(got, port.residual_blocks(tus, n, coeffs, pred))
+
+
+@pytest.mark.parametrize("seed,w,h,kw", [(41, 176, 144, dict(p_intra=0.3)), (42, 64, 64, dict(slice_type=2)),
+                                         (43, 256, 192, dict(p_intra=0.6, p_intra_nxn=1.0))])
+def test_port_matches_reference_scaled_pictures(hb, port, seed, w, h, kw):
+    ref = _ref()
+    pic = hb.Picture(hb.default_cfg(w, h, seed, scaling_lists=1, **kw))
+    refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
+    assert np.array_equal(port.reconstruct_picture(pic, refs), ref.reconstruct_picture(pic, refs))
+
+
 @pytest.mark.parametrize("seed,w,h,kw", [(31, 176, 144, dict(p_intra=0.3)), (32, 64, 64, dict(slice_type=2)),
                                          (33, 136, 72, dict(p_intra=0.2, p_skip=0.5, p_merge=0.6)),
                                          (34, 256, 192, dict(p_intra=0.7, p_intra_nxn=1.0)),
