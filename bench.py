@@ -1,35 +1,41 @@
 """Benchmark of the hevc.js B200 reconstruction back end.
 
-Workload (one step): reconstruct B 1920x1080 4:2:0 8-bit pictures — motion
-compensation from two reference pictures held in the HBM DPB, dequant + inverse
-transform, intra wavefront, deblocking, SAO — from seeded synthetic P/B picture syntax
-(CU quadtree split 0.5 to 8x8, 10 % intra CUs, 20 % skip, 50 % bi-prediction, 10 %
-explicit WP, MVs +-256 qpel, QP 22..37, SAO per CTU), one picture per stream, B streams
-merged into shared launches (the batched form).  The plain form (one launch per stage
-per picture) is timed beside it and reported as "plain".  Output is bit-exact against
-the reference (checked by the tests; the bench verifies one picture per stream against
-the oracle before timing).
+Workload (one step): one 60-picture GOP of 8 streams of 1920x1080 4:2:0 8-bit pictures —
+per stream an I picture, then 59 P/B pictures, each predicted from the stream's two
+previous pictures in its HBM DPB (a ring of 3 slots) — reconstructed from seeded
+synthetic picture syntax (CU quadtree split 0.5 to 8x8; P/B: 10 % intra CUs, 20 % skip,
+50 % bi-prediction, 10 % explicit WP, MVs +-256 qpel; QP 22..37; SAO per CTU): motion
+compensation, dequant + inverse transform, intra wavefront, deblocking, SAO.  The 8
+streams' pictures of one GOP position are merged into one batch (one launch per stage);
+the 60 batches run in decode order, each after the one it references.  The plain form
+(one launch per stage per picture) is timed beside it.  Output is bit-exact against the
+reference (checked by the tests; the bench checks the first three pictures of every
+stream against the oracle before timing, chaining the oracle's own outputs as references).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-value      frames/s over the whole job with the records already in HBM, served form: two
-           groups of B streams whose batches alternate over two lanes (hevcgpu_lane_*), so
-           consecutive batches overlap on the device (device time from an event both lanes
-           wait for to the later lane's last event, max over ranks).  "batched" is the same
-           batches on one queue; "plain" one launch per stage per picture.
-e2e        frames/s through the C ABI from host memory: per step the pictures' records, kept
-           in page-locked host memory (hevcgpu_host_alloc, as a recorder writing there would),
-           are copied host->device with the work lists the library's host workers derive from
-           them (hevcgpu_jobs_prepare), the batch is launched on a lane, and every reconstructed
-           picture is copied device->host into pinned host frame buffers
-           (hevcgpu_lane_slots_download_async, waited for with hevcgpu_lane_wait before the
-           buffers are reused two steps later and at the end); consecutive steps alternate
-           lanes, so step k's host preparation overlaps step k-1 on the device and its copies.
-stages     per-stage device times from CUDA events recorded around each stage on the
-           library's stream, in a separate pass of the same batched step (the timed region
-           itself carries no extra events).
+value      frames/s over the whole job with the records already in HBM: K GOPs, batched
+           form, timed on the device from before the first batch to after the last (max
+           over ranks).  "plain" is one launch per stage per picture on the same GOPs.
+frame_ms   device time of each GOP position's batch (all its pictures complete with it),
+           p50 and p99 over the timed batches; i_frame_ms / pb_frame_ms split it by kind.
+e2e        frames/s through the C ABI from host memory: per pair of GOP positions the 16
+           pictures' records, kept in page-locked host memory (hevcgpu_host_alloc, as a
+           recorder writing there would), are copied host->device with the work lists the
+           library's host workers derive from them (hevcgpu_jobs_prepare); the two batches are
+           launched in order on the streams' lane and every reconstructed picture is copied
+           device->host into pinned frame buffers (hevcgpu_lane_slots_download_async, waited
+           for with hevcgpu_lane_wait before the buffers are reused and at the end).
+stages     per-stage device times over one GOP from CUDA events recorded around each stage
+           on the library's stream, in a separate pass (the timed region carries no extra
+           events); the roofline is that of the dominant stage.
+pb16       the P/B steady state: 2 groups of 16 streams of P/B pictures whose batches
+           alternate over two lanes (consecutive batches overlap on the device), with its
+           batched and plain forms and its own end-to-end rate.
+serving    64 live streams of mixed resolutions with Poisson segment arrivals (4 lanes,
+           continuous batching): per-frame latency p50/p99.
 --impl reference runs privaloops/hevc.js's own reconstruction functions (oracle/_ref,
-           compiled from the reference's sources) on all host cores for the same workload.
+           compiled from the reference's sources) on all host cores for the same GOP mix.
 """
 import argparse
 import json
@@ -46,20 +52,26 @@ sys.path.insert(0, ROOT)
 W_DEFAULT, H_DEFAULT = 1920, 1080
 PICTURE_CFG = dict(p_intra=0.1, p_skip=0.2, p_merge=0.3)
 METRIC = "bit-exact 1080p frames/s on 1 B200, batched/served vs plain GPU; p50/p99 frame ms"
+SLOTS = 3   # DPB ring per stream: picture n writes slot n % 3 and references the two before
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--steps", type=int, default=20, help="GOPs timed")
+    ap.add_argument("--warmup", type=int, default=3, help="GOPs run before timing")
+    ap.add_argument("--streams", type=int, default=8, help="streams per batch (GOP workload)")
+    ap.add_argument("--gop", type=int, default=60, help="pictures per GOP (an I picture, then P/B)")
+    ap.add_argument("--batch", type=int, default=16, help="streams per batch of the P/B steady state")
     ap.add_argument("--width", type=int, default=W_DEFAULT)
     ap.add_argument("--height", type=int, default=H_DEFAULT)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-only", action="store_true", help="short run for ncu captures")
+    ap.add_argument("--profile-only", action="store_true", help="short run for ncu captures (batched launches only)")
+    ap.add_argument("--workload", default="gop", choices=["gop", "pb16"],
+                    help="--profile-only: GOP batches, or the P/B steady state's batches of --batch pictures")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving (Poisson) measurement")
+    ap.add_argument("--no-pb16", action="store_true", help="skip the P/B steady-state measurement")
     ap.add_argument("--serve-seconds", type=float, default=6.0)
     return ap.parse_args()
 
@@ -102,7 +114,7 @@ def job_rate(units_per_rank, world, seconds):
 # --------------------------------------------------------------------------- workload
 
 def make_streams(hb, n, w, h, seed0):
-    """n pictures' syntax and their two reference pictures (content seeds per stream)."""
+    """n P/B pictures' syntax and their two reference pictures (content seeds per stream)."""
     pics, refs = [], []
     for i in range(n):
         seed = seed0 + 97 * i
@@ -111,22 +123,66 @@ def make_streams(hb, n, w, h, seed0):
     return pics, refs
 
 
+def ref_slots_of(n):
+    """(list-0, list-1) DPB slots that picture n >= 1 of a stream references."""
+    a, b = (n - 1) % SLOTS, (n - 2) % SLOTS
+    return [a, b], [b, a]
+
+
+def make_gop(hb, n_streams, w, h, seed0):
+    """Per stream: (I picture, P/B pictures by DPB phase n % 3, contents of its 3 slots
+    before picture 0).  Picture n >= 1 of a stream uses the P/B syntax of its phase, whose
+    reference slots are the two pictures before it."""
+    gop = []
+    for i in range(n_streams):
+        seed = seed0 + 97 * i
+        ipic = hb.Picture(hb.default_cfg(w, h, seed, slice_type=2, poc=0))
+        pb = []
+        for ph in range(SLOTS):
+            pic = hb.Picture(hb.default_cfg(w, h, seed + 11 + ph, poc=8, **PICTURE_CFG))
+            l0, l1 = ref_slots_of(ph + SLOTS)
+            prm = pic.syn.params
+            for k in range(prm.num_ref[0]):
+                prm.ref_slot[0][k] = l0[k]
+            for k in range(prm.num_ref[1]):
+                prm.ref_slot[1][k] = l1[k]
+            pb.append(pic)
+        gop.append((ipic, pb, [hb.content(w, h, seed + 1 + s) for s in range(SLOTS)]))
+    return gop
+
+
+def gop_picture(stream, n):
+    ipic, pb, _ = stream
+    return ipic if n == 0 else pb[n % SLOTS]
+
+
+def gop_sequence(gop, frames):
+    """(picture, reference planes) of every picture of one GOP in decode order, position
+    by position: the CPU arms' work list (every picture reads the stream's initial slots,
+    so the pictures are independent there; the work per picture is the same)."""
+    return [(gop_picture(s, n), s[2]) for n in range(frames) for s in gop]
+
+
 def algorithmic_bytes(hb, pic):
     """Algorithmic HBM bytes per stage of one picture (reads + writes the stage must do)."""
     import numpy as np
     s = pic.syn
     W, H = s.params.width, s.params.height
     npu, ntu = s.num_pus, s.num_tus
-    pu = np.ctypeslib.as_array(C.cast(s.pus, C.POINTER(C.c_uint8)), (npu * 20,)).view(
-        np.dtype([("x", "<u2"), ("y", "<u2"), ("w", "u1"), ("h", "u1"), ("r", "i1", 2), ("mv", "<i2", 4),
-                  ("wp", "<i2"), ("pad", "<u2")]))
+
+    def records(ptr, n, dtype):   # an array of n records at ptr (none for n == 0: ptr may be NULL)
+        if n == 0:
+            return np.zeros(0, dtype)
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint8)), (n * dtype.itemsize,)).view(dtype)
+
+    pu = records(s.pus, npu, np.dtype([("x", "<u2"), ("y", "<u2"), ("w", "u1"), ("h", "u1"), ("r", "i1", 2),
+                                       ("mv", "<i2", 4), ("wp", "<i2"), ("pad", "<u2")]))
     pw, ph = pu["w"].astype(np.int64), pu["h"].astype(np.int64)
     lists = (pu["r"] >= 0).sum(axis=1)
     mc_read = int((lists * ((pw + 7) * (ph + 7) + 2 * (pw // 2 + 3) * (ph // 2 + 3))).sum())
     mc_write = int((pw * ph * 3 // 2).sum())
-    tu = np.ctypeslib.as_array(C.cast(s.tus, C.POINTER(C.c_uint8)), (ntu * 16,)).view(
-        np.dtype([("x", "<u2"), ("y", "<u2"), ("l", "u1"), ("c", "u1"), ("qp", "u1"), ("f", "u1"), ("m", "u1"),
-                  ("r", "u1", 3), ("off", "<u4")]))
+    tu = records(s.tus, ntu, np.dtype([("x", "<u2"), ("y", "<u2"), ("l", "u1"), ("c", "u1"), ("qp", "u1"),
+                                       ("f", "u1"), ("m", "u1"), ("r", "u1", 3), ("off", "<u4")]))
     n2 = (1 << tu["l"].astype(np.int64)) ** 2
     coded = (tu["f"] & 2) != 0
     intra = (tu["f"] & 1) != 0
@@ -239,13 +295,13 @@ class ClockSampler:
 
 # --------------------------------------------------------------------------- CPU arms
 
-def cpu_run(checker, pics, refs, n_pictures, threads):
-    """Reconstruct n_pictures (round robin over the generated ones) on host threads."""
+def cpu_run(checker, seq, first, n_pictures, threads):
+    """Reconstruct n_pictures of the work list seq (round robin from index first) on host
+    threads."""
     from concurrent.futures import ThreadPoolExecutor
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=threads) as ex:
-        list(ex.map(lambda i: checker.reconstruct_picture(pics[i % len(pics)], refs[i % len(pics)]),
-                    range(n_pictures)))
+        list(ex.map(lambda i: checker.reconstruct_picture(*seq[(first + i) % len(seq)]), range(n_pictures)))
     return time.perf_counter() - t0
 
 
@@ -256,26 +312,40 @@ def cpu_checker():
     return oracle.port(), "port"
 
 
+def gop_workload_name(W, H, G, F):
+    return (f"{W}x{H} 4:2:0 8-bit GOP reconstruction: {G} streams x {F} pictures (an I picture, then P/B "
+            f"pictures predicted from the two before), MC + residual + intra wavefront + deblocking + SAO, "
+            f"the {G} streams' pictures of a GOP position in one batch, batches in decode order")
+
+
 def run_reference(args, hb, rank, world):
+    """privaloops/hevc.js's own functions on the host cores, on the GOP mix: each step
+    reconstructs the next `batch` pictures of the GOP work list."""
     if rank != 0:
         return None
-    pics, refs = make_streams(hb, args.batch, args.width, args.height, 1000)
+    W, H, G, F, B = args.width, args.height, args.streams, args.gop, args.batch
+    seq = gop_sequence(make_gop(hb, G, W, H, rank_seed0(0)), F)
     checker, kind = cpu_checker()
     threads = os.cpu_count() or 1
+    pos = 0
     for _ in range(args.warmup):
-        cpu_run(checker, pics, refs, args.batch, threads)
-    times = [cpu_run(checker, pics, refs, args.batch, threads) for _ in range(args.steps)]
+        cpu_run(checker, seq, pos, B, threads)
+        pos += B
+    times = []
+    for _ in range(args.steps):
+        times.append(cpu_run(checker, seq, pos, B, threads))
+        pos += B
     total = sum(times)
-    value = args.batch * args.steps / total
+    value = B * args.steps / total
     line = {"metric": METRIC, "value": round(value, 3), "unit": "frames/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * total / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/int16/int32",
-            "data": "synthetic (seeded P/B picture syntax and sinusoid references)", "impl": "reference",
-            "config": {"workload": f"{args.width}x{args.height} 4:2:0 8-bit P/B picture reconstruction "
-                                   f"(MC + residual + intra + deblocking + SAO), {args.batch} pictures per step",
-                       "batch": args.batch, "parallelism": f"{threads} host threads, one picture per thread"},
+            "data": "synthetic (seeded picture syntax and sinusoid reference pictures)", "impl": "reference",
+            "config": {"workload": gop_workload_name(W, H, G, F), "global_batch": G,
+                       "parallelism": f"{threads} host threads, one picture per thread",
+                       "step": f"{B} consecutive pictures of the GOP work list"},
             "cpu_baseline": {"value": round(value, 3), "unit": "frames/s", "cores": threads, "kind": kind,
-                             "sample": f"{args.batch} pictures per step x {args.steps} steps"},
+                             "sample": f"{B} pictures of the GOP mix per step x {args.steps} steps"},
             "e2e": {"value": round(value, 3), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
 
@@ -283,6 +353,11 @@ def run_reference(args, hb, rank, world):
 # --------------------------------------------------------------------------- GPU arm
 
 import ctypes as C  # noqa: E402
+
+
+def pct(v, q):
+    s = sorted(v)
+    return s[min(len(s) - 1, int(q * len(s)))] if s else None
 
 
 def run_ours(args, hb, rank, world, local):
@@ -296,14 +371,281 @@ def run_ours(args, hb, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     ctx = hb.Context(local)
     stream = torch.cuda.ExternalStream(ctx.cuda_stream, device=dev)
-    W, H, B = args.width, args.height, args.batch
-    slots = [2] * B
+    W, H, G, F = args.width, args.height, args.streams, args.gop
+    if args.profile_only and args.workload == "pb16":
+        # one set-up launch of B P/B pictures, then --steps batched launches of them
+        pics, refs = make_streams(hb, args.batch, W, H, rank_seed0(rank))
+        sts, js = [], []
+        for i in range(args.batch):
+            st = ctx.open_stream(W, H, 3)
+            st.upload(0, refs[i][0])
+            st.upload(1, refs[i][1])
+            sts.append(st)
+            js.append(st.prepare(pics[i]))
+        for _ in range(1 + max(1, args.steps)):
+            hb.batch_launch(js, [2] * args.batch)
+        ctx.sync()
+        return None
     import oracle
     check = oracle.port()
 
-    def build_group(seed0, verify):
-        """B streams with their two reference pictures in HBM and one prepared P/B
-        picture each; verify: every picture bit-exact against the oracle first."""
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def rank_max(x):
+        return max_over_ranks(x, world, dev)
+
+    # ---- the GOP workload: G streams, records of their I and P/B pictures resident in HBM
+    gop = make_gop(hb, G, W, H, rank_seed0(rank))
+    gop_streams = []
+    for ipic, pb, init in gop:
+        st = ctx.open_stream(W, H, SLOTS)
+        for s in range(SLOTS):
+            st.upload(s, init[s])
+        gop_streams.append(st)
+    jobs_i = [st.prepare(s[0]) for st, s in zip(gop_streams, gop)]
+    jobs_pb = [[st.prepare(s[1][ph]) for st, s in zip(gop_streams, gop)] for ph in range(SLOTS)]
+
+    def frame_jobs(n):
+        return jobs_i if n == 0 else jobs_pb[n % SLOTS]
+
+    def gop_batched(evs=None):
+        for n in range(F):
+            if evs is not None:
+                evs[n][0].record(stream)
+            hb.batch_launch(frame_jobs(n), [n % SLOTS] * G)
+            if evs is not None:
+                evs[n][1].record(stream)
+
+    def gop_plain():
+        for n in range(F):
+            for j in frame_jobs(n):
+                j.launch(n % SLOTS)
+
+    if args.profile_only:
+        for _ in range(max(1, args.steps)):
+            gop_batched()
+        ctx.sync()
+        return None
+
+    # the first three pictures of every stream against the oracle, each picture predicted
+    # from the oracle's own earlier outputs
+    verify_n = min(3, F)
+    for n in range(verify_n):
+        hb.batch_launch(frame_jobs(n), [n % SLOTS] * G)
+    ctx.sync()
+    from concurrent.futures import ThreadPoolExecutor
+
+    def verify_stream(i):
+        dpb = list(gop[i][2])
+        for n in range(verify_n):
+            dpb[n % SLOTS] = check.reconstruct_picture(gop_picture(gop[i], n), dpb)
+        for n in range(verify_n):
+            got = gop_streams[i].download(n % SLOTS)
+            if not np.array_equal(got, dpb[n % SLOTS]):
+                return f"stream {i} picture {n} differs from the oracle in {int((got != dpb[n % SLOTS]).sum())} samples"
+        return None
+
+    with ThreadPoolExecutor(max_workers=G) as ex:
+        errs = [e for e in ex.map(verify_stream, range(G)) if e]
+    if errs:
+        raise SystemExit("bench: " + errs[0])
+
+    # batched GOPs, timed on the library's stream
+    K = args.steps
+    for _ in range(args.warmup):
+        gop_batched()
+    ctx.sync()
+    barrier()
+    torch.cuda.synchronize()
+    evs = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(F)]
+           for _ in range(K)]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.launches
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for k in range(K):
+            gop_batched(evs[k])
+        ev1.record(stream)
+        ev1.synchronize()
+    launches = ctx.launches - l0
+    torch.cuda.synchronize()
+    barrier()
+    gop_ms = rank_max(ev0.elapsed_time(ev1))
+    frame_ms = [[a.elapsed_time(b) for (a, b) in evs[k]] for k in range(K)]
+    all_ms = [x for row in frame_ms for x in row]
+    i_ms = [row[0] for row in frame_ms]
+    pb_ms = [x for row in frame_ms for x in row[1:]]
+    value = job_rate(G * F * K, world, gop_ms / 1000.0)
+
+    # plain form over the same GOPs
+    plain_k = max(2, K // 4)
+    gop_plain()
+    ctx.sync()
+    barrier()
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pl0 = ctx.launches
+    p0.record(stream)
+    for _ in range(plain_k):
+        gop_plain()
+    p1.record(stream)
+    p1.synchronize()
+    plain_launches = ctx.launches - pl0
+    barrier()
+    plain_ms = rank_max(p0.elapsed_time(p1))
+    plain_value = job_rate(G * F * plain_k, world, plain_ms / 1000.0)
+
+    # stage profile over one GOP (separate pass; events between stages)
+    ctx.profile(True)
+    gop_batched()
+    stages = ctx.profile_read()
+    ctx.profile(False)
+
+    # roofline of the dominant stage over the GOP
+    import json as _json
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(_json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    alg_of = {}
+    alg_sum = None
+    for n in range(F):
+        for s in gop:
+            pic = gop_picture(s, n)
+            if id(pic) not in alg_of:
+                alg_of[id(pic)] = algorithmic_bytes(hb, pic)
+            a = alg_of[id(pic)]
+            alg_sum = dict(a) if alg_sum is None else {k: alg_sum[k] + a[k] for k in a}
+    stage_ms = {"mc": stages["mc"][0], "residual": stages["residual"][0], "intra": stages["intra"][0],
+                "deblock": stages["deblock_v"][0] + stages["deblock_h"][0], "sao": stages["sao"][0]}
+    per_stage = {}
+    for k, ms in stage_ms.items():
+        gbs = alg_sum[k] / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
+        per_stage[k] = {"ms_per_gop": round(ms, 4), "alg_bytes_per_gop": alg_sum[k], "GB/s": round(gbs, 1),
+                        "frac_of_hbm": round(gbs / peak, 4)}
+    dom = max(stage_ms, key=lambda k: stage_ms[k])
+    # DRAM bytes (read + write) per batch of each stage's kernels on this workload: one ncu
+    # capture of a GOP of 2 streams at 1080p, scaled by 4 to 8 pictures per launch (each
+    # picture is independent work), the GOP's total divided by its 60 batches
+    # (profiles/kernels_gop8_1080p.md)
+    ncu_dram_gop8 = {"mc": 57565798, "residual": 83249101, "intra": 26371635, "deblock": 78732544, "sao": 25039838}
+    traffic = (ncu_dram_gop8[dom] if dom in ncu_dram_gop8 and (W, H, G, F) == (W_DEFAULT, H_DEFAULT, 8, 60)
+               else None)
+
+    # end to end through the C ABI from host memory: pairs of GOP positions, the 2G
+    # pictures prepared together on the host workers, the two batches launched in decode
+    # order on the streams' lane with their frame copies queued behind them
+    lane = hb.Lane(ctx)
+    frame_bytes = hb.i420_size(W, H)
+    out_host = [[[torch.empty(frame_bytes, dtype=torch.uint8).pin_memory().numpy() for _ in range(G)]
+                 for _ in range(2)] for _ in range(2)]
+    for s in gop:   # records in page-locked memory (set up outside the timing)
+        for pic in [s[0]] + s[1]:
+            pic.pin()
+    e2e_h2d = [0]
+
+    def e2e_gop():
+        tickets, held = [None, None], [[], []]
+        h2d = 0
+        for n0 in range(0, F, 2):
+            i = (n0 // 2) % 2
+            if tickets[i] is not None:
+                for t in tickets[i]:
+                    lane.wait(t)
+                for j in held[i]:
+                    j.free()
+            ns = [n for n in (n0, n0 + 1) if n < F]
+            pics = [gop_picture(s, n) for n in ns for s in gop]
+            js = hb.prepare_batch(gop_streams * len(ns), pics)
+            h2d += sum(j.upload_bytes for j in js)
+            tickets[i] = []
+            for q, n in enumerate(ns):
+                lane.batch_launch(js[q * G:(q + 1) * G], [n % SLOTS] * G)
+                tickets[i].append(lane.download_batch_async(gop_streams, [n % SLOTS] * G, out_host[i][q]))
+            held[i] = js
+        for i in range(2):
+            if tickets[i] is not None:
+                for t in tickets[i]:
+                    lane.wait(t)
+                for j in held[i]:
+                    j.free()
+        e2e_h2d[0] = h2d
+
+    e2e_k = max(2, K // 4)
+    e2e_gop()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_k):
+        e2e_gop()
+    e2e_s = rank_max(time.perf_counter() - t0)
+    e2e_value = job_rate(G * F * e2e_k, world, e2e_s)
+
+    clk = clocks.summary()
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "frames/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(gop_ms / K, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8/int16/int32", "data": "synthetic (seeded picture "
+        "syntax and sinusoid reference pictures; no public dataset)",
+        "config": {"workload": gop_workload_name(W, H, G, F), "global_batch": G * world,
+                   "step": f"one GOP: {F} batches of {G} pictures", "parallelism":
+                   f"replicas x{world} (streams sharded, no collective)",
+                   "l2": "inputs larger than L2: a GOP's working set (the streams' DPB slots and the records "
+                         "and work buffers of 4 x G prepared pictures) is several hundred MB; each batch reads "
+                         "the pictures the batch before it wrote, as decoding does"},
+        "plain": {"value": round(plain_value, 2), "unit": "frames/s",
+                  "ms_per_picture": round(plain_ms / plain_k / (G * F), 4),
+                  "gpu_launches_per_picture": round(plain_launches / plain_k / (G * F), 1)},
+        "batched_over_plain": round(value / plain_value, 3),
+        "frame_ms": {"p50": round(statistics.median(all_ms), 4), "p99": round(pct(all_ms, 0.99), 4),
+                     "note": "device time of a GOP position's batch; every picture of a batch completes with it"},
+        "i_frame_ms": {"p50": round(statistics.median(i_ms), 4), "max": round(max(i_ms), 4)},
+        "pb_frame_ms": {"p50": round(statistics.median(pb_ms), 4), "p99": round(pct(pb_ms, 0.99), 4)},
+        "e2e": {"value": round(e2e_value, 2), "unit": "frames/s", "h2d_bytes_per_step": int(e2e_h2d[0]),
+                "d2h_bytes_per_step": int(G * F * frame_bytes)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": per_stage[dom]["GB/s"], "peak": peak,
+                     "unit": "GB/s", "frac": per_stage[dom]["frac_of_hbm"],
+                     "traffic": None if traffic is None else int(traffic),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, one capture",
+                     "peak_source": peak_src},
+        "stages": per_stage,
+        "clocks": clk,
+    }
+    lane.close()
+    if not args.no_pb16:
+        line["pb16"] = run_pb16(args, hb, ctx, stream, rank, world, dev, check, rank_max, barrier)
+    if not args.no_serving and rank == 0 and W == W_DEFAULT and H == H_DEFAULT:
+        line["serving"] = run_serving(args, hb, local)
+    if rank == 0 and not args.no_cpu_baseline:
+        # last, so that its all-core host load is over before anything host-bound is timed
+        checker, kind = cpu_checker()
+        threads = os.cpu_count() or 1
+        seq = gop_sequence(gop, F)
+        # bounded sample: about 10 s of host work, whole GOPs of the same mix
+        t_probe = cpu_run(checker, seq, 0, len(seq), threads)
+        reps = max(1, int(round(10.0 / max(t_probe, 1e-3))))
+        t = cpu_run(checker, seq, 0, reps * len(seq), threads)
+        line["cpu_baseline"] = {"value": round(reps * len(seq) / t, 3), "unit": "frames/s", "cores": threads,
+                                "kind": kind, "sample": f"{reps} GOP(s) of {G} streams x {F} pictures "
+                                f"({reps * len(seq)} pictures) on {threads} host threads ({t:.1f} s)"}
+    for st in gop_streams:
+        st.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def run_pb16(args, hb, ctx, stream, rank, world, dev, check, rank_max, barrier):
+    """The P/B steady state: two groups of B streams with one prepared P/B picture each;
+    their batches alternate over two lanes, so consecutive batches overlap on the device."""
+    import numpy as np
+    import torch
+    W, H, B, K = args.width, args.height, args.batch, max(20, 5 * args.steps)
+    slots = [2] * B
+
+    def build_group(seed0):
         g_pics, g_refs = make_streams(hb, B, W, H, seed0)
         g_streams, g_jobs = [], []
         for i in range(B):
@@ -314,123 +656,70 @@ def run_ours(args, hb, rank, world, local):
             g_jobs.append(st.prepare(g_pics[i]))
         hb.batch_launch(g_jobs, slots)
         ctx.sync()
-        for i in range(B if verify else 0):
+        for i in range(B):
             got = g_streams[i].download(2)
             want = check.reconstruct_picture(g_pics[i], g_refs[i])
             if not np.array_equal(got, want):
-                raise SystemExit(f"bench: picture {i} differs from the oracle in {int((got != want).sum())} samples")
-        return g_pics, g_refs, g_streams, g_jobs
+                raise SystemExit(f"bench: P/B picture {i} differs from the oracle in {int((got != want).sum())} samples")
+        return g_pics, g_streams, g_jobs
 
-    # replicas: each rank reconstructs its own streams (different seeds), no collective.
-    # Two groups of B streams: the served form alternates their batches over two lanes.
-    verify = args.steps > 0 and not args.profile_only
-    pics, refs, streams, jobs = build_group(rank_seed0(rank), verify)
-    groups = [jobs]
-    grp_pics, grp_streams = [pics], [streams]
-    if not args.profile_only:
-        pics_b, _, streams_b, jobs_b = build_group(rank_seed0(rank) + 50000, verify)
-        groups.append(jobs_b)
-        grp_pics.append(pics_b)
-        grp_streams.append(streams_b)
-
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-
-    def rank_max(x):
-        return max_over_ranks(x, world, dev)
-
-    def timed(fn, steps, warmup):
-        for _ in range(warmup):
-            fn()
-        ctx.sync()
-        barrier()
-        torch.cuda.synchronize()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        step_ms = []
-        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
-        l0 = ctx.launches
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-            evs[0].record(stream)
-            for k in range(steps):
-                fn()
-                evs[k + 1].record(stream)
-            ev1.record(stream)
-        ev1.synchronize()
-        torch.cuda.synchronize()
-        barrier()
-        ms = ev0.elapsed_time(ev1)
-        step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
-        return rank_max(ms), step_ms, ctx.launches - l0
-
-    if args.profile_only:
-        for _ in range(max(1, args.steps)):
-            hb.batch_launch(jobs, slots)
-        ctx.sync()
-        return None
-
-    # served form: batch k of B pictures goes to lane k % 2 (group k % 2), so consecutive
-    # batches overlap on the device; timed from an event that both lanes wait for to the
-    # later of the lanes' last events
+    seed0 = rank_seed0(rank) + 70000
+    pics_a, streams_a, jobs_a = build_group(seed0)
+    pics_b, streams_b, jobs_b = build_group(seed0 + 50000)
+    groups, grp_pics, grp_streams = [jobs_a, jobs_b], [pics_a, pics_b], [streams_a, streams_b]
     lanes = [hb.Lane(ctx), hb.Lane(ctx)]
     lane_st = [torch.cuda.ExternalStream(ln.cuda_stream, device=dev) for ln in lanes]
 
-    def timed_served(steps, warmup):
-        for k in range(warmup):
-            lanes[k % 2].batch_launch(groups[k % 2], slots)
-        for ln in lanes:
-            ln.sync()
+    for k in range(args.warmup):
+        lanes[k % 2].batch_launch(groups[k % 2], slots)
+    for ln in lanes:
+        ln.sync()
+    ctx.sync()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev0.record(lane_st[0])
+    lane_st[1].wait_event(ev0)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    for k in range(K):
+        i = k % 2
+        starts[k].record(lane_st[i])
+        lanes[i].batch_launch(groups[i], slots)
+        ends[k].record(lane_st[i])
+    for ln in lanes:
+        ln.sync()
+    torch.cuda.synchronize()
+    barrier()
+    served_ms = rank_max(max(ev0.elapsed_time(ends[K - 1]), ev0.elapsed_time(ends[K - 2])))
+    batch_ms = [starts[k].elapsed_time(ends[k]) for k in range(K)]
+
+    def timed(fn, steps):
+        fn()
         ctx.sync()
         barrier()
         torch.cuda.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev0.record(lane_st[0])
-        lane_st[1].wait_event(ev0)
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-        l0 = ctx.launches
-        for k in range(steps):
-            i = k % 2
-            starts[k].record(lane_st[i])
-            lanes[i].batch_launch(groups[i], slots)
-            ends[k].record(lane_st[i])
-        for ln in lanes:
-            ln.sync()
-        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            fn()
+        b.record(stream)
+        b.synchronize()
         barrier()
-        ms = max(ev0.elapsed_time(ends[steps - 1]), ev0.elapsed_time(ends[steps - 2]) if steps > 1 else 0.0)
-        batch_ms = [starts[k].elapsed_time(ends[k]) for k in range(steps)]
-        return rank_max(ms), batch_ms, ctx.launches - l0
+        return rank_max(a.elapsed_time(b))
 
-    with ClockSampler(local) as clocks:
-        served_ms, step_ms, launches = timed_served(args.steps, args.warmup)
-    batched_steps = max(3, args.steps // 2)
-    batched_ms, _, _ = timed(lambda: hb.batch_launch(jobs, slots), batched_steps, args.warmup)
-    plain_steps = max(3, args.steps // 4)
-    plain_ms, _, plain_launches = timed(lambda: [j.launch(2) for j in jobs], plain_steps, args.warmup)
+    batched_k, plain_k = max(3, K // 2), max(3, K // 4)
+    batched_ms = timed(lambda: hb.batch_launch(jobs_a, slots), batched_k)
+    plain_ms = timed(lambda: [j.launch(2) for j in jobs_a], plain_k)
 
-    # stage profile (separate pass; events between stages)
-    ctx.profile(True)
-    prof_steps = max(3, args.steps // 4)
-    for _ in range(prof_steps):
-        hb.batch_launch(jobs, slots)
-    stages = ctx.profile_read()
-    ctx.profile(False)
-
-    # end to end through the C ABI from host memory, pipelined over the two lanes: step k
-    # prepares its B pictures on the host workers (records packed into pinned memory and
-    # copied host->device: hevcgpu_jobs_prepare), launches them on lane k % 2 and queues the
-    # copies of its frames into pinned host frame buffers behind them
-    # (hevcgpu_lane_slots_download_async); the frames of step k are waited for
-    # (hevcgpu_lane_wait) when their buffers come round again at step k + 2, and at the end
     frame_bytes = hb.i420_size(W, H)
     out_host = [[torch.empty(frame_bytes, dtype=torch.uint8).pin_memory().numpy() for _ in range(B)]
                 for _ in range(2)]
-    h2d_bytes = 0
+    for g_pics in grp_pics:
+        for p in g_pics:
+            p.pin()
 
     def e2e_run(steps):
-        nonlocal h2d_bytes
         tickets, held = [None, None], [[], []]
         for k in range(steps):
             i = k % 2
@@ -439,7 +728,6 @@ def run_ours(args, hb, rank, world, local):
                 for j in held[i]:
                     j.free()
             js = hb.prepare_batch(grp_streams[i], grp_pics[i])
-            h2d_bytes = sum(j.upload_bytes for j in js)
             lanes[i].batch_launch(js, slots)
             tickets[i] = lanes[i].download_batch_async(grp_streams[i], slots, out_host[i])
             held[i] = js
@@ -449,123 +737,49 @@ def run_ours(args, hb, rank, world, local):
                 for j in held[i]:
                     j.free()
 
-    # the records in page-locked memory, where a recorder writing into hevcgpu_host_alloc
-    # buffers keeps them: their upload needs no staging copy (set up outside the timing)
-    for g_pics in grp_pics:
-        for p in g_pics:
-            p.pin()
-    e2e_steps = max(4, args.steps // 5)
+    e2e_k = max(4, K // 5)
     e2e_run(2)
     barrier()
     t0 = time.perf_counter()
-    e2e_run(e2e_steps)
+    e2e_run(e2e_k)
     e2e_s = rank_max(time.perf_counter() - t0)
-    d2h_bytes = B * frame_bytes
-
-    value = job_rate(B * args.steps, world, served_ms / 1000.0)
-    batched_value = job_rate(B * batched_steps, world, batched_ms / 1000.0)
-    plain_value = job_rate(B * plain_steps, world, plain_ms / 1000.0)
-    e2e_value = job_rate(B * e2e_steps, world, e2e_s)
-
-    # roofline of the dominant stage
-    import json as _json
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peak, peak_src = 6650.0, "fallback"
-    if os.path.exists(peaks_path):
-        peak, peak_src = float(_json.load(open(peaks_path))["hbm_gbs"]), "measured"
-    alg = [algorithmic_bytes(hb, p) for p in pics]
-    alg_sum = {k: sum(a[k] for a in alg) for k in alg[0]}
-    stage_ms = {"mc": stages["mc"][0], "residual": stages["residual"][0], "intra": stages["intra"][0],
-                "deblock": stages["deblock_v"][0] + stages["deblock_h"][0], "sao": stages["sao"][0]}
-    per_stage = {}
-    for k, ms in stage_ms.items():
-        per_launch_ms = ms / prof_steps
-        gbs = alg_sum[k] / (per_launch_ms / 1000.0) / 1e9 if per_launch_ms > 0 else 0.0
-        per_stage[k] = {"ms_per_step": round(per_launch_ms, 4), "alg_bytes_per_step": alg_sum[k],
-                        "GB/s": round(gbs, 1), "frac_of_hbm": round(gbs / peak, 4)}
-    dom = max(stage_ms, key=lambda k: stage_ms[k])
-    # DRAM bytes (read + write) per launch of each stage's kernels, from one ncu capture of
-    # this workload at 16 pictures per launch (profiles/kernels_pb16_1080p.md); scaled by
-    # the pictures per launch when --batch differs (the traffic grows with the pictures).
-    ncu_dram_16 = {"mc": 146.71e6, "residual": 170.51e6, "intra": 50.43e6, "deblock": 160.87e6, "sao": 68.79e6}
-    traffic = ncu_dram_16[dom] * B / 16.0 if W == W_DEFAULT and H == H_DEFAULT else None
-
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        checker, kind = cpu_checker()
-        threads = os.cpu_count() or 1
-        # bounded sample: about 10 s of wall time on all host threads
-        t_probe = cpu_run(checker, pics, refs, threads, threads)
-        n = threads * max(1, int(10.0 / max(t_probe, 1e-3)))
-        t = cpu_run(checker, pics, refs, n, threads)
-        cpu = {"value": round(n / t, 3), "unit": "frames/s", "cores": threads, "kind": kind,
-               "sample": f"{n} of the bench's {W}x{H} pictures on {threads} host threads ({t:.1f} s)"}
-
-    clk = clocks.summary()
-    step_sorted = sorted(step_ms)
-    line = {
-        "metric": METRIC, "value": round(value, 2), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(served_ms / args.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8/int16/int32", "data": "synthetic (seeded P/B picture "
-        "syntax and sinusoid reference pictures; no public dataset)",
-        "config": {"workload": f"{W}x{H} 4:2:0 8-bit P/B picture reconstruction (MC + residual + intra wavefront + "
-                               f"deblocking + SAO), {B} streams per batched launch, batches alternating over 2 "
-                               f"lanes (2 x {B} streams, consecutive batches overlap on the device)",
-                   "global_batch": B * world, "streams_in_flight": 2 * B * world,
-                   "parallelism": f"replicas x{world} (streams sharded, no collective)",
-                   "l2": "inputs larger than L2 (2 x B streams x 4 HBM buffers)"},
-        "batched": {"value": round(batched_value, 2), "unit": "frames/s",
-                    "ms_per_step": round(batched_ms / batched_steps, 4),
-                    "note": "the same batches on one queue, no overlap between consecutive batches"},
-        "plain": {"value": round(plain_value, 2), "unit": "frames/s", "ms_per_picture": round(plain_ms / plain_steps / B, 4),
-                  "gpu_launches_per_picture": round(plain_launches / plain_steps / B, 1)},
-        "batched_over_plain": round(value / plain_value, 3),
-        "frame_ms": {"p50": round(statistics.median(step_ms), 4),
-                     "p99": round(step_sorted[min(len(step_sorted) - 1, int(0.99 * len(step_sorted)))], 4),
-                     "note": "device time from a batch's start on its lane to its completion; every "
-                             "picture of a batch completes with it"},
-        "e2e": {"value": round(e2e_value, 2), "unit": "frames/s", "h2d_bytes_per_step": int(h2d_bytes),
-                "d2h_bytes_per_step": int(d2h_bytes)},
-        "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": per_stage[dom]["GB/s"], "peak": peak,
-                     "unit": "GB/s", "frac": per_stage[dom]["frac_of_hbm"],
-                     "traffic": None if traffic is None else int(traffic),
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture",
-                     "peak_source": peak_src},
-        "stages": per_stage,
-        "clocks": clk,
-    }
-    if cpu:
-        line["cpu_baseline"] = cpu
-    if not args.no_serving and rank == 0 and W == W_DEFAULT and H == H_DEFAULT:
-        # the serving workload: 64 streams of mixed resolutions, Poisson segment arrivals
-        from hevc_b200 import serve
-        sctx = hb.Context(local)   # a serving process owns its context
-        pool = serve.PicturePool(hb, [(416, 240), (1280, 720), (1920, 1080), (3840, 2160)], pin=True)
-        # an unmeasured 2 s run first: the first use of a context's pools and launch paths
-        # in a process costs once what a long-running server pays at start-up
-        serve.run_poisson(hb, sctx, seconds=2.0, n_streams=64, seed=5, lanes=4, pool=pool)
-        res = serve.run_poisson(hb, sctx, seconds=args.serve_seconds, n_streams=64, seed=4, lanes=4, pool=pool)
-        sctx.close()
-        line["serving"] = {
-            "workload": "64 live streams, 416x240 / 1280x720 / 1920x1080 / 3840x2160 in ratio 4:3:2:1, "
-                        "30 or 60 fps, 2-second segments (I picture, then P/B) arriving as a Poisson process "
-                        f"(seed 4) for {args.serve_seconds:g} s; 4 lanes, continuous batching",
-            "frames": res["frames"], "frames_per_s": round(res["frames_per_s"], 1),
-            "p50_ms": round(res["p50_ms"], 2), "p99_ms": round(res["p99_ms"], 2), "max_ms": round(res["max_ms"], 2),
-            "steady_p50_ms": round(res["steady_p50_ms"], 2), "steady_p99_ms": round(res["steady_p99_ms"], 2),
-            "steady": "frames released after the first 2 s, when every stream's first segment (and its "
-                      "I picture) has arrived",
-            "latency": "device completion of the picture's batch minus the picture's live release time "
-                       "(segment start + i / fps); records prepared on host workers, CABAC not included; "
-                       "measured after an unmeasured 2 s warm-up run on the same context"}
     for ln in lanes:
         ln.close()
-    for st in streams:
+    for st in streams_a + streams_b:
         st.close()
-    if world > 1:
-        torch.distributed.destroy_process_group()
-    return line if rank == 0 else None
+    return {"workload": f"{W}x{H} P/B pictures, 2 groups of {B} streams whose batches alternate over 2 lanes "
+                        "(consecutive batches overlap on the device)",
+            "value": round(job_rate(B * K, world, served_ms / 1000.0), 2), "unit": "frames/s", "steps": K,
+            "batched": round(job_rate(B * batched_k, world, batched_ms / 1000.0), 2),
+            "plain": round(job_rate(B * plain_k, world, plain_ms / 1000.0), 2),
+            "frame_ms": {"p50": round(statistics.median(batch_ms), 4), "p99": round(pct(batch_ms, 0.99), 4)},
+            "e2e": round(job_rate(B * e2e_k, world, e2e_s), 2)}
+
+
+def run_serving(args, hb, local):
+    """64 live streams of mixed resolutions, Poisson segment arrivals (serve.run_poisson)."""
+    from hevc_b200 import serve
+    sctx = hb.Context(local)   # a serving process owns its context
+    pool = serve.PicturePool(hb, [(416, 240), (1280, 720), (1920, 1080), (3840, 2160)], pin=True)
+    # an unmeasured 2 s run first: the first use of a context's pools and launch paths in a
+    # process costs once what a long-running server pays at start-up
+    serve.run_poisson(hb, sctx, seconds=2.0, n_streams=64, seed=5, lanes=4, pool=pool)
+    res = serve.run_poisson(hb, sctx, seconds=args.serve_seconds, n_streams=64, seed=4, lanes=4, pool=pool)
+    sctx.close()
+    return {
+        "workload": "64 live streams, 416x240 / 1280x720 / 1920x1080 / 3840x2160 in ratio 4:3:2:1, "
+                    "30 or 60 fps, 2-second segments (I picture, then P/B) arriving as a Poisson process "
+                    f"(seed 4) for {args.serve_seconds:g} s; 4 lanes, continuous batching",
+        "frames": res["frames"], "frames_per_s": round(res["frames_per_s"], 1),
+        "p50_ms": round(res["p50_ms"], 2), "p99_ms": round(res["p99_ms"], 2), "max_ms": round(res["max_ms"], 2),
+        "steady_p50_ms": round(res["steady_p50_ms"], 2), "steady_p99_ms": round(res["steady_p99_ms"], 2),
+        "frames_over_100ms": res["frames_over_100ms"], "worst_release_s": round(res["worst_release_s"], 3),
+        "steady": "frames released after the first 2 s, when every stream's first segment (and its "
+                  "I picture) has arrived",
+        "latency": "device completion of the picture's batch minus the picture's live release time "
+                   "(segment start + i / fps); records prepared on host workers, CABAC not included; "
+                   "frames/s is the offered load served (the run ends when the last released frame "
+                   "is done); measured after an unmeasured 2 s warm-up run on the same context"}
 
 
 def main():

@@ -247,6 +247,8 @@ def gpu_lib():
             "hevcgpu_stream_close": ([P], None),
             "hevcgpu_slot_upload": ([P, C.c_int32, u8p], C.c_int),
             "hevcgpu_slot_download": ([P, C.c_int32, u8p], C.c_int),
+            "hevcgpu_slot_download_frame": ([P, C.c_int32, C.POINTER(abi.Crop), C.POINTER(C.c_uint16), C.c_int32,
+                                             C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), C.c_int32], C.c_int),
             "hevcgpu_slot_device_ptr": ([P, C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P),
                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
             "hevcgpu_job_prepare": ([P, C.POINTER(PictureSyntax), C.POINTER(P)], C.c_int),
@@ -416,6 +418,19 @@ class Stream:
             out = np.empty(i420_size(self.width, self.height), np.uint8)
         _check(self.lib.hevcgpu_slot_download(self.h, slot, as_ptr(out, C.c_uint8)))
         return out
+
+    def download_frame(self, slot, crop=None, stride_y=None, stride_c=None):
+        """The slot as hevc_decoder_get_frame gives a picture (hevcgpu_slot_download_frame):
+        (y, cb, cr) uint16 planes inside the conformance window crop = (left, right, top,
+        bottom) in luma samples, each a view of width x height samples of rows of the stride."""
+        left, right, top, bottom = crop or (0, 0, 0, 0)
+        w, h = self.width - left - right, self.height - top - bottom
+        sy, sc = stride_y or w, stride_c or w // 2
+        bufs = [np.zeros((h, sy), np.uint16), np.zeros((h // 2, sc), np.uint16), np.zeros((h // 2, sc), np.uint16)]
+        c = abi.Crop(left, right, top, bottom)
+        _check(self.lib.hevcgpu_slot_download_frame(self.h, slot, C.byref(c), as_ptr(bufs[0], C.c_uint16), sy,
+                                                    as_ptr(bufs[1], C.c_uint16), as_ptr(bufs[2], C.c_uint16), sc))
+        return bufs[0][:, :w], bufs[1][:, :w // 2], bufs[2][:, :w // 2]
 
     def prepare(self, pic):
         return Job(self, pic)

@@ -61,6 +61,10 @@ class Scaling(C.Structure):
     _fields_ = [("list", ((C.c_uint8 * 64) * 6) * 4), ("dc", (C.c_uint8 * 6) * 2), ("reserved", C.c_uint8 * 4)]
 
 
+class Crop(C.Structure):
+    _fields_ = [("left", C.c_int32), ("right", C.c_int32), ("top", C.c_int32), ("bottom", C.c_int32)]
+
+
 class PicParams(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("bit_depth", C.c_int32),
                 ("log2_ctb", C.c_int32), ("log2_min_cb", C.c_int32), ("log2_min_tb", C.c_int32),

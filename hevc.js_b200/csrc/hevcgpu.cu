@@ -1700,6 +1700,51 @@ int hevcgpu_slot_download(hevcgpu_stream_t* st, int32_t slot, uint8_t* i420) {
     return HEVCGPU_OK;
 }
 
+int hevcgpu_slot_download_frame(hevcgpu_stream_t* st, int32_t slot, const hevc_crop_t* crop, uint16_t* y,
+                                int32_t stride_y, uint16_t* cb, uint16_t* cr, int32_t stride_c) {
+    if (!st || slot < 0 || slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);
+    if (!y || !cb || !cr) return fail(HEVCGPU_EINVAL, "null planes");
+    const Layout& L = st->lay;
+    const hevc_crop_t c = crop ? *crop : hevc_crop_t{0, 0, 0, 0};
+    if (c.left < 0 || c.right < 0 || c.top < 0 || c.bottom < 0 || ((c.left | c.right | c.top | c.bottom) & 1) ||
+        c.left + c.right >= L.W || c.top + c.bottom >= L.H)
+        return fail(HEVCGPU_EINVAL, "conformance window %d,%d,%d,%d (even luma offsets inside %dx%d)", c.left, c.right,
+                    c.top, c.bottom, L.W, L.H);
+    const int w = L.W - c.left - c.right, h = L.H - c.top - c.bottom;
+    if (stride_y < w || stride_c < w / 2) return fail(HEVCGPU_EINVAL, "strides %d/%d below %d/%d", stride_y, stride_c, w, w / 2);
+    int rc = check_ctx(st->ctx);
+    if (rc) return rc;
+    const uint8_t* s = static_cast<const uint8_t*>(st->slots[(size_t)slot].p);
+    WidenArgs a{};
+    uint16_t* host[3] = {y, cb, cr};
+    const int32_t host_stride[3] = {stride_y, stride_c, stride_c};
+    a.src[0] = s + (int64_t)c.top * L.pitch_y + c.left;
+    a.src[1] = s + L.off_cb + (int64_t)(c.top / 2) * L.pitch_c + c.left / 2;
+    a.src[2] = s + L.off_cr + (int64_t)(c.top / 2) * L.pitch_c + c.left / 2;
+    size_t bytes = 0, off[3];
+    for (int p = 0; p < 3; p++) {
+        a.src_pitch[p] = p ? L.pitch_c : L.pitch_y;
+        a.w[p] = p ? w / 2 : w;
+        a.h[p] = p ? h / 2 : h;
+        a.vecs[p] = (a.w[p] + 7) / 8;
+        a.first[p] = p ? a.first[p - 1] + (int64_t)a.vecs[p - 1] * a.h[p - 1] : 0;
+        off[p] = bytes;
+        bytes += (size_t)align_up((int64_t)a.vecs[p] * 16 * a.h[p], 256);
+    }
+    a.total = a.first[2] + (int64_t)a.vecs[2] * a.h[2];
+    DevBuf stage;
+    if ((rc = stage.get(st->ctx, bytes))) return rc;
+    for (int p = 0; p < 3; p++) a.dst[p] = reinterpret_cast<uint16_t*>(static_cast<uint8_t*>(stage.p) + off[p]);
+    const int threads = 256;
+    k_widen_frame<<<(unsigned)((a.total + threads - 1) / threads), threads, 0, st->ctx->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    for (int p = 0; p < 3; p++)
+        CUDA_TRY(cudaMemcpy2DAsync(host[p], (size_t)host_stride[p] * 2, a.dst[p], (size_t)a.vecs[p] * 16,
+                                   (size_t)a.w[p] * 2, (size_t)a.h[p], cudaMemcpyDeviceToHost, st->ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(st->ctx->stream));
+    return HEVCGPU_OK;
+}
+
 int hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void** cb, void** cr, int32_t* pitch_y,
                             int32_t* pitch_c) {
     if (!st || slot < 0 || slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);

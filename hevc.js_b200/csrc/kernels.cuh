@@ -755,4 +755,35 @@ __global__ void __launch_bounds__(256) k_sao(const __grid_constant__ SegTable st
     }
 }
 
+// Frame output: the conformance window of a slot's three planes widened to 16-bit
+// samples (the HEVCFrame planes of hevc_decoder_get_frame).  Plane p covers rows
+// [0, h[p]) of its window; each thread writes 8 samples (one 16-byte store) of a staged
+// row whose pitch is the window width rounded up to 8 samples, so every store is aligned;
+// the bytes are read one by one (the window may start on any even column).
+struct WidenArgs {
+    const uint8_t* src[3];   // first sample of the window in each plane of the slot
+    int32_t src_pitch[3];
+    uint16_t* dst[3];        // staged planes
+    int32_t w[3], h[3], vecs[3];   // window size; 8-sample vectors per staged row
+    int64_t first[3];              // first vector index of each plane (first[0] = 0)
+    int64_t total;
+};
+
+__global__ void __launch_bounds__(256) k_widen_frame(const __grid_constant__ WidenArgs a) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.total) return;
+    const int p = i >= a.first[2] ? 2 : (i >= a.first[1] ? 1 : 0);
+    const int64_t k = i - a.first[p];
+    const int row = (int)(k / a.vecs[p]), x0 = (int)(k % a.vecs[p]) * 8;
+    const uint8_t* s = a.src[p] + (int64_t)row * a.src_pitch[p];
+    uint32_t v[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int x = x0 + 2 * q;
+        const uint32_t lo = x < a.w[p] ? s[x] : 0u, hi = x + 1 < a.w[p] ? s[x + 1] : 0u;
+        v[q] = lo | (hi << 16);
+    }
+    *reinterpret_cast<uint4*>(a.dst[p] + (int64_t)row * a.vecs[p] * 8 + x0) = make_uint4(v[0], v[1], v[2], v[3]);
+}
+
 }  // namespace hevcgpu

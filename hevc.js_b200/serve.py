@@ -332,4 +332,6 @@ def run_poisson(hb, ctx, seconds=5.0, n_streams=64, seed=4, lanes=4, max_batch=6
     return {"streams": len(admitted), "frames": int(len(lat)), "offered_frames": offered,
             "frames_per_s": len(lat) / (t_stop - t0), "p50_ms": pct(lat_ms, 50), "p99_ms": pct(lat_ms, 99),
             "max_ms": float(lat_ms.max()) if len(lat) else None, "steady_frames": int(len(steady)),
+            "frames_over_100ms": int((records[:, 1] > 0.1).sum()) if len(records) else 0,
+            "worst_release_s": float(records[records[:, 1].argmax(), 0] - t0) if len(records) else 0.0,
             "steady_p50_ms": pct(steady, 50), "steady_p99_ms": pct(steady, 99), "wall_s": t_stop - t0}

@@ -240,6 +240,22 @@ int  hevcgpu_stream_open(hevcgpu_ctx_t* ctx, int32_t width, int32_t height,
 void hevcgpu_stream_close(hevcgpu_stream_t* st);
 int  hevcgpu_slot_upload(hevcgpu_stream_t* st, int32_t slot, const uint8_t* i420);
 int  hevcgpu_slot_download(hevcgpu_stream_t* st, int32_t slot, uint8_t* i420);
+
+/* Conformance window in luma samples: conf_win_*_offset times SubWidthC / SubHeightC, as
+ * the reference's Picture keeps it (src/wasm/hevc_api.cpp:58-65); even values for 4:2:0. */
+typedef struct hevc_crop {
+    int32_t left, right, top, bottom;
+} hevc_crop_t;
+
+/* A slot as hevc_decoder_get_frame hands a picture out (src/wasm/hevc_api.cpp:49-77,
+ * HEVCFrame of src/wasm/hevc_api.h:21-33): the samples inside the conformance window as
+ * 16-bit planes.  Writes (W - left - right) x (H - top - bottom) samples to y (row
+ * stride stride_y samples) and half of each to cb and cr (stride_c).  crop NULL is the
+ * whole picture.  The widening runs on the device; the call returns when the planes have
+ * landed.  Replaces the frame copy a caller of hevc_decoder_get_frame makes. */
+int  hevcgpu_slot_download_frame(hevcgpu_stream_t* st, int32_t slot, const hevc_crop_t* crop,
+                                 uint16_t* y, int32_t stride_y, uint16_t* cb, uint16_t* cr,
+                                 int32_t stride_c);
 /* Device address of a slot's Y plane and the row pitches (for zero-copy consumers). */
 int  hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void** cb,
                              void** cr, int32_t* pitch_y, int32_t* pitch_c);

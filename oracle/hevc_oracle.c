@@ -117,7 +117,7 @@ static void inverse_transform(const int16_t* d, int n, int flags, int c_idx, int
         return;
     }
     int use_dst = (flags & HEVC_TU_INTRA) && c_idx == 0 && n == 4;
-    static int B[32][32];
+    int B[32][32];   /* per call: the checkers run on several host threads at once */
     basis(n, use_dst, B);
     int16_t tmp[32 * 32];
     int s2 = 20 - bit_depth;

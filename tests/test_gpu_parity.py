@@ -102,6 +102,35 @@ def test_dpb_jobs_plain_and_batched(hb, gpu_ctx, port):
         assert _diff(st.download(2), wnt) == 0
 
 
+def test_frame_output_cropped_16bit(hb, gpu_ctx, port):
+    """hevcgpu_slot_download_frame gives the reconstructed picture inside the conformance
+    window as 16-bit planes, as hevc_decoder_get_frame does (hevc_api.cpp:49-77)."""
+    w, h, seed = 216, 136, 91
+    st = gpu_ctx.open_stream(w, h, 3)
+    refs = [hb.content(w, h, seed + 1), hb.content(w, h, seed + 2)]
+    st.upload(0, refs[0])
+    st.upload(1, refs[1])
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **cases.PICTURE))
+    want = hb.split_i420(port.reconstruct_picture(pic, refs), w, h)
+    job = st.prepare(pic)
+    job.launch(2)
+    st.sync()
+    for crop, strides in [(None, (None, None)), ((2, 6, 4, 8), (None, None)), ((8, 0, 0, 2), (240, 130)),
+                          ((0, 14, 6, 0), (202, 101))]:
+        l, r, t, b = crop or (0, 0, 0, 0)
+        got = st.download_frame(2, crop, *strides)
+        for p, (g, full) in enumerate(zip(got, want)):
+            sub = 2 if p else 1
+            exp = full[t // sub: (h - b) // sub, l // sub: (w - r) // sub].astype(np.uint16)
+            assert g.dtype == np.uint16 and g.shape == exp.shape, (crop, p)
+            assert _diff(g, exp) == 0, (crop, p)
+    for bad in [(1, 0, 0, 0), (0, 0, -2, 0), (108, 108, 0, 0), (0, 0, 70, 66)]:
+        with pytest.raises(hb.HevcGpuError) as e:
+            st.download_frame(2, bad)
+        assert e.value.code == hb.abi.HEVCGPU_EINVAL
+    job.free()
+
+
 def test_batched_prepare_and_download(hb, gpu_ctx, port):
     """hevcgpu_jobs_prepare + hevcgpu_batch_launch + hevcgpu_slots_download over streams
     of mixed sizes give the oracle's pictures into pageable and pinned host buffers; a

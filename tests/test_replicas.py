@@ -46,7 +46,7 @@ def _rank_main(rank, world, port, out):
         rate = bench.job_rate(16 * 10, world, slowest)
 
         class Args:
-            batch, steps, warmup, width, height, gpus = 2, 1, 0, 64, 64, world
+            batch, steps, warmup, width, height, gpus, streams, gop = 2, 1, 0, 64, 64, world, 2, 3
         ref_line = bench.run_reference(Args, hb, rank, world) if rank != 0 else "rank0"
         out.put((rank, digests, slowest, rate, ref_line))
     finally:
