@@ -548,10 +548,11 @@ enum StageMask : int {
 // the context), so that their memory is reused from one picture to the next: no allocation
 // and no first-touch page faults per picture.
 struct BuildScratch {
-    std::vector<int32_t> bins[4], intra_list, itu, level, ctu_of, order, owner[3];
-    // an owner map entry is valid when its stamp is this picture's generation, so the maps
-    // need no clearing between pictures
-    std::vector<uint32_t> owner_gen[3];
+    std::vector<int32_t> bins[4], intra_list, itu, level, ctu_of, order;
+    // intra owner maps, one word per 4x4 unit: (generation << 40) | (CTU address << 16) |
+    // level.  An entry is valid when its generation is this picture's, so the maps need no
+    // clearing between pictures.
+    std::vector<uint64_t> owner[3];
     uint32_t gen = 0;
     std::vector<hevc_tu_t> itu_rec;
     std::vector<int4> itu_res;
@@ -693,74 +694,79 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         // done); the dependency publishes after level need - 1
         auto& reqs = BS.reqs;
         reqs.clear();
-        // owner maps: (CTU address << 16) | level of the latest intra TU per 4x4 unit, valid
-        // where the unit's stamp is this picture's generation (else no owner)
+        // owner maps: the CTU address and level of the latest intra TU per 4x4 unit, in words
+        // tagged with this picture's generation (a word of another generation: no owner).  The
+        // address takes 24 bits (an 8192 x 8192 picture of 16 x 16 CTBs has 2^18 CTUs).
         auto& owner = BS.owner;
         int uw[3], uh[3];
-        if (++BS.gen == 0) {   // wrapped: every old stamp must differ from the new generation
-            for (auto& g : BS.owner_gen) std::fill(g.begin(), g.end(), 0u);
+        if (++BS.gen == (1u << 24)) {   // wrapped: no old word may carry the new generation
+            for (auto& m : owner) std::fill(m.begin(), m.end(), 0ull);
             BS.gen = 1;
         }
-        const uint32_t gen = BS.gen;
+        const uint64_t gtag = (uint64_t)BS.gen << 40;
+        constexpr uint64_t GEN_BITS = ~((1ull << 40) - 1);
         for (int c = 0; c < 3; c++) {
             uw[c] = (c ? W / 2 : W) / 4;
             uh[c] = (c ? H / 2 : H) / 4;
             const size_t nu = (size_t)uw[c] * uh[c];
-            if (owner[c].size() < nu) {
-                owner[c].resize(nu);
-                BS.owner_gen[c].resize(nu, 0u);
-            }
+            if (owner[c].size() < nu) owner[c].resize(nu, 0ull);
         }
+        reqs.reserve((size_t)n_intra);
         for (int b = 0; b < n_intra; b++) {
             const hevc_tu_t& t = s->tus[intra_list[(size_t)b]];
             const int c = t.c_idx, n = 1 << t.log2_size, sub = c ? 2 : 1;
             const int a = ((t.y * sub) >> p.log2_ctb) * wctb + ((t.x * sub) >> p.log2_ctb);
             ctu_of[(size_t)b] = a;
-            int32_t* own = owner[c].data();
-            uint32_t* own_gen = BS.owner_gen[c].data();
+            uint64_t* own = owner[c].data();
             const int row = uw[c];
-            const size_t r0 = reqs.size();
+            const bool up = t.y > 0, left = t.x > 0;
+            const size_t rrow = up ? (size_t)((t.y - 1) / 4) * row : 0;
+            const int ux0 = left ? (t.x - 1) / 4 : 0, ux1 = std::min(row - 1, (t.x + 2 * n - 1) / 4);
+            const int lx = left ? (t.x - 1) / 4 : 0;
+            const int uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
+            // First pass, with no branch on the owners: the level from the owners in this CTU,
+            // and whether a unit has an owner in another CTU.
+            const uint64_t self = gtag | ((uint64_t)a << 16);
+            constexpr uint64_t OWNER_BITS = ~0xFFFFull;   // generation and CTU address
             int lv = 0;
-            int32_t last = -1;   // a run of units with one owner adds what its first unit added
-            auto dep = [&](size_t u) {
-                const int32_t o = own_gen[u] == gen ? own[u] : -1;
-                if (o < 0 || o == last) return;
-                last = o;
-                const int oa = o >> 16, ol = o & 0xFFFF;
-                if (oa == a) {
-                    lv = std::max(lv, ol + 1);
-                    return;
-                }
-                int32_t* dl = &dep_list[(size_t)a * 4];
-                int32_t& dn = dep_n[(size_t)a];
-                bool have = false;
-                for (int q = 0; q < std::min<int32_t>(dn, 4); q++) have |= dl[q] == oa;
-                if (!have) {
-                    if (dn < 4) dl[dn] = oa;
-                    dn++;
-                }
-                reqs.push_back({a, 0, oa, ol + 1});
+            bool other = false;
+            auto scan = [&](uint64_t o) {
+                const bool same = (o & OWNER_BITS) == self;
+                lv = std::max(lv, same ? (int)(o & 0xFFFF) + 1 : 0);
+                other |= ((o & GEN_BITS) == gtag) & !same;
             };
-            if (t.y > 0) {
-                const size_t r = (size_t)((t.y - 1) / 4) * row;
-                const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(row - 1, (t.x + 2 * n - 1) / 4);
-                for (int ux = ux0; ux <= ux1; ux++) dep(r + ux);
-            }
-            if (t.x > 0) {
-                const int ux = (t.x - 1) / 4;
-                const int uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
-                for (int uy = uy0; uy <= uy1; uy++) dep((size_t)uy * row + ux);
-            }
+            if (up)
+                for (int ux = ux0; ux <= ux1; ux++) scan(own[rrow + ux]);
+            if (left)
+                for (int uy = uy0; uy <= uy1; uy++) scan(own[(size_t)uy * row + lx]);
             if (lv > 0xFFFF) return fail(HEVCGPU_EINVAL, "intra dependency chain too deep in CTU %d", a);
             level[(size_t)b] = lv;
-            for (size_t q = r0; q < reqs.size(); q++) reqs[q].lv = lv;
-            const int32_t mark = (a << 16) | lv;
+            if (other) {   // second pass, the same units in the same order: the other CTUs
+                uint64_t last = 0;   // a run of units with one owner adds what its first unit added
+                auto dep = [&](uint64_t o) {
+                    if ((o & GEN_BITS) != gtag || o == last) return;
+                    last = o;
+                    if ((o & OWNER_BITS) == self) return;
+                    const int oa = (int)((o >> 16) & 0xFFFFFF), ol = (int)(o & 0xFFFF);
+                    int32_t* dl = &dep_list[(size_t)a * 4];
+                    int32_t& dn = dep_n[(size_t)a];
+                    bool have = false;
+                    for (int q = 0; q < std::min<int32_t>(dn, 4); q++) have |= dl[q] == oa;
+                    if (!have) {
+                        if (dn < 4) dl[dn] = oa;
+                        dn++;
+                    }
+                    reqs.push_back({a, lv, oa, ol + 1});
+                };
+                if (up)
+                    for (int ux = ux0; ux <= ux1; ux++) dep(own[rrow + ux]);
+                if (left)
+                    for (int uy = uy0; uy <= uy1; uy++) dep(own[(size_t)uy * row + lx]);
+            }
+            const uint64_t mark = gtag | ((uint64_t)a << 16) | (uint64_t)lv;
             for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++) {
-                const size_t r = (size_t)uy * row;
-                for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) {
-                    own[r + ux] = mark;
-                    own_gen[r + ux] = gen;
-                }
+                uint64_t* r = own + (size_t)uy * row;
+                for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) r[ux] = mark;
             }
         }
         for (int a = 0; a < nctb; a++)
