@@ -19,13 +19,14 @@ value      frames/s over the whole job with the records already in HBM: K GOPs, 
            over ranks).  "plain" is one launch per stage per picture on the same GOPs.
 frame_ms   device time of each GOP position's batch (all its pictures complete with it),
            p50 and p99 over the timed batches; i_frame_ms / pb_frame_ms split it by kind.
-e2e        frames/s through the C ABI from host memory: per pair of GOP positions the 16
+e2e        frames/s through the C ABI from host memory: per group of 4 GOP positions the 32
            pictures' records, kept in page-locked host memory (hevcgpu_host_alloc, as a
            recorder writing there would), are copied host->device with the work lists the
-           library's host workers derive from them (hevcgpu_jobs_prepare); the two batches are
-           launched in order on the streams' lane and every reconstructed picture is copied
-           device->host into pinned frame buffers (hevcgpu_lane_slots_download_async, waited
-           for with hevcgpu_lane_wait before the buffers are reused and at the end).
+           library's host workers derive from them (hevcgpu_jobs_prepare_async: the copies
+           overlap the next group's building); the four batches are launched in order on the
+           streams' lane and every reconstructed picture is copied device->host into pinned
+           frame buffers (hevcgpu_lane_slots_download_async, waited for with hevcgpu_lane_wait
+           before the buffers are reused and at the end).
 stages     per-stage device times over one GOP from CUDA events recorded around each stage
            on the library's stream, in a separate pass (the timed region carries no extra
            events); the roofline is that of the dominant stage.
@@ -534,13 +535,14 @@ def run_ours(args, hb, rank, world, local):
     traffic = (ncu_dram_gop8[dom] if dom in ncu_dram_gop8 and (W, H, G, F) == (W_DEFAULT, H_DEFAULT, 8, 60)
                else None)
 
-    # end to end through the C ABI from host memory: pairs of GOP positions, the 2G
-    # pictures prepared together on the host workers, the two batches launched in decode
-    # order on the streams' lane with their frame copies queued behind them
+    # end to end through the C ABI from host memory: groups of E2E_POS GOP positions, their
+    # pictures prepared together on the host workers, the batches launched in decode order
+    # on the streams' lane with their frame copies queued behind them
+    E2E_POS = 4
     lane = hb.Lane(ctx)
     frame_bytes = hb.i420_size(W, H)
     out_host = [[[torch.empty(frame_bytes, dtype=torch.uint8).pin_memory().numpy() for _ in range(G)]
-                 for _ in range(2)] for _ in range(2)]
+                 for _ in range(E2E_POS)] for _ in range(2)]
     for s in gop:   # records in page-locked memory (set up outside the timing)
         for pic in [s[0]] + s[1]:
             pic.pin()
@@ -549,16 +551,16 @@ def run_ours(args, hb, rank, world, local):
     def e2e_gop():
         tickets, held = [None, None], [[], []]
         h2d = 0
-        for n0 in range(0, F, 2):
-            i = (n0 // 2) % 2
+        for n0 in range(0, F, E2E_POS):
+            i = (n0 // E2E_POS) % 2
             if tickets[i] is not None:
                 for t in tickets[i]:
                     lane.wait(t)
                 for j in held[i]:
                     j.free()
-            ns = [n for n in (n0, n0 + 1) if n < F]
+            ns = [n for n in range(n0, n0 + E2E_POS) if n < F]
             pics = [gop_picture(s, n) for n in ns for s in gop]
-            js = hb.prepare_batch(gop_streams * len(ns), pics)
+            js = hb.prepare_batch(gop_streams * len(ns), pics, wait_uploads=False)
             h2d += sum(j.upload_bytes for j in js)
             tickets[i] = []
             for q, n in enumerate(ns):
@@ -727,7 +729,7 @@ def run_pb16(args, hb, ctx, stream, rank, world, dev, check, rank_max, barrier):
                 lanes[i].wait(tickets[i])
                 for j in held[i]:
                     j.free()
-            js = hb.prepare_batch(grp_streams[i], grp_pics[i])
+            js = hb.prepare_batch(grp_streams[i], grp_pics[i], wait_uploads=False)
             lanes[i].batch_launch(js, slots)
             tickets[i] = lanes[i].download_batch_async(grp_streams[i], slots, out_host[i])
             held[i] = js

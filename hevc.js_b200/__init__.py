@@ -252,6 +252,7 @@ def gpu_lib():
             "hevcgpu_slot_device_ptr": ([P, C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P),
                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
             "hevcgpu_job_prepare": ([P, C.POINTER(PictureSyntax), C.POINTER(P)], C.c_int),
+            "hevcgpu_job_wait_uploaded": ([P], C.c_int),
             "hevcgpu_job_free": ([P], None),
             "hevcgpu_job_upload_bytes": ([P], C.c_uint64),
             "hevcgpu_host_alloc": ([C.c_size_t, C.POINTER(P)], C.c_int),
@@ -260,6 +261,7 @@ def gpu_lib():
             "hevcgpu_batch_launch": ([C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
             "hevcgpu_stream_sync": ([P], C.c_int),
             "hevcgpu_jobs_prepare": ([C.POINTER(P), C.POINTER(P), C.c_int32, C.POINTER(P)], C.c_int),
+            "hevcgpu_jobs_prepare_async": ([C.POINTER(P), C.POINTER(P), C.c_int32, C.POINTER(P)], C.c_int),
             "hevcgpu_lane_open": ([P, C.POINTER(P)], C.c_int),
             "hevcgpu_lane_close": ([P], None),
             "hevcgpu_lane_batch_launch": ([P, C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
@@ -454,6 +456,10 @@ class Job:
         self.h = handle
         stream.ctx._children.add(self)
 
+    def wait_uploaded(self):
+        """Returns once the copies of the picture's page-locked record arrays have read them."""
+        _check(self.lib.hevcgpu_job_wait_uploaded(self.h))
+
     def launch(self, dst_slot):
         _check(self.lib.hevcgpu_job_launch(self.h, dst_slot))
 
@@ -542,15 +548,18 @@ class Lane:
             pass
 
 
-def prepare_batch(streams, pics):
+def prepare_batch(streams, pics, wait_uploads=True):
     """Jobs for pics[i] on streams[i], built on the context's host workers
-    (hevcgpu_jobs_prepare)."""
+    (hevcgpu_jobs_prepare).  wait_uploads=False: hevcgpu_jobs_prepare_async, which returns
+    with the copies of page-locked record arrays still in flight (Job.wait_uploaded before
+    writing into them)."""
     lib = gpu_lib()
     n = len(pics)
     sts = (C.c_void_p * n)(*[st.h for st in streams])
     syns = (C.c_void_p * n)(*[C.cast(p.syn_ptr, C.c_void_p) for p in pics])
     out = (C.c_void_p * n)()
-    _check(lib.hevcgpu_jobs_prepare(sts, syns, n, out))
+    f = lib.hevcgpu_jobs_prepare if wait_uploads else lib.hevcgpu_jobs_prepare_async
+    _check(f(sts, syns, n, out))
     return [Job(st, None, C.c_void_p(h)) for st, h in zip(streams, out)]
 
 

@@ -335,6 +335,10 @@ struct hevcgpu_lane {
     cudaEvent_t done[hevcgpu_ctx::EVENT_RING] = {};   // batch completion events, used in turn
     int done_next = 0;
     cudaEvent_t ctx_ready = nullptr;   // the context stream's work before a batch
+    // Asynchronous downloads run on a stream of their own after the lane's work queued
+    // before them (src_ready), so the lane's next batches do not queue behind the copies.
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t src_ready = nullptr;
     // Asynchronous downloads: download k (k = 1, 2, ...) records dl_done[k % EVENT_RING]
     // after its copies; a later download reuses the slot, whose event then completes later,
     // so waiting on it still waits for download k.
@@ -350,9 +354,12 @@ struct hevcgpu_lane {
         if (flow) cudaFree(flow);
         for (auto e : done)
             if (e) cudaEventDestroy(e);
+        if (cstream) cudaStreamSynchronize(cstream);
         for (auto e : dl_done)
             if (e) cudaEventDestroy(e);
         if (ctx_ready) cudaEventDestroy(ctx_ready);
+        if (src_ready) cudaEventDestroy(src_ready);
+        if (cstream) cudaStreamDestroy(cstream);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -361,6 +368,22 @@ struct hevcgpu_stream {
     hevcgpu_ctx* ctx = nullptr;
     Layout lay;
     std::vector<DevBuf> slots;
+    // Per slot: an event recorded on a lane's copy stream after the last asynchronous
+    // download of the slot (or null); a launch or upload that writes the slot first waits
+    // for it on the device.
+    std::vector<cudaEvent_t> slot_read;
+    ~hevcgpu_stream() {
+        for (cudaEvent_t e : slot_read)
+            if (e) {
+                cudaEventSynchronize(e);   // no copy may still read a slot being released
+                cudaEventDestroy(e);
+            }
+    }
+    // Orders `stream` after the downloads still reading slot k.
+    int wait_slot_read(int k, cudaStream_t stream) {
+        if (k < 0 || k >= (int)slot_read.size() || !slot_read[(size_t)k]) return HEVCGPU_OK;
+        return cudaStreamWaitEvent(stream, slot_read[(size_t)k], 0) == cudaSuccess ? HEVCGPU_OK : HEVCGPU_ECUDA;
+    }
 };
 
 // ---------------------------------------------------------------------------------------
@@ -569,7 +592,7 @@ struct BuildScratch {
 };
 thread_local BuildScratch t_build;
 
-int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
+int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool wait_uploads = true) {
     BuildScratch& BS = t_build;
     hevcgpu_ctx* ctx = j->ctx;
     const hevc_pic_params_t& p = s->params;
@@ -1063,8 +1086,9 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages) {
         j->n_mc[c] = (int32_t)mc[c].size();
         j->d_mc[c] = reinterpret_cast<const uint32_t*>(base + o_mc[c]);
     }
-    // the caller may change its arrays once this returns: the direct uploads must have read them
-    if (any_direct) CUDA_TRY(cudaEventSynchronize(j->direct_read));
+    // the caller may change its arrays once this returns: the direct uploads must have read
+    // them, unless the caller waits for that itself (hevcgpu_job_wait_uploaded)
+    if (any_direct && wait_uploads) CUDA_TRY(cudaEventSynchronize(j->direct_read));
     return HEVCGPU_OK;
 }
 
@@ -1281,26 +1305,39 @@ int run_stages(hevcgpu_ctx* ctx, hevcgpu_job* const* jobs, int n, int stages, in
     return run_stages(ctx, Exec{ctx->stream, ctx->flow}, jobs, n, stages, res_mode);
 }
 
-int upload_i420(hevcgpu_ctx* ctx, const Layout& L, uint8_t* dev, const uint8_t* host) {
+// Copies between a pitched slot and a packed I420 host frame.  When the pitches equal the
+// plane widths (widths that are multiples of 128) the slot is the packed frame itself and
+// one linear copy moves it: the DMA engines run 2-D copies of many short rows well below
+// the rate of a linear copy.
+bool packed_layout(const Layout& L) {
+    return L.pitch_y == L.W && L.pitch_c == L.W / 2 && L.off_cb == (int64_t)L.W * L.H &&
+           L.off_cr == L.off_cb + (int64_t)(L.W / 2) * (L.H / 2);
+}
+
+int copy_i420(const Layout& L, uint8_t* dev, uint8_t* host, cudaMemcpyKind kind, cudaStream_t stream) {
     const int W = L.W, H = L.H, cw = W / 2, ch = H / 2;
-    CUDA_TRY(cudaMemcpy2DAsync(dev, L.pitch_y, host, W, W, H, cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(cudaMemcpy2DAsync(dev + L.off_cb, L.pitch_c, host + (size_t)W * H, cw, cw, ch, cudaMemcpyHostToDevice,
-                               ctx->stream));
-    CUDA_TRY(cudaMemcpy2DAsync(dev + L.off_cr, L.pitch_c, host + (size_t)W * H + (size_t)cw * ch, cw, cw, ch,
-                               cudaMemcpyHostToDevice, ctx->stream));
+    const bool up = kind == cudaMemcpyHostToDevice;
+    if (packed_layout(L)) {
+        const size_t n = (size_t)W * H + 2 * (size_t)cw * ch;
+        CUDA_TRY(up ? cudaMemcpyAsync(dev, host, n, kind, stream) : cudaMemcpyAsync(host, dev, n, kind, stream));
+        return HEVCGPU_OK;
+    }
+    uint8_t* d[3] = {dev, dev + L.off_cb, dev + L.off_cr};
+    uint8_t* h[3] = {host, host + (size_t)W * H, host + (size_t)W * H + (size_t)cw * ch};
+    const int w[3] = {W, cw, cw}, rows[3] = {H, ch, ch}, pitch[3] = {L.pitch_y, L.pitch_c, L.pitch_c};
+    for (int p = 0; p < 3; p++)
+        CUDA_TRY(up ? cudaMemcpy2DAsync(d[p], pitch[p], h[p], w[p], w[p], rows[p], kind, stream)
+                    : cudaMemcpy2DAsync(h[p], w[p], d[p], pitch[p], w[p], rows[p], kind, stream));
     return HEVCGPU_OK;
+}
+
+int upload_i420(hevcgpu_ctx* ctx, const Layout& L, uint8_t* dev, const uint8_t* host) {
+    return copy_i420(L, dev, const_cast<uint8_t*>(host), cudaMemcpyHostToDevice, ctx->stream);
 }
 
 int download_i420(hevcgpu_ctx* ctx, const Layout& L, const uint8_t* dev, uint8_t* host,
                   cudaStream_t stream = nullptr) {
-    const int W = L.W, H = L.H, cw = W / 2, ch = H / 2;
-    if (!stream) stream = ctx->stream;
-    CUDA_TRY(cudaMemcpy2DAsync(host, W, dev, L.pitch_y, W, H, cudaMemcpyDeviceToHost, stream));
-    CUDA_TRY(cudaMemcpy2DAsync(host + (size_t)W * H, cw, dev + L.off_cb, L.pitch_c, cw, ch, cudaMemcpyDeviceToHost,
-                               stream));
-    CUDA_TRY(cudaMemcpy2DAsync(host + (size_t)W * H + (size_t)cw * ch, cw, dev + L.off_cr, L.pitch_c, cw, ch,
-                               cudaMemcpyDeviceToHost, stream));
-    return HEVCGPU_OK;
+    return copy_i420(L, const_cast<uint8_t*>(dev), host, cudaMemcpyDeviceToHost, stream ? stream : ctx->stream);
 }
 
 int check_ctx(hevcgpu_ctx* ctx) {
@@ -1692,7 +1729,9 @@ void hevcgpu_stream_close(hevcgpu_stream_t* st) {
 
 int hevcgpu_slot_upload(hevcgpu_stream_t* st, int32_t slot, const uint8_t* i420) {
     if (!st || !i420 || slot < 0 || slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);
-    int rc = upload_i420(st->ctx, st->lay, static_cast<uint8_t*>(st->slots[(size_t)slot].p), i420);
+    int rc = st->wait_slot_read(slot, st->ctx->stream);
+    if (rc) return fail(rc, "waiting for the downloads of slot %d", slot);
+    rc = upload_i420(st->ctx, st->lay, static_cast<uint8_t*>(st->slots[(size_t)slot].p), i420);
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(st->ctx->stream));
     return HEVCGPU_OK;
@@ -1763,7 +1802,8 @@ int hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void**
     return HEVCGPU_OK;
 }
 
-int hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, hevcgpu_job_t** out) {
+namespace {
+int job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, hevcgpu_job_t** out, bool wait_uploads) {
     if (!st || !out) return fail(HEVCGPU_EINVAL, "null arguments");
     *out = nullptr;
     int rc = check_ctx(st->ctx);
@@ -1782,7 +1822,7 @@ int hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, 
     if (!j) return fail(HEVCGPU_ENOMEM, "host allocation");
     j->ctx = st->ctx;
     j->st = st;
-    if ((rc = job_build(j, syn, ST_ALL)) || (rc = j->rec.get(st->ctx, (size_t)j->lay.bytes))) {
+    if ((rc = job_build(j, syn, ST_ALL, wait_uploads)) || (rc = j->rec.get(st->ctx, (size_t)j->lay.bytes))) {
         delete j;
         return rc;
     }
@@ -1792,6 +1832,17 @@ int hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, 
         j->registered = true;
     }
     *out = j;
+    return HEVCGPU_OK;
+}
+}  // namespace
+
+int hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, hevcgpu_job_t** out) {
+    return job_prepare(st, syn, out, true);
+}
+
+int hevcgpu_job_wait_uploaded(hevcgpu_job_t* job) {
+    if (!job) return fail(HEVCGPU_EINVAL, "null job");
+    if (job->direct_read) CUDA_TRY(cudaEventSynchronize(job->direct_read));
     return HEVCGPU_OK;
 }
 
@@ -1892,8 +1943,11 @@ int launch_batch(hevcgpu_ctx* ctx, const Exec& ex, cudaEvent_t done, hevcgpu_job
                  const int32_t* dst_slots, int n) {
     int rc = order_jobs(jobs, n, ex.stream);
     if (rc) return rc;
-    for (int k = 0; k < n; k++)
+    for (int k = 0; k < n; k++) {
+        if (jobs[k]->st && (rc = jobs[k]->st->wait_slot_read(dst_slots[k], ex.stream)))
+            return fail(rc, "waiting for the downloads of slot %d", dst_slots[k]);
         if ((rc = job_target(jobs[k], dst_slots[k], ex.stream))) return rc;
+    }
     if ((rc = run_stages(ctx, ex, jobs, n, ST_ALL, RES_PICTURE))) return rc;
     return mark_jobs(jobs, n, ex.stream, done);
 }
@@ -1928,6 +1982,8 @@ int hevcgpu_lane_open(hevcgpu_ctx_t* ctx, hevcgpu_lane_t** out) {
     for (int k = 0; k < hevcgpu_ctx::EVENT_RING && e == cudaSuccess; k++)
         e = cudaEventCreateWithFlags(&ln->done[k], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ln->ctx_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ln->cstream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ln->src_ready, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         cudaGetLastError();
         delete ln;
@@ -1941,6 +1997,7 @@ void hevcgpu_lane_close(hevcgpu_lane_t* lane) {
     if (!lane) return;
     cudaSetDevice(lane->ctx->device);
     cudaStreamSynchronize(lane->stream);
+    cudaStreamSynchronize(lane->cstream);
     {   // jobs last launched on this lane forget it: its work is done
         std::lock_guard<std::mutex> g(lane->ctx->jobs_mu);
         for (hevcgpu_job* j : lane->ctx->live_jobs)
@@ -1968,13 +2025,15 @@ int hevcgpu_lane_batch_launch(hevcgpu_lane_t* lane, hevcgpu_job_t* const* jobs, 
 int hevcgpu_lane_sync(hevcgpu_lane_t* lane) {
     if (!lane) return fail(HEVCGPU_EINVAL, "null lane");
     CUDA_TRY(cudaStreamSynchronize(lane->stream));
+    CUDA_TRY(cudaStreamSynchronize(lane->cstream));
     return hevcgpu_ctx::take_status_of(lane->flow);
 }
 
 void* hevcgpu_lane_cuda_stream(hevcgpu_lane_t* lane) { return lane ? (void*)lane->stream : nullptr; }
 
-int hevcgpu_jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns, int32_t n,
-                         hevcgpu_job_t** out) {
+namespace {
+int jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns, int32_t n,
+                 hevcgpu_job_t** out, bool wait_uploads) {
     if (n < 0 || (n && (!sts || !syns || !out))) return fail(HEVCGPU_EINVAL, "null arrays");
     if (n == 0) return HEVCGPU_OK;
     for (int i = 0; i < n; i++) {
@@ -1991,7 +2050,7 @@ int hevcgpu_jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax
         std::lock_guard<std::mutex> g(ctx->pool.run_mu);
         ctx->pool.ensure(ctx->device);
         ctx->pool.run(n, [&](int i) {
-            rcs[(size_t)i] = hevcgpu_job_prepare(sts[i], syns[i], &out[i]);
+            rcs[(size_t)i] = job_prepare(sts[i], syns[i], &out[i], wait_uploads);
             if (rcs[(size_t)i]) msgs[(size_t)i] = g_err;
         });
     }
@@ -2004,6 +2063,17 @@ int hevcgpu_jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax
         return fail(rcs[(size_t)i], "picture %d: %s", i, msgs[(size_t)i].c_str());
     }
     return HEVCGPU_OK;
+}
+}  // namespace
+
+int hevcgpu_jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns, int32_t n,
+                         hevcgpu_job_t** out) {
+    return jobs_prepare(sts, syns, n, out, true);
+}
+
+int hevcgpu_jobs_prepare_async(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns, int32_t n,
+                               hevcgpu_job_t** out) {
+    return jobs_prepare(sts, syns, n, out, false);
 }
 
 }  // extern "C"
@@ -2099,14 +2169,24 @@ int hevcgpu_lane_slots_download_async(hevcgpu_lane_t* lane, hevcgpu_stream_t* co
     }
     int rc = check_ctx(lane->ctx);
     if (rc) return rc;
+    // the copies follow the lane's work queued so far, on the lane's copy stream
+    CUDA_TRY(cudaEventRecord(lane->src_ready, lane->stream));
+    CUDA_TRY(cudaStreamWaitEvent(lane->cstream, lane->src_ready, 0));
     for (int i = 0; i < n; i++)
         if ((rc = download_i420(lane->ctx, sts[i]->lay, static_cast<uint8_t*>(sts[i]->slots[(size_t)slots[i]].p),
-                                outs[i], lane->stream)))
+                                outs[i], lane->cstream)))
             return rc;
+    for (int i = 0; i < n; i++) {   // later writes of these slots wait for the copies
+        hevcgpu_stream* st = sts[i];
+        if (st->slot_read.size() < st->slots.size()) st->slot_read.resize(st->slots.size(), nullptr);
+        cudaEvent_t& r = st->slot_read[(size_t)slots[i]];
+        if (!r) CUDA_TRY(cudaEventCreateWithFlags(&r, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventRecord(r, lane->cstream));
+    }
     const uint64_t t = lane->dl_seq + 1;
     cudaEvent_t& e = lane->dl_done[t % hevcgpu_ctx::EVENT_RING];
     if (!e) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    CUDA_TRY(cudaEventRecord(e, lane->stream));
+    CUDA_TRY(cudaEventRecord(e, lane->cstream));
     lane->dl_seq = t;
     *ticket = t;
     return HEVCGPU_OK;

@@ -310,10 +310,12 @@ void* hevcgpu_lane_cuda_stream(hevcgpu_lane_t* lane);
  * Returns the lane's device status, like hevcgpu_lane_sync. */
 int   hevcgpu_lane_slots_download(hevcgpu_lane_t* lane, hevcgpu_stream_t* const* sts,
                                   const int32_t* slots, int32_t n, uint8_t* const* outs);
-/* The same copies, queued on the lane after its batches, without waiting: every
- * destination must be page-locked host memory (cudaHostAlloc / cudaHostRegister), which
- * the copies write directly.  *ticket identifies the download; the frames are complete
- * once hevcgpu_lane_wait(lane, ticket) has returned (or after hevcgpu_lane_sync).  A
+/* The same copies without waiting: they run on the lane's own copy stream after the work
+ * queued on the lane so far, so the lane's next batches do not wait for them; a later
+ * launch or upload that writes one of these slots waits for their copies on the device.
+ * Every destination must be page-locked host memory (cudaHostAlloc / cudaHostRegister),
+ * which the copies write directly.  *ticket identifies the download; the frames are
+ * complete once hevcgpu_lane_wait(lane, ticket) has returned (or after hevcgpu_lane_sync).  A
  * decoder pipeline overlaps the copies of one batch with the preparation of the next
  * (the reference hands each frame out synchronously: hevc_decoder_get_frame,
  * wasm/hevc_api.h:63). */
@@ -340,6 +342,18 @@ int   hevcgpu_lane_wait(hevcgpu_lane_t* lane, uint64_t ticket);
  * wasm/hevc_api.cpp:49), as packed I420 host frames. */
 int  hevcgpu_jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns,
                           int32_t n, hevcgpu_job_t** out);
+
+/* hevcgpu_jobs_prepare without waiting for the copies of the caller's page-locked arrays:
+ * it returns once the jobs are built, with those copies still in flight (arrays in
+ * pageable memory were copied to staging, so they may change at once).  Before it writes
+ * into a page-locked array of a picture again, the caller waits for that picture's job
+ * with hevcgpu_job_wait_uploaded; launching, downloading and freeing the jobs need no
+ * wait.  A recorder that fills several page-locked record buffers in turn uses this to
+ * overlap a batch's transfer with the building of the next. */
+int  hevcgpu_jobs_prepare_async(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns,
+                                int32_t n, hevcgpu_job_t** out);
+/* Returns once the copies of a job's page-locked record arrays have read them. */
+int  hevcgpu_job_wait_uploaded(hevcgpu_job_t* job);
 int  hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n,
                             uint8_t* const* outs);
 /* CUDA stream (cudaStream_t) the context launches on. */

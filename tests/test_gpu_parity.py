@@ -102,6 +102,84 @@ def test_dpb_jobs_plain_and_batched(hb, gpu_ctx, port):
         assert _diff(st.download(2), wnt) == 0
 
 
+def test_gop_through_a_lane_with_pending_downloads(hb, gpu_ctx, port):
+    """A GOP (an I picture, then P/B pictures predicted from the two before them, over a
+    ring of 3 DPB slots) through one lane, prepared from host records two positions at a
+    time as the bench's end-to-end loop does, every picture downloaded asynchronously and
+    nothing waited for until the end: picture n + 3 rewrites the slot whose download of
+    picture n may still be pending, so it must wait for those copies on the device."""
+    import torch
+    import bench
+    w, h, g, frames = 416, 240, 2, 7
+    gop = bench.make_gop(hb, g, w, h, 4242)
+    sts = []
+    for s in gop:
+        st = gpu_ctx.open_stream(w, h, 3)
+        for k in range(3):
+            st.upload(k, s[2][k])
+        sts.append(st)
+    want = []
+    for s in gop:   # the oracle's chain
+        dpb, outs = list(s[2]), []
+        for n in range(frames):
+            dpb[n % 3] = port.reconstruct_picture(bench.gop_picture(s, n), dpb)
+            outs.append(dpb[n % 3])
+        want.append(outs)
+    lane = hb.Lane(gpu_ctx)
+    size = hb.i420_size(w, h)
+    got = [[torch.empty(size, dtype=torch.uint8).pin_memory().numpy() for _ in range(g)] for _ in range(frames)]
+    for s in gop:   # page-locked records, prepared without waiting for their copies
+        for pic in [s[0]] + s[1]:
+            pic.pin()
+    tickets, jobs = [], []
+    for n0 in range(0, frames, 2):
+        ns = [n for n in (n0, n0 + 1) if n < frames]
+        js = hb.prepare_batch(sts * len(ns), [bench.gop_picture(s, n) for n in ns for s in gop], wait_uploads=False)
+        for q, n in enumerate(ns):
+            lane.batch_launch(js[q * g:(q + 1) * g], [n % 3] * g)
+            tickets.append(lane.download_batch_async(sts, [n % 3] * g, got[n]))
+        jobs += js
+    for t in tickets:
+        lane.wait(t)
+    for n in range(frames):
+        for i in range(g):
+            assert _diff(got[n][i], want[i][n]) == 0, (n, i)
+    for j in jobs:
+        j.free()
+    lane.close()
+
+
+def test_prepare_async_then_overwrite_the_records(hb, gpu_ctx, port):
+    """hevcgpu_jobs_prepare_async + hevcgpu_job_wait_uploaded: once the wait returns, the
+    caller may overwrite its page-locked record arrays; the job keeps the picture it was
+    prepared from."""
+    w, h = 320, 192
+    streams, pics, want = [], [], []
+    for seed in (95, 96):
+        st = gpu_ctx.open_stream(w, h, 3)
+        refs = [hb.content(w, h, seed + 1), hb.content(w, h, seed + 2)]
+        st.upload(0, refs[0])
+        st.upload(1, refs[1])
+        pic = hb.Picture(hb.default_cfg(w, h, seed, **cases.PICTURE))
+        want.append(port.reconstruct_picture(pic, refs))
+        pic.pin()
+        streams.append(st)
+        pics.append(pic)
+    jobs = hb.prepare_batch(streams, pics, wait_uploads=False)
+    for j, pic in zip(jobs, pics):
+        j.wait_uploaded()
+        s = pic.syn
+        np.ctypeslib.as_array(s.coeffs, (s.num_coeffs,))[:] = 0   # the recorder reuses its buffers
+        for k in range(s.num_pus):
+            s.pus[k].mv[0][0] += 64
+    hb.batch_launch(jobs, [2, 2])
+    gpu_ctx.sync()
+    for st, wnt in zip(streams, want):
+        assert _diff(st.download(2), wnt) == 0
+    for j in jobs:
+        j.free()
+
+
 def test_frame_output_cropped_16bit(hb, gpu_ctx, port):
     """hevcgpu_slot_download_frame gives the reconstructed picture inside the conformance
     window as 16-bit planes, as hevc_decoder_get_frame does (hevc_api.cpp:49-77)."""
