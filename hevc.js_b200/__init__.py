@@ -253,6 +253,7 @@ def gpu_lib():
                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
             "hevcgpu_job_prepare": ([P, C.POINTER(PictureSyntax), C.POINTER(P)], C.c_int),
             "hevcgpu_job_wait_uploaded": ([P], C.c_int),
+            "hevcgpu_job_plant_unmet_wait": ([P], C.c_int),
             "hevcgpu_job_free": ([P], None),
             "hevcgpu_job_upload_bytes": ([P], C.c_uint64),
             "hevcgpu_host_alloc": ([C.c_size_t, C.POINTER(P)], C.c_int),
@@ -455,6 +456,11 @@ class Job:
             _check(self.lib.hevcgpu_job_prepare(stream.h, pic.syn_ptr, C.byref(handle)))
         self.h = handle
         stream.ctx._children.add(self)
+
+    def plant_unmet_wait(self):
+        """Test hook: the job's next launch times out in its intra stage (HEVCGPU_ETIMEOUT
+        at the next sync); hevcgpu_job_plant_unmet_wait."""
+        _check(self.lib.hevcgpu_job_plant_unmet_wait(self.h))
 
     def wait_uploaded(self):
         """Returns once the copies of the picture's page-locked record arrays have read them."""

@@ -1840,6 +1840,26 @@ int hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, 
     return job_prepare(st, syn, out, true);
 }
 
+int hevcgpu_job_plant_unmet_wait(hevcgpu_job_t* job) {
+    if (!job) return fail(HEVCGPU_EINVAL, "null job");
+    if (job->n_ictu <= 0) return fail(HEVCGPU_EINVAL, "the job has no intra CTU to plant a wait in");
+    int rc = check_ctx(job->ctx);
+    if (rc) return rc;
+    // The first intra CTU depends on no other.  It now names itself in dependency slot 0 and
+    // needs one completed level of it before its first level: a level only it could publish.
+    const PicDesc& D = job->host_desc;
+    cudaStream_t s = job->ctx->stream;
+    IntraLevel e{};
+    const int32_t self = 0;
+    CUDA_TRY(cudaMemcpyAsync(&e, D.ictu_lvl, sizeof(e), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    e.x = (e.x & ~0x3FFu) | 1u;
+    CUDA_TRY(cudaMemcpyAsync(const_cast<int32_t*>(D.ictu_deps), &self, sizeof(self), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(const_cast<IntraLevel*>(D.ictu_lvl), &e, sizeof(e), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaStreamSynchronize(s));   // the copies read e and self before they go
+    return HEVCGPU_OK;
+}
+
 int hevcgpu_job_wait_uploaded(hevcgpu_job_t* job) {
     if (!job) return fail(HEVCGPU_EINVAL, "null job");
     if (job->direct_read) CUDA_TRY(cudaEventSynchronize(job->direct_read));

@@ -11,8 +11,9 @@
 // residuals in shared memory, and runs the TUs level by level, one warp per TU; before a
 // level that reads samples of those CTUs it waits (bounded) until they have completed
 // the levels that write them, and reads such samples from the picture through L2.
-// Every wait gives up after SPIN_LIMIT polls, sets ST_TIMEOUT in the context's sticky
-// status word (the host turns it into HEVCGPU_ETIMEOUT) and returns.
+// Every wait gives up after WAIT_LIMIT_NS of the GPU's global timer (or SPIN_LIMIT polls,
+// should the timer not advance), sets ST_TIMEOUT in the context's sticky status word (the
+// host turns it into HEVCGPU_ETIMEOUT) and returns.
 #pragma once
 
 #include <cuda/atomic>
@@ -335,7 +336,14 @@ constexpr int IC_LP = 64, IC_LH = 64;                // luma tile (the CTU): pit
 constexpr int IC_CP = 32, IC_CH = 32;                // chroma tiles
 constexpr int IC_MAX_TUS = 256 + 2 * 64;             // 4x4 TUs of a 64x64 CTU, all planes
 constexpr int IC_MAX_RES = 64 * 64 + 2 * 32 * 32;    // residual samples of a 64x64 CTU
-constexpr long long SPIN_LIMIT = 1ll << 24;          // polls of ~64 ns: about a second
+constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;   // a wait gives up after a second
+constexpr unsigned SPIN_LIMIT = 1u << 26;            // backstop: polls of at least 64 ns
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // 16-byte asynchronous global -> shared copy (through L2 only, so that samples other
 // CTUs wrote are seen), and the wait for all of a thread's copies.
@@ -464,13 +472,17 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
                 const int need = intra_req(info, tid);
                 if (need > s_seen[tid]) {
                     cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[dep]);
-                    long long polls = 0;
+                    unsigned long long t0 = 0;
                     int v;
-                    while ((v = done.load(cuda::memory_order_acquire)) < (stamp | need)) {
-                        if (++polls > SPIN_LIMIT) {
-                            atomicOr(sticky, ST_TIMEOUT);
-                            s_abort = 1;
-                            break;
+                    for (unsigned polls = 0; (v = done.load(cuda::memory_order_acquire)) < (stamp | need); polls++) {
+                        if ((polls & 255u) == 0) {   // the timer, every 256 polls
+                            const unsigned long long now = global_ns();
+                            if (polls == 0) t0 = now;
+                            if (now - t0 > WAIT_LIMIT_NS || polls >= SPIN_LIMIT) {
+                                atomicOr(sticky, ST_TIMEOUT);
+                                s_abort = 1;
+                                break;
+                            }
                         }
                         __nanosleep(32);
                     }

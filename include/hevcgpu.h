@@ -354,6 +354,14 @@ int  hevcgpu_jobs_prepare_async(hevcgpu_stream_t* const* sts, const hevc_picture
                                 int32_t n, hevcgpu_job_t** out);
 /* Returns once the copies of a job's page-locked record arrays have read them. */
 int  hevcgpu_job_wait_uploaded(hevcgpu_job_t* job);
+
+/* Test hook for the device timeout path (no counterpart in the reference): the job's first
+ * intra CTU is made to wait, before its first level, for a level of itself that it can
+ * never publish.  Its bounded wait gives up after about a second, the kernel returns, and
+ * the next sync reports HEVCGPU_ETIMEOUT; the context stays usable.  The injection is a
+ * change of the job's uploaded schedule on the host side: nothing faults or traps.
+ * HEVCGPU_EINVAL for a job without intra TUs. */
+int  hevcgpu_job_plant_unmet_wait(hevcgpu_job_t* job);
 int  hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n,
                             uint8_t* const* outs);
 /* CUDA stream (cudaStream_t) the context launches on. */

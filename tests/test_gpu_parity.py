@@ -180,6 +180,40 @@ def test_prepare_async_then_overwrite_the_records(hb, gpu_ctx, port):
         j.free()
 
 
+def test_bounded_wait_times_out_and_the_context_recovers(hb, gpu_ctx, port):
+    """The intra stage's cross-CTU waits are bounded: a wait for a level that nothing
+    publishes (planted in the job's schedule on the host) gives up after about a second,
+    the sync reports HEVCGPU_ETIMEOUT, and the context then decodes correctly again."""
+    import time
+    w, h, seed = 128, 64, 97
+    st = gpu_ctx.open_stream(w, h, 3)
+    refs = [hb.content(w, h, seed + 1), hb.content(w, h, seed + 2)]
+    st.upload(0, refs[0])
+    st.upload(1, refs[1])
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **dict(cases.PICTURE, p_intra=0.5)))
+    job = st.prepare(pic)
+    job.plant_unmet_wait()
+    t0 = time.perf_counter()
+    job.launch(2)
+    with pytest.raises(hb.HevcGpuError) as e:
+        st.sync()
+    waited = time.perf_counter() - t0
+    assert e.value.code == hb.abi.HEVCGPU_ETIMEOUT
+    assert 0.5 < waited < 30.0
+    job.free()
+    fresh = st.prepare(pic)
+    fresh.launch(2)
+    st.sync()
+    assert _diff(st.download(2), port.reconstruct_picture(pic, refs)) == 0
+    fresh.free()
+    flat = hb.Picture(hb.default_cfg(w, h, seed, p_intra=0.0))
+    j = st.prepare(flat)
+    with pytest.raises(hb.HevcGpuError) as e:
+        j.plant_unmet_wait()
+    assert e.value.code == hb.abi.HEVCGPU_EINVAL
+    j.free()
+
+
 def test_frame_output_cropped_16bit(hb, gpu_ctx, port):
     """hevcgpu_slot_download_frame gives the reconstructed picture inside the conformance
     window as 16-bit planes, as hevc_decoder_get_frame does (hevc_api.cpp:49-77)."""
