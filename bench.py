@@ -17,6 +17,8 @@ stream against the oracle before timing, chaining the oracle's own outputs as re
 value      frames/s over the whole job with the records already in HBM: K GOPs, batched
            form, timed on the device from before the first batch to after the last (max
            over ranks).  "plain" is one launch per stage per picture on the same GOPs.
+samples_per_s and alg_bytes_per_step: value in samples/s (W x H x 1.5 per picture) and the
+           algorithmic bytes of a GOP summed over the stages.
 frame_ms   device time of each GOP position's batch (all its pictures complete with it),
            p50 and p99 over the timed batches; i_frame_ms / pb_frame_ms split it by kind.
 e2e        frames/s through the C ABI from host memory: per group of 4 GOP positions the 32
@@ -599,6 +601,8 @@ def run_ours(args, hb, rank, world, local):
         "plain": {"value": round(plain_value, 2), "unit": "frames/s",
                   "ms_per_picture": round(plain_ms / plain_k / (G * F), 4),
                   "gpu_launches_per_picture": round(plain_launches / plain_k / (G * F), 1)},
+        "samples_per_s": round(value * W * H * 3 // 2),
+        "alg_bytes_per_step": int(sum(alg_sum.values())),
         "batched_over_plain": round(value / plain_value, 3),
         "frame_ms": {"p50": round(statistics.median(all_ms), 4), "p99": round(pct(all_ms, 0.99), 4),
                      "note": "device time of a GOP position's batch; every picture of a batch completes with it"},
