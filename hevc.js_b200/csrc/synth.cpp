@@ -351,7 +351,7 @@ struct Gen {
     }
 
     void run() {
-        const int log2_ctb = 6;
+        const int log2_ctb = c.log2_ctb ? c.log2_ctb : 6;
         int ctb = 1 << log2_ctb;
         int wc = (W + ctb - 1) / ctb, hc = (H + ctb - 1) / ctb;
         P.blk.assign((size_t)(W / 4) * (H / 4), (uint32_t)log2_ctb << HEVC_BLK_TU_SHIFT);
@@ -460,7 +460,8 @@ void hevcsynth_default_cfg(hevcsynth_cfg_t* c, int32_t width, int32_t height, ui
 hevcsynth_picture_t* hevcsynth_picture(const hevcsynth_cfg_t* cfg) {
     if (!cfg || cfg->width <= 0 || cfg->height <= 0 || (cfg->width & 7) || (cfg->height & 7) ||
         cfg->width > 8192 || cfg->height > 4352 || cfg->num_refs < 1 || cfg->num_refs > 2 ||
-        cfg->qp_min < 0 || cfg->qp_max > 51 || cfg->qp_min > cfg->qp_max)
+        cfg->qp_min < 0 || cfg->qp_max > 51 || cfg->qp_min > cfg->qp_max ||
+        (cfg->log2_ctb != 0 && (cfg->log2_ctb < 4 || cfg->log2_ctb > 6)))
         return nullptr;
     Picture* P = new Picture();
     Gen g(*cfg, *P);

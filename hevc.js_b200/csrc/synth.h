@@ -44,6 +44,7 @@ typedef struct hevcsynth_cfg {
     int32_t  cb_qp_offset, cr_qp_offset;
     int32_t  beta_offset_div2, tc_offset_div2;
     int32_t  scaling_lists;      /* attach scaling lists drawn by hevcsynth_scaling     */
+    int32_t  log2_ctb;           /* CtbLog2SizeY 4..6; 0 means 6                        */
 } hevcsynth_cfg_t;
 
 /* One coding unit (synth-only: used by the reference harness to replay decode order). */

@@ -38,6 +38,13 @@ CASES = {
                                        cfg=dict(PICTURE, p_intra=0.3, scaling_lists=1), refs=(141, 142)),
     "picture_scaled_1080p_s15": dict(kind="picture", w=1920, h=1080, seed=15, cfg=dict(PICTURE, scaling_lists=1),
                                      refs=(151, 152)),
+    # 16x16 and 32x32 CTBs (CtbLog2SizeY 4 and 5)
+    "picture_ctb16_352x288_s16": dict(kind="picture", w=352, h=288, seed=16, cfg=dict(PICTURE, log2_ctb=4),
+                                      refs=(161, 162)),
+    "picture_ctb32_416x240_s17": dict(kind="picture", w=416, h=240, seed=17,
+                                      cfg=dict(PICTURE, log2_ctb=5, p_intra=0.4), refs=(171, 172)),
+    "picture_intra_ctb16_208x120_s18": dict(kind="picture", w=208, h=120, seed=18, cfg=dict(ALL_INTRA, log2_ctb=4),
+                                            refs=(181, 182)),
 }
 
 

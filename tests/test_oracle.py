@@ -58,6 +58,18 @@ def test_port_matches_reference_blocks(hb, port, seed, opts):
     assert np.array_equal(port.residual_blocks(tus, n, coeffs, pred), ref.residual_blocks(tus, n, coeffs, pred))
 
 
+@pytest.mark.parametrize("seed,w,h,kw", [(51, 176, 144, dict(log2_ctb=4, p_intra=0.3)),
+                                         (52, 208, 120, dict(log2_ctb=5, p_intra=0.3)),
+                                         (53, 128, 96, dict(log2_ctb=4, slice_type=2)),
+                                         (54, 320, 192, dict(log2_ctb=5, p_intra=0.6, p_intra_nxn=1.0))])
+def test_port_matches_reference_small_ctbs(hb, port, seed, w, h, kw):
+    ref = _ref()
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+    assert pic.syn.params.log2_ctb == kw["log2_ctb"]
+    refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
+    assert np.array_equal(port.reconstruct_picture(pic, refs), ref.reconstruct_picture(pic, refs))
+
+
 @pytest.mark.parametrize("seed,opts", [(25, dict()), (26, dict(big=True)), (27, dict(tskip=True, big=True))])
 def test_port_matches_reference_scaled_blocks(hb, port, seed, opts):
     # scaling lists with factors up to 255: with levels near the int16 limits the
