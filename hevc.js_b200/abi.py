@@ -100,7 +100,8 @@ class SynthCfg(C.Structure):
                 ("num_refs", C.c_int32), ("slice_type", C.c_int32), ("poc", C.c_int32),
                 ("strong_intra_smoothing", C.c_int32), ("cb_qp_offset", C.c_int32),
                 ("cr_qp_offset", C.c_int32), ("beta_offset_div2", C.c_int32),
-                ("tc_offset_div2", C.c_int32), ("scaling_lists", C.c_int32), ("log2_ctb", C.c_int32)]
+                ("tc_offset_div2", C.c_int32), ("scaling_lists", C.c_int32), ("log2_ctb", C.c_int32),
+                ("tile_cols", C.c_int32), ("tile_rows", C.c_int32), ("no_lf_across_tiles", C.c_int32)]
 
 
 class SynthCU(C.Structure):

@@ -685,7 +685,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     // (x-1 .. x+2N-1 at y-1) and column (y .. y+2N-1 at x-1).  An owner in B's CTU puts B
     // one level above it in the CTU-local DAG; an owner in another CTU makes B's CTU wait
     // for that CTU.  A unit whose samples B may not use (availability) can only add an
-    // unneeded level or wait, never change a sample.
+    // unneeded level or wait, never change a sample; owners in CTUs later in raster order
+    // (decoded earlier only in tile scan) are never available and add nothing.
     const int n_intra = (int)intra_list.size();
     auto& ictu_addr = BS.ictu_addr;
     auto& ictu_deps = BS.ictu_deps;
@@ -771,6 +772,11 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
                     last = o;
                     if ((o & OWNER_BITS) == self) return;
                     const int oa = (int)((o >> 16) & 0xFFFFFF), ol = (int)(o & 0xFFFF);
+                    // a CTU later in raster order is never available to this one
+                    // (intra_prediction.cpp:113); in tile scan one can be decoded earlier
+                    // (the tile to the left, below-left), and waiting for it could wait
+                    // for a CTA not yet started: CTAs take CTUs in raster order
+                    if (oa > a) return;
                     int32_t* dl = &dep_list[(size_t)a * 4];
                     int32_t& dn = dep_n[(size_t)a];
                     bool have = false;

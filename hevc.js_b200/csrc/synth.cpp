@@ -86,6 +86,7 @@ struct Picture {
     std::vector<uint32_t> blk;
     std::vector<hevc_sao_t> sao;
     std::vector<uint8_t> ctb_slice;
+    std::vector<uint16_t> ctb_tile;
     std::vector<hevc_slice_t> slices;
     std::vector<hevcsynth_cu_t> cus;
 };
@@ -357,11 +358,19 @@ struct Gen {
         P.blk.assign((size_t)(W / 4) * (H / 4), (uint32_t)log2_ctb << HEVC_BLK_TU_SHIFT);
         P.sao.assign((size_t)wc * hc, hevc_sao_t{});
         P.ctb_slice.assign((size_t)wc * hc, 0);
-        for (int ry = 0; ry < hc; ry++)
-            for (int rx = 0; rx < wc; rx++) {
-                if (c.sao) sao_params(P.sao[(size_t)ry * wc + rx]);
-                quadtree(rx * ctb, ry * ctb, log2_ctb);
-            }
+        // tiles with uniform spacing (column i spans CTB columns i*wc/tc .. (i+1)*wc/tc - 1);
+        // the CTBs of a tile are decoded in raster order, the tiles in raster order
+        const int tc = std::max(1, std::min(c.tile_cols, wc)), tr = std::max(1, std::min(c.tile_rows, hc));
+        const bool tiles = tc * tr > 1;
+        P.ctb_tile.assign((size_t)wc * hc, 0);
+        for (int ty = 0; ty < tr; ty++)
+            for (int tx = 0; tx < tc; tx++)
+                for (int ry = ty * hc / tr; ry < (ty + 1) * hc / tr; ry++)
+                    for (int rx = tx * wc / tc; rx < (tx + 1) * wc / tc; rx++) {
+                        P.ctb_tile[(size_t)ry * wc + rx] = (uint16_t)(ty * tc + tx);
+                        if (c.sao) sao_params(P.sao[(size_t)ry * wc + rx]);
+                        quadtree(rx * ctb, ry * ctb, log2_ctb);
+                    }
         hevc_slice_t s{};
         s.beta_offset_div2 = (int8_t)c.beta_offset_div2;
         s.tc_offset_div2 = (int8_t)c.tc_offset_div2;
@@ -384,8 +393,8 @@ struct Gen {
         p.sao_enabled = c.sao ? 1 : 0;
         p.cb_qp_offset = c.cb_qp_offset;
         p.cr_qp_offset = c.cr_qp_offset;
-        p.tiles_enabled = 0;
-        p.loop_filter_across_tiles = 1;
+        p.tiles_enabled = tiles ? 1 : 0;
+        p.loop_filter_across_tiles = c.no_lf_across_tiles ? 0 : 1;
         int nref = c.slice_type == 2 ? 0 : c.num_refs;
         for (int l = 0; l < 2; l++) {
             p.num_ref[l] = (l == 1 && c.slice_type != 0) ? 0 : nref;
@@ -411,7 +420,7 @@ struct Gen {
         syn.blk = P.blk.data();
         syn.sao = P.sao.data();
         syn.ctb_slice = P.ctb_slice.data();
-        syn.ctb_tile = nullptr;
+        syn.ctb_tile = tiles ? P.ctb_tile.data() : nullptr;
         syn.num_slices = 1;
         syn.slices = P.slices.data();
         syn.scaling = nullptr;

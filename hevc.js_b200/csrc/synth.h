@@ -45,6 +45,9 @@ typedef struct hevcsynth_cfg {
     int32_t  beta_offset_div2, tc_offset_div2;
     int32_t  scaling_lists;      /* attach scaling lists drawn by hevcsynth_scaling     */
     int32_t  log2_ctb;           /* CtbLog2SizeY 4..6; 0 means 6                        */
+    int32_t  tile_cols, tile_rows;   /* uniformly spaced tiles (0 or 1: none); CTBs are  */
+                                     /* then drawn in tile scan, the decoding order      */
+    int32_t  no_lf_across_tiles; /* loop_filter_across_tiles_enabled_flag = 0           */
 } hevcsynth_cfg_t;
 
 /* One coding unit (synth-only: used by the reference harness to replay decode order). */

@@ -125,6 +125,19 @@ void setup(Env& e, const hevc_picture_syntax_t& syn, const uint8_t* in, const ui
     e.pps.pps_cb_qp_offset = p.cb_qp_offset;
     e.pps.pps_cr_qp_offset = p.cr_qp_offset;
     e.pps.loop_filter_across_tiles_enabled_flag = p.loop_filter_across_tiles != 0;
+    // tiles: TileId by tile-scan address with the identity scan conversion, so that
+    // TileId[CtbAddrRsToTs[a]] (deblocking.cpp:79-81, sao.cpp:173-181,
+    // intra_prediction.cpp:118-120) is the record's tile of raster CTB a
+    e.pps.tiles_enabled_flag = p.tiles_enabled != 0 && syn.ctb_tile;
+    e.pps.CtbAddrRsToTs.clear();
+    e.pps.TileId.clear();
+    if (e.pps.tiles_enabled_flag) {
+        const int n = e.sps.PicSizeInCtbsY;
+        for (int a = 0; a < n; a++) {
+            e.pps.CtbAddrRsToTs.push_back(a);
+            e.pps.TileId.push_back(syn.ctb_tile[a]);
+        }
+    }
     e.pps.transquant_bypass_enabled_flag = true;  // SAO/deblock then honour per-CU bypass
     e.sh.slice_type = SliceType::B;
     int ns = std::max(1, (int)syn.num_slices);

@@ -45,6 +45,14 @@ CASES = {
                                       cfg=dict(PICTURE, log2_ctb=5, p_intra=0.4), refs=(171, 172)),
     "picture_intra_ctb16_208x120_s18": dict(kind="picture", w=208, h=120, seed=18, cfg=dict(ALL_INTRA, log2_ctb=4),
                                             refs=(181, 182)),
+    # tiles (uniform spacing, CTBs in tile scan), with and without filtering across them
+    "picture_tiles_416x240_s19": dict(kind="picture", w=416, h=240, seed=19,
+                                      cfg=dict(PICTURE, p_intra=0.4, tile_cols=3, tile_rows=2), refs=(191, 192)),
+    "picture_tiles_1080p_s20": dict(kind="picture", w=1920, h=1080, seed=20,
+                                    cfg=dict(PICTURE, tile_cols=4, tile_rows=3, no_lf_across_tiles=1), refs=(201, 202)),
+    "picture_intra_tiles_ctb16_352x288_s21": dict(kind="picture", w=352, h=288, seed=21,
+                                                  cfg=dict(ALL_INTRA, log2_ctb=4, tile_cols=4, tile_rows=3,
+                                                           no_lf_across_tiles=1), refs=(211, 212)),
 }
 
 

@@ -70,6 +70,20 @@ def test_port_matches_reference_small_ctbs(hb, port, seed, w, h, kw):
     assert np.array_equal(port.reconstruct_picture(pic, refs), ref.reconstruct_picture(pic, refs))
 
 
+@pytest.mark.parametrize("seed,w,h,kw", [(61, 320, 192, dict(tile_cols=3, tile_rows=2, p_intra=0.4)),
+                                         (62, 320, 192, dict(tile_cols=2, tile_rows=2, p_intra=0.4, no_lf_across_tiles=1)),
+                                         (63, 256, 128, dict(tile_cols=4, tile_rows=1, slice_type=2, no_lf_across_tiles=1,
+                                                             log2_ctb=5)),
+                                         (64, 416, 240, dict(tile_cols=3, tile_rows=3, p_intra=0.3, log2_ctb=4,
+                                                             no_lf_across_tiles=1))])
+def test_port_matches_reference_tiles(hb, port, seed, w, h, kw):
+    ref = _ref()
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+    assert pic.syn.params.tiles_enabled == 1
+    refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
+    assert np.array_equal(port.reconstruct_picture(pic, refs), ref.reconstruct_picture(pic, refs))
+
+
 @pytest.mark.parametrize("seed,opts", [(25, dict()), (26, dict(big=True)), (27, dict(tskip=True, big=True))])
 def test_port_matches_reference_scaled_blocks(hb, port, seed, opts):
     # scaling lists with factors up to 255: with levels near the int16 limits the
