@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import cases
-from test_oracle import _edit_blocks, with_filter_edits
+from test_oracle import RESIDUAL_EDIT_CASES, _edit_blocks, with_filter_edits, with_residual_edits
 
 pytestmark = pytest.mark.gpu
 
@@ -62,6 +62,16 @@ def test_gpu_blocks_empty(hb, gpu_ctx):
                                          (47, 1280, 720, dict(tile_cols=4, tile_rows=2, p_intra=0.4))])
 def test_gpu_pictures(hb, gpu_ctx, port, seed, w, h, kw):
     pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+    refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
+    assert _diff(gpu_ctx.reconstruct_picture(pic, refs), port.reconstruct_picture(pic, refs)) == 0
+
+
+@pytest.mark.parametrize("seed,w,h,kw,params", RESIDUAL_EDIT_CASES + [(75, 1920, 1080, dict(p_intra=0.3), {})])
+def test_gpu_bypass_tskip_qp_offsets(hb, gpu_ctx, port, seed, w, h, kw, params):
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+    assert min(with_residual_edits(hb, pic, seed)) > 0
+    for k, v in params.items():
+        setattr(pic.syn.params, k, v)
     refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
     assert _diff(gpu_ctx.reconstruct_picture(pic, refs), port.reconstruct_picture(pic, refs)) == 0
 

@@ -154,6 +154,54 @@ def with_filter_edits(hb, pic, seed, slices=True, pcm_bypass=True):
     return keep
 
 
+def with_residual_edits(hb, pic, seed, p_bypass=0.1, p_tskip=0.5):
+    """Mutate a generated picture: some CUs transquant-bypass (their TUs' levels are the
+    residual, coding_tree.cpp:1302-1304, and the grid marks them, so that the filters leave
+    their samples alone), and about half the coded 4x4 TUs of the others transform-skipped.
+    Returns the numbers of bypass and transform-skip TUs made."""
+    syn, p = pic.syn, pic.syn.params
+    rng = np.random.default_rng(seed)
+    cus = pic.ptr.contents
+    gw, gh = p.width // 4, p.height // 4
+    blk = np.ctypeslib.as_array(syn.blk, (gh * gw,))
+    n_bypass = n_tskip = 0
+    for i in range(cus.num_cus):
+        cu = cus.cus[i]
+        bypass = rng.random() < p_bypass
+        for k in range(cu.first_tu, cu.first_tu + cu.num_tu):
+            t = syn.tus[k]
+            if bypass:
+                t.flags |= hb.abi.HEVC_TU_BYPASS
+                n_bypass += 1
+            elif (t.flags & hb.abi.HEVC_TU_CODED) and t.log2_size == 2 and rng.random() < p_tskip:
+                t.flags |= hb.abi.HEVC_TU_TSKIP
+                n_tskip += 1
+        if bypass:
+            n = 1 << cu.log2_size
+            for y in range(cu.y // 4, min((cu.y + n) // 4, gh)):
+                blk[y * gw + cu.x // 4: y * gw + min((cu.x + n) // 4, gw)] |= hb.abi.HEVC_BLK_BYPASS
+    return n_bypass, n_tskip
+
+
+# pictures with bypass and transform-skip TUs, chroma QP offsets, intra smoothing off
+RESIDUAL_EDIT_CASES = [(71, 320, 192, dict(p_intra=0.4), {}),
+                       (72, 256, 128, dict(slice_type=2), {}),
+                       (73, 320, 192, dict(p_intra=0.3, cb_qp_offset=5, cr_qp_offset=-4), {}),
+                       (74, 256, 192, dict(p_intra=0.6, p_intra_nxn=1.0), {"intra_smoothing_disabled": 1})]
+
+
+@pytest.mark.parametrize("seed,w,h,kw,params", RESIDUAL_EDIT_CASES)
+def test_port_matches_reference_bypass_tskip_qp_offsets(hb, port, seed, w, h, kw, params):
+    ref = _ref()
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+    assert min(with_residual_edits(hb, pic, seed)) > 0
+    for k, v in params.items():
+        setattr(pic.syn.params, k, v)
+    refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
+    got = port.reconstruct_picture(pic, refs)
+    assert np.array_equal(got, ref.reconstruct_picture(pic, refs))
+
+
 @pytest.mark.parametrize("seed,w,h", [(41, 320, 192), (42, 200, 136)])
 def test_port_matches_reference_filters_with_slices_pcm_bypass(hb, port, seed, w, h):
     ref = _ref()
