@@ -20,6 +20,7 @@ HEVC_TU_INTRA = 0x01
 HEVC_TU_CODED = 0x02
 HEVC_TU_TSKIP = 0x04
 HEVC_TU_BYPASS = 0x08
+HEVC_TU_PCM = 0x10
 
 HEVC_BLK_EDGE_V = 0x01
 HEVC_BLK_EDGE_H = 0x02
@@ -101,7 +102,8 @@ class SynthCfg(C.Structure):
                 ("strong_intra_smoothing", C.c_int32), ("cb_qp_offset", C.c_int32),
                 ("cr_qp_offset", C.c_int32), ("beta_offset_div2", C.c_int32),
                 ("tc_offset_div2", C.c_int32), ("scaling_lists", C.c_int32), ("log2_ctb", C.c_int32),
-                ("tile_cols", C.c_int32), ("tile_rows", C.c_int32), ("no_lf_across_tiles", C.c_int32)]
+                ("tile_cols", C.c_int32), ("tile_rows", C.c_int32), ("no_lf_across_tiles", C.c_int32),
+                ("p_pcm", C.c_double)]
 
 
 class SynthCU(C.Structure):

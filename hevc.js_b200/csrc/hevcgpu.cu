@@ -471,7 +471,8 @@ bool tus_pass(const hevc_picture_syntax_t* s, int W, int H) {
         const uint32_t pw = t.c_idx ? (uint32_t)W / 2 : (uint32_t)W, ph = t.c_idx ? (uint32_t)H / 2 : (uint32_t)H;
         bad |= (uint32_t)(t.log2_size - 2u > 3u) | (uint32_t)(t.c_idx > 2) | (uint32_t)(((t.x | t.y) & (n - 1)) != 0) |
                (uint32_t)(t.x + n > pw) | (uint32_t)(t.y + n > ph) |
-               (uint32_t)((t.flags & HEVC_TU_INTRA) && t.intra_mode > 34);
+               (uint32_t)((t.flags & HEVC_TU_INTRA) && t.intra_mode > 34) |
+               (uint32_t)((t.flags & HEVC_TU_PCM) && (~t.flags & (HEVC_TU_INTRA | HEVC_TU_CODED)));
         const uint64_t end = (uint64_t)t.coeff_offset + (uint64_t)n * n;
         bad |= (uint32_t)((t.flags & HEVC_TU_CODED) && ((t.coeff_offset & 15) | (uint32_t)(end > ncoef) |
                                                         (uint32_t)(t.qp > 51 + 48)));
@@ -513,6 +514,8 @@ int validate(const hevc_picture_syntax_t* s, bool need_tus, bool need_pus, bool 
                             t.x, t.y, n, t.c_idx);
             if ((t.flags & HEVC_TU_INTRA) && t.intra_mode > 34)
                 return fail(HEVCGPU_EINVAL, "TU %d intra mode %d", i, t.intra_mode);
+            if ((t.flags & HEVC_TU_PCM) && (~t.flags & (HEVC_TU_INTRA | HEVC_TU_CODED)))
+                return fail(HEVCGPU_EINVAL, "TU %d is PCM but not an intra TU with levels", i);
             if (t.flags & HEVC_TU_CODED) {
                 if ((t.coeff_offset & 15) || (uint64_t)t.coeff_offset + (uint64_t)n * n > s->num_coeffs)
                     return fail(HEVCGPU_EINVAL, "TU %d coeff_offset %u (multiple of 16, inside the pool)", i,

@@ -280,6 +280,10 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
                 for (int j = 0; j < 4; j++) p[j] = clip_u8(p[j] + ((ctop[j] - corner) >> 1));
             }
         }
+        if (t.flags & HEVC_TU_PCM) {   // the PCM samples are the levels, with no prediction
+#pragma unroll
+            for (int j = 0; j < 4; j++) p[j] = 0;
+        }
         // residual (four int16 in one 8-byte load), clip, one word to the tile and the picture
         int rv[4] = {0, 0, 0, 0};
         if (res) {

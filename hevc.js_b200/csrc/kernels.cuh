@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(128) k_residual(const __grid_constant__ SegTab
     const bool live = item < sg.n_items;
     const PicDesc& P = *sg.pic;
     hevc_tu_t t = live ? P.tus[static_cast<const int32_t*>(sg.items)[item]] : hevc_tu_t{};
-    const bool bypass = t.flags & HEVC_TU_BYPASS;
+    const bool bypass = t.flags & (HEVC_TU_BYPASS | HEVC_TU_PCM);   // levels are the residual
     const bool tskip = (t.flags & HEVC_TU_TSKIP) && !bypass;
     const bool dst4 = (LOG2 == 2) && (t.flags & HEVC_TU_INTRA) && t.c_idx == 0;
 

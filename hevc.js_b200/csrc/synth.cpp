@@ -145,6 +145,23 @@ struct Gen {
         P.tus.push_back(t);
     }
 
+    // A PCM block: its samples (uniform 0..255) as the levels of an intra TU.
+    void emit_pcm(int x, int y, int log2, int cidx, int qp) {
+        hevc_tu_t t{};
+        t.x = (uint16_t)x;
+        t.y = (uint16_t)y;
+        t.log2_size = (uint8_t)log2;
+        t.c_idx = (uint8_t)cidx;
+        t.qp = (uint8_t)std::max(0, qp);
+        t.flags = (uint8_t)(HEVC_TU_INTRA | HEVC_TU_CODED | HEVC_TU_PCM);
+        t.intra_mode = 1;
+        const int n = 1 << log2;
+        t.coeff_offset = (uint32_t)P.coeffs.size();
+        P.coeffs.resize(P.coeffs.size() + (size_t)n * n);
+        for (int i = 0; i < n * n; i++) P.coeffs[t.coeff_offset + (size_t)i] = (int16_t)r.range(0, 255);
+        P.tus.push_back(t);
+    }
+
     // Transform tree in parse order (decode_transform_tree, coding_tree.cpp:1146-1250).
     void tree(const hevcsynth_cu_t& cu, int chroma_mode, int x0, int y0, int xb, int yb,
               int log2, int depth, int blk_idx, bool cbf_cb_par, bool cbf_cr_par) {
@@ -268,9 +285,12 @@ struct Gen {
             }
         }
         cu.num_pu = (int32_t)P.pus.size() - cu.first_pu;
+        // PCM (pcm_flag of a 2Nx2N intra CU, coding_tree.cpp:1425-1469); drawn only when asked,
+        // so that the pictures of other settings stay the same
+        const bool pcm = intra && part == 0 && log2 <= 5 && c.p_pcm > 0 && r.bern(c.p_pcm);
 
         // CU-level grid initialisation (coding_tree.cpp:960-1021)
-        uint32_t base = (intra ? HEVC_BLK_INTRA : 0u) |
+        uint32_t base = (intra ? HEVC_BLK_INTRA : 0u) | (pcm ? HEVC_BLK_PCM : 0u) |
                         ((uint32_t)(uint8_t)cu.qp_y << HEVC_BLK_QP_SHIFT) |
                         ((uint32_t)log2 << HEVC_BLK_TU_SHIFT);
         for (int dy = 0; dy < n; dy += 4)
@@ -294,7 +314,12 @@ struct Gen {
             chroma_mode = chroma_mode_from(r.range(0, 4), cu_luma_mode[0]);
         }
         cu.first_tu = (int32_t)P.tus.size();
-        cu.has_tree = cu.pred_mode != 2;
+        cu.has_tree = cu.pred_mode != 2 && !pcm;
+        if (pcm) {   // the samples in decode order: luma, then Cb and Cr
+            emit_pcm(x0, y0, log2, 0, cu.qp_y);
+            emit_pcm(x0 / 2, y0 / 2, log2 - 1, 1, cu.qp_y);
+            emit_pcm(x0 / 2, y0 / 2, log2 - 1, 2, cu.qp_y);
+        }
         if (cu.has_tree) tree(cu, chroma_mode, x0, y0, x0, y0, log2, 0, 0, true, true);
         cu.num_tu = (int32_t)P.tus.size() - cu.first_tu;
         P.cus.push_back(cu);

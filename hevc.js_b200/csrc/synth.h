@@ -48,6 +48,7 @@ typedef struct hevcsynth_cfg {
     int32_t  tile_cols, tile_rows;   /* uniformly spaced tiles (0 or 1: none); CTBs are  */
                                      /* then drawn in tile scan, the decoding order      */
     int32_t  no_lf_across_tiles; /* loop_filter_across_tiles_enabled_flag = 0           */
+    double   p_pcm;              /* probability that a 2Nx2N intra CU of 8..32 is PCM   */
 } hevcsynth_cfg_t;
 
 /* One coding unit (synth-only: used by the reference harness to replay decode order). */

@@ -56,6 +56,8 @@ extern "C" {
 #define HEVC_TU_CODED   0x02  /* has coefficient levels at coeff_offset (cbf set)        */
 #define HEVC_TU_TSKIP   0x04  /* transform_skip_flag                                    */
 #define HEVC_TU_BYPASS  0x08  /* cu_transquant_bypass: levels are the residual          */
+#define HEVC_TU_PCM     0x10  /* pcm_flag: the levels are the samples, no prediction     */
+                              /* (coding_tree.cpp:1425-1469; with INTRA and CODED)      */
 
 /* One transform block of one colour component (decode order = z-scan, luma before
  * chroma, 4x4-luma chroma deferred to blkIdx 3; src/decoding/coding_tree.cpp:1256). */

@@ -141,7 +141,7 @@ static void tu_residual(const hevc_tu_t* t, const int16_t* levels, int bit_depth
                         int16_t* res) {
     int n = 1 << t->log2_size;
     if (!(t->flags & HEVC_TU_CODED)) { memset(res, 0, sizeof(int16_t) * n * n); return; }
-    if (t->flags & HEVC_TU_BYPASS) { memcpy(res, levels, sizeof(int16_t) * n * n); return; }
+    if (t->flags & (HEVC_TU_BYPASS | HEVC_TU_PCM)) { memcpy(res, levels, sizeof(int16_t) * n * n); return; }
     int16_t d[32 * 32];
     dequant(levels, n, t->qp, bit_depth, sl, t->c_idx, (t->flags & HEVC_TU_INTRA) != 0, d);
     inverse_transform(d, n, t->flags, t->c_idx, bit_depth, res);
@@ -459,11 +459,13 @@ static void intra_tu(const intra_env_t* e, const hevc_tu_t* t, const int16_t* re
                 for (int x = 0; x < n; x++) pred[x] = CLIP3(0, 255, pred[x] + ((top[x + 1] - top[0]) >> 1));
         }
     }
+    /* a PCM block's samples are its levels (coding_tree.cpp:1425-1469): no prediction */
+    int pcm = (t->flags & HEVC_TU_PCM) != 0;
     uint8_t* D = pic->p[ci];
     for (int y = 0; y < n; y++)
         for (int x = 0; x < n; x++) {
             if (xc + x >= pw || yc + y >= ph) continue;
-            int v = (int16_t)pred[y * n + x] + (res ? res[y * n + x] : 0);
+            int v = (pcm ? 0 : (int16_t)pred[y * n + x]) + (res ? res[y * n + x] : 0);
             D[(size_t)(yc + y) * pw + xc + x] = (uint8_t)CLIP3(0, 255, v);
         }
 }

@@ -329,6 +329,14 @@ void tu_residual(Env& e, const hevc_tu_t& t, const int16_t* coeffs, int16_t* res
 // the MC samples already in the picture), then reconstruct_block's add and clip.
 void tu_recon(Env& e, const hevc_tu_t& t, const int16_t* coeffs) {
     int n = 1 << t.log2_size, c = t.c_idx, sub = c ? 2 : 1;
+    if (t.flags & HEVC_TU_PCM) {   // pcm_sample values written as they are (coding_tree.cpp:1425-1469)
+        const int16_t* lv = coeffs + t.coeff_offset;
+        for (int y = 0; y < n; y++)
+            for (int x = 0; x < n; x++)
+                if (t.x + x < e.pic.width[c] && t.y + y < e.pic.height[c])
+                    e.pic.sample(c, t.x + x, t.y + y) = (uint16_t)lv[y * n + x];
+        return;
+    }
     int16_t residual[32 * 32];
     tu_residual(e, t, coeffs, residual);
     int16_t pred[32 * 32] = {};

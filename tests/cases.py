@@ -50,6 +50,8 @@ CASES = {
                                       cfg=dict(PICTURE, p_intra=0.4, tile_cols=3, tile_rows=2), refs=(191, 192)),
     "picture_tiles_1080p_s20": dict(kind="picture", w=1920, h=1080, seed=20,
                                     cfg=dict(PICTURE, tile_cols=4, tile_rows=3, no_lf_across_tiles=1), refs=(201, 202)),
+    "picture_pcm_416x240_s22": dict(kind="picture", w=416, h=240, seed=22, cfg=dict(PICTURE, p_intra=0.5, p_pcm=0.3),
+                                    refs=(221, 222)),
     "picture_intra_tiles_ctb16_352x288_s21": dict(kind="picture", w=352, h=288, seed=21,
                                                   cfg=dict(ALL_INTRA, log2_ctb=4, tile_cols=4, tile_rows=3,
                                                            no_lf_across_tiles=1), refs=(211, 212)),

@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import cases
-from test_oracle import RESIDUAL_EDIT_CASES, _edit_blocks, with_filter_edits, with_residual_edits
+from test_oracle import PCM_CASES, RESIDUAL_EDIT_CASES, _edit_blocks, with_filter_edits, with_residual_edits
 
 pytestmark = pytest.mark.gpu
 
@@ -72,6 +72,14 @@ def test_gpu_bypass_tskip_qp_offsets(hb, gpu_ctx, port, seed, w, h, kw, params):
     assert min(with_residual_edits(hb, pic, seed)) > 0
     for k, v in params.items():
         setattr(pic.syn.params, k, v)
+    refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
+    assert _diff(gpu_ctx.reconstruct_picture(pic, refs), port.reconstruct_picture(pic, refs)) == 0
+
+
+@pytest.mark.parametrize("seed,w,h,kw,lf_off", PCM_CASES + [(85, 1920, 1080, dict(p_intra=0.3, p_pcm=0.3), 1)])
+def test_gpu_pcm(hb, gpu_ctx, port, seed, w, h, kw, lf_off):
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+    pic.syn.params.pcm_loop_filter_disabled = lf_off
     refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
     assert _diff(gpu_ctx.reconstruct_picture(pic, refs), port.reconstruct_picture(pic, refs)) == 0
 
@@ -392,6 +400,12 @@ def test_invalid_records_are_refused(hb, gpu_ctx):
         gpu_ctx.reconstruct_picture(pic, refs)
     assert e.value.code == hb.abi.HEVCGPU_EINVAL
     s.tus[0].x = old[0]
+    flags = s.tus[0].flags
+    s.tus[0].flags = hb.abi.HEVC_TU_CODED | hb.abi.HEVC_TU_PCM   # PCM needs an intra TU
+    with pytest.raises(hb.HevcGpuError) as e:
+        gpu_ctx.reconstruct_picture(pic, refs)
+    assert e.value.code == hb.abi.HEVCGPU_EINVAL and "PCM" in str(e.value)
+    s.tus[0].flags = flags
     s.pus[0].ref_idx[0] = 9
     with pytest.raises(hb.HevcGpuError):
         gpu_ctx.reconstruct_picture(pic, refs)

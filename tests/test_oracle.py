@@ -202,6 +202,21 @@ def test_port_matches_reference_bypass_tskip_qp_offsets(hb, port, seed, w, h, kw
     assert np.array_equal(got, ref.reconstruct_picture(pic, refs))
 
 
+# PCM CUs (HEVC_TU_PCM: the levels are the samples), with and without pcm_loop_filter_disabled
+PCM_CASES = [(81, 320, 192, dict(p_intra=0.5, p_pcm=0.3), 0), (82, 320, 192, dict(p_intra=0.5, p_pcm=0.3), 1),
+             (83, 256, 128, dict(slice_type=2, p_pcm=0.4), 1), (84, 208, 120, dict(slice_type=2, p_pcm=0.5, log2_ctb=4), 0)]
+
+
+@pytest.mark.parametrize("seed,w,h,kw,lf_off", PCM_CASES)
+def test_port_matches_reference_pcm(hb, port, seed, w, h, kw, lf_off):
+    ref = _ref()
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+    pic.syn.params.pcm_loop_filter_disabled = lf_off
+    assert any(pic.syn.tus[i].flags & hb.abi.HEVC_TU_PCM for i in range(pic.syn.num_tus))
+    refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
+    assert np.array_equal(port.reconstruct_picture(pic, refs), ref.reconstruct_picture(pic, refs))
+
+
 @pytest.mark.parametrize("seed,w,h", [(41, 320, 192), (42, 200, 136)])
 def test_port_matches_reference_filters_with_slices_pcm_bypass(hb, port, seed, w, h):
     ref = _ref()
