@@ -59,7 +59,10 @@ def test_gpu_blocks_empty(hb, gpu_ctx):
                                          (45, 1280, 720, dict(log2_ctb=5, p_intra=0.5, p_intra_nxn=1.0)),
                                          (46, 1920, 1080, dict(tile_cols=5, tile_rows=3, log2_ctb=4, slice_type=2,
                                                                no_lf_across_tiles=1)),
-                                         (47, 1280, 720, dict(tile_cols=4, tile_rows=2, p_intra=0.4))])
+                                         (47, 1280, 720, dict(tile_cols=4, tile_rows=2, p_intra=0.4)),
+                                         (91, 320, 192, dict(slice_type=1, p_intra=0.2, p_wp=0.4)),
+                                         (92, 256, 128, dict(num_refs=1, p_intra=0.2)),
+                                         (94, 1920, 1080, dict(slice_type=1, p_wp=0.3))])
 def test_gpu_pictures(hb, gpu_ctx, port, seed, w, h, kw):
     pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
     refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]

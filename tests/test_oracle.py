@@ -109,7 +109,10 @@ def test_port_matches_reference_scaled_pictures(hb, port, seed, w, h, kw):
 @pytest.mark.parametrize("seed,w,h,kw", [(31, 176, 144, dict(p_intra=0.3)), (32, 64, 64, dict(slice_type=2)),
                                          (33, 136, 72, dict(p_intra=0.2, p_skip=0.5, p_merge=0.6)),
                                          (34, 256, 192, dict(p_intra=0.7, p_intra_nxn=1.0)),
-                                         (35, 320, 128, dict(p_wp=0.6, mv_range=4096))])
+                                         (35, 320, 128, dict(p_wp=0.6, mv_range=4096)),
+                                         (91, 320, 192, dict(slice_type=1, p_intra=0.2, p_wp=0.4)),
+                                         (92, 256, 128, dict(num_refs=1, p_intra=0.2)),
+                                         (93, 320, 192, dict(slice_type=1, num_refs=1, p_wp=0.5))])
 def test_port_matches_reference_pictures(hb, port, seed, w, h, kw):
     ref = _ref()
     pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
