@@ -205,6 +205,19 @@ def test_port_matches_reference_bypass_tskip_qp_offsets(hb, port, seed, w, h, kw
     assert np.array_equal(got, ref.reconstruct_picture(pic, refs))
 
 
+@pytest.mark.parametrize("seed,w,h,kw", [
+    (101, 320, 192, dict(qp_min=0, qp_max=51, p_intra=0.3, beta_offset_div2=6, tc_offset_div2=6)),
+    (102, 320, 192, dict(qp_min=0, qp_max=51, p_intra=0.3, beta_offset_div2=-6, tc_offset_div2=-6)),
+    (103, 256, 128, dict(qp_min=45, qp_max=51, slice_type=2, tc_offset_div2=6, cb_qp_offset=12, cr_qp_offset=-12)),
+    (104, 256, 128, dict(qp_min=0, qp_max=4, p_intra=0.5, cb_qp_offset=-12, cr_qp_offset=12))])
+def test_port_matches_reference_extreme_qps_and_offsets(hb, port, seed, w, h, kw):
+    # the ends of the beta / tC / chroma QP tables (clipped indices) in whole pictures
+    ref = _ref()
+    pic = hb.Picture(hb.default_cfg(w, h, seed, **kw))
+    refs = [hb.content(w, h, seed + 1000), hb.content(w, h, seed + 2000)]
+    assert np.array_equal(port.reconstruct_picture(pic, refs), ref.reconstruct_picture(pic, refs))
+
+
 # PCM CUs (HEVC_TU_PCM: the levels are the samples), with and without pcm_loop_filter_disabled
 PCM_CASES = [(81, 320, 192, dict(p_intra=0.5, p_pcm=0.3), 0), (82, 320, 192, dict(p_intra=0.5, p_pcm=0.3), 1),
              (83, 256, 128, dict(slice_type=2, p_pcm=0.4), 1), (84, 208, 120, dict(slice_type=2, p_pcm=0.5, log2_ctb=4), 0)]
