@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libhevcref.so")
 REF_CLI = os.path.join(HERE, "_ref", "hevc-decode")
+RECORDER = os.path.join(HERE, "_ref", "hevc-record")
 REF_DIR = os.environ.get("HEVC_REF_DIR", "/root/reference")
 
 _libs = {}
@@ -28,7 +29,7 @@ def build(with_ref=None):
     if with_ref is None:
         with_ref = os.path.isdir(os.path.join(REF_DIR, "src"))
     if with_ref:
-        targets.append("ref")
+        targets += ["ref", "record"]
     subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={REF_DIR}", "-j8", *targets], check=True)
 
 
