@@ -17,7 +17,15 @@
 // Per picture, after the reference's SAO, the oracle (hevc_oracle.c) reconstructs the
 // picture from the records and from its own earlier outputs as reference pictures, and the
 // result is compared with the reference's picture.  One line per picture:
-//   picture <n> poc <p>: match | mismatch <samples> | unsupported (<why>)
+//   picture <n> poc <p>: match (<TUs>, <PUs>) fnv <FNV-1a 64 of the reference's I420 picture>
+//                      | mismatch <samples> | unsupported (<why>)
+// With a second argument the records of every picture the oracle matched are written to that
+// file, with the references as decode indices of earlier pictures:
+//   "HREC" u32 version (1), then per picture: hevc_pic_params_t (ref_slot entries: decode
+//   index of the referenced picture), i32 counts of TUs, levels, PUs, WP rows and slices,
+//   u8 has_scaling, u8 has_tiles, 2 pad bytes, then the arrays: TUs, levels, PUs, WP rows,
+//   the blk grid, SAO per CTB, slice index per CTB, tile id per CTB (when has_tiles),
+//   slices, scaling lists (when has_scaling).
 #include <dlfcn.h>
 
 #include <cstdio>
@@ -72,6 +80,8 @@ struct Recording {
     std::vector<const Picture*> pu_ref[2];   // per PU: the reference picture of each list
     std::string unsupported;
     std::map<const Picture*, Picture8> ours;  // the oracle's output for each reference Picture object
+    std::map<const Picture*, int> index_of;   // decode index of the picture each Picture object holds
+    FILE* dump = nullptr;
     // the picture's records, built at apply_deblocking
     hevc_picture_syntax_t syn{};
     std::vector<uint32_t> blk;
@@ -364,13 +374,39 @@ void apply_sao(DecodingContext& ctx) {
                 for (int x = 0; x < w; x++, at++) diff += out.s[at] != (uint8_t)pic.planes[c][(size_t)y * pic.stride[c] + x];
         }
         if (diff == 0) {
-            std::printf("picture %d poc %d: match (%d TUs, %d PUs)\n", n, pic.poc, R.syn.num_tus, R.syn.num_pus);
+            uint64_t fnv = 1469598103934665603ull;   // equal to the reference's samples here
+            for (uint8_t v : out.s) fnv = (fnv ^ v) * 1099511628211ull;
+            std::printf("picture %d poc %d: match (%d TUs, %d PUs) fnv %016llx\n", n, pic.poc, R.syn.num_tus,
+                        R.syn.num_pus, (unsigned long long)fnv);
             R.matched++;
         } else {
             std::printf("picture %d poc %d: mismatch %zu samples\n", n, pic.poc, diff);
             R.mismatched++;
         }
     }
+    if (R.dump && R.mismatched == 0 && why.empty()) {   // the records of a matched picture
+        hevc_picture_syntax_t s = R.syn;
+        for (int l = 0; l < 2; l++)
+            for (int i = 0; i < s.params.num_ref[l]; i++)
+                if (s.params.ref_slot[l][i] >= 0) s.params.ref_slot[l][i] = R.index_of[R.refs[(size_t)s.params.ref_slot[l][i]]];
+        const int32_t counts[5] = {s.num_tus, (int32_t)s.num_coeffs, s.num_pus, s.num_wp, s.num_slices};
+        const uint8_t flags[4] = {(uint8_t)(s.scaling != nullptr), (uint8_t)(s.ctb_tile != nullptr), 0, 0};
+        const int ctb = 1 << s.params.log2_ctb, nctb = ((W + ctb - 1) / ctb) * ((H + ctb - 1) / ctb);
+        std::fwrite(&s.params, sizeof(s.params), 1, R.dump);
+        std::fwrite(counts, sizeof(counts), 1, R.dump);
+        std::fwrite(flags, sizeof(flags), 1, R.dump);
+        std::fwrite(s.tus, sizeof(hevc_tu_t), (size_t)s.num_tus, R.dump);
+        std::fwrite(s.coeffs, sizeof(int16_t), (size_t)s.num_coeffs, R.dump);
+        std::fwrite(s.pus, sizeof(hevc_pu_t), (size_t)s.num_pus, R.dump);
+        std::fwrite(s.wp, sizeof(hevc_wp_t), (size_t)s.num_wp, R.dump);
+        std::fwrite(s.blk, sizeof(uint32_t), (size_t)(W / 4) * (H / 4), R.dump);
+        std::fwrite(s.sao, sizeof(hevc_sao_t), (size_t)nctb, R.dump);
+        std::fwrite(s.ctb_slice, 1, (size_t)nctb, R.dump);
+        if (s.ctb_tile) std::fwrite(s.ctb_tile, sizeof(uint16_t), (size_t)nctb, R.dump);
+        std::fwrite(s.slices, sizeof(hevc_slice_t), (size_t)s.num_slices, R.dump);
+        if (s.scaling) std::fwrite(s.scaling, sizeof(hevc_scaling_t), 1, R.dump);
+    }
+    R.index_of[&pic] = n;
     R.ours[&pic] = std::move(out);
     R.tus.clear();
     R.coeffs.clear();
@@ -398,10 +434,21 @@ int main(int argc, char** argv) {
     size_t got;
     while ((got = std::fread(buf, 1, sizeof(buf), fp)) > 0) data.insert(data.end(), buf, buf + got);
     std::fclose(fp);
+    if (argc > 2) {
+        R.dump = std::fopen(argv[2], "wb");
+        if (!R.dump) {
+            std::fprintf(stderr, "hevc-record: cannot write %s\n", argv[2]);
+            return 2;
+        }
+        const uint32_t version = 1;
+        std::fwrite("HREC", 1, 4, R.dump);
+        std::fwrite(&version, 4, 1, R.dump);
+    }
     HEVCDecoder* dec = hevc_decoder_create();
     const int rc = hevc_decoder_decode(dec, data.data(), data.size());
     hevc_decoder_flush(dec);
     hevc_decoder_destroy(dec);
+    if (R.dump) std::fclose(R.dump);
     std::printf("pictures %d matched %d mismatched %d unsupported %d decode_rc %d\n", R.pictures, R.matched,
                 R.mismatched, R.skipped, rc);
     return R.mismatched ? 1 : 0;
