@@ -430,3 +430,29 @@ def test_budget_admission(hb, gpu_ctx):
     assert ctx.bytes_in_use() <= 8 << 20
     st.close()
     ctx.close()
+
+
+def test_gpu_reconstructs_recorded_real_streams(hb, gpu_ctx):
+    """The records of the reference's own conformance streams (tests/golden/real/, recorded
+    inside privaloops/hevc.js by oracle/recorder.cpp) through the DPB API: every picture,
+    predicted from the GPU's own earlier pictures in its stream's slots, has the MD5 of the
+    picture the reference decoded."""
+    import hashlib
+    import json
+    import os
+    import sys
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, golden)
+    import real_streams
+    want = json.load(open(os.path.join(golden, "real_streams.json")))["streams"]
+    for name in sorted(want):
+        pics = real_streams.load(hb.abi, os.path.join(real_streams.DIR, name + ".hrec.xz"))
+        assert len(pics) <= 16   # one slot per picture: params.ref_slot (decode indices) are the slots
+        st = gpu_ctx.open_stream(pics[0].width, pics[0].height, 16)
+        for k, pic in enumerate(pics):
+            job = st.prepare(pic)
+            job.launch(k)
+            st.sync()
+            assert hashlib.md5(st.download(k).tobytes()).hexdigest() == want[name]["md5"][k], (name, k)
+            job.free()
+        st.close()
