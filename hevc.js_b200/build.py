@@ -3,6 +3,10 @@
   libhevcsynth.so  host: seeded workload generator (csrc/synth.cpp)
   libhevcgpu.so    the CUDA back end for sm_100a (csrc/hevcgpu.cu + kernels) with the
                    C ABI of include/hevcgpu.h
+  libhevcdec_gpu.so  the hevc.js decoder C API (include/hevc_api_gpu.h): the reference's
+                   host parser compiled from its sources (HEVC_REF_DIR, or a checkout beside
+                   this repository) with the recording hooks of dropin/, over libhevcgpu.so;
+                   built only where the reference tree is present (the built library travels)
 
 Both are written next to this file so that they travel with the source tree.
 """
@@ -18,6 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 SYNTH_SO = os.path.join(PKG, "libhevcsynth.so")
 GPU_SO = os.path.join(PKG, "libhevcgpu.so")
+DROPIN_SO = os.path.join(PKG, "libhevcdec_gpu.so")
+DROPIN_CLI = os.path.join(PKG, "dropin", "_build", "hevc-decode")
 
 GPU_SOURCES = ["hevcgpu.cu"]
 GPU_DEPS = ["hevcgpu.cu", "kernels.cuh", "mc.cuh", "intra.cuh", "device_common.cuh", "../../include/hevcgpu.h"]
@@ -60,9 +66,26 @@ def build_gpu(force=False, verbose_ptxas=False):
     return GPU_SO
 
 
+def ref_dir():
+    return os.environ.get("HEVC_REF_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
+
+
+def build_dropin(force=False):
+    """The drop-in decoder library and the reference's CLI over it (dropin/Makefile)."""
+    ref = ref_dir()
+    if not os.path.isdir(os.path.join(ref, "src")):
+        return None
+    cmd = ["make", "-s", "-C", os.path.join(PKG, "dropin"), f"REF_DIR={ref}", "-j8"]
+    if force:
+        cmd.insert(1, "-B")
+    _run(cmd)
+    return DROPIN_SO
+
+
 def build_all(force=False):
     build_synth(force)
     build_gpu(force)
+    build_dropin(force)
 
 
 if __name__ == "__main__":

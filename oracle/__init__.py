@@ -18,7 +18,9 @@ PORT_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libhevcref.so")
 REF_CLI = os.path.join(HERE, "_ref", "hevc-decode")
 RECORDER = os.path.join(HERE, "_ref", "hevc-record")
-REF_DIR = os.environ.get("HEVC_REF_DIR", "/root/reference")
+DROPIN_SO = os.path.join(HERE, "_ref", "libhevcdec_oracle.so")
+# the reference tree: HEVC_REF_DIR, else a checkout beside this repository
+REF_DIR = os.environ.get("HEVC_REF_DIR", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 _libs = {}
 
@@ -29,7 +31,7 @@ def build(with_ref=None):
     if with_ref is None:
         with_ref = os.path.isdir(os.path.join(REF_DIR, "src"))
     if with_ref:
-        targets += ["ref", "record"]
+        targets += ["ref", "record", "dropin"]
     subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={REF_DIR}", "-j8", *targets], check=True)
 
 
