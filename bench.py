@@ -9,8 +9,8 @@ compensation, dequant + inverse transform, intra wavefront, deblocking, SAO.  Th
 streams' pictures of one GOP position are merged into one batch (one launch per stage);
 the 60 batches run in decode order, each after the one it references.  The plain form
 (one launch per stage per picture) is timed beside it.  Output is bit-exact against the
-reference (checked by the tests; the bench checks the first three pictures of every
-stream against the oracle before timing, chaining the oracle's own outputs as references).
+reference (checked by the tests; before timing, the bench checks every picture of the GOP
+chain of every stream against the oracle, chaining the oracle's own outputs as references).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -164,6 +164,34 @@ def gop_sequence(gop, frames):
     by position: the CPU arms' work list (every picture reads the stream's initial slots,
     so the pictures are independent there; the work per picture is the same)."""
     return [(gop_picture(s, n), s[2]) for n in range(frames) for s in gop]
+
+
+def verify_gop_chain(hb, check, gop, sts, frame_jobs, frames):
+    """Every picture of every stream of a GOP, reconstructed batch by batch in decode order,
+    against the oracle's chain (each oracle picture predicted from the oracle's own earlier
+    outputs).  Returns the list of mismatches (empty when bit-exact)."""
+    import hashlib
+    from concurrent.futures import ThreadPoolExecutor
+
+    def oracle_chain(i):
+        dpb = list(gop[i][2])
+        out = []
+        for n in range(frames):
+            dpb[n % SLOTS] = check.reconstruct_picture(gop_picture(gop[i], n), dpb)
+            out.append(hashlib.md5(dpb[n % SLOTS].tobytes()).hexdigest())
+        return out
+
+    with ThreadPoolExecutor(max_workers=len(gop)) as ex:
+        want = list(ex.map(oracle_chain, range(len(gop))))
+    errs = []
+    buf = None
+    for n in range(frames):
+        hb.batch_launch(frame_jobs(n), [n % SLOTS] * len(gop))
+        for i, st in enumerate(sts):
+            buf = st.download(n % SLOTS, buf)
+            if hashlib.md5(buf.tobytes()).hexdigest() != want[i][n]:
+                errs.append(f"stream {i} picture {n} differs from the oracle")
+    return errs
 
 
 def algorithmic_bytes(hb, pic):
@@ -432,26 +460,9 @@ def run_ours(args, hb, rank, world, local):
         ctx.sync()
         return None
 
-    # the first three pictures of every stream against the oracle, each picture predicted
-    # from the oracle's own earlier outputs
-    verify_n = min(3, F)
-    for n in range(verify_n):
-        hb.batch_launch(frame_jobs(n), [n % SLOTS] * G)
-    ctx.sync()
-    from concurrent.futures import ThreadPoolExecutor
-
-    def verify_stream(i):
-        dpb = list(gop[i][2])
-        for n in range(verify_n):
-            dpb[n % SLOTS] = check.reconstruct_picture(gop_picture(gop[i], n), dpb)
-        for n in range(verify_n):
-            got = gop_streams[i].download(n % SLOTS)
-            if not np.array_equal(got, dpb[n % SLOTS]):
-                return f"stream {i} picture {n} differs from the oracle in {int((got != dpb[n % SLOTS]).sum())} samples"
-        return None
-
-    with ThreadPoolExecutor(max_workers=G) as ex:
-        errs = [e for e in ex.map(verify_stream, range(G)) if e]
+    # every picture of the GOP chain of every stream against the oracle, each predicted from
+    # the oracle's own earlier outputs
+    errs = verify_gop_chain(hb, check, gop, gop_streams, frame_jobs, F)
     if errs:
         raise SystemExit("bench: " + errs[0])
 

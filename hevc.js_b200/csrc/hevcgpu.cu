@@ -1510,12 +1510,25 @@ constexpr size_t STATIC_SCRATCH_BYTES = STATIC_LISTS_OFF + (size_t)HEVCGPU_STATI
 
 static __device__ __align__(256) uint8_t g_static_scratch[STATIC_SCRATCH_BYTES];
 
-// Host side: the per-size lists are built in a static array, and one lock serialises
-// whole calls, since every call on a device shares the one scratch array.
-constexpr int STATIC_MAX_DEVICES = 64;
-std::mutex g_static_mu;
-uint8_t* g_static_dev[STATIC_MAX_DEVICES];  // scratch address per device, set by the first call
-int32_t g_static_lists[HEVCGPU_STATIC_MAX_TUS];
+// Host side, per device: a lock that serialises whole calls (every call on a device
+// shares that device's scratch array), the scratch address looked up by the device's
+// first call, and the static array the per-size lists are built in.  Calls on different
+// devices run side by side.
+constexpr int STATIC_MAX_DEVICES = 16;
+struct StaticDevice {
+    std::mutex mu;
+    uint8_t* base = nullptr;
+    int32_t lists[HEVCGPU_STATIC_MAX_TUS];
+};
+StaticDevice g_static[STATIC_MAX_DEVICES];
+
+// Waits for the calling stream when it goes out of scope, so that a call leaving early
+// after queuing copies or kernels still releases its device's lock only once they are done
+// with the scratch.
+struct SyncOnExit {
+    cudaStream_t stream;
+    ~SyncOnExit() { cudaStreamSynchronize(stream); }
+};
 
 // The buffer must be device (or managed) memory of this device.
 int check_device_buffer(const void* p, int device, const char* what) {
@@ -1561,22 +1574,24 @@ int hevcgpu_residual_blocks_static(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int
                         t.coeff_offset);
     }
 
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    uint8_t*& base = g_static_dev[ctx->device];
+    StaticDevice& sd = g_static[ctx->device];
+    std::lock_guard<std::mutex> lock(sd.mu);
+    uint8_t*& base = sd.base;
     if (!base) {
         // first call on this device (its device is current): look up the scratch address
         void* p = nullptr;
         CUDA_TRY(cudaGetSymbolAddress(&p, g_static_scratch));
         base = static_cast<uint8_t*>(p);
     }
+    const SyncOnExit drained{ctx->stream};   // declared after the lock: runs before it is released
 
-    // per-size lists of TU indices, back to back in g_static_lists
+    // per-size lists of TU indices, back to back in the device's list array
     int32_t count[4] = {0, 0, 0, 0}, start[4];
     for (int i = 0; i < num_tus; i++) count[tus[i].log2_size - 2]++;
     start[0] = 0;
     for (int k = 1; k < 4; k++) start[k] = start[k - 1] + count[k - 1];
     int32_t fill[4] = {start[0], start[1], start[2], start[3]};
-    for (int i = 0; i < num_tus; i++) g_static_lists[fill[tus[i].log2_size - 2]++] = i;
+    for (int i = 0; i < num_tus; i++) sd.lists[fill[tus[i].log2_size - 2]++] = i;
 
     PicDesc D;
     std::memset(&D, 0, sizeof(D));
@@ -1588,7 +1603,7 @@ int hevcgpu_residual_blocks_static(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int
     CUDA_TRY(cudaMemcpyAsync(base, &D, sizeof(D), cudaMemcpyHostToDevice, ctx->stream));
     CUDA_TRY(cudaMemcpyAsync(base + STATIC_TUS_OFF, tus, sizeof(hevc_tu_t) * (size_t)num_tus,
                              cudaMemcpyHostToDevice, ctx->stream));
-    CUDA_TRY(cudaMemcpyAsync(base + STATIC_LISTS_OFF, g_static_lists, sizeof(int32_t) * (size_t)num_tus,
+    CUDA_TRY(cudaMemcpyAsync(base + STATIC_LISTS_OFF, sd.lists, sizeof(int32_t) * (size_t)num_tus,
                              cudaMemcpyHostToDevice, ctx->stream));
 
     Launcher L{ctx, ctx->stream};
@@ -1606,7 +1621,8 @@ int hevcgpu_residual_blocks_static(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int
         if ((rc = L.go(kr[k], dim3((count[k] + per_block - 1) / per_block), dim3(128), t, (int)RES_PACKED)))
             return rc;
     }
-    // the lock is held until the kernels are done with the scratch
+    // the lock is held until the kernels are done with the scratch (and `drained` waits
+    // again on the way out of every earlier return)
     CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return HEVCGPU_OK;
 }

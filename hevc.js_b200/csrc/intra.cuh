@@ -410,7 +410,10 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
             if (v < n_k) got = v;
             else k = k + 1 == st.n ? 0 : k + 1;
         }
-        s_ticket = got;
+        // a wait of this launch (or an earlier one not yet read) gave up: the CTU could only
+        // wait for work that will not come, so the CTA ends at once
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> status(*sticky);
+        s_ticket = (status.load(cuda::memory_order_relaxed) & ST_TIMEOUT) ? -1 : got;
         s_pic = k;
         s_abort = 0;
     }
@@ -479,11 +482,18 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
                     unsigned long long t0 = 0;
                     int v;
                     for (unsigned polls = 0; (v = done.load(cuda::memory_order_acquire)) < (stamp | need); polls++) {
-                        if ((polls & 255u) == 0) {   // the timer, every 256 polls
+                        if ((polls & 255u) == 0) {   // the timer and the status word, every 256 polls
                             const unsigned long long now = global_ns();
                             if (polls == 0) t0 = now;
                             if (now - t0 > WAIT_LIMIT_NS || polls >= SPIN_LIMIT) {
                                 atomicOr(sticky, ST_TIMEOUT);
+                                s_abort = 1;
+                                break;
+                            }
+                            // another CTU's wait gave up (maybe the one this CTU waits for):
+                            // stop now rather than after a full limit of its own
+                            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> status(*sticky);
+                            if (status.load(cuda::memory_order_relaxed) & ST_TIMEOUT) {
                                 s_abort = 1;
                                 break;
                             }

@@ -386,17 +386,18 @@ int  hevcgpu_picture_decode(hevcgpu_stream_t* st, const hevc_picture_syntax_t* s
                             int32_t dst_slot);
 
 /* Residual blocks with no allocation.  No counterpart in the reference: same blocks and
- * results as hevcgpu_residual_blocks, for callers that must not allocate while decoding
- * (a serving process that sized its device memory once at start-up; decode threads on
- * which cudaMalloc/cudaFree would synchronise the device and stall other streams).
- * tus is a host array; d_coeffs (num_coeffs int16 levels), d_pred and d_out (num_coeffs
- * bytes each) are caller-owned DEVICE buffers of ctx's device, 16-byte aligned.  The
- * call allocates no memory: its scratch is a fixed static device array sized for
- * HEVCGPU_STATIC_MAX_TUS blocks, and more blocks are rejected with HEVCGPU_EINVAL.
- * Runs on ctx's stream and returns once d_out is written.  The first call on each
- * device looks up the scratch address (and may load the module on that device): make
- * it before any stream capture begins.  All calls share the scratch of their device,
- * so a process-wide lock serialises them. */
+ * results as hevcgpu_residual_blocks (flat dequantisation: scaling lists are not offered
+ * here), for callers that must not allocate while decoding (a serving process that sized
+ * its device memory once at start-up; decode threads on which cudaMalloc/cudaFree would
+ * synchronise the device and stall other streams).  tus is a host array; d_coeffs
+ * (num_coeffs int16 levels), d_pred and d_out (num_coeffs bytes each) are caller-owned
+ * DEVICE buffers of ctx's device, 16-byte aligned.  The call allocates no memory: its
+ * scratch is a fixed static device array sized for HEVCGPU_STATIC_MAX_TUS blocks, and more
+ * blocks are rejected with HEVCGPU_EINVAL; so are devices numbered 16 and above.  Runs on
+ * ctx's stream and returns once d_out is written.  The first call on each device looks up
+ * the scratch address (and may load the module on that device): make it before any stream
+ * capture begins.  All calls on one device share that device's scratch, so a lock per
+ * device serialises them; calls on different devices do not wait for each other. */
 #define HEVCGPU_STATIC_MAX_TUS 65536
 int  hevcgpu_residual_blocks_static(hevcgpu_ctx_t* ctx, const hevc_tu_t* tus, int32_t num_tus,
                                     const int16_t* d_coeffs, uint64_t num_coeffs,

@@ -241,6 +241,32 @@ def test_bounded_wait_times_out_and_the_context_recovers(hb, gpu_ctx, port):
     j.free()
 
 
+def test_bounded_wait_gives_up_once_on_a_large_picture(hb, gpu_ctx, port):
+    """A 1080p all-intra picture with 16x16 CTBs (8160 CTUs, many more than the launch holds
+    resident): when the first CTU's wait gives up, the CTUs that wait behind it, and the CTAs
+    that start after it, see the status word and end at once instead of each running out a
+    second of their own.  The context then decodes the picture correctly."""
+    import time
+    w, h, seed = 1920, 1080, 98
+    st = gpu_ctx.open_stream(w, h, 3)
+    pic = hb.Picture(hb.default_cfg(w, h, seed, slice_type=2, log2_ctb=4))
+    job = st.prepare(pic)
+    job.plant_unmet_wait()
+    t0 = time.perf_counter()
+    job.launch(2)
+    with pytest.raises(hb.HevcGpuError) as e:
+        st.sync()
+    waited = time.perf_counter() - t0
+    assert e.value.code == hb.abi.HEVCGPU_ETIMEOUT
+    assert 0.5 < waited < 5.0
+    job.free()
+    fresh = st.prepare(pic)
+    fresh.launch(2)
+    st.sync()
+    assert _diff(st.download(2), port.reconstruct_picture(pic, [])) == 0
+    fresh.free()
+
+
 def test_frame_output_cropped_16bit(hb, gpu_ctx, port):
     """hevcgpu_slot_download_frame gives the reconstructed picture inside the conformance
     window as 16-bit planes, as hevc_decoder_get_frame does (hevc_api.cpp:49-77)."""
@@ -456,3 +482,21 @@ def test_gpu_reconstructs_recorded_real_streams(hb, gpu_ctx):
             assert hashlib.md5(st.download(k).tobytes()).hexdigest() == want[name]["md5"][k], (name, k)
             job.free()
         st.close()
+
+
+def test_gpu_full_gop_chain_1080p(hb, gpu_ctx, port):
+    """Two streams of the bench's GOP workload (1920x1080, an I picture then 59 P/B pictures,
+    each predicted from the two before it in a 3-slot DPB ring), batched as the bench runs
+    them: every one of the 120 pictures equals the oracle's chain."""
+    import bench
+    gop = bench.make_gop(hb, 2, 1920, 1080, 4242)
+    sts = []
+    for _, _, init in gop:
+        st = gpu_ctx.open_stream(1920, 1080, bench.SLOTS)
+        for s in range(bench.SLOTS):
+            st.upload(s, init[s])
+        sts.append(st)
+    jobs_i = [st.prepare(g[0]) for st, g in zip(sts, gop)]
+    jobs_pb = [[st.prepare(g[1][ph]) for st, g in zip(sts, gop)] for ph in range(bench.SLOTS)]
+    errs = bench.verify_gop_chain(hb, port, gop, sts, lambda n: jobs_i if n == 0 else jobs_pb[n % bench.SLOTS], 60)
+    assert not errs, errs[:4]

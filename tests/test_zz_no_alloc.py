@@ -70,3 +70,37 @@ def test_static_rejects_host_buffers(hb, gpu_ctx):
     out = np.zeros_like(pred)
     rc = f(gpu_ctx.h, tus, n, coeffs.ctypes.data, coeffs.size, pred.ctypes.data, out.ctypes.data)
     assert rc == abi.HEVCGPU_EINVAL
+
+
+def test_static_block_ending_at_the_pool_end(hb, gpu_ctx):
+    """The last block's levels end exactly at num_coeffs (accepted, same bytes); one level
+    fewer in the pool is refused."""
+    import torch
+    from hevc_b200 import abi
+    lib, f = _static_fn(hb)
+    tus, n, coeffs, pred = hb.blocks(300, 76)
+    ends = [tus[i].coeff_offset + (1 << (2 * tus[i].log2_size)) for i in range(n)]
+    assert max(ends) == coeffs.size
+    assert np.array_equal(_run_static(hb, gpu_ctx, f, tus, n, coeffs, pred), gpu_ctx.residual_blocks(tus, n, coeffs, pred))
+    dev = torch.device("cuda", 0)
+    d_coeffs = torch.from_numpy(coeffs).to(dev)
+    d_pred = torch.from_numpy(pred).to(dev)
+    d_out = torch.zeros(pred.size, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    rc = f(gpu_ctx.h, tus, n, d_coeffs.data_ptr(), coeffs.size - 1, d_pred.data_ptr(), d_out.data_ptr())
+    assert rc == abi.HEVCGPU_EINVAL
+
+
+def test_static_rejects_unaligned_device_buffers(hb, gpu_ctx):
+    import torch
+    from hevc_b200 import abi
+    lib, f = _static_fn(hb)
+    tus, n, coeffs, pred = hb.blocks(16, 77)
+    dev = torch.device("cuda", 0)
+    d_coeffs = torch.zeros(coeffs.size + 8, dtype=torch.int16, device=dev)
+    d_pred = torch.from_numpy(pred).to(dev)
+    d_out = torch.zeros(pred.size, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    rc = f(gpu_ctx.h, tus, n, d_coeffs.data_ptr() + 2, coeffs.size, d_pred.data_ptr(), d_out.data_ptr())
+    assert rc == abi.HEVCGPU_EINVAL
+    assert b"aligned" in lib.hevcgpu_last_error()
