@@ -21,21 +21,16 @@ struct MotionEnt {           // 4x4 motion grid entry (PUMotionInfo, inter_predi
 };
 static_assert(sizeof(MotionEnt) == 12, "MotionEnt is written as three words by the MC kernel");
 
-// One level of an intra CTU task, packed in 8 bytes (staged into shared memory):
-// req(d) > 0 means "dependency slot d must have completed req(d) levels before this level
-// runs" (only where the requirement rises); publish means other CTUs wait for this level's
-// completion; end is the first task entry of the next level, counted from the CTU's first.
-// Fields of 10 bits: x = req(0) | req(1) << 10 | req(2) << 20 | publish << 31,
-// y = req(3) | end << 10.
-struct IntraLevel {
-    uint32_t x, y;
-};
-constexpr uint32_t INTRA_LEVEL_PUBLISH = 0x80000000u;
-constexpr int INTRA_FIELD_MAX = 1023;
-__host__ __device__ __forceinline__ int intra_req(const IntraLevel& e, int d) {
-    return (int)((d < 3 ? e.x >> (10 * d) : e.y) & 0x3FFu);
-}
-__host__ __device__ __forceinline__ int intra_end(const IntraLevel& e) { return (int)((e.y >> 10) & 0x3FFu); }
+// Intra schedule entries.  Each intra TU in task order has a dependency list: entries
+// without INTRA_DEP_EXTERNAL name a TU of the same CTU by its task index counted from the
+// CTU's first; entries with it name a TU of an earlier CTU of the picture by its task
+// index in the picture (only a planted test wait is left in that form: the host turns
+// each into INTRA_DEP_WATCH | the slot of the CTU's watch list that holds that TU).  A TU
+// that some other CTU depends on carries ITU_PUBLISH in reserved[0] of its task-order
+// record and publishes its completion in itu_done.
+constexpr uint32_t INTRA_DEP_EXTERNAL = 0x80000000u;
+constexpr uint32_t INTRA_DEP_WATCH = 0x40000000u;   // | watch slot of the CTU (see ictu_watch)
+constexpr uint8_t ITU_PUBLISH = 1u;
 
 struct PicDesc {
     int32_t width, height;               // luma
@@ -58,19 +53,22 @@ struct PicDesc {
     const uint16_t* ctb_tile;            // may be null
     const hevc_slice_t* slices;
     const hevc_scaling_t* scaling;       // scaling lists, or null for flat scaling
-    // intra CTU tasks (intra.cuh): the CTUs that hold intra TUs, raster order, and their
-    // TUs ordered by level of the CTU-local dependency DAG
+    // intra CTU tasks (intra.cuh): the CTUs that hold intra TUs in wavefront order (key
+    // 2 * row + column), and their TUs ordered by level of the CTU-local dependency DAG
+    // (task order)
     const int32_t* ictu_addr;            // raster address of intra CTU k
-    const int32_t* ictu_deps;            // 4 per intra CTU: intra CTUs it reads from, or -1
-    const int32_t* ictu_tu_off;          // TUs of intra CTU k: itu[ictu_tu_off[k] .. [k+1])
+    const int32_t* ictu_tu_off;          // TUs of intra CTU k: task entries [ictu_tu_off[k], [k+1])
     const hevc_tu_t* itu_rec;            // TU records in task order; coeff_offset holds the
-                                         // offset of the TU's residual in the CTU's staged ones
+                                         // offset of the TU's residual in the CTU's staged ones,
+                                         // reserved[0] ITU_PUBLISH
     const int4* itu_res;                 // per task entry: residual source offset (-1: none),
                                          // offset in the CTU's staged residuals, 16-byte chunks
-    const int32_t* ictu_lvl_off;         // levels of intra CTU k: ictu_lvl[ictu_lvl_off[k] ..]
-    const IntraLevel* ictu_lvl;
-    int32_t* ictu_done;                  // per intra CTU: (epoch << 16) | levels completed
-    int32_t n_ictu;
+    const uint32_t* itu_dep;             // per task entry: (offset in dep_list << 6) | count
+    const uint32_t* dep_list;            // dependency entries (INTRA_DEP_EXTERNAL | index)
+    int32_t* itu_done;                   // per task entry: epoch of the launch that completed it
+    const uint32_t* ictu_watch;          // per intra CTU: (offset in watch << 8) | count
+    const uint32_t* watch;               // TUs of other CTUs each CTU waits for (task indices)
+    int32_t n_ictu, n_itu;
     int32_t num_pus;
     int32_t num_slices;
     int32_t log2_ctb, wctb, hctb;

@@ -409,6 +409,7 @@ struct hevcgpu_job {
     int32_t n_mc[2] = {0, 0};            // luma strips, chroma strips (mc.cuh items)
     const uint32_t* d_mc[2] = {nullptr, nullptr};
     int32_t n_ictu = 0;                 // CTUs that hold intra TUs
+    uint32_t spare_dep = 0;             // dependency list entry kept for the planted wait
     int32_t epoch = 0;                  // intra launches of this job so far
     int32_t n_pus = 0;
     int has_intra = 0;
@@ -575,21 +576,18 @@ enum StageMask : int {
 // and no first-touch page faults per picture.
 struct BuildScratch {
     std::vector<int32_t> bins[4], intra_list, itu, level, ctu_of, order;
-    // intra owner maps, one word per 4x4 unit: (generation << 40) | (CTU address << 16) |
-    // level.  An entry is valid when its generation is this picture's, so the maps need no
+    // intra owner maps, one word per 4x4 unit: (generation << 40) | decode-order index of the
+    // intra TU.  An entry is valid when its generation is this picture's, so the maps need no
     // clearing between pictures.
     std::vector<uint64_t> owner[3];
     uint32_t gen = 0;
     std::vector<hevc_tu_t> itu_rec;
     std::vector<int4> itu_res;
     // intra schedule
-    struct Req { int32_t a, lv, dep, need; };
-    std::vector<Req> reqs;
-    std::vector<int32_t> dep_list, dep_n, index_of, nlev, cnt;
-    std::vector<int32_t> ictu_addr, ictu_deps, ictu_tu_off, ictu_lvl_off;
-    std::vector<IntraLevel> ictu_lvl;
-    std::vector<std::array<uint16_t, 4>> req;
-    std::vector<uint8_t> publish;
+    std::vector<int32_t> dep_at, deps, pos, cnt;
+    std::vector<std::pair<int64_t, int32_t>> runs;   // (wavefront key, first TU) of each CTU's run
+    std::vector<int32_t> ictu_addr, ictu_tu_off, slot_of;
+    std::vector<uint32_t> itu_dep, dep_out, watch, ictu_watch;
     std::vector<uint32_t> mc[2];
     std::vector<uint8_t> mc_cls;
 };
@@ -685,45 +683,42 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     j->has_intra = !intra_list.empty();
     // Intra schedule.  Per plane an owner map at 4-sample granularity records the latest
     // intra TU written there; intra TU B reads the units of its reference row
-    // (x-1 .. x+2N-1 at y-1) and column (y .. y+2N-1 at x-1).  An owner in B's CTU puts B
-    // one level above it in the CTU-local DAG; an owner in another CTU makes B's CTU wait
-    // for that CTU.  A unit whose samples B may not use (availability) can only add an
-    // unneeded level or wait, never change a sample; owners in CTUs later in raster order
-    // (decoded earlier only in tile scan) are never available and add nothing.
+    // (x-1 .. x+2N-1 at y-1) and column (y .. y+2N-1 at x-1).  Each distinct owner is a
+    // dependency of B: an owner in B's CTU is a local one (B is one level above it in the
+    // CTU-local DAG, which orders the CTU's tasks), an owner in an earlier CTU an external
+    // one.  A unit whose samples B may not use (availability) can only add an unneeded wait,
+    // never change a sample; owners in CTUs later in raster order (decoded earlier only in
+    // tile scan) are never available and add nothing.
     const int n_intra = (int)intra_list.size();
     auto& ictu_addr = BS.ictu_addr;
-    auto& ictu_deps = BS.ictu_deps;
     auto& ictu_tu_off = BS.ictu_tu_off;
-    auto& ictu_lvl_off = BS.ictu_lvl_off;
-    auto& ictu_lvl = BS.ictu_lvl;
     auto& itu = BS.itu;
     auto& itu_rec = BS.itu_rec;         // intra TU records in task order
     auto& itu_res = BS.itu_res;         // per task entry: residual source, staged offset, 16-byte chunks
+    auto& itu_dep = BS.itu_dep;         // per task entry: (dependency list offset << 6) | count
+    auto& dep_out = BS.dep_out;         // dependency lists in task order
+    auto& ictu_watch = BS.ictu_watch;   // per CTU: (offset in watch << 8) | count
     ictu_addr.clear();
-    ictu_deps.clear();
+    ictu_watch.clear();
+    BS.watch.clear();
     ictu_tu_off.clear();
-    ictu_lvl_off.clear();
-    ictu_lvl.clear();
     itu.clear();
     itu_rec.clear();
     itu_res.clear();
+    itu_dep.clear();
+    dep_out.clear();
     if (n_intra) {
         auto& level = BS.level;
         auto& ctu_of = BS.ctu_of;
+        auto& dep_at = BS.dep_at;       // decode order: first entry of TU b's owners in deps
+        auto& deps = BS.deps;           // decode-order indices of the owners, per TU
         level.resize((size_t)n_intra);
         ctu_of.resize((size_t)n_intra);
-        // up to 4 dependency CTU addresses per CTU address (dep_n counts past 4 to report)
-        auto& dep_list = BS.dep_list;
-        auto& dep_n = BS.dep_n;
-        dep_list.assign((size_t)nctb * 4, -1);
-        dep_n.assign((size_t)nctb, 0);
-        // cross-CTU requirements: (CTU, level, dependency CTU address, levels it must have
-        // done); the dependency publishes after level need - 1
-        auto& reqs = BS.reqs;
-        reqs.clear();
-        // owner maps: the CTU address and level of the latest intra TU per 4x4 unit, in words
-        // tagged with this picture's generation (a word of another generation: no owner).  The
-        // address takes 24 bits (an 8192 x 8192 picture of 16 x 16 CTBs has 2^18 CTUs).
+        dep_at.resize((size_t)n_intra + 1);
+        deps.clear();
+        deps.reserve((size_t)n_intra * 3);
+        // owner maps: the decode-order index of the latest intra TU per 4x4 unit, in words
+        // tagged with this picture's generation (a word of another generation: no owner)
         auto& owner = BS.owner;
         int uw[3], uh[3];
         if (++BS.gen == (1u << 24)) {   // wrapped: no old word may carry the new generation
@@ -738,98 +733,99 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
             const size_t nu = (size_t)uw[c] * uh[c];
             if (owner[c].size() < nu) owner[c].resize(nu, 0ull);
         }
-        reqs.reserve((size_t)n_intra);
         for (int b = 0; b < n_intra; b++) {
             const hevc_tu_t& t = s->tus[intra_list[(size_t)b]];
             const int c = t.c_idx, n = 1 << t.log2_size, sub = c ? 2 : 1;
             const int a = ((t.y * sub) >> p.log2_ctb) * wctb + ((t.x * sub) >> p.log2_ctb);
             ctu_of[(size_t)b] = a;
+            dep_at[(size_t)b] = (int32_t)deps.size();
             uint64_t* own = owner[c].data();
             const int row = uw[c];
-            const bool up = t.y > 0, left = t.x > 0;
-            const size_t rrow = up ? (size_t)((t.y - 1) / 4) * row : 0;
-            const int ux0 = left ? (t.x - 1) / 4 : 0, ux1 = std::min(row - 1, (t.x + 2 * n - 1) / 4);
-            const int lx = left ? (t.x - 1) / 4 : 0;
-            const int uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
-            // First pass, with no branch on the owners: the level from the owners in this CTU,
-            // and whether a unit has an owner in another CTU.
-            const uint64_t self = gtag | ((uint64_t)a << 16);
-            constexpr uint64_t OWNER_BITS = ~0xFFFFull;   // generation and CTU address
             int lv = 0;
-            bool other = false;
-            auto scan = [&](uint64_t o) {
-                const bool same = (o & OWNER_BITS) == self;
-                lv = std::max(lv, same ? (int)(o & 0xFFFF) + 1 : 0);
-                other |= ((o & GEN_BITS) == gtag) & !same;
+            uint64_t last = 0;   // a run of units with one owner adds what its first unit added
+            auto dep = [&](uint64_t o) {
+                if ((o & GEN_BITS) != gtag || o == last) return;
+                last = o;
+                const int32_t ob = (int32_t)(o & 0xFFFFFFFFull);
+                const int oa = ctu_of[(size_t)ob];
+                // a CTU later in raster order is never available to this one
+                // (intra_prediction.cpp:113); in tile scan one can be decoded earlier (the
+                // tile to the left, below-left), and waiting for it could wait for a CTA not
+                // yet started: CTAs take CTUs in raster order
+                if (oa > a) return;
+                for (size_t q = (size_t)dep_at[(size_t)b]; q < deps.size(); q++)
+                    if (deps[q] == ob) return;
+                deps.push_back(ob);
+                if (oa == a) lv = std::max(lv, level[(size_t)ob] + 1);
             };
-            if (up)
-                for (int ux = ux0; ux <= ux1; ux++) scan(own[rrow + ux]);
-            if (left)
-                for (int uy = uy0; uy <= uy1; uy++) scan(own[(size_t)uy * row + lx]);
-            if (lv > 0xFFFF) return fail(HEVCGPU_EINVAL, "intra dependency chain too deep in CTU %d", a);
-            level[(size_t)b] = lv;
-            if (other) {   // second pass, the same units in the same order: the other CTUs
-                uint64_t last = 0;   // a run of units with one owner adds what its first unit added
-                auto dep = [&](uint64_t o) {
-                    if ((o & GEN_BITS) != gtag || o == last) return;
-                    last = o;
-                    if ((o & OWNER_BITS) == self) return;
-                    const int oa = (int)((o >> 16) & 0xFFFFFF), ol = (int)(o & 0xFFFF);
-                    // a CTU later in raster order is never available to this one
-                    // (intra_prediction.cpp:113); in tile scan one can be decoded earlier
-                    // (the tile to the left, below-left), and waiting for it could wait
-                    // for a CTA not yet started: CTAs take CTUs in raster order
-                    if (oa > a) return;
-                    int32_t* dl = &dep_list[(size_t)a * 4];
-                    int32_t& dn = dep_n[(size_t)a];
-                    bool have = false;
-                    for (int q = 0; q < std::min<int32_t>(dn, 4); q++) have |= dl[q] == oa;
-                    if (!have) {
-                        if (dn < 4) dl[dn] = oa;
-                        dn++;
-                    }
-                    reqs.push_back({a, lv, oa, ol + 1});
-                };
-                if (up)
-                    for (int ux = ux0; ux <= ux1; ux++) dep(own[rrow + ux]);
-                if (left)
-                    for (int uy = uy0; uy <= uy1; uy++) dep(own[(size_t)uy * row + lx]);
+            if (t.y > 0) {
+                const size_t rrow = (size_t)((t.y - 1) / 4) * row;
+                const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(row - 1, (t.x + 2 * n - 1) / 4);
+                for (int ux = ux0; ux <= ux1; ux++) dep(own[rrow + ux]);
             }
-            const uint64_t mark = gtag | ((uint64_t)a << 16) | (uint64_t)lv;
+            if (t.x > 0) {
+                const int lx = (t.x - 1) / 4, uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
+                for (int uy = uy0; uy <= uy1; uy++) dep(own[(size_t)uy * row + lx]);
+            }
+            level[(size_t)b] = lv;
+            const uint64_t mark = gtag | (uint64_t)(uint32_t)b;
             for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++) {
                 uint64_t* r = own + (size_t)uy * row;
                 for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) r[ux] = mark;
             }
         }
-        for (int a = 0; a < nctb; a++)
-            if (dep_n[(size_t)a] > 4) return fail(HEVCGPU_EINVAL, "CTU %d depends on %d CTUs", a, dep_n[(size_t)a]);
-        // order by (CTU raster address, level, decode order): the TUs come CTU by CTU in
-        // decode order, so a counting sort by level within each CTU's run keeps it stable
+        dep_at[(size_t)n_intra] = (int32_t)deps.size();
+        // Task order: CTUs in wavefront order (key 2 * row + column, then raster), each
+        // CTU's TUs by level, then decode order.  CTAs take CTUs by ticket in this order, so
+        // the CTUs held by resident CTAs are those of the diagonal band the picture's
+        // dependencies advance along (a row trails the one above by two CTUs), not whole
+        // rows in raster order.  Every CTU a CTU reads from (left, above-left, above,
+        // above-right) has a smaller key, so a CTA only waits for CTUs taken before its own.
+        auto wave = [&](int a) { return (int64_t)(2 * (a / wctb) + a % wctb) * nctb + a; };
         auto& order = BS.order;
         order.resize((size_t)n_intra);
-        bool grouped = true;
-        for (int b = 1; b < n_intra && grouped; b++) grouped = ctu_of[(size_t)b] >= ctu_of[(size_t)b - 1];
-        if (grouped) {
-            auto& cnt = BS.cnt;
-            for (int r0 = 0; r0 < n_intra;) {
-                int r1 = r0, maxl = 0;
-                while (r1 < n_intra && ctu_of[(size_t)r1] == ctu_of[(size_t)r0]) maxl = std::max(maxl, level[(size_t)r1++]);
-                cnt.assign((size_t)maxl + 2, 0);
-                for (int b = r0; b < r1; b++) cnt[(size_t)level[(size_t)b] + 1]++;
-                for (int l = 1; l <= maxl + 1; l++) cnt[(size_t)l] += cnt[(size_t)l - 1];
-                for (int b = r0; b < r1; b++) order[(size_t)(r0 + cnt[(size_t)level[(size_t)b]]++)] = b;
-                r0 = r1;
+        bool grouped = true;   // the TUs come CTU by CTU (decode order without WPP threads)
+        auto& runs = BS.runs;
+        runs.clear();
+        for (int b = 0; b < n_intra; b++)
+            if (b == 0 || ctu_of[(size_t)b] != ctu_of[(size_t)b - 1]) runs.push_back({wave(ctu_of[(size_t)b]), b});
+        {   // a CTU must form a single run: no two runs with one key
+            const int nr = (int)runs.size();
+            runs.push_back({INT64_MAX, n_intra});
+            std::vector<std::pair<int64_t, int32_t>> sorted(runs.begin(), runs.end() - 1);
+            for (int q = 0; q < nr; q++) sorted[(size_t)q].second = q;
+            std::sort(sorted.begin(), sorted.end());
+            for (int q = 1; q < nr && grouped; q++) grouped = sorted[(size_t)q].first != sorted[(size_t)q - 1].first;
+            if (grouped) {
+                auto& cnt = BS.cnt;
+                int at = 0;
+                for (int q = 0; q < nr; q++) {
+                    const int rq = sorted[(size_t)q].second;
+                    const int r0 = runs[(size_t)rq].second, r1 = runs[(size_t)rq + 1].second;
+                    int maxl = 0;
+                    for (int b = r0; b < r1; b++) maxl = std::max(maxl, level[(size_t)b]);
+                    cnt.assign((size_t)maxl + 2, 0);
+                    for (int b = r0; b < r1; b++) cnt[(size_t)level[(size_t)b] + 1]++;
+                    for (int l = 1; l <= maxl + 1; l++) cnt[(size_t)l] += cnt[(size_t)l - 1];
+                    for (int b = r0; b < r1; b++) order[(size_t)(at + cnt[(size_t)level[(size_t)b]]++)] = b;
+                    at += r1 - r0;
+                }
             }
-        } else {
+        }
+        if (!grouped) {
             for (int b = 0; b < n_intra; b++) order[(size_t)b] = b;
             std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
-                if (ctu_of[(size_t)x] != ctu_of[(size_t)y]) return ctu_of[(size_t)x] < ctu_of[(size_t)y];
+                const int64_t wx = wave(ctu_of[(size_t)x]), wy = wave(ctu_of[(size_t)y]);
+                if (wx != wy) return wx < wy;
                 return level[(size_t)x] < level[(size_t)y];
             });
         }
+        auto& pos = BS.pos;   // decode order -> task order
+        pos.resize((size_t)n_intra);
         itu.resize((size_t)n_intra);
         for (int i = 0; i < n_intra; i++) {
             const int b = order[(size_t)i];
+            pos[(size_t)b] = i;
             itu[(size_t)i] = intra_list[(size_t)b];
             if (i == 0 || ctu_of[(size_t)b] != ctu_of[(size_t)order[(size_t)i - 1]]) {
                 ictu_addr.push_back(ctu_of[(size_t)b]);
@@ -838,83 +834,78 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
         }
         ictu_tu_off.push_back(n_intra);
         // residual offsets inside each CTU's staged residuals (coded TUs, in itu order); the
-        // task-order record carries its TU's offset there in coeff_offset
+        // task-order record carries its TU's offset there in coeff_offset, and in reserved[0]
+        // whether a TU of another CTU depends on it (it then publishes its completion)
         itu_res.assign((size_t)n_intra, make_int4(-1, 0, 0, 0));
         itu_rec.resize((size_t)n_intra);
+        itu_dep.resize((size_t)n_intra);
+        dep_out.reserve(deps.size() + 1);
         const int nic = (int)ictu_addr.size();
         for (int k = 0; k < nic; k++) {
             int acc = 0;
-            for (int i = ictu_tu_off[(size_t)k]; i < ictu_tu_off[(size_t)k + 1]; i++) {
+            const int t0 = ictu_tu_off[(size_t)k], t1 = ictu_tu_off[(size_t)k + 1];
+            if (t1 - t0 > IC_MAX_TUS)
+                return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", ictu_addr[(size_t)k]);
+            for (int i = t0; i < t1; i++) {
+                const int b = order[(size_t)i];
                 const hevc_tu_t& t = s->tus[itu[(size_t)i]];
                 hevc_tu_t& r = itu_rec[(size_t)i];
                 r = t;
                 r.coeff_offset = 0;
+                r.reserved[0] = 0;
+                const int d0 = dep_at[(size_t)b], d1 = dep_at[(size_t)b + 1];
+                itu_dep[(size_t)i] = ((uint32_t)dep_out.size() << 6) | (uint32_t)(d1 - d0);
+                for (int q = d0; q < d1; q++) {
+                    const int ob = deps[(size_t)q], oi = pos[(size_t)ob];
+                    dep_out.push_back(ctu_of[(size_t)ob] == ctu_of[(size_t)b] ? (uint32_t)(oi - t0)
+                                                                              : (INTRA_DEP_EXTERNAL | (uint32_t)oi));
+                }
                 if (!(t.flags & HEVC_TU_CODED)) continue;
                 const int nn = 1 << (2 * t.log2_size);
                 itu_res[(size_t)i] = make_int4((int)t.coeff_offset, acc, nn / 8, 0);
                 r.coeff_offset = (uint32_t)acc;
                 acc += nn;
             }
-            if (acc > IC_MAX_RES || ictu_tu_off[(size_t)k + 1] - ictu_tu_off[(size_t)k] > IC_MAX_TUS)
+            if (acc > IC_MAX_RES)
                 return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", ictu_addr[(size_t)k]);
         }
-        // dependencies by intra-CTU index (earlier CTUs in raster order: at most left,
-        // above-left, above and above-right)
-        auto& index_of = BS.index_of;
-        index_of.assign((size_t)nctb, -1);
-        for (int k = 0; k < nic; k++) index_of[(size_t)ictu_addr[(size_t)k]] = k;
-        ictu_deps.assign((size_t)nic * 4, -1);
+        // External dependencies go through the CTU's watcher: per CTU, the distinct TUs of
+        // other CTUs its TUs depend on, in the order their first dependent TU comes, each with
+        // a watch slot; the dependency entry names the slot (INTRA_DEP_WATCH).  Those TUs
+        // publish their completion.
+        auto& watch = BS.watch;
+        auto& slot_of = BS.slot_of;   // (CTU index << 8 | slot) of a watched TU, per task entry
+        watch.clear();
+        ictu_watch.assign((size_t)nic, 0u);
+        slot_of.assign((size_t)n_intra, -1);
         for (int k = 0; k < nic; k++) {
-            const size_t a = (size_t)ictu_addr[(size_t)k];
-            for (int q = 0; q < dep_n[a]; q++) ictu_deps[(size_t)k * 4 + q] = index_of[(size_t)dep_list[a * 4 + q]];
-        }
-        // per CTU level: the levels each dependency slot must have completed before it runs
-        // (only where the requirement rises) and whether dependents wait for its completion
-        ictu_lvl_off.resize((size_t)nic + 1);
-        auto& nlev = BS.nlev;
-        nlev.resize((size_t)nic);
-        for (int k = 0; k < nic; k++) {
-            const int last = ictu_tu_off[(size_t)k + 1] - 1;
-            nlev[(size_t)k] = level[(size_t)order[(size_t)last]] + 1;
-            ictu_lvl_off[(size_t)k] = k ? ictu_lvl_off[(size_t)k - 1] + nlev[(size_t)k - 1] : 0;
-        }
-        ictu_lvl_off[(size_t)nic] = nic ? ictu_lvl_off[(size_t)nic - 1] + nlev[(size_t)nic - 1] : 0;
-        const size_t nlv = (size_t)ictu_lvl_off[(size_t)nic];
-        auto& req = BS.req;
-        req.assign(nlv, std::array<uint16_t, 4>{0, 0, 0, 0});
-        auto& publish = BS.publish;   // by level entry: dependents wait for that level
-        publish.assign(nlv, 0);
-        for (const BuildScratch::Req& r : reqs) {
-            const int k = index_of[(size_t)r.a];
-            const int32_t* dl = &dep_list[(size_t)r.a * 4];
-            const int slot = (int)(std::find(dl, dl + dep_n[(size_t)r.a], r.dep) - dl);
-            uint16_t& q = req[(size_t)(ictu_lvl_off[(size_t)k] + r.lv)][(size_t)slot];
-            q = (uint16_t)std::max<int>(q, r.need);
-            publish[(size_t)(ictu_lvl_off[(size_t)index_of[(size_t)r.dep]] + r.need - 1)] = 1;
-        }
-        // one padding entry: the kernel stages levels in 16-byte pairs from an even entry
-        ictu_lvl.assign(nlv + 1, IntraLevel{0u, 0u});
-        for (int k = 0; k < nic; k++) {
-            uint16_t seen[4] = {0, 0, 0, 0};
-            const int t0 = ictu_tu_off[(size_t)k], t1 = ictu_tu_off[(size_t)k + 1];
-            int i = t0;
-            for (int L = 0; L < nlev[(size_t)k]; L++) {
-                const size_t e_at = (size_t)(ictu_lvl_off[(size_t)k] + L);
-                std::array<uint16_t, 4>& rq = req[e_at];
-                for (int q = 0; q < 4; q++) {
-                    if (rq[(size_t)q] > seen[q]) seen[q] = rq[(size_t)q];
-                    else rq[(size_t)q] = 0;   // already satisfied by an earlier check
+            const uint32_t w0 = (uint32_t)watch.size();
+            int nw = 0;
+            for (int i = ictu_tu_off[(size_t)k]; i < ictu_tu_off[(size_t)k + 1]; i++) {
+                const uint32_t dd = itu_dep[(size_t)i];
+                for (uint32_t q = dd >> 6; q < (dd >> 6) + (dd & 63u); q++) {
+                    uint32_t& e = dep_out[q];
+                    if (!(e & INTRA_DEP_EXTERNAL)) continue;
+                    const uint32_t g = e & ~INTRA_DEP_EXTERNAL;
+                    int32_t& so = slot_of[g];
+                    if (so < 0 || (so >> 8) != k) {
+                        if (nw == IC_MAX_WATCH)
+                            return fail(HEVCGPU_EINVAL, "CTU %d reads from more than %d intra TUs of other CTUs",
+                                        ictu_addr[(size_t)k], IC_MAX_WATCH);
+                        so = (k << 8) | nw++;
+                        watch.push_back(g);
+                        itu_rec[g].reserved[0] = ITU_PUBLISH;
+                    }
+                    e = INTRA_DEP_WATCH | (uint32_t)(so & 0xFF);
                 }
-                while (i < t1 && level[(size_t)order[(size_t)i]] == L) i++;
-                if (i - t0 > INTRA_FIELD_MAX || rq[0] > INTRA_FIELD_MAX || rq[1] > INTRA_FIELD_MAX ||
-                    rq[2] > INTRA_FIELD_MAX || rq[3] > INTRA_FIELD_MAX)
-                    return fail(HEVCGPU_EINVAL, "CTU %d intra schedule out of range", ictu_addr[(size_t)k]);
-                IntraLevel& e = ictu_lvl[e_at];
-                e.x = (uint32_t)rq[0] | ((uint32_t)rq[1] << 10) | ((uint32_t)rq[2] << 20);
-                e.y = (uint32_t)rq[3] | ((uint32_t)(i - t0) << 10);
-                if (publish[e_at]) e.x |= INTRA_LEVEL_PUBLISH;
             }
+            ictu_watch[(size_t)k] = (w0 << 8) | (uint32_t)nw;
         }
+        // one spare entry: an external dependency of task 0 on itself (the planted wait of
+        // hevcgpu_job_plant_unmet_wait points task 0's list at it)
+        j->spare_dep = (uint32_t)dep_out.size();
+        dep_out.push_back(INTRA_DEP_EXTERNAL | 0u);
+        if (dep_out.size() >= (1u << 26)) return fail(HEVCGPU_EINVAL, "intra dependency lists too long");
     }
     j->n_ictu = (int32_t)ictu_addr.size();
     // MC strips: 4 columns x up to 16 rows of one PU in one plane, one thread each; luma
@@ -987,7 +978,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     }
     j->n_pus = s->num_pus;
 
-    size_t o_wp, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc[2], o_ia, o_idp, o_ito, o_itu, o_iro, o_ilo, o_ilv;
+    size_t o_wp, o_sao, o_sl, o_ti, o_slices, o_res[4], o_mc[2], o_ia, o_idp, o_ito, o_itu, o_iro, o_dl, o_iw, o_wl;
     size_t o_scal = 0;
     hevc_slice_t dflt{0, 0, 0, 1};
     const bool scaled = s->scaling && (stages & (ST_RESID | ST_INTRA));
@@ -1002,12 +993,13 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
         for (int k = 0; k < 4; k++) o_res[k] = pk.add(bins[k].data(), sizeof(int32_t) * bins[k].size());
         for (int c = 0; c < 2; c++) o_mc[c] = pk.add(mc[c].data(), sizeof(uint32_t) * mc[c].size());
         o_ia = pk.add(ictu_addr.data(), sizeof(int32_t) * ictu_addr.size());
-        o_idp = pk.add(ictu_deps.data(), sizeof(int32_t) * ictu_deps.size());
         o_ito = pk.add(ictu_tu_off.data(), sizeof(int32_t) * ictu_tu_off.size());
         o_itu = pk.add(itu_rec.data(), sizeof(hevc_tu_t) * itu_rec.size());
         o_iro = pk.add(itu_res.data(), sizeof(int4) * itu_res.size());
-        o_ilo = pk.add(ictu_lvl_off.data(), sizeof(int32_t) * ictu_lvl_off.size());
-        o_ilv = pk.add(ictu_lvl.data(), sizeof(IntraLevel) * ictu_lvl.size());
+        o_idp = pk.add(itu_dep.data(), sizeof(uint32_t) * itu_dep.size());
+        o_dl = pk.add(dep_out.data(), sizeof(uint32_t) * dep_out.size());
+        o_iw = pk.add(ictu_watch.data(), sizeof(uint32_t) * ictu_watch.size());
+        o_wl = pk.add(BS.watch.data(), sizeof(uint32_t) * BS.watch.size());
     };
     Packer measure;
     pack(measure);
@@ -1025,7 +1017,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
 
     size_t resid_bytes = j->has_intra ? sizeof(int16_t) * (size_t)align_up((int64_t)s->num_coeffs, 128) : 0;
     size_t mot_bytes = (stages & ST_DEBLOCK) ? sizeof(MotionEnt) * (size_t)align_up((int64_t)gw * gh, 32) : 0;
-    size_t done_bytes = sizeof(int32_t) * ictu_addr.size();
+    size_t done_bytes = sizeof(int32_t) * (size_t)n_intra;
     rc = j->scratch.get(ctx, std::max<size_t>(resid_bytes + mot_bytes + done_bytes, 256));
     if (rc) return rc;
     rc = j->desc.get(ctx, sizeof(PicDesc));
@@ -1056,16 +1048,18 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     D.slices = reinterpret_cast<const hevc_slice_t*>(base + o_slices);
     D.scaling = scaled ? reinterpret_cast<const hevc_scaling_t*>(base + o_scal) : nullptr;
     D.ictu_addr = reinterpret_cast<const int32_t*>(base + o_ia);
-    D.ictu_deps = reinterpret_cast<const int32_t*>(base + o_idp);
     D.ictu_tu_off = reinterpret_cast<const int32_t*>(base + o_ito);
     D.itu_rec = reinterpret_cast<const hevc_tu_t*>(base + o_itu);
     D.itu_res = reinterpret_cast<const int4*>(base + o_iro);
-    D.ictu_lvl_off = reinterpret_cast<const int32_t*>(base + o_ilo);
-    D.ictu_lvl = reinterpret_cast<const IntraLevel*>(base + o_ilv);
-    D.ictu_done = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(j->scratch.p) + resid_bytes + mot_bytes);
+    D.itu_dep = reinterpret_cast<const uint32_t*>(base + o_idp);
+    D.dep_list = reinterpret_cast<const uint32_t*>(base + o_dl);
+    D.ictu_watch = reinterpret_cast<const uint32_t*>(base + o_iw);
+    D.watch = reinterpret_cast<const uint32_t*>(base + o_wl);
+    D.itu_done = reinterpret_cast<int32_t*>(static_cast<uint8_t*>(j->scratch.p) + resid_bytes + mot_bytes);
     D.n_ictu = (int32_t)ictu_addr.size();
+    D.n_itu = n_intra;
     // completion flags start below every epoch a launch can use
-    if (done_bytes) CUDA_TRY(cudaMemsetAsync(D.ictu_done, 0, done_bytes, ctx->stream));
+    if (done_bytes) CUDA_TRY(cudaMemsetAsync(D.itu_done, 0, done_bytes, ctx->stream));
     D.num_pus = s->num_pus;
     D.num_slices = std::max(1, (int)s->num_slices);
     D.log2_ctb = p.log2_ctb;
@@ -1263,10 +1257,10 @@ int run_stages(hevcgpu_ctx* ctx, const Exec& ex, hevcgpu_job* const* jobs, int n
                 Seg& sg = t.s[t.n++];
                 sg.pic = static_cast<const PicDesc*>(j->desc.p);
                 sg.aux0 = total;
-                // completion words are (epoch << 16) | levels; restart the epochs from zero
-                // flags before they would reach the sign bit
-                if (j->epoch >= 32767) {
-                    CUDA_TRY(cudaMemsetAsync(j->host_desc.ictu_done, 0, sizeof(int32_t) * (size_t)j->n_ictu,
+                // completion flags hold the epoch of the launch that set them; restart the
+                // epochs from zero flags before they would reach the sign bit
+                if (j->epoch >= 0x7FFFFFF0) {
+                    CUDA_TRY(cudaMemsetAsync(j->host_desc.itu_done, 0, sizeof(int32_t) * (size_t)j->host_desc.n_itu,
                                              ex.stream));
                     j->epoch = 0;
                 }
@@ -1870,18 +1864,14 @@ int hevcgpu_job_plant_unmet_wait(hevcgpu_job_t* job) {
     if (job->n_ictu <= 0) return fail(HEVCGPU_EINVAL, "the job has no intra CTU to plant a wait in");
     int rc = check_ctx(job->ctx);
     if (rc) return rc;
-    // The first intra CTU depends on no other.  It now names itself in dependency slot 0 and
-    // needs one completed level of it before its first level: a level only it could publish.
+    // Task 0 (the first TU of the first intra CTU) depends on nothing.  Its dependency list
+    // now is the job's spare entry: an external dependency on its own completion, which only
+    // it could publish.
     const PicDesc& D = job->host_desc;
     cudaStream_t s = job->ctx->stream;
-    IntraLevel e{};
-    const int32_t self = 0;
-    CUDA_TRY(cudaMemcpyAsync(&e, D.ictu_lvl, sizeof(e), cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    e.x = (e.x & ~0x3FFu) | 1u;
-    CUDA_TRY(cudaMemcpyAsync(const_cast<int32_t*>(D.ictu_deps), &self, sizeof(self), cudaMemcpyHostToDevice, s));
-    CUDA_TRY(cudaMemcpyAsync(const_cast<IntraLevel*>(D.ictu_lvl), &e, sizeof(e), cudaMemcpyHostToDevice, s));
-    CUDA_TRY(cudaStreamSynchronize(s));   // the copies read e and self before they go
+    const uint32_t e = (job->spare_dep << 6) | 1u;
+    CUDA_TRY(cudaMemcpyAsync(const_cast<uint32_t*>(D.itu_dep), &e, sizeof(e), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaStreamSynchronize(s));   // the copy read e before it goes
     return HEVCGPU_OK;
 }
 

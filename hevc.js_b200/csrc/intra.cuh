@@ -3,17 +3,17 @@
 //
 // Every intra TU reads reference samples left of and above it.  Those samples are final
 // when this stage runs, except where an earlier intra TU writes them (MC and the inter
-// residuals ran before).  The host turns that into two levels of schedule:
-//   - per CTU, a level for each intra TU in the DAG of the CTU's own intra TUs;
-//   - per CTU, the at most four earlier CTUs (left, above-left, above, above-right) whose
-//     intra TUs own samples it reads.
-// k_intra_ctus runs one CTA per CTU with intra TUs: it stages the CTU, its TU records and
-// residuals in shared memory, and runs the TUs level by level, one warp per TU; before a
-// level that reads samples of those CTUs it waits (bounded) until they have completed
-// the levels that write them, and reads such samples from the picture through L2.
-// Every wait gives up after WAIT_LIMIT_NS of the GPU's global timer (or SPIN_LIMIT polls,
-// should the timer not advance), sets ST_TIMEOUT in the context's sticky status word (the
-// host turns it into HEVCGPU_ETIMEOUT) and returns.
+// residuals ran before).  The host turns that into a dependency list per intra TU: the
+// TUs that write samples it reads, in its own CTU (local) or in an earlier CTU
+// (external), and orders each CTU's TUs by their level in the CTU-local DAG.
+// k_intra_ctus runs one CTA per CTU with intra TUs: it stages the CTU, its TU records,
+// dependency lists and residuals in shared memory; its warps take the TUs in order and run
+// each one once its dependencies are complete (one-arrival barriers in shared memory for
+// local ones, published flags in global memory for external ones), reading samples of
+// other CTUs from the picture through L2.  Every wait gives up after WAIT_LIMIT_NS of the
+// GPU's global timer (or SPIN_LIMIT polls, should the timer not advance), sets ST_TIMEOUT
+// in the context's sticky status word (the host turns it into HEVCGPU_ETIMEOUT) and
+// returns.
 #pragma once
 
 #include <cuda/atomic>
@@ -28,6 +28,15 @@ __constant__ int8_t c_intra_angle[35] = {0,   0,   32,  26,  21,  17,  13,  9,  
 __constant__ int16_t c_inv_angle[35] = {0,    0,    256, 315, 390, 482,  630,  910,  1638, 4096, 0,   4096,
                                         1638, 910,  630, 482, 390, 315,  256,  315,  390,  482,  630, 910,
                                         1638, 4096, 0,   4096, 1638, 910, 630, 482,  390,  315,  256};
+
+// The picture fields intra_tu reads, copied into shared memory once per CTA: reads of the
+// descriptor in global memory would go through L1, which every GPU-scope acquire on the SM
+// invalidates, and sit in each TU's chain of dependent loads.
+struct IntraPic {
+    uint8_t* rec;
+    int64_t off_cb, off_cr;
+    int32_t width, height, log2_ctb, pitch_y, pitch_c, intra_smoothing_disabled, strong_intra;
+};
 
 struct IntraWarpSmem {
     int16_t s[129];    // final references: bottom-left .. corner (index 2n) .. top-right
@@ -49,9 +58,9 @@ enum : uint32_t { NB_LEFT = 1u, NB_ABOVE_LEFT = 2u, NB_ABOVE = 4u, NB_ABOVE_RIGH
 // with one warp (perform_intra_prediction, then reconstruct_block's add and clip).
 // Reference samples come from the CTU tile; results go to the tile (for later TUs) and
 // the picture.  res is the TU's residual (null when it has none).
-template <int LOG2, bool CHROMA>
-__device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W,
-                                         const CtuTile& tile, uint32_t nb_mask, const int16_t* res) {
+template <int LOG2, bool CHROMA, typename Pic, typename Wait>
+__device__ __forceinline__ bool intra_tu(const Pic& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W,
+                                         const CtuTile& tile, uint32_t nb_mask, const int16_t* res, Wait&& wait) {
     constexpr int n = 1 << LOG2, sub = CHROMA ? 2 : 1;
     constexpr int total = 4 * n + 1, R = (total + 31) / 32;  // reference samples, lane rounds
     const int ci = t.c_idx;
@@ -68,13 +77,15 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
     //    earlier CTB of the same slice and tile, or in this CTB at a lower z-scan address
     //    of the 4x4 luma unit (intra_prediction.cpp:102-133).  Index i runs from the
     //    bottom-left sample (0) through the corner (2n) to the top-right one (4n).
+    //    Availability and the address of each sample depend on positions only, so they are
+    //    found before the wait for the TUs that write the samples; the loads follow it.
     uint32_t mask[R];
-    int val[R];
+    int val[R], where[R];   // where: tile index, or ~(picture offset) for samples of other CTUs
 #pragma unroll
     for (int r = 0; r < R; r++) {
         const int i = lane + 32 * r;
         bool ok = false;
-        int v = 0;
+        int at = 0;
         if (i < total) {
             int px, py;
             if (i < 2 * n) { px = xc - 1; py = yc + 2 * n - 1 - i; }
@@ -94,16 +105,21 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
                 } else {
                     ok = zorder16((uint32_t)((px * sub - ox) >> 2), (uint32_t)((py * sub - oy) >> 2)) < cur_z;
                 }
-                if (ok) {
-                    // samples of other CTUs come from the picture through L2 (those CTUs
-                    // published them before this level), this CTU's from the tile
-                    v = outside ? __ldcg(plane + (int64_t)py * pitch + px)
-                                : tile.t[(py - tile.y0) * tile.pitch + (px - tile.x0)];
-                }
+                if (ok) at = outside ? ~(py * pitch + px) : (py - tile.y0) * tile.pitch + (px - tile.x0);
             }
         }
-        val[r] = v;
+        where[r] = at;
         mask[r] = __ballot_sync(0xffffffffu, ok);
+    }
+    if (!wait()) return false;
+    // samples of other CTUs come from the picture through L2 (the TUs of those CTUs that
+    // write them have published their completion), this CTU's from the tile
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int at = where[r];
+        int v = 0;
+        if ((mask[r] >> lane) & 1u) v = at < 0 ? __ldcg(plane + ~at) : tile.t[at];
+        val[r] = v;
     }
     // Phases 2-4 keep the reference array in registers, element i in lane i % 32 of round
     // i / 32, and move elements between lanes with shuffles: fetch(a, j) gives every lane
@@ -237,7 +253,7 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
         cidx[j] = ((x + 1) * ang) >> 5;
         cfr[j] = ((x + 1) * ang) & 31;
     }
-#pragma unroll
+#pragma unroll 2
     for (int q = 0; q < G_PER_LANE; q++) {
         const int g = lane + 32 * q;
         if (g >= NG) break;
@@ -299,47 +315,54 @@ __device__ __forceinline__ void intra_tu(const PicDesc& P, const hevc_tu_t& t, i
         *reinterpret_cast<uint32_t*>(tile.t + (yc + y - tile.y0) * tile.pitch + (xc + x0 - tile.x0)) = w;
         *reinterpret_cast<uint32_t*>(plane + (int64_t)(yc + y) * pitch + xc + x0) = w;
     }
+    return true;
 }
 
-// Size/plane dispatch of intra_tu.
-__device__ __forceinline__ void intra_tu_any(const PicDesc& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W,
-                                             const CtuTile& tile, uint32_t nb_mask, const int16_t* res) {
+// Size/plane dispatch of intra_tu; false when the wait gave up.
+template <typename Pic, typename Wait>
+__device__ __forceinline__ bool intra_tu_any(const Pic& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W,
+                                             const CtuTile& tile, uint32_t nb_mask, const int16_t* res, Wait&& wait) {
     if (t.c_idx == 0) {
         switch (t.log2_size) {
-            case 2: intra_tu<2, false>(P, t, lane, W, tile, nb_mask, res); break;
-            case 3: intra_tu<3, false>(P, t, lane, W, tile, nb_mask, res); break;
-            case 4: intra_tu<4, false>(P, t, lane, W, tile, nb_mask, res); break;
-            default: intra_tu<5, false>(P, t, lane, W, tile, nb_mask, res); break;
+            case 2: return intra_tu<2, false>(P, t, lane, W, tile, nb_mask, res, wait);
+            case 3: return intra_tu<3, false>(P, t, lane, W, tile, nb_mask, res, wait);
+            case 4: return intra_tu<4, false>(P, t, lane, W, tile, nb_mask, res, wait);
+            default: return intra_tu<5, false>(P, t, lane, W, tile, nb_mask, res, wait);
         }
-    } else {
-        switch (t.log2_size) {
-            case 2: intra_tu<2, true>(P, t, lane, W, tile, nb_mask, res); break;
-            case 3: intra_tu<3, true>(P, t, lane, W, tile, nb_mask, res); break;
-            case 4: intra_tu<4, true>(P, t, lane, W, tile, nb_mask, res); break;
-            default: intra_tu<5, true>(P, t, lane, W, tile, nb_mask, res); break;
-        }
+    }
+    switch (t.log2_size) {
+        case 2: return intra_tu<2, true>(P, t, lane, W, tile, nb_mask, res, wait);
+        case 3: return intra_tu<3, true>(P, t, lane, W, tile, nb_mask, res, wait);
+        case 4: return intra_tu<4, true>(P, t, lane, W, tile, nb_mask, res, wait);
+        default: return intra_tu<5, true>(P, t, lane, W, tile, nb_mask, res, wait);
     }
 }
 
 // ---------------------------------------------------------------------------------------
-// CTU tasks.  One CTA per CTU that holds intra TUs.  CTAs take CTUs by ticket in raster
-// order per picture, the pictures of a launch side by side.  The CTA stages the CTU and its neighbourhood, its TU
-// records and their residuals in shared memory, then runs the TUs level by level of the
-// CTU-local dependency DAG (one warp per TU, a barrier between levels).  Dependencies on
-// the at most four earlier intra CTUs whose intra samples it reads (left, above-left,
-// above, above-right, found on the host) are per level: before a level the CTA waits
-// (bounded) until each such CTU has completed the levels that own those samples, so a
-// CTU starts while its neighbours are still running and the critical path is the TU
-// dependency chain, not a chain of whole CTUs.  Every wait is for a CTU with an earlier
-// ticket, which already holds a running CTA.
+// CTU tasks.  One CTA per CTU that holds intra TUs.  CTAs take CTUs by ticket in wavefront
+// order per picture (2 * row + column: the diagonal band along which a picture's
+// dependencies advance), the pictures of a launch side by side.  The CTA stages the CTU, its TU
+// records and their residuals in shared memory; then its warps take the TUs one at a time
+// in task order (the CTU-local DAG's levels, so every TU comes after the TUs it depends
+// on) and run each as soon as the TUs it reads from are complete: a TU of the same CTU
+// through its one-arrival barrier in shared memory, a TU of an earlier CTU through that
+// TU's published completion in global memory.  No barrier ties the warps together, so the
+// critical path is the chain of dependent TUs itself.  Every wait is for a TU taken
+// earlier, by this CTA or by a CTA holding an earlier ticket, which is already running;
+// every wait is bounded.  The CTA's last warp is its watcher: it alone polls the global
+// flags of the TUs of other CTUs, so the workers only wait on shared-memory barriers, which
+// suspend them without taking issue slots.
 // ---------------------------------------------------------------------------------------
-constexpr int IC_WARPS = 4;
+constexpr int IC_WARPS = 8;
 constexpr int IC_THREADS = 32 * IC_WARPS;
-constexpr int IC_PUBLISHER = 32 * (IC_WARPS - 1);    // lane 0 of the last warp
+constexpr int IC_MIN_BLOCKS = 3;
 constexpr int IC_LP = 64, IC_LH = 64;                // luma tile (the CTU): pitch, rows
 constexpr int IC_CP = 32, IC_CH = 32;                // chroma tiles
 constexpr int IC_MAX_TUS = 256 + 2 * 64;             // 4x4 TUs of a 64x64 CTU, all planes
 constexpr int IC_MAX_RES = 64 * 64 + 2 * 32 * 32;    // residual samples of a 64x64 CTU
+constexpr int IC_DEP_STAGE = 2048;                   // dependency entries staged per CTU
+constexpr int IC_MAX_WATCH = 128;                    // TUs of other CTUs a CTU waits for
+constexpr int IC_WATCHER = IC_WARPS - 1;             // the warp that watches them
 constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;   // a wait gives up after a second
 constexpr unsigned SPIN_LIMIT = 1u << 26;            // backstop: polls of at least 64 ns
 
@@ -357,6 +380,30 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// One-arrival barriers in shared memory, one per TU of the CTU: the warp that completes
+// the TU arrives (release), the warps whose TUs read its samples wait on phase 0 (acquire).
+// A waiting thread is suspended by the hardware until the phase completes or the time hint
+// runs out, so waiting warps take no issue slots from the working ones.
+__device__ __forceinline__ void mbar_init1(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.release.cta.shared::cta.b64 st, [%0];\n\t}" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(bar))
+                 : "memory");
+}
+// true once phase 0 of the barrier has completed; false when the time hint ran out first
+__device__ __forceinline__ bool mbar_try_wait0(uint64_t* bar) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], 0, %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"((uint32_t)__cvta_generic_to_shared(bar)), "r"(20000u)
+        : "memory");
+    return ok != 0;
 }
 
 // Copy plane c of CTU (rx, ry) into its tile with 16-byte copies (issued, not waited
@@ -386,20 +433,101 @@ __device__ __forceinline__ void stage_tile(const PicDesc& P, int c, int rx, int 
     }
 }
 
-__global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_constant__ SegTable st, int32_t* tickets,
-                                                           int total, uint32_t* sticky) {
+// The state one worker's wait for a TU's dependencies reads.
+struct IntraWait {
+    const uint32_t* s_dep;      // the CTU's staged dependency entries
+    const uint32_t* dep_list;   // all entries (those past the staged ones)
+    uint64_t* s_bar;            // completion barriers of the CTU's TUs
+    uint64_t* s_wbar;           // watch barriers
+    int32_t* itu_done;          // published completions (direct external entries)
+    uint32_t* sticky;
+    volatile int* s_abort;
+    int dfirst, doff, dcount, staged, task, n_watch, n_itu, epoch, lane;
+};
+
+// The wait for a TU's dependencies, between the position work and the loads of intra_tu:
+// each lane waits for the entries lane, lane + 32, ...  Local and watched entries wait on
+// shared-memory barriers; a direct external entry (only a planted test wait has one) polls
+// the published completion.  Every wait reads the global timer and gives up after
+// WAIT_LIMIT_NS (SPIN_LIMIT tries as a backstop), marking the sticky status; a wait also
+// ends when another warp of the CTA gave up (s_abort) or, for external waits, when a wait
+// anywhere did (the status word).  Not inlined: one copy serves every TU size, which keeps
+// the size-specialised TU code small in the instruction cache.
+__device__ __noinline__ bool intra_wait(const IntraWait& w) {
+    bool gave_up = false;
+    for (int q = w.lane; q < w.dcount && !gave_up; q += 32) {
+        const int at = w.doff + q;
+        const uint32_t e = at >= 0 && at < w.staged ? w.s_dep[at] : __ldg(&w.dep_list[w.dfirst + at]);
+        unsigned long long t0 = 0;
+        const bool watched = (e & INTRA_DEP_WATCH) != 0, local = !(e & (INTRA_DEP_EXTERNAL | INTRA_DEP_WATCH));
+        if ((local && e >= (uint32_t)w.task) || (watched && (int)(e & 0xFFu) >= w.n_watch)) {
+            atomicOr(w.sticky, ST_BAD_RECORD);   // not an earlier TU, or no such watch slot: refused
+            gave_up = true;
+        } else if (local || watched) {
+            uint64_t* bar = watched ? &w.s_wbar[e & 0xFFu] : &w.s_bar[e];
+            for (unsigned polls = 0; !mbar_try_wait0(bar); polls++) {
+                if (*w.s_abort) {
+                    gave_up = true;
+                    break;
+                }
+                const unsigned long long now = global_ns();
+                if (polls == 0) t0 = now;
+                if (now - t0 > WAIT_LIMIT_NS || polls >= SPIN_LIMIT) {
+                    atomicOr(w.sticky, ST_TIMEOUT);
+                    gave_up = true;
+                    break;
+                }
+            }
+        } else if ((e & ~INTRA_DEP_EXTERNAL) >= (uint32_t)w.n_itu) {
+            atomicOr(w.sticky, ST_BAD_RECORD);
+            gave_up = true;
+        } else {
+            cuda::atomic_ref<int32_t, cuda::thread_scope_device> f(w.itu_done[e & ~INTRA_DEP_EXTERNAL]);
+            for (unsigned polls = 0; f.load(cuda::memory_order_relaxed) != w.epoch; polls++) {
+                if ((polls & 255u) == 0) {   // the timer and the status words, every 256 polls
+                    const unsigned long long now = global_ns();
+                    if (polls == 0) t0 = now;
+                    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> status(*w.sticky);
+                    if (now - t0 > WAIT_LIMIT_NS || polls >= SPIN_LIMIT) {
+                        atomicOr(w.sticky, ST_TIMEOUT);
+                        gave_up = true;
+                        break;
+                    }
+                    if (*w.s_abort || (status.load(cuda::memory_order_relaxed) & ST_TIMEOUT)) {
+                        gave_up = true;
+                        break;
+                    }
+                }
+                __nanosleep(32);
+            }
+            if (!gave_up) cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
+        }
+    }
+    // the warp barrier orders each lane's acquires before every lane's reads of the samples;
+    // then every lane decides alike
+    __syncwarp();
+    return !__any_sync(0xffffffffu, gave_up);
+}
+
+__global__ void __launch_bounds__(IC_THREADS, IC_MIN_BLOCKS) k_intra_ctus(const __grid_constant__ SegTable st,
+                                                                       int32_t* tickets, int total, uint32_t* sticky) {
     __shared__ __align__(16) uint8_t t_luma[IC_LH * IC_LP];
     __shared__ __align__(16) uint8_t t_chroma[2][IC_CH * IC_CP];
     __shared__ __align__(16) hevc_tu_t s_tu[IC_MAX_TUS];
     __shared__ __align__(16) int16_t s_res[IC_MAX_RES];
     __shared__ IntraWarpSmem ws[IC_WARPS];
-    __shared__ __align__(16) IntraLevel s_lvl[IC_MAX_TUS + 2];   // the CTU's levels (from an even entry)
-    __shared__ int s_ticket, s_pic, s_abort;
-    __shared__ int s_seen[4];   // levels each dependency CTU was seen to have completed
+    __shared__ uint64_t s_bar[IC_MAX_TUS];    // completion of the CTU's TUs, by task index
+    __shared__ uint32_t s_itu_dep[IC_MAX_TUS];   // their dependency lists: (offset << 6) | count
+    __shared__ uint32_t s_dep[IC_DEP_STAGE];     // the CTU's dependency entries
+    __shared__ uint64_t s_wbar[IC_MAX_WATCH];    // completion of the watched TUs of other CTUs
+    __shared__ uint32_t s_watch[IC_MAX_WATCH];   // their task indices in the picture
+    __shared__ int s_ticket, s_pic, s_next;
+    __shared__ IntraPic s_ipic;
+    __shared__ volatile int s_abort;
     __shared__ uint32_t s_nb;
     const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
     if (tid == 0) {
-        // Each picture hands out its CTUs by ticket in raster order.  CTAs start at picture
+        // Each picture hands out its CTUs by ticket in wavefront order.  CTAs start at picture
         // blockIdx.x % n, so the pictures of a launch progress side by side; a picture whose
         // tickets are used up passes the CTA on.  There are as many CTAs as CTUs, so every
         // CTA finds one.
@@ -416,15 +544,28 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
         s_ticket = (status.load(cuda::memory_order_relaxed) & ST_TIMEOUT) ? -1 : got;
         s_pic = k;
         s_abort = 0;
+        s_next = 0;
     }
     __syncthreads();
     if (s_ticket < 0) return;
     const int k = s_pic;
     const PicDesc& P = *st.s[k].pic;
-    const int epoch = st.s[k].aux1;
+    const int32_t epoch = st.s[k].aux1;
     const int idx = s_ticket;
     const int a = P.ictu_addr[idx], rx = a % P.wctb, ry = a / P.wctb;
 
+    if (tid == 32) {
+        s_ipic.rec = P.rec;
+        s_ipic.off_cb = P.off_cb;
+        s_ipic.off_cr = P.off_cr;
+        s_ipic.width = P.width;
+        s_ipic.height = P.height;
+        s_ipic.log2_ctb = P.log2_ctb;
+        s_ipic.pitch_y = P.pitch_y;
+        s_ipic.pitch_c = P.pitch_c;
+        s_ipic.intra_smoothing_disabled = P.intra_smoothing_disabled;
+        s_ipic.strong_intra = P.strong_intra;
+    }
     if (tid == 4) {  // which neighbour CTBs share this CTB's slice and tile
         const int sl = P.ctb_slice ? P.ctb_slice[a] : 0, ti = P.ctb_tile ? P.ctb_tile[a] : 0;
         auto same = [&](int nx, int ny) {
@@ -436,16 +577,25 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
                (same(rx, ry - 1) ? NB_ABOVE : 0u) | (same(rx + 1, ry - 1) ? NB_ABOVE_RIGHT : 0u);
     }
 
-    // stage the neighbourhood and the TU records
+    // stage the CTU's tiles, TU records and residuals (packed in task order, one thread per
+    // TU) in one round of asynchronous copies
     const int off = P.ictu_tu_off[idx], n_tu = P.ictu_tu_off[idx + 1] - off;
-    const int lvl0 = P.ictu_lvl_off[idx], n_lvl = P.ictu_lvl_off[idx + 1] - lvl0;
-    if (tid < 4) s_seen[tid] = 0;
-    // one round of asynchronous copies: TU records, levels (two per 16-byte copy, from the
-    // even entry at or below the first), the three tiles, the residuals of the coded TUs
-    // (packed in task order, one thread per TU)
-    for (int i = tid; i < n_tu; i += IC_THREADS) cp_async16(&s_tu[i], &P.itu_rec[off + i]);
-    for (int i = tid; 2 * i < n_lvl + (lvl0 & 1); i += IC_THREADS)
-        cp_async16(&s_lvl[2 * i], &P.ictu_lvl[(lvl0 & ~1) + 2 * i]);
+    for (int i = tid; i < n_tu; i += IC_THREADS) {
+        cp_async16(&s_tu[i], &P.itu_rec[off + i]);
+        mbar_init1(&s_bar[i]);
+        s_itu_dep[i] = __ldg(&P.itu_dep[off + i]);
+    }
+    // the CTU's dependency entries are contiguous in task order
+    const uint32_t dfirst = __ldg(&P.itu_dep[off]) >> 6, dlast_e = __ldg(&P.itu_dep[off + n_tu - 1]);
+    const int n_dep = (int)((dlast_e >> 6) + (dlast_e & 63u)) - (int)dfirst;
+    const int staged = max(0, min(n_dep, IC_DEP_STAGE));
+    for (int q = tid; q < staged; q += IC_THREADS) s_dep[q] = __ldg(&P.dep_list[dfirst + q]);
+    const uint32_t wd = __ldg(&P.ictu_watch[idx]);
+    const int n_watch = min((int)(wd & 0xFFu), IC_MAX_WATCH);
+    for (int q = tid; q < n_watch; q += IC_THREADS) {
+        s_watch[q] = __ldg(&P.watch[(wd >> 8) + q]);
+        mbar_init1(&s_wbar[q]);
+    }
     stage_tile(P, 0, rx, ry, t_luma, tid);
     stage_tile(P, 1, rx, ry, t_chroma[0], tid);
     stage_tile(P, 2, rx, ry, t_chroma[1], tid);
@@ -458,79 +608,81 @@ __global__ void __launch_bounds__(IC_THREADS, 6) k_intra_ctus(const __grid_const
 
     const int ctbl = 1 << P.log2_ctb;
     const uint32_t nb = s_nb;
-    // Levels of the CTU-local DAG.  Before a level whose requirement on a dependency CTU
-    // exceeds what was last seen of it, threads 0-3 wait (bounded) until their dependency
-    // CTU has completed the levels this level needs, then the CTA meets at a barrier; a
-    // requirement already seen met needs neither (the barrier that ended the level where it
-    // was seen orders it for every thread).  After a level that other CTUs need, the CTU
-    // publishes (epoch << 16) | levels completed.
-    const IntraLevel* lvl = s_lvl + (lvl0 & 1);
-    const int dep = tid < 4 ? P.ictu_deps[4 * idx + tid] : -1;
-    const int32_t stamp = epoch << 16;
-    int pos = 0;
-    for (int L = 0; pos < n_tu; L++) {
-        const IntraLevel info = lvl[L];
-        bool wait = false;
-#pragma unroll
-        for (int d = 0; d < 4; d++) wait = wait || intra_req(info, d) > s_seen[d];
-        if (wait) {
-            int seen = -1;   // levels the dependency was seen to have completed, when polled
-            if (dep >= 0) {
-                const int need = intra_req(info, tid);
-                if (need > s_seen[tid]) {
-                    cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[dep]);
-                    unsigned long long t0 = 0;
-                    int v;
-                    for (unsigned polls = 0; (v = done.load(cuda::memory_order_acquire)) < (stamp | need); polls++) {
-                        if ((polls & 255u) == 0) {   // the timer and the status word, every 256 polls
-                            const unsigned long long now = global_ns();
-                            if (polls == 0) t0 = now;
-                            if (now - t0 > WAIT_LIMIT_NS || polls >= SPIN_LIMIT) {
-                                atomicOr(sticky, ST_TIMEOUT);
-                                s_abort = 1;
-                                break;
-                            }
-                            // another CTU's wait gave up (maybe the one this CTU waits for):
-                            // stop now rather than after a full limit of its own
-                            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> status(*sticky);
-                            if (status.load(cuda::memory_order_relaxed) & ST_TIMEOUT) {
-                                s_abort = 1;
-                                break;
-                            }
-                        }
-                        __nanosleep(32);
-                    }
-                    seen = v - stamp;   // same epoch: levels completed (>= need)
+    if (warp == IC_WATCHER) {
+        // The watcher: one lane waits for the CTU's watched TUs of other CTUs in the order
+        // their first dependent TU comes, polling each published completion through L2 and
+        // sleeping between polls (the wait is bounded like every other), and arrives on the
+        // TU's watch barrier when it sees it.  Its acquire, then that release arrival, order
+        // the other CTU's samples before every read of a worker that waits on the barrier.
+        if (lane == 0) {
+            for (int j = 0; j < n_watch; j++) {
+                if (s_watch[j] >= (uint32_t)P.n_itu) {   // no such TU: refused
+                    atomicOr(sticky, ST_BAD_RECORD);
+                    s_abort = 1;
+                    break;
                 }
+                cuda::atomic_ref<int32_t, cuda::thread_scope_device> f(P.itu_done[s_watch[j]]);
+                unsigned long long t0 = 0;
+                unsigned nap = 32;
+                bool gave_up = false;
+                // relaxed polls (a GPU-scope acquire invalidates the SM's L1, which the
+                // workers use), one acquire fence once the flag is seen
+                for (unsigned polls = 0; f.load(cuda::memory_order_relaxed) != epoch; polls++) {
+                    const unsigned long long now = global_ns();
+                    if (polls == 0) t0 = now;
+                    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> status(*sticky);
+                    if (now - t0 > WAIT_LIMIT_NS || polls >= SPIN_LIMIT) {
+                        atomicOr(sticky, ST_TIMEOUT);
+                        gave_up = true;
+                    } else if (s_abort || (status.load(cuda::memory_order_relaxed) & ST_TIMEOUT)) {
+                        gave_up = true;
+                    }
+                    if (gave_up) break;
+                    __nanosleep(nap);
+                    nap = min(nap * 2, 256u);
+                }
+                if (gave_up) {
+                    s_abort = 1;
+                    break;
+                }
+                cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
+                mbar_arrive(&s_wbar[j]);
             }
-            __syncthreads();
-            if (s_abort) return;
-            // after the barrier, so that no thread still reads s_seen for this level's test
-            if (seen >= 0) s_seen[tid] = seen;
         }
-        const int lvl_end = intra_end(info);
-        for (int i = pos + warp; i < lvl_end; i += IC_WARPS) {
-            const hevc_tu_t& tu = s_tu[i];
-            const int ctbc = tu.c_idx ? ctbl / 2 : ctbl;
-            CtuTile tile;
-            tile.t = tu.c_idx == 0 ? t_luma : t_chroma[tu.c_idx - 1];
-            tile.pitch = tu.c_idx ? IC_CP : IC_LP;
-            tile.x0 = rx * ctbc;
-            tile.y0 = ry * ctbc;
-            const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + tu.coeff_offset : nullptr;
-            intra_tu_any(P, tu, lane, ws[warp], tile, nb, res);
+        return;
+    }
+    for (;;) {
+        int i = 0;
+        if (lane == 0) i = s_abort ? n_tu : atomicAdd(&s_next, 1);
+        i = __shfl_sync(0xffffffffu, i, 0);
+        if (i >= n_tu) break;
+        const hevc_tu_t tu = s_tu[i];
+        const uint32_t dd = s_itu_dep[i];
+        const int dcount = (int)(dd & 63u), doff = (int)(dd >> 6) - (int)dfirst;
+        const IntraWait wc{s_dep, P.dep_list, s_bar, s_wbar, P.itu_done, sticky, &s_abort, (int)dfirst, doff, dcount,
+                           staged, i, n_watch, P.n_itu, epoch, lane};
+        auto wait = [&]() -> bool { return intra_wait(wc); };
+        const int ctbc = tu.c_idx ? ctbl / 2 : ctbl;
+        CtuTile tile;
+        tile.t = tu.c_idx == 0 ? t_luma : t_chroma[tu.c_idx - 1];
+        tile.pitch = tu.c_idx ? IC_CP : IC_LP;
+        tile.x0 = rx * ctbc;
+        tile.y0 = ry * ctbc;
+        const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + tu.coeff_offset : nullptr;
+        if (!intra_tu_any(s_ipic, tu, lane, ws[warp], tile, nb, res, wait)) {
+            if (lane == 0) s_abort = 1;
+            break;
         }
-        __syncthreads();
-        if ((info.x & INTRA_LEVEL_PUBLISH) && tid == IC_PUBLISHER) {
-            // after the barrier, the release store orders the CTA's picture writes before
-            // the word (the barrier makes them prior to this thread's release).  The last
-            // warp publishes: TUs go to warps from warp 0 up, so it is the warp most often
-            // idle in the next level, and the release's wait for the stores overlaps the
-            // other warps' next TUs.
-            cuda::atomic_ref<int32_t, cuda::thread_scope_device> done(P.ictu_done[idx]);
-            done.store(stamp | (L + 1), cuda::memory_order_release);
+        // after the warp barrier, lane 0's release arrival and store order the warp's sample
+        // writes (tile and picture) before the completion
+        __syncwarp();
+        if (lane == 0) {
+            mbar_arrive(&s_bar[i]);
+            if (tu.reserved[0] & ITU_PUBLISH) {
+                cuda::atomic_ref<int32_t, cuda::thread_scope_device> g(P.itu_done[off + i]);
+                g.store(epoch, cuda::memory_order_release);
+            }
         }
-        pos = lvl_end;
     }
 }
 
