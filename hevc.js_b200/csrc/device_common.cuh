@@ -54,7 +54,7 @@ struct PicDesc {
     const hevc_slice_t* slices;
     const hevc_scaling_t* scaling;       // scaling lists, or null for flat scaling
     // intra CTU tasks (intra.cuh): the CTUs that hold intra TUs in wavefront order (key
-    // 2 * row + column), and their TUs ordered by level of the CTU-local dependency DAG
+    // 2 * row + column), and their TUs ordered by depth in the picture's dependency DAG
     // (task order)
     const int32_t* ictu_addr;            // raster address of intra CTU k
     const int32_t* ictu_tu_off;          // TUs of intra CTU k: task entries [ictu_tu_off[k], [k+1])

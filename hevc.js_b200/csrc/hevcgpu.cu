@@ -684,9 +684,9 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     // Intra schedule.  Per plane an owner map at 4-sample granularity records the latest
     // intra TU written there; intra TU B reads the units of its reference row
     // (x-1 .. x+2N-1 at y-1) and column (y .. y+2N-1 at x-1).  Each distinct owner is a
-    // dependency of B: an owner in B's CTU is a local one (B is one level above it in the
-    // CTU-local DAG, which orders the CTU's tasks), an owner in an earlier CTU an external
-    // one.  A unit whose samples B may not use (availability) can only add an unneeded wait,
+    // dependency of B: an owner in B's CTU a local one, an owner in an earlier CTU an
+    // external one.  B's depth is one more than its deepest dependency's: the length of the
+    // longest dependency chain over the picture that ends at B.  A unit whose samples B may not use (availability) can only add an unneeded wait,
     // never change a sample; owners in CTUs later in raster order (decoded earlier only in
     // tile scan) are never available and add nothing.
     const int n_intra = (int)intra_list.size();
@@ -741,7 +741,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
             dep_at[(size_t)b] = (int32_t)deps.size();
             uint64_t* own = owner[c].data();
             const int row = uw[c];
-            int lv = 0;
+            int dp = 0;
             uint64_t last = 0;   // a run of units with one owner adds what its first unit added
             auto dep = [&](uint64_t o) {
                 if ((o & GEN_BITS) != gtag || o == last) return;
@@ -756,7 +756,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
                 for (size_t q = (size_t)dep_at[(size_t)b]; q < deps.size(); q++)
                     if (deps[q] == ob) return;
                 deps.push_back(ob);
-                if (oa == a) lv = std::max(lv, level[(size_t)ob] + 1);
+                dp = std::max(dp, level[(size_t)ob] + 1);   // local and external dependencies alike
             };
             if (t.y > 0) {
                 const size_t rrow = (size_t)((t.y - 1) / 4) * row;
@@ -767,7 +767,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
                 const int lx = (t.x - 1) / 4, uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
                 for (int uy = uy0; uy <= uy1; uy++) dep(own[(size_t)uy * row + lx]);
             }
-            level[(size_t)b] = lv;
+            level[(size_t)b] = dp;
             const uint64_t mark = gtag | (uint64_t)(uint32_t)b;
             for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++) {
                 uint64_t* r = own + (size_t)uy * row;
@@ -776,7 +776,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
         }
         dep_at[(size_t)n_intra] = (int32_t)deps.size();
         // Task order: CTUs in wavefront order (key 2 * row + column, then raster), each
-        // CTU's TUs by level, then decode order.  CTAs take CTUs by ticket in this order, so
+        // CTU's TUs by depth (every TU after the TUs it depends on, and about in the order
+        // they can run), then decode order.  CTAs take CTUs by ticket in this order, so
         // the CTUs held by resident CTAs are those of the diagonal band the picture's
         // dependencies advance along (a row trails the one above by two CTUs), not whole
         // rows in raster order.  Every CTU a CTU reads from (left, above-left, above,
@@ -802,12 +803,15 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
                 for (int q = 0; q < nr; q++) {
                     const int rq = sorted[(size_t)q].second;
                     const int r0 = runs[(size_t)rq].second, r1 = runs[(size_t)rq + 1].second;
-                    int maxl = 0;
-                    for (int b = r0; b < r1; b++) maxl = std::max(maxl, level[(size_t)b]);
-                    cnt.assign((size_t)maxl + 2, 0);
-                    for (int b = r0; b < r1; b++) cnt[(size_t)level[(size_t)b] + 1]++;
-                    for (int l = 1; l <= maxl + 1; l++) cnt[(size_t)l] += cnt[(size_t)l - 1];
-                    for (int b = r0; b < r1; b++) order[(size_t)(at + cnt[(size_t)level[(size_t)b]]++)] = b;
+                    int minl = level[(size_t)r0], maxl = minl;
+                    for (int b = r0; b < r1; b++) {
+                        minl = std::min(minl, level[(size_t)b]);
+                        maxl = std::max(maxl, level[(size_t)b]);
+                    }
+                    cnt.assign((size_t)(maxl - minl) + 2, 0);
+                    for (int b = r0; b < r1; b++) cnt[(size_t)(level[(size_t)b] - minl) + 1]++;
+                    for (int l = 1; l <= maxl - minl + 1; l++) cnt[(size_t)l] += cnt[(size_t)l - 1];
+                    for (int b = r0; b < r1; b++) order[(size_t)(at + cnt[(size_t)(level[(size_t)b] - minl)]++)] = b;
                     at += r1 - r0;
                 }
             }

@@ -5,7 +5,7 @@
 // when this stage runs, except where an earlier intra TU writes them (MC and the inter
 // residuals ran before).  The host turns that into a dependency list per intra TU: the
 // TUs that write samples it reads, in its own CTU (local) or in an earlier CTU
-// (external), and orders each CTU's TUs by their level in the CTU-local DAG.
+// (external), and orders each CTU's TUs by their depth in the picture's dependency DAG.
 // k_intra_ctus runs one CTA per CTU with intra TUs: it stages the CTU, its TU records,
 // dependency lists and residuals in shared memory; its warps take the TUs in order and run
 // each one once its dependencies are complete (one-arrival barriers in shared memory for
@@ -54,22 +54,25 @@ struct CtuTile {
 // current CTB in raster order and share its slice and tile (intra_prediction.cpp:108-124).
 enum : uint32_t { NB_LEFT = 1u, NB_ABOVE_LEFT = 2u, NB_ABOVE = 4u, NB_ABOVE_RIGHT = 8u };
 
-// Predict + reconstruct one intra TU of size 1 << LOG2 in plane CI (0 luma, 1/2 chroma)
-// with one warp (perform_intra_prediction, then reconstruct_block's add and clip).
-// Reference samples come from the CTU tile; results go to the tile (for later TUs) and
-// the picture.  res is the TU's residual (null when it has none).
-template <int LOG2, bool CHROMA, typename Pic, typename Wait>
+// Predict + reconstruct one intra TU (any size 4..32, any plane) with one warp
+// (perform_intra_prediction, then reconstruct_block's add and clip).  Reference samples
+// come from the CTU tile, or from the picture for samples of other CTUs; results go to the
+// tile (for later TUs) and the picture.  res is the TU's residual (null when it has none).
+// The size is a run-time value: one copy of the code serves every TU, which keeps the
+// kernel small in the instruction cache (TUs of every size alternate on an SM).  Between
+// the lanes the reference array goes through the warp's shared memory.
+template <typename Pic, typename Wait>
 __device__ __forceinline__ bool intra_tu(const Pic& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W,
                                          const CtuTile& tile, uint32_t nb_mask, const int16_t* res, Wait&& wait) {
-    constexpr int n = 1 << LOG2, sub = CHROMA ? 2 : 1;
-    constexpr int total = 4 * n + 1, R = (total + 31) / 32;  // reference samples, lane rounds
-    const int ci = t.c_idx;
+    constexpr int RMAX = 5;                       // lane rounds of the largest reference array
+    const int ci = t.c_idx, chroma = ci != 0, log2 = t.log2_size, n = 1 << log2, sub = chroma ? 2 : 1;
+    const int total = 4 * n + 1, R = (total + 31) >> 5;   // reference samples, lane rounds
     const int xc = t.x, yc = t.y;
-    const int log2c = P.log2_ctb - (CHROMA ? 1 : 0);          // CTB size in this plane
+    const int log2c = P.log2_ctb - chroma;                // CTB size in this plane
     const int rx = xc >> log2c, ry = yc >> log2c;
     const int pw = P.width / sub, ph = P.height / sub;
     const int ox = rx << P.log2_ctb, oy = ry << P.log2_ctb;   // CTB origin in luma samples
-    const int pitch = CHROMA ? P.pitch_c : P.pitch_y;
+    const int pitch = chroma ? P.pitch_c : P.pitch_y;
     uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));
     const uint32_t cur_z = zorder16((uint32_t)((xc * sub - ox) >> 2), (uint32_t)((yc * sub - oy) >> 2));
 
@@ -79,10 +82,13 @@ __device__ __forceinline__ bool intra_tu(const Pic& P, const hevc_tu_t& t, int l
     //    bottom-left sample (0) through the corner (2n) to the top-right one (4n).
     //    Availability and the address of each sample depend on positions only, so they are
     //    found before the wait for the TUs that write the samples; the loads follow it.
-    uint32_t mask[R];
-    int val[R], where[R];   // where: tile index, or ~(picture offset) for samples of other CTUs
+    uint32_t mask[RMAX];
+    int val[RMAX], where[RMAX];   // where: tile index, or ~(picture offset) for samples of other CTUs
 #pragma unroll
-    for (int r = 0; r < R; r++) {
+    for (int r = 0; r < RMAX; r++) {
+        mask[r] = 0;
+        where[r] = 0;
+        if (r >= R) continue;
         const int i = lane + 32 * r;
         bool ok = false;
         int at = 0;
@@ -115,111 +121,95 @@ __device__ __forceinline__ bool intra_tu(const Pic& P, const hevc_tu_t& t, int l
     // samples of other CTUs come from the picture through L2 (the TUs of those CTUs that
     // write them have published their completion), this CTU's from the tile
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-        const int at = where[r];
+    for (int r = 0; r < RMAX; r++) {
         int v = 0;
-        if ((mask[r] >> lane) & 1u) v = at < 0 ? __ldcg(plane + ~at) : tile.t[at];
+        if (r < R && ((mask[r] >> lane) & 1u)) v = where[r] < 0 ? __ldcg(plane + ~where[r]) : tile.t[where[r]];
         val[r] = v;
     }
-    // Phases 2-4 keep the reference array in registers, element i in lane i % 32 of round
-    // i / 32, and move elements between lanes with shuffles: fetch(a, j) gives every lane
-    // element j of its own choosing, fetch_at(a, J) element J (the same in all lanes).
-    auto fetch = [&](const int (&a)[R], int j) {
-        int v = 0;
-#pragma unroll
-        for (int q = 0; q < R; q++) {
-            const int tq = __shfl_sync(0xffffffffu, a[q], j & 31);
-            if ((j >> 5) == q) v = tq;
-        }
-        return v;
-    };
-    auto fetch_at = [&](const int (&a)[R], int J) { return __shfl_sync(0xffffffffu, a[J >> 5], J & 31); };
 
     // 2. substitution (:177-197): an unavailable sample takes the nearest available one
-    //    below it in the array, or the first available one; none available -> 128
-    constexpr uint32_t LAST_LANES = (total & 31) ? ((1u << (total & 31)) - 1u) : 0xffffffffu;
+    //    below it in the array, or the first available one; none available -> 128.  The
+    //    raw samples go through W.m (free until step 4).
+    const uint32_t last_lanes = (total & 31) ? ((1u << (total & 31)) - 1u) : 0xffffffffu;
     bool all = true;
     int first = -1;
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-        all = all && mask[r] == (r == R - 1 ? LAST_LANES : 0xffffffffu);
+    for (int r = 0; r < RMAX; r++) {
+        if (r >= R) continue;
+        all = all && mask[r] == (r == R - 1 ? last_lanes : 0xffffffffu);
         if (first < 0 && mask[r]) first = 32 * r + __ffs(mask[r]) - 1;
     }
-    int s[R];
-    if (all) {
+    if (!all) {
+        if (first >= 0) {
 #pragma unroll
-        for (int r = 0; r < R; r++) s[r] = val[r];
-    } else if (first < 0) {
+            for (int r = 0; r < RMAX; r++)
+                if (r < R && lane + 32 * r < total) W.m[lane + 32 * r] = (int16_t)val[r];
+            __syncwarp();
+        }
 #pragma unroll
-        for (int r = 0; r < R; r++) s[r] = 128;
-    } else {
-#pragma unroll
-        for (int r = 0; r < R; r++) {
+        for (int r = 0; r < RMAX; r++) {
+            if (r >= R) continue;
+            if (first < 0) {
+                val[r] = 128;
+                continue;
+            }
+            if ((mask[r] >> lane) & 1u) continue;
             const uint32_t below = mask[r] & ((1u << lane) - 1u);
             int j = below ? 32 * r + 31 - __clz(below) : -1;
 #pragma unroll
-            for (int q = r - 1; q >= 0; q--)
-                if (j < 0 && mask[q]) j = 32 * q + 31 - __clz(mask[q]);
-            if ((mask[r] >> lane) & 1u) j = lane + 32 * r;
-            else if (j < 0) j = first;
-            s[r] = fetch(val, j);
+            for (int q = RMAX - 1; q >= 0; q--)
+                if (q < r && j < 0 && mask[q]) j = 32 * q + 31 - __clz(mask[q]);
+            val[r] = W.m[j < 0 ? first : j];
         }
     }
+    // the substituted references to W.s
+#pragma unroll
+    for (int r = 0; r < RMAX; r++)
+        if (r < R && lane + 32 * r < total) W.s[lane + 32 * r] = (int16_t)val[r];
+    __syncwarp();
+
     // 3. smoothing of luma references (:217-257, :443-471): [1 2 1] over the linear array
     //    (which also gives the corner filter), or the bilinear strong smoothing of 32x32
     const int mode = t.intra_mode;
-    int f[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) f[r] = s[r];
-    if constexpr (!CHROMA && n != 4) {
-        constexpr int thr = n == 8 ? 7 : (n == 16 ? 1 : 0);
+    if (!chroma && n != 4) {
+        const int thr = n == 8 ? 7 : (n == 16 ? 1 : 0);
         const int d = min(abs(mode - 26), abs(mode - 10));
         if (!P.intra_smoothing_disabled && mode != 1 && d > thr) {
-            const int c = fetch_at(s, 2 * n), e_top = fetch_at(s, 4 * n), e_left = fetch_at(s, 0);
-            bool bil = false;
-            if constexpr (n == 32) {
-                if (P.strong_intra)
-                    bil = abs(c + e_top - 2 * fetch_at(s, 3 * n)) < 8 && abs(c + e_left - 2 * fetch_at(s, n)) < 8;
-            }
+            const int c = W.s[2 * n], e_top = W.s[4 * n], e_left = W.s[0];
+            const bool bil = n == 32 && P.strong_intra && abs(c + e_top - 2 * W.s[3 * n]) < 8 &&
+                             abs(c + e_left - 2 * W.s[n]) < 8;
+            int f[RMAX];
 #pragma unroll
-            for (int r = 0; r < R; r++) {
+            for (int r = 0; r < RMAX; r++) {
                 const int i = lane + 32 * r;
-                int prev = __shfl_up_sync(0xffffffffu, s[r], 1), next = __shfl_down_sync(0xffffffffu, s[r], 1);
-                if (r > 0) {
-                    const int pl = __shfl_sync(0xffffffffu, s[r > 0 ? r - 1 : 0], 31);
-                    if (lane == 0) prev = pl;
-                }
-                if (r + 1 < R) {
-                    const int nf = __shfl_sync(0xffffffffu, s[r + 1 < R ? r + 1 : r], 0);
-                    if (lane == 31) next = nf;
-                }
-                if (i == 0 || i >= 4 * n) f[r] = s[r];
-                else if (bil) {
-                    if (i == 2 * n) f[r] = s[r];
-                    else if (i > 2 * n) { const int k = i - 2 * n; f[r] = ((2 * n - k) * c + k * e_top + n) >> (LOG2 + 1); }
-                    else { const int k = 2 * n - i; f[r] = ((2 * n - k) * c + k * e_left + n) >> (LOG2 + 1); }
+                f[r] = val[r];
+                if (r >= R || i == 0 || i >= 4 * n) continue;
+                if (bil) {
+                    if (i > 2 * n) { const int k = i - 2 * n; f[r] = ((2 * n - k) * c + k * e_top + n) >> (log2 + 1); }
+                    else if (i < 2 * n) { const int k = 2 * n - i; f[r] = ((2 * n - k) * c + k * e_left + n) >> (log2 + 1); }
                 } else {
-                    f[r] = (prev + 2 * s[r] + next + 2) >> 2;
+                    f[r] = (W.s[i - 1] + 2 * val[r] + W.s[i + 1] + 2) >> 2;
                 }
             }
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < RMAX; r++)
+                if (r < R && lane + 32 * r < total) W.s[lane + 32 * r] = (int16_t)f[r];
+            __syncwarp();
         }
     }
-    // 4. the final references to shared memory (top[k] = R_[2n + k], left[k] = R_[2n - k])
-    //    and, for the angular modes, the main reference with the side reference projected
+    // 4. for the angular modes, the main reference with the side reference projected
     //    through invAngle (:346-368): m[q + n] = top[q] (vertical) / left[q] (horizontal)
     //    for q >= 0, the other side's sample min(2n, (-q * invAngle + 128) >> 8) for q < 0
+    //    (top[k] = R_[2n + k], left[k] = R_[2n - k])
     const int16_t* R_ = W.s;
-#pragma unroll
-    for (int r = 0; r < R; r++)
-        if (lane + 32 * r < total) W.s[lane + 32 * r] = (int16_t)f[r];
     const int ang = c_intra_angle[mode];
     const bool vert = mode >= 18;
     if (mode >= 2) {
         const int inv = c_inv_angle[mode];
-        constexpr int ME = 3 * n + 2;   // entries q = -n .. 2n + 1 (the last one padding, never weighted)
-#pragma unroll
-        for (int k = 0; k < (ME + 31) / 32; k++) {
-            const int e = lane + 32 * k, q = e - n;
+        const int me = 3 * n + 2;   // entries q = -n .. 2n + 1 (the last one padding, never weighted)
+        for (int e = lane; e < me; e += 32) {
+            const int q = e - n;
             int src;
             if (q > 2 * n) src = -1;
             else if (q >= 0) src = vert ? 2 * n + q : 2 * n - q;
@@ -227,23 +217,22 @@ __device__ __forceinline__ bool intra_tu(const Pic& P, const hevc_tu_t& t, int l
                 const int si = min(2 * n, ((-q) * inv + 128) >> 8);
                 src = vert ? 2 * n - si : 2 * n + si;
             }
-            const int v = fetch(f, src < 0 ? 0 : src);
-            if (e < ME) W.m[e] = (int16_t)(src < 0 ? 0 : v);
+            W.m[e] = src < 0 ? (int16_t)0 : R_[src];
         }
+        __syncwarp();
     }
-    __syncwarp();
     // 5. prediction + residual, clip, store.  Each lane takes groups of 4 samples of a row;
     //    its column x0 = 4 * (lane % (n / 4)) is the same for all its groups, so column
     //    terms are computed once.
-    constexpr int GPR = n / 4, NG = n * n / 4, G_PER_LANE = (NG + 31) / 32;
+    const int gpr = n >> 2, ng = (n * n) >> 2;
     int dc = 0;
     if (mode == 1) {  // predict_dc :295-317
-        int s = 0;
-        for (int i = lane; i < n; i += 32) s += R_[2 * n + 1 + i] + R_[2 * n - 1 - i];
-        s = __reduce_add_sync(0xffffffffu, s);
-        dc = (s + n) >> (LOG2 + 1);
+        int sum = 0;
+        for (int i = lane; i < n; i += 32) sum += R_[2 * n + 1 + i] + R_[2 * n - 1 - i];
+        sum = __reduce_add_sync(0xffffffffu, sum);
+        dc = (sum + n) >> (log2 + 1);
     }
-    const int x0 = 4 * (lane % GPR);
+    const int x0 = 4 * (lane & (gpr - 1));
     const int corner = R_[2 * n], tr = R_[3 * n + 1], bl = R_[n - 1];
     int ctop[4], cidx[4], cfr[4];
 #pragma unroll
@@ -253,23 +242,21 @@ __device__ __forceinline__ bool intra_tu(const Pic& P, const hevc_tu_t& t, int l
         cidx[j] = ((x + 1) * ang) >> 5;
         cfr[j] = ((x + 1) * ang) & 31;
     }
-#pragma unroll 2
-    for (int q = 0; q < G_PER_LANE; q++) {
-        const int g = lane + 32 * q;
-        if (g >= NG) break;
-        const int y = g / GPR;
+    const bool edge_filters = !chroma && n < 32;
+    for (int g = lane; g < ng; g += 32) {
+        const int y = g >> (log2 - 2);
         const int left = R_[2 * n - 1 - y];
         int p[4];
         if (mode == 0) {  // predict_planar :263-289
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int x = x0 + j;
-                p[j] = ((n - 1 - x) * left + (x + 1) * tr + (n - 1 - y) * ctop[j] + (y + 1) * bl + n) >> (LOG2 + 1);
+                p[j] = ((n - 1 - x) * left + (x + 1) * tr + (n - 1 - y) * ctop[j] + (y + 1) * bl + n) >> (log2 + 1);
             }
         } else if (mode == 1) {
 #pragma unroll
             for (int j = 0; j < 4; j++) p[j] = dc;
-            if (!CHROMA && n < 32) {
+            if (edge_filters) {
                 if (y == 0) {
 #pragma unroll
                     for (int j = 0; j < 4; j++) p[j] = (ctop[j] + 3 * dc + 2) >> 2;
@@ -279,19 +266,19 @@ __device__ __forceinline__ bool intra_tu(const Pic& P, const hevc_tu_t& t, int l
         } else if (vert) {  // predict_angular :323-422, main reference on top
             const int idx = ((y + 1) * ang) >> 5, fr = ((y + 1) * ang) & 31;
             const int16_t* m = W.m + n + x0 + 1 + idx;
-            int r[5];
+            int r5[5];
 #pragma unroll
-            for (int j = 0; j < 5; j++) r[j] = m[j];
+            for (int j = 0; j < 5; j++) r5[j] = m[j];
 #pragma unroll
-            for (int j = 0; j < 4; j++) p[j] = fr ? ((32 - fr) * r[j] + fr * r[j + 1] + 16) >> 5 : r[j];
-            if (!CHROMA && n < 32 && mode == 26 && x0 == 0) p[0] = clip_u8(p[0] + ((left - corner) >> 1));
+            for (int j = 0; j < 4; j++) p[j] = fr ? ((32 - fr) * r5[j] + fr * r5[j + 1] + 16) >> 5 : r5[j];
+            if (edge_filters && mode == 26 && x0 == 0) p[0] = clip_u8(p[0] + ((left - corner) >> 1));
         } else {  // main reference on the left
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int16_t* m = W.m + n + y + 1 + cidx[j];
                 p[j] = cfr[j] ? ((32 - cfr[j]) * m[0] + cfr[j] * m[1] + 16) >> 5 : m[0];
             }
-            if (!CHROMA && n < 32 && mode == 10 && y == 0) {
+            if (edge_filters && mode == 10 && y == 0) {
 #pragma unroll
                 for (int j = 0; j < 4; j++) p[j] = clip_u8(p[j] + ((ctop[j] - corner) >> 1));
             }
@@ -318,24 +305,102 @@ __device__ __forceinline__ bool intra_tu(const Pic& P, const hevc_tu_t& t, int l
     return true;
 }
 
-// Size/plane dispatch of intra_tu; false when the wait gave up.
+// The 4x4 TU (luma or chroma; most TUs, and most of an intra picture's dependency chain):
+// the same prediction with the 17 reference samples held one per lane and moved by
+// shuffles, no smoothing (4x4 references are never filtered, :217-230 and :443-445), and one
+// output sample per lane (x = lane & 3, y = lane >> 2) — no shared-memory staging.
 template <typename Pic, typename Wait>
-__device__ __forceinline__ bool intra_tu_any(const Pic& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W,
-                                             const CtuTile& tile, uint32_t nb_mask, const int16_t* res, Wait&& wait) {
-    if (t.c_idx == 0) {
-        switch (t.log2_size) {
-            case 2: return intra_tu<2, false>(P, t, lane, W, tile, nb_mask, res, wait);
-            case 3: return intra_tu<3, false>(P, t, lane, W, tile, nb_mask, res, wait);
-            case 4: return intra_tu<4, false>(P, t, lane, W, tile, nb_mask, res, wait);
-            default: return intra_tu<5, false>(P, t, lane, W, tile, nb_mask, res, wait);
+__device__ __forceinline__ bool intra_tu4(const Pic& P, const hevc_tu_t& t, int lane, const CtuTile& tile,
+                                          uint32_t nb_mask, const int16_t* res, Wait&& wait) {
+    constexpr uint32_t FULL = 0xffffffffu, ALL17 = 0x1FFFFu;
+    const int ci = t.c_idx, chroma = ci != 0, sub = chroma ? 2 : 1;
+    const int xc = t.x, yc = t.y;
+    const int log2c = P.log2_ctb - chroma;
+    const int rx = xc >> log2c, ry = yc >> log2c;
+    const int pw = P.width / sub, ph = P.height / sub;
+    const int ox = rx << P.log2_ctb, oy = ry << P.log2_ctb;
+    const int pitch = chroma ? P.pitch_c : P.pitch_y;
+    uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));
+    // 1. reference sample `lane` (0 bottom-left .. 8 corner .. 16 top-right), its availability
+    //    (intra_prediction.cpp:102-133) and where it lies, before the wait
+    bool ok = false;
+    int at = 0;
+    if (lane < 17) {
+        int px, py;
+        if (lane < 8) { px = xc - 1; py = yc + 7 - lane; }
+        else if (lane == 8) { px = xc - 1; py = yc - 1; }
+        else { px = xc + lane - 9; py = yc - 1; }
+        if (px >= 0 && py >= 0 && px < pw && py < ph) {
+            const int ncx = px >> log2c, ncy = py >> log2c;
+            const bool outside = ncx != rx || ncy != ry;
+            if (outside) {
+                uint32_t bit = 0u;
+                if (ncy == ry) bit = ncx == rx - 1 ? NB_LEFT : 0u;
+                else if (ncy == ry - 1)
+                    bit = ncx == rx - 1 ? NB_ABOVE_LEFT : (ncx == rx ? NB_ABOVE : (ncx == rx + 1 ? NB_ABOVE_RIGHT : 0u));
+                ok = (nb_mask & bit) != 0;
+            } else {
+                const uint32_t cur_z = zorder16((uint32_t)((xc * sub - ox) >> 2), (uint32_t)((yc * sub - oy) >> 2));
+                ok = zorder16((uint32_t)((px * sub - ox) >> 2), (uint32_t)((py * sub - oy) >> 2)) < cur_z;
+            }
+            if (ok) at = outside ? ~(py * pitch + px) : (py - tile.y0) * tile.pitch + (px - tile.x0);
         }
     }
-    switch (t.log2_size) {
-        case 2: return intra_tu<2, true>(P, t, lane, W, tile, nb_mask, res, wait);
-        case 3: return intra_tu<3, true>(P, t, lane, W, tile, nb_mask, res, wait);
-        case 4: return intra_tu<4, true>(P, t, lane, W, tile, nb_mask, res, wait);
-        default: return intra_tu<5, true>(P, t, lane, W, tile, nb_mask, res, wait);
+    const uint32_t mask = __ballot_sync(FULL, ok);
+    if (!wait()) return false;
+    int v = ok ? (at < 0 ? (int)__ldcg(plane + ~at) : (int)tile.t[at]) : 0;
+    // 2. substitution (:177-197): the nearest available sample below, else the first one;
+    //    none available -> 128
+    if (mask != ALL17) {
+        const uint32_t below = mask & ((1u << lane) - 1u);
+        const int j = ((mask >> lane) & 1u) ? lane : (below ? 31 - __clz(below) : __ffs(mask) - 1);
+        v = __shfl_sync(FULL, v, j < 0 ? 0 : j);
+        if (mask == 0u) v = 128;
     }
+    // 3. prediction of sample (x, y) of this lane (planar :263-289, DC :295-317, angular
+    //    :323-422 with the main reference projected through invAngle :346-368)
+    const int x = lane & 3, y = (lane >> 2) & 3, mode = t.intra_mode;
+    const int left = __shfl_sync(FULL, v, 7 - y), top = __shfl_sync(FULL, v, 9 + x);
+    const int corner = __shfl_sync(FULL, v, 8);
+    int p;
+    if (mode == 0) {
+        const int tr = __shfl_sync(FULL, v, 13), bl = __shfl_sync(FULL, v, 3);
+        p = ((3 - x) * left + (x + 1) * tr + (3 - y) * top + (y + 1) * bl + 4) >> 3;
+    } else if (mode == 1) {
+        const int dc = (__reduce_add_sync(FULL, ((lane >= 4 && lane <= 7) || (lane >= 9 && lane <= 12)) ? v : 0) + 4) >> 3;
+        p = dc;
+        if (!chroma) {
+            if (y == 0) p = x == 0 ? (top + left + 2 * dc + 2) >> 2 : (top + 3 * dc + 2) >> 2;
+            else if (x == 0) p = (left + 3 * dc + 2) >> 2;
+        }
+    } else {
+        const bool vert = mode >= 18;
+        const int ang = c_intra_angle[mode], inv = c_inv_angle[mode];
+        const int along = vert ? y : x, across = vert ? x : y;
+        const int idx = ((along + 1) * ang) >> 5, fr = ((along + 1) * ang) & 31;
+        // main reference entry q (q >= 0: the main side; q < 0: the other side projected)
+        auto src = [&](int q) {
+            int s;
+            if (q >= 0) s = vert ? 8 + q : 8 - q;
+            else {
+                const int si = min(8, ((-q) * inv + 128) >> 8);
+                s = vert ? 8 - si : 8 + si;
+            }
+            return min(16, max(0, s));   // past the end only with weight 0
+        };
+        const int q = across + 1 + idx;
+        const int a = __shfl_sync(FULL, v, src(q)), b = __shfl_sync(FULL, v, src(q + 1));
+        p = fr ? ((32 - fr) * a + fr * b + 16) >> 5 : a;
+        if (!chroma && mode == 26 && x == 0) p = clip_u8(p + ((left - corner) >> 1));
+        if (!chroma && mode == 10 && y == 0) p = clip_u8(p + ((top - corner) >> 1));
+    }
+    if (t.flags & HEVC_TU_PCM) p = 0;   // the PCM samples are the levels, with no prediction
+    if (lane < 16) {
+        const uint8_t o = (uint8_t)clip_u8(p + (res ? res[lane] : 0));
+        tile.t[(yc + y - tile.y0) * tile.pitch + (xc + x - tile.x0)] = o;
+        plane[(int64_t)(yc + y) * pitch + xc + x] = o;
+    }
+    return true;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -343,7 +408,7 @@ __device__ __forceinline__ bool intra_tu_any(const Pic& P, const hevc_tu_t& t, i
 // order per picture (2 * row + column: the diagonal band along which a picture's
 // dependencies advance), the pictures of a launch side by side.  The CTA stages the CTU, its TU
 // records and their residuals in shared memory; then its warps take the TUs one at a time
-// in task order (the CTU-local DAG's levels, so every TU comes after the TUs it depends
+// in task order (by depth in the picture's DAG, so every TU comes after the TUs it depends
 // on) and run each as soon as the TUs it reads from are complete: a TU of the same CTU
 // through its one-arrival barrier in shared memory, a TU of an earlier CTU through that
 // TU's published completion in global memory.  No barrier ties the warps together, so the
@@ -445,23 +510,24 @@ struct IntraWait {
     int dfirst, doff, dcount, staged, task, n_watch, n_itu, epoch, lane;
 };
 
-// The wait for a TU's dependencies, between the position work and the loads of intra_tu:
-// each lane waits for the entries lane, lane + 32, ...  Local and watched entries wait on
-// shared-memory barriers; a direct external entry (only a planted test wait has one) polls
+// The wait for a TU's dependencies, between the position work and the loads of intra_tu.
+// Local and watched entries wait on shared-memory barriers; a direct external entry (only a planted test wait has one) polls
 // the published completion.  Every wait reads the global timer and gives up after
 // WAIT_LIMIT_NS (SPIN_LIMIT tries as a backstop), marking the sticky status; a wait also
 // ends when another warp of the CTA gave up (s_abort) or, for external waits, when a wait
 // anywhere did (the status word).  Not inlined: one copy serves every TU size, which keeps
 // the size-specialised TU code small in the instruction cache.
 __device__ __noinline__ bool intra_wait(const IntraWait& w) {
+    // The entries one after another, every lane on the same one (warp-uniform waits: the
+    // warp is suspended as a whole on a barrier).
     bool gave_up = false;
-    for (int q = w.lane; q < w.dcount && !gave_up; q += 32) {
+    for (int q = 0; q < w.dcount && !gave_up; q++) {
         const int at = w.doff + q;
         const uint32_t e = at >= 0 && at < w.staged ? w.s_dep[at] : __ldg(&w.dep_list[w.dfirst + at]);
         unsigned long long t0 = 0;
         const bool watched = (e & INTRA_DEP_WATCH) != 0, local = !(e & (INTRA_DEP_EXTERNAL | INTRA_DEP_WATCH));
         if ((local && e >= (uint32_t)w.task) || (watched && (int)(e & 0xFFu) >= w.n_watch)) {
-            atomicOr(w.sticky, ST_BAD_RECORD);   // not an earlier TU, or no such watch slot: refused
+            if (w.lane == 0) atomicOr(w.sticky, ST_BAD_RECORD);   // not an earlier TU, or no such watch slot: refused
             gave_up = true;
         } else if (local || watched) {
             uint64_t* bar = watched ? &w.s_wbar[e & 0xFFu] : &w.s_bar[e];
@@ -473,13 +539,13 @@ __device__ __noinline__ bool intra_wait(const IntraWait& w) {
                 const unsigned long long now = global_ns();
                 if (polls == 0) t0 = now;
                 if (now - t0 > WAIT_LIMIT_NS || polls >= SPIN_LIMIT) {
-                    atomicOr(w.sticky, ST_TIMEOUT);
+                    if (w.lane == 0) atomicOr(w.sticky, ST_TIMEOUT);
                     gave_up = true;
                     break;
                 }
             }
         } else if ((e & ~INTRA_DEP_EXTERNAL) >= (uint32_t)w.n_itu) {
-            atomicOr(w.sticky, ST_BAD_RECORD);
+            if (w.lane == 0) atomicOr(w.sticky, ST_BAD_RECORD);
             gave_up = true;
         } else {
             cuda::atomic_ref<int32_t, cuda::thread_scope_device> f(w.itu_done[e & ~INTRA_DEP_EXTERNAL]);
@@ -489,7 +555,7 @@ __device__ __noinline__ bool intra_wait(const IntraWait& w) {
                     if (polls == 0) t0 = now;
                     cuda::atomic_ref<uint32_t, cuda::thread_scope_device> status(*w.sticky);
                     if (now - t0 > WAIT_LIMIT_NS || polls >= SPIN_LIMIT) {
-                        atomicOr(w.sticky, ST_TIMEOUT);
+                        if (w.lane == 0) atomicOr(w.sticky, ST_TIMEOUT);
                         gave_up = true;
                         break;
                     }
@@ -502,11 +568,12 @@ __device__ __noinline__ bool intra_wait(const IntraWait& w) {
             }
             if (!gave_up) cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
         }
+        // the lanes may have seen a barrier, the abort word or the clock at different moments
+        gave_up = __any_sync(0xffffffffu, gave_up);
     }
-    // the warp barrier orders each lane's acquires before every lane's reads of the samples;
-    // then every lane decides alike
+    // the warp barrier orders each lane's acquires before every lane's reads of the samples
     __syncwarp();
-    return !__any_sync(0xffffffffu, gave_up);
+    return !gave_up;
 }
 
 __global__ void __launch_bounds__(IC_THREADS, IC_MIN_BLOCKS) k_intra_ctus(const __grid_constant__ SegTable st,
@@ -669,7 +736,9 @@ __global__ void __launch_bounds__(IC_THREADS, IC_MIN_BLOCKS) k_intra_ctus(const 
         tile.x0 = rx * ctbc;
         tile.y0 = ry * ctbc;
         const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + tu.coeff_offset : nullptr;
-        if (!intra_tu_any(s_ipic, tu, lane, ws[warp], tile, nb, res, wait)) {
+        const bool done = tu.log2_size == 2 ? intra_tu4(s_ipic, tu, lane, tile, nb, res, wait)
+                                            : intra_tu(s_ipic, tu, lane, ws[warp], tile, nb, res, wait);
+        if (!done) {
             if (lane == 0) s_abort = 1;
             break;
         }
