@@ -576,10 +576,10 @@ enum StageMask : int {
 // and no first-touch page faults per picture.
 struct BuildScratch {
     std::vector<int32_t> bins[4], intra_list, itu, level, ctu_of, order;
-    // intra owner maps, one word per 4x4 unit: (generation << 40) | decode-order index of the
-    // intra TU.  An entry is valid when its generation is this picture's, so the maps need no
-    // clearing between pictures.
-    std::vector<uint64_t> owner[3];
+    // intra owner maps, one word per 4x4 unit: (generation << 24) | decode-order index of the
+    // intra TU.  An entry is valid when its generation is this picture's, so the maps need
+    // clearing only when the 8-bit generation wraps.
+    std::vector<uint32_t> owner[3];
     uint32_t gen = 0;
     std::vector<hevc_tu_t> itu_rec;
     std::vector<int4> itu_res;
@@ -686,9 +686,10 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     // (x-1 .. x+2N-1 at y-1) and column (y .. y+2N-1 at x-1).  Each distinct owner is a
     // dependency of B: an owner in B's CTU a local one, an owner in an earlier CTU an
     // external one.  B's depth is one more than its deepest dependency's: the length of the
-    // longest dependency chain over the picture that ends at B.  A unit whose samples B may not use (availability) can only add an unneeded wait,
-    // never change a sample; owners in CTUs later in raster order (decoded earlier only in
-    // tile scan) are never available and add nothing.
+    // longest dependency chain over the picture that ends at B.  A unit whose samples B may
+    // not use (availability) can only add an unneeded wait, never change a sample; owners in
+    // CTUs later in raster order (decoded earlier only in tile scan) are never available
+    // and add nothing.
     const int n_intra = (int)intra_list.size();
     auto& ictu_addr = BS.ictu_addr;
     auto& ictu_tu_off = BS.ictu_tu_off;
@@ -717,21 +718,23 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
         dep_at.resize((size_t)n_intra + 1);
         deps.clear();
         deps.reserve((size_t)n_intra * 3);
-        // owner maps: the decode-order index of the latest intra TU per 4x4 unit, in words
-        // tagged with this picture's generation (a word of another generation: no owner)
+        // owner maps: the decode-order index of the latest intra TU per 4x4 unit (24 bits),
+        // in words tagged with this picture's generation (8 bits; a word of another
+        // generation: no owner)
+        if (n_intra >= (1 << 24)) return fail(HEVCGPU_EINVAL, "%d intra TUs in one picture", n_intra);
         auto& owner = BS.owner;
         int uw[3], uh[3];
-        if (++BS.gen == (1u << 24)) {   // wrapped: no old word may carry the new generation
-            for (auto& m : owner) std::fill(m.begin(), m.end(), 0ull);
+        if (++BS.gen == 256u) {   // wrapped: no old word may carry the new generation
+            for (auto& m : owner) std::fill(m.begin(), m.end(), 0u);
             BS.gen = 1;
         }
-        const uint64_t gtag = (uint64_t)BS.gen << 40;
-        constexpr uint64_t GEN_BITS = ~((1ull << 40) - 1);
+        const uint32_t gtag = BS.gen << 24;
+        constexpr uint32_t GEN_BITS = 0xFF000000u;
         for (int c = 0; c < 3; c++) {
             uw[c] = (c ? W / 2 : W) / 4;
             uh[c] = (c ? H / 2 : H) / 4;
             const size_t nu = (size_t)uw[c] * uh[c];
-            if (owner[c].size() < nu) owner[c].resize(nu, 0ull);
+            if (owner[c].size() < nu) owner[c].resize(nu, 0u);
         }
         for (int b = 0; b < n_intra; b++) {
             const hevc_tu_t& t = s->tus[intra_list[(size_t)b]];
@@ -739,14 +742,14 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
             const int a = ((t.y * sub) >> p.log2_ctb) * wctb + ((t.x * sub) >> p.log2_ctb);
             ctu_of[(size_t)b] = a;
             dep_at[(size_t)b] = (int32_t)deps.size();
-            uint64_t* own = owner[c].data();
+            uint32_t* own = owner[c].data();
             const int row = uw[c];
             int dp = 0;
-            uint64_t last = 0;   // a run of units with one owner adds what its first unit added
-            auto dep = [&](uint64_t o) {
+            uint32_t last = 0;   // a run of units with one owner adds what its first unit added
+            auto dep = [&](uint32_t o) {
                 if ((o & GEN_BITS) != gtag || o == last) return;
                 last = o;
-                const int32_t ob = (int32_t)(o & 0xFFFFFFFFull);
+                const int32_t ob = (int32_t)(o & 0xFFFFFFu);
                 const int oa = ctu_of[(size_t)ob];
                 // a CTU later in raster order is never available to this one
                 // (intra_prediction.cpp:113); in tile scan one can be decoded earlier (the
@@ -768,9 +771,9 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
                 for (int uy = uy0; uy <= uy1; uy++) dep(own[(size_t)uy * row + lx]);
             }
             level[(size_t)b] = dp;
-            const uint64_t mark = gtag | (uint64_t)(uint32_t)b;
+            const uint32_t mark = gtag | (uint32_t)b;
             for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++) {
-                uint64_t* r = own + (size_t)uy * row;
+                uint32_t* r = own + (size_t)uy * row;
                 for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) r[ux] = mark;
             }
         }
@@ -837,19 +840,30 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
             }
         }
         ictu_tu_off.push_back(n_intra);
-        // residual offsets inside each CTU's staged residuals (coded TUs, in itu order); the
-        // task-order record carries its TU's offset there in coeff_offset, and in reserved[0]
-        // whether a TU of another CTU depends on it (it then publishes its completion)
+        // Per CTU in task order: the task-order records (coeff_offset: the TU's offset in the
+        // CTU's staged residuals; reserved[0]: ITU_PUBLISH when a TU of another CTU depends on
+        // it), the residual staging entries and the dependency lists.  A dependency on a TU
+        // of another CTU goes through the CTU's watcher: the distinct such TUs, in the order
+        // their first dependent TU comes, each get a watch slot, and the entry names the slot
+        // (INTRA_DEP_WATCH).  Earlier CTUs come first, so the records those entries mark are
+        // already written.
         itu_res.assign((size_t)n_intra, make_int4(-1, 0, 0, 0));
         itu_rec.resize((size_t)n_intra);
         itu_dep.resize((size_t)n_intra);
         dep_out.reserve(deps.size() + 1);
         const int nic = (int)ictu_addr.size();
+        auto& watch = BS.watch;
+        auto& slot_of = BS.slot_of;   // (CTU index << 8) | slot of a watched TU, by task index
+        watch.clear();
+        ictu_watch.assign((size_t)nic, 0u);
+        slot_of.assign((size_t)n_intra, -1);
         for (int k = 0; k < nic; k++) {
-            int acc = 0;
+            int acc = 0, nw = 0;
+            const uint32_t w0 = (uint32_t)watch.size();
             const int t0 = ictu_tu_off[(size_t)k], t1 = ictu_tu_off[(size_t)k + 1];
             if (t1 - t0 > IC_MAX_TUS)
                 return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", ictu_addr[(size_t)k]);
+            const int a = ictu_addr[(size_t)k];
             for (int i = t0; i < t1; i++) {
                 const int b = order[(size_t)i];
                 const hevc_tu_t& t = s->tus[itu[(size_t)i]];
@@ -861,8 +875,20 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
                 itu_dep[(size_t)i] = ((uint32_t)dep_out.size() << 6) | (uint32_t)(d1 - d0);
                 for (int q = d0; q < d1; q++) {
                     const int ob = deps[(size_t)q], oi = pos[(size_t)ob];
-                    dep_out.push_back(ctu_of[(size_t)ob] == ctu_of[(size_t)b] ? (uint32_t)(oi - t0)
-                                                                              : (INTRA_DEP_EXTERNAL | (uint32_t)oi));
+                    if (ctu_of[(size_t)ob] == a) {
+                        dep_out.push_back((uint32_t)(oi - t0));
+                        continue;
+                    }
+                    int32_t& so = slot_of[(size_t)oi];
+                    if (so < 0 || (so >> 8) != k) {
+                        if (nw == IC_MAX_WATCH)
+                            return fail(HEVCGPU_EINVAL, "CTU %d reads from more than %d intra TUs of other CTUs", a,
+                                        IC_MAX_WATCH);
+                        so = (k << 8) | nw++;
+                        watch.push_back((uint32_t)oi);
+                        itu_rec[(size_t)oi].reserved[0] = ITU_PUBLISH;
+                    }
+                    dep_out.push_back(INTRA_DEP_WATCH | (uint32_t)(so & 0xFF));
                 }
                 if (!(t.flags & HEVC_TU_CODED)) continue;
                 const int nn = 1 << (2 * t.log2_size);
@@ -871,38 +897,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
                 acc += nn;
             }
             if (acc > IC_MAX_RES)
-                return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", ictu_addr[(size_t)k]);
-        }
-        // External dependencies go through the CTU's watcher: per CTU, the distinct TUs of
-        // other CTUs its TUs depend on, in the order their first dependent TU comes, each with
-        // a watch slot; the dependency entry names the slot (INTRA_DEP_WATCH).  Those TUs
-        // publish their completion.
-        auto& watch = BS.watch;
-        auto& slot_of = BS.slot_of;   // (CTU index << 8 | slot) of a watched TU, per task entry
-        watch.clear();
-        ictu_watch.assign((size_t)nic, 0u);
-        slot_of.assign((size_t)n_intra, -1);
-        for (int k = 0; k < nic; k++) {
-            const uint32_t w0 = (uint32_t)watch.size();
-            int nw = 0;
-            for (int i = ictu_tu_off[(size_t)k]; i < ictu_tu_off[(size_t)k + 1]; i++) {
-                const uint32_t dd = itu_dep[(size_t)i];
-                for (uint32_t q = dd >> 6; q < (dd >> 6) + (dd & 63u); q++) {
-                    uint32_t& e = dep_out[q];
-                    if (!(e & INTRA_DEP_EXTERNAL)) continue;
-                    const uint32_t g = e & ~INTRA_DEP_EXTERNAL;
-                    int32_t& so = slot_of[g];
-                    if (so < 0 || (so >> 8) != k) {
-                        if (nw == IC_MAX_WATCH)
-                            return fail(HEVCGPU_EINVAL, "CTU %d reads from more than %d intra TUs of other CTUs",
-                                        ictu_addr[(size_t)k], IC_MAX_WATCH);
-                        so = (k << 8) | nw++;
-                        watch.push_back(g);
-                        itu_rec[g].reserved[0] = ITU_PUBLISH;
-                    }
-                    e = INTRA_DEP_WATCH | (uint32_t)(so & 0xFF);
-                }
-            }
+                return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", a);
             ictu_watch[(size_t)k] = (w0 << 8) | (uint32_t)nw;
         }
         // one spare entry: an external dependency of task 0 on itself (the planted wait of
