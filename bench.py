@@ -326,13 +326,19 @@ class ClockSampler:
 
 # --------------------------------------------------------------------------- CPU arms
 
+_CPU_POOLS = {}
+
+
 def cpu_run(checker, seq, first, n_pictures, threads):
     """Reconstruct n_pictures of the work list seq (round robin from index first) on host
-    threads."""
+    threads of a pool that persists across calls (its threads start once)."""
     from concurrent.futures import ThreadPoolExecutor
+    ex = _CPU_POOLS.get(threads)
+    if ex is None:
+        ex = _CPU_POOLS[threads] = ThreadPoolExecutor(max_workers=threads)
+        list(ex.map(lambda i: None, range(4 * threads)))   # start the threads
     t0 = time.perf_counter()
-    with ThreadPoolExecutor(max_workers=threads) as ex:
-        list(ex.map(lambda i: checker.reconstruct_picture(*seq[(first + i) % len(seq)]), range(n_pictures)))
+    list(ex.map(lambda i: checker.reconstruct_picture(*seq[(first + i) % len(seq)]), range(n_pictures)))
     return time.perf_counter() - t0
 
 
@@ -540,11 +546,13 @@ def run_ours(args, hb, rank, world, local):
         per_stage[k] = {"ms_per_gop": round(ms, 4), "alg_bytes_per_gop": alg_sum[k], "GB/s": round(gbs, 1),
                         "frac_of_hbm": round(gbs / peak, 4)}
     dom = max(stage_ms, key=lambda k: stage_ms[k])
-    # DRAM bytes (read + write) per batch of each stage's kernels on this workload: one ncu
-    # capture of a GOP of 2 streams at 1080p, scaled by 4 to 8 pictures per launch (each
-    # picture is independent work), the GOP's total divided by its 60 batches
-    # (profiles/kernels_gop8_1080p.md)
-    ncu_dram_gop8 = {"mc": 57565798, "residual": 83249101, "intra": 26371635, "deblock": 78732544, "sao": 25039838}
+    # DRAM bytes (read + write) per batch of each stage's kernels on this workload, from one
+    # ncu capture of a GOP of 2 streams at 1080p (ncu --metrics dram__bytes_read.sum,
+    # dram__bytes_write.sum --clock-control none python bench.py --profile-only --steps 1
+    # --warmup 0 --streams 2), scaled by 4 to 8 pictures per launch (each picture is
+    # independent work), the GOP's total divided by its 60 batches; taken again whenever the
+    # stage's kernels change
+    ncu_dram_gop8 = {"mc": 57523456, "residual": 83246882, "intra": 26904610, "deblock": 78733380, "sao": 25038301}
     traffic = (ncu_dram_gop8[dom] if dom in ncu_dram_gop8 and (W, H, G, F) == (W_DEFAULT, H_DEFAULT, 8, 60)
                else None)
 
@@ -644,14 +652,79 @@ def run_ours(args, hb, rank, world, local):
         t_probe = cpu_run(checker, seq, 0, len(seq), threads)
         reps = max(1, int(round(10.0 / max(t_probe, 1e-3))))
         t = cpu_run(checker, seq, 0, reps * len(seq), threads)
+        # one thread: a bounded sample (about 5 s) of pictures spread evenly over the GOP work
+        # list, so that it holds I and P/B pictures in the GOP's proportion
+        n1 = min(len(seq), max(G, int(round(5.0 / max(t_probe * threads / len(seq), 1e-4)))))
+        t0_1 = time.perf_counter()
+        for i in range(n1):
+            checker.reconstruct_picture(*seq[(i * len(seq)) // n1])
+        t1 = time.perf_counter() - t0_1
         line["cpu_baseline"] = {"value": round(reps * len(seq) / t, 3), "unit": "frames/s", "cores": threads,
                                 "kind": kind, "sample": f"{reps} GOP(s) of {G} streams x {F} pictures "
-                                f"({reps * len(seq)} pictures) on {threads} host threads ({t:.1f} s)"}
+                                f"({reps * len(seq)} pictures) on {threads} host threads ({t:.1f} s)",
+                                "single_thread": {"value": round(n1 / t1, 3), "unit": "frames/s", "cores": 1,
+                                                  "sample": f"{n1} pictures spread over the GOP work list on "
+                                                            f"one thread ({t1:.1f} s)"}}
+        line["dropin"] = run_dropin()
     for st in gop_streams:
         st.close()
     if world > 1:
         torch.distributed.destroy_process_group()
     return line if rank == 0 else None
+
+
+DROPIN_STREAM = "bbb1080_50f.265"
+
+
+def run_dropin(reps=3):
+    """The drop-in decoder on the reference's own 1080p stream (Big Buck Bunny, 50 pictures,
+    I/P/B, scaling lists, SAO): the whole decode through hevc_decoder_decode (src/wasm/
+    hevc_api.h:53) — NAL parsing, parameter sets, DPB logic and CABAC on this host thread,
+    reconstruction on the GPU (libhevcdec_gpu.so) — beside the reference's own build of the
+    same API (oracle/_ref/libhevcdec.so: its parser and its CPU reconstruction) on the same
+    host.  Frames/s of the decode call; both outputs checked against the reference's
+    whole-stream MD5.  The GPU decoder's context is made by an unmeasured decode of a 64x64
+    stream first (as a long-running process has it)."""
+    import hashlib
+    from hevc_b200 import decoder as D
+    import oracle
+    here = os.path.join(ROOT, "tests", "golden")
+    with open(os.path.join(here, "streams.json")) as f:
+        want = json.load(f)[DROPIN_STREAM]
+    with open(os.path.join(here, "streams", DROPIN_STREAM), "rb") as f:
+        data = f.read()
+    with open(os.path.join(here, "streams", "toy_qp30.265"), "rb") as f:
+        toy = f.read()
+    n = len(want["frames"])
+
+    def md5_of(frames):
+        return hashlib.md5(b"".join(fr.yuv_bytes() for fr in frames[-n:])).hexdigest()
+
+    out = {"stream": DROPIN_STREAM, "frames": n, "width": want["width"], "height": want["height"]}
+    ref_lib = os.path.join(oracle.HERE, "_ref", "libhevcdec.so")
+    for name, lib, warm in (("gpu", None, True), ("reference", ref_lib, False)):
+        if lib is not None and not os.path.exists(lib):
+            out[name] = {"unavailable": f"{lib} is not built"}
+            continue
+        times, ok = [], True
+        for _ in range(reps):
+            dec = D.Decoder(lib)
+            if warm and dec.decode(toy) != 0:
+                raise SystemExit("bench: drop-in warm-up decode failed: " + dec.last_error())
+            t0 = time.perf_counter()
+            rc = dec.decode(data)
+            times.append(time.perf_counter() - t0)
+            if rc != 0:
+                raise SystemExit(f"bench: {name} decode of {DROPIN_STREAM} failed: {dec.last_error()}")
+            ok = ok and md5_of(dec.frames()) == want["md5"]
+            dec.close()
+        t = statistics.median(times)
+        out[name] = {"frames_per_s": round(n / t, 2), "ms_per_frame": round(1000 * t / n, 3), "md5_ok": ok}
+    if "frames_per_s" in out.get("reference", {}):
+        out["gpu_over_reference"] = round(out["gpu"]["frames_per_s"] / out["reference"]["frames_per_s"], 2)
+    out["note"] = ("the whole decode call, CABAC included: one host thread parses in both (the stream has no "
+                   "WPP entry points), the GPU decoder reconstructs each picture while the next is parsed")
+    return out
 
 
 def run_pb16(args, hb, ctx, stream, rank, world, dev, check, rank_max, barrier):
@@ -774,29 +847,38 @@ def run_pb16(args, hb, ctx, stream, rank, world, dev, check, rank_max, barrier):
 
 
 def run_serving(args, hb, local):
-    """64 live streams of mixed resolutions, Poisson segment arrivals (serve.run_poisson)."""
+    """Live streams with Poisson segment arrivals (serve.run_poisson), latency ending when
+    each frame has landed in page-locked host memory: the mixed-resolution load of the
+    serving config, and 64 concurrent 1080p streams (the north-star latency target)."""
     from hevc_b200 import serve
     sctx = hb.Context(local)   # a serving process owns its context
-    pool = serve.PicturePool(hb, [(416, 240), (1280, 720), (1920, 1080), (3840, 2160)], pin=True)
-    # an unmeasured 2 s run first: the first use of a context's pools and launch paths in a
-    # process costs once what a long-running server pays at start-up
-    serve.run_poisson(hb, sctx, seconds=2.0, n_streams=64, seed=5, lanes=4, pool=pool)
-    res = serve.run_poisson(hb, sctx, seconds=args.serve_seconds, n_streams=64, seed=4, lanes=4, pool=pool)
+    mixed = [(416, 240), (1280, 720), (1920, 1080), (3840, 2160)]
+    pool = serve.PicturePool(hb, mixed, pin=True)
+    out = {}
+    for name, res, ratio in (("mixed", mixed, (4, 3, 2, 1)), ("1080p", [(1920, 1080)], (1,))):
+        # an unmeasured 2 s run first: the first use of a context's pools and launch paths in
+        # a process costs once what a long-running server pays at start-up
+        serve.run_poisson(hb, sctx, seconds=2.0, n_streams=64, seed=5, lanes=4, pool=pool, resolutions=res,
+                          ratio=ratio, download=True)
+        r = serve.run_poisson(hb, sctx, seconds=args.serve_seconds, n_streams=64, seed=4, lanes=4, pool=pool,
+                              resolutions=res, ratio=ratio, download=True)
+        out[name] = {
+            "streams": r["streams"], "hbm_bytes": r["hbm_bytes"], "frames": r["frames"],
+            "frames_per_s": round(r["frames_per_s"], 1), "p50_ms": round(r["p50_ms"], 2),
+            "p99_ms": round(r["p99_ms"], 2), "max_ms": round(r["max_ms"], 2),
+            "steady_p50_ms": round(r["steady_p50_ms"], 2), "steady_p99_ms": round(r["steady_p99_ms"], 2),
+            "frames_over_100ms": r["frames_over_100ms"], "worst_release_s": round(r["worst_release_s"], 3)}
     sctx.close()
-    return {
-        "workload": "64 live streams, 416x240 / 1280x720 / 1920x1080 / 3840x2160 in ratio 4:3:2:1, "
-                    "30 or 60 fps, 2-second segments (I picture, then P/B) arriving as a Poisson process "
-                    f"(seed 4) for {args.serve_seconds:g} s; 4 lanes, continuous batching",
-        "frames": res["frames"], "frames_per_s": round(res["frames_per_s"], 1),
-        "p50_ms": round(res["p50_ms"], 2), "p99_ms": round(res["p99_ms"], 2), "max_ms": round(res["max_ms"], 2),
-        "steady_p50_ms": round(res["steady_p50_ms"], 2), "steady_p99_ms": round(res["steady_p99_ms"], 2),
-        "frames_over_100ms": res["frames_over_100ms"], "worst_release_s": round(res["worst_release_s"], 3),
-        "steady": "frames released after the first 2 s, when every stream's first segment (and its "
-                  "I picture) has arrived",
-        "latency": "device completion of the picture's batch minus the picture's live release time "
-                   "(segment start + i / fps); records prepared on host workers, CABAC not included; "
-                   "frames/s is the offered load served (the run ends when the last released frame "
-                   "is done); measured after an unmeasured 2 s warm-up run on the same context"}
+    out["workload"] = ("64 live streams (mixed: 416x240 / 1280x720 / 1920x1080 / 3840x2160 in ratio 4:3:2:1; "
+                       "1080p: all 1920x1080), 30 or 60 fps, 2-second segments (I picture, then P/B) arriving "
+                       f"as a Poisson process (seed 4) for {args.serve_seconds:g} s; 4 lanes, continuous batching")
+    out["latency"] = ("from the picture's live release time (segment start + i / fps) to the moment its frame "
+                      "has landed in a page-locked host buffer (device event after the lane's copy); records "
+                      "prepared on host workers, CABAC not included; frames/s is the offered load served; "
+                      "measured after an unmeasured 2 s warm-up run on the same context")
+    out["steady"] = ("frames released after the first 2 s, when every stream's first segment (and its I "
+                     "picture) has arrived")
+    return out
 
 
 def main():

@@ -268,6 +268,7 @@ def gpu_lib():
             "hevcgpu_lane_batch_launch": ([P, C.POINTER(P), C.POINTER(C.c_int32), C.c_int32], C.c_int),
             "hevcgpu_lane_sync": ([P], C.c_int),
             "hevcgpu_lane_cuda_stream": ([P], P),
+            "hevcgpu_lane_copy_stream": ([P], P),
             "hevcgpu_lane_slots_download": ([P, C.POINTER(P), C.POINTER(C.c_int32), C.c_int32, C.POINTER(P)],
                                             C.c_int),
             "hevcgpu_lane_slots_download_async": ([P, C.POINTER(P), C.POINTER(C.c_int32), C.c_int32,
@@ -541,6 +542,11 @@ class Lane:
     @property
     def cuda_stream(self):
         return self.lib.hevcgpu_lane_cuda_stream(self.h)
+
+    @property
+    def copy_stream(self):
+        """CUDA stream of the lane's asynchronous downloads (hevcgpu_lane_copy_stream)."""
+        return self.lib.hevcgpu_lane_copy_stream(self.h)
 
     def close(self):
         if self.h and self.ctx.h:

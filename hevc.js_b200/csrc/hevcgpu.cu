@@ -2064,6 +2064,7 @@ int hevcgpu_lane_sync(hevcgpu_lane_t* lane) {
 }
 
 void* hevcgpu_lane_cuda_stream(hevcgpu_lane_t* lane) { return lane ? (void*)lane->stream : nullptr; }
+void* hevcgpu_lane_copy_stream(hevcgpu_lane_t* lane) { return lane ? (void*)lane->cstream : nullptr; }
 
 namespace {
 int jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* const* syns, int32_t n,

@@ -70,7 +70,7 @@ __device__ __forceinline__ bool intra_tu(const Pic& P, const hevc_tu_t& t, int l
     const int xc = t.x, yc = t.y;
     const int log2c = P.log2_ctb - chroma;                // CTB size in this plane
     const int rx = xc >> log2c, ry = yc >> log2c;
-    const int pw = P.width / sub, ph = P.height / sub;
+    const int pw = P.width >> chroma, ph = P.height >> chroma;
     const int ox = rx << P.log2_ctb, oy = ry << P.log2_ctb;   // CTB origin in luma samples
     const int pitch = chroma ? P.pitch_c : P.pitch_y;
     uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));
@@ -317,7 +317,7 @@ __device__ __forceinline__ bool intra_tu4(const Pic& P, const hevc_tu_t& t, int 
     const int xc = t.x, yc = t.y;
     const int log2c = P.log2_ctb - chroma;
     const int rx = xc >> log2c, ry = yc >> log2c;
-    const int pw = P.width / sub, ph = P.height / sub;
+    const int pw = P.width >> chroma, ph = P.height >> chroma;
     const int ox = rx << P.log2_ctb, oy = ry << P.log2_ctb;
     const int pitch = chroma ? P.pitch_c : P.pitch_y;
     uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));

@@ -395,8 +395,11 @@ __device__ __forceinline__ void luma_segment(int (&p)[4][4], int (&q)[4][4], int
     }
 }
 
+#ifndef HEVCGPU_DEBLOCK_MIN_CTAS
+#define HEVCGPU_DEBLOCK_MIN_CTAS 3   // CTAs of 256 threads per SM the register budget is sized for
+#endif
 template <bool VERT>
-__global__ void __launch_bounds__(256, 3) k_deblock(const __grid_constant__ SegTable st) {
+__global__ void __launch_bounds__(256, HEVCGPU_DEBLOCK_MIN_CTAS) k_deblock(const __grid_constant__ SegTable st) {
     const PicDesc& P = *st.s[blockIdx.y].pic;
     const int W = P.width, H = P.height, gw = W >> 2;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;

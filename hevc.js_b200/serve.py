@@ -11,7 +11,9 @@ released, prepares their records in one batched call on the host workers
 (hevcgpu_jobs_prepare) and launches them as one batch: pictures of many streams and
 resolutions share the kernels, and batches on different lanes overlap on the device.
 A picture's latency is its batch's completion on the device (CUDA event) minus its
-release time.
+release time; with downloads on, it ends instead when the picture's frame has landed in
+page-locked host memory (the lane's asynchronous copies, hevcgpu_lane_slots_download_async,
+timed by an event on the lane's copy stream), which is when a client could have it.
 
 The reference decoder has no counterpart: it decodes one stream, picture after picture
 (Decoder::decode_picture, src/decoding/decoder.cpp:52-304).
@@ -104,7 +106,7 @@ class Server:
     unless the preparation is slower than the stream."""
 
     def __init__(self, hb, ctx, pool, lanes=2, max_batch=64, depth=2, budget_bytes=None, content_seed=7,
-                 lookahead=4, prep_threads=None, min_batch=1, max_wait=0.0):
+                 lookahead=4, prep_threads=None, min_batch=1, max_wait=0.0, download=False):
         import torch
         self.hb, self.ctx, self.pool = hb, ctx, pool
         self.lookahead = lookahead
@@ -112,6 +114,12 @@ class Server:
         self.torch = torch
         self.lanes = [hb.Lane(ctx) for _ in range(lanes)]
         self.lane_cuda = [torch.cuda.ExternalStream(ln.cuda_stream) for ln in self.lanes]
+        # downloads: every picture's frame is copied into a page-locked host buffer of its
+        # stream (a ring of `depth` + 2 per stream, so that no copy still in flight is
+        # overwritten) and its latency ends when the copy has landed
+        self.download = download
+        self.lane_copy = [torch.cuda.ExternalStream(ln.copy_stream) for ln in self.lanes] if download else None
+        self.frames = {}
         self.max_batch, self.depth = max_batch, depth
         # a lane launches when min_batch pictures are ready or the oldest ready one has
         # waited max_wait seconds since its release
@@ -166,6 +174,10 @@ class Server:
             st.upload(slot, self.hb.content(w, h, seed + slot))
         lane = min(range(len(self.lanes)), key=lambda k: len(self.by_lane[k]))
         s = _Stream(sid, w, h, fps, st, lane, variant)
+        if self.download:
+            size = self.hb.i420_size(w, h)
+            self.frames[sid] = [self.torch.empty(size, dtype=self.torch.uint8).pin_memory().numpy()
+                                for _ in range(self.depth + 2)]
         self.streams[sid] = s
         self.by_lane[lane].append(s)
         return True
@@ -246,7 +258,12 @@ class Server:
                 self._feed(s)
             lane.batch_launch(jobs, slots)
             ev = self.torch.cuda.Event(enable_timing=True)
-            ev.record(self.lane_cuda[k])
+            if self.download:
+                outs = [self.frames[s.sid][s.n % len(self.frames[s.sid])] for s in ready]
+                lane.download_batch_async([s.st for s in ready], slots, outs)
+                ev.record(self.lane_copy[k])
+            else:
+                ev.record(self.lane_cuda[k])
             for s in ready:
                 s.n += 1
                 s.inflight += 1
@@ -272,7 +289,7 @@ class Server:
 
 def run_poisson(hb, ctx, seconds=5.0, n_streams=64, seed=4, lanes=4, max_batch=64, pool=None,
                 resolutions=((416, 240), (1280, 720), (1920, 1080), (3840, 2160)), ratio=(4, 3, 2, 1),
-                segment_s=2.0, clock=None, min_batch=8, max_wait=0.004):
+                segment_s=2.0, clock=None, min_batch=8, max_wait=0.004, download=False):
     """Serve n_streams whose segments arrive for `seconds` of wall time (the run ends when
     every queued frame is decoded): resolutions in `ratio`, 30 or 60 fps, 2-second
     segments arriving as a Poisson process per stream (mean gap = segment length, so each
@@ -283,7 +300,8 @@ def run_poisson(hb, ctx, seconds=5.0, n_streams=64, seed=4, lanes=4, max_batch=6
     rng = random.Random(seed)
     if pool is None:
         pool = PicturePool(hb, resolutions)
-    srv = Server(hb, ctx, pool, lanes=lanes, max_batch=max_batch, min_batch=min_batch, max_wait=max_wait)
+    srv = Server(hb, ctx, pool, lanes=lanes, max_batch=max_batch, min_batch=min_batch, max_wait=max_wait,
+                 download=download)
     mix = [r for r, k in zip(resolutions, ratio) for _ in range(k)]
     specs = []
     for sid in range(n_streams):
@@ -292,6 +310,7 @@ def run_poisson(hb, ctx, seconds=5.0, n_streams=64, seed=4, lanes=4, max_batch=6
         specs.append((sid, w, h, fps))
     admitted = [sid for sid, w, h, fps in specs if srv.admit(sid, w, h, fps, variant=sid)]
     srv.warm()
+    hbm = ctx.bytes_in_use()
     # the loop allocates no cycles; a cyclic collection pass over the whole process's
     # objects would stall it (for a long-running process holding many objects, by
     # hundreds of ms), so collect once now and keep the collector off while serving
@@ -329,7 +348,7 @@ def run_poisson(hb, ctx, seconds=5.0, n_streams=64, seed=4, lanes=4, max_batch=6
     # first segments, each opening with an I picture, all arrive within segment_s)
     steady = records[records[:, 0] >= t0 + segment_s, 1] * 1000.0 if len(records) else np.zeros(0)
     pct = lambda v, q: float(np.percentile(v, q)) if len(v) else None
-    return {"streams": len(admitted), "frames": int(len(lat)), "offered_frames": offered,
+    return {"streams": len(admitted), "hbm_bytes": int(hbm), "frames": int(len(lat)), "offered_frames": offered,
             "frames_per_s": len(lat) / (t_stop - t0), "p50_ms": pct(lat_ms, 50), "p99_ms": pct(lat_ms, 99),
             "max_ms": float(lat_ms.max()) if len(lat) else None, "steady_frames": int(len(steady)),
             "frames_over_100ms": int((records[:, 1] > 0.1).sum()) if len(records) else 0,

@@ -307,6 +307,10 @@ int   hevcgpu_lane_batch_launch(hevcgpu_lane_t* lane, hevcgpu_job_t* const* jobs
 int   hevcgpu_lane_sync(hevcgpu_lane_t* lane);
 /* CUDA stream (cudaStream_t) of the lane. */
 void* hevcgpu_lane_cuda_stream(hevcgpu_lane_t* lane);
+/* CUDA stream (cudaStream_t) the lane's asynchronous downloads run on: a caller records an
+ * event there after hevcgpu_lane_slots_download_async to learn on the device when the
+ * frames landed (the serving loop's latency ends there). */
+void* hevcgpu_lane_copy_stream(hevcgpu_lane_t* lane);
 /* hevcgpu_slots_download with the copies queued on the lane, after its batches: the
  * pictures of a lane batch can be read back without waiting for the other lanes.
  * Returns the lane's device status, like hevcgpu_lane_sync. */

@@ -18,7 +18,9 @@
 #include <array>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <tuple>
 #include <vector>
 
 #include "common/picture.h"
@@ -58,6 +60,9 @@ struct Env {
     std::vector<uint8_t> cbf, tu_log2, edge_v, edge_h, slice_idx;
     std::vector<DecodingContext::SaoParams> sao;
     std::vector<uint16_t> sao_backup[3];
+    // the PPS and slice header a PU's weighted prediction selects, built once per (WP row,
+    // refIdxL0, refIdxL1) of the picture (the default form under the key (-1, 0, 0))
+    std::map<std::tuple<int, int, int>, std::pair<PPS, SliceHeader>> wp_forms;
     DecodingContext ctx;
     int W = 0, H = 0;
 };
@@ -287,13 +292,18 @@ void set_pu_wp(Env& e, const hevc_pu_t& pu, const hevc_wp_t* wp_tab, PPS& pps, S
 }
 
 void mc_pu(Env& e, const hevc_pu_t& pu, const hevc_wp_t* wp_tab) {
-    PPS pps;
-    SliceHeader sh;
-    set_pu_wp(e, pu, wp_tab, pps, sh);
+    const auto key = pu.wp < 0 ? std::make_tuple(-1, 0, 0)
+                               : std::make_tuple((int)pu.wp, pu.ref_idx[0] >= 0 ? (int)pu.ref_idx[0] : 0,
+                                                 pu.ref_idx[1] >= 0 ? (int)pu.ref_idx[1] : 0);
+    auto it = e.wp_forms.find(key);
+    if (it == e.wp_forms.end()) {
+        it = e.wp_forms.emplace(key, std::pair<PPS, SliceHeader>()).first;
+        set_pu_wp(e, pu, wp_tab, it->second.first, it->second.second);
+    }
     const PPS* saved_pps = e.ctx.pps;
     const SliceHeader* saved_sh = e.ctx.sh;
-    e.ctx.pps = &pps;
-    e.ctx.sh = &sh;
+    e.ctx.pps = &it->second.first;
+    e.ctx.sh = &it->second.second;
     MV mv0, mv1;
     mv0.x = pu.mv[0][0]; mv0.y = pu.mv[0][1];
     mv1.x = pu.mv[1][0]; mv1.y = pu.mv[1][1];
