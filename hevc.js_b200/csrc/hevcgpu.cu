@@ -389,6 +389,18 @@ struct hevcgpu_stream {
 // ---------------------------------------------------------------------------------------
 // jobs: one picture's records, prepared and uploaded
 // ---------------------------------------------------------------------------------------
+// A CUDA call of a job's preparation: a host->device copy, zeroing device memory, or
+// recording the event that marks the copies straight from the caller's arrays as done.
+// Prepared on the context's host workers, the calls are queued in the job and issued by
+// the thread that asked for the batch, so that the workers make no CUDA calls (which would
+// contend for the driver's locks) and every upload goes out from one thread in order.
+struct UploadOp {
+    enum Kind : int { COPY, ZERO, MARK_DIRECT } kind;
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+
 struct hevcgpu_job {
     hevcgpu_ctx* ctx = nullptr;
     hevcgpu_stream* st = nullptr;  // may be null for stage entry points
@@ -418,6 +430,7 @@ struct hevcgpu_job {
     cudaEvent_t last_done = nullptr;    // recorded after that launch
     bool registered = false;            // in ctx->live_jobs
     uint64_t upload_bytes = 0;          // host -> device bytes of the prepare call
+    std::vector<UploadOp> ops;          // CUDA calls of the preparation not yet issued
     hevc_pic_params_t params{};
     ~hevcgpu_job() {
         // buffers go back to the pools only after every queued use of them has run: a job's
@@ -593,7 +606,266 @@ struct BuildScratch {
 };
 thread_local BuildScratch t_build;
 
-int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool wait_uploads = true) {
+// Issue one queued CUDA call of a job's preparation on the context stream.
+int run_upload(hevcgpu_job* j, const UploadOp& o) {
+    cudaStream_t cs = j->ctx->stream;
+    switch (o.kind) {
+    case UploadOp::COPY:
+        CUDA_TRY(cudaMemcpyAsync(o.dst, o.src, o.bytes, cudaMemcpyHostToDevice, cs));
+        break;
+    case UploadOp::ZERO:
+        CUDA_TRY(cudaMemsetAsync(o.dst, 0, o.bytes, cs));
+        break;
+    case UploadOp::MARK_DIRECT:
+        if (!j->direct_read) CUDA_TRY(cudaEventCreateWithFlags(&j->direct_read, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventRecord(j->direct_read, cs));
+        break;
+    }
+    return HEVCGPU_OK;
+}
+
+// Issue the calls a deferred job_build queued, in order.
+int job_issue(hevcgpu_job* j) {
+    int rc = HEVCGPU_OK;
+    for (const UploadOp& o : j->ops)
+        if ((rc = run_upload(j, o))) break;
+    j->ops.clear();
+    return rc;
+}
+
+// defer: queue the CUDA calls in j->ops (job_issue issues them) instead of making them.
+// The intra schedule of a picture (the intra TUs of BS.intra_list, in decode order): the
+// CTUs that hold intra TUs in wavefront order, their TUs in task order, each TU's
+// dependency list and each CTU's watch list (intra.cuh, k_intra_ctus).  *spare_dep
+// receives the index of the spare dependency entry (hevcgpu_job_plant_unmet_wait).
+int build_intra_schedule(BuildScratch& BS, const hevc_picture_syntax_t* s, uint32_t* spare_dep) {
+    const hevc_pic_params_t& p = s->params;
+    const int W = p.width, H = p.height;
+    const int ctb = 1 << p.log2_ctb;
+    const int wctb = (W + ctb - 1) / ctb, hctb = (H + ctb - 1) / ctb, nctb = wctb * hctb;
+    (void)hctb;
+    const auto& intra_list = BS.intra_list;
+    const int n_intra = (int)intra_list.size();
+    auto& ictu_addr = BS.ictu_addr;
+    auto& ictu_tu_off = BS.ictu_tu_off;
+    auto& itu = BS.itu;
+    auto& itu_rec = BS.itu_rec;
+    auto& itu_res = BS.itu_res;
+    auto& itu_dep = BS.itu_dep;
+    auto& dep_out = BS.dep_out;
+    auto& ictu_watch = BS.ictu_watch;
+    ictu_addr.clear();
+    ictu_watch.clear();
+    BS.watch.clear();
+    ictu_tu_off.clear();
+    itu.clear();
+    itu_rec.clear();
+    itu_res.clear();
+    itu_dep.clear();
+    dep_out.clear();
+    if (!n_intra) return HEVCGPU_OK;
+    auto& level = BS.level;
+    auto& ctu_of = BS.ctu_of;
+    auto& dep_at = BS.dep_at;       // decode order: first entry of TU b's owners in deps
+    auto& deps = BS.deps;           // decode-order indices of the owners, per TU
+    level.resize((size_t)n_intra);
+    ctu_of.resize((size_t)n_intra);
+    dep_at.resize((size_t)n_intra + 1);
+    deps.clear();
+    deps.reserve((size_t)n_intra * 3);
+    // owner maps: the decode-order index of the latest intra TU per 4x4 unit (24 bits),
+    // in words tagged with this picture's generation (8 bits; a word of another
+    // generation: no owner)
+    if (n_intra >= (1 << 24)) return fail(HEVCGPU_EINVAL, "%d intra TUs in one picture", n_intra);
+    auto& owner = BS.owner;
+    int uw[3], uh[3];
+    if (++BS.gen == 256u) {   // wrapped: no old word may carry the new generation
+        for (auto& m : owner) std::fill(m.begin(), m.end(), 0u);
+        BS.gen = 1;
+    }
+    const uint32_t gtag = BS.gen << 24;
+    constexpr uint32_t GEN_BITS = 0xFF000000u;
+    for (int c = 0; c < 3; c++) {
+        uw[c] = (c ? W / 2 : W) / 4;
+        uh[c] = (c ? H / 2 : H) / 4;
+        const size_t nu = (size_t)uw[c] * uh[c];
+        if (owner[c].size() < nu) owner[c].resize(nu, 0u);
+    }
+    for (int b = 0; b < n_intra; b++) {
+        const hevc_tu_t& t = s->tus[intra_list[(size_t)b]];
+        const int c = t.c_idx, n = 1 << t.log2_size, sub = c ? 2 : 1;
+        const int a = ((t.y * sub) >> p.log2_ctb) * wctb + ((t.x * sub) >> p.log2_ctb);
+        ctu_of[(size_t)b] = a;
+        dep_at[(size_t)b] = (int32_t)deps.size();
+        uint32_t* own = owner[c].data();
+        const int row = uw[c];
+        int dp = 0;
+        uint32_t last = 0;   // a run of units with one owner adds what its first unit added
+        auto dep = [&](uint32_t o) {
+            if ((o & GEN_BITS) != gtag || o == last) return;
+            last = o;
+            const int32_t ob = (int32_t)(o & 0xFFFFFFu);
+            const int oa = ctu_of[(size_t)ob];
+            // a CTU later in raster order is never available to this one
+            // (intra_prediction.cpp:113); in tile scan one can be decoded earlier (the
+            // tile to the left, below-left), and waiting for it could wait for a CTA not
+            // yet started: CTAs take CTUs in raster order
+            if (oa > a) return;
+            for (size_t q = (size_t)dep_at[(size_t)b]; q < deps.size(); q++)
+                if (deps[q] == ob) return;
+            deps.push_back(ob);
+            dp = std::max(dp, level[(size_t)ob] + 1);   // local and external dependencies alike
+        };
+        const int ux = t.x / 4, uy = t.y / 4;
+        if (t.y > 0) {
+            const size_t rrow = (size_t)((t.y - 1) / 4) * row;
+            const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(row - 1, (t.x + 2 * n - 1) / 4);
+            for (int x = ux0; x <= ux1; x++) dep(own[rrow + x]);
+        }
+        if (t.x > 0) {
+            const int lx = (t.x - 1) / 4, uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
+            for (int y = uy0; y <= uy1; y++) dep(own[(size_t)y * row + lx]);
+        }
+        level[(size_t)b] = dp;
+        const uint32_t mark = gtag | (uint32_t)b;
+        for (int y = uy; y < uy + n / 4; y++) {
+            uint32_t* r = own + (size_t)y * row;
+            for (int x = ux; x < ux + n / 4; x++) r[x] = mark;
+        }
+    }
+    dep_at[(size_t)n_intra] = (int32_t)deps.size();
+    // Task order: CTUs in wavefront order (key 2 * row + column, then raster), each
+    // CTU's TUs by depth (every TU after the TUs it depends on, and about in the order
+    // they can run), then decode order.  CTAs take CTUs by ticket in this order, so
+    // the CTUs held by resident CTAs are those of the diagonal band the picture's
+    // dependencies advance along (a row trails the one above by two CTUs), not whole
+    // rows in raster order.  Every CTU a CTU reads from (left, above-left, above,
+    // above-right) has a smaller key, so a CTA only waits for CTUs taken before its own.
+    auto wave = [&](int a) { return (int64_t)(2 * (a / wctb) + a % wctb) * nctb + a; };
+    auto& order = BS.order;
+    order.resize((size_t)n_intra);
+    bool grouped = true;   // the TUs come CTU by CTU (decode order without WPP threads)
+    auto& runs = BS.runs;
+    runs.clear();
+    for (int b = 0; b < n_intra; b++)
+        if (b == 0 || ctu_of[(size_t)b] != ctu_of[(size_t)b - 1]) runs.push_back({wave(ctu_of[(size_t)b]), b});
+    {   // a CTU must form a single run: no two runs with one key
+        const int nr = (int)runs.size();
+        runs.push_back({INT64_MAX, n_intra});
+        std::vector<std::pair<int64_t, int32_t>> sorted(runs.begin(), runs.end() - 1);
+        for (int q = 0; q < nr; q++) sorted[(size_t)q].second = q;
+        std::sort(sorted.begin(), sorted.end());
+        for (int q = 1; q < nr && grouped; q++) grouped = sorted[(size_t)q].first != sorted[(size_t)q - 1].first;
+        if (grouped) {
+            auto& cnt = BS.cnt;
+            int at = 0;
+            for (int q = 0; q < nr; q++) {
+                const int rq = sorted[(size_t)q].second;
+                const int r0 = runs[(size_t)rq].second, r1 = runs[(size_t)rq + 1].second;
+                int minl = level[(size_t)r0], maxl = minl;
+                for (int b = r0; b < r1; b++) {
+                    minl = std::min(minl, level[(size_t)b]);
+                    maxl = std::max(maxl, level[(size_t)b]);
+                }
+                cnt.assign((size_t)(maxl - minl) + 2, 0);
+                for (int b = r0; b < r1; b++) cnt[(size_t)(level[(size_t)b] - minl) + 1]++;
+                for (int l = 1; l <= maxl - minl + 1; l++) cnt[(size_t)l] += cnt[(size_t)l - 1];
+                for (int b = r0; b < r1; b++) order[(size_t)(at + cnt[(size_t)(level[(size_t)b] - minl)]++)] = b;
+                at += r1 - r0;
+            }
+        }
+    }
+    if (!grouped) {
+        for (int b = 0; b < n_intra; b++) order[(size_t)b] = b;
+        std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+            const int64_t wx = wave(ctu_of[(size_t)x]), wy = wave(ctu_of[(size_t)y]);
+            if (wx != wy) return wx < wy;
+            return level[(size_t)x] < level[(size_t)y];
+        });
+    }
+    auto& pos = BS.pos;   // decode order -> task order
+    pos.resize((size_t)n_intra);
+    itu.resize((size_t)n_intra);
+    for (int i = 0; i < n_intra; i++) {
+        const int b = order[(size_t)i];
+        pos[(size_t)b] = i;
+        itu[(size_t)i] = intra_list[(size_t)b];
+        if (i == 0 || ctu_of[(size_t)b] != ctu_of[(size_t)order[(size_t)i - 1]]) {
+            ictu_addr.push_back(ctu_of[(size_t)b]);
+            ictu_tu_off.push_back(i);
+        }
+    }
+    ictu_tu_off.push_back(n_intra);
+    // Per CTU in task order: the task-order records (coeff_offset: the TU's offset in the
+    // CTU's staged residuals; reserved[0]: ITU_PUBLISH when a TU of another CTU depends on
+    // it), the residual staging entries and the dependency lists.  A dependency on a TU
+    // of another CTU goes through the CTU's watcher: the distinct such TUs, in the order
+    // their first dependent TU comes, each get a watch slot, and the entry names the slot
+    // (INTRA_DEP_WATCH).  Earlier CTUs come first, so the records those entries mark are
+    // already written.
+    itu_res.assign((size_t)n_intra, make_int4(-1, 0, 0, 0));
+    itu_rec.resize((size_t)n_intra);
+    itu_dep.resize((size_t)n_intra);
+    dep_out.reserve(deps.size() + 1);
+    const int nic = (int)ictu_addr.size();
+    auto& watch = BS.watch;
+    auto& slot_of = BS.slot_of;   // (CTU index << 8) | slot of a watched TU, by task index
+    watch.clear();
+    ictu_watch.assign((size_t)nic, 0u);
+    slot_of.assign((size_t)n_intra, -1);
+    for (int k = 0; k < nic; k++) {
+        int acc = 0, nw = 0;
+        const uint32_t w0 = (uint32_t)watch.size();
+        const int t0 = ictu_tu_off[(size_t)k], t1 = ictu_tu_off[(size_t)k + 1];
+        if (t1 - t0 > IC_MAX_TUS)
+            return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", ictu_addr[(size_t)k]);
+        const int a = ictu_addr[(size_t)k];
+        for (int i = t0; i < t1; i++) {
+            const int b = order[(size_t)i];
+            const hevc_tu_t& t = s->tus[itu[(size_t)i]];
+            hevc_tu_t& r = itu_rec[(size_t)i];
+            r = t;
+            r.coeff_offset = 0;
+            r.reserved[0] = 0;
+            const int d0 = dep_at[(size_t)b], d1 = dep_at[(size_t)b + 1];
+            itu_dep[(size_t)i] = ((uint32_t)dep_out.size() << 6) | (uint32_t)(d1 - d0);
+            for (int q = d0; q < d1; q++) {
+                const int ob = deps[(size_t)q], oi = pos[(size_t)ob];
+                if (ctu_of[(size_t)ob] == a) {
+                    dep_out.push_back((uint32_t)(oi - t0));
+                    continue;
+                }
+                int32_t& so = slot_of[(size_t)oi];
+                if (so < 0 || (so >> 8) != k) {
+                    if (nw == IC_MAX_WATCH)
+                        return fail(HEVCGPU_EINVAL, "CTU %d reads from more than %d intra TUs of other CTUs", a,
+                                    IC_MAX_WATCH);
+                    so = (k << 8) | nw++;
+                    watch.push_back((uint32_t)oi);
+                    itu_rec[(size_t)oi].reserved[0] = ITU_PUBLISH;
+                }
+                dep_out.push_back(INTRA_DEP_WATCH | (uint32_t)(so & 0xFF));
+            }
+            if (!(t.flags & HEVC_TU_CODED)) continue;
+            const int nn = 1 << (2 * t.log2_size);
+            itu_res[(size_t)i] = make_int4((int)t.coeff_offset, acc, nn / 8, 0);
+            r.coeff_offset = (uint32_t)acc;
+            acc += nn;
+        }
+        if (acc > IC_MAX_RES)
+            return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", a);
+        ictu_watch[(size_t)k] = (w0 << 8) | (uint32_t)nw;
+    }
+    // one spare entry: an external dependency of task 0 on itself (the planted wait of
+    // hevcgpu_job_plant_unmet_wait points task 0's list at it)
+    *spare_dep = (uint32_t)dep_out.size();
+    dep_out.push_back(INTRA_DEP_EXTERNAL | 0u);
+    if (dep_out.size() >= (1u << 26)) return fail(HEVCGPU_EINVAL, "intra dependency lists too long");
+    return HEVCGPU_OK;
+}
+
+int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool wait_uploads = true,
+              bool defer = false) {
     BuildScratch& BS = t_build;
     hevcgpu_ctx* ctx = j->ctx;
     const hevc_pic_params_t& p = s->params;
@@ -629,6 +901,11 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     big_bytes = std::max<size_t>(big_bytes, 256);
     int rc = j->big.get(ctx, big_bytes);
     if (rc) return rc;
+    auto up = [&](const UploadOp& o) -> int {
+        if (!defer) return run_upload(j, o);
+        j->ops.push_back(o);
+        return HEVCGPU_OK;
+    };
     if (any_staged && (rc = j->pin_big.get(ctx, big_bytes))) return rc;
     // Page-locked arrays that sit in one block in this same layout (each at its offset from
     // one base, as a recorder that lays them out so puts them) go up in one copy: the gaps
@@ -648,8 +925,8 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
         used = b.off + b.bytes;
     }
     if (one_block && host0) {
-        CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->big.p) + first, host0 + first, used - first,
-                                 cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = up({UploadOp::COPY, static_cast<uint8_t*>(j->big.p) + first, host0 + first, used - first})))
+            return rc;
     } else {
         for (const BigArray& b : big) {
             if (!b.bytes) continue;
@@ -658,14 +935,11 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
                 std::memcpy(static_cast<uint8_t*>(j->pin_big.p) + b.off, b.src, b.bytes);
                 from = static_cast<uint8_t*>(j->pin_big.p) + b.off;
             }
-            CUDA_TRY(cudaMemcpyAsync(static_cast<uint8_t*>(j->big.p) + b.off, from, b.bytes, cudaMemcpyHostToDevice,
-                                     ctx->stream));
+            if ((rc = up({UploadOp::COPY, static_cast<uint8_t*>(j->big.p) + b.off, from, b.bytes}))) return rc;
         }
     }
-    if (any_direct) {   // the caller's arrays must have been read before this call returns
-        if (!j->direct_read) CUDA_TRY(cudaEventCreateWithFlags(&j->direct_read, cudaEventDisableTiming));
-        CUDA_TRY(cudaEventRecord(j->direct_read, ctx->stream));
-    }
+    // the caller's arrays must have been read before this call returns
+    if (any_direct && (rc = up({UploadOp::MARK_DIRECT, nullptr, nullptr, 0}))) return rc;
 
     // residual bins (coded TUs by size) and the intra TUs in decode order
     auto& bins = BS.bins;
@@ -693,219 +967,12 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     const int n_intra = (int)intra_list.size();
     auto& ictu_addr = BS.ictu_addr;
     auto& ictu_tu_off = BS.ictu_tu_off;
-    auto& itu = BS.itu;
     auto& itu_rec = BS.itu_rec;         // intra TU records in task order
     auto& itu_res = BS.itu_res;         // per task entry: residual source, staged offset, 16-byte chunks
     auto& itu_dep = BS.itu_dep;         // per task entry: (dependency list offset << 6) | count
     auto& dep_out = BS.dep_out;         // dependency lists in task order
     auto& ictu_watch = BS.ictu_watch;   // per CTU: (offset in watch << 8) | count
-    ictu_addr.clear();
-    ictu_watch.clear();
-    BS.watch.clear();
-    ictu_tu_off.clear();
-    itu.clear();
-    itu_rec.clear();
-    itu_res.clear();
-    itu_dep.clear();
-    dep_out.clear();
-    if (n_intra) {
-        auto& level = BS.level;
-        auto& ctu_of = BS.ctu_of;
-        auto& dep_at = BS.dep_at;       // decode order: first entry of TU b's owners in deps
-        auto& deps = BS.deps;           // decode-order indices of the owners, per TU
-        level.resize((size_t)n_intra);
-        ctu_of.resize((size_t)n_intra);
-        dep_at.resize((size_t)n_intra + 1);
-        deps.clear();
-        deps.reserve((size_t)n_intra * 3);
-        // owner maps: the decode-order index of the latest intra TU per 4x4 unit (24 bits),
-        // in words tagged with this picture's generation (8 bits; a word of another
-        // generation: no owner)
-        if (n_intra >= (1 << 24)) return fail(HEVCGPU_EINVAL, "%d intra TUs in one picture", n_intra);
-        auto& owner = BS.owner;
-        int uw[3], uh[3];
-        if (++BS.gen == 256u) {   // wrapped: no old word may carry the new generation
-            for (auto& m : owner) std::fill(m.begin(), m.end(), 0u);
-            BS.gen = 1;
-        }
-        const uint32_t gtag = BS.gen << 24;
-        constexpr uint32_t GEN_BITS = 0xFF000000u;
-        for (int c = 0; c < 3; c++) {
-            uw[c] = (c ? W / 2 : W) / 4;
-            uh[c] = (c ? H / 2 : H) / 4;
-            const size_t nu = (size_t)uw[c] * uh[c];
-            if (owner[c].size() < nu) owner[c].resize(nu, 0u);
-        }
-        for (int b = 0; b < n_intra; b++) {
-            const hevc_tu_t& t = s->tus[intra_list[(size_t)b]];
-            const int c = t.c_idx, n = 1 << t.log2_size, sub = c ? 2 : 1;
-            const int a = ((t.y * sub) >> p.log2_ctb) * wctb + ((t.x * sub) >> p.log2_ctb);
-            ctu_of[(size_t)b] = a;
-            dep_at[(size_t)b] = (int32_t)deps.size();
-            uint32_t* own = owner[c].data();
-            const int row = uw[c];
-            int dp = 0;
-            uint32_t last = 0;   // a run of units with one owner adds what its first unit added
-            auto dep = [&](uint32_t o) {
-                if ((o & GEN_BITS) != gtag || o == last) return;
-                last = o;
-                const int32_t ob = (int32_t)(o & 0xFFFFFFu);
-                const int oa = ctu_of[(size_t)ob];
-                // a CTU later in raster order is never available to this one
-                // (intra_prediction.cpp:113); in tile scan one can be decoded earlier (the
-                // tile to the left, below-left), and waiting for it could wait for a CTA not
-                // yet started: CTAs take CTUs in raster order
-                if (oa > a) return;
-                for (size_t q = (size_t)dep_at[(size_t)b]; q < deps.size(); q++)
-                    if (deps[q] == ob) return;
-                deps.push_back(ob);
-                dp = std::max(dp, level[(size_t)ob] + 1);   // local and external dependencies alike
-            };
-            if (t.y > 0) {
-                const size_t rrow = (size_t)((t.y - 1) / 4) * row;
-                const int ux0 = t.x > 0 ? (t.x - 1) / 4 : 0, ux1 = std::min(row - 1, (t.x + 2 * n - 1) / 4);
-                for (int ux = ux0; ux <= ux1; ux++) dep(own[rrow + ux]);
-            }
-            if (t.x > 0) {
-                const int lx = (t.x - 1) / 4, uy0 = t.y / 4, uy1 = std::min(uh[c] - 1, (t.y + 2 * n - 1) / 4);
-                for (int uy = uy0; uy <= uy1; uy++) dep(own[(size_t)uy * row + lx]);
-            }
-            level[(size_t)b] = dp;
-            const uint32_t mark = gtag | (uint32_t)b;
-            for (int uy = t.y / 4; uy < (t.y + n) / 4; uy++) {
-                uint32_t* r = own + (size_t)uy * row;
-                for (int ux = t.x / 4; ux < (t.x + n) / 4; ux++) r[ux] = mark;
-            }
-        }
-        dep_at[(size_t)n_intra] = (int32_t)deps.size();
-        // Task order: CTUs in wavefront order (key 2 * row + column, then raster), each
-        // CTU's TUs by depth (every TU after the TUs it depends on, and about in the order
-        // they can run), then decode order.  CTAs take CTUs by ticket in this order, so
-        // the CTUs held by resident CTAs are those of the diagonal band the picture's
-        // dependencies advance along (a row trails the one above by two CTUs), not whole
-        // rows in raster order.  Every CTU a CTU reads from (left, above-left, above,
-        // above-right) has a smaller key, so a CTA only waits for CTUs taken before its own.
-        auto wave = [&](int a) { return (int64_t)(2 * (a / wctb) + a % wctb) * nctb + a; };
-        auto& order = BS.order;
-        order.resize((size_t)n_intra);
-        bool grouped = true;   // the TUs come CTU by CTU (decode order without WPP threads)
-        auto& runs = BS.runs;
-        runs.clear();
-        for (int b = 0; b < n_intra; b++)
-            if (b == 0 || ctu_of[(size_t)b] != ctu_of[(size_t)b - 1]) runs.push_back({wave(ctu_of[(size_t)b]), b});
-        {   // a CTU must form a single run: no two runs with one key
-            const int nr = (int)runs.size();
-            runs.push_back({INT64_MAX, n_intra});
-            std::vector<std::pair<int64_t, int32_t>> sorted(runs.begin(), runs.end() - 1);
-            for (int q = 0; q < nr; q++) sorted[(size_t)q].second = q;
-            std::sort(sorted.begin(), sorted.end());
-            for (int q = 1; q < nr && grouped; q++) grouped = sorted[(size_t)q].first != sorted[(size_t)q - 1].first;
-            if (grouped) {
-                auto& cnt = BS.cnt;
-                int at = 0;
-                for (int q = 0; q < nr; q++) {
-                    const int rq = sorted[(size_t)q].second;
-                    const int r0 = runs[(size_t)rq].second, r1 = runs[(size_t)rq + 1].second;
-                    int minl = level[(size_t)r0], maxl = minl;
-                    for (int b = r0; b < r1; b++) {
-                        minl = std::min(minl, level[(size_t)b]);
-                        maxl = std::max(maxl, level[(size_t)b]);
-                    }
-                    cnt.assign((size_t)(maxl - minl) + 2, 0);
-                    for (int b = r0; b < r1; b++) cnt[(size_t)(level[(size_t)b] - minl) + 1]++;
-                    for (int l = 1; l <= maxl - minl + 1; l++) cnt[(size_t)l] += cnt[(size_t)l - 1];
-                    for (int b = r0; b < r1; b++) order[(size_t)(at + cnt[(size_t)(level[(size_t)b] - minl)]++)] = b;
-                    at += r1 - r0;
-                }
-            }
-        }
-        if (!grouped) {
-            for (int b = 0; b < n_intra; b++) order[(size_t)b] = b;
-            std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
-                const int64_t wx = wave(ctu_of[(size_t)x]), wy = wave(ctu_of[(size_t)y]);
-                if (wx != wy) return wx < wy;
-                return level[(size_t)x] < level[(size_t)y];
-            });
-        }
-        auto& pos = BS.pos;   // decode order -> task order
-        pos.resize((size_t)n_intra);
-        itu.resize((size_t)n_intra);
-        for (int i = 0; i < n_intra; i++) {
-            const int b = order[(size_t)i];
-            pos[(size_t)b] = i;
-            itu[(size_t)i] = intra_list[(size_t)b];
-            if (i == 0 || ctu_of[(size_t)b] != ctu_of[(size_t)order[(size_t)i - 1]]) {
-                ictu_addr.push_back(ctu_of[(size_t)b]);
-                ictu_tu_off.push_back(i);
-            }
-        }
-        ictu_tu_off.push_back(n_intra);
-        // Per CTU in task order: the task-order records (coeff_offset: the TU's offset in the
-        // CTU's staged residuals; reserved[0]: ITU_PUBLISH when a TU of another CTU depends on
-        // it), the residual staging entries and the dependency lists.  A dependency on a TU
-        // of another CTU goes through the CTU's watcher: the distinct such TUs, in the order
-        // their first dependent TU comes, each get a watch slot, and the entry names the slot
-        // (INTRA_DEP_WATCH).  Earlier CTUs come first, so the records those entries mark are
-        // already written.
-        itu_res.assign((size_t)n_intra, make_int4(-1, 0, 0, 0));
-        itu_rec.resize((size_t)n_intra);
-        itu_dep.resize((size_t)n_intra);
-        dep_out.reserve(deps.size() + 1);
-        const int nic = (int)ictu_addr.size();
-        auto& watch = BS.watch;
-        auto& slot_of = BS.slot_of;   // (CTU index << 8) | slot of a watched TU, by task index
-        watch.clear();
-        ictu_watch.assign((size_t)nic, 0u);
-        slot_of.assign((size_t)n_intra, -1);
-        for (int k = 0; k < nic; k++) {
-            int acc = 0, nw = 0;
-            const uint32_t w0 = (uint32_t)watch.size();
-            const int t0 = ictu_tu_off[(size_t)k], t1 = ictu_tu_off[(size_t)k + 1];
-            if (t1 - t0 > IC_MAX_TUS)
-                return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", ictu_addr[(size_t)k]);
-            const int a = ictu_addr[(size_t)k];
-            for (int i = t0; i < t1; i++) {
-                const int b = order[(size_t)i];
-                const hevc_tu_t& t = s->tus[itu[(size_t)i]];
-                hevc_tu_t& r = itu_rec[(size_t)i];
-                r = t;
-                r.coeff_offset = 0;
-                r.reserved[0] = 0;
-                const int d0 = dep_at[(size_t)b], d1 = dep_at[(size_t)b + 1];
-                itu_dep[(size_t)i] = ((uint32_t)dep_out.size() << 6) | (uint32_t)(d1 - d0);
-                for (int q = d0; q < d1; q++) {
-                    const int ob = deps[(size_t)q], oi = pos[(size_t)ob];
-                    if (ctu_of[(size_t)ob] == a) {
-                        dep_out.push_back((uint32_t)(oi - t0));
-                        continue;
-                    }
-                    int32_t& so = slot_of[(size_t)oi];
-                    if (so < 0 || (so >> 8) != k) {
-                        if (nw == IC_MAX_WATCH)
-                            return fail(HEVCGPU_EINVAL, "CTU %d reads from more than %d intra TUs of other CTUs", a,
-                                        IC_MAX_WATCH);
-                        so = (k << 8) | nw++;
-                        watch.push_back((uint32_t)oi);
-                        itu_rec[(size_t)oi].reserved[0] = ITU_PUBLISH;
-                    }
-                    dep_out.push_back(INTRA_DEP_WATCH | (uint32_t)(so & 0xFF));
-                }
-                if (!(t.flags & HEVC_TU_CODED)) continue;
-                const int nn = 1 << (2 * t.log2_size);
-                itu_res[(size_t)i] = make_int4((int)t.coeff_offset, acc, nn / 8, 0);
-                r.coeff_offset = (uint32_t)acc;
-                acc += nn;
-            }
-            if (acc > IC_MAX_RES)
-                return fail(HEVCGPU_EINVAL, "CTU %d holds more intra TUs than a CTU can", a);
-            ictu_watch[(size_t)k] = (w0 << 8) | (uint32_t)nw;
-        }
-        // one spare entry: an external dependency of task 0 on itself (the planted wait of
-        // hevcgpu_job_plant_unmet_wait points task 0's list at it)
-        j->spare_dep = (uint32_t)dep_out.size();
-        dep_out.push_back(INTRA_DEP_EXTERNAL | 0u);
-        if (dep_out.size() >= (1u << 26)) return fail(HEVCGPU_EINVAL, "intra dependency lists too long");
-    }
+    if ((rc = build_intra_schedule(BS, s, &j->spare_dep))) return rc;
     j->n_ictu = (int32_t)ictu_addr.size();
     // MC strips: 4 columns x up to 16 rows of one PU in one plane, one thread each; luma
     // and chroma (Cb and Cr strips) are two lists, each ordered by class: bi-predicted
@@ -1009,7 +1076,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     Packer write;
     write.out = static_cast<uint8_t*>(j->pin.p);
     pack(write);
-    CUDA_TRY(cudaMemcpyAsync(j->recs.p, j->pin.p, img, cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = up({UploadOp::COPY, j->recs.p, j->pin.p, img}))) return rc;
     j->upload_bytes = big_bytes + img + sizeof(PicDesc);
     uint8_t* big_base = static_cast<uint8_t*>(j->big.p);
     uint8_t* base = static_cast<uint8_t*>(j->recs.p);
@@ -1058,7 +1125,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     D.n_ictu = (int32_t)ictu_addr.size();
     D.n_itu = n_intra;
     // completion flags start below every epoch a launch can use
-    if (done_bytes) CUDA_TRY(cudaMemsetAsync(D.itu_done, 0, done_bytes, ctx->stream));
+    if (done_bytes && (rc = up({UploadOp::ZERO, D.itu_done, nullptr, done_bytes}))) return rc;
     D.num_pus = s->num_pus;
     D.num_slices = std::max(1, (int)s->num_slices);
     D.log2_ctb = p.log2_ctb;
@@ -1090,7 +1157,7 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     }
     // the caller may change its arrays once this returns: the direct uploads must have read
     // them, unless the caller waits for that itself (hevcgpu_job_wait_uploaded)
-    if (any_direct && wait_uploads) CUDA_TRY(cudaEventSynchronize(j->direct_read));
+    if (!defer && any_direct && wait_uploads) CUDA_TRY(cudaEventSynchronize(j->direct_read));
     return HEVCGPU_OK;
 }
 
@@ -1821,7 +1888,9 @@ int hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void**
 }
 
 namespace {
-int job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, hevcgpu_job_t** out, bool wait_uploads) {
+// defer: the job's CUDA calls stay queued in it for job_issue (batched preparation).
+int job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, hevcgpu_job_t** out, bool wait_uploads,
+                bool defer = false) {
     if (!st || !out) return fail(HEVCGPU_EINVAL, "null arguments");
     *out = nullptr;
     int rc = check_ctx(st->ctx);
@@ -1840,7 +1909,7 @@ int job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, hevcgpu_
     if (!j) return fail(HEVCGPU_ENOMEM, "host allocation");
     j->ctx = st->ctx;
     j->st = st;
-    if ((rc = job_build(j, syn, ST_ALL, wait_uploads)) || (rc = j->rec.get(st->ctx, (size_t)j->lay.bytes))) {
+    if ((rc = job_build(j, syn, ST_ALL, wait_uploads, defer)) || (rc = j->rec.get(st->ctx, (size_t)j->lay.bytes))) {
         delete j;
         return rc;
     }
@@ -2084,11 +2153,20 @@ int jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* cons
     {
         std::lock_guard<std::mutex> g(ctx->pool.run_mu);
         ctx->pool.ensure(ctx->device);
+        // the workers build the jobs' host images; their CUDA calls are issued below, from
+        // this thread, picture by picture
         ctx->pool.run(n, [&](int i) {
-            rcs[(size_t)i] = job_prepare(sts[i], syns[i], &out[i], wait_uploads);
+            rcs[(size_t)i] = job_prepare(sts[i], syns[i], &out[i], wait_uploads, true);
             if (rcs[(size_t)i]) msgs[(size_t)i] = g_err;
         });
     }
+    bool built = true;
+    for (int i = 0; i < n; i++) built = built && !rcs[(size_t)i];
+    for (int i = 0; i < n && built; i++)
+        if ((rcs[(size_t)i] = job_issue(out[i]))) {
+            msgs[(size_t)i] = g_err;
+            built = false;
+        }
     for (int i = 0; i < n; i++) {
         if (!rcs[(size_t)i]) continue;
         for (int k = 0; k < n; k++) {
@@ -2097,6 +2175,11 @@ int jobs_prepare(hevcgpu_stream_t* const* sts, const hevc_picture_syntax_t* cons
         }
         return fail(rcs[(size_t)i], "picture %d: %s", i, msgs[(size_t)i].c_str());
     }
+    // the caller may change its arrays once this returns (unless it waits for the uploads
+    // itself, hevcgpu_job_wait_uploaded)
+    if (wait_uploads)
+        for (int i = 0; i < n; i++)
+            if (out[i]->direct_read) CUDA_TRY(cudaEventSynchronize(out[i]->direct_read));
     return HEVCGPU_OK;
 }
 }  // namespace
