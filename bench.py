@@ -728,20 +728,32 @@ def run_dropin(reps=3):
         if lib is not None and not os.path.exists(lib):
             out[name] = {"unavailable": f"{lib} is not built"}
             continue
-        times, ok = [], True
+        times, host, ok = [], [], True
         for _ in range(reps):
             dec = D.Decoder(lib)
             if warm and dec.decode(toy) != 0:
                 raise SystemExit("bench: drop-in warm-up decode failed: " + dec.last_error())
+            w0 = dec.gpu_wait_ns() if warm else 0
             t0 = time.perf_counter()
             rc = dec.decode(data)
             times.append(time.perf_counter() - t0)
+            if warm:   # the decode call's own host time: its waits for the GPU back end taken out
+                host.append(times[-1] - (dec.gpu_wait_ns() - w0) / 1e9)
             if rc != 0:
                 raise SystemExit(f"bench: {name} decode of {DROPIN_STREAM} failed: {dec.last_error()}")
             ok = ok and md5_of(dec.frames()) == want["md5"]
             dec.close()
         t = statistics.median(times)
         out[name] = {"frames_per_s": round(n / t, 2), "ms_per_frame": round(1000 * t / n, 3), "md5_ok": ok}
+        if host:
+            h = statistics.median(host)
+            cores = os.cpu_count() or 1
+            out[name]["host_ms_per_frame"] = round(1000 * h / n, 3)
+            out[name]["host_frames_per_s_per_core"] = round(n / h, 2)
+            out[name]["host_note"] = (
+                "the decode call's time outside its waits for the GPU (hevc_decoder_gpu_wait_ns): NAL and "
+                f"slice parsing, CABAC and the recording of each picture, on one core; {cores} such "
+                f"decoders would parse about {round(cores * n / h)} pictures/s of this stream")
     if "frames_per_s" in out.get("reference", {}):
         out["gpu_over_reference"] = round(out["gpu"]["frames_per_s"] / out["reference"]["frames_per_s"], 2)
     out["note"] = ("the whole decode call, CABAC included: one host thread parses in both (the stream has no "

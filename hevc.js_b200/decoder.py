@@ -86,6 +86,8 @@ def _bind(lib):
         lib.hevc_decoder_set_device.restype = C.c_int
         lib.hevc_decoder_gpu_stats.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         lib.hevc_decoder_gpu_stats.restype = C.c_int
+        lib.hevc_decoder_gpu_wait_ns.argtypes = [vp, C.POINTER(C.c_uint64)]
+        lib.hevc_decoder_gpu_wait_ns.restype = C.c_int
     return lib
 
 
@@ -134,6 +136,12 @@ class Decoder:
         p, n = C.c_uint64(0), C.c_uint64(0)
         self.lib.hevc_decoder_gpu_stats(self.h, C.byref(p), C.byref(n))
         return p.value, n.value
+
+    def gpu_wait_ns(self):
+        """Nanoseconds the decoder's calls have waited for the GPU back end."""
+        ns = C.c_uint64(0)
+        self.lib.hevc_decoder_gpu_wait_ns(self.h, C.byref(ns))
+        return ns.value
 
     def decode(self, data):
         return self.lib.hevc_decoder_decode(self.h, bytes(data), len(data))

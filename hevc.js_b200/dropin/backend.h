@@ -34,5 +34,8 @@ int set_device(Backend* b, int device);
 // Whether the GPU reconstructed this picture (its planes hold the GPU's samples).
 bool reconstructed(Backend* b, const hevc::Picture* pic);
 void stats(Backend* b, uint64_t* pictures, uint64_t* launches);
+// Nanoseconds the decoder's calling threads have spent waiting for the back end: for room
+// in the worker's queue, or for pictures to be written back.
+uint64_t wait_ns(Backend* b);
 
 }  // namespace dropin

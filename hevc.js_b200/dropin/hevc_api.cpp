@@ -166,4 +166,10 @@ int hevc_decoder_gpu_stats(HEVCDecoder* dec, uint64_t* pictures, uint64_t* launc
     return HEVC_OK;
 }
 
+int hevc_decoder_gpu_wait_ns(HEVCDecoder* dec, uint64_t* ns) {
+    if (!dec || !ns) return HEVC_ERROR;
+    *ns = dropin::wait_ns(dec->gpu);
+    return HEVC_OK;
+}
+
 }  // extern "C"

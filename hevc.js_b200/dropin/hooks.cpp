@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -127,6 +128,7 @@ public:
     std::string error;   // first failure; guarded by q_mu
     std::map<const Picture*, std::weak_ptr<Picture>> done;   // written back; guarded by q_mu
     uint64_t pictures = 0;
+    uint64_t wait_ns = 0;   // guarded by q_mu
 
     ~Backend() {
         {
@@ -258,9 +260,17 @@ void stats(Backend* b, uint64_t* pictures, uint64_t* launches) {
 }
 
 int Backend::wait_idle() {
+    const auto t0 = std::chrono::steady_clock::now();
     std::unique_lock<std::mutex> g(q_mu);
     idle_cv.wait(g, [&] { return queue.empty() && !busy; });
+    wait_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
     return error.empty() ? 0 : -1;
+}
+
+uint64_t wait_ns(Backend* b) {
+    if (!b) return 0;
+    std::lock_guard<std::mutex> g(b->q_mu);
+    return b->wait_ns;
 }
 
 void Backend::worker_loop() {
@@ -575,8 +585,10 @@ void Backend::submit(DecodingContext& ctx) {
     // hand the records to the worker and keep parsing; at most two pictures wait
     std::unique_ptr<Work> next;
     {
+        const auto t0 = std::chrono::steady_clock::now();
         std::unique_lock<std::mutex> g(q_mu);
         idle_cv.wait(g, [&] { return queue.size() < 2 || !error.empty(); });
+        wait_ns += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
         if (!error.empty()) {
             g.unlock();
             raise();

@@ -96,6 +96,10 @@ const char* hevc_decoder_last_error(HEVCDecoder* dec);
 int hevc_decoder_set_device(HEVCDecoder* dec, int device);
 /* Pictures reconstructed on the GPU by this decoder, and the kernel launches they took. */
 int hevc_decoder_gpu_stats(HEVCDecoder* dec, uint64_t* pictures, uint64_t* launches);
+/* Nanoseconds the decoder's calls have waited for the GPU back end so far (for room in its
+ * queue of pictures, or for frames to be written back).  The rest of their time is the
+ * host's own: NAL and slice parsing, CABAC and the recording of the picture's syntax. */
+int hevc_decoder_gpu_wait_ns(HEVCDecoder* dec, uint64_t* ns);
 
 #ifdef __cplusplus
 }

@@ -117,7 +117,7 @@ def test_dropin_library_exports_the_reference_api(gpu_lib):
         header = f.read()
     import re
     declared = set(re.findall(r"\b(hevc_decoder_\w+)\s*\(", header))
-    assert len(declared) == 13
+    assert len(declared) == 14
     for name in declared:
         assert f" T {name}\n" in syms, name
     # the reconstruction hooks are this library's own recording definitions: the reference
