@@ -403,6 +403,133 @@ __device__ __forceinline__ bool intra_tu4(const Pic& P, const hevc_tu_t& t, int 
     return true;
 }
 
+// The 8x8 TU: the same prediction as intra_tu with its 33 reference samples in registers,
+// sample k in lane k for k < 32 and the last one (the far end of the top row) held by every
+// lane, moved by shuffles; luma smoothing (:217-257, 8x8 threshold 7) with the lanes'
+// neighbours; two output samples per lane, (x, y) and (x, y + 4) with x = lane & 7 and
+// y = lane >> 3.
+template <typename Pic, typename Wait>
+__device__ __forceinline__ bool intra_tu8(const Pic& P, const hevc_tu_t& t, int lane, const CtuTile& tile,
+                                          uint32_t nb_mask, const int16_t* res, Wait&& wait) {
+    constexpr uint32_t FULL = 0xffffffffu;
+    const int ci = t.c_idx, chroma = ci != 0, sub = chroma ? 2 : 1;
+    const int xc = t.x, yc = t.y;
+    const int log2c = P.log2_ctb - chroma;
+    const int rx = xc >> log2c, ry = yc >> log2c;
+    const int pw = P.width >> chroma, ph = P.height >> chroma;
+    const int ox = rx << P.log2_ctb, oy = ry << P.log2_ctb;
+    const int pitch = chroma ? P.pitch_c : P.pitch_y;
+    uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));
+    const uint32_t cur_z = zorder16((uint32_t)((xc * sub - ox) >> 2), (uint32_t)((yc * sub - oy) >> 2));
+    // 1. reference sample k (0 bottom-left .. 16 corner .. 32 top-right), its availability
+    //    (intra_prediction.cpp:102-133) and where it lies, before the wait
+    auto locate = [&](int k, int& at) -> bool {
+        int px, py;
+        if (k < 16) { px = xc - 1; py = yc + 15 - k; }
+        else if (k == 16) { px = xc - 1; py = yc - 1; }
+        else { px = xc + k - 17; py = yc - 1; }
+        if (px < 0 || py < 0 || px >= pw || py >= ph) return false;
+        const int ncx = px >> log2c, ncy = py >> log2c;
+        const bool outside = ncx != rx || ncy != ry;
+        bool ok;
+        if (outside) {
+            uint32_t bit = 0u;
+            if (ncy == ry) bit = ncx == rx - 1 ? NB_LEFT : 0u;
+            else if (ncy == ry - 1)
+                bit = ncx == rx - 1 ? NB_ABOVE_LEFT : (ncx == rx ? NB_ABOVE : (ncx == rx + 1 ? NB_ABOVE_RIGHT : 0u));
+            ok = (nb_mask & bit) != 0;
+        } else {
+            ok = zorder16((uint32_t)((px * sub - ox) >> 2), (uint32_t)((py * sub - oy) >> 2)) < cur_z;
+        }
+        if (ok) at = outside ? ~(py * pitch + px) : (py - tile.y0) * tile.pitch + (px - tile.x0);
+        return ok;
+    };
+    int at = 0, at32 = 0;
+    const bool ok = locate(lane, at);
+    const bool ok32 = locate(32, at32);   // the same in every lane
+    const uint32_t mask = __ballot_sync(FULL, ok);
+    // substitution (:177-197) as a map from k to the sample it takes: k itself when
+    // available, else the nearest available one below, else the first available one; 32 is
+    // the last entry.  None available: every sample is 128.
+    const bool none = mask == 0u && !ok32;
+    auto sl = [&](int k) -> int {
+        if (k == 32) return ok32 ? 32 : (mask ? 31 - __clz(mask) : 32);
+        if ((mask >> k) & 1u) return k;
+        const uint32_t below = mask & ((1u << k) - 1u);
+        return below ? 31 - __clz(below) : (mask ? __ffs(mask) - 1 : 32);
+    };
+    const int mode = t.intra_mode;
+    const int x = lane & 7, y0 = lane >> 3;
+    const bool smooth = !chroma && !P.intra_smoothing_disabled && mode != 1 && min(abs(mode - 26), abs(mode - 10)) > 7;
+    const int own = sl(lane), own_prev = sl(max(lane - 1, 0)), own_next = sl(lane + 1);
+    const int rv0 = res != nullptr ? res[y0 * 8 + x] : 0, rv1 = res != nullptr ? res[(y0 + 4) * 8 + x] : 0;
+    if (!wait()) return false;
+    // 2. the samples, substituted: lane k holds R[k] (k < 32), every lane R[32]
+    const int raw = ok ? (at < 0 ? (int)__ldcg(plane + ~at) : (int)tile.t[at]) : 0;
+    const int raw32 = ok32 ? (at32 < 0 ? (int)__ldcg(plane + ~at32) : (int)tile.t[at32]) : 0;
+    auto take = [&](int j) { const int v = __shfl_sync(FULL, raw, j & 31); return j == 32 ? raw32 : v; };
+    int r = none ? 128 : take(own);
+    int r32 = none ? 128 : take(sl(32));
+    // 3. smoothing of luma references: [1 2 1] over the linear array, ends kept
+    if (smooth) {
+        const int prev = none ? 128 : take(own_prev), next = none ? 128 : take(own_next);
+        r = lane == 0 ? r : (prev + 2 * r + next + 2) >> 2;
+    }
+    // 4. prediction of (x, y0) and (x, y0 + 4)
+    auto R = [&](int k) { const int v = __shfl_sync(FULL, r, k & 31); return k >= 32 ? r32 : v; };
+    int p[2];
+    if (mode == 0) {   // planar (:263-289)
+        const int tr = R(25), bl = R(7), top = R(17 + x);
+        const int l0 = R(15 - y0), l1 = R(11 - y0);
+        p[0] = ((7 - x) * l0 + (x + 1) * tr + (7 - y0) * top + (y0 + 1) * bl + 8) >> 4;
+        p[1] = ((7 - x) * l1 + (x + 1) * tr + (3 - y0) * top + (y0 + 5) * bl + 8) >> 4;
+    } else if (mode == 1) {   // DC (:295-317): left R[8..15], top R[17..24]
+        const bool in_sum = (lane >= 8 && lane <= 15) || (lane >= 17 && lane <= 24);
+        const int dc = (__reduce_add_sync(FULL, in_sum ? r : 0) + 8) >> 4;
+        const int top = R(17 + x), l0 = R(15 - y0), l1 = R(11 - y0);
+        p[0] = dc;
+        p[1] = dc;
+        if (!chroma) {
+            if (y0 == 0) p[0] = x == 0 ? (top + l0 + 2 * dc + 2) >> 2 : (top + 3 * dc + 2) >> 2;
+            else if (x == 0) p[0] = (l0 + 3 * dc + 2) >> 2;
+            if (x == 0) p[1] = (l1 + 3 * dc + 2) >> 2;
+        }
+    } else {   // angular (:323-422), main reference projected through invAngle (:346-368)
+        const bool vert = mode >= 18;
+        const int ang = c_intra_angle[mode], inv = c_inv_angle[mode];
+        auto src = [&](int q) {
+            int s;
+            if (q >= 0) s = vert ? 16 + q : 16 - q;
+            else {
+                const int si = min(16, ((-q) * inv + 128) >> 8);
+                s = vert ? 16 - si : 16 + si;
+            }
+            return min(32, max(0, s));   // past the end only with weight 0
+        };
+        const int corner = R(16);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int y = y0 + 4 * h;
+            const int along = vert ? y : x, across = vert ? x : y;
+            const int idx = ((along + 1) * ang) >> 5, fr = ((along + 1) * ang) & 31;
+            const int q = across + 1 + idx;
+            // every shuffle by all lanes: left and top are read before the lane-dependent tests
+            const int a = R(src(q)), b = R(src(q + 1)), left = R(15 - y), top = R(17 + x);
+            int v = ((32 - fr) * a + fr * b + 16) >> 5;
+            if (!chroma && mode == 26 && x == 0) v = clip_u8(v + ((left - corner) >> 1));
+            if (!chroma && mode == 10 && y == 0) v = clip_u8(v + ((top - corner) >> 1));
+            p[h] = v;
+        }
+    }
+    if (t.flags & HEVC_TU_PCM) p[0] = p[1] = 0;   // the PCM samples are the levels, with no prediction
+    const uint8_t o0 = (uint8_t)clip_u8(p[0] + rv0), o1 = (uint8_t)clip_u8(p[1] + rv1);
+    tile.t[(yc + y0 - tile.y0) * tile.pitch + (xc + x - tile.x0)] = o0;
+    tile.t[(yc + y0 + 4 - tile.y0) * tile.pitch + (xc + x - tile.x0)] = o1;
+    plane[(int64_t)(yc + y0) * pitch + xc + x] = o0;
+    plane[(int64_t)(yc + y0 + 4) * pitch + xc + x] = o1;
+    return true;
+}
+
 // ---------------------------------------------------------------------------------------
 // CTU tasks.  One CTA per CTU that holds intra TUs.  CTAs take CTUs by ticket in wavefront
 // order per picture (2 * row + column: the diagonal band along which a picture's
@@ -736,8 +863,9 @@ __global__ void __launch_bounds__(IC_THREADS, IC_MIN_BLOCKS) k_intra_ctus(const 
         tile.x0 = rx * ctbc;
         tile.y0 = ry * ctbc;
         const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + tu.coeff_offset : nullptr;
-        const bool done = tu.log2_size == 2 ? intra_tu4(s_ipic, tu, lane, tile, nb, res, wait)
-                                            : intra_tu(s_ipic, tu, lane, ws[warp], tile, nb, res, wait);
+        const bool done = tu.log2_size == 2   ? intra_tu4(s_ipic, tu, lane, tile, nb, res, wait)
+                          : tu.log2_size == 3 ? intra_tu8(s_ipic, tu, lane, tile, nb, res, wait)
+                                              : intra_tu(s_ipic, tu, lane, ws[warp], tile, nb, res, wait);
         if (!done) {
             if (lane == 0) s_abort = 1;
             break;
