@@ -530,6 +530,147 @@ __device__ __forceinline__ bool intra_tu8(const Pic& P, const hevc_tu_t& t, int 
     return true;
 }
 
+// The 16x16 TU: its 65 reference samples in registers for substitution and smoothing,
+// samples k and k + 32 in lane k (k < 32) and the last one (the far end of the top row) in
+// every lane, moved by shuffles; then the final array in the warp's shared memory, from
+// which each lane predicts (x, y) for x = lane & 15 and y = (lane >> 4) + 2i, i < 8, the
+// angular ones straight from the reference array through invAngle (no projected copy).
+template <typename Pic, typename Wait>
+__device__ __forceinline__ bool intra_tu16(const Pic& P, const hevc_tu_t& t, int lane, IntraWarpSmem& W,
+                                           const CtuTile& tile, uint32_t nb_mask, const int16_t* res, Wait&& wait) {
+    constexpr uint32_t FULL = 0xffffffffu;
+    const int ci = t.c_idx, chroma = ci != 0, sub = chroma ? 2 : 1;
+    const int xc = t.x, yc = t.y;
+    const int log2c = P.log2_ctb - chroma;
+    const int rx = xc >> log2c, ry = yc >> log2c;
+    const int pw = P.width >> chroma, ph = P.height >> chroma;
+    const int ox = rx << P.log2_ctb, oy = ry << P.log2_ctb;
+    const int pitch = chroma ? P.pitch_c : P.pitch_y;
+    uint8_t* plane = P.rec + (ci == 0 ? 0 : (ci == 1 ? P.off_cb : P.off_cr));
+    const uint32_t cur_z = zorder16((uint32_t)((xc * sub - ox) >> 2), (uint32_t)((yc * sub - oy) >> 2));
+    // 1. reference sample k (0 bottom-left .. 32 corner .. 64 top-right), its availability
+    //    (intra_prediction.cpp:102-133) and where it lies, before the wait
+    auto locate = [&](int k, int& at) -> bool {
+        int px, py;
+        if (k < 32) { px = xc - 1; py = yc + 31 - k; }
+        else if (k == 32) { px = xc - 1; py = yc - 1; }
+        else { px = xc + k - 33; py = yc - 1; }
+        if (px < 0 || py < 0 || px >= pw || py >= ph) return false;
+        const int ncx = px >> log2c, ncy = py >> log2c;
+        const bool outside = ncx != rx || ncy != ry;
+        bool ok;
+        if (outside) {
+            uint32_t bit = 0u;
+            if (ncy == ry) bit = ncx == rx - 1 ? NB_LEFT : 0u;
+            else if (ncy == ry - 1)
+                bit = ncx == rx - 1 ? NB_ABOVE_LEFT : (ncx == rx ? NB_ABOVE : (ncx == rx + 1 ? NB_ABOVE_RIGHT : 0u));
+            ok = (nb_mask & bit) != 0;
+        } else {
+            ok = zorder16((uint32_t)((px * sub - ox) >> 2), (uint32_t)((py * sub - oy) >> 2)) < cur_z;
+        }
+        if (ok) at = outside ? ~(py * pitch + px) : (py - tile.y0) * tile.pitch + (px - tile.x0);
+        return ok;
+    };
+    int at_a = 0, at_b = 0, at64 = 0;
+    const bool ok_a = locate(lane, at_a), ok_b = locate(lane + 32, at_b);
+    const bool ok64 = locate(64, at64);   // the same in every lane
+    const uint32_t m0 = __ballot_sync(FULL, ok_a), m1 = __ballot_sync(FULL, ok_b);
+    // substitution (:177-197) as a map from k to the sample it takes: k itself when
+    // available, else the nearest available one below, else the first available one.
+    // None available: every sample is 128.
+    const bool none = m0 == 0u && m1 == 0u && !ok64;
+    auto sl = [&](int k) -> int {
+        const bool av = k < 32 ? ((m0 >> k) & 1u) != 0 : (k < 64 ? ((m1 >> (k - 32)) & 1u) != 0 : ok64);
+        if (av) return k;
+        if (k > 32) {
+            const uint32_t b1 = k >= 64 ? m1 : (m1 & ((1u << (k - 32)) - 1u));
+            if (b1) return 63 - __clz(b1);
+        }
+        const uint32_t b0 = k >= 32 ? m0 : (m0 & ((1u << k) - 1u));
+        if (b0) return 31 - __clz(b0);
+        if (m0) return __ffs(m0) - 1;
+        if (m1) return 31 + __ffs(m1);
+        return 64;
+    };
+    const int mode = t.intra_mode;
+    const bool smooth = !chroma && !P.intra_smoothing_disabled && mode != 1 && min(abs(mode - 26), abs(mode - 10)) > 1;
+    const int ja = sl(lane), jb = sl(lane + 32), j64 = sl(64);
+    if (!wait()) return false;
+    // 2. the samples, substituted: lane k holds R[k] and R[k + 32], every lane R[64]
+    auto load = [&](bool ok, int at) { return ok ? (at < 0 ? (int)__ldcg(plane + ~at) : (int)tile.t[at]) : 0; };
+    const int raw_a = load(ok_a, at_a), raw_b = load(ok_b, at_b), raw64 = load(ok64, at64);
+    auto take = [&](int j) {
+        const int va = __shfl_sync(FULL, raw_a, j & 31), vb = __shfl_sync(FULL, raw_b, j & 31);
+        return j < 32 ? va : (j < 64 ? vb : raw64);
+    };
+    int ra = none ? 128 : take(ja), rb = none ? 128 : take(jb);
+    const int r64 = none ? 128 : take(j64);
+    // 3. smoothing of luma references (:217-257, 16x16 threshold 1): [1 2 1] over the linear
+    //    array, ends kept; the neighbours by shuffles of all lanes
+    if (smooth) {
+        const int up_a = __shfl_sync(FULL, ra, (lane + 31) & 31), dn_a = __shfl_sync(FULL, ra, (lane + 1) & 31);
+        const int up_b = __shfl_sync(FULL, rb, (lane + 31) & 31), dn_b = __shfl_sync(FULL, rb, (lane + 1) & 31);
+        const int next_a = lane < 31 ? dn_a : dn_b;            // lane 31: R[32], lane 0's rb
+        const int prev_b = lane > 0 ? up_b : up_a;             // lane 0: R[31], lane 31's ra
+        const int next_b = lane < 31 ? dn_b : r64;
+        const int fa = lane == 0 ? ra : (up_a + 2 * ra + next_a + 2) >> 2;
+        rb = (prev_b + 2 * rb + next_b + 2) >> 2;
+        ra = fa;
+    }
+    W.s[lane] = (int16_t)ra;
+    W.s[32 + lane] = (int16_t)rb;
+    if (lane == 0) W.s[64] = (int16_t)r64;
+    __syncwarp();
+    // 4. prediction, residual, clip, store: (x, y) for y = (lane >> 4) + 2i
+    const int16_t* Rs = W.s;
+    const int x = lane & 15, ys = lane >> 4;
+    const int corner = Rs[32], top_x = Rs[33 + x];
+    int dc = 0;
+    if (mode == 1) {   // DC (:295-317): left R[16..31], top R[33..48]
+        const int part = (lane >= 16 ? ra : 0) + (lane >= 1 && lane <= 16 ? rb : 0);
+        dc = (__reduce_add_sync(FULL, part) + 16) >> 5;
+    }
+    const bool vert = mode >= 18;
+    const int ang = c_intra_angle[mode], inv = c_inv_angle[mode];
+    auto src = [&](int q) {
+        int s;
+        if (q >= 0) s = vert ? 32 + q : 32 - q;
+        else {
+            const int si = min(32, ((-q) * inv + 128) >> 8);
+            s = vert ? 32 - si : 32 + si;
+        }
+        return min(64, max(0, s));   // past the end only with weight 0
+    };
+    const bool pcm = (t.flags & HEVC_TU_PCM) != 0;   // the PCM samples are the levels, with no prediction
+#pragma unroll 2
+    for (int i = 0; i < 8; i++) {
+        const int y = ys + 2 * i;
+        const int left = Rs[31 - y];
+        int p;
+        if (mode == 0) {   // planar (:263-289)
+            p = ((15 - x) * left + (x + 1) * Rs[49] + (15 - y) * top_x + (y + 1) * Rs[15] + 16) >> 5;
+        } else if (mode == 1) {
+            p = dc;
+            if (!chroma) {
+                if (y == 0) p = x == 0 ? (top_x + left + 2 * dc + 2) >> 2 : (top_x + 3 * dc + 2) >> 2;
+                else if (x == 0) p = (left + 3 * dc + 2) >> 2;
+            }
+        } else {   // angular (:323-422)
+            const int along = vert ? y : x, across = vert ? x : y;
+            const int idx = ((along + 1) * ang) >> 5, fr = ((along + 1) * ang) & 31;
+            const int q = across + 1 + idx;
+            p = ((32 - fr) * Rs[src(q)] + fr * Rs[src(q + 1)] + 16) >> 5;
+            if (!chroma && mode == 26 && x == 0) p = clip_u8(p + ((left - corner) >> 1));
+            if (!chroma && mode == 10 && y == 0) p = clip_u8(p + ((top_x - corner) >> 1));
+        }
+        if (pcm) p = 0;
+        const uint8_t o = (uint8_t)clip_u8(p + (res != nullptr ? res[y * 16 + x] : 0));
+        tile.t[(yc + y - tile.y0) * tile.pitch + (xc + x - tile.x0)] = o;
+        plane[(int64_t)(yc + y) * pitch + xc + x] = o;
+    }
+    return true;
+}
+
 // ---------------------------------------------------------------------------------------
 // CTU tasks.  One CTA per CTU that holds intra TUs.  CTAs take CTUs by ticket in wavefront
 // order per picture (2 * row + column: the diagonal band along which a picture's
@@ -865,6 +1006,7 @@ __global__ void __launch_bounds__(IC_THREADS, IC_MIN_BLOCKS) k_intra_ctus(const 
         const int16_t* res = (tu.flags & HEVC_TU_CODED) ? s_res + tu.coeff_offset : nullptr;
         const bool done = tu.log2_size == 2   ? intra_tu4(s_ipic, tu, lane, tile, nb, res, wait)
                           : tu.log2_size == 3 ? intra_tu8(s_ipic, tu, lane, tile, nb, res, wait)
+                          : tu.log2_size == 4 ? intra_tu16(s_ipic, tu, lane, ws[warp], tile, nb, res, wait)
                                               : intra_tu(s_ipic, tu, lane, ws[warp], tile, nb, res, wait);
         if (!done) {
             if (lane == 0) s_abort = 1;
