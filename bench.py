@@ -554,7 +554,7 @@ def run_ours(args, hb, rank, world, local):
     # --warmup 0 --streams 2), scaled by 4 to 8 pictures per launch (each picture is
     # independent work), the GOP's total divided by its 60 batches; taken again whenever the
     # stage's kernels change
-    ncu_dram_gop8 = {"mc": 57523456, "residual": 83246882, "intra": 26904610, "deblock": 78733380, "sao": 25038301}
+    ncu_dram_gop8 = {"mc": 57564587, "residual": 83248384, "intra": 26987537, "deblock": 78734404, "sao": 25038421}
     traffic = (ncu_dram_gop8[dom] if dom in ncu_dram_gop8 and (W, H, G, F) == (W_DEFAULT, H_DEFAULT, 8, 60)
                else None)
 
@@ -612,7 +612,7 @@ def run_ours(args, hb, rank, world, local):
 
     # the median of three timed runs of e2e_k GOPs: the host side shares its cores and
     # memory bandwidth with whatever else runs on the machine
-    e2e_k = max(2, K // 4)
+    e2e_k = max(4, K // 2)
     e2e_run(1)
     e2e_times = []
     for _ in range(3):
