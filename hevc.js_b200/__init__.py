@@ -249,6 +249,7 @@ def gpu_lib():
             "hevcgpu_slot_download": ([P, C.c_int32, u8p], C.c_int),
             "hevcgpu_slot_download_frame": ([P, C.c_int32, C.POINTER(abi.Crop), C.POINTER(C.c_uint16), C.c_int32,
                                              C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), C.c_int32], C.c_int),
+            "hevcgpu_slot_checksum": ([P, C.c_int32, C.POINTER(abi.Crop), C.POINTER(C.c_uint32)], C.c_int),
             "hevcgpu_slot_device_ptr": ([P, C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P),
                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
             "hevcgpu_job_prepare": ([P, C.POINTER(PictureSyntax), C.POINTER(P)], C.c_int),
@@ -435,6 +436,16 @@ class Stream:
         _check(self.lib.hevcgpu_slot_download_frame(self.h, slot, C.byref(c), as_ptr(bufs[0], C.c_uint16), sy,
                                                     as_ptr(bufs[1], C.c_uint16), as_ptr(bufs[2], C.c_uint16), sc))
         return bufs[0][:, :w], bufs[1][:, :w // 2], bufs[2][:, :w // 2]
+
+    def checksum(self, slot, crop=None):
+        """(Y, Cb, Cr) checksums of the slot's frame (hevcgpu_slot_checksum: the H.265
+        picture hash SEI checksum over the conformance window crop = (left, right, top,
+        bottom)), computed on the device."""
+        left, right, top, bottom = crop or (0, 0, 0, 0)
+        c = abi.Crop(left, right, top, bottom)
+        out = (C.c_uint32 * 3)()
+        _check(self.lib.hevcgpu_slot_checksum(self.h, slot, C.byref(c), out))
+        return tuple(out)
 
     def prepare(self, pic):
         return Job(self, pic)

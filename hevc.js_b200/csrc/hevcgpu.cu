@@ -1875,6 +1875,42 @@ int hevcgpu_slot_download_frame(hevcgpu_stream_t* st, int32_t slot, const hevc_c
     return HEVCGPU_OK;
 }
 
+int hevcgpu_slot_checksum(hevcgpu_stream_t* st, int32_t slot, const hevc_crop_t* crop, uint32_t* out) {
+    if (!st || slot < 0 || slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);
+    if (!out) return fail(HEVCGPU_EINVAL, "null out");
+    const Layout& L = st->lay;
+    const hevc_crop_t c = crop ? *crop : hevc_crop_t{0, 0, 0, 0};
+    if (c.left < 0 || c.right < 0 || c.top < 0 || c.bottom < 0 || ((c.left | c.right | c.top | c.bottom) & 1) ||
+        c.left + c.right >= L.W || c.top + c.bottom >= L.H)
+        return fail(HEVCGPU_EINVAL, "conformance window %d,%d,%d,%d (even luma offsets inside %dx%d)", c.left, c.right,
+                    c.top, c.bottom, L.W, L.H);
+    int rc = check_ctx(st->ctx);
+    if (rc) return rc;
+    const int w = L.W - c.left - c.right, h = L.H - c.top - c.bottom;
+    const uint8_t* s = static_cast<const uint8_t*>(st->slots[(size_t)slot].p);
+    ChecksumArgs a{};
+    a.src[0] = s + (int64_t)c.top * L.pitch_y + c.left;
+    a.src[1] = s + L.off_cb + (int64_t)(c.top / 2) * L.pitch_c + c.left / 2;
+    a.src[2] = s + L.off_cr + (int64_t)(c.top / 2) * L.pitch_c + c.left / 2;
+    for (int p = 0; p < 3; p++) {
+        a.pitch[p] = p ? L.pitch_c : L.pitch_y;
+        a.w[p] = p ? w / 2 : w;
+        a.h[p] = p ? h / 2 : h;
+    }
+    DevBuf sums;
+    if ((rc = sums.get(st->ctx, 3 * sizeof(uint32_t)))) return rc;
+    a.out = static_cast<uint32_t*>(sums.p);
+    CUDA_TRY(cudaMemsetAsync(a.out, 0, 3 * sizeof(uint32_t), st->ctx->stream));
+    k_picture_checksum<<<dim3((unsigned)std::min(h, 2 * st->ctx->sm_count), 3), 256, 0, st->ctx->stream>>>(a);
+    st->ctx->launches++;
+    CUDA_TRY(cudaGetLastError());
+    uint32_t host[3];
+    CUDA_TRY(cudaMemcpyAsync(host, a.out, sizeof(host), cudaMemcpyDeviceToHost, st->ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(st->ctx->stream));
+    for (int p = 0; p < 3; p++) out[p] = host[p];
+    return HEVCGPU_OK;
+}
+
 int hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void** cb, void** cr, int32_t* pitch_y,
                             int32_t* pitch_c) {
     if (!st || slot < 0 || slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);

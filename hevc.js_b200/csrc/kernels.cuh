@@ -8,6 +8,7 @@
 //                     (deblocking.cpp:50-614)
 //   k_sao             band/edge offset from the deblocked picture into the DPB slot
 //                     (sao.cpp:20-243)
+//   k_picture_checksum  per-plane checksum of a frame (H.265 picture hash SEI, D.3.19)
 #pragma once
 
 #include "device_common.cuh"
@@ -763,6 +764,30 @@ __global__ void __launch_bounds__(256) k_sao(const __grid_constant__ SegTable st
 // [0, h[p]) of its window; each thread writes 8 samples (one 16-byte store) of a staged
 // row whose pitch is the window width rounded up to 8 samples, so every store is aligned;
 // the bytes are read one by one (the window may start on any even column).
+// The checksum of the H.265 decoded picture hash SEI (Rec. ITU-T H.265 D.3.19) of each
+// plane of a frame, for 8-bit samples: the sum modulo 2^32 of sample ^ xorMask over the
+// plane, xorMask = (x & 0xFF) ^ (y & 0xFF) ^ (x >> 8) ^ (y >> 8).  A sum, so the planes'
+// rows are shared out over the CTAs (grid.y = plane) and the partial sums added atomically
+// (32-bit wrap-around is the modulo).
+struct ChecksumArgs {
+    const uint8_t* src[3];
+    int32_t pitch[3], w[3], h[3];
+    uint32_t* out;   // three words, zero before the launch
+};
+__global__ void __launch_bounds__(256) k_picture_checksum(const __grid_constant__ ChecksumArgs a) {
+    const int p = blockIdx.y;
+    const int w = a.w[p], h = a.h[p];
+    uint32_t sum = 0;
+    for (int y = blockIdx.x; y < h; y += gridDim.x) {
+        const uint8_t* row = a.src[p] + (int64_t)y * a.pitch[p];
+        const uint32_t ym = (uint32_t)(y & 0xFF) ^ (uint32_t)(y >> 8);
+        for (int x = threadIdx.x; x < w; x += blockDim.x)
+            sum += (uint32_t)row[x] ^ ym ^ (uint32_t)(x & 0xFF) ^ (uint32_t)(x >> 8);
+    }
+    sum = __reduce_add_sync(0xffffffffu, sum);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(&a.out[p], sum);
+}
+
 struct WidenArgs {
     const uint8_t* src[3];   // first sample of the window in each plane of the slot
     int32_t src_pitch[3];

@@ -258,6 +258,16 @@ typedef struct hevc_crop {
 int  hevcgpu_slot_download_frame(hevcgpu_stream_t* st, int32_t slot, const hevc_crop_t* crop,
                                  uint16_t* y, int32_t stride_y, uint16_t* cb, uint16_t* cr,
                                  int32_t stride_c);
+/* The checksum of the H.265 decoded picture hash SEI (Rec. ITU-T H.265 D.3.19) of each plane
+ * of the frame hevcgpu_slot_download_frame would hand out (the same conformance window,
+ * with x and y counted from its top-left corner): out[0..2] = Y, Cb, Cr, each the sum
+ * modulo 2^32 of sample ^ ((x & 0xFF) ^ (y & 0xFF) ^ (x >> 8) ^ (y >> 8)).  Computed on the
+ * device; only the three words come back, so a decoder checks a frame against a picture
+ * hash (or a test against its oracle) without copying the frame.  The reference carries
+ * no such call: it checks frames by MD5 of the whole output on the host
+ * (tools/oracle_test.sh). */
+int  hevcgpu_slot_checksum(hevcgpu_stream_t* st, int32_t slot, const hevc_crop_t* crop,
+                           uint32_t* out);
 /* Device address of a slot's Y plane and the row pitches (for zero-copy consumers). */
 int  hevcgpu_slot_device_ptr(hevcgpu_stream_t* st, int32_t slot, void** y, void** cb,
                              void** cr, int32_t* pitch_y, int32_t* pitch_c);

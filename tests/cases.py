@@ -113,3 +113,14 @@ def digest(hb, case, out):
         import hashlib
         return [hashlib.md5(np.ascontiguousarray(out).tobytes()).hexdigest()]
     return list(hb.md5_planes(out, case["w"], case["h"]))
+
+
+def picture_checksum(plane):
+    """The checksum of the H.265 decoded picture hash SEI (Rec. ITU-T H.265 D.3.19) of one
+    8-bit plane: the sum modulo 2^32 of sample ^ ((x & 0xFF) ^ (y & 0xFF) ^ (x >> 8) ^
+    (y >> 8)), x and y counted from the plane's top-left corner."""
+    h, w = plane.shape
+    x = np.arange(w, dtype=np.uint32)
+    y = np.arange(h, dtype=np.uint32)
+    mask = ((x & 0xFF) ^ (x >> 8))[None, :] ^ ((y & 0xFF) ^ (y >> 8))[:, None]
+    return int(((plane.astype(np.uint32) & 0xFF) ^ mask).sum(dtype=np.uint64) & 0xFFFFFFFF)

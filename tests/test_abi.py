@@ -5,6 +5,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -60,6 +61,21 @@ int main(void) {
                      C.sizeof(a.PicParams), C.sizeof(a.PictureSyntax)]
     assert offs == [a.PictureSyntax.tus.offset, a.PictureSyntax.coeffs.offset, a.PictureSyntax.blk.offset,
                     a.PictureSyntax.slices.offset, a.PicParams.ref_slot.offset]
+
+
+def test_picture_checksum_helper_follows_the_sei_definition():
+    """The tests' checksum of a plane (the one hevcgpu_slot_checksum computes on the device)
+    against the definition's loop, sample by sample, on a plane with coordinates past 255."""
+    import cases
+    rng = np.random.default_rng(7)
+    plane = rng.integers(0, 256, size=(261, 300), dtype=np.uint8)
+    want = 0
+    for yy in range(plane.shape[0]):
+        for xx in range(plane.shape[1]):
+            mask = (xx & 0xFF) ^ (yy & 0xFF) ^ (xx >> 8) ^ (yy >> 8)
+            want = (want + ((int(plane[yy, xx]) & 0xFF) ^ mask)) & 0xFFFFFFFF
+    assert cases.picture_checksum(plane) == want
+    assert cases.picture_checksum(np.zeros((2, 2), np.uint8)) == 0 + 1 + 1 + 0
 
 
 def test_abi_version(lib):

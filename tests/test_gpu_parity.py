@@ -296,6 +296,35 @@ def test_frame_output_cropped_16bit(hb, gpu_ctx, port):
     job.free()
 
 
+def test_slot_checksum_on_the_device(hb, gpu_ctx, port):
+    """hevcgpu_slot_checksum gives the H.265 picture hash SEI checksum (D.3.19) of each plane of
+    the frame hevcgpu_slot_download_frame hands out: equal to the checksum of the oracle's
+    picture (no frame copy needed) and of the downloaded frame, with and without a
+    conformance window, at a size with coordinates past 255 (the >> 8 terms of the mask)."""
+    for w, h, seed in ((216, 136, 91), (1920, 1080, 4)):
+        st = gpu_ctx.open_stream(w, h, 3)
+        refs = [hb.content(w, h, seed + 1), hb.content(w, h, seed + 2)]
+        st.upload(0, refs[0])
+        st.upload(1, refs[1])
+        pic = hb.Picture(hb.default_cfg(w, h, seed, **cases.PICTURE))
+        want = hb.split_i420(port.reconstruct_picture(pic, refs), w, h)
+        job = st.prepare(pic)
+        job.launch(2)
+        st.sync()
+        for crop in (None, (2, 6, 4, 8), (0, 14, 6, 0), (8, 0, 0, 2)):
+            l, r, t, b = crop or (0, 0, 0, 0)
+            got = st.checksum(2, crop)
+            exp = tuple(cases.picture_checksum(full[t // sub: (h - b) // sub, l // sub: (w - r) // sub])
+                        for full, sub in zip(want, (1, 2, 2)))
+            assert got == exp, (w, crop)
+            assert got == tuple(cases.picture_checksum(pl) for pl in st.download_frame(2, crop)), (w, crop)
+        for bad in [(1, 0, 0, 0), (0, 0, -2, 0), (w // 2, w // 2, 0, 0)]:
+            with pytest.raises(hb.HevcGpuError) as e:
+                st.checksum(2, bad)
+            assert e.value.code == hb.abi.HEVCGPU_EINVAL
+        job.free()
+
+
 def test_batched_prepare_and_download(hb, gpu_ctx, port):
     """hevcgpu_jobs_prepare + hevcgpu_batch_launch + hevcgpu_slots_download over streams
     of mixed sizes give the oracle's pictures into pageable and pinned host buffers; a
