@@ -778,14 +778,15 @@ struct IntraWait {
     int dfirst, doff, dcount, staged, task, n_watch, n_itu, epoch, lane;
 };
 
-// The wait for a TU's dependencies, between the position work and the loads of intra_tu.
-// Local and watched entries wait on shared-memory barriers; a direct external entry (only a planted test wait has one) polls
-// the published completion.  Every wait reads the global timer and gives up after
-// WAIT_LIMIT_NS (SPIN_LIMIT tries as a backstop), marking the sticky status; a wait also
-// ends when another warp of the CTA gave up (s_abort) or, for external waits, when a wait
-// anywhere did (the status word).  Not inlined: one copy serves every TU size, which keeps
-// the size-specialised TU code small in the instruction cache.
-__device__ __noinline__ bool intra_wait(const IntraWait& w) {
+// The wait for a TU's dependencies, between the position work and the loads of a TU path.
+// Local and watched entries wait on shared-memory barriers; a direct external entry (only a
+// planted test wait has one) polls the published completion.  Every wait reads the global
+// timer and gives up after WAIT_LIMIT_NS (SPIN_LIMIT tries as a backstop), marking the
+// sticky status; a wait also ends when another warp of the CTA gave up (s_abort) or, for
+// external waits, when a wait anywhere did (the status word).  Inlined into the four TU
+// paths: as a call it passed its arguments through the stack and saved and restored
+// registers around every wait, on the critical path of each dependency step.
+__device__ __forceinline__ bool intra_wait(const IntraWait& w) {
     // The entries one after another, every lane on the same one (warp-uniform waits: the
     // warp is suspended as a whole on a barrier).
     bool gave_up = false;
