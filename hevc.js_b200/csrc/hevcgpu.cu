@@ -671,8 +671,11 @@ int build_intra_schedule(BuildScratch& BS, const hevc_picture_syntax_t* s, uint3
     level.resize((size_t)n_intra);
     ctu_of.resize((size_t)n_intra);
     dep_at.resize((size_t)n_intra + 1);
-    deps.clear();
-    deps.reserve((size_t)n_intra * 3);
+    // owners found, written through a raw pointer into a buffer kept 34 entries (the most
+    // one TU can add) ahead of the count
+    size_t n_own = 0;
+    if (deps.size() < (size_t)n_intra * 3 + 64) deps.resize((size_t)n_intra * 3 + 64);
+    int32_t* D = deps.data();
     // owner maps: the decode-order index of the latest intra TU per 4x4 unit (24 bits),
     // in words tagged with this picture's generation (8 bits; a word of another
     // generation: no owner)
@@ -696,7 +699,12 @@ int build_intra_schedule(BuildScratch& BS, const hevc_picture_syntax_t* s, uint3
         const int c = t.c_idx, n = 1 << t.log2_size, sub = c ? 2 : 1;
         const int a = ((t.y * sub) >> p.log2_ctb) * wctb + ((t.x * sub) >> p.log2_ctb);
         ctu_of[(size_t)b] = a;
-        dep_at[(size_t)b] = (int32_t)deps.size();
+        dep_at[(size_t)b] = (int32_t)n_own;
+        if (n_own + 34 > deps.size()) {
+            deps.resize(deps.size() * 2);
+            D = deps.data();
+        }
+        const size_t first_dep = n_own;
         uint32_t* own = owner[c].data();
         const int row = uw[c];
         int dp = 0;
@@ -711,9 +719,9 @@ int build_intra_schedule(BuildScratch& BS, const hevc_picture_syntax_t* s, uint3
             // tile to the left, below-left), and waiting for it could wait for a CTA not
             // yet started: CTAs take CTUs in raster order
             if (oa > a) return;
-            for (size_t q = (size_t)dep_at[(size_t)b]; q < deps.size(); q++)
-                if (deps[q] == ob) return;
-            deps.push_back(ob);
+            for (size_t q = first_dep; q < n_own; q++)
+                if (D[q] == ob) return;
+            D[n_own++] = ob;
             dp = std::max(dp, level[(size_t)ob] + 1);   // local and external dependencies alike
         };
         const int ux = t.x / 4, uy = t.y / 4;
@@ -733,7 +741,8 @@ int build_intra_schedule(BuildScratch& BS, const hevc_picture_syntax_t* s, uint3
             for (int x = ux; x < ux + n / 4; x++) r[x] = mark;
         }
     }
-    dep_at[(size_t)n_intra] = (int32_t)deps.size();
+    dep_at[(size_t)n_intra] = (int32_t)n_own;
+    deps.resize(n_own);
     // Task order: CTUs in wavefront order (key 2 * row + column, then raster), each
     // CTU's TUs by depth (every TU after the TUs it depends on, and about in the order
     // they can run), then decode order.  CTAs take CTUs by ticket in this order, so
@@ -806,7 +815,9 @@ int build_intra_schedule(BuildScratch& BS, const hevc_picture_syntax_t* s, uint3
     itu_res.assign((size_t)n_intra, make_int4(-1, 0, 0, 0));
     itu_rec.resize((size_t)n_intra);
     itu_dep.resize((size_t)n_intra);
-    dep_out.reserve(deps.size() + 1);
+    dep_out.resize(deps.size() + 1);   // one entry per owner found, and the spare entry
+    uint32_t* dout = dep_out.data();
+    uint32_t nd = 0;
     const int nic = (int)ictu_addr.size();
     auto& watch = BS.watch;
     auto& slot_of = BS.slot_of;   // (CTU index << 8) | slot of a watched TU, by task index
@@ -828,11 +839,11 @@ int build_intra_schedule(BuildScratch& BS, const hevc_picture_syntax_t* s, uint3
             r.coeff_offset = 0;
             r.reserved[0] = 0;
             const int d0 = dep_at[(size_t)b], d1 = dep_at[(size_t)b + 1];
-            itu_dep[(size_t)i] = ((uint32_t)dep_out.size() << 6) | (uint32_t)(d1 - d0);
+            itu_dep[(size_t)i] = (nd << 6) | (uint32_t)(d1 - d0);
             for (int q = d0; q < d1; q++) {
                 const int ob = deps[(size_t)q], oi = pos[(size_t)ob];
                 if (ctu_of[(size_t)ob] == a) {
-                    dep_out.push_back((uint32_t)(oi - t0));
+                    dout[nd++] = (uint32_t)(oi - t0);
                     continue;
                 }
                 int32_t& so = slot_of[(size_t)oi];
@@ -844,7 +855,7 @@ int build_intra_schedule(BuildScratch& BS, const hevc_picture_syntax_t* s, uint3
                     watch.push_back((uint32_t)oi);
                     itu_rec[(size_t)oi].reserved[0] = ITU_PUBLISH;
                 }
-                dep_out.push_back(INTRA_DEP_WATCH | (uint32_t)(so & 0xFF));
+                dout[nd++] = INTRA_DEP_WATCH | (uint32_t)(so & 0xFF);
             }
             if (!(t.flags & HEVC_TU_CODED)) continue;
             const int nn = 1 << (2 * t.log2_size);
@@ -858,8 +869,9 @@ int build_intra_schedule(BuildScratch& BS, const hevc_picture_syntax_t* s, uint3
     }
     // one spare entry: an external dependency of task 0 on itself (the planted wait of
     // hevcgpu_job_plant_unmet_wait points task 0's list at it)
-    *spare_dep = (uint32_t)dep_out.size();
-    dep_out.push_back(INTRA_DEP_EXTERNAL | 0u);
+    *spare_dep = nd;
+    dout[nd++] = INTRA_DEP_EXTERNAL | 0u;
+    dep_out.resize(nd);
     if (dep_out.size() >= (1u << 26)) return fail(HEVCGPU_EINVAL, "intra dependency lists too long");
     return HEVCGPU_OK;
 }
