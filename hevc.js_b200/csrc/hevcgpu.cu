@@ -1155,9 +1155,15 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
         for (int a = 1; a < nctb && !multi; a++) multi = s->ctb_slice[a] != s->ctb_slice[0];
     D.slice_check = multi ? 1 : 0;
     bool pcm_bypass = false;
-    if (s->blk)
-        for (size_t i = 0; i < (size_t)gw * gh && !pcm_bypass; i++)
-            pcm_bypass = (s->blk[i] & (HEVC_BLK_PCM | HEVC_BLK_BYPASS)) != 0;
+    if (s->blk) {   // an OR over chunks of the grid (which the compiler vectorises), stopping at the first hit
+        const size_t nu = (size_t)gw * gh;
+        for (size_t i0 = 0; i0 < nu && !pcm_bypass; i0 += 4096) {
+            const size_t i1 = std::min(nu, i0 + 4096);
+            uint32_t any = 0;
+            for (size_t i = i0; i < i1; i++) any |= s->blk[i];
+            pcm_bypass = (any & (HEVC_BLK_PCM | HEVC_BLK_BYPASS)) != 0;
+        }
+    }
     D.pcm_bypass_any = pcm_bypass ? 1 : 0;
     for (int k = 0; k < 4; k++) {
         j->n_res[k] = (int32_t)bins[k].size();
