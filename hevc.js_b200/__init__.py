@@ -250,6 +250,7 @@ def gpu_lib():
             "hevcgpu_slot_download_frame": ([P, C.c_int32, C.POINTER(abi.Crop), C.POINTER(C.c_uint16), C.c_int32,
                                              C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), C.c_int32], C.c_int),
             "hevcgpu_slot_checksum": ([P, C.c_int32, C.POINTER(abi.Crop), C.POINTER(C.c_uint32)], C.c_int),
+            "hevcgpu_intra_schedule": ([P, C.POINTER(abi.IntraSchedule)], C.c_int),
             "hevcgpu_slot_device_ptr": ([P, C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P),
                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
             "hevcgpu_job_prepare": ([P, C.POINTER(PictureSyntax), C.POINTER(P)], C.c_int),
@@ -569,6 +570,21 @@ class Lane:
             self.close()
         except Exception:
             pass
+
+
+def intra_schedule(pic):
+    """The intra schedule the back end builds for a picture (hevcgpu_intra_schedule; host
+    work only): a dict of numpy copies of its arrays."""
+    lib = gpu_lib()
+    out = abi.IntraSchedule()
+    _check(lib.hevcgpu_intra_schedule(C.cast(pic.syn_ptr, C.c_void_p), C.byref(out)))
+
+    def arr(ptr, n, dt):
+        return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt) if n > 0 else np.zeros(0, dt)
+    return {"ctu_addr": arr(out.ctu_addr, out.n_ctu, np.int64), "ctu_first": arr(out.ctu_first, out.n_ctu + 1, np.int64),
+            "task_tu": arr(out.task_tu, out.n_task, np.int64), "task_deps": arr(out.task_deps, out.n_task, np.uint32),
+            "deps": arr(out.deps, out.n_dep, np.uint32), "task_flags": arr(out.task_flags, out.n_task, np.uint8),
+            "ctu_watch": arr(out.ctu_watch, out.n_ctu, np.uint32), "watch": arr(out.watch, out.n_watch, np.int64)}
 
 
 def prepare_batch(streams, pics, wait_uploads=True):

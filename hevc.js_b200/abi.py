@@ -66,6 +66,19 @@ class Crop(C.Structure):
     _fields_ = [("left", C.c_int32), ("right", C.c_int32), ("top", C.c_int32), ("bottom", C.c_int32)]
 
 
+HEVC_INTRA_DEP_WATCH = 0x40000000
+HEVC_INTRA_PUBLISH = 1
+
+
+class IntraSchedule(C.Structure):
+    """hevc_intra_schedule_t: views into the calling thread's arrays (hevcgpu_intra_schedule)."""
+    _fields_ = [("n_ctu", C.c_int32), ("n_task", C.c_int32), ("n_dep", C.c_int32), ("n_watch", C.c_int32),
+                ("ctu_addr", C.POINTER(C.c_int32)), ("ctu_first", C.POINTER(C.c_int32)),
+                ("task_tu", C.POINTER(C.c_int32)), ("task_deps", C.POINTER(C.c_uint32)),
+                ("deps", C.POINTER(C.c_uint32)), ("task_flags", C.POINTER(C.c_uint8)),
+                ("ctu_watch", C.POINTER(C.c_uint32)), ("watch", C.POINTER(C.c_uint32))]
+
+
 class PicParams(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("bit_depth", C.c_int32),
                 ("log2_ctb", C.c_int32), ("log2_min_cb", C.c_int32), ("log2_min_tb", C.c_int32),

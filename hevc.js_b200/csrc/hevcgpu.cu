@@ -601,6 +601,7 @@ struct BuildScratch {
     std::vector<std::pair<int64_t, int32_t>> runs;   // (wavefront key, first TU) of each CTU's run
     std::vector<int32_t> ictu_addr, ictu_tu_off, slot_of;
     std::vector<uint32_t> itu_dep, dep_out, watch, ictu_watch;
+    std::vector<uint8_t> task_flags;   // hevcgpu_intra_schedule's copy of the tasks' flags
     std::vector<uint32_t> mc[2];
     std::vector<uint8_t> mc_cls;
 };
@@ -1979,6 +1980,37 @@ int job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, hevcgpu_
 
 int hevcgpu_job_prepare(hevcgpu_stream_t* st, const hevc_picture_syntax_t* syn, hevcgpu_job_t** out) {
     return job_prepare(st, syn, out, true);
+}
+
+static_assert(HEVC_INTRA_DEP_WATCH == INTRA_DEP_WATCH && HEVC_INTRA_PUBLISH == ITU_PUBLISH,
+              "the schedule the diagnostic hands out is the one the kernel reads");
+
+int hevcgpu_intra_schedule(const hevc_picture_syntax_t* syn, hevc_intra_schedule_t* out) {
+    if (!out) return fail(HEVCGPU_EINVAL, "null out");
+    std::memset(out, 0, sizeof(*out));
+    int rc = validate(syn, true, false, false);
+    if (rc) return rc;
+    BuildScratch& BS = t_build;
+    BS.intra_list.clear();
+    for (int i = 0; i < syn->num_tus; i++)
+        if (syn->tus[i].flags & HEVC_TU_INTRA) BS.intra_list.push_back(i);
+    uint32_t spare = 0;
+    if ((rc = build_intra_schedule(BS, syn, &spare))) return rc;
+    BS.task_flags.resize(BS.itu_rec.size());
+    for (size_t i = 0; i < BS.itu_rec.size(); i++) BS.task_flags[i] = BS.itu_rec[i].reserved[0];
+    out->n_ctu = (int32_t)BS.ictu_addr.size();
+    out->n_task = (int32_t)BS.intra_list.size();
+    out->n_dep = BS.intra_list.empty() ? 0 : (int32_t)spare;   // the entries before the spare one
+    out->n_watch = (int32_t)BS.watch.size();
+    out->ctu_addr = BS.ictu_addr.data();
+    out->ctu_first = BS.ictu_tu_off.data();
+    out->task_tu = BS.itu.data();
+    out->task_deps = BS.itu_dep.data();
+    out->deps = BS.dep_out.data();
+    out->task_flags = BS.task_flags.data();
+    out->ctu_watch = BS.ictu_watch.data();
+    out->watch = BS.watch.data();
+    return HEVCGPU_OK;
 }
 
 int hevcgpu_job_plant_unmet_wait(hevcgpu_job_t* job) {

@@ -371,13 +371,36 @@ int  hevcgpu_jobs_prepare_async(hevcgpu_stream_t* const* sts, const hevc_picture
 /* Returns once the copies of a job's page-locked record arrays have read them. */
 int  hevcgpu_job_wait_uploaded(hevcgpu_job_t* job);
 
-/* Test hook for the device timeout path (no counterpart in the reference): the job's first
- * intra CTU is made to wait, before its first level, for a level of itself that it can
- * never publish.  Its bounded wait gives up after about a second, the kernel returns, and
- * the next sync reports HEVCGPU_ETIMEOUT; the context stays usable.  The injection is a
- * change of the job's uploaded schedule on the host side: nothing faults or traps.
+/* Test hook for the device timeout path (no counterpart in the reference): the first task
+ * of the job's intra schedule is made to wait for its own completion, which it can never
+ * publish.  Its bounded wait gives up after about a second, the kernel returns, and the
+ * next sync reports HEVCGPU_ETIMEOUT; the context stays usable.  The injection is a change
+ * of the job's uploaded schedule on the host side: nothing faults or traps.
  * HEVCGPU_EINVAL for a job without intra TUs. */
 int  hevcgpu_job_plant_unmet_wait(hevcgpu_job_t* job);
+
+/* The intra schedule the back end builds for a picture (no counterpart in the reference;
+ * host work only, no device is needed), for tools and tests: the CTUs that hold intra TUs
+ * in the order CTAs take them (wavefront order, key 2 * row + column), each CTU's tasks
+ * (its intra TUs, every one after the TUs it depends on), each task's dependency list and
+ * each CTU's watch list (the TUs of earlier CTUs it waits for).  A dependency entry is the
+ * index of a task of the same CTU counted from the CTU's first, or
+ * HEVC_INTRA_DEP_WATCH | the slot of the CTU's watch list.  The arrays belong to the
+ * calling thread and stay valid until its next call. */
+#define HEVC_INTRA_DEP_WATCH 0x40000000u
+#define HEVC_INTRA_PUBLISH 1u          /* task_flags: a TU of another CTU depends on it */
+typedef struct hevc_intra_schedule {
+    int32_t n_ctu, n_task, n_dep, n_watch;
+    const int32_t*  ctu_addr;      /* n_ctu: raster address of each CTU, in task order     */
+    const int32_t*  ctu_first;     /* n_ctu + 1: first task of each CTU                    */
+    const int32_t*  task_tu;       /* n_task: the task's TU (index into syn->tus)          */
+    const uint32_t* task_deps;     /* n_task: (offset into deps << 6) | number of entries  */
+    const uint32_t* deps;          /* n_dep dependency entries                             */
+    const uint8_t*  task_flags;    /* n_task: HEVC_INTRA_PUBLISH                           */
+    const uint32_t* ctu_watch;     /* n_ctu: (offset into watch << 8) | number of slots    */
+    const uint32_t* watch;         /* n_watch: the watched TUs, as task indices            */
+} hevc_intra_schedule_t;
+int  hevcgpu_intra_schedule(const hevc_picture_syntax_t* syn, hevc_intra_schedule_t* out);
 int  hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n,
                             uint8_t* const* outs);
 /* CUDA stream (cudaStream_t) the context launches on. */

@@ -43,8 +43,9 @@ def test_record_layouts_match_header(hb, tmp_path):
 #include <stddef.h>
 #include "hevcgpu.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(hevc_tu_t), sizeof(hevc_pu_t), sizeof(hevc_wp_t),
-         sizeof(hevc_sao_t), sizeof(hevc_slice_t), sizeof(hevc_pic_params_t), sizeof(hevc_picture_syntax_t));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(hevc_tu_t), sizeof(hevc_pu_t), sizeof(hevc_wp_t),
+         sizeof(hevc_sao_t), sizeof(hevc_slice_t), sizeof(hevc_pic_params_t), sizeof(hevc_picture_syntax_t),
+         sizeof(hevc_intra_schedule_t));
   printf("%zu %zu %zu %zu %zu\\n", offsetof(hevc_picture_syntax_t, tus), offsetof(hevc_picture_syntax_t, coeffs),
          offsetof(hevc_picture_syntax_t, blk), offsetof(hevc_picture_syntax_t, slices),
          offsetof(hevc_pic_params_t, ref_slot));
@@ -58,7 +59,7 @@ int main(void) {
     offs = [int(x) for x in out[1].split()]
     a = hb.abi
     assert sizes == [C.sizeof(a.TU), C.sizeof(a.PU), C.sizeof(a.WP), C.sizeof(a.SAO), C.sizeof(a.Slice),
-                     C.sizeof(a.PicParams), C.sizeof(a.PictureSyntax)]
+                     C.sizeof(a.PicParams), C.sizeof(a.PictureSyntax), C.sizeof(a.IntraSchedule)]
     assert offs == [a.PictureSyntax.tus.offset, a.PictureSyntax.coeffs.offset, a.PictureSyntax.blk.offset,
                     a.PictureSyntax.slices.offset, a.PicParams.ref_slot.offset]
 
