@@ -121,12 +121,11 @@ enum : uint32_t {
     ST_TIMEOUT = 2u,      // a bounded wait gave up; the kernel returned early
 };
 
-// Shared state of one intra dataflow launch (see intra.cuh).
+// Header of a flow area (the intra launches' state of a context or lane): 16 bytes kept
+// free; the sticky status word (ST_* bits) follows it, then one CTU ticket counter per
+// picture of a launch.
 struct FlowState {
-    int32_t head;         // next queue slot to claim
-    int32_t tail;         // next queue slot to publish
-    uint32_t status;      // ST_* bits
-    int32_t pad;
+    int32_t reserved[4];
 };
 
 __device__ __forceinline__ int clip3(int lo, int hi, int v) { return v < lo ? lo : (v > hi ? hi : v); }
