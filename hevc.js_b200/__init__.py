@@ -251,6 +251,8 @@ def gpu_lib():
                                              C.POINTER(C.c_uint16), C.POINTER(C.c_uint16), C.c_int32], C.c_int),
             "hevcgpu_slot_checksum": ([P, C.c_int32, C.POINTER(abi.Crop), C.POINTER(C.c_uint32)], C.c_int),
             "hevcgpu_intra_schedule": ([P, C.POINTER(abi.IntraSchedule)], C.c_int),
+            "hevcgpu_mc_strips": ([P, C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_int32),
+                                   C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_int32)], C.c_int),
             "hevcgpu_slot_device_ptr": ([P, C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P),
                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
             "hevcgpu_job_prepare": ([P, C.POINTER(PictureSyntax), C.POINTER(P)], C.c_int),
@@ -585,6 +587,19 @@ def intra_schedule(pic):
             "task_tu": arr(out.task_tu, out.n_task, np.int64), "task_deps": arr(out.task_deps, out.n_task, np.uint32),
             "deps": arr(out.deps, out.n_dep, np.uint32), "task_flags": arr(out.task_flags, out.n_task, np.uint8),
             "ctu_watch": arr(out.ctu_watch, out.n_ctu, np.uint32), "watch": arr(out.watch, out.n_watch, np.int64)}
+
+
+def mc_strips(pic):
+    """The MC strip lists the back end builds for a picture (hevcgpu_mc_strips; host work
+    only): (luma items, chroma items) as numpy copies."""
+    lib = gpu_lib()
+    lp, cp = C.POINTER(C.c_uint32)(), C.POINTER(C.c_uint32)()
+    nl, nc = C.c_int32(0), C.c_int32(0)
+    _check(lib.hevcgpu_mc_strips(C.cast(pic.syn_ptr, C.c_void_p), C.byref(lp), C.byref(nl), C.byref(cp), C.byref(nc)))
+
+    def arr(ptr, n):
+        return np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n > 0 else np.zeros(0, np.uint32)
+    return arr(lp, nl.value), arr(cp, nc.value)
 
 
 def prepare_batch(streams, pics, wait_uploads=True):

@@ -607,6 +607,76 @@ struct BuildScratch {
 };
 thread_local BuildScratch t_build;
 
+// MC strips: 4 columns x up to 16 rows of one PU in one plane, one thread each; luma
+// and chroma (Cb and Cr strips) are two lists, each ordered by class: bi-predicted
+// first, then windows inside the picture first, then taller first, so that the
+// threads of a warp share their path and row count; PU order inside a class.  One pass
+// finds each PU's class word in both planes and counts its strips per class by row
+// band; a second pass writes the items of each row band.
+void build_mc_strips(BuildScratch& BS, const hevc_picture_syntax_t* s, int pitch_y, int pitch_c) {
+    const int W = s->params.width, H = s->params.height;
+    auto& mc = BS.mc;
+    mc[0].clear();
+    mc[1].clear();
+    const int n_pu = s->num_pus;
+    int32_t cnt[2][33] = {};
+    auto& cls = BS.mc_cls;   // per PU and plane: (bi ? 0 : 2) + (inside ? 0 : 1)
+    cls.resize((size_t)n_pu * 2);
+    for (int i = 0; i < n_pu; i++) {
+        const hevc_pu_t& u = s->pus[i];
+        const bool bi = u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0;
+        const int wl = u.w, hl = u.h, wc = u.w / 2, hc = u.h / 2;
+        // list windows at the PU's top-left, extended over the PU: its strips are
+        // inside when every list's window of the whole PU is
+        bool in_l = true, in_c = true;
+        for (int l = 0; l < 2; l++) {
+            if (u.ref_idx[l] < 0) continue;
+            const int mvx = u.mv[l][0], mvy = u.mv[l][1];
+            const int x0 = u.x + (mvx >> 2) - 3, y0 = u.y + (mvy >> 2) - 3;
+            in_l = in_l && mc_inside<false>(x0, y0, hl, W, H, pitch_y) &&
+                   mc_inside<false>(x0 + ((wl - 1) & ~3), y0, hl, W, H, pitch_y);
+            const int cx0 = u.x / 2 + (mvx >> 3) - 1, cy0 = u.y / 2 + (mvy >> 3) - 1;
+            in_c = in_c && mc_inside<true>(cx0, cy0, hc, W / 2, H / 2, pitch_c) &&
+                   mc_inside<true>(cx0 + ((wc - 1) & ~3), cy0, hc, W / 2, H / 2, pitch_c);
+        }
+        const int kl = (bi ? 0 : 2) + (in_l ? 0 : 1), kc = (bi ? 0 : 2) + (in_c ? 0 : 1);
+        cls[2 * (size_t)i] = (uint8_t)kl;
+        cls[2 * (size_t)i + 1] = (uint8_t)kc;
+        // class = kind * (row classes) + (row classes) - rows / (rows per class)
+        const int nl = wl / 4, nc = 2 * ((wc + 3) / 4);
+        for (int sy = 0; sy < hl; sy += MC_STRIP_ROWS)
+            cnt[0][kl * 4 + 4 - std::min(MC_STRIP_ROWS, hl - sy) / 4 + 1] += nl;
+        for (int sy = 0; sy < hc; sy += MC_STRIP_ROWS)
+            cnt[1][kc * 8 + 8 - std::min(MC_STRIP_ROWS, hc - sy) / 2 + 1] += nc;
+    }
+    for (int c = 0; c < 2; c++) {
+        const int ncls = c ? 32 : 16;
+        for (int k = 1; k <= ncls; k++) cnt[c][k] += cnt[c][k - 1];
+        mc[c].resize((size_t)cnt[c][ncls]);
+    }
+    uint32_t* out_l = mc[0].data();
+    uint32_t* out_c = mc[1].data();
+    for (int i = 0; i < n_pu; i++) {
+        const hevc_pu_t& u = s->pus[i];
+        const int kl = cls[2 * (size_t)i], kc = cls[2 * (size_t)i + 1];
+        for (int sy = 0; sy < u.h; sy += MC_STRIP_ROWS) {
+            const int rows = std::min(MC_STRIP_ROWS, u.h - sy);
+            int32_t& pos = cnt[0][kl * 4 + 4 - rows / 4];
+            uint32_t item = mc_item(i, 0, sy, rows, false, 0);
+            for (int sx = 0; sx < u.w; sx += 4, item += 1u << 20) out_l[pos++] = item;
+        }
+        const int wc = u.w / 2, hc = u.h / 2;
+        for (int sy = 0; sy < hc; sy += MC_STRIP_ROWS) {
+            const int rows = std::min(MC_STRIP_ROWS, hc - sy);
+            int32_t& pos = cnt[1][kc * 8 + 8 - rows / 2];
+            for (int pl = 0; pl < 2; pl++) {
+                uint32_t item = mc_item(i, 0, sy, rows, true, pl);
+                for (int sx = 0; sx < wc; sx += 4, item += 1u << 20) out_c[pos++] = item;
+            }
+        }
+    }
+}
+
 // Issue one queued CUDA call of a job's preparation on the context stream.
 int run_upload(hevcgpu_job* j, const UploadOp& o) {
     cudaStream_t cs = j->ctx->stream;
@@ -987,73 +1057,12 @@ int job_build(hevcgpu_job* j, const hevc_picture_syntax_t* s, int stages, bool w
     auto& ictu_watch = BS.ictu_watch;   // per CTU: (offset in watch << 8) | count
     if ((rc = build_intra_schedule(BS, s, &j->spare_dep))) return rc;
     j->n_ictu = (int32_t)ictu_addr.size();
-    // MC strips: 4 columns x up to 16 rows of one PU in one plane, one thread each; luma
-    // and chroma (Cb and Cr strips) are two lists, each ordered by class: bi-predicted
-    // first, then windows inside the picture first, then taller first, so that the
-    // threads of a warp share their path and row count; PU order inside a class.  One pass
-    // finds each PU's class word in both planes and counts its strips per class by row
-    // band; a second pass writes the items of each row band.
+    // MC strips (build_mc_strips)
     auto& mc = BS.mc;
-    mc[0].clear();
-    mc[1].clear();
-    if (stages & ST_MC) {
-        const int n_pu = s->num_pus, pitch_y = j->lay.pitch_y, pitch_c = j->lay.pitch_c;
-        int32_t cnt[2][33] = {};
-        auto& cls = BS.mc_cls;   // per PU and plane: (bi ? 0 : 2) + (inside ? 0 : 1)
-        cls.resize((size_t)n_pu * 2);
-        for (int i = 0; i < n_pu; i++) {
-            const hevc_pu_t& u = s->pus[i];
-            const bool bi = u.ref_idx[0] >= 0 && u.ref_idx[1] >= 0;
-            const int wl = u.w, hl = u.h, wc = u.w / 2, hc = u.h / 2;
-            // list windows at the PU's top-left, extended over the PU: its strips are
-            // inside when every list's window of the whole PU is
-            bool in_l = true, in_c = true;
-            for (int l = 0; l < 2; l++) {
-                if (u.ref_idx[l] < 0) continue;
-                const int mvx = u.mv[l][0], mvy = u.mv[l][1];
-                const int x0 = u.x + (mvx >> 2) - 3, y0 = u.y + (mvy >> 2) - 3;
-                in_l = in_l && mc_inside<false>(x0, y0, hl, W, H, pitch_y) &&
-                       mc_inside<false>(x0 + ((wl - 1) & ~3), y0, hl, W, H, pitch_y);
-                const int cx0 = u.x / 2 + (mvx >> 3) - 1, cy0 = u.y / 2 + (mvy >> 3) - 1;
-                in_c = in_c && mc_inside<true>(cx0, cy0, hc, W / 2, H / 2, pitch_c) &&
-                       mc_inside<true>(cx0 + ((wc - 1) & ~3), cy0, hc, W / 2, H / 2, pitch_c);
-            }
-            const int kl = (bi ? 0 : 2) + (in_l ? 0 : 1), kc = (bi ? 0 : 2) + (in_c ? 0 : 1);
-            cls[2 * (size_t)i] = (uint8_t)kl;
-            cls[2 * (size_t)i + 1] = (uint8_t)kc;
-            // class = kind * (row classes) + (row classes) - rows / (rows per class)
-            const int nl = wl / 4, nc = 2 * ((wc + 3) / 4);
-            for (int sy = 0; sy < hl; sy += MC_STRIP_ROWS)
-                cnt[0][kl * 4 + 4 - std::min(MC_STRIP_ROWS, hl - sy) / 4 + 1] += nl;
-            for (int sy = 0; sy < hc; sy += MC_STRIP_ROWS)
-                cnt[1][kc * 8 + 8 - std::min(MC_STRIP_ROWS, hc - sy) / 2 + 1] += nc;
-        }
-        for (int c = 0; c < 2; c++) {
-            const int ncls = c ? 32 : 16;
-            for (int k = 1; k <= ncls; k++) cnt[c][k] += cnt[c][k - 1];
-            mc[c].resize((size_t)cnt[c][ncls]);
-        }
-        uint32_t* out_l = mc[0].data();
-        uint32_t* out_c = mc[1].data();
-        for (int i = 0; i < n_pu; i++) {
-            const hevc_pu_t& u = s->pus[i];
-            const int kl = cls[2 * (size_t)i], kc = cls[2 * (size_t)i + 1];
-            for (int sy = 0; sy < u.h; sy += MC_STRIP_ROWS) {
-                const int rows = std::min(MC_STRIP_ROWS, u.h - sy);
-                int32_t& pos = cnt[0][kl * 4 + 4 - rows / 4];
-                uint32_t item = mc_item(i, 0, sy, rows, false, 0);
-                for (int sx = 0; sx < u.w; sx += 4, item += 1u << 20) out_l[pos++] = item;
-            }
-            const int wc = u.w / 2, hc = u.h / 2;
-            for (int sy = 0; sy < hc; sy += MC_STRIP_ROWS) {
-                const int rows = std::min(MC_STRIP_ROWS, hc - sy);
-                int32_t& pos = cnt[1][kc * 8 + 8 - rows / 2];
-                for (int pl = 0; pl < 2; pl++) {
-                    uint32_t item = mc_item(i, 0, sy, rows, true, pl);
-                    for (int sx = 0; sx < wc; sx += 4, item += 1u << 20) out_c[pos++] = item;
-                }
-            }
-        }
+    if (stages & ST_MC) build_mc_strips(BS, s, j->lay.pitch_y, j->lay.pitch_c);
+    else {
+        mc[0].clear();
+        mc[1].clear();
     }
     j->n_pus = s->num_pus;
 
@@ -2010,6 +2019,24 @@ int hevcgpu_intra_schedule(const hevc_picture_syntax_t* syn, hevc_intra_schedule
     out->task_flags = BS.task_flags.data();
     out->ctu_watch = BS.ictu_watch.data();
     out->watch = BS.watch.data();
+    return HEVCGPU_OK;
+}
+
+int hevcgpu_mc_strips(const hevc_picture_syntax_t* syn, const uint32_t** luma, int32_t* n_luma,
+                      const uint32_t** chroma, int32_t* n_chroma) {
+    if (!luma || !n_luma || !chroma || !n_chroma) return fail(HEVCGPU_EINVAL, "null out");
+    *luma = *chroma = nullptr;
+    *n_luma = *n_chroma = 0;
+    int rc = validate(syn, false, true, false);
+    if (rc) return rc;
+    Layout lay;
+    lay.init(syn->params.width, syn->params.height);
+    BuildScratch& BS = t_build;
+    build_mc_strips(BS, syn, lay.pitch_y, lay.pitch_c);
+    *luma = BS.mc[0].data();
+    *n_luma = (int32_t)BS.mc[0].size();
+    *chroma = BS.mc[1].data();
+    *n_chroma = (int32_t)BS.mc[1].size();
     return HEVCGPU_OK;
 }
 

@@ -401,6 +401,17 @@ typedef struct hevc_intra_schedule {
     const uint32_t* watch;         /* n_watch: the watched TUs, as task indices            */
 } hevc_intra_schedule_t;
 int  hevcgpu_intra_schedule(const hevc_picture_syntax_t* syn, hevc_intra_schedule_t* out);
+
+/* The motion-compensation work lists the back end builds for a picture (no counterpart in
+ * the reference; host work only), for tools and tests: one item per strip of 4 columns and
+ * up to 16 rows of one PU in one plane, luma and chroma lists.  Item bits: 0-19 the PU,
+ * 20-23 the strip's column / 4, 24-25 its first row / 16, 26-28 its rows / 4 - 1 (luma) or
+ * rows / 2 - 1 (chroma), 29 the chroma plane (0 Cb, 1 Cr).  Each list is ordered by class:
+ * bi-predicted strips first, then strips whose reference windows lie inside the picture,
+ * then taller strips first.  The arrays belong to the calling thread and stay valid until
+ * its next call. */
+int  hevcgpu_mc_strips(const hevc_picture_syntax_t* syn, const uint32_t** luma, int32_t* n_luma,
+                       const uint32_t** chroma, int32_t* n_chroma);
 int  hevcgpu_slots_download(hevcgpu_stream_t* const* sts, const int32_t* slots, int32_t n,
                             uint8_t* const* outs);
 /* CUDA stream (cudaStream_t) the context launches on. */
