@@ -1,0 +1,71 @@
+"""ctypes binding of the random-syntax bitstream generator (csrc/bitgen.h).
+
+``generate(width, height, seed, **cfg)`` returns the Annex-B byte stream of IDR pictures and,
+per picture, the intra TU records the generator drew (``hevc_tu_t`` list and the level pool),
+which is what a recorder inside the reference decoder sees when it parses the stream."""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+BITGEN_SO = os.path.join(PKG, "libhevcbitgen.so")
+
+
+class GenCfg(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("seed", C.c_uint64), ("pictures", C.c_int32),
+                ("log2_ctb", C.c_int32), ("p_split", C.c_double), ("p_nxn", C.c_double), ("p_tu_split", C.c_double),
+                ("p_cbf", C.c_double), ("p_sig", C.c_double), ("max_level", C.c_int32), ("qp_min", C.c_int32),
+                ("qp_max", C.c_int32), ("sao", C.c_int32)]
+
+
+class GenStream(C.Structure):
+    _fields_ = [("bytes", C.POINTER(C.c_uint8)), ("size", C.c_size_t), ("pictures", C.c_int32),
+                ("num_tus", C.POINTER(C.c_int32)), ("tus", C.POINTER(C.POINTER(abi.TU))),
+                ("num_coeffs", C.POINTER(C.c_uint64)), ("coeffs", C.POINTER(C.POINTER(C.c_int16)))]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(BITGEN_SO):
+            raise RuntimeError(f"{BITGEN_SO} is not built (run __graft_entry__.build())")
+        _lib = C.CDLL(BITGEN_SO)
+        _lib.hevcgen_default_cfg.argtypes = [C.POINTER(GenCfg), C.c_int32, C.c_int32, C.c_uint64]
+        _lib.hevcgen_default_cfg.restype = None
+        _lib.hevcgen_stream.argtypes = [C.POINTER(GenCfg)]
+        _lib.hevcgen_stream.restype = C.POINTER(GenStream)
+        _lib.hevcgen_stream_free.argtypes = [C.POINTER(GenStream)]
+        _lib.hevcgen_stream_free.restype = None
+    return _lib
+
+
+def generate(width, height, seed, **cfg):
+    """(stream bytes, [(list of abi.TU, int16 level pool) per picture])."""
+    g = lib()
+    c = GenCfg()
+    g.hevcgen_default_cfg(C.byref(c), width, height, seed)
+    for k, v in cfg.items():
+        if not hasattr(c, k):
+            raise KeyError(k)
+        setattr(c, k, v)
+    sp = g.hevcgen_stream(C.byref(c))
+    if not sp:
+        raise ValueError("hevcgen_stream: bad configuration")
+    try:
+        s = sp.contents
+        data = C.string_at(s.bytes, s.size)
+        pics = []
+        for k in range(s.pictures):
+            tus = [abi.TU.from_buffer_copy(s.tus[k][i]) for i in range(s.num_tus[k])]
+            n = int(s.num_coeffs[k])
+            levels = np.ctypeslib.as_array(s.coeffs[k], shape=(n,)).copy() if n else np.zeros(0, np.int16)
+            pics.append((tus, levels))
+        return data, pics
+    finally:
+        g.hevcgen_stream_free(sp)

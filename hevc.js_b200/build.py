@@ -21,6 +21,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 SYNTH_SO = os.path.join(PKG, "libhevcsynth.so")
+BITGEN_SO = os.path.join(PKG, "libhevcbitgen.so")
 GPU_SO = os.path.join(PKG, "libhevcgpu.so")
 DROPIN_SO = os.path.join(PKG, "libhevcdec_gpu.so")
 DROPIN_CLI = os.path.join(PKG, "dropin", "_build", "hevc-decode")
@@ -82,8 +83,19 @@ def build_dropin(force=False):
     return DROPIN_SO
 
 
+def build_bitgen(force=False):
+    """The random-syntax bitstream generator (host code, csrc/bitgen.cpp)."""
+    src = os.path.join(CSRC, "bitgen.cpp")
+    deps = [src, os.path.join(CSRC, "bitgen.h"), os.path.join(ROOT, "include", "hevcgpu.h")]
+    if force or _newer(BITGEN_SO, deps):
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-I", os.path.join(ROOT, "include"),
+              "-o", BITGEN_SO, src])
+    return BITGEN_SO
+
+
 def build_all(force=False):
     build_synth(force)
+    build_bitgen(force)
     build_gpu(force)
     build_dropin(force)
 
