@@ -1,8 +1,13 @@
 """ctypes binding of the random-syntax bitstream generator (csrc/bitgen.h).
 
-``generate(width, height, seed, **cfg)`` returns the Annex-B byte stream of IDR pictures and,
-per picture, the intra TU records the generator drew (``hevc_tu_t`` list and the level pool),
-which is what a recorder inside the reference decoder sees when it parses the stream."""
+``generate(width, height, seed, **cfg)`` returns the Annex-B byte stream (an IDR picture,
+then IDR pictures or, with ``inter=1``, low-delay P and B pictures) and, per picture, the
+records the generator drew: the TUs (``hevc_tu_t``: every TU of an intra CU, the coded ones
+of an inter CU) with their level pool, and the PUs (``hevc_pu_t``: position and size; an
+AMVP-coded PU's ref_idx and coded mvd; -2 in ref_idx for a merged or skipped PU).  That is
+what a recorder inside the reference decoder sees when it parses the stream, up to the
+motion the decoder derives."""
+import collections
 import ctypes as C
 import os
 
@@ -18,13 +23,23 @@ class GenCfg(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("seed", C.c_uint64), ("pictures", C.c_int32),
                 ("log2_ctb", C.c_int32), ("p_split", C.c_double), ("p_nxn", C.c_double), ("p_tu_split", C.c_double),
                 ("p_cbf", C.c_double), ("p_sig", C.c_double), ("max_level", C.c_int32), ("qp_min", C.c_int32),
-                ("qp_max", C.c_int32), ("sao", C.c_int32)]
+                ("qp_max", C.c_int32), ("sao", C.c_int32), ("inter", C.c_int32), ("p_b", C.c_double),
+                ("max_refs", C.c_int32), ("p_intra_cu", C.c_double), ("p_skip", C.c_double),
+                ("p_merge", C.c_double), ("max_mvd", C.c_int32), ("amp", C.c_int32), ("tmvp", C.c_int32),
+                ("max_merge", C.c_int32), ("wp", C.c_int32), ("depth_inter", C.c_int32)]
 
 
 class GenStream(C.Structure):
     _fields_ = [("bytes", C.POINTER(C.c_uint8)), ("size", C.c_size_t), ("pictures", C.c_int32),
                 ("num_tus", C.POINTER(C.c_int32)), ("tus", C.POINTER(C.POINTER(abi.TU))),
-                ("num_coeffs", C.POINTER(C.c_uint64)), ("coeffs", C.POINTER(C.POINTER(C.c_int16)))]
+                ("num_coeffs", C.POINTER(C.c_uint64)), ("coeffs", C.POINTER(C.POINTER(C.c_int16))),
+                ("slice_type", C.POINTER(C.c_int32)), ("num_pus", C.POINTER(C.c_int32)),
+                ("pus", C.POINTER(C.POINTER(abi.PU)))]
+
+# slice_type values (7.4.7.1)
+SLICE_B, SLICE_P, SLICE_I = 0, 1, 2
+
+GenPicture = collections.namedtuple("GenPicture", "tus levels pus slice_type")
 
 
 _lib = None
@@ -46,7 +61,7 @@ def lib():
 
 
 def generate(width, height, seed, **cfg):
-    """(stream bytes, [(list of abi.TU, int16 level pool) per picture])."""
+    """(stream bytes, [GenPicture per picture])."""
     g = lib()
     c = GenCfg()
     g.hevcgen_default_cfg(C.byref(c), width, height, seed)
@@ -65,7 +80,8 @@ def generate(width, height, seed, **cfg):
             tus = [abi.TU.from_buffer_copy(s.tus[k][i]) for i in range(s.num_tus[k])]
             n = int(s.num_coeffs[k])
             levels = np.ctypeslib.as_array(s.coeffs[k], shape=(n,)).copy() if n else np.zeros(0, np.int16)
-            pics.append((tus, levels))
+            pus = [abi.PU.from_buffer_copy(s.pus[k][i]) for i in range(s.num_pus[k])]
+            pics.append(GenPicture(tus, levels, pus, int(s.slice_type[k])))
         return data, pics
     finally:
         g.hevcgen_stream_free(sp)

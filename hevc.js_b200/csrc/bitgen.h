@@ -1,10 +1,14 @@
 /* bitgen.h — seeded generator of random-syntax HEVC Main-profile bitstreams.
  *
  * It draws a legal coding tree per CTU (CU splits, intra 2Nx2N / NxN partitions, intra
- * prediction modes, transform trees, coded blocks and their levels, SAO parameters, slice
+ * prediction modes, skipped and inter CUs with their partitions (AMP included), merge
+ * indices, inter prediction directions, reference indices, motion vector differences and
+ * predictor flags, transform trees, coded blocks and their levels, SAO parameters, slice
  * QPs) and CABAC-encodes it (Rec. ITU-T H.265 clause 9.3: binarisations, context selection
- * and initialisation, arithmetic encoding) into an Annex-B byte stream of IDR pictures:
- * VPS, SPS, PPS, then one slice per picture.  The reference decoder parses these streams
+ * and initialisation, arithmetic encoding) into an Annex-B byte stream: VPS, SPS, PPS, then
+ * one slice per picture; an IDR picture first, then IDR pictures or low-delay P and B
+ * pictures (short-term reference picture sets in the slice headers, reference list sizes,
+ * TMVP, weighted prediction tables).  The reference decoder parses these streams
  * (src/decoding/syntax_elements.cpp, residual_coding.cpp:175, cabac.cpp:38); the records
  * it produces are the ones the generator drew, which tests/test_bitgen.py checks.
  *
@@ -34,12 +38,32 @@ typedef struct hevcgen_cfg {
     int32_t  max_level;          /* largest |level| drawn                                 */
     int32_t  qp_min, qp_max;     /* slice QP range                                        */
     int32_t  sao;                /* SAO enabled (parameters drawn per CTB)                */
+    /* inter pictures; inter = 0 makes every picture an IDR picture */
+    int32_t  inter;              /* 1: picture 0 is IDR, the others P or B (TRAIL_R)      */
+    double   p_b;                /* a non-IDR picture is a B picture (low delay: both     */
+                                 /* lists hold earlier pictures)                          */
+    int32_t  max_refs;           /* 1..4: the reference picture set keeps the last        */
+                                 /* max_refs pictures, each used by the current one or not */
+    double   p_intra_cu;         /* an intra CU in a P/B slice                            */
+    double   p_skip;             /* cu_skip_flag                                          */
+    double   p_merge;            /* merge_flag of a PU of a CU not skipped                */
+    int32_t  max_mvd;            /* largest |mvd| component drawn, quarter samples        */
+    int32_t  amp;                /* amp_enabled_flag (asymmetric partitions)              */
+    int32_t  tmvp;               /* sps_temporal_mvp_enabled_flag (slice flag drawn)      */
+    int32_t  max_merge;          /* MaxNumMergeCand 1..5; 0: drawn per slice              */
+    int32_t  wp;                 /* weighted_pred_flag and weighted_bipred_flag (tables   */
+                                 /* drawn per slice)                                      */
+    int32_t  depth_inter;        /* max_transform_hierarchy_depth_inter 0..2              */
 } hevcgen_cfg_t;
 
 void hevcgen_default_cfg(hevcgen_cfg_t* cfg, int32_t width, int32_t height, uint64_t seed);
 
-/* The stream and, per picture, the TU records the generator drew (intra TUs in decode
- * order, each with its N x N levels at coeff_offset in the picture's level pool). */
+/* The stream and, per picture, the records the generator drew: the TUs in decode order
+ * (every TU of an intra CU; the coded ones of an inter CU, as a decoder dequantises them),
+ * each coded one with its N x N levels at coeff_offset in the picture's level pool; and
+ * the PUs in decode order: position and size, and for a PU coded with AMVP its ref_idx
+ * (-1: list unused) and its coded mvd in mv (the decoder adds its predictor); a merged or
+ * skipped PU has ref_idx -2 in both lists (the decoder derives its motion). */
 typedef struct hevcgen_stream {
     uint8_t*  bytes;
     size_t    size;
@@ -48,6 +72,9 @@ typedef struct hevcgen_stream {
     hevc_tu_t** tus;             /* per picture                                           */
     uint64_t* num_coeffs;        /* per picture                                           */
     int16_t** coeffs;            /* per picture                                           */
+    int32_t*  slice_type;        /* per picture: 0 B, 1 P, 2 I (slice_type of 7.4.7.1)   */
+    int32_t*  num_pus;           /* per picture                                           */
+    hevc_pu_t** pus;             /* per picture                                           */
 } hevcgen_stream_t;
 
 hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg);
