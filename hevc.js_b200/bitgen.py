@@ -26,7 +26,14 @@ class GenCfg(C.Structure):
                 ("qp_max", C.c_int32), ("sao", C.c_int32), ("inter", C.c_int32), ("p_b", C.c_double),
                 ("max_refs", C.c_int32), ("p_intra_cu", C.c_double), ("p_skip", C.c_double),
                 ("p_merge", C.c_double), ("max_mvd", C.c_int32), ("amp", C.c_int32), ("tmvp", C.c_int32),
-                ("max_merge", C.c_int32), ("wp", C.c_int32), ("depth_inter", C.c_int32)]
+                ("max_merge", C.c_int32), ("wp", C.c_int32), ("depth_inter", C.c_int32),
+                ("qp_delta_depth", C.c_int32), ("chroma_qp_offsets", C.c_int32), ("deblock_ctl", C.c_int32),
+                ("slices", C.c_int32), ("dependent_slices", C.c_int32), ("tile_cols", C.c_int32), ("tile_rows", C.c_int32), ("wpp", C.c_int32),
+                ("p_bypass", C.c_double), ("p_tskip", C.c_double), ("sdh", C.c_int32), ("p_pcm", C.c_double),
+                ("scaling", C.c_int32), ("ref_quirks", C.c_int32)]
+
+# ref_quirks bits (csrc/bitgen.h): tools written the way the reference's parser reads them
+QUIRK_TILES_PCM, QUIRK_DEPENDENT = 1, 2
 
 
 class GenStream(C.Structure):

@@ -67,6 +67,24 @@ void nal(std::vector<uint8_t>& out, int type, const std::vector<uint8_t>& rbsp) 
     }
 }
 
+// Where each RBSP byte lands in the NAL unit payload once nal() inserts the emulation
+// prevention bytes (7.4.2): entry point offsets count payload bytes.
+std::vector<size_t> nal_positions(const std::vector<uint8_t>& rbsp) {
+    std::vector<size_t> pos(rbsp.size() + 1);
+    size_t o = 0;
+    int zeros = 0;
+    for (size_t i = 0; i < rbsp.size(); i++) {
+        if (zeros >= 2 && rbsp[i] <= 3) {
+            o++;
+            zeros = 0;
+        }
+        pos[i] = o++;
+        zeros = rbsp[i] == 0 ? zeros + 1 : 0;
+    }
+    pos[rbsp.size()] = o;
+    return pos;
+}
+
 // ---- CABAC encoder (9.3.4.3) ------------------------------------------------------------
 const uint8_t kRangeLps[64][4] = {
     {128, 176, 208, 240}, {128, 167, 197, 227}, {128, 158, 187, 216}, {123, 150, 178, 205}, {116, 142, 169, 195},
@@ -212,12 +230,19 @@ const uint8_t kInitGreater1[3][24] = {
     {154, 196, 196, 167, 154, 152, 167, 182, 182, 134, 149, 136, 153, 121, 136, 137, 169, 194, 166, 167, 154, 167, 137, 182},
     {154, 196, 167, 167, 154, 152, 167, 182, 182, 134, 149, 136, 153, 121, 136, 122, 169, 208, 166, 167, 154, 152, 167, 182}};
 const uint8_t kInitGreater2[3][6] = {{138, 153, 136, 167, 152, 152}, {107, 167, 91, 122, 107, 167}, {107, 167, 91, 107, 107, 167}};
+// cu_qp_delta_abs (2), cu_transquant_bypass_flag (1), transform_skip_flag (luma, chroma):
+// the same values for every initType
+const uint8_t kInitQpDelta = 154, kInitBypass = 154, kInitTskip = 139;
 
 struct Contexts {
     Ctx sao_merge, sao_type, split_cu[3], skip[3], pred_mode, part_mode[4], prev_intra_luma, intra_chroma, rqt_root_cbf,
         merge_flag, merge_idx, inter_pred_idc[5], ref_idx[2], mvp_flag, mvd_greater0, mvd_greater1, split_transform[3],
-        cbf_luma[2], cbf_chroma[4], last_x[18], last_y[18], csbf[4], sig[42], greater1[24], greater2[6];
+        cbf_luma[2], cbf_chroma[4], last_x[18], last_y[18], csbf[4], sig[42], greater1[24], greater2[6], qp_delta[2],
+        bypass, tskip[2];
     void init(int t, int qp) {   // t: initType
+        for (int i = 0; i < 2; i++) qp_delta[i].init(kInitQpDelta, qp);
+        bypass.init(kInitBypass, qp);
+        for (int i = 0; i < 2; i++) tskip[i].init(kInitTskip, qp);
         sao_merge.init(kInitSaoMerge[t], qp);
         sao_type.init(kInitSaoType[t], qp);
         for (int i = 0; i < 3; i++) split_cu[i].init(kInitSplitCu[t][i], qp);
@@ -267,11 +292,51 @@ void profile_tier_level(Bits& b) {
     b.put(120, 8);         // general_level_idc: 4
 }
 
+// The stream's parameter sets: what the SPS and PPS enable, drawn once per stream.
 struct Params {
     int W, H, log2_ctb, sao;
-    int inter = 0, dpb_minus1 = 1, amp = 0, tmvp = 0, wp = 0, depth_inter = 1;
+    int inter = 0, dpb_minus1 = 1, amp = 0, tmvp = 0, wp = 0, depth_inter = 1, log2_pml = 2;
+    int qp_delta = 0, qp_delta_depth = 0;                       // cu_qp_delta_enabled_flag, diff_cu_qp_delta_depth
+    int cb_qp_offset = 0, cr_qp_offset = 0, slice_chroma_offsets = 0;
+    int dbk_ctl = 0, dbk_override = 0, dbk_disabled = 0, beta_div2 = 0, tc_div2 = 0;
+    int lf_across_slices = 1, dependent_slices = 0;
+    int bypass = 0, tskip = 0, sdh = 0;
+    int pcm = 0, pcm_bits_y = 8, pcm_bits_c = 8, pcm_log2_min = 3, pcm_log2_max = 3, pcm_lf_disabled = 0;
+    int scaling = 0;                                            // 0 off, 1 default lists, 2 SPS lists, 3 PPS lists
+    int wpp = 0;                                                // entropy_coding_sync_enabled_flag
+    std::vector<int> col_bd, row_bd;                            // tile boundaries in CTBs (one tile: {0, w})
+    int uniform_tiles = 0, lf_across_tiles = 1;
     int log2_max_tb() const { return std::min(5, log2_ctb); }
+    int tiles() const { return (int)(col_bd.size() - 1) * (int)(row_bd.size() - 1); }
 };
+
+// scaling_list_data() (7.3.4): per size and matrix, a reference to an earlier (or the
+// default) list, or the list itself as DPCM deltas (every ScalingList entry 1..255).
+void scaling_list_data(Bits& b, std::mt19937_64& rng) {
+    auto uni = [&](int lo, int hi) { return std::uniform_int_distribution<int>(lo, hi)(rng); };
+    for (int size_id = 0; size_id < 4; size_id++)
+        for (int matrix_id = 0; matrix_id < 6; matrix_id += size_id == 3 ? 3 : 1) {
+            const bool explicit_list = uni(0, 2) != 0;
+            b.bit(explicit_list ? 1 : 0);                      // scaling_list_pred_mode_flag
+            if (!explicit_list) {
+                b.ue((uint32_t)uni(0, size_id == 3 ? matrix_id / 3 : matrix_id));   // ..._pred_matrix_id_delta
+                continue;
+            }
+            int next = 8;
+            const int n = std::min(64, 1 << (4 + (size_id << 1)));
+            if (size_id > 1) {
+                const int dc = uni(1, 255);
+                b.se(dc - 8);                                  // scaling_list_dc_coef_minus8
+                next = dc;
+            }
+            for (int i = 0; i < n; i++) {
+                const int v = uni(0, 3) ? uni(8, 40) : uni(1, 255);
+                const int delta = ((v - next + 128) & 255) - 128;
+                b.se(delta);                                   // scaling_list_delta_coef
+                next = v;
+            }
+        }
+}
 
 std::vector<uint8_t> vps(const Params& p) {
     Bits b;
@@ -295,7 +360,7 @@ std::vector<uint8_t> vps(const Params& p) {
     return b.buf;
 }
 
-std::vector<uint8_t> sps(const Params& p) {
+std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
     Bits b;
     b.put(0, 4);           // sps_video_parameter_set_id
     b.put(0, 3);           // sps_max_sub_layers_minus1
@@ -319,10 +384,21 @@ std::vector<uint8_t> sps(const Params& p) {
     b.ue((uint32_t)(p.log2_max_tb() - 2));   // log2_diff_max_min_luma_transform_block_size
     b.ue((uint32_t)p.depth_inter);           // max_transform_hierarchy_depth_inter
     b.ue(1);               // max_transform_hierarchy_depth_intra
-    b.bit(0);              // scaling_list_enabled_flag
+    b.bit(p.scaling ? 1 : 0);                // scaling_list_enabled_flag
+    if (p.scaling) {
+        b.bit(p.scaling == 2 ? 1 : 0);       // sps_scaling_list_data_present_flag
+        if (p.scaling == 2) scaling_list_data(b, rng);
+    }
     b.bit(p.amp ? 1 : 0);  // amp_enabled_flag
     b.bit(p.sao ? 1 : 0);  // sample_adaptive_offset_enabled_flag
-    b.bit(0);              // pcm_enabled_flag
+    b.bit(p.pcm ? 1 : 0);  // pcm_enabled_flag
+    if (p.pcm) {
+        b.put((uint32_t)(p.pcm_bits_y - 1), 4);              // pcm_sample_bit_depth_luma_minus1
+        b.put((uint32_t)(p.pcm_bits_c - 1), 4);              // pcm_sample_bit_depth_chroma_minus1
+        b.ue((uint32_t)(p.pcm_log2_min - 3));                // log2_min_pcm_luma_coding_block_size_minus3
+        b.ue((uint32_t)(p.pcm_log2_max - p.pcm_log2_min));   // log2_diff_max_min_pcm_luma_coding_block_size
+        b.bit(p.pcm_lf_disabled ? 1 : 0);                    // pcm_loop_filter_disabled_flag
+    }
     b.ue(0);               // num_short_term_ref_pic_sets
     b.bit(0);              // long_term_ref_pics_present_flag
     b.bit(p.tmvp ? 1 : 0); // sps_temporal_mvp_enabled_flag
@@ -333,34 +409,56 @@ std::vector<uint8_t> sps(const Params& p) {
     return b.buf;
 }
 
-std::vector<uint8_t> pps(const Params& p) {
+std::vector<uint8_t> pps(const Params& p, std::mt19937_64& rng) {
     Bits b;
     b.ue(0);               // pps_pic_parameter_set_id
     b.ue(0);               // pps_seq_parameter_set_id
-    b.bit(0);              // dependent_slice_segments_enabled_flag
+    b.bit(p.dependent_slices ? 1 : 0);       // dependent_slice_segments_enabled_flag
     b.bit(0);              // output_flag_present_flag
     b.put(0, 3);           // num_extra_slice_header_bits
-    b.bit(0);              // sign_data_hiding_enabled_flag
+    b.bit(p.sdh ? 1 : 0);  // sign_data_hiding_enabled_flag
     b.bit(p.inter ? 1 : 0);   // cabac_init_present_flag (cabac_init_flag drawn per slice)
     b.ue(0);               // num_ref_idx_l0_default_active_minus1
     b.ue(0);               // num_ref_idx_l1_default_active_minus1
     b.se(0);               // init_qp_minus26
     b.bit(0);              // constrained_intra_pred_flag
-    b.bit(0);              // transform_skip_enabled_flag
-    b.bit(0);              // cu_qp_delta_enabled_flag
-    b.se(0);               // pps_cb_qp_offset
-    b.se(0);               // pps_cr_qp_offset
-    b.bit(0);              // pps_slice_chroma_qp_offsets_present_flag
+    b.bit(p.tskip ? 1 : 0);                  // transform_skip_enabled_flag
+    b.bit(p.qp_delta ? 1 : 0);               // cu_qp_delta_enabled_flag
+    if (p.qp_delta) b.ue((uint32_t)p.qp_delta_depth);   // diff_cu_qp_delta_depth
+    b.se(p.cb_qp_offset);  // pps_cb_qp_offset
+    b.se(p.cr_qp_offset);  // pps_cr_qp_offset
+    b.bit(p.slice_chroma_offsets ? 1 : 0);   // pps_slice_chroma_qp_offsets_present_flag
     b.bit(p.wp ? 1 : 0);   // weighted_pred_flag
     b.bit(p.wp ? 1 : 0);   // weighted_bipred_flag
-    b.bit(0);              // transquant_bypass_enabled_flag
-    b.bit(0);              // tiles_enabled_flag
-    b.bit(0);              // entropy_coding_sync_enabled_flag
-    b.bit(1);              // pps_loop_filter_across_slices_enabled_flag
-    b.bit(0);              // deblocking_filter_control_present_flag
-    b.bit(0);              // pps_scaling_list_data_present_flag
+    b.bit(p.bypass ? 1 : 0);                 // transquant_bypass_enabled_flag
+    const bool tiles = p.tiles() > 1;
+    b.bit(tiles ? 1 : 0);  // tiles_enabled_flag
+    b.bit(p.wpp ? 1 : 0);  // entropy_coding_sync_enabled_flag
+    if (tiles) {
+        const int nc = (int)p.col_bd.size() - 1, nr = (int)p.row_bd.size() - 1;
+        b.ue((uint32_t)(nc - 1));            // num_tile_columns_minus1
+        b.ue((uint32_t)(nr - 1));            // num_tile_rows_minus1
+        b.bit(p.uniform_tiles ? 1 : 0);      // uniform_spacing_flag
+        if (!p.uniform_tiles) {
+            for (int i = 0; i < nc - 1; i++) b.ue((uint32_t)(p.col_bd[(size_t)i + 1] - p.col_bd[(size_t)i] - 1));
+            for (int i = 0; i < nr - 1; i++) b.ue((uint32_t)(p.row_bd[(size_t)i + 1] - p.row_bd[(size_t)i] - 1));
+        }
+        b.bit(p.lf_across_tiles ? 1 : 0);    // loop_filter_across_tiles_enabled_flag
+    }
+    b.bit(p.lf_across_slices ? 1 : 0);       // pps_loop_filter_across_slices_enabled_flag
+    b.bit(p.dbk_ctl ? 1 : 0);                // deblocking_filter_control_present_flag
+    if (p.dbk_ctl) {
+        b.bit(p.dbk_override ? 1 : 0);       // deblocking_filter_override_enabled_flag
+        b.bit(p.dbk_disabled ? 1 : 0);       // pps_deblocking_filter_disabled_flag
+        if (!p.dbk_disabled) {
+            b.se(p.beta_div2);               // pps_beta_offset_div2
+            b.se(p.tc_div2);                 // pps_tc_offset_div2
+        }
+    }
+    b.bit(p.scaling == 3 ? 1 : 0);           // pps_scaling_list_data_present_flag
+    if (p.scaling == 3) scaling_list_data(b, rng);
     b.bit(0);              // lists_modification_present_flag
-    b.ue(0);               // log2_parallel_merge_level_minus2
+    b.ue((uint32_t)(p.log2_pml - 2));        // log2_parallel_merge_level_minus2
     b.bit(0);              // slice_segment_header_extension_present_flag
     b.bit(0);              // pps_extension_present_flag
     b.trailing();
@@ -389,11 +487,23 @@ struct Picture {
     const hevcgen_cfg_t& cfg;
     std::mt19937_64& rng;
     Params p;
-    int qp = 26;
     int wctb = 0, hctb = 0;
-    // the slice: type (0 B, 1 P, 2 I), active reference list sizes, MaxNumMergeCand
-    int slice_type = 2, num_ref[2] = {0, 0}, max_merge = 5;
+    // the picture's slices and tiles: per raster CTB address, the SliceAddrRs of its slice
+    // and its TileId; CtbAddrTsToRs
+    std::vector<int> ctb_slice, ctb_tile, ts_to_rs;
+    int cur_slice = 0, cur_tile = 0;
+    // the slice: type (0 B, 1 P, 2 I), SliceQpY, chroma QP offsets (PPS + slice), SAO
+    // flags, active reference list sizes, MaxNumMergeCand
+    int slice_type = 2, qp = 26, cb_off = 0, cr_off = 0;
+    bool sao_luma = true, sao_chroma = true;
+    int num_ref[2] = {0, 0}, max_merge = 5;
     bool mvd_l1_zero = false;
+    // quantization groups (8.6.1): QpY per 8x8 unit, the last CU's QpY, the current group
+    std::vector<uint8_t> qp8;
+    int last_cu_qp = 26, qg_x = 0, qg_y = 0, qg_pred = 26, qp_delta_val = 0;
+    bool first_qg = true, qg_new = false, qp_delta_coded = false;
+    bool cu_bypass = false;   // cu_transquant_bypass_flag of the current CU
+    bool pcm_cu = false;      // pcm_flag of the current CU
     std::vector<uint8_t> depth8;   // CtDepth per 8x8 unit
     std::vector<uint8_t> skip8;    // cu_skip_flag per 8x8 unit
     std::vector<uint8_t> mode4;    // IntraPredModeY per 4x4 luma unit (DC for inter CUs)
@@ -408,15 +518,47 @@ struct Picture {
     double u01() { return std::uniform_real_distribution<double>(0.0, 1.0)(rng); }
     int uni(int lo, int hi) { return std::uniform_int_distribution<int>(lo, hi)(rng); }
 
-    // split_cu_flag context: neighbours deeper than this node (9.3.4.2.2)
+    // z-scan availability of a neighbouring luma location (6.4.1): inside the picture, in
+    // the current slice and tile (left and above neighbours there are decoded already)
+    bool avail(int xN, int yN) const {
+        if (xN < 0 || yN < 0 || xN >= p.W || yN >= p.H) return false;
+        const size_t a = (size_t)(yN >> p.log2_ctb) * (size_t)wctb + (size_t)(xN >> p.log2_ctb);
+        return ctb_slice[a] == cur_slice && ctb_tile[a] == cur_tile;
+    }
+
+    // QpY of the current CU (8.6.1): the group's prediction plus CuQpDeltaVal
+    int cu_qp() const { return p.qp_delta ? (qg_pred + qp_delta_val + 52) % 52 : qp; }
+
+    // qPY_PRED of a new quantization group at (qg_x, qg_y): the left and above groups'
+    // QpY when they lie in the same CTB, else qPY_PREV (the previous CU's QpY, or SliceQpY
+    // for the first group of a slice, a tile, or a CTB row under WPP)
+    void start_quantization_group() {
+        const int prev = first_qg ? qp : last_cu_qp;
+        first_qg = false;
+        const int w8 = p.W / 8, mask = (1 << p.log2_ctb) - 1;
+        const int qa = (qg_x & mask) ? qp8[(size_t)(qg_y / 8) * w8 + (qg_x - 1) / 8] : prev;
+        const int qb = (qg_y & mask) ? qp8[(size_t)((qg_y - 1) / 8) * w8 + qg_x / 8] : prev;
+        qg_pred = (qa + qb + 1) >> 1;
+    }
+
+    // coding_quadtree() (7.3.8.4); split_cu_flag context: available neighbours deeper than
+    // this node (9.3.4.2.2).  A node of the quantization group size or larger starts a
+    // group (IsCuQpDeltaCoded = 0, CuQpDeltaVal = 0).
     void coding_quadtree(int x0, int y0, int log2, int depth) {
         const int size = 1 << log2;
+        if (p.qp_delta && log2 >= p.log2_ctb - p.qp_delta_depth) {
+            qp_delta_coded = false;
+            qp_delta_val = 0;
+            qg_x = x0;
+            qg_y = y0;
+            qg_new = true;
+        }
         bool split;
         if (x0 + size <= p.W && y0 + size <= p.H && log2 > 3) {
             split = u01() < cfg.p_split;
             const int w8 = p.W / 8;
-            const int inc = (x0 > 0 && depth8[(size_t)(y0 / 8) * w8 + (x0 - 1) / 8] > depth) +
-                            (y0 > 0 && depth8[(size_t)((y0 - 1) / 8) * w8 + x0 / 8] > depth);
+            const int inc = (avail(x0 - 1, y0) && depth8[(size_t)(y0 / 8) * w8 + (x0 - 1) / 8] > depth) +
+                            (avail(x0, y0 - 1) && depth8[(size_t)((y0 - 1) / 8) * w8 + x0 / 8] > depth);
             E.decision(C.split_cu[inc], split);
         } else {
             split = log2 > 3;
@@ -432,7 +574,14 @@ struct Picture {
         const int w8 = p.W / 8;
         for (int y = y0 / 8; y < (y0 + size) / 8; y++)
             for (int x = x0 / 8; x < (x0 + size) / 8; x++) depth8[(size_t)y * w8 + x] = (uint8_t)depth;
+        if (qg_new || !p.qp_delta) {
+            if (p.qp_delta) start_quantization_group();
+            qg_new = false;
+        }
+        pcm_cu = false;
         coding_unit(x0, y0, log2, depth);
+        if (!(pcm_cu && (cfg.ref_quirks & HEVCGEN_QUIRK_TILES_PCM))) last_cu_qp = cu_qp();
+        fill(qp8, 8, w8, x0, y0, size, size, (uint8_t)last_cu_qp);
     }
 
     // fill a per-unit map over a rectangle of luma samples
@@ -444,9 +593,9 @@ struct Picture {
     // candModeList of a prediction block (8.4.2)
     void mpm(int xPb, int yPb, int cand[3]) {
         const int w4 = p.W / 4;
-        const int a = xPb > 0 ? mode4[(size_t)(yPb / 4) * w4 + (xPb - 1) / 4] : 1;
+        const int a = avail(xPb - 1, yPb) ? mode4[(size_t)(yPb / 4) * w4 + (xPb - 1) / 4] : 1;
         const bool above_in_ctb_row = yPb - 1 >= ((yPb >> p.log2_ctb) << p.log2_ctb);
-        const int b = (yPb > 0 && above_in_ctb_row) ? mode4[(size_t)((yPb - 1) / 4) * w4 + xPb / 4] : 1;
+        const int b = (avail(xPb, yPb - 1) && above_in_ctb_row) ? mode4[(size_t)((yPb - 1) / 4) * w4 + xPb / 4] : 1;
         if (a == b) {
             if (a < 2) {
                 cand[0] = 0;
@@ -468,11 +617,16 @@ struct Picture {
     // above CUs' flags, 9.3.4.2.2), then pred_mode_flag; inter CUs go to inter_cu.
     void coding_unit(int x0, int y0, int log2, int depth) {
         const int size = 1 << log2;
+        cu_bypass = false;
+        if (p.bypass) {
+            cu_bypass = u01() < cfg.p_bypass;
+            E.decision(C.bypass, cu_bypass);   // cu_transquant_bypass_flag
+        }
         if (slice_type != 2) {
             const int w8 = p.W / 8;
             const bool skip = u01() < cfg.p_skip;
-            const int inc = (x0 > 0 && skip8[(size_t)(y0 / 8) * w8 + (x0 - 1) / 8]) +
-                            (y0 > 0 && skip8[(size_t)((y0 - 1) / 8) * w8 + x0 / 8]);
+            const int inc = (avail(x0 - 1, y0) && skip8[(size_t)(y0 / 8) * w8 + (x0 - 1) / 8]) +
+                            (avail(x0, y0 - 1) && skip8[(size_t)((y0 - 1) / 8) * w8 + x0 / 8]);
             E.decision(C.skip[inc], skip);
             fill(skip8, 8, w8, x0, y0, size, size, skip ? 1 : 0);
             if (skip) {
@@ -489,6 +643,14 @@ struct Picture {
         }
         const bool nxn = log2 == 3 && u01() < cfg.p_nxn;
         if (log2 == 3) E.decision(C.part_mode[0], nxn ? 0 : 1);   // part_mode: PART_2Nx2N = 1, PART_NxN = 0
+        if (!nxn && p.pcm && log2 >= p.pcm_log2_min && log2 <= p.pcm_log2_max) {
+            const bool pcm = u01() < cfg.p_pcm;
+            E.terminate(pcm);   // pcm_flag
+            if (pcm) {
+                pcm_sample(x0, y0, log2);
+                return;
+            }
+        }
         const int npb = nxn ? 4 : 1, pbs = nxn ? size / 2 : size;
         int mode[4], flag[4], idx[4];
         const int w4 = p.W / 4;
@@ -680,6 +842,52 @@ struct Picture {
         return false;
     }
 
+    // cu_qp_delta_abs (9.3.3.10: prefix TR cMax 5, first bin context 0, the others context
+    // 1; suffix EG0 bypass) and cu_qp_delta_sign_flag; CuQpDeltaVal in -26..25 (7.4.9.14)
+    void cu_qp_delta() {
+        const int v = u01() < 0.6 ? uni(-3, 3) : uni(-26, 25), a = std::abs(v);
+        for (int k = 0; k < 5; k++) {
+            E.decision(C.qp_delta[k ? 1 : 0], k < a);
+            if (k >= a) break;
+        }
+        if (a >= 5) exp_golomb((uint32_t)(a - 5), 0);
+        if (a) E.bypass(v < 0);
+        qp_delta_val = v;
+        qp_delta_coded = true;
+    }
+
+    // pcm_sample() (7.3.8.7) after a pcm_flag of 1: the arithmetic code is flushed (the
+    // terminate bin's flush ends in a 1 bit), pcm_alignment_zero_bits, the samples at
+    // PcmBitDepth bits, then the arithmetic encoder restarts (9.3.2.5).  The records: one
+    // PCM TU per plane whose levels are the reconstructed samples (value << (8 - depth)).
+    void pcm_sample(int x0, int y0, int log2) {
+        pcm_cu = true;
+        Bits& b = *E.out;
+        if ((cfg.ref_quirks & HEVCGEN_QUIRK_TILES_PCM) && b.n == 0) b.put(0x80, 8);
+        b.align_zero();
+        fill(mode4, 4, p.W / 4, x0, y0, 1 << log2, 1 << log2, 1);
+        for (int c = 0; c < 3; c++) {
+            const int l2 = c ? log2 - 1 : log2, bits = c ? p.pcm_bits_c : p.pcm_bits_y;
+            hevc_tu_t t{};
+            t.x = (uint16_t)(c ? x0 / 2 : x0);
+            t.y = (uint16_t)(c ? y0 / 2 : y0);
+            t.log2_size = (uint8_t)l2;
+            t.c_idx = (uint8_t)c;
+            t.qp = (uint8_t)cu_qp();
+            t.flags = (uint8_t)(HEVC_TU_INTRA | HEVC_TU_CODED | HEVC_TU_PCM | (cu_bypass ? HEVC_TU_BYPASS : 0));
+            t.intra_mode = 1;
+            t.coeff_offset = (uint32_t)coeffs.size();
+            for (int i = 0; i < 1 << (2 * l2); i++) {
+                const int v = uni(0, (1 << bits) - 1);
+                b.put((uint32_t)v, bits);
+                coeffs.push_back((int16_t)(v << (8 - bits)));
+            }
+            tus.push_back(t);
+        }
+        E.start(&b);
+        if (cfg.ref_quirks & HEVCGEN_QUIRK_TILES_PCM) C.init(init_type, qp);
+    }
+
     void record(int c, int x, int y, int log2, int mode, bool coded, bool inter) {
         if (inter && !coded) return;   // a decoder sees the coded TUs of an inter CU only
         hevc_tu_t t{};
@@ -687,8 +895,10 @@ struct Picture {
         t.y = (uint16_t)y;
         t.log2_size = (uint8_t)log2;
         t.c_idx = (uint8_t)c;
-        t.qp = (uint8_t)(c ? chroma_qp(qp) : qp);
-        t.flags = (uint8_t)((inter ? 0 : HEVC_TU_INTRA) | (coded ? HEVC_TU_CODED : 0));
+        const int qpy = cu_qp();
+        t.qp = (uint8_t)(c ? chroma_qp(qpy + (c == 1 ? cb_off : cr_off)) : qpy);
+        t.flags = (uint8_t)((inter ? 0 : HEVC_TU_INTRA) | (coded ? HEVC_TU_CODED : 0) |
+                            (coded && cu_bypass ? HEVC_TU_BYPASS : 0));
         t.intra_mode = (uint8_t)(inter ? 0 : mode);
         t.coeff_offset = 0;
         if (coded) {
@@ -736,6 +946,7 @@ struct Picture {
             cbf_luma = u01() < cfg.p_cbf;
             E.decision(C.cbf_luma[depth == 0 ? 1 : 0], cbf_luma);
         }
+        if ((cbf_luma || cb || cr) && p.qp_delta && !qp_delta_coded) cu_qp_delta();
         const int w4 = p.W / 4;
         const int lmode = inter ? -1 : mode4[(size_t)(y0 / 4) * w4 + x0 / 4];
         record(0, x0, y0, log2, lmode, cbf_luma, inter);
@@ -782,62 +993,136 @@ struct Picture {
         }
     }
 
-    // slice_segment_header() (7.3.6.1) and slice_segment_data() (7.3.8.1) of the picture's
-    // one slice.  A P/B picture's short-term RPS (7.3.7, coded in the header) keeps the
-    // pictures in gop.refs (most recent first, each used by this picture or not); both
-    // reference lists repeat the used ones, most recent first (8.3.4, low delay).
-    std::vector<uint8_t> slice_data_and_header(int poc, GopState& gop) {
-        Bits b;
+    // The picture's slice segments in tile scan: [start, end) CtbAddrInTs and whether the
+    // segment is dependent.  Cuts are drawn; with tiles a slice or segment either lies in one
+    // tile or holds whole tiles, and under WPP a segment that starts inside a CTB row ends
+    // in that row (7.4.7.1 constraints).
+    struct Segment {
+        int start, end;
+        bool dependent;
+    };
+    std::vector<Segment> draw_segments() {
+        const int n = wctb * hctb;
+        std::vector<uint8_t> cut((size_t)n + 1, 0), indep((size_t)n + 1, 0);
+        cut[0] = indep[0] = 1;
+        cut[(size_t)n] = 1;
+        const int max_seg = std::max(1, cfg.slices);
+        const double p_cut = max_seg > 1 ? std::min(0.5, 1.5 * (max_seg - 1) / n) : 0.0;
+        std::vector<uint8_t> tile_start((size_t)n + 1, 0), split_tile((size_t)p.tiles(), 0);
+        for (int ts = 0; ts < n; ts++) tile_start[(size_t)ts] = ts == 0 || ctb_tile[(size_t)ts_to_rs[(size_t)ts]] != ctb_tile[(size_t)ts_to_rs[(size_t)ts - 1]];
+        tile_start[(size_t)n] = 1;
+        if (p.tiles() > 1) {
+            for (int t = 0; t < p.tiles(); t++) split_tile[(size_t)t] = max_seg > 1 && u01() < 0.4;
+            for (int ts = 1; ts < n; ts++) {
+                const int t = ctb_tile[(size_t)ts_to_rs[(size_t)ts]];
+                if (tile_start[(size_t)ts]) {
+                    const int tp = ctb_tile[(size_t)ts_to_rs[(size_t)ts - 1]];
+                    const bool forced = split_tile[(size_t)t] || split_tile[(size_t)tp];
+                    cut[(size_t)ts] = forced || (max_seg > 1 && u01() < 0.5);
+                    indep[(size_t)ts] = forced;
+                } else if (split_tile[(size_t)t]) {
+                    cut[(size_t)ts] = u01() < p_cut * 2;
+                }
+            }
+        } else {
+            for (int ts = 1; ts < n; ts++) cut[(size_t)ts] = u01() < p_cut;
+            if (p.wpp) {   // a segment starting inside a row ends in it
+                bool mid = false;
+                for (int ts = 1; ts <= n; ts++) {
+                    if (ts % wctb == 0 && mid) cut[(size_t)ts] = 1;
+                    if (ts % wctb == 0) mid = false;
+                    if (cut[(size_t)ts] && ts % wctb != 0) mid = true;
+                }
+            }
+        }
+        std::vector<Segment> segs;
+        for (int ts = 0; ts < n;) {
+            int e = ts + 1;
+            while (!cut[(size_t)e]) e++;
+            const bool dep = !indep[(size_t)ts] && p.dependent_slices && u01() < 0.5;
+            segs.push_back({ts, e, dep});
+            ts = e;
+        }
+        return segs;
+    }
+
+    // The reference picture set, the reference lists and TMVP of a P/B picture: the same
+    // in every slice of the picture.  used: StCurrBefore (most recent first).
+    struct InterPic {
+        std::vector<int> used_flags, used;
+        bool tmvp = false, col_l0 = true;
+        int col_ref = 0;
+    };
+    InterPic draw_inter(int poc, GopState& gop) {
+        InterPic ip;
+        const int n = (int)gop.refs.size();
+        int n_used = 0;
+        for (int i = 0; i < n; i++) {
+            const int u = (i == n - 1 && !n_used) || u01() < 0.7;
+            ip.used_flags.push_back(u);
+            n_used += u;
+            if (u) ip.used.push_back(gop.refs[(size_t)i]);
+        }
+        const bool override_refs = u01() < 0.7;
+        num_ref[0] = override_refs ? uni(1, 4) : 1;
+        num_ref[1] = slice_type == 0 ? (override_refs ? uni(1, 4) : 1) : 0;
+        ip.tmvp = p.tmvp && u01() < 0.8;
+        if (ip.tmvp) {
+            ip.col_l0 = slice_type == 1 || u01() < 0.5;
+            const int nl = num_ref[ip.col_l0 ? 0 : 1];
+            std::vector<int> ok;   // entries after the last picture without TMVP (7.4.7.1)
+            for (int i = 0; i < nl; i++)
+                if (ip.used[(size_t)i % ip.used.size()] >= gop.tmvp_barrier) ok.push_back(i);
+            if (ok.empty()) ip.tmvp = false;
+            else ip.col_ref = ok[(size_t)uni(0, (int)ok.size() - 1)];
+        }
+        if (!ip.tmvp) gop.tmvp_barrier = poc;
+        return ip;
+    }
+
+    // slice_segment_header() (7.3.6.1) up to (not including) the entry points; draws the
+    // slice's values for an independent segment.  Returns the initType.
+    int segment_header(Bits& b, const Segment& sg, int poc, const InterPic& ip) {
         const bool idr = slice_type == 2;
-        b.bit(1);            // first_slice_segment_in_pic_flag
-        if (idr) b.bit(0);   // no_output_of_prior_pics_flag
-        b.ue(0);             // slice_pic_parameter_set_id
+        const int nctb = wctb * hctb;
+        b.bit(sg.start == 0);   // first_slice_segment_in_pic_flag
+        if (idr) b.bit(0);      // no_output_of_prior_pics_flag
+        b.ue(0);                // slice_pic_parameter_set_id
+        if (sg.start > 0) {
+            if (p.dependent_slices) b.bit(sg.dependent ? 1 : 0);   // dependent_slice_segment_flag
+            int bits = 0;
+            while ((1 << bits) < nctb) bits++;
+            b.put((uint32_t)ts_to_rs[(size_t)sg.start], bits);      // slice_segment_address
+        }
+        if (sg.dependent) return init_type;
         b.ue((uint32_t)slice_type);
-        int init_type = 0;
         if (!idr) {
             b.put((uint32_t)(poc & 255), 8);   // slice_pic_order_cnt_lsb
             b.bit(0);                          // short_term_ref_pic_set_sps_flag
-            const int n = (int)gop.refs.size();
-            std::vector<int> used((size_t)n);
-            int n_used = 0;
-            for (int i = 0; i < n; i++) n_used += used[(size_t)i] = (i == n - 1 && !n_used) || u01() < 0.7;
-            b.ue((uint32_t)n);                 // num_negative_pics
-            b.ue(0);                           // num_positive_pics
-            int prev = poc;
-            std::vector<int> cur;              // StCurrBefore
-            for (int i = 0; i < n; i++) {
-                b.ue((uint32_t)(prev - gop.refs[(size_t)i] - 1));   // delta_poc_s0_minus1
-                b.bit(used[(size_t)i]);                              // used_by_curr_pic_s0_flag
-                prev = gop.refs[(size_t)i];
-                if (used[(size_t)i]) cur.push_back(gop.refs[(size_t)i]);
+            b.ue((uint32_t)ip.used_flags.size());   // num_negative_pics
+            b.ue(0);                                // num_positive_pics
+            for (size_t i = 0; i < ip.used_flags.size(); i++) {
+                b.ue(0);                       // delta_poc_s0_minus1: consecutive earlier pictures
+                b.bit(ip.used_flags[i]);       // used_by_curr_pic_s0_flag
             }
-            // the reference lists and the collocated picture
-            const bool override_refs = u01() < 0.7;
-            num_ref[0] = override_refs ? uni(1, 4) : 1;
-            num_ref[1] = slice_type == 0 ? (override_refs ? uni(1, 4) : 1) : 0;
-            bool tmvp = p.tmvp && u01() < 0.8;
-            bool col_l0 = true;
-            int col_ref = 0;
-            if (tmvp) {
-                col_l0 = slice_type == 1 || u01() < 0.5;
-                const int nl = num_ref[col_l0 ? 0 : 1];
-                std::vector<int> ok;   // entries after the last picture without TMVP (7.4.7.1)
-                for (int i = 0; i < nl; i++)
-                    if (cur[(size_t)i % cur.size()] >= gop.tmvp_barrier) ok.push_back(i);
-                if (ok.empty()) tmvp = false;
-                else col_ref = ok[(size_t)uni(0, (int)ok.size() - 1)];
-            }
-            if (!tmvp) gop.tmvp_barrier = poc;
-            if (p.tmvp) b.bit(tmvp ? 1 : 0);   // slice_temporal_mvp_enabled_flag
-            if (p.sao) {
-                b.bit(1);    // slice_sao_luma_flag
-                b.bit(1);    // slice_sao_chroma_flag
-            }
+            if (p.tmvp) b.bit(ip.tmvp ? 1 : 0);   // slice_temporal_mvp_enabled_flag
+        }
+        sao_luma = sao_chroma = false;
+        if (p.sao) {
+            sao_luma = u01() < 0.85;
+            sao_chroma = u01() < 0.85;
+            b.bit(sao_luma ? 1 : 0);           // slice_sao_luma_flag
+            b.bit(sao_chroma ? 1 : 0);         // slice_sao_chroma_flag
+        }
+        init_type = 0;
+        if (!idr) {
+            const bool override_refs = num_ref[0] != 1 || (slice_type == 0 && num_ref[1] != 1) || u01() < 0.3;
             b.bit(override_refs ? 1 : 0);      // num_ref_idx_active_override_flag
             if (override_refs) {
                 b.ue((uint32_t)(num_ref[0] - 1));
                 if (slice_type == 0) b.ue((uint32_t)(num_ref[1] - 1));
             }
+            mvd_l1_zero = false;
             if (slice_type == 0) {
                 mvd_l1_zero = u01() < 0.3;
                 b.bit(mvd_l1_zero ? 1 : 0);    // mvd_l1_zero_flag
@@ -845,35 +1130,155 @@ struct Picture {
             const bool cabac_init = u01() < 0.3;
             b.bit(cabac_init ? 1 : 0);         // cabac_init_flag
             init_type = slice_type == 1 ? (cabac_init ? 2 : 1) : (cabac_init ? 1 : 2);
-            if (tmvp) {
-                if (slice_type == 0) b.bit(col_l0 ? 1 : 0);   // collocated_from_l0_flag
-                if (num_ref[col_l0 ? 0 : 1] > 1) b.ue((uint32_t)col_ref);   // collocated_ref_idx
+            if (ip.tmvp) {
+                if (slice_type == 0) b.bit(ip.col_l0 ? 1 : 0);                  // collocated_from_l0_flag
+                if (num_ref[ip.col_l0 ? 0 : 1] > 1) b.ue((uint32_t)ip.col_ref);  // collocated_ref_idx
             }
             if (p.wp) pred_weight_table(b);
             max_merge = cfg.max_merge ? cfg.max_merge : uni(1, 5);
             b.ue((uint32_t)(5 - max_merge));   // five_minus_max_num_merge_cand
-        } else if (p.sao) {
-            b.bit(1);        // slice_sao_luma_flag
-            b.bit(1);        // slice_sao_chroma_flag
         }
-        b.se(qp - 26);       // slice_qp_delta
-        b.bit(1);            // slice_loop_filter_across_slices_enabled_flag
-        b.trailing();        // byte_alignment()
-        // the pictures kept for the next picture: this one and the most recent others
+        qp = uni(cfg.qp_min, cfg.qp_max);
+        b.se(qp - 26);                         // slice_qp_delta
+        cb_off = p.cb_qp_offset;
+        cr_off = p.cr_qp_offset;
+        if (p.slice_chroma_offsets) {
+            const int scb = uni(std::max(-12, -12 - p.cb_qp_offset), std::min(12, 12 - p.cb_qp_offset));
+            const int scr = uni(std::max(-12, -12 - p.cr_qp_offset), std::min(12, 12 - p.cr_qp_offset));
+            b.se(scb);                         // slice_cb_qp_offset
+            b.se(scr);                         // slice_cr_qp_offset
+            cb_off += scb;
+            cr_off += scr;
+        }
+        bool dbk_disabled = p.dbk_disabled;
+        if (p.dbk_override) {
+            const bool ov = u01() < 0.5;
+            b.bit(ov ? 1 : 0);                 // deblocking_filter_override_flag
+            if (ov) {
+                dbk_disabled = u01() < 0.3;
+                b.bit(dbk_disabled ? 1 : 0);   // slice_deblocking_filter_disabled_flag
+                if (!dbk_disabled) {
+                    b.se(uni(-6, 6));          // slice_beta_offset_div2
+                    b.se(uni(-6, 6));          // slice_tc_offset_div2
+                }
+            }
+        }
+        if (p.lf_across_slices && (sao_luma || sao_chroma || !dbk_disabled))
+            b.bit(u01() < 0.5 ? 1 : 0);        // slice_loop_filter_across_slices_enabled_flag
+        return init_type;
+    }
+    int init_type = 0;
+
+    // slice_segment_data() (7.3.8.1) of one segment into d: CTUs in tile scan, each
+    // followed by end_of_slice_segment_flag, and end_of_subset_one_bit + byte_alignment()
+    // before a new tile or (WPP) a new CTB row; starts[k] is the byte offset of substream k.
+    // Contexts (9.3.1): initialised at the segment (unless dependent), at each tile, and
+    // at each row under WPP, where they come from the state stored after the second CTB of
+    // the row above when that CTB is available.
+    void segment_data(Bits& d, const Segment& sg, std::vector<size_t>& starts) {
+        Contexts wpp_saved;
+        for (int ts = sg.start; ts < sg.end; ts++) {
+            const int rs = ts_to_rs[(size_t)ts], rx = rs % wctb, ry = rs / wctb;
+            cur_tile = ctb_tile[(size_t)rs];
+            cur_slice = ctb_slice[(size_t)rs];
+            const bool new_tile = ts == 0 || ctb_tile[(size_t)ts_to_rs[(size_t)ts - 1]] != cur_tile;
+            const bool row_start = p.wpp && rx == 0;
+            if (ts == sg.start || new_tile || row_start) {
+                starts.push_back(d.buf.size());
+                E.start(&d);
+                const bool quirk_tiles = cfg.ref_quirks & HEVCGEN_QUIRK_TILES_PCM;
+                if (new_tile && !(quirk_tiles && (ts != sg.start || sg.dependent))) {
+                    C.init(init_type, qp);
+                } else if (new_tile) {
+                } else if (row_start) {
+                    if (avail((rx + 1) << p.log2_ctb, (ry - 1) << p.log2_ctb)) C = wpp_saved;
+                    else C.init(init_type, qp);
+                } else if (!sg.dependent) {
+                    C.init(init_type, qp);
+                }
+                if (new_tile || row_start || !sg.dependent || (cfg.ref_quirks & HEVCGEN_QUIRK_DEPENDENT)) {
+                    first_qg = true;
+                    last_cu_qp = qp;   // qPY_PREV of the group; also the QpY a PCM CU takes in quirk mode
+                }
+            }
+            if (p.sao && (sao_luma || sao_chroma)) sao(rx, ry);
+            coding_quadtree(rx << p.log2_ctb, ry << p.log2_ctb, p.log2_ctb, 0);
+            if (p.wpp && rx == 1) wpp_saved = C;
+            const bool last = ts == sg.end - 1;
+            E.terminate(last);   // end_of_slice_segment_flag
+            if (last) {
+                d.align_zero();  // the flush's last bit is rbsp_stop_one_bit
+            } else {
+                const int nrs = ts_to_rs[(size_t)ts + 1];
+                if (ctb_tile[(size_t)nrs] != cur_tile || (p.wpp && nrs % wctb == 0)) {
+                    E.terminate(1);   // end_of_subset_one_bit; the flush ends in alignment_bit_equal_to_one
+                    if ((cfg.ref_quirks & HEVCGEN_QUIRK_TILES_PCM) && p.tiles() > 1 && d.n == 0) d.put(0x80, 8);
+                    d.align_zero();
+                }
+            }
+        }
+    }
+
+    // Every slice segment NAL unit of the picture into out.
+    void code_picture(int poc, GopState& gop, std::vector<uint8_t>& out) {
+        const bool idr = slice_type == 2;
+        const int nal_type = idr ? 19 : 1;   // IDR_W_RADL or TRAIL_R
+        InterPic ip;
+        if (!idr) ip = draw_inter(poc, gop);
+        const std::vector<Segment> segs = draw_segments();
+        int slice_addr = 0;
+        for (const Segment& sg : segs) {
+            if (!sg.dependent || (cfg.ref_quirks & HEVCGEN_QUIRK_DEPENDENT)) slice_addr = ts_to_rs[(size_t)sg.start];
+            for (int ts = sg.start; ts < sg.end; ts++) ctb_slice[(size_t)ts_to_rs[(size_t)ts]] = slice_addr;
+        }
+        for (const Segment& sg : segs) {
+            Bits h;
+            segment_header(h, sg, poc, ip);
+            Bits d;
+            std::vector<size_t> starts;
+            segment_data(d, sg, starts);
+            const bool entry = p.tiles() > 1 || p.wpp;
+            std::vector<uint32_t> sizes;   // substream sizes in NAL bytes (emulation prevention included)
+            for (size_t k = 0; k + 1 < starts.size(); k++) sizes.push_back((uint32_t)(starts[k + 1] - starts[k]));
+            const bool quirk_dep = sg.dependent && (cfg.ref_quirks & HEVCGEN_QUIRK_DEPENDENT);
+            for (int iter = 0;; iter++) {
+                Bits hh = h;
+                if (quirk_dep) {
+                    if (hh.n) hh.trailing();
+                    std::vector<uint8_t> rbsp = hh.buf;
+                    rbsp.insert(rbsp.end(), d.buf.begin(), d.buf.end());
+                    nal(out, nal_type, rbsp);
+                    break;
+                }
+                if (entry) {
+                    hh.ue((uint32_t)sizes.size());   // num_entry_point_offsets
+                    if (!sizes.empty()) {
+                        uint32_t mx = 1;
+                        for (uint32_t v : sizes) mx = std::max(mx, v);
+                        int len = 1;
+                        while (len < 32 && ((mx - 1) >> len) != 0) len++;
+                        hh.ue((uint32_t)(len - 1));  // offset_len_minus1
+                        for (uint32_t v : sizes) hh.put(v - 1, len);   // entry_point_offset_minus1
+                    }
+                }
+                hh.trailing();   // byte_alignment()
+                std::vector<uint8_t> rbsp = hh.buf;
+                const size_t hsize = rbsp.size();
+                rbsp.insert(rbsp.end(), d.buf.begin(), d.buf.end());
+                const std::vector<size_t> pos = nal_positions(rbsp);
+                std::vector<uint32_t> got;
+                for (size_t k = 0; k + 1 < starts.size(); k++)
+                    got.push_back((uint32_t)(pos[hsize + starts[k + 1]] - pos[hsize + starts[k]]));
+                if (got == sizes || iter == 8) {
+                    nal(out, nal_type, rbsp);
+                    break;
+                }
+                sizes = got;
+            }
+        }
         if (idr) gop.refs.clear();
         gop.refs.insert(gop.refs.begin(), poc);
         if ((int)gop.refs.size() > cfg.max_refs) gop.refs.resize((size_t)cfg.max_refs);
-        C.init(init_type, qp);
-        E.start(&b);
-        const int nctb = wctb * hctb;
-        for (int a = 0; a < nctb; a++) {
-            const int rx = a % wctb, ry = a / wctb;
-            if (p.sao) sao(rx, ry);
-            coding_quadtree(rx << p.log2_ctb, ry << p.log2_ctb, p.log2_ctb, 0);
-            E.terminate(a == nctb - 1);   // end_of_slice_segment_flag
-        }
-        b.align_zero();
-        return b.buf;
     }
 
     void sao(int rx, int ry);   // below
@@ -946,6 +1351,32 @@ void Picture::residual(int x0, int y0, int log2, int c, int mode) {
         const auto xy = at(i);
         if (i == last || u01() < cfg.p_sig) lv[xy.second * n + xy.first] = draw_level();
     }
+    // sign data hiding (7.3.8.11, 7.4.9.11): in a sub-block whose first and last nonzero
+    // scan positions are more than 3 apart, the sign of the first is not coded but is the
+    // parity of the sub-block's sum of magnitudes (odd: negative); the drawn sign obeys it
+    const bool sdh = p.sdh && !cu_bypass;
+    if (sdh)
+        for (int i = 0; i <= (last >> 4); i++) {
+            int lo = -1, hi = -1, sum = 0;
+            for (int q = 0; q < 16 && 16 * i + q <= last; q++) {
+                const auto xy = at(16 * i + q);
+                const int v = lv[xy.second * n + xy.first];
+                if (!v) continue;
+                if (lo < 0) lo = q;
+                hi = q;
+                sum += std::abs(v);
+            }
+            if (lo < 0 || hi - lo <= 3) continue;
+            const auto xy = at(16 * i + lo);
+            int16_t& v = lv[xy.second * n + xy.first];
+            v = (int16_t)((sum & 1) ? -std::abs(v) : std::abs(v));
+        }
+    // transform_skip_flag: first syntax element of a 4x4 block's residual_coding()
+    if (p.tskip && !cu_bypass && log2 == 2) {
+        const bool ts = u01() < cfg.p_tskip;
+        E.decision(C.tskip[c ? 1 : 0], ts);
+        if (ts) tus.back().flags |= HEVC_TU_TSKIP;
+    }
     // last_sig_coeff_x/y (swapped for the vertical scan) and their contexts (9.3.4.2.3)
     const auto lxy = at(last);
     const int lx = scan_idx == 2 ? lxy.second : lxy.first, ly = scan_idx == 2 ? lxy.first : lxy.second;
@@ -979,7 +1410,11 @@ void Picture::residual(int x0, int y0, int log2, int c, int mode) {
         }
         const bool coded = i == last_sb || i == 0 || csbf[(size_t)ys * nsb + xs];
         std::vector<int> sig;   // levels of the significant positions, in coding order
-        if (i == last_sb) sig.push_back(lv[lxy.second * n + lxy.first]);
+        int lo_q = -1, hi_q = -1;   // firstSigScanPos, lastSigScanPos in the sub-block
+        if (i == last_sb) {
+            sig.push_back(lv[lxy.second * n + lxy.first]);
+            lo_q = hi_q = last & 15;
+        }
         const int prev_csbf = right + 2 * below;
         for (int q = (i == last_sb) ? (last & 15) - 1 : 15; q >= 0 && coded; q--) {
             const int xc = (xs << 2) + pos_scan[(size_t)q].first, yc = (ys << 2) + pos_scan[(size_t)q].second;
@@ -1004,9 +1439,14 @@ void Picture::residual(int x0, int y0, int log2, int c, int mode) {
                 E.decision(C.sig[c ? 27 + sctx : sctx], v != 0);
                 if (v) infer_dc = false;
             }
-            if (v) sig.push_back(v);
+            if (v) {
+                sig.push_back(v);
+                if (hi_q < 0) hi_q = q;
+                lo_q = q;
+            }
         }
         if (sig.empty()) continue;
+        const bool hidden = sdh && hi_q - lo_q > 3;
         // greater-1 / greater-2 flags (9.3.4.2.6, 9.3.4.2.7), signs, remainders (9.3.3.11)
         int ctx_set = (i > 0 && c == 0) ? 2 : 0;
         if (c1 == 0) ctx_set++;
@@ -1024,7 +1464,8 @@ void Picture::residual(int x0, int y0, int log2, int c, int mode) {
             }
         }
         if (first_c2 >= 0) E.decision(C.greater2[(c ? 4 : 0) + ctx_set], std::abs(sig[(size_t)first_c2]) > 2);
-        for (int k = 0; k < ns; k++) E.bypass(sig[(size_t)k] < 0);
+        for (int k = 0; k < ns; k++)
+            if (!(hidden && k == ns - 1)) E.bypass(sig[(size_t)k] < 0);
         int rice = 0;
         for (int k = 0; k < ns; k++) {
             const int a = std::abs(sig[(size_t)k]);
@@ -1053,19 +1494,23 @@ void Picture::residual(int x0, int y0, int log2, int c, int mode) {
 }
 
 // sao() (7.3.8.3) of one CTB: merges, types, offsets, band positions, edge classes.
+// Merge candidates: the left / above CTB when in the slice (raster address at or after
+// SliceAddrRs) and the tile; components the slice's SAO flags leave off have no syntax.
 void Picture::sao(int rx, int ry) {
+    const int rs = ry * wctb + rx;
     bool merge = false;
-    if (rx > 0) {
+    if (rx > 0 && rs > cur_slice && ctb_tile[(size_t)rs] == ctb_tile[(size_t)rs - 1]) {
         merge = u01() < 0.3;
         E.decision(C.sao_merge, merge);
     }
-    if (!merge && ry > 0) {
+    if (!merge && ry > 0 && rs - wctb >= cur_slice && ctb_tile[(size_t)rs] == ctb_tile[(size_t)(rs - wctb)]) {
         merge = u01() < 0.3;
         E.decision(C.sao_merge, merge);
     }
     if (merge) return;
     int type = 0;
     for (int c = 0; c < 3; c++) {
+        if (c == 0 ? !sao_luma : !sao_chroma) continue;
         if (c < 2) {   // sao_type_idx: TR cMax 2, first bin context-coded
             type = uni(0, 2);
             E.decision(C.sao_type, type != 0);
@@ -1118,6 +1563,9 @@ void hevcgen_default_cfg(hevcgen_cfg_t* cfg, int32_t width, int32_t height, uint
     cfg->max_merge = 0;
     cfg->wp = 0;
     cfg->depth_inter = 1;
+    cfg->slices = 1;
+    cfg->tile_cols = 1;
+    cfg->tile_rows = 1;
 }
 
 hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
@@ -1125,22 +1573,93 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         cfg->log2_ctb < 4 || cfg->log2_ctb > 6 || cfg->max_level < 1 || cfg->qp_min < 0 || cfg->qp_max > 51 ||
         cfg->qp_min > cfg->qp_max || cfg->max_refs < 1 || cfg->max_refs > 4 || cfg->max_mvd < 1 ||
         cfg->max_mvd > 1 << 14 || cfg->max_merge < 0 || cfg->max_merge > 5 || cfg->depth_inter < 0 ||
-        cfg->depth_inter > 2)
+        cfg->depth_inter > 2 || cfg->slices < 1 || cfg->tile_cols < 1 || cfg->tile_rows < 1 || cfg->scaling < 0 ||
+        cfg->scaling > 3 || cfg->qp_delta_depth < 0 ||
+        (cfg->wpp && cfg->dependent_slices && (cfg->ref_quirks & HEVCGEN_QUIRK_DEPENDENT)))
         return nullptr;
     std::mt19937_64 rng(cfg->seed);
+    auto uni = [&](int lo, int hi) { return std::uniform_int_distribution<int>(lo, hi)(rng); };
+    auto coin = [&]() { return uni(0, 1) == 1; };
     Params p{cfg->width, cfg->height, cfg->log2_ctb, cfg->sao ? 1 : 0};
+    const int ctb = 1 << p.log2_ctb;
+    const int wctb = (p.W + ctb - 1) / ctb, hctb = (p.H + ctb - 1) / ctb;
     if (cfg->inter) {
         p.inter = 1;
         p.dpb_minus1 = cfg->max_refs;
         p.amp = cfg->amp ? 1 : 0;
         p.tmvp = cfg->tmvp ? 1 : 0;
         p.wp = cfg->wp ? 1 : 0;
+        p.log2_pml = uni(2, p.log2_ctb);
     }
     p.depth_inter = cfg->depth_inter;
+    if (cfg->qp_delta_depth > 0) {
+        p.qp_delta = 1;
+        p.qp_delta_depth = std::min(cfg->qp_delta_depth - 1, p.log2_ctb - 3);
+    }
+    if (cfg->chroma_qp_offsets) {
+        p.cb_qp_offset = uni(-12, 12);
+        p.cr_qp_offset = uni(-12, 12);
+        p.slice_chroma_offsets = coin() ? 1 : 0;
+    }
+    if (cfg->deblock_ctl) {
+        p.dbk_ctl = 1;
+        p.dbk_override = coin() ? 1 : 0;
+        p.dbk_disabled = uni(0, 3) == 0 ? 1 : 0;
+        p.beta_div2 = uni(-6, 6);
+        p.tc_div2 = uni(-6, 6);
+    }
+    // tiles: as many as Main's minimum tile size (256 x 64 luma samples) allows
+    {
+        const int min_w = (256 + ctb - 1) / ctb, min_h = (64 + ctb - 1) / ctb;
+        const int nc = std::max(1, std::min(cfg->tile_cols, wctb / min_w));
+        const int nr = std::max(1, std::min(cfg->tile_rows, hctb / min_h));
+        p.uniform_tiles = coin() ? 1 : 0;
+        auto bounds = [&](int n, int total, int min_size, std::vector<int>& bd) {
+            bd.assign(1, 0);
+            if (p.uniform_tiles) {
+                for (int i = 1; i <= n; i++) bd.push_back((i * total) / n);
+                return;
+            }
+            int left = total;
+            for (int i = 0; i < n - 1; i++) {
+                const int sz = uni(min_size, left - min_size * (n - 1 - i));
+                bd.push_back(bd.back() + sz);
+                left -= sz;
+            }
+            bd.push_back(total);
+        };
+        bounds(nc, wctb, min_w, p.col_bd);
+        bounds(nr, hctb, min_h, p.row_bd);
+        p.lf_across_tiles = coin() ? 1 : 0;
+    }
+    p.wpp = cfg->wpp && p.tiles() == 1 ? 1 : 0;
+    p.dependent_slices = cfg->dependent_slices ? 1 : 0;
+    p.lf_across_slices = cfg->slices > 1 ? (coin() ? 1 : 0) : 1;
+    p.bypass = cfg->p_bypass > 0 ? 1 : 0;
+    p.tskip = cfg->p_tskip > 0 ? 1 : 0;
+    p.sdh = cfg->sdh ? 1 : 0;
+    if (cfg->p_pcm > 0) {
+        p.pcm = 1;
+        p.pcm_bits_y = uni(1, 8);
+        p.pcm_bits_c = uni(1, 8);
+        p.pcm_log2_min = uni(3, std::min(5, p.log2_ctb));
+        p.pcm_log2_max = uni(p.pcm_log2_min, std::min(5, p.log2_ctb));
+        p.pcm_lf_disabled = coin() ? 1 : 0;
+    }
+    p.scaling = cfg->scaling;
+    // tile scan (6.5.1): CtbAddrTsToRs and the TileId of each raster address
+    std::vector<int> ts_to_rs, ctb_tile((size_t)wctb * hctb);
+    for (size_t j = 0; j + 1 < p.row_bd.size(); j++)
+        for (size_t i = 0; i + 1 < p.col_bd.size(); i++)
+            for (int y = p.row_bd[j]; y < p.row_bd[j + 1]; y++)
+                for (int x = p.col_bd[i]; x < p.col_bd[i + 1]; x++) {
+                    ts_to_rs.push_back(y * wctb + x);
+                    ctb_tile[(size_t)y * wctb + x] = (int)(j * (p.col_bd.size() - 1) + i);
+                }
     std::vector<uint8_t> out;
     nal(out, 32, vps(p));
-    nal(out, 33, sps(p));
-    nal(out, 34, pps(p));
+    nal(out, 33, sps(p, rng));
+    nal(out, 34, pps(p, rng));
     auto* s = static_cast<hevcgen_stream_t*>(std::calloc(1, sizeof(hevcgen_stream_t)));
     s->pictures = cfg->pictures;
     s->num_tus = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
@@ -1153,16 +1672,19 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     GopState gop;
     for (int k = 0; k < cfg->pictures; k++) {
         Picture pic(*cfg, rng, p);
-        pic.qp = std::uniform_int_distribution<int>(cfg->qp_min, cfg->qp_max)(rng);
         const bool idr = k == 0 || !cfg->inter;
         pic.slice_type = idr ? 2 : (std::uniform_real_distribution<double>(0.0, 1.0)(rng) < cfg->p_b ? 0 : 1);
-        pic.wctb = (p.W + (1 << p.log2_ctb) - 1) >> p.log2_ctb;
-        pic.hctb = (p.H + (1 << p.log2_ctb) - 1) >> p.log2_ctb;
+        pic.wctb = wctb;
+        pic.hctb = hctb;
+        pic.ts_to_rs = ts_to_rs;
+        pic.ctb_tile = ctb_tile;
+        pic.ctb_slice.assign((size_t)wctb * hctb, 0);
         pic.depth8.assign((size_t)(p.W / 8) * (p.H / 8), 0);
         pic.skip8.assign((size_t)(p.W / 8) * (p.H / 8), 0);
+        pic.qp8.assign((size_t)(p.W / 8) * (p.H / 8), 0);
         pic.mode4.assign((size_t)(p.W / 4) * (p.H / 4), 1);
         pic.coeffs.reserve((size_t)p.W * p.H * 3 / 2);
-        nal(out, idr ? 19 : 1, pic.slice_data_and_header(idr ? 0 : k, gop));   // IDR_W_RADL or TRAIL_R
+        pic.code_picture(idr ? 0 : k, gop, out);
         s->slice_type[k] = pic.slice_type;
         s->num_pus[k] = (int32_t)pic.pus.size();
         s->pus[k] = static_cast<hevc_pu_t*>(std::malloc(sizeof(hevc_pu_t) * std::max<size_t>(1, pic.pus.size())));

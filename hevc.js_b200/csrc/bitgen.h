@@ -8,7 +8,9 @@
  * and initialisation, arithmetic encoding) into an Annex-B byte stream: VPS, SPS, PPS, then
  * one slice per picture; an IDR picture first, then IDR pictures or low-delay P and B
  * pictures (short-term reference picture sets in the slice headers, reference list sizes,
- * TMVP, weighted prediction tables).  The reference decoder parses these streams
+ * TMVP, weighted prediction tables).  Coding tools on request: cu_qp_delta, chroma QP
+ * offsets, deblocking control, several (and dependent) slice segments, tiles, WPP with
+ * entry points, transquant bypass, transform skip, sign data hiding, PCM, scaling lists.  The reference decoder parses these streams
  * (src/decoding/syntax_elements.cpp, residual_coding.cpp:175, cabac.cpp:38); the records
  * it produces are the ones the generator drew, which tests/test_bitgen.py checks.
  *
@@ -54,7 +56,41 @@ typedef struct hevcgen_cfg {
     int32_t  wp;                 /* weighted_pred_flag and weighted_bipred_flag (tables   */
                                  /* drawn per slice)                                      */
     int32_t  depth_inter;        /* max_transform_hierarchy_depth_inter 0..2              */
+    /* coding tools; 0 leaves a tool off */
+    int32_t  qp_delta_depth;     /* cu_qp_delta_enabled_flag, diff_cu_qp_delta_depth =    */
+                                 /* qp_delta_depth - 1 (at most log2_ctb - 3)             */
+    int32_t  chroma_qp_offsets;  /* PPS and slice Cb / Cr QP offsets drawn                */
+    int32_t  deblock_ctl;        /* PPS deblocking flags and offsets, slice overrides drawn */
+    int32_t  slices;             /* about this many slice segments per picture (more where */
+                                 /* tiles or WPP force boundaries)                        */
+    int32_t  dependent_slices;   /* dependent_slice_segments_enabled_flag; about half the */
+                                 /* segments after the first then continue their slice    */
+    int32_t  tile_cols, tile_rows;   /* tiles, within Main's 256 x 64 minimum tile size   */
+    int32_t  wpp;                /* entropy_coding_sync_enabled_flag (not with tiles)     */
+    double   p_bypass;           /* cu_transquant_bypass_flag                             */
+    double   p_tskip;            /* transform_skip_flag of a 4x4 block                    */
+    int32_t  sdh;                /* sign_data_hiding_enabled_flag                         */
+    double   p_pcm;              /* pcm_flag of a CU of a PCM size (bit depths, sizes and */
+                                 /* pcm_loop_filter_disabled_flag drawn)                  */
+    int32_t  scaling;            /* 1 default scaling lists, 2 lists in the SPS, 3 in the PPS */
+    /* HEVCGEN_QUIRK_* bits: write some tools the way the reference's parser reads them
+     * (where it departs from H.265) instead of the way the standard defines them */
+    int32_t  ref_quirks;
 } hevcgen_cfg_t;
+
+/* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an
+ * alignment bit equal to one although the arithmetic code's flush already ends in it, so it
+ * skips a byte when the flush ends on a byte boundary (coding_tree.cpp:628-632, :1432); it
+ * does not initialise the context variables at the first CTU of a tile (coding_tree.cpp:628)
+ * and does initialise them after PCM samples (coding_tree.cpp:1466); a PCM CU takes the QpY
+ * of the CU before it (coding_tree.cpp:872) rather than qPY_PRED + CuQpDeltaVal. */
+#define HEVCGEN_QUIRK_TILES_PCM  1
+/* Dependent slice segments (not with WPP): the reference takes availability, the SAO merge
+ * candidates and qPY_PREV per slice segment rather than per slice (coding_tree.cpp:189, :68,
+ * :587), and its header parse of a dependent segment stops at slice_segment_address: no
+ * entry points, and byte_alignment() only when the header is not byte aligned
+ * (slice_header.cpp:141, decoder.cpp:243). */
+#define HEVCGEN_QUIRK_DEPENDENT  2
 
 void hevcgen_default_cfg(hevcgen_cfg_t* cfg, int32_t width, int32_t height, uint64_t seed);
 

@@ -20,7 +20,9 @@
 //   picture <n> poc <p>: match (<TUs>, <PUs>) fnv <FNV-1a 64 of the reference's I420 picture>
 //                      | mismatch <samples> | unsupported (<why>)
 // With a second argument the records of every picture the oracle matched are written to that
-// file, with the references as decode indices of earlier pictures:
+// file (with a third argument "--all", those of unsupported pictures too, as long as no
+// picture mismatched: the syntax the reference parsed, for checking a stream's parse), with
+// the references as decode indices of earlier pictures:
 //   "HREC" u32 version (1), then per picture: hevc_pic_params_t (ref_slot entries: decode
 //   index of the referenced picture), i32 counts of TUs, levels, PUs, WP rows and slices,
 //   u8 has_scaling, u8 has_tiles, 2 pad bytes, then the arrays: TUs, levels, PUs, WP rows,
@@ -82,6 +84,7 @@ struct Recording {
     std::map<const Picture*, Picture8> ours;  // the oracle's output for each reference Picture object
     std::map<const Picture*, int> index_of;   // decode index of the picture each Picture object holds
     FILE* dump = nullptr;
+    bool dump_all = false;   // also write the records of unsupported pictures
     // the picture's records, built at apply_deblocking
     hevc_picture_syntax_t syn{};
     std::vector<uint32_t> blk;
@@ -384,7 +387,7 @@ void apply_sao(DecodingContext& ctx) {
             R.mismatched++;
         }
     }
-    if (R.dump && R.mismatched == 0 && why.empty()) {   // the records of a matched picture
+    if (R.dump && R.mismatched == 0 && (why.empty() || R.dump_all)) {   // the records of a matched picture
         hevc_picture_syntax_t s = R.syn;
         for (int l = 0; l < 2; l++)
             for (int i = 0; i < s.params.num_ref[l]; i++)
@@ -421,7 +424,7 @@ void apply_sao(DecodingContext& ctx) {
 
 int main(int argc, char** argv) {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: hevc-record <stream.265>\n");
+        std::fprintf(stderr, "usage: hevc-record <stream.265> [records.hrec [--all]]\n");
         return 2;
     }
     FILE* fp = std::fopen(argv[1], "rb");
@@ -434,6 +437,7 @@ int main(int argc, char** argv) {
     size_t got;
     while ((got = std::fread(buf, 1, sizeof(buf), fp)) > 0) data.insert(data.end(), buf, buf + got);
     std::fclose(fp);
+    if (argc > 3 && std::strcmp(argv[3], "--all") == 0) R.dump_all = true;
     if (argc > 2) {
         R.dump = std::fopen(argv[2], "wb");
         if (!R.dump) {
