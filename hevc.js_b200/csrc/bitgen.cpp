@@ -9,6 +9,7 @@
 #include "bitgen.h"
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -295,7 +296,7 @@ void profile_tier_level(Bits& b) {
 // The stream's parameter sets: what the SPS and PPS enable, drawn once per stream.
 struct Params {
     int W, H, log2_ctb, sao;
-    int inter = 0, dpb_minus1 = 1, amp = 0, tmvp = 0, wp = 0, depth_inter = 1, log2_pml = 2;
+    int inter = 0, dpb_minus1 = 1, num_reorder = 0, amp = 0, tmvp = 0, wp = 0, depth_inter = 1, log2_pml = 2;
     int qp_delta = 0, qp_delta_depth = 0;                       // cu_qp_delta_enabled_flag, diff_cu_qp_delta_depth
     int cb_qp_offset = 0, cr_qp_offset = 0, slice_chroma_offsets = 0;
     int dbk_ctl = 0, dbk_override = 0, dbk_disabled = 0, beta_div2 = 0, tc_div2 = 0;
@@ -350,7 +351,7 @@ std::vector<uint8_t> vps(const Params& p) {
     profile_tier_level(b);
     b.bit(1);              // vps_sub_layer_ordering_info_present_flag
     b.ue((uint32_t)p.dpb_minus1);            // vps_max_dec_pic_buffering_minus1
-    b.ue(0);               // vps_max_num_reorder_pics
+    b.ue((uint32_t)p.num_reorder);           // vps_max_num_reorder_pics
     b.ue(0);               // vps_max_latency_increase_plus1
     b.put(0, 6);           // vps_max_layer_id
     b.ue(0);               // vps_num_layer_sets_minus1
@@ -376,7 +377,7 @@ std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
     b.ue(4);               // log2_max_pic_order_cnt_lsb_minus4
     b.bit(1);              // sps_sub_layer_ordering_info_present_flag
     b.ue((uint32_t)p.dpb_minus1);            // sps_max_dec_pic_buffering_minus1
-    b.ue(0);               // sps_max_num_reorder_pics
+    b.ue((uint32_t)p.num_reorder);           // sps_max_num_reorder_pics
     b.ue(0);               // sps_max_latency_increase_plus1
     b.ue(0);               // log2_min_luma_coding_block_size_minus3: 8x8
     b.ue((uint32_t)(p.log2_ctb - 3));        // log2_diff_max_min_luma_coding_block_size
@@ -478,9 +479,21 @@ namespace {
 
 // ---- one picture ----------------------------------------------------------------------------
 // The reference picture state carried from one picture to the next.
+// One picture of the coded sequence, planned before any is coded: its POC, slice type and
+// decode index, and its short-term RPS (7.4.8): the pictures kept, those before it in output
+// order (closest first) and those after it (closest first), each used by it or not.
+struct PicPlan {
+    int poc = 0, slice_type = 2, decode_idx = 0;
+    std::vector<int> neg, pos;
+    std::vector<int> neg_used, pos_used;
+};
+
+// State carried from one picture to the next: each coded POC's decode index, and the decode
+// index of the last picture whose slice_temporal_mvp_enabled_flag was 0 (7.4.7.1: later
+// pictures take no collocated picture decoded before it).
 struct GopState {
-    std::vector<int> refs;   // POCs the next picture's RPS keeps, most recent first
-    int tmvp_barrier = 0;    // POC of the last picture with slice_temporal_mvp_enabled_flag 0
+    std::vector<int> decode_idx_of_poc;
+    int tmvp_barrier = 0;
 };
 
 struct Picture {
@@ -1046,37 +1059,39 @@ struct Picture {
         return segs;
     }
 
-    // The reference picture set, the reference lists and TMVP of a P/B picture: the same
-    // in every slice of the picture.  used: StCurrBefore (most recent first).
+    // The reference list sizes and TMVP of a P/B picture: the same in every slice of it.
     struct InterPic {
-        std::vector<int> used_flags, used;
         bool tmvp = false, col_l0 = true;
         int col_ref = 0;
     };
-    InterPic draw_inter(int poc, GopState& gop) {
+    // The lists (8.3.4): RefPicList0 repeats StCurrBefore then StCurrAfter, RefPicList1
+    // StCurrAfter then StCurrBefore, up to the active sizes.
+    InterPic draw_inter(const PicPlan& pl, GopState& gop) {
         InterPic ip;
-        const int n = (int)gop.refs.size();
-        int n_used = 0;
-        for (int i = 0; i < n; i++) {
-            const int u = (i == n - 1 && !n_used) || u01() < 0.7;
-            ip.used_flags.push_back(u);
-            n_used += u;
-            if (u) ip.used.push_back(gop.refs[(size_t)i]);
-        }
+        std::vector<int> before, after;
+        for (size_t i = 0; i < pl.neg.size(); i++)
+            if (pl.neg_used[i]) before.push_back(pl.neg[i]);
+        for (size_t i = 0; i < pl.pos.size(); i++)
+            if (pl.pos_used[i]) after.push_back(pl.pos[i]);
+        std::vector<int> src[2] = {before, after};
+        src[0].insert(src[0].end(), after.begin(), after.end());
+        src[1].insert(src[1].end(), before.begin(), before.end());
         const bool override_refs = u01() < 0.7;
         num_ref[0] = override_refs ? uni(1, 4) : 1;
         num_ref[1] = slice_type == 0 ? (override_refs ? uni(1, 4) : 1) : 0;
         ip.tmvp = p.tmvp && u01() < 0.8;
         if (ip.tmvp) {
             ip.col_l0 = slice_type == 1 || u01() < 0.5;
-            const int nl = num_ref[ip.col_l0 ? 0 : 1];
-            std::vector<int> ok;   // entries after the last picture without TMVP (7.4.7.1)
-            for (int i = 0; i < nl; i++)
-                if (ip.used[(size_t)i % ip.used.size()] >= gop.tmvp_barrier) ok.push_back(i);
+            const int l = ip.col_l0 ? 0 : 1, nl = num_ref[l];
+            std::vector<int> ok;   // entries decoded after the last picture without TMVP
+            for (int i = 0; i < nl; i++) {
+                const int poc = src[l][(size_t)i % src[l].size()];
+                if (gop.decode_idx_of_poc[(size_t)poc] >= gop.tmvp_barrier) ok.push_back(i);
+            }
             if (ok.empty()) ip.tmvp = false;
             else ip.col_ref = ok[(size_t)uni(0, (int)ok.size() - 1)];
         }
-        if (!ip.tmvp) gop.tmvp_barrier = poc;
+        if (!ip.tmvp) gop.tmvp_barrier = pl.decode_idx;
         return ip;
     }
 
@@ -1099,11 +1114,19 @@ struct Picture {
         if (!idr) {
             b.put((uint32_t)(poc & 255), 8);   // slice_pic_order_cnt_lsb
             b.bit(0);                          // short_term_ref_pic_set_sps_flag
-            b.ue((uint32_t)ip.used_flags.size());   // num_negative_pics
-            b.ue(0);                                // num_positive_pics
-            for (size_t i = 0; i < ip.used_flags.size(); i++) {
-                b.ue(0);                       // delta_poc_s0_minus1: consecutive earlier pictures
-                b.bit(ip.used_flags[i]);       // used_by_curr_pic_s0_flag
+            b.ue((uint32_t)plan->neg.size());  // num_negative_pics
+            b.ue((uint32_t)plan->pos.size());  // num_positive_pics
+            int prev = poc;
+            for (size_t i = 0; i < plan->neg.size(); i++) {
+                b.ue((uint32_t)(prev - plan->neg[i] - 1));   // delta_poc_s0_minus1
+                b.bit(plan->neg_used[i]);                    // used_by_curr_pic_s0_flag
+                prev = plan->neg[i];
+            }
+            prev = poc;
+            for (size_t i = 0; i < plan->pos.size(); i++) {
+                b.ue((uint32_t)(plan->pos[i] - prev - 1));   // delta_poc_s1_minus1
+                b.bit(plan->pos_used[i]);                    // used_by_curr_pic_s1_flag
+                prev = plan->pos[i];
             }
             if (p.tmvp) b.bit(ip.tmvp ? 1 : 0);   // slice_temporal_mvp_enabled_flag
         }
@@ -1220,11 +1243,15 @@ struct Picture {
     }
 
     // Every slice segment NAL unit of the picture into out.
-    void code_picture(int poc, GopState& gop, std::vector<uint8_t>& out) {
+    const PicPlan* plan = nullptr;
+    void code_picture(const PicPlan& pl, GopState& gop, std::vector<uint8_t>& out) {
+        plan = &pl;
+        const int poc = pl.poc;
+        slice_type = pl.slice_type;
         const bool idr = slice_type == 2;
         const int nal_type = idr ? 19 : 1;   // IDR_W_RADL or TRAIL_R
         InterPic ip;
-        if (!idr) ip = draw_inter(poc, gop);
+        if (!idr) ip = draw_inter(pl, gop);
         const std::vector<Segment> segs = draw_segments();
         int slice_addr = 0;
         for (const Segment& sg : segs) {
@@ -1276,9 +1303,6 @@ struct Picture {
                 sizes = got;
             }
         }
-        if (idr) gop.refs.clear();
-        gop.refs.insert(gop.refs.begin(), poc);
-        if ((int)gop.refs.size() > cfg.max_refs) gop.refs.resize((size_t)cfg.max_refs);
     }
 
     void sao(int rx, int ry);   // below
@@ -1533,6 +1557,105 @@ void Picture::sao(int rx, int ry) {
     }
 }
 
+namespace {
+
+// The coded sequence (pictures in decode order).  Low delay: POC = decode index, each P/B
+// picture's RPS keeps the last max_refs pictures.  Random access (ra_gop = G > 1): after
+// the IDR picture, mini-GOPs of G pictures: the last one first (predicted from earlier
+// pictures), then the ones between by bisection, each predicted from the two pictures
+// around it (and one earlier one when max_refs allows).  A picture's RPS keeps every
+// earlier-decoded picture that it or a later picture uses (8.3.2).
+std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rng) {
+    auto u01 = [&]() { return std::uniform_real_distribution<double>(0.0, 1.0)(rng); };
+    const int n = cfg.pictures;
+    std::vector<PicPlan> plan;
+    std::vector<std::vector<int>> refs;   // POCs each picture uses
+    if (!cfg.inter) {
+        for (int k = 0; k < n; k++) {
+            PicPlan pl;
+            pl.decode_idx = k;
+            plan.push_back(pl);
+            refs.emplace_back();
+        }
+        return plan;
+    }
+    std::vector<int> order{0};
+    const int g = std::max(1, cfg.ra_gop);
+    std::function<void(int, int)> bisect = [&](int lo, int hi) {
+        if (hi - lo < 2) return;
+        const int mid = (lo + hi) / 2;
+        order.push_back(mid);
+        bisect(lo, mid);
+        bisect(mid, hi);
+    };
+    for (int base = 0; base < n - 1; base += g) {
+        const int anchor = std::min(base + g, n - 1);
+        order.push_back(anchor);
+        bisect(base, anchor);
+    }
+    for (size_t j = 0; j < order.size(); j++) {
+        const int poc = order[j];
+        std::vector<int> r;
+        if (j > 0) {
+            if (g == 1) {   // low delay: the last max_refs pictures, at least one used
+                for (int q = poc - 1; q >= 0 && q >= poc - cfg.max_refs; q--)
+                    if (u01() < 0.7 || r.empty()) r.push_back(q);
+            } else {
+                std::vector<int> past, future;   // decoded before: below and above in output order
+                for (size_t i = 0; i < j; i++) (order[i] < poc ? past : future).push_back(order[i]);
+                std::sort(past.begin(), past.end(), std::greater<int>());
+                std::sort(future.begin(), future.end());
+                r.push_back(past[0]);
+                if (!future.empty()) r.push_back(future[0]);
+                if ((int)r.size() < cfg.max_refs && past.size() > 1 && u01() < 0.5) r.push_back(past[1]);
+            }
+        }
+        refs.push_back(r);
+    }
+    for (size_t j = 0; j < order.size(); j++) {
+        PicPlan pl;
+        pl.poc = order[j];
+        pl.decode_idx = (int)j;
+        pl.slice_type = j == 0 ? 2 : (u01() < cfg.p_b ? 0 : 1);
+        if (j > 0) {
+            std::vector<int> keep;   // decoded before j, used by j or by a later picture
+            for (size_t i = 0; i < j; i++) {
+                bool needed = false;
+                for (size_t m = j; m < order.size() && !needed; m++)
+                    needed = std::find(refs[m].begin(), refs[m].end(), order[i]) != refs[m].end();
+                if (needed) keep.push_back(order[i]);
+            }
+            std::sort(keep.begin(), keep.end());
+            for (auto it = keep.rbegin(); it != keep.rend(); ++it)
+                if (*it < pl.poc) pl.neg.push_back(*it);
+            for (int q : keep)
+                if (q > pl.poc) pl.pos.push_back(q);
+            auto used = [&](int q) { return (int)(std::find(refs[j].begin(), refs[j].end(), q) != refs[j].end()); };
+            for (int q : pl.neg) pl.neg_used.push_back(used(q));
+            for (int q : pl.pos) pl.pos_used.push_back(used(q));
+        }
+        plan.push_back(pl);
+    }
+    return plan;
+}
+
+// sps_max_num_reorder_pics: the most pictures that precede one in decode order and follow it
+// in output order; sps_max_dec_pic_buffering_minus1: room for the largest RPS, the pictures
+// waiting for output and the current one.
+void dpb_sizes(const std::vector<PicPlan>& plan, int& num_reorder, int& dpb_minus1) {
+    num_reorder = 0;
+    size_t rps = 0;
+    for (size_t j = 0; j < plan.size(); j++) {
+        int c = 0;
+        for (size_t i = 0; i < j; i++) c += plan[i].poc > plan[j].poc;
+        num_reorder = std::max(num_reorder, c);
+        rps = std::max(rps, plan[j].neg.size() + plan[j].pos.size());
+    }
+    dpb_minus1 = std::min(15, std::max(1, (int)rps + num_reorder));
+}
+
+}  // namespace
+
 extern "C" {
 
 void hevcgen_default_cfg(hevcgen_cfg_t* cfg, int32_t width, int32_t height, uint64_t seed) {
@@ -1592,6 +1715,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         p.log2_pml = uni(2, p.log2_ctb);
     }
     p.depth_inter = cfg->depth_inter;
+    if (cfg->ra_gop > 1 && !cfg->inter) return nullptr;
     if (cfg->qp_delta_depth > 0) {
         p.qp_delta = 1;
         p.qp_delta_depth = std::min(cfg->qp_delta_depth - 1, p.log2_ctb - 3);
@@ -1656,6 +1780,8 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
                     ts_to_rs.push_back(y * wctb + x);
                     ctb_tile[(size_t)y * wctb + x] = (int)(j * (p.col_bd.size() - 1) + i);
                 }
+    const std::vector<PicPlan> plan = plan_sequence(*cfg, rng);
+    if (cfg->inter) dpb_sizes(plan, p.num_reorder, p.dpb_minus1);
     std::vector<uint8_t> out;
     nal(out, 32, vps(p));
     nal(out, 33, sps(p, rng));
@@ -1669,11 +1795,13 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     s->slice_type = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
     s->num_pus = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
     s->pus = static_cast<hevc_pu_t**>(std::calloc((size_t)cfg->pictures, sizeof(hevc_pu_t*)));
+    s->poc = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
     GopState gop;
+    gop.decode_idx_of_poc.assign((size_t)cfg->pictures, 0);
     for (int k = 0; k < cfg->pictures; k++) {
         Picture pic(*cfg, rng, p);
-        const bool idr = k == 0 || !cfg->inter;
-        pic.slice_type = idr ? 2 : (std::uniform_real_distribution<double>(0.0, 1.0)(rng) < cfg->p_b ? 0 : 1);
+        const PicPlan& pl = plan[(size_t)k];
+        gop.decode_idx_of_poc[(size_t)pl.poc] = k;
         pic.wctb = wctb;
         pic.hctb = hctb;
         pic.ts_to_rs = ts_to_rs;
@@ -1684,8 +1812,9 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         pic.qp8.assign((size_t)(p.W / 8) * (p.H / 8), 0);
         pic.mode4.assign((size_t)(p.W / 4) * (p.H / 4), 1);
         pic.coeffs.reserve((size_t)p.W * p.H * 3 / 2);
-        pic.code_picture(idr ? 0 : k, gop, out);
+        pic.code_picture(pl, gop, out);
         s->slice_type[k] = pic.slice_type;
+        s->poc[k] = pl.poc;
         s->num_pus[k] = (int32_t)pic.pus.size();
         s->pus[k] = static_cast<hevc_pu_t*>(std::malloc(sizeof(hevc_pu_t) * std::max<size_t>(1, pic.pus.size())));
         if (!pic.pus.empty())
@@ -1713,6 +1842,7 @@ void hevcgen_stream_free(hevcgen_stream_t* s) {
         std::free(s->pus[k]);
     }
     std::free(s->slice_type);
+    std::free(s->poc);
     std::free(s->num_pus);
     std::free(s->pus);
     std::free(s->num_tus);

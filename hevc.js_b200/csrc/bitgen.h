@@ -3,16 +3,18 @@
  * It draws a legal coding tree per CTU (CU splits, intra 2Nx2N / NxN partitions, intra
  * prediction modes, skipped and inter CUs with their partitions (AMP included), merge
  * indices, inter prediction directions, reference indices, motion vector differences and
- * predictor flags, transform trees, coded blocks and their levels, SAO parameters, slice
- * QPs) and CABAC-encodes it (Rec. ITU-T H.265 clause 9.3: binarisations, context selection
- * and initialisation, arithmetic encoding) into an Annex-B byte stream: VPS, SPS, PPS, then
- * one slice per picture; an IDR picture first, then IDR pictures or low-delay P and B
- * pictures (short-term reference picture sets in the slice headers, reference list sizes,
- * TMVP, weighted prediction tables).  Coding tools on request: cu_qp_delta, chroma QP
- * offsets, deblocking control, several (and dependent) slice segments, tiles, WPP with
- * entry points, transquant bypass, transform skip, sign data hiding, PCM, scaling lists.  The reference decoder parses these streams
- * (src/decoding/syntax_elements.cpp, residual_coding.cpp:175, cabac.cpp:38); the records
- * it produces are the ones the generator drew, which tests/test_bitgen.py checks.
+ * predictor flags, transform trees, coded blocks and their levels, SAO parameters, QPs) and
+ * CABAC-encodes it (Rec. ITU-T H.265 clause 9.3: binarisations, context selection and
+ * initialisation, arithmetic encoding) into an Annex-B byte stream: VPS, SPS, PPS, then the
+ * slice segments of each picture.  An IDR picture comes first, then IDR pictures or P and B
+ * pictures, low delay or random access (hierarchical mini-GOPs, reordered for output), with
+ * short-term reference picture sets in the slice headers, reference list sizes, TMVP and
+ * weighted prediction tables.  Coding tools on request: cu_qp_delta, chroma QP offsets,
+ * deblocking control, several (and dependent) slice segments, tiles, WPP with entry points,
+ * transquant bypass, transform skip, sign data hiding, PCM, scaling lists.  The reference
+ * decoder parses these streams (src/decoding/syntax_elements.cpp, residual_coding.cpp:175,
+ * cabac.cpp:38); the records it produces are the ones the generator drew, which
+ * tests/test_bitgen.py checks.
  *
  * Host code only; no counterpart in the reference (its streams come from x265/ffmpeg). */
 #ifndef HEVC_BITGEN_H
@@ -76,6 +78,9 @@ typedef struct hevcgen_cfg {
     /* HEVCGEN_QUIRK_* bits: write some tools the way the reference's parser reads them
      * (where it departs from H.265) instead of the way the standard defines them */
     int32_t  ref_quirks;
+    int32_t  ra_gop;             /* with inter: 0 or 1 low delay; G > 1 random access, mini-GOPs */
+                                 /* of G pictures coded last-first then by bisection (pictures */
+                                 /* reordered for output)                                 */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an
@@ -109,6 +114,7 @@ typedef struct hevcgen_stream {
     uint64_t* num_coeffs;        /* per picture                                           */
     int16_t** coeffs;            /* per picture                                           */
     int32_t*  slice_type;        /* per picture: 0 B, 1 P, 2 I (slice_type of 7.4.7.1)   */
+    int32_t*  poc;               /* per picture: PicOrderCntVal (output order)            */
     int32_t*  num_pus;           /* per picture                                           */
     hevc_pu_t** pus;             /* per picture                                           */
 } hevcgen_stream_t;

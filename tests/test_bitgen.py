@@ -52,6 +52,12 @@ CONFIGS = {
         w=416, h=240, seed=26, inter=1, pictures=3, slices=5, deblock_ctl=1, scaling=1, qp_delta_depth=1),
     "I 128x64, scaling lists in the PPS, transquant bypass": dict(w=128, h=64, seed=24, pictures=2, scaling=3,
                                                                   p_bypass=0.3, p_tskip=0.3, sdh=1),
+    "B 200x136, random access, mini-GOPs of 8, four references": dict(
+        w=200, h=136, seed=31, inter=1, pictures=11, ra_gop=8, max_refs=4, p_b=1.0, log2_ctb=5),
+    "P/B 208x120, random access, mini-GOPs of 4, weighted prediction": dict(
+        w=208, h=120, seed=32, inter=1, pictures=10, ra_gop=4, wp=1, log2_ctb=4),
+    "P/B 128x64, random access, mini-GOPs of 2, slices, cu_qp_delta": dict(
+        w=128, h=64, seed=33, inter=1, pictures=7, ra_gop=2, slices=3, qp_delta_depth=2),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
     # test_reference_reads_these_tools_its_own_way
     "I 640x256, 2x3 tiles, slices [reference's tile reading]": dict(
@@ -204,6 +210,19 @@ def test_reference_reads_these_tools_its_own_way(tmp_path, name):
     assert _differences(pics, rec) == [], log
 
 
+def test_random_access_streams_are_reordered():
+    """A random-access stream codes each mini-GOP's last picture first and the others by
+    bisection; every POC appears once."""
+    for name, c in CONFIGS.items():
+        if c.get("ra_gop", 0) < 2:
+            continue
+        _, pics = _generate(name)
+        pocs = [g.poc for g in pics]
+        assert sorted(pocs) == list(range(len(pics)))
+        assert pocs != sorted(pocs), name
+        assert pocs[1] == min(c["ra_gop"], len(pics) - 1)
+
+
 def test_inter_streams_hold_every_kind_of_pu():
     """The inter configurations together draw every PU kind the syntax has: skipped and
     merged PUs, AMVP PUs of each direction, every partition shape."""
@@ -241,7 +260,9 @@ def test_dropin_host_code_decodes_generated_streams(name):
     assert len(want) == len(pics)
     dec = D.Decoder(checker)
     assert dec.decode(data) == 0, dec.last_error()
-    assert _md5(dec.frames()) == _md5(want)
+    got = dec.frames()
+    assert _md5(got) == _md5(want)
+    assert [f.poc for f in got] == sorted(g.poc for g in pics)   # output order
 
 
 @pytest.mark.gpu
@@ -255,5 +276,7 @@ def test_gpu_dropin_decodes_generated_streams(name):
     assert ref.decode(data) == 0
     dec = D.Decoder()
     assert dec.decode(data) == 0, dec.last_error()
-    assert _md5(dec.frames()) == _md5(ref.frames())
+    got = dec.frames()
+    assert _md5(got) == _md5(ref.frames())
+    assert [f.poc for f in got] == sorted(g.poc for g in pics)   # output order
     assert dec.gpu_stats()[0] == len(pics)
