@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving (Poisson) measurement")
     ap.add_argument("--no-pb16", action="store_true", help="skip the P/B steady-state measurement")
     ap.add_argument("--serve-seconds", type=float, default=6.0)
+    ap.add_argument("--dropin-generated", action="store_true",
+                    help="only the drop-in on the generated 1080p stream (the bench's child process)")
     return ap.parse_args()
 
 
@@ -688,6 +690,7 @@ def run_ours(args, hb, rank, world, local):
                                                   "sample": f"{n1} pictures spread over the GOP work list on "
                                                             f"one thread ({t1:.1f} s)"}}
         line["dropin"] = run_dropin()
+        line["dropin_generated"] = run_dropin_generated()
     for st in gop_streams:
         st.close()
     if world > 1:
@@ -698,31 +701,24 @@ def run_ours(args, hb, rank, world, local):
 DROPIN_STREAM = "bbb1080_50f.265"
 
 
-def run_dropin(reps=3):
-    """The drop-in decoder on the reference's own 1080p stream (Big Buck Bunny, 50 pictures,
-    I/P/B, scaling lists, SAO): the whole decode through hevc_decoder_decode (src/wasm/
-    hevc_api.h:53) — NAL parsing, parameter sets, DPB logic and CABAC on this host thread,
-    reconstruction on the GPU (libhevcdec_gpu.so) — beside the reference's own build of the
-    same API (oracle/_ref/libhevcdec.so: its parser and its CPU reconstruction) on the same
-    host.  Frames/s of the decode call; both outputs checked against the reference's
-    whole-stream MD5.  The GPU decoder's context is made by an unmeasured decode of a 64x64
-    stream first (as a long-running process has it)."""
+def time_dropin(data, n, want_md5, reps=3):
+    """Frames/s of hevc_decoder_decode (src/wasm/hevc_api.h:53) on one stream: the GPU drop-in
+    (libhevcdec_gpu.so: NAL parsing, parameter sets, DPB logic and CABAC on this host thread,
+    reconstruction on the GPU) beside the reference's own build of the same API
+    (oracle/_ref/libhevcdec.so: its parser and its CPU reconstruction) on the same host; both
+    outputs checked against want_md5, the MD5 of the stream's last n output frames.  The GPU
+    decoder's context is made by an unmeasured decode of a 64x64 stream first (as a
+    long-running process has it)."""
     import hashlib
     from hevc_b200 import decoder as D
     import oracle
-    here = os.path.join(ROOT, "tests", "golden")
-    with open(os.path.join(here, "streams.json")) as f:
-        want = json.load(f)[DROPIN_STREAM]
-    with open(os.path.join(here, "streams", DROPIN_STREAM), "rb") as f:
-        data = f.read()
-    with open(os.path.join(here, "streams", "toy_qp30.265"), "rb") as f:
+    with open(os.path.join(ROOT, "tests", "golden", "streams", "toy_qp30.265"), "rb") as f:
         toy = f.read()
-    n = len(want["frames"])
 
     def md5_of(frames):
         return hashlib.md5(b"".join(fr.yuv_bytes() for fr in frames[-n:])).hexdigest()
 
-    out = {"stream": DROPIN_STREAM, "frames": n, "width": want["width"], "height": want["height"]}
+    out = {}
     ref_lib = os.path.join(oracle.HERE, "_ref", "libhevcdec.so")
     for name, lib, warm in (("gpu", None, True), ("reference", ref_lib, False)):
         if lib is not None and not os.path.exists(lib):
@@ -740,8 +736,8 @@ def run_dropin(reps=3):
             if warm:   # the decode call's own host time: its waits for the GPU back end taken out
                 host.append(times[-1] - (dec.gpu_wait_ns() - w0) / 1e9)
             if rc != 0:
-                raise SystemExit(f"bench: {name} decode of {DROPIN_STREAM} failed: {dec.last_error()}")
-            ok = ok and md5_of(dec.frames()) == want["md5"]
+                raise SystemExit(f"bench: {name} decode failed: {dec.last_error()}")
+            ok = ok and md5_of(dec.frames()) == want_md5
             dec.close()
         t = statistics.median(times)
         out[name] = {"frames_per_s": round(n / t, 2), "ms_per_frame": round(1000 * t / n, 3), "md5_ok": ok}
@@ -756,9 +752,69 @@ def run_dropin(reps=3):
                 f"decoders would parse about {round(cores * n / h)} pictures/s of this stream")
     if "frames_per_s" in out.get("reference", {}):
         out["gpu_over_reference"] = round(out["gpu"]["frames_per_s"] / out["reference"]["frames_per_s"], 2)
+    return out
+
+
+def run_dropin(reps=3):
+    """The drop-in decoder on the reference's own 1080p stream (Big Buck Bunny, 50 pictures,
+    I/P/B, scaling lists, SAO), checked against the reference's whole-stream MD5."""
+    here = os.path.join(ROOT, "tests", "golden")
+    with open(os.path.join(here, "streams.json")) as f:
+        want = json.load(f)[DROPIN_STREAM]
+    with open(os.path.join(here, "streams", DROPIN_STREAM), "rb") as f:
+        data = f.read()
+    n = len(want["frames"])
+    out = {"stream": DROPIN_STREAM, "frames": n, "width": want["width"], "height": want["height"]}
+    out.update(time_dropin(data, n, want["md5"], reps))
     out["note"] = ("the whole decode call, CABAC included: one host thread parses in both (the stream has no "
                    "WPP entry points), the GPU decoder reconstructs each picture while the next is parsed")
     return out
+
+
+# The generated 1080p stream of the drop-in's second measurement: random-access mini-GOPs of
+# 8 (reordered B pictures), cu_qp_delta, deblocking control, SAO, TMVP, AMP; levels and skip
+# rates that give about 60 KB per picture.
+GENERATED_1080P = dict(width=1920, height=1080, seed=4242, inter=1, pictures=32, ra_gop=8, p_b=0.8, max_refs=3,
+                       log2_ctb=6, p_cbf=0.3, p_sig=0.15, max_level=40, qp_min=22, qp_max=37, qp_delta_depth=2,
+                       deblock_ctl=1, p_skip=0.35, p_merge=0.5, p_intra_cu=0.05)
+
+
+def dropin_generated_child(reps=3):
+    """The drop-in on a stream of the random-syntax generator (csrc/bitgen.cpp), in this
+    process: the reference's own decode gives the MD5 both are checked against."""
+    import hashlib
+    from hevc_b200 import bitgen, decoder as D
+    import oracle
+    c = dict(GENERATED_1080P)
+    w, h, seed = c.pop("width"), c.pop("height"), c.pop("seed")
+    data, pics = bitgen.generate(w, h, seed, **c)
+    ref = D.Decoder(os.path.join(oracle.HERE, "_ref", "libhevcdec.so"))
+    if ref.decode(data) != 0:
+        raise SystemExit("bench: the reference cannot decode the generated stream: " + ref.last_error())
+    frames = ref.frames()
+    want = hashlib.md5(b"".join(fr.yuv_bytes() for fr in frames)).hexdigest()
+    ref.close()
+    out = {"stream": "generated (csrc/bitgen.cpp)", "config": GENERATED_1080P, "frames": len(frames),
+           "bytes": len(data), "width": w, "height": h}
+    out.update(time_dropin(data, len(frames), want, reps))
+    out["note"] = ("random-access mini-GOPs of 8 from the seeded generator; both decoders checked against the "
+                   "reference's own decode of the stream; the CABAC parse is the reference's on one host thread")
+    return out
+
+
+def run_dropin_generated(timeout_s=600):
+    """dropin_generated_child in a child process (bench.py --dropin-generated), bounded by a
+    timeout, so that this measurement cannot hold up or end the bench line."""
+    import subprocess
+    try:
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--dropin-generated"], capture_output=True,
+                           text=True, timeout=timeout_s, cwd=ROOT)
+    except subprocess.TimeoutExpired:
+        return {"error": f"timed out after {timeout_s} s"}
+    lines = [ln for ln in r.stdout.strip().split("\n") if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"error": f"exit {r.returncode}: {(r.stderr or r.stdout)[-400:]}"}
+    return json.loads(lines[-1])
 
 
 def run_pb16(args, hb, ctx, stream, rank, world, dev, check, rank_max, barrier):
@@ -935,6 +991,9 @@ def main():
     rank, world, local = dist_env()
     import __graft_entry__ as ge
     hb = ge.load_package()
+    if args.dropin_generated:
+        print(json.dumps(dropin_generated_child()), flush=True)
+        return
     if args.impl == "reference":
         line = run_reference(args, hb, rank, world)
     else:

@@ -58,6 +58,10 @@ CONFIGS = {
         w=208, h=120, seed=32, inter=1, pictures=10, ra_gop=4, wp=1, log2_ctb=4),
     "P/B 128x64, random access, mini-GOPs of 2, slices, cu_qp_delta": dict(
         w=128, h=64, seed=33, inter=1, pictures=7, ra_gop=2, slices=3, qp_delta_depth=2),
+    "P/B 1920x1080, random access, mini-GOPs of 4, cu_qp_delta, deblocking control": dict(
+        w=1920, h=1080, seed=4242, inter=1, pictures=8, ra_gop=4, p_b=0.8, max_refs=3, log2_ctb=6, p_cbf=0.3,
+        p_sig=0.15, max_level=40, qp_min=22, qp_max=37, qp_delta_depth=2, deblock_ctl=1, p_skip=0.35, p_merge=0.5,
+        p_intra_cu=0.05),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
     # test_reference_reads_these_tools_its_own_way
     "I 640x256, 2x3 tiles, slices [reference's tile reading]": dict(
