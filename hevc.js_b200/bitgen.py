@@ -30,7 +30,8 @@ class GenCfg(C.Structure):
                 ("qp_delta_depth", C.c_int32), ("chroma_qp_offsets", C.c_int32), ("deblock_ctl", C.c_int32),
                 ("slices", C.c_int32), ("dependent_slices", C.c_int32), ("tile_cols", C.c_int32), ("tile_rows", C.c_int32), ("wpp", C.c_int32),
                 ("p_bypass", C.c_double), ("p_tskip", C.c_double), ("sdh", C.c_int32), ("p_pcm", C.c_double),
-                ("scaling", C.c_int32), ("ref_quirks", C.c_int32), ("ra_gop", C.c_int32)]
+                ("scaling", C.c_int32), ("ref_quirks", C.c_int32), ("ra_gop", C.c_int32),
+                ("idr_period", C.c_int32), ("crop", C.c_int32), ("p_no_output", C.c_double)]
 
 # ref_quirks bits (csrc/bitgen.h): tools written the way the reference's parser reads them
 QUIRK_TILES_PCM, QUIRK_DEPENDENT = 1, 2
@@ -41,13 +42,14 @@ class GenStream(C.Structure):
                 ("num_tus", C.POINTER(C.c_int32)), ("tus", C.POINTER(C.POINTER(abi.TU))),
                 ("num_coeffs", C.POINTER(C.c_uint64)), ("coeffs", C.POINTER(C.POINTER(C.c_int16))),
                 ("slice_type", C.POINTER(C.c_int32)), ("poc", C.POINTER(C.c_int32)),
+                ("output", C.POINTER(C.c_int32)), ("crop", C.c_int32 * 4),
                 ("num_pus", C.POINTER(C.c_int32)),
                 ("pus", C.POINTER(C.POINTER(abi.PU)))]
 
 # slice_type values (7.4.7.1)
 SLICE_B, SLICE_P, SLICE_I = 0, 1, 2
 
-GenPicture = collections.namedtuple("GenPicture", "tus levels pus slice_type poc")
+GenPicture = collections.namedtuple("GenPicture", "tus levels pus slice_type poc output")
 
 
 _lib = None
@@ -89,7 +91,7 @@ def generate(width, height, seed, **cfg):
             n = int(s.num_coeffs[k])
             levels = np.ctypeslib.as_array(s.coeffs[k], shape=(n,)).copy() if n else np.zeros(0, np.int16)
             pus = [abi.PU.from_buffer_copy(s.pus[k][i]) for i in range(s.num_pus[k])]
-            pics.append(GenPicture(tus, levels, pus, int(s.slice_type[k]), int(s.poc[k])))
+            pics.append(GenPicture(tus, levels, pus, int(s.slice_type[k]), int(s.poc[k]), bool(s.output[k])))
         return data, pics
     finally:
         g.hevcgen_stream_free(sp)

@@ -304,6 +304,8 @@ struct Params {
     int bypass = 0, tskip = 0, sdh = 0;
     int pcm = 0, pcm_bits_y = 8, pcm_bits_c = 8, pcm_log2_min = 3, pcm_log2_max = 3, pcm_lf_disabled = 0;
     int scaling = 0;                                            // 0 off, 1 default lists, 2 SPS lists, 3 PPS lists
+    int crop[4] = {0, 0, 0, 0};                                 // conformance window offsets (chroma units)
+    int output_flag = 0;                                        // output_flag_present_flag
     int wpp = 0;                                                // entropy_coding_sync_enabled_flag
     std::vector<int> col_bd, row_bd;                            // tile boundaries in CTBs (one tile: {0, w})
     int uniform_tiles = 0, lf_across_tiles = 1;
@@ -371,7 +373,9 @@ std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
     b.ue(1);               // chroma_format_idc: 4:2:0
     b.ue((uint32_t)p.W);   // pic_width_in_luma_samples
     b.ue((uint32_t)p.H);   // pic_height_in_luma_samples
-    b.bit(0);              // conformance_window_flag
+    b.bit(p.crop[0] | p.crop[1] | p.crop[2] | p.crop[3] ? 1 : 0);   // conformance_window_flag
+    if (p.crop[0] | p.crop[1] | p.crop[2] | p.crop[3])
+        for (int k = 0; k < 4; k++) b.ue((uint32_t)p.crop[k]);   // conf_win_left/right/top/bottom_offset
     b.ue(0);               // bit_depth_luma_minus8
     b.ue(0);               // bit_depth_chroma_minus8
     b.ue(4);               // log2_max_pic_order_cnt_lsb_minus4
@@ -415,7 +419,7 @@ std::vector<uint8_t> pps(const Params& p, std::mt19937_64& rng) {
     b.ue(0);               // pps_pic_parameter_set_id
     b.ue(0);               // pps_seq_parameter_set_id
     b.bit(p.dependent_slices ? 1 : 0);       // dependent_slice_segments_enabled_flag
-    b.bit(0);              // output_flag_present_flag
+    b.bit(p.output_flag ? 1 : 0);             // output_flag_present_flag
     b.put(0, 3);           // num_extra_slice_header_bits
     b.bit(p.sdh ? 1 : 0);  // sign_data_hiding_enabled_flag
     b.bit(p.inter ? 1 : 0);   // cabac_init_present_flag (cabac_init_flag drawn per slice)
@@ -483,7 +487,8 @@ namespace {
 // decode index, and its short-term RPS (7.4.8): the pictures kept, those before it in output
 // order (closest first) and those after it (closest first), each used by it or not.
 struct PicPlan {
-    int poc = 0, slice_type = 2, decode_idx = 0;
+    int poc = 0, slice_type = 2, decode_idx = 0, nal_type = 19;
+    bool output = true, no_output_of_prior = false;   // pic_output_flag, no_output_of_prior_pics_flag
     std::vector<int> neg, pos;
     std::vector<int> neg_used, pos_used;
 };
@@ -1101,7 +1106,7 @@ struct Picture {
         const bool idr = slice_type == 2;
         const int nctb = wctb * hctb;
         b.bit(sg.start == 0);   // first_slice_segment_in_pic_flag
-        if (idr) b.bit(0);      // no_output_of_prior_pics_flag
+        if (idr) b.bit(plan->no_output_of_prior ? 1 : 0);   // no_output_of_prior_pics_flag
         b.ue(0);                // slice_pic_parameter_set_id
         if (sg.start > 0) {
             if (p.dependent_slices) b.bit(sg.dependent ? 1 : 0);   // dependent_slice_segment_flag
@@ -1111,6 +1116,7 @@ struct Picture {
         }
         if (sg.dependent) return init_type;
         b.ue((uint32_t)slice_type);
+        if (p.output_flag) b.bit(plan->output ? 1 : 0);   // pic_output_flag
         if (!idr) {
             b.put((uint32_t)(poc & 255), 8);   // slice_pic_order_cnt_lsb
             b.bit(0);                          // short_term_ref_pic_set_sps_flag
@@ -1249,9 +1255,10 @@ struct Picture {
         const int poc = pl.poc;
         slice_type = pl.slice_type;
         const bool idr = slice_type == 2;
-        const int nal_type = idr ? 19 : 1;   // IDR_W_RADL or TRAIL_R
+        const int nal_type = pl.nal_type;
         InterPic ip;
         if (!idr) ip = draw_inter(pl, gop);
+        else gop.tmvp_barrier = pl.decode_idx;   // slice_temporal_mvp_enabled_flag is 0 in an IDR picture
         const std::vector<Segment> segs = draw_segments();
         int slice_addr = 0;
         for (const Segment& sg : segs) {
@@ -1559,82 +1566,84 @@ void Picture::sao(int rx, int ry) {
 
 namespace {
 
-// The coded sequence (pictures in decode order).  Low delay: POC = decode index, each P/B
-// picture's RPS keeps the last max_refs pictures.  Random access (ra_gop = G > 1): after
-// the IDR picture, mini-GOPs of G pictures: the last one first (predicted from earlier
-// pictures), then the ones between by bisection, each predicted from the two pictures
-// around it (and one earlier one when max_refs allows).  A picture's RPS keeps every
-// earlier-decoded picture that it or a later picture uses (8.3.2).
+// The coded sequence (pictures in decode order), in IDR periods of idr_period pictures (the
+// whole stream when 0); POCs restart at 0 in each.  Low delay: POC = decode index within the
+// period, each P/B picture using some of the last max_refs pictures.  Random access
+// (ra_gop = G > 1): after the IDR picture, mini-GOPs of G pictures: the last one first
+// (predicted from earlier pictures), then the ones between by bisection, each predicted
+// from the two pictures around it (and one earlier one when max_refs allows).  A picture's
+// RPS keeps every earlier-decoded picture of its period that it or a later picture uses
+// (8.3.2).  An IDR picture after the first draws no_output_of_prior_pics_flag; with
+// p_no_output a picture draws pic_output_flag = 0.
 std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rng) {
     auto u01 = [&]() { return std::uniform_real_distribution<double>(0.0, 1.0)(rng); };
-    const int n = cfg.pictures;
     std::vector<PicPlan> plan;
-    std::vector<std::vector<int>> refs;   // POCs each picture uses
-    if (!cfg.inter) {
-        for (int k = 0; k < n; k++) {
+    const int period = !cfg.inter ? 1 : cfg.idr_period > 0 ? cfg.idr_period : cfg.pictures;
+    for (int first = 0; first < cfg.pictures; first += period) {
+        const int n = std::min(period, cfg.pictures - first);
+        std::vector<int> order{0};
+        std::vector<std::vector<int>> refs;   // POCs each picture uses
+        if (cfg.inter) {
+            const int g = std::max(1, cfg.ra_gop);
+            std::function<void(int, int)> bisect = [&](int lo, int hi) {
+                if (hi - lo < 2) return;
+                const int mid = (lo + hi) / 2;
+                order.push_back(mid);
+                bisect(lo, mid);
+                bisect(mid, hi);
+            };
+            for (int base = 0; base < n - 1; base += g) {
+                const int anchor = std::min(base + g, n - 1);
+                order.push_back(anchor);
+                bisect(base, anchor);
+            }
+        }
+        for (size_t j = 0; j < order.size(); j++) {
+            const int poc = order[j];
+            std::vector<int> r;
+            if (j > 0) {
+                if (cfg.ra_gop < 2) {   // low delay: the last max_refs pictures, at least one used
+                    for (int q = poc - 1; q >= 0 && q >= poc - cfg.max_refs; q--)
+                        if (u01() < 0.7 || r.empty()) r.push_back(q);
+                } else {
+                    std::vector<int> past, future;   // decoded before: below and above in output order
+                    for (size_t i = 0; i < j; i++) (order[i] < poc ? past : future).push_back(order[i]);
+                    std::sort(past.begin(), past.end(), std::greater<int>());
+                    std::sort(future.begin(), future.end());
+                    r.push_back(past[0]);
+                    if (!future.empty()) r.push_back(future[0]);
+                    if ((int)r.size() < cfg.max_refs && past.size() > 1 && u01() < 0.5) r.push_back(past[1]);
+                }
+            }
+            refs.push_back(r);
+        }
+        for (size_t j = 0; j < order.size(); j++) {
             PicPlan pl;
-            pl.decode_idx = k;
+            pl.poc = order[j];
+            pl.decode_idx = (int)plan.size();
+            pl.slice_type = j == 0 ? 2 : (u01() < cfg.p_b ? 0 : 1);
+            pl.output = !(cfg.p_no_output > 0 && u01() < cfg.p_no_output);
+            pl.no_output_of_prior = j == 0 && first > 0 && u01() < 0.3;
+            pl.nal_type = j == 0 ? (u01() < 0.5 ? 19 : 20) : 1;   // IDR_W_RADL / IDR_N_LP, TRAIL_R
+            if (j > 0) {
+                std::vector<int> keep;   // decoded before j, used by j or by a later picture
+                for (size_t i = 0; i < j; i++) {
+                    bool needed = false;
+                    for (size_t m = j; m < order.size() && !needed; m++)
+                        needed = std::find(refs[m].begin(), refs[m].end(), order[i]) != refs[m].end();
+                    if (needed) keep.push_back(order[i]);
+                }
+                std::sort(keep.begin(), keep.end());
+                for (auto it = keep.rbegin(); it != keep.rend(); ++it)
+                    if (*it < pl.poc) pl.neg.push_back(*it);
+                for (int q : keep)
+                    if (q > pl.poc) pl.pos.push_back(q);
+                auto used = [&](int q) { return (int)(std::find(refs[j].begin(), refs[j].end(), q) != refs[j].end()); };
+                for (int q : pl.neg) pl.neg_used.push_back(used(q));
+                for (int q : pl.pos) pl.pos_used.push_back(used(q));
+            }
             plan.push_back(pl);
-            refs.emplace_back();
         }
-        return plan;
-    }
-    std::vector<int> order{0};
-    const int g = std::max(1, cfg.ra_gop);
-    std::function<void(int, int)> bisect = [&](int lo, int hi) {
-        if (hi - lo < 2) return;
-        const int mid = (lo + hi) / 2;
-        order.push_back(mid);
-        bisect(lo, mid);
-        bisect(mid, hi);
-    };
-    for (int base = 0; base < n - 1; base += g) {
-        const int anchor = std::min(base + g, n - 1);
-        order.push_back(anchor);
-        bisect(base, anchor);
-    }
-    for (size_t j = 0; j < order.size(); j++) {
-        const int poc = order[j];
-        std::vector<int> r;
-        if (j > 0) {
-            if (g == 1) {   // low delay: the last max_refs pictures, at least one used
-                for (int q = poc - 1; q >= 0 && q >= poc - cfg.max_refs; q--)
-                    if (u01() < 0.7 || r.empty()) r.push_back(q);
-            } else {
-                std::vector<int> past, future;   // decoded before: below and above in output order
-                for (size_t i = 0; i < j; i++) (order[i] < poc ? past : future).push_back(order[i]);
-                std::sort(past.begin(), past.end(), std::greater<int>());
-                std::sort(future.begin(), future.end());
-                r.push_back(past[0]);
-                if (!future.empty()) r.push_back(future[0]);
-                if ((int)r.size() < cfg.max_refs && past.size() > 1 && u01() < 0.5) r.push_back(past[1]);
-            }
-        }
-        refs.push_back(r);
-    }
-    for (size_t j = 0; j < order.size(); j++) {
-        PicPlan pl;
-        pl.poc = order[j];
-        pl.decode_idx = (int)j;
-        pl.slice_type = j == 0 ? 2 : (u01() < cfg.p_b ? 0 : 1);
-        if (j > 0) {
-            std::vector<int> keep;   // decoded before j, used by j or by a later picture
-            for (size_t i = 0; i < j; i++) {
-                bool needed = false;
-                for (size_t m = j; m < order.size() && !needed; m++)
-                    needed = std::find(refs[m].begin(), refs[m].end(), order[i]) != refs[m].end();
-                if (needed) keep.push_back(order[i]);
-            }
-            std::sort(keep.begin(), keep.end());
-            for (auto it = keep.rbegin(); it != keep.rend(); ++it)
-                if (*it < pl.poc) pl.neg.push_back(*it);
-            for (int q : keep)
-                if (q > pl.poc) pl.pos.push_back(q);
-            auto used = [&](int q) { return (int)(std::find(refs[j].begin(), refs[j].end(), q) != refs[j].end()); };
-            for (int q : pl.neg) pl.neg_used.push_back(used(q));
-            for (int q : pl.pos) pl.pos_used.push_back(used(q));
-        }
-        plan.push_back(pl);
     }
     return plan;
 }
@@ -1644,10 +1653,11 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
 // waiting for output and the current one.
 void dpb_sizes(const std::vector<PicPlan>& plan, int& num_reorder, int& dpb_minus1) {
     num_reorder = 0;
-    size_t rps = 0;
+    size_t rps = 0, start = 0;   // start: the IDR picture of j's period (output order restarts there)
     for (size_t j = 0; j < plan.size(); j++) {
+        if (plan[j].slice_type == 2) start = j;
         int c = 0;
-        for (size_t i = 0; i < j; i++) c += plan[i].poc > plan[j].poc;
+        for (size_t i = start; i < j; i++) c += plan[i].poc > plan[j].poc;
         num_reorder = std::max(num_reorder, c);
         rps = std::max(rps, plan[j].neg.size() + plan[j].pos.size());
     }
@@ -1698,7 +1708,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         cfg->max_mvd > 1 << 14 || cfg->max_merge < 0 || cfg->max_merge > 5 || cfg->depth_inter < 0 ||
         cfg->depth_inter > 2 || cfg->slices < 1 || cfg->tile_cols < 1 || cfg->tile_rows < 1 || cfg->scaling < 0 ||
         cfg->scaling > 3 || cfg->qp_delta_depth < 0 ||
-        (cfg->wpp && cfg->dependent_slices && (cfg->ref_quirks & HEVCGEN_QUIRK_DEPENDENT)))
+        (cfg->wpp && cfg->dependent_slices && (cfg->ref_quirks & HEVCGEN_QUIRK_DEPENDENT)) || cfg->idr_period < 0)
         return nullptr;
     std::mt19937_64 rng(cfg->seed);
     auto uni = [&](int lo, int hi) { return std::uniform_int_distribution<int>(lo, hi)(rng); };
@@ -1771,6 +1781,14 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         p.pcm_lf_disabled = coin() ? 1 : 0;
     }
     p.scaling = cfg->scaling;
+    if (cfg->crop) {   // the window keeps at least 16 x 16 luma samples
+        const int mx = std::min(8, (p.W - 16) / 8), my = std::min(8, (p.H - 16) / 8);
+        p.crop[0] = uni(0, std::max(0, mx));
+        p.crop[1] = uni(0, std::max(0, mx));
+        p.crop[2] = uni(0, std::max(0, my));
+        p.crop[3] = uni(0, std::max(0, my));
+    }
+    p.output_flag = cfg->p_no_output > 0 ? 1 : 0;
     // tile scan (6.5.1): CtbAddrTsToRs and the TileId of each raster address
     std::vector<int> ts_to_rs, ctb_tile((size_t)wctb * hctb);
     for (size_t j = 0; j + 1 < p.row_bd.size(); j++)
@@ -1796,6 +1814,8 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     s->num_pus = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
     s->pus = static_cast<hevc_pu_t**>(std::calloc((size_t)cfg->pictures, sizeof(hevc_pu_t*)));
     s->poc = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
+    s->output = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
+    for (int k = 0; k < 4; k++) s->crop[k] = p.crop[k];
     GopState gop;
     gop.decode_idx_of_poc.assign((size_t)cfg->pictures, 0);
     for (int k = 0; k < cfg->pictures; k++) {
@@ -1815,6 +1835,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         pic.code_picture(pl, gop, out);
         s->slice_type[k] = pic.slice_type;
         s->poc[k] = pl.poc;
+        s->output[k] = pl.output ? 1 : 0;
         s->num_pus[k] = (int32_t)pic.pus.size();
         s->pus[k] = static_cast<hevc_pu_t*>(std::malloc(sizeof(hevc_pu_t) * std::max<size_t>(1, pic.pus.size())));
         if (!pic.pus.empty())
@@ -1843,6 +1864,7 @@ void hevcgen_stream_free(hevcgen_stream_t* s) {
     }
     std::free(s->slice_type);
     std::free(s->poc);
+    std::free(s->output);
     std::free(s->num_pus);
     std::free(s->pus);
     std::free(s->num_tus);

@@ -81,6 +81,10 @@ typedef struct hevcgen_cfg {
     int32_t  ra_gop;             /* with inter: 0 or 1 low delay; G > 1 random access, mini-GOPs */
                                  /* of G pictures coded last-first then by bisection (pictures */
                                  /* reordered for output)                                 */
+    int32_t  idr_period;         /* an IDR picture every idr_period pictures (POCs restart; */
+                                 /* no_output_of_prior_pics_flag drawn); 0: only the first */
+    int32_t  crop;               /* a conformance cropping window drawn                   */
+    double   p_no_output;        /* pic_output_flag = 0 (output_flag_present_flag set)    */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an
@@ -115,6 +119,9 @@ typedef struct hevcgen_stream {
     int16_t** coeffs;            /* per picture                                           */
     int32_t*  slice_type;        /* per picture: 0 B, 1 P, 2 I (slice_type of 7.4.7.1)   */
     int32_t*  poc;               /* per picture: PicOrderCntVal (output order)            */
+    int32_t*  output;            /* per picture: pic_output_flag                          */
+    int32_t   crop[4];           /* conformance window: left, right, top, bottom, in      */
+                                 /* chroma samples (SubWidthC = SubHeightC = 2)           */
     int32_t*  num_pus;           /* per picture                                           */
     hevc_pu_t** pus;             /* per picture                                           */
 } hevcgen_stream_t;

@@ -62,6 +62,9 @@ CONFIGS = {
         w=1920, h=1080, seed=4242, inter=1, pictures=8, ra_gop=4, p_b=0.8, max_refs=3, log2_ctb=6, p_cbf=0.3,
         p_sig=0.15, max_level=40, qp_min=22, qp_max=37, qp_delta_depth=2, deblock_ctl=1, p_skip=0.35, p_merge=0.5,
         p_intra_cu=0.05),
+    "P/B 200x136, an IDR picture every 6, random access, cropping window": dict(
+        w=200, h=136, seed=34, inter=1, pictures=14, ra_gop=4, idr_period=6, crop=1, log2_ctb=5),
+    "I 120x72, cropping window": dict(w=120, h=72, seed=35, pictures=3, crop=1, log2_ctb=4),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
     # test_reference_reads_these_tools_its_own_way
     "I 640x256, 2x3 tiles, slices [reference's tile reading]": dict(
@@ -104,6 +107,17 @@ def _as_parsed(abi, tus):
             t.flags = abi.HEVC_TU_INTRA
         out.append(t)
     return out
+
+
+def _output_order(pics):
+    """POCs in output order: period by period (an IDR picture starts one), each in POC order."""
+    out, period = [], []
+    for g in pics:
+        if g.slice_type == 2 and g.poc == 0 and period:
+            out += sorted(period)
+            period = []
+        period.append(g.poc)
+    return out + sorted(period)
 
 
 def _md5(frames):
@@ -214,6 +228,32 @@ def test_reference_reads_these_tools_its_own_way(tmp_path, name):
     assert _differences(pics, rec) == [], log
 
 
+def test_reference_outputs_pictures_whose_pic_output_flag_is_0():
+    """Another departure, in the output process: pic_output_flag = 0 makes PicOutputFlag 0
+    (8.1.3), so the picture is never output (C.5.2); the reference marks every picture as
+    needed for output (decoder.cpp:298, after :85 had taken the flag).  Reading its code, it
+    does not apply no_output_of_prior_pics_flag either (parsed at slice_header.cpp:124 and not
+    used), which C.5.2.2 applies at an IDR picture."""
+    _needs_reference()
+    from hevc_b200 import bitgen, decoder as D
+    data, pics = bitgen.generate(200, 136, 36, inter=1, pictures=8, ra_gop=4, p_no_output=0.5)
+    assert not all(g.output for g in pics)
+    ref = D.Decoder(REF_LIB)
+    assert ref.decode(data) == 0
+    assert [f.poc for f in ref.frames()] == _output_order(pics)   # every picture, the hidden ones too
+
+
+def test_generated_cropping_windows():
+    """A cropping window is drawn: the reference's frames have the cropped size."""
+    _needs_reference()
+    from hevc_b200 import bitgen, decoder as D
+    data, pics = _generate("I 120x72, cropping window")
+    ref = D.Decoder(REF_LIB)
+    assert ref.decode(data) == 0
+    f = ref.frames()[0]
+    assert (f.width, f.height) != (120, 72) and f.width >= 16 and f.height >= 16
+
+
 def test_random_access_streams_are_reordered():
     """A random-access stream codes each mini-GOP's last picture first and the others by
     bisection; every POC appears once."""
@@ -222,9 +262,10 @@ def test_random_access_streams_are_reordered():
             continue
         _, pics = _generate(name)
         pocs = [g.poc for g in pics]
-        assert sorted(pocs) == list(range(len(pics)))
+        period = c.get("idr_period") or len(pics)
+        assert sorted(pocs[:period]) == list(range(min(period, len(pics))))
         assert pocs != sorted(pocs), name
-        assert pocs[1] == min(c["ra_gop"], len(pics) - 1)
+        assert pocs[1] == min(c["ra_gop"], period - 1)
 
 
 def test_inter_streams_hold_every_kind_of_pu():
@@ -237,7 +278,7 @@ def test_inter_streams_hold_every_kind_of_pu():
             continue
         _, pics = _generate(name)
         assert pics[0].slice_type == bitgen.SLICE_I
-        assert all(p.slice_type in (bitgen.SLICE_P, bitgen.SLICE_B) for p in pics[1:])
+        assert all((p.slice_type == bitgen.SLICE_I) == (p.poc == 0) for p in pics)   # IDR pictures only
         for p in pics:
             for u in p.pus:
                 shapes.add((u.w, u.h))
@@ -266,7 +307,13 @@ def test_dropin_host_code_decodes_generated_streams(name):
     assert dec.decode(data) == 0, dec.last_error()
     got = dec.frames()
     assert _md5(got) == _md5(want)
-    assert [f.poc for f in got] == sorted(g.poc for g in pics)   # output order
+    assert [f.poc for f in got] == [f.poc for f in want] == _output_order(pics)
+    c = CONFIGS[name]
+    crop = (0, 0, 0, 0) if not c.get("crop") else None
+    for f in got:   # the conformance window
+        assert (f.width, f.height) == (want[0].width, want[0].height)
+        if crop is not None:
+            assert (f.width, f.height) == (c["w"], c["h"])
 
 
 @pytest.mark.gpu
@@ -282,5 +329,5 @@ def test_gpu_dropin_decodes_generated_streams(name):
     assert dec.decode(data) == 0, dec.last_error()
     got = dec.frames()
     assert _md5(got) == _md5(ref.frames())
-    assert [f.poc for f in got] == sorted(g.poc for g in pics)   # output order
+    assert [f.poc for f in got] == _output_order(pics)
     assert dec.gpu_stats()[0] == len(pics)
