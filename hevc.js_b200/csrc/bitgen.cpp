@@ -306,6 +306,7 @@ struct Params {
     int scaling = 0;                                            // 0 off, 1 default lists, 2 SPS lists, 3 PPS lists
     int crop[4] = {0, 0, 0, 0};                                 // conformance window offsets (chroma units)
     int output_flag = 0;                                        // output_flag_present_flag
+    int long_term = 0;                                          // long_term_ref_pics_present_flag
     int wpp = 0;                                                // entropy_coding_sync_enabled_flag
     std::vector<int> col_bd, row_bd;                            // tile boundaries in CTBs (one tile: {0, w})
     int uniform_tiles = 0, lf_across_tiles = 1;
@@ -405,7 +406,8 @@ std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
         b.bit(p.pcm_lf_disabled ? 1 : 0);                    // pcm_loop_filter_disabled_flag
     }
     b.ue(0);               // num_short_term_ref_pic_sets
-    b.bit(0);              // long_term_ref_pics_present_flag
+    b.bit(p.long_term ? 1 : 0);              // long_term_ref_pics_present_flag
+    if (p.long_term) b.ue(0);                // num_long_term_ref_pics_sps
     b.bit(p.tmvp ? 1 : 0); // sps_temporal_mvp_enabled_flag
     b.bit(1);              // strong_intra_smoothing_enabled_flag
     b.bit(0);              // vui_parameters_present_flag
@@ -489,8 +491,8 @@ namespace {
 struct PicPlan {
     int poc = 0, slice_type = 2, decode_idx = 0, nal_type = 19;
     bool output = true, no_output_of_prior = false;   // pic_output_flag, no_output_of_prior_pics_flag
-    std::vector<int> neg, pos;
-    std::vector<int> neg_used, pos_used;
+    std::vector<int> neg, pos, lt;   // lt: POCs kept as long-term reference pictures
+    std::vector<int> neg_used, pos_used, lt_used, lt_msb;   // lt_msb: delta_poc_msb_present_flag
 };
 
 // State carried from one picture to the next: each coded POC's decode index, and the decode
@@ -1073,14 +1075,17 @@ struct Picture {
     // StCurrAfter then StCurrBefore, up to the active sizes.
     InterPic draw_inter(const PicPlan& pl, GopState& gop) {
         InterPic ip;
-        std::vector<int> before, after;
+        std::vector<int> before, after, lt;
         for (size_t i = 0; i < pl.neg.size(); i++)
             if (pl.neg_used[i]) before.push_back(pl.neg[i]);
         for (size_t i = 0; i < pl.pos.size(); i++)
             if (pl.pos_used[i]) after.push_back(pl.pos[i]);
+        for (size_t i = 0; i < pl.lt.size(); i++)
+            if (pl.lt_used[i]) lt.push_back(pl.lt[i]);
         std::vector<int> src[2] = {before, after};
         src[0].insert(src[0].end(), after.begin(), after.end());
         src[1].insert(src[1].end(), before.begin(), before.end());
+        for (auto& v : src) v.insert(v.end(), lt.begin(), lt.end());
         const bool override_refs = u01() < 0.7;
         num_ref[0] = override_refs ? uni(1, 4) : 1;
         num_ref[1] = slice_type == 0 ? (override_refs ? uni(1, 4) : 1) : 0;
@@ -1133,6 +1138,15 @@ struct Picture {
                 b.ue((uint32_t)(plan->pos[i] - prev - 1));   // delta_poc_s1_minus1
                 b.bit(plan->pos_used[i]);                    // used_by_curr_pic_s1_flag
                 prev = plan->pos[i];
+            }
+            if (p.long_term) {
+                b.ue((uint32_t)plan->lt.size());             // num_long_term_pics
+                for (size_t i = 0; i < plan->lt.size(); i++) {
+                    b.put((uint32_t)(plan->lt[i] & 255), 8); // poc_lsb_lt
+                    b.bit(plan->lt_used[i]);                 // used_by_curr_pic_lt_flag
+                    b.bit(plan->lt_msb[i]);                  // delta_poc_msb_present_flag
+                    if (plan->lt_msb[i]) b.ue((uint32_t)((poc >> 8) - (plan->lt[i] >> 8)));   // delta_poc_msb_cycle_lt
+                }
             }
             if (p.tmvp) b.bit(ip.tmvp ? 1 : 0);   // slice_temporal_mvp_enabled_flag
         }
@@ -1598,13 +1612,19 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
                 bisect(base, anchor);
             }
         }
+        // long-term (low delay only): from the period's third picture on, its IDR picture
+        // (POC 0) is a long-term reference picture, kept in every RPS, used or not
+        const bool lt_mode = cfg.long_term && cfg.inter && cfg.ra_gop < 2;
+        std::vector<int> lt_used(order.size(), 0);
         for (size_t j = 0; j < order.size(); j++) {
             const int poc = order[j];
             std::vector<int> r;
             if (j > 0) {
                 if (cfg.ra_gop < 2) {   // low delay: the last max_refs pictures, at least one used
-                    for (int q = poc - 1; q >= 0 && q >= poc - cfg.max_refs; q--)
+                    const int lowest = lt_mode && j >= 2 ? 1 : 0;
+                    for (int q = poc - 1; q >= lowest && q >= poc - cfg.max_refs; q--)
                         if (u01() < 0.7 || r.empty()) r.push_back(q);
+                    if (lt_mode && j >= 2) lt_used[j] = u01() < 0.5;
                 } else {
                     std::vector<int> past, future;   // decoded before: below and above in output order
                     for (size_t i = 0; i < j; i++) (order[i] < poc ? past : future).push_back(order[i]);
@@ -1633,6 +1653,14 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
                         needed = std::find(refs[m].begin(), refs[m].end(), order[i]) != refs[m].end();
                     if (needed) keep.push_back(order[i]);
                 }
+                if (lt_mode && j == 1 && std::find(keep.begin(), keep.end(), 0) == keep.end())
+                    keep.push_back(0);   // kept for the pictures that take it as long-term
+                if (lt_mode && j >= 2) {
+                    keep.erase(std::remove(keep.begin(), keep.end(), 0), keep.end());
+                    pl.lt.push_back(0);
+                    pl.lt_used.push_back(lt_used[j]);
+                    pl.lt_msb.push_back(u01() < 0.3);
+                }
                 std::sort(keep.begin(), keep.end());
                 for (auto it = keep.rbegin(); it != keep.rend(); ++it)
                     if (*it < pl.poc) pl.neg.push_back(*it);
@@ -1659,7 +1687,7 @@ void dpb_sizes(const std::vector<PicPlan>& plan, int& num_reorder, int& dpb_minu
         int c = 0;
         for (size_t i = start; i < j; i++) c += plan[i].poc > plan[j].poc;
         num_reorder = std::max(num_reorder, c);
-        rps = std::max(rps, plan[j].neg.size() + plan[j].pos.size());
+        rps = std::max(rps, plan[j].neg.size() + plan[j].pos.size() + plan[j].lt.size());
     }
     dpb_minus1 = std::min(15, std::max(1, (int)rps + num_reorder));
 }
@@ -1789,6 +1817,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         p.crop[3] = uni(0, std::max(0, my));
     }
     p.output_flag = cfg->p_no_output > 0 ? 1 : 0;
+    p.long_term = cfg->long_term ? 1 : 0;
     // tile scan (6.5.1): CtbAddrTsToRs and the TileId of each raster address
     std::vector<int> ts_to_rs, ctb_tile((size_t)wctb * hctb);
     for (size_t j = 0; j + 1 < p.row_bd.size(); j++)

@@ -85,6 +85,9 @@ typedef struct hevcgen_cfg {
                                  /* no_output_of_prior_pics_flag drawn); 0: only the first */
     int32_t  crop;               /* a conformance cropping window drawn                   */
     double   p_no_output;        /* pic_output_flag = 0 (output_flag_present_flag set)    */
+    int32_t  long_term;          /* long_term_ref_pics_present_flag; with low delay, each */
+                                 /* period's IDR picture is a long-term reference from its */
+                                 /* third picture on                                      */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an

@@ -65,6 +65,8 @@ CONFIGS = {
     "P/B 200x136, an IDR picture every 6, random access, cropping window": dict(
         w=200, h=136, seed=34, inter=1, pictures=14, ra_gop=4, idr_period=6, crop=1, log2_ctb=5),
     "I 120x72, cropping window": dict(w=120, h=72, seed=35, pictures=3, crop=1, log2_ctb=4),
+    "P/B 200x136, long-term reference pictures, an IDR picture every 5": dict(
+        w=200, h=136, seed=37, inter=1, pictures=12, long_term=1, idr_period=5, max_refs=2, tmvp=1),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
     # test_reference_reads_these_tools_its_own_way
     "I 640x256, 2x3 tiles, slices [reference's tile reading]": dict(
