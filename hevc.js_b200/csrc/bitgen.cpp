@@ -307,6 +307,9 @@ struct Params {
     int crop[4] = {0, 0, 0, 0};                                 // conformance window offsets (chroma units)
     int output_flag = 0;                                        // output_flag_present_flag
     int long_term = 0;                                          // long_term_ref_pics_present_flag
+    int list_mod = 0;                                           // lists_modification_present_flag
+    int extra = 0;             // AUD, SEI, filler, EOS/EOB NAL units, VUI, slice_reserved_flag, header extensions
+    int extra_bits = 0;                                         // num_extra_slice_header_bits
     int wpp = 0;                                                // entropy_coding_sync_enabled_flag
     std::vector<int> col_bd, row_bd;                            // tile boundaries in CTBs (one tile: {0, w})
     int uniform_tiles = 0, lf_across_tiles = 1;
@@ -364,6 +367,74 @@ std::vector<uint8_t> vps(const Params& p) {
     return b.buf;
 }
 
+// vui_parameters() (E.2.1) with fields drawn; no HRD parameters, progressive frames
+// (field_seq_flag 0, as general_frame_only_constraint_flag requires), motion vectors over
+// picture boundaries allowed.
+void vui_parameters(Bits& b, std::mt19937_64& rng) {
+    auto uni = [&](int lo, int hi) { return std::uniform_int_distribution<int>(lo, hi)(rng); };
+    const bool ar = uni(0, 1);
+    b.bit(ar);                                   // aspect_ratio_info_present_flag
+    if (ar) {
+        const int idc = uni(0, 1) ? 255 : uni(0, 16);
+        b.put((uint32_t)idc, 8);                 // aspect_ratio_idc
+        if (idc == 255) {
+            b.put((uint32_t)uni(1, 65535), 16);  // sar_width
+            b.put((uint32_t)uni(1, 65535), 16);  // sar_height
+        }
+    }
+    const bool ov = uni(0, 1);
+    b.bit(ov);                                   // overscan_info_present_flag
+    if (ov) b.bit(uni(0, 1));                    // overscan_appropriate_flag
+    const bool vs = uni(0, 1);
+    b.bit(vs);                                   // video_signal_type_present_flag
+    if (vs) {
+        b.put((uint32_t)uni(0, 5), 3);           // video_format
+        b.bit(uni(0, 1));                        // video_full_range_flag
+        const bool cd = uni(0, 1);
+        b.bit(cd);                               // colour_description_present_flag
+        if (cd) {
+            b.put((uint32_t)uni(1, 12), 8);      // colour_primaries
+            b.put((uint32_t)uni(1, 18), 8);      // transfer_characteristics
+            b.put((uint32_t)uni(0, 11), 8);      // matrix_coeffs
+        }
+    }
+    const bool cl = uni(0, 1);
+    b.bit(cl);                                   // chroma_loc_info_present_flag
+    if (cl) {
+        b.ue((uint32_t)uni(0, 5));               // chroma_sample_loc_type_top_field
+        b.ue((uint32_t)uni(0, 5));               // chroma_sample_loc_type_bottom_field
+    }
+    b.bit(0);                                    // neutral_chroma_indication_flag
+    b.bit(0);                                    // field_seq_flag
+    b.bit(0);                                    // frame_field_info_present_flag
+    const bool dw = uni(0, 1);
+    b.bit(dw);                                   // default_display_window_flag
+    if (dw)
+        for (int k = 0; k < 4; k++) b.ue((uint32_t)uni(0, 4));   // def_disp_win_*_offset
+    const bool ti = uni(0, 1);
+    b.bit(ti);                                   // vui_timing_info_present_flag
+    if (ti) {
+        b.put(1001, 32);                         // vui_num_units_in_tick
+        b.put(60000, 32);                        // vui_time_scale
+        const bool pp = uni(0, 1);
+        b.bit(pp);                               // vui_poc_proportional_to_timing_flag
+        if (pp) b.ue(0);                         // vui_num_ticks_poc_diff_one_minus1
+        b.bit(0);                                // vui_hrd_parameters_present_flag
+    }
+    const bool br = uni(0, 1);
+    b.bit(br);                                   // bitstream_restriction_flag
+    if (br) {
+        b.bit(0);                                // tiles_fixed_structure_flag
+        b.bit(1);                                // motion_vectors_over_pic_boundaries_flag
+        b.bit(0);                                // restricted_ref_pic_lists_flag
+        b.ue(0);                                 // min_spatial_segmentation_idc
+        b.ue(0);                                 // max_bytes_per_pic_denom
+        b.ue(0);                                 // max_bits_per_min_cu_denom
+        b.ue(15);                                // log2_max_mv_length_horizontal
+        b.ue(15);                                // log2_max_mv_length_vertical
+    }
+}
+
 std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
     Bits b;
     b.put(0, 4);           // sps_video_parameter_set_id
@@ -410,7 +481,8 @@ std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
     if (p.long_term) b.ue(0);                // num_long_term_ref_pics_sps
     b.bit(p.tmvp ? 1 : 0); // sps_temporal_mvp_enabled_flag
     b.bit(1);              // strong_intra_smoothing_enabled_flag
-    b.bit(0);              // vui_parameters_present_flag
+    b.bit(p.extra ? 1 : 0);  // vui_parameters_present_flag
+    if (p.extra) vui_parameters(b, rng);
     b.bit(0);              // sps_extension_present_flag
     b.trailing();
     return b.buf;
@@ -422,7 +494,7 @@ std::vector<uint8_t> pps(const Params& p, std::mt19937_64& rng) {
     b.ue(0);               // pps_seq_parameter_set_id
     b.bit(p.dependent_slices ? 1 : 0);       // dependent_slice_segments_enabled_flag
     b.bit(p.output_flag ? 1 : 0);             // output_flag_present_flag
-    b.put(0, 3);           // num_extra_slice_header_bits
+    b.put((uint32_t)p.extra_bits, 3);        // num_extra_slice_header_bits
     b.bit(p.sdh ? 1 : 0);  // sign_data_hiding_enabled_flag
     b.bit(p.inter ? 1 : 0);   // cabac_init_present_flag (cabac_init_flag drawn per slice)
     b.ue(0);               // num_ref_idx_l0_default_active_minus1
@@ -464,9 +536,9 @@ std::vector<uint8_t> pps(const Params& p, std::mt19937_64& rng) {
     }
     b.bit(p.scaling == 3 ? 1 : 0);           // pps_scaling_list_data_present_flag
     if (p.scaling == 3) scaling_list_data(b, rng);
-    b.bit(0);              // lists_modification_present_flag
+    b.bit(p.list_mod ? 1 : 0);               // lists_modification_present_flag
     b.ue((uint32_t)(p.log2_pml - 2));        // log2_parallel_merge_level_minus2
-    b.bit(0);              // slice_segment_header_extension_present_flag
+    b.bit(p.extra ? 1 : 0);                  // slice_segment_header_extension_present_flag
     b.bit(0);              // pps_extension_present_flag
     b.trailing();
     return b.buf;
@@ -1070,9 +1142,13 @@ struct Picture {
     struct InterPic {
         bool tmvp = false, col_l0 = true;
         int col_ref = 0;
+        int total_curr = 0;                     // NumPicTotalCurr
+        bool mod[2] = {false, false};           // ref_pic_list_modification_flag_lX
+        std::vector<int> entry[2];              // list_entry_lX
     };
-    // The lists (8.3.4): RefPicList0 repeats StCurrBefore then StCurrAfter, RefPicList1
-    // StCurrAfter then StCurrBefore, up to the active sizes.
+    // The lists (8.3.4): RefPicListTemp0 repeats StCurrBefore, StCurrAfter, LtCurr,
+    // RefPicListTemp1 StCurrAfter, StCurrBefore, LtCurr; each list takes its first entries,
+    // or with ref_pic_list_modification_flag_lX the entries list_entry_lX names.
     InterPic draw_inter(const PicPlan& pl, GopState& gop) {
         InterPic ip;
         std::vector<int> before, after, lt;
@@ -1089,13 +1165,22 @@ struct Picture {
         const bool override_refs = u01() < 0.7;
         num_ref[0] = override_refs ? uni(1, 4) : 1;
         num_ref[1] = slice_type == 0 ? (override_refs ? uni(1, 4) : 1) : 0;
+        ip.total_curr = (int)src[0].size();
+        for (int l = 0; l < (slice_type == 0 ? 2 : 1); l++)
+            if (p.list_mod && ip.total_curr > 1 && u01() < 0.6) {
+                ip.mod[l] = true;
+                for (int i = 0; i < num_ref[l]; i++) ip.entry[l].push_back(uni(0, ip.total_curr - 1));
+            }
+        auto list_poc = [&](int l, int i) {
+            return src[l][(size_t)(ip.mod[l] ? ip.entry[l][(size_t)i] : i % ip.total_curr)];
+        };
         ip.tmvp = p.tmvp && u01() < 0.8;
         if (ip.tmvp) {
             ip.col_l0 = slice_type == 1 || u01() < 0.5;
             const int l = ip.col_l0 ? 0 : 1, nl = num_ref[l];
             std::vector<int> ok;   // entries decoded after the last picture without TMVP
             for (int i = 0; i < nl; i++) {
-                const int poc = src[l][(size_t)i % src[l].size()];
+                const int poc = list_poc(l, i);
                 if (gop.decode_idx_of_poc[(size_t)poc] >= gop.tmvp_barrier) ok.push_back(i);
             }
             if (ok.empty()) ip.tmvp = false;
@@ -1120,6 +1205,7 @@ struct Picture {
             b.put((uint32_t)ts_to_rs[(size_t)sg.start], bits);      // slice_segment_address
         }
         if (sg.dependent) return init_type;
+        for (int i = 0; i < p.extra_bits; i++) b.bit(uni(0, 1));   // slice_reserved_flag
         b.ue((uint32_t)slice_type);
         if (p.output_flag) b.bit(plan->output ? 1 : 0);   // pic_output_flag
         if (!idr) {
@@ -1164,6 +1250,15 @@ struct Picture {
             if (override_refs) {
                 b.ue((uint32_t)(num_ref[0] - 1));
                 if (slice_type == 0) b.ue((uint32_t)(num_ref[1] - 1));
+            }
+            if (p.list_mod && ip.total_curr > 1) {   // ref_pic_lists_modification() (7.3.6.2)
+                int bits = 0;
+                while ((1 << bits) < ip.total_curr) bits++;
+                for (int l = 0; l < (slice_type == 0 ? 2 : 1); l++) {
+                    b.bit(ip.mod[l] ? 1 : 0);   // ref_pic_list_modification_flag_lX
+                    if (ip.mod[l])
+                        for (int e : ip.entry[l]) b.put((uint32_t)e, bits);   // list_entry_lX
+                }
             }
             mvd_l1_zero = false;
             if (slice_type == 0) {
@@ -1264,8 +1359,11 @@ struct Picture {
 
     // Every slice segment NAL unit of the picture into out.
     const PicPlan* plan = nullptr;
-    void code_picture(const PicPlan& pl, GopState& gop, std::vector<uint8_t>& out) {
+    void code_picture(const PicPlan& pl, GopState& gop, std::vector<uint8_t>& out, bool aud) {
         plan = &pl;
+        if (p.extra && aud) nal(out, 35, access_unit_delimiter());
+        if (p.extra)
+            for (int i = uni(0, 2); i > 0; i--) nal(out, 39, sei_user_data());   // PREFIX_SEI
         const int poc = pl.poc;
         slice_type = pl.slice_type;
         const bool idr = slice_type == 2;
@@ -1289,6 +1387,9 @@ struct Picture {
             std::vector<uint32_t> sizes;   // substream sizes in NAL bytes (emulation prevention included)
             for (size_t k = 0; k + 1 < starts.size(); k++) sizes.push_back((uint32_t)(starts[k + 1] - starts[k]));
             const bool quirk_dep = sg.dependent && (cfg.ref_quirks & HEVCGEN_QUIRK_DEPENDENT);
+            std::vector<uint8_t> ext;   // slice_segment_header_extension_data_byte
+            if (p.extra)
+                for (int i = uni(0, 3); i > 0; i--) ext.push_back((uint8_t)uni(0, 255));
             for (int iter = 0;; iter++) {
                 Bits hh = h;
                 if (quirk_dep) {
@@ -1309,6 +1410,10 @@ struct Picture {
                         for (uint32_t v : sizes) hh.put(v - 1, len);   // entry_point_offset_minus1
                     }
                 }
+                if (p.extra) {
+                    hh.ue((uint32_t)ext.size());   // slice_segment_header_extension_length
+                    for (uint8_t v : ext) hh.put(v, 8);
+                }
                 hh.trailing();   // byte_alignment()
                 std::vector<uint8_t> rbsp = hh.buf;
                 const size_t hsize = rbsp.size();
@@ -1324,6 +1429,45 @@ struct Picture {
                 sizes = got;
             }
         }
+        if (p.extra) {
+            for (int i = uni(0, 1); i > 0; i--) nal(out, 40, sei_user_data());   // SUFFIX_SEI
+            if (uni(0, 2) == 0) nal(out, 38, filler_data());                     // FD_NUT
+        }
+    }
+
+    // access_unit_delimiter_rbsp() (7.3.2.5): pic_type 2 (I, P and B slices may follow)
+    static std::vector<uint8_t> access_unit_delimiter() {
+        Bits b;
+        b.put(2, 3);
+        b.trailing();
+        return b.buf;
+    }
+
+    // sei_rbsp() (7.3.2.4) with one user_data_unregistered message (D.2.7): payloadType 5,
+    // a 16-byte UUID and some random bytes; a decoder ignores it
+    std::vector<uint8_t> sei_user_data() {
+        Bits b;
+        const int size = 16 + uni(0, 300);
+        b.put(5, 8);   // last_payload_type_byte
+        for (int v = size; ; v -= 255) {   // ff_byte ... last_payload_size_byte
+            if (v >= 255) {
+                b.put(255, 8);
+            } else {
+                b.put((uint32_t)v, 8);
+                break;
+            }
+        }
+        for (int i = 0; i < size; i++) b.put((uint32_t)uni(0, 255), 8);
+        b.trailing();
+        return b.buf;
+    }
+
+    // filler_data_rbsp() (7.3.2.8): 0xFF bytes
+    std::vector<uint8_t> filler_data() {
+        Bits b;
+        for (int i = uni(1, 64); i > 0; i--) b.put(0xFF, 8);
+        b.trailing();
+        return b.buf;
     }
 
     void sao(int rx, int ry);   // below
@@ -1818,6 +1962,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     }
     p.output_flag = cfg->p_no_output > 0 ? 1 : 0;
     p.long_term = cfg->long_term ? 1 : 0;
+    p.list_mod = cfg->list_mod ? 1 : 0;
     // tile scan (6.5.1): CtbAddrTsToRs and the TileId of each raster address
     std::vector<int> ts_to_rs, ctb_tile((size_t)wctb * hctb);
     for (size_t j = 0; j + 1 < p.row_bd.size(); j++)
@@ -1829,7 +1974,10 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
                 }
     const std::vector<PicPlan> plan = plan_sequence(*cfg, rng);
     if (cfg->inter) dpb_sizes(plan, p.num_reorder, p.dpb_minus1);
+    p.extra = cfg->extra_syntax ? 1 : 0;
+    if (p.extra) p.extra_bits = uni(0, 2);
     std::vector<uint8_t> out;
+    if (p.extra) nal(out, 35, Picture::access_unit_delimiter());
     nal(out, 32, vps(p));
     nal(out, 33, sps(p, rng));
     nal(out, 34, pps(p, rng));
@@ -1861,7 +2009,8 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         pic.qp8.assign((size_t)(p.W / 8) * (p.H / 8), 0);
         pic.mode4.assign((size_t)(p.W / 4) * (p.H / 4), 1);
         pic.coeffs.reserve((size_t)p.W * p.H * 3 / 2);
-        pic.code_picture(pl, gop, out);
+        if (p.extra && k > 0 && pl.slice_type == 2 && uni(0, 1)) nal(out, 36, {});   // EOS_NUT before an IDR picture
+        pic.code_picture(pl, gop, out, k > 0);
         s->slice_type[k] = pic.slice_type;
         s->poc[k] = pl.poc;
         s->output[k] = pl.output ? 1 : 0;
@@ -1878,6 +2027,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         if (!pic.coeffs.empty())
             std::memcpy(s->coeffs[k], pic.coeffs.data(), sizeof(int16_t) * pic.coeffs.size());
     }
+    if (p.extra && uni(0, 1)) nal(out, 37, {});   // EOB_NUT
     s->size = out.size();
     s->bytes = static_cast<uint8_t*>(std::malloc(out.size()));
     std::memcpy(s->bytes, out.data(), out.size());

@@ -88,6 +88,11 @@ typedef struct hevcgen_cfg {
     int32_t  long_term;          /* long_term_ref_pics_present_flag; with low delay, each */
                                  /* period's IDR picture is a long-term reference from its */
                                  /* third picture on                                      */
+    int32_t  list_mod;           /* lists_modification_present_flag (list entries drawn)  */
+    int32_t  extra_syntax;       /* syntax a decoder reads past: access unit delimiters,  */
+                                 /* prefix and suffix SEI (user data), filler data, end of */
+                                 /* sequence / bitstream NAL units, VUI, slice_reserved_flag */
+                                 /* bits and slice header extensions                      */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an

@@ -65,6 +65,10 @@ CONFIGS = {
     "P/B 200x136, an IDR picture every 6, random access, cropping window": dict(
         w=200, h=136, seed=34, inter=1, pictures=14, ra_gop=4, idr_period=6, crop=1, log2_ctb=5),
     "I 120x72, cropping window": dict(w=120, h=72, seed=35, pictures=3, crop=1, log2_ctb=4),
+    "P/B 200x136, list modification, long-term, slices, AUD/SEI/filler/EOS/VUI": dict(
+        w=200, h=136, seed=38, inter=1, pictures=8, list_mod=1, long_term=1, slices=3, extra_syntax=1),
+    "P/B 208x120, random access, list modification, an IDR picture every 4, AUD/SEI/VUI": dict(
+        w=208, h=120, seed=39, inter=1, pictures=10, ra_gop=2, idr_period=4, list_mod=1, extra_syntax=1),
     "P/B 200x136, long-term reference pictures, an IDR picture every 5": dict(
         w=200, h=136, seed=37, inter=1, pictures=12, long_term=1, idr_period=5, max_refs=2, tmvp=1),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
