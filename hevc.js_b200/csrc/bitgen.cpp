@@ -293,6 +293,78 @@ void profile_tier_level(Bits& b) {
     b.put(120, 8);         // general_level_idc: 4
 }
 
+// A short-term RPS as deltas to the current POC: before it (closest first) and after it
+// (closest first), each with used_by_curr_pic.
+struct Rps {
+    std::vector<int> d0, d1, u0, u1;
+    bool operator==(const Rps& o) const { return d0 == o.d0 && d1 == o.d1 && u0 == o.u0 && u1 == o.u1; }
+};
+
+// st_ref_pic_set(idx) (7.3.7) of t.  With idx > 0 it is predicted from a set of sets[]
+// (inter_ref_pic_set_prediction_flag) when some deltaRps makes every entry of t a
+// candidate (7.4.8: each entry of the reference set moved by deltaRps, and deltaRps
+// itself); the derivation then lists them in t's order.  In a slice header (idx equal to
+// the number of SPS sets) any SPS set may be the reference, through delta_idx_minus1.
+void st_ref_pic_set(Bits& b, const Rps& t, int idx, const std::vector<Rps>& sets, bool in_slice, std::mt19937_64& rng) {
+    auto uni = [&](int lo, int hi) { return std::uniform_int_distribution<int>(lo, hi)(rng); };
+    if (idx != 0) {
+        bool predicted = false;
+        if (uni(0, 9) < 7) {
+            const int ref = in_slice ? uni(0, idx - 1) : idx - 1;
+            const Rps& r = sets[(size_t)ref];
+            std::vector<int> cand(r.d0);   // j = 0 .. NumDeltaPocs: S0, S1, then deltaRps itself
+            cand.insert(cand.end(), r.d1.begin(), r.d1.end());
+            std::vector<int> deltas;
+            for (int d = -16; d <= 16; d++)
+                if (d) deltas.push_back(d);
+            std::shuffle(deltas.begin(), deltas.end(), rng);
+            for (int drps : deltas) {
+                auto used_of = [&](int v) -> int {   // -1: not in t
+                    for (size_t i = 0; i < t.d0.size(); i++)
+                        if (t.d0[i] == v) return t.u0[i];
+                    for (size_t i = 0; i < t.d1.size(); i++)
+                        if (t.d1[i] == v) return t.u1[i];
+                    return -1;
+                };
+                size_t covered = 0;
+                for (size_t j = 0; j <= cand.size(); j++) {
+                    const int v = j < cand.size() ? cand[j] + drps : drps;
+                    covered += v != 0 && used_of(v) >= 0;
+                }
+                if (covered != t.d0.size() + t.d1.size()) continue;
+                b.bit(1);                                        // inter_ref_pic_set_prediction_flag
+                if (in_slice) b.ue((uint32_t)(idx - 1 - ref));   // delta_idx_minus1
+                b.bit(drps < 0 ? 1 : 0);                         // delta_rps_sign
+                b.ue((uint32_t)(std::abs(drps) - 1));            // abs_delta_rps_minus1
+                for (size_t j = 0; j <= cand.size(); j++) {
+                    const int v = j < cand.size() ? cand[j] + drps : drps;
+                    const int u = v != 0 ? used_of(v) : -1;
+                    b.bit(u == 1 ? 1 : 0);                       // used_by_curr_pic_flag
+                    if (u != 1) b.bit(u == 0 ? 1 : 0);           // use_delta_flag
+                }
+                predicted = true;
+                break;
+            }
+        }
+        if (predicted) return;
+        b.bit(0);                                                // inter_ref_pic_set_prediction_flag
+    }
+    b.ue((uint32_t)t.d0.size());                                 // num_negative_pics
+    b.ue((uint32_t)t.d1.size());                                 // num_positive_pics
+    int prev = 0;
+    for (size_t i = 0; i < t.d0.size(); i++) {
+        b.ue((uint32_t)(prev - t.d0[i] - 1));                    // delta_poc_s0_minus1
+        b.bit(t.u0[i]);                                          // used_by_curr_pic_s0_flag
+        prev = t.d0[i];
+    }
+    prev = 0;
+    for (size_t i = 0; i < t.d1.size(); i++) {
+        b.ue((uint32_t)(t.d1[i] - prev - 1));                    // delta_poc_s1_minus1
+        b.bit(t.u1[i]);                                          // used_by_curr_pic_s1_flag
+        prev = t.d1[i];
+    }
+}
+
 // The stream's parameter sets: what the SPS and PPS enable, drawn once per stream.
 struct Params {
     int W, H, log2_ctb, sao;
@@ -310,6 +382,7 @@ struct Params {
     int list_mod = 0;                                           // lists_modification_present_flag
     int extra = 0;             // AUD, SEI, filler, EOS/EOB NAL units, VUI, slice_reserved_flag, header extensions
     int extra_bits = 0;                                         // num_extra_slice_header_bits
+    std::vector<Rps> rps_sets;                                  // the SPS's st_ref_pic_set()s
     int wpp = 0;                                                // entropy_coding_sync_enabled_flag
     std::vector<int> col_bd, row_bd;                            // tile boundaries in CTBs (one tile: {0, w})
     int uniform_tiles = 0, lf_across_tiles = 1;
@@ -476,7 +549,8 @@ std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
         b.ue((uint32_t)(p.pcm_log2_max - p.pcm_log2_min));   // log2_diff_max_min_pcm_luma_coding_block_size
         b.bit(p.pcm_lf_disabled ? 1 : 0);                    // pcm_loop_filter_disabled_flag
     }
-    b.ue(0);               // num_short_term_ref_pic_sets
+    b.ue((uint32_t)p.rps_sets.size());       // num_short_term_ref_pic_sets
+    for (size_t i = 0; i < p.rps_sets.size(); i++) st_ref_pic_set(b, p.rps_sets[i], (int)i, p.rps_sets, false, rng);
     b.bit(p.long_term ? 1 : 0);              // long_term_ref_pics_present_flag
     if (p.long_term) b.ue(0);                // num_long_term_ref_pics_sps
     b.bit(p.tmvp ? 1 : 0); // sps_temporal_mvp_enabled_flag
@@ -566,6 +640,19 @@ struct PicPlan {
     std::vector<int> neg, pos, lt;   // lt: POCs kept as long-term reference pictures
     std::vector<int> neg_used, pos_used, lt_used, lt_msb;   // lt_msb: delta_poc_msb_present_flag
 };
+
+Rps rps_of(const PicPlan& pl) {
+    Rps r;
+    for (size_t i = 0; i < pl.neg.size(); i++) {
+        r.d0.push_back(pl.neg[i] - pl.poc);
+        r.u0.push_back(pl.neg_used[i]);
+    }
+    for (size_t i = 0; i < pl.pos.size(); i++) {
+        r.d1.push_back(pl.pos[i] - pl.poc);
+        r.u1.push_back(pl.pos_used[i]);
+    }
+    return r;
+}
 
 // State carried from one picture to the next: each coded POC's decode index, and the decode
 // index of the last picture whose slice_temporal_mvp_enabled_flag was 0 (7.4.7.1: later
@@ -1210,20 +1297,19 @@ struct Picture {
         if (p.output_flag) b.bit(plan->output ? 1 : 0);   // pic_output_flag
         if (!idr) {
             b.put((uint32_t)(poc & 255), 8);   // slice_pic_order_cnt_lsb
-            b.bit(0);                          // short_term_ref_pic_set_sps_flag
-            b.ue((uint32_t)plan->neg.size());  // num_negative_pics
-            b.ue((uint32_t)plan->pos.size());  // num_positive_pics
-            int prev = poc;
-            for (size_t i = 0; i < plan->neg.size(); i++) {
-                b.ue((uint32_t)(prev - plan->neg[i] - 1));   // delta_poc_s0_minus1
-                b.bit(plan->neg_used[i]);                    // used_by_curr_pic_s0_flag
-                prev = plan->neg[i];
-            }
-            prev = poc;
-            for (size_t i = 0; i < plan->pos.size(); i++) {
-                b.ue((uint32_t)(plan->pos[i] - prev - 1));   // delta_poc_s1_minus1
-                b.bit(plan->pos_used[i]);                    // used_by_curr_pic_s1_flag
-                prev = plan->pos[i];
+            const Rps t = rps_of(*plan);
+            const int k = (int)p.rps_sets.size();
+            int in_sps = -1;
+            for (int i = 0; i < k && in_sps < 0; i++)
+                if (p.rps_sets[(size_t)i] == t) in_sps = i;
+            if (in_sps >= 0 && u01() < 0.8) {
+                b.bit(1);                      // short_term_ref_pic_set_sps_flag
+                int bits = 0;
+                while ((1 << bits) < k) bits++;
+                if (k > 1) b.put((uint32_t)in_sps, bits);   // short_term_ref_pic_set_idx
+            } else {
+                b.bit(0);                      // short_term_ref_pic_set_sps_flag
+                st_ref_pic_set(b, t, k, p.rps_sets, true, rng);
             }
             if (p.long_term) {
                 b.ue((uint32_t)plan->lt.size());             // num_long_term_pics
@@ -1974,6 +2060,20 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
                 }
     const std::vector<PicPlan> plan = plan_sequence(*cfg, rng);
     if (cfg->inter) dpb_sizes(plan, p.num_reorder, p.dpb_minus1);
+    if (cfg->inter && cfg->sps_rps) {   // the SPS holds the RPSs of most P/B pictures (the more frequent first)
+        std::vector<std::pair<int, Rps>> count;
+        for (const PicPlan& pl : plan) {
+            if (pl.slice_type == 2) continue;
+            const Rps r = rps_of(pl);
+            auto it = std::find_if(count.begin(), count.end(), [&](const std::pair<int, Rps>& c) { return c.second == r; });
+            if (it == count.end()) count.push_back({1, r});
+            else it->first++;
+        }
+        std::stable_sort(count.begin(), count.end(),
+                         [](const std::pair<int, Rps>& a, const std::pair<int, Rps>& b) { return a.first > b.first; });
+        const size_t k = std::min<size_t>(count.size(), (size_t)uni(1, 8));
+        for (size_t i = 0; i < k; i++) p.rps_sets.push_back(count[i].second);
+    }
     p.extra = cfg->extra_syntax ? 1 : 0;
     if (p.extra) p.extra_bits = uni(0, 2);
     std::vector<uint8_t> out;

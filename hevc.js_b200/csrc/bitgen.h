@@ -93,6 +93,8 @@ typedef struct hevcgen_cfg {
                                  /* prefix and suffix SEI (user data), filler data, end of */
                                  /* sequence / bitstream NAL units, VUI, slice_reserved_flag */
                                  /* bits and slice header extensions                      */
+    int32_t  sps_rps;            /* short-term RPSs in the SPS (picked by index in the slice */
+                                 /* headers), some coded by inter RPS prediction          */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an

@@ -69,6 +69,10 @@ CONFIGS = {
         w=200, h=136, seed=38, inter=1, pictures=8, list_mod=1, long_term=1, slices=3, extra_syntax=1),
     "P/B 208x120, random access, list modification, an IDR picture every 4, AUD/SEI/VUI": dict(
         w=208, h=120, seed=39, inter=1, pictures=10, ra_gop=2, idr_period=4, list_mod=1, extra_syntax=1),
+    "B 200x136, random access, mini-GOPs of 8, RPS sets in the SPS (inter RPS prediction)": dict(
+        w=200, h=136, seed=40, inter=1, pictures=17, ra_gop=8, max_refs=3, sps_rps=1, p_b=1.0),
+    "P/B 72x40, low delay, RPS sets in the SPS, long-term": dict(
+        w=72, h=40, seed=41, inter=1, pictures=10, sps_rps=1, long_term=1, max_refs=3),
     "P/B 200x136, long-term reference pictures, an IDR picture every 5": dict(
         w=200, h=136, seed=37, inter=1, pictures=12, long_term=1, idr_period=5, max_refs=2, tmvp=1),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
