@@ -12,6 +12,14 @@ sys.path.insert(0, HERE)
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    config.addinivalue_line("markers", "last: runs after every other test of the session")
+
+
+def pytest_collection_modifyitems(session, config, items):
+    """Tests marked `last` run at the end (in their collected order), so that under -x a
+    failure there stops nothing else."""
+    items[:] = [i for i in items if not i.get_closest_marker("last")] + \
+        [i for i in items if i.get_closest_marker("last")]
 
 
 @pytest.fixture(scope="session")

@@ -327,9 +327,11 @@ def test_dropin_host_code_decodes_generated_streams(name):
 
 
 @pytest.mark.gpu
+@pytest.mark.last
 @pytest.mark.parametrize("name", sorted(CONFIGS))
 def test_gpu_dropin_decodes_generated_streams(name):
-    """libhevcdec_gpu.so on the generated streams: the reference's frames."""
+    """libhevcdec_gpu.so on the generated streams: the reference's frames.  Run last: the
+    widest spread of syntax through the GPU decoder."""
     _needs_reference()
     from hevc_b200 import decoder as D
     data, pics = _generate(name)

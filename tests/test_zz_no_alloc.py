@@ -1,8 +1,9 @@
 """hevcgpu_residual_blocks_static — residual blocks on caller-owned device buffers with
 no allocation inside the call — gives the same bytes as hevcgpu_residual_blocks.
 
-Collected last (file name) so that it runs both after the other GPU tests and, when
-selected alone, in a fresh process where its first call does the per-device set-up."""
+Collected after the other test files (file name) so that it runs both after their GPU tests
+(those marked `last` aside) and, when selected alone, in a fresh process where its first
+call does the per-device set-up."""
 import ctypes as C
 
 import numpy as np
