@@ -1280,10 +1280,12 @@ struct Picture {
     // slice_segment_header() (7.3.6.1) up to (not including) the entry points; draws the
     // slice's values for an independent segment.  Returns the initType.
     int segment_header(Bits& b, const Segment& sg, int poc, const InterPic& ip) {
-        const bool idr = slice_type == 2;
+        const bool idr = plan->nal_type == 19 || plan->nal_type == 20;   // IDR_W_RADL, IDR_N_LP
+        const bool irap = plan->nal_type >= 16 && plan->nal_type <= 23;
+        const bool intra = slice_type == 2;
         const int nctb = wctb * hctb;
         b.bit(sg.start == 0);   // first_slice_segment_in_pic_flag
-        if (idr) b.bit(plan->no_output_of_prior ? 1 : 0);   // no_output_of_prior_pics_flag
+        if (irap) b.bit(plan->no_output_of_prior ? 1 : 0);   // no_output_of_prior_pics_flag
         b.ue(0);                // slice_pic_parameter_set_id
         if (sg.start > 0) {
             if (p.dependent_slices) b.bit(sg.dependent ? 1 : 0);   // dependent_slice_segment_flag
@@ -1330,7 +1332,7 @@ struct Picture {
             b.bit(sao_chroma ? 1 : 0);         // slice_sao_chroma_flag
         }
         init_type = 0;
-        if (!idr) {
+        if (!intra) {
             const bool override_refs = num_ref[0] != 1 || (slice_type == 0 && num_ref[1] != 1) || u01() < 0.3;
             b.bit(override_refs ? 1 : 0);      // num_ref_idx_active_override_flag
             if (override_refs) {
@@ -1452,11 +1454,11 @@ struct Picture {
             for (int i = uni(0, 2); i > 0; i--) nal(out, 39, sei_user_data());   // PREFIX_SEI
         const int poc = pl.poc;
         slice_type = pl.slice_type;
-        const bool idr = slice_type == 2;
+        const bool intra = slice_type == 2;
         const int nal_type = pl.nal_type;
         InterPic ip;
-        if (!idr) ip = draw_inter(pl, gop);
-        else gop.tmvp_barrier = pl.decode_idx;   // slice_temporal_mvp_enabled_flag is 0 in an IDR picture
+        if (!intra) ip = draw_inter(pl, gop);
+        else gop.tmvp_barrier = pl.decode_idx;   // slice_temporal_mvp_enabled_flag 0 (or absent, IDR)
         const std::vector<Segment> segs = draw_segments();
         int slice_addr = 0;
         for (const Segment& sg : segs) {
@@ -1827,6 +1829,10 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
         const int n = std::min(period, cfg.pictures - first);
         std::vector<int> order{0};
         std::vector<std::vector<int>> refs;   // POCs each picture uses
+        // random access with cra: some mini-GOPs end in a CRA picture (intra, POCs go on);
+        // their inner pictures are its leading pictures: RADL from POC radl_from on (they
+        // use only the CRA picture and other RADL pictures), RASL below it
+        std::vector<int> cra, radl_from;
         if (cfg.inter) {
             const int g = std::max(1, cfg.ra_gop);
             std::function<void(int, int)> bisect = [&](int lo, int hi) {
@@ -1839,6 +1845,10 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
             for (int base = 0; base < n - 1; base += g) {
                 const int anchor = std::min(base + g, n - 1);
                 order.push_back(anchor);
+                if (cfg.cra && g > 1 && u01() < 0.5) {   // a CRA picture, its mini-GOP's inner pictures leading
+                    cra.push_back(anchor);
+                    radl_from.push_back(anchor - base >= 2 && u01() < 0.5 ? (base + anchor) / 2 : anchor);
+                }
                 bisect(base, anchor);
             }
         }
@@ -1855,14 +1865,27 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
                     for (int q = poc - 1; q >= lowest && q >= poc - cfg.max_refs; q--)
                         if (u01() < 0.7 || r.empty()) r.push_back(q);
                     if (lt_mode && j >= 2) lt_used[j] = u01() < 0.5;
-                } else {
+                } else if (std::find(cra.begin(), cra.end(), poc) == cra.end()) {
+                    // the IRAP picture this one follows in decode order: its trailing pictures
+                    // use only pictures from it on; its RADL pictures only it and RADL pictures
+                    int floor = 0;
+                    for (size_t i = 0; i < j; i++)
+                        if (std::find(cra.begin(), cra.end(), order[i]) != cra.end()) {
+                            const size_t c = (size_t)(std::find(cra.begin(), cra.end(), order[i]) - cra.begin());
+                            if (poc > order[i]) floor = order[i];
+                            else if (poc >= radl_from[c]) floor = radl_from[c] == poc ? order[i] : radl_from[c];
+                        }
                     std::vector<int> past, future;   // decoded before: below and above in output order
-                    for (size_t i = 0; i < j; i++) (order[i] < poc ? past : future).push_back(order[i]);
+                    for (size_t i = 0; i < j; i++) {
+                        if (order[i] < floor && !(floor > poc)) continue;
+                        (order[i] < poc ? past : future).push_back(order[i]);
+                    }
                     std::sort(past.begin(), past.end(), std::greater<int>());
                     std::sort(future.begin(), future.end());
-                    r.push_back(past[0]);
+                    if (!past.empty() && !(floor > poc)) r.push_back(past[0]);
                     if (!future.empty()) r.push_back(future[0]);
-                    if ((int)r.size() < cfg.max_refs && past.size() > 1 && u01() < 0.5) r.push_back(past[1]);
+                    if (!(floor > poc) && (int)r.size() < cfg.max_refs && past.size() > 1 && u01() < 0.5)
+                        r.push_back(past[1]);
                 }
             }
             refs.push_back(r);
@@ -1871,10 +1894,15 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
             PicPlan pl;
             pl.poc = order[j];
             pl.decode_idx = (int)plan.size();
-            pl.slice_type = j == 0 ? 2 : (u01() < cfg.p_b ? 0 : 1);
+            const bool is_cra = std::find(cra.begin(), cra.end(), pl.poc) != cra.end();
+            pl.slice_type = j == 0 || is_cra ? 2 : (u01() < cfg.p_b ? 0 : 1);
             pl.output = !(cfg.p_no_output > 0 && u01() < cfg.p_no_output);
             pl.no_output_of_prior = j == 0 && first > 0 && u01() < 0.3;
-            pl.nal_type = j == 0 ? (u01() < 0.5 ? 19 : 20) : 1;   // IDR_W_RADL / IDR_N_LP, TRAIL_R
+            pl.nal_type = j == 0 ? (u01() < 0.5 ? 19 : 20) : is_cra ? 21 : 1;   // IDR_W_RADL / IDR_N_LP, CRA_NUT, TRAIL_R
+            for (size_t c = 0; c < cra.size(); c++)   // a leading picture: RASL_R or RADL_R
+                if (j > 0 && pl.poc < cra[c] && pl.poc > cra[c] - std::max(1, cfg.ra_gop) &&
+                    std::find(order.begin(), order.begin() + (long)j, cra[c]) != order.begin() + (long)j)
+                    pl.nal_type = pl.poc >= radl_from[c] ? 7 : 9;
             if (j > 0) {
                 std::vector<int> keep;   // decoded before j, used by j or by a later picture
                 for (size_t i = 0; i < j; i++) {
@@ -1913,7 +1941,7 @@ void dpb_sizes(const std::vector<PicPlan>& plan, int& num_reorder, int& dpb_minu
     num_reorder = 0;
     size_t rps = 0, start = 0;   // start: the IDR picture of j's period (output order restarts there)
     for (size_t j = 0; j < plan.size(); j++) {
-        if (plan[j].slice_type == 2) start = j;
+        if (plan[j].nal_type == 19 || plan[j].nal_type == 20) start = j;
         int c = 0;
         for (size_t i = start; i < j; i++) c += plan[i].poc > plan[j].poc;
         num_reorder = std::max(num_reorder, c);

@@ -95,6 +95,9 @@ typedef struct hevcgen_cfg {
                                  /* bits and slice header extensions                      */
     int32_t  sps_rps;            /* short-term RPSs in the SPS (picked by index in the slice */
                                  /* headers), some coded by inter RPS prediction          */
+    int32_t  cra;                /* random access: some mini-GOPs end in a CRA picture   */
+                                 /* whose inner pictures are its leading pictures (RASL, */
+                                 /* and RADL from the middle one on)                      */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an

@@ -69,6 +69,7 @@ namespace dropin {
 struct Work {
     std::shared_ptr<Picture> pic;
     int slot = -1;
+    int fill_generated = -1;   // a slot to fill with the generated picture before this one
     hevc_picture_syntax_t syn{};
     std::vector<hevc_tu_t> tus;
     std::vector<int16_t> coeffs;
@@ -94,6 +95,7 @@ struct Work {
         unsupported.clear();
         pic.reset();
         slot = -1;
+        fill_generated = -1;
     }
 };
 
@@ -115,8 +117,11 @@ public:
         std::weak_ptr<Picture> pic;
         const Picture* raw = nullptr;
         bool used = false;
+        bool generated = false;   // holds the generated picture of 8.3.3.2, not a decoded one
     };
     std::vector<Slot> slots;
+    int gen_slot = -1;                // the slot with the generated picture, once one was needed
+    std::vector<uint8_t> gen_samples; // its I420 samples (1 << (BitDepth - 1) everywhere)
 
     // ---- worker (deferred mode) ----
     std::mutex q_mu;
@@ -302,7 +307,12 @@ void Backend::worker_loop() {
 // so a slot reused by a later picture is written only after every earlier read of it.
 int Backend::run(Work& w) {
     hevcgpu_job_t* job = nullptr;
-    int rc = hevcgpu_job_prepare(st, &w.syn, &job);
+    int rc = HEVCGPU_OK;
+    if (w.fill_generated >= 0) {   // the generated picture, written before the first picture that reads it
+        gen_samples.assign((size_t)W * H * 3 / 2, 128);
+        rc = hevcgpu_slot_upload(st, w.fill_generated, gen_samples.data());
+    }
+    if (rc == HEVCGPU_OK) rc = hevcgpu_job_prepare(st, &w.syn, &job);
     if (rc == HEVCGPU_OK) rc = hevcgpu_job_launch(job, w.slot);
     Picture& p = *w.pic;
     if (rc == HEVCGPU_OK)
@@ -336,6 +346,7 @@ int Backend::ensure_gpu(const hevc::SPS& sps) {
     if (st) hevcgpu_stream_close(st);
     st = nullptr;
     slots.clear();
+    gen_slot = -1;
     // every picture the DPB may hold as a reference, the current one, and two spare so that
     // the worker can still be writing back a picture whose slot is no longer a reference
     const int tid = (int)sps.sps_max_sub_layers_minus1;
@@ -504,7 +515,7 @@ void Backend::submit(DecodingContext& ctx) {
         raise();
     }
     for (Slot& s : slots) {
-        if (!s.used) continue;
+        if (!s.used || s.generated) continue;
         std::shared_ptr<Picture> p = s.pic.lock();
         if (!p || !p->is_reference()) s = Slot{};
     }
@@ -542,6 +553,7 @@ void Backend::submit(DecodingContext& ctx) {
     // every PU must predict from the picture the final lists name at its index: the
     // records carry one pair of lists per picture, the pair the reference's deblocking
     // reads (deblocking.cpp:183-193)
+    bool reads_missing = false;
     for (size_t k = 0; k < w.pus.size(); k++)
         for (int l = 0; l < 2; l++) {
             const int idx = w.pus[k].ref_idx[l];
@@ -552,11 +564,28 @@ void Backend::submit(DecodingContext& ctx) {
                      ": slices with different reference lists are not supported");
                 raise();
             }
-            if (missing[l][idx]) {
-                fail("picture POC " + std::to_string(ctx.pic->poc) + " predicts from a picture the GPU does not hold");
+            reads_missing = reads_missing || missing[l][idx];
+        }
+    // A list entry with no picture ("no reference picture": a RASL picture of the CRA picture
+    // decoding started at, whose references precede it) is the generated picture of 8.3.3.2,
+    // every sample 1 << (BitDepth - 1), in a slot kept for it.  (The reference predicts from
+    // its uninitialised prediction buffer there, interpolation.cpp:327-331; the standard does
+    // not output such a picture.)
+    if (reads_missing) {
+        if (gen_slot < 0) {
+            for (size_t k = 0; k < slots.size() && gen_slot < 0; k++)
+                if (!slots[k].used && (int)k != dst) gen_slot = (int)k;
+            if (gen_slot < 0) {
+                fail("no free DPB slot for the generated reference picture");
                 raise();
             }
+            slots[(size_t)gen_slot] = Slot{{}, nullptr, true, true};
+            w.fill_generated = gen_slot;
         }
+        for (int l = 0; l < 2; l++)
+            for (int i = 0; i < p.num_ref[l]; i++)
+                if (missing[l][i]) p.ref_slot[l][i] = gen_slot;
+    }
     slots[(size_t)dst] = Slot{self, self.get(), true};
     w.pic = self;
     w.slot = dst;

@@ -99,6 +99,12 @@ int hevcgpu_job_launch(hevcgpu_job_t* job, int32_t dst_slot) {
     return HEVCGPU_OK;
 }
 
+int hevcgpu_slot_upload(hevcgpu_stream_t* st, int32_t slot, const uint8_t* i420) {
+    if (!st || slot < 0 || slot >= (int)st->slots.size() || !i420) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);
+    st->slots[(size_t)slot].assign(i420, i420 + (size_t)st->W * st->H * 3 / 2);
+    return HEVCGPU_OK;
+}
+
 int hevcgpu_slot_download_frame(hevcgpu_stream_t* st, int32_t slot, const hevc_crop_t* crop, uint16_t* y,
                                 int32_t stride_y, uint16_t* cb, uint16_t* cr, int32_t stride_c) {
     if (slot < 0 || slot >= (int)st->slots.size()) return fail(HEVCGPU_EINVAL, "bad slot %d", slot);

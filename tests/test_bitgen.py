@@ -73,6 +73,8 @@ CONFIGS = {
         w=200, h=136, seed=40, inter=1, pictures=17, ra_gop=8, max_refs=3, sps_rps=1, p_b=1.0),
     "P/B 72x40, low delay, RPS sets in the SPS, long-term": dict(
         w=72, h=40, seed=41, inter=1, pictures=10, sps_rps=1, long_term=1, max_refs=3),
+    "P/B 200x136, random access with CRA pictures (RASL and RADL leading pictures)": dict(
+        w=200, h=136, seed=42, inter=1, pictures=17, ra_gop=4, cra=1, tmvp=1),
     "P/B 200x136, long-term reference pictures, an IDR picture every 5": dict(
         w=200, h=136, seed=37, inter=1, pictures=12, long_term=1, idr_period=5, max_refs=2, tmvp=1),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
@@ -264,6 +266,63 @@ def test_generated_cropping_windows():
     assert (f.width, f.height) != (120, 72) and f.width >= 16 and f.height >= 16
 
 
+def _from_a_cra(seed):
+    """A random-access stream with CRA pictures, cut at its first CRA picture (the parameter
+    sets kept), and the POCs of that picture's RASL pictures."""
+    from hevc_b200 import bitgen
+    data, pics = bitgen.generate(200, 136, seed, inter=1, pictures=17, ra_gop=4, cra=1)
+    pos = [k for k in range(len(data) - 3) if data[k:k + 4] == b"\x00\x00\x00\x01"]
+    nals = [data[a:b] for a, b in zip(pos, pos[1:] + [len(data)])]
+    types = [(n[4] >> 1) & 63 for n in nals]
+    vcl = [t for t in types if t < 32]   # one slice per picture: one VCL NAL unit each
+    assert 21 in vcl, "no CRA picture drawn"
+    first, k = vcl.index(21), types.index(21)
+    cut = b"".join([n for n, t in zip(nals, types) if t in (32, 33, 34)] + nals[k:])
+    rasl = {pics[i].poc for i in range(first + 1, len(pics)) if vcl[i] in (8, 9) and pics[i].poc < pics[first].poc}
+    return cut, rasl
+
+
+def _check_from_a_cra(lib, seed):
+    from hevc_b200 import decoder as D
+    cut, rasl = _from_a_cra(seed)
+    assert rasl
+    ref = D.Decoder(REF_LIB)
+    assert ref.decode(cut) == 0
+    want = ref.frames()
+    runs = []
+    for _ in range(2):
+        dec = D.Decoder(lib)
+        assert dec.decode(cut) == 0, dec.last_error()
+        runs.append(dec.frames())
+    got = runs[0]
+    assert [f.poc for f in got] == [f.poc for f in want]
+    for f, g in zip(got, want):
+        if f.poc not in rasl:
+            assert _md5([f]) == _md5([g]), f.poc
+    assert _md5(runs[0]) == _md5(runs[1])   # the RASL pictures too: deterministic
+
+
+@pytest.mark.parametrize("seed", [1, 3])
+def test_decoding_from_a_cra_picture(seed):
+    """Random access at a CRA picture: its RASL pictures have references the decoder never
+    saw.  The drop-in predicts from the generated picture of 8.3.3.2 there (the reference
+    reads an uninitialised buffer, interpolation.cpp:327-331, and the standard outputs no
+    such picture); every other picture is the reference's, in the reference's output order."""
+    _needs_reference()
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    _check_from_a_cra(checker, seed)
+
+
+@pytest.mark.gpu
+@pytest.mark.last
+@pytest.mark.parametrize("seed", [1, 3])
+def test_gpu_decoding_from_a_cra_picture(seed):
+    _needs_reference()
+    _check_from_a_cra(None, seed)
+
+
 def test_random_access_streams_are_reordered():
     """A random-access stream codes each mini-GOP's last picture first and the others by
     bisection; every POC appears once."""
@@ -288,7 +347,8 @@ def test_inter_streams_hold_every_kind_of_pu():
             continue
         _, pics = _generate(name)
         assert pics[0].slice_type == bitgen.SLICE_I
-        assert all((p.slice_type == bitgen.SLICE_I) == (p.poc == 0) for p in pics)   # IDR pictures only
+        if not c.get("cra"):   # I slices in IDR pictures only (CRA pictures are I too)
+            assert all((p.slice_type == bitgen.SLICE_I) == (p.poc == 0) for p in pics)
         for p in pics:
             for u in p.pus:
                 shapes.add((u.w, u.h))
