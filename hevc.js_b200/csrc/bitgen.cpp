@@ -380,6 +380,7 @@ struct Params {
     int output_flag = 0;                                        // output_flag_present_flag
     int long_term = 0;                                          // long_term_ref_pics_present_flag
     int list_mod = 0;                                           // lists_modification_present_flag
+    int poc_bits = 8;                                           // log2_max_pic_order_cnt_lsb
     int extra = 0;             // AUD, SEI, filler, EOS/EOB NAL units, VUI, slice_reserved_flag, header extensions
     int extra_bits = 0;                                         // num_extra_slice_header_bits
     std::vector<Rps> rps_sets;                                  // the SPS's st_ref_pic_set()s
@@ -523,7 +524,7 @@ std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
         for (int k = 0; k < 4; k++) b.ue((uint32_t)p.crop[k]);   // conf_win_left/right/top/bottom_offset
     b.ue(0);               // bit_depth_luma_minus8
     b.ue(0);               // bit_depth_chroma_minus8
-    b.ue(4);               // log2_max_pic_order_cnt_lsb_minus4
+    b.ue((uint32_t)(p.poc_bits - 4));        // log2_max_pic_order_cnt_lsb_minus4
     b.bit(1);              // sps_sub_layer_ordering_info_present_flag
     b.ue((uint32_t)p.dpb_minus1);            // sps_max_dec_pic_buffering_minus1
     b.ue((uint32_t)p.num_reorder);           // sps_max_num_reorder_pics
@@ -1298,7 +1299,8 @@ struct Picture {
         b.ue((uint32_t)slice_type);
         if (p.output_flag) b.bit(plan->output ? 1 : 0);   // pic_output_flag
         if (!idr) {
-            b.put((uint32_t)(poc & 255), 8);   // slice_pic_order_cnt_lsb
+            const uint32_t lsb_mask = (1u << p.poc_bits) - 1u;
+            b.put((uint32_t)poc & lsb_mask, p.poc_bits);   // slice_pic_order_cnt_lsb
             const Rps t = rps_of(*plan);
             const int k = (int)p.rps_sets.size();
             int in_sps = -1;
@@ -1316,10 +1318,13 @@ struct Picture {
             if (p.long_term) {
                 b.ue((uint32_t)plan->lt.size());             // num_long_term_pics
                 for (size_t i = 0; i < plan->lt.size(); i++) {
-                    b.put((uint32_t)(plan->lt[i] & 255), 8); // poc_lsb_lt
+                    // the MSB is sent whenever it differs from the current picture's (low
+                    // delay: then another kept picture may share the LSBs)
+                    const bool msb = plan->lt_msb[i] || (poc >> p.poc_bits) != (plan->lt[i] >> p.poc_bits);
+                    b.put((uint32_t)plan->lt[i] & lsb_mask, p.poc_bits);   // poc_lsb_lt
                     b.bit(plan->lt_used[i]);                 // used_by_curr_pic_lt_flag
-                    b.bit(plan->lt_msb[i]);                  // delta_poc_msb_present_flag
-                    if (plan->lt_msb[i]) b.ue((uint32_t)((poc >> 8) - (plan->lt[i] >> 8)));   // delta_poc_msb_cycle_lt
+                    b.bit(msb ? 1 : 0);                      // delta_poc_msb_present_flag
+                    if (msb) b.ue((uint32_t)((poc >> p.poc_bits) - (plan->lt[i] >> p.poc_bits)));   // delta_poc_msb_cycle_lt
                 }
             }
             if (p.tmvp) b.bit(ip.tmvp ? 1 : 0);   // slice_temporal_mvp_enabled_flag
@@ -2077,6 +2082,11 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     p.output_flag = cfg->p_no_output > 0 ? 1 : 0;
     p.long_term = cfg->long_term ? 1 : 0;
     p.list_mod = cfg->list_mod ? 1 : 0;
+    {   // POC LSBs: at least enough that every step from prevTid0Pic stays below half the range
+        int need = 4;
+        while ((1 << need) <= 2 * std::max(1, cfg->ra_gop) + 2) need++;
+        p.poc_bits = cfg->poc_lsb_bits ? std::max(need, std::min(16, cfg->poc_lsb_bits)) : 8;
+    }
     // tile scan (6.5.1): CtbAddrTsToRs and the TileId of each raster address
     std::vector<int> ts_to_rs, ctb_tile((size_t)wctb * hctb);
     for (size_t j = 0; j + 1 < p.row_bd.size(); j++)

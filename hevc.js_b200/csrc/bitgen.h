@@ -98,6 +98,8 @@ typedef struct hevcgen_cfg {
     int32_t  cra;                /* random access: some mini-GOPs end in a CRA picture   */
                                  /* whose inner pictures are its leading pictures (RASL, */
                                  /* and RADL from the middle one on)                      */
+    int32_t  poc_lsb_bits;       /* log2_max_pic_order_cnt_lsb (0: 8); raised where the   */
+                                 /* GOP needs more; small values make POCs wrap            */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an

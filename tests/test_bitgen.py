@@ -75,6 +75,10 @@ CONFIGS = {
         w=72, h=40, seed=41, inter=1, pictures=10, sps_rps=1, long_term=1, max_refs=3),
     "P/B 200x136, random access with CRA pictures (RASL and RADL leading pictures)": dict(
         w=200, h=136, seed=42, inter=1, pictures=17, ra_gop=4, cra=1, tmvp=1),
+    "P/B 72x40, 40 pictures, POC LSBs of 4 bits (wrapping), long-term": dict(
+        w=72, h=40, seed=43, inter=1, pictures=40, poc_lsb_bits=4, long_term=1, max_refs=3),
+    "P/B 72x40, 40 pictures, random access with CRA pictures, POC LSBs of 4 bits": dict(
+        w=72, h=40, seed=44, inter=1, pictures=40, poc_lsb_bits=4, ra_gop=4, cra=1),
     "P/B 200x136, long-term reference pictures, an IDR picture every 5": dict(
         w=200, h=136, seed=37, inter=1, pictures=12, long_term=1, idr_period=5, max_refs=2, tmvp=1),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
