@@ -1452,9 +1452,11 @@ struct Picture {
 
     // Every slice segment NAL unit of the picture into out.
     const PicPlan* plan = nullptr;
-    void code_picture(const PicPlan& pl, GopState& gop, std::vector<uint8_t>& out, bool aud) {
+    void code_picture(const PicPlan& pl, GopState& gop, std::vector<uint8_t>& out, bool aud,
+                      const std::vector<uint8_t>& param_sets) {
         plan = &pl;
         if (p.extra && aud) nal(out, 35, access_unit_delimiter());
+        out.insert(out.end(), param_sets.begin(), param_sets.end());   // a new SPS and PPS (after the AUD)
         if (p.extra)
             for (int i = uni(0, 2); i > 0; i--) nal(out, 39, sei_user_data());   // PREFIX_SEI
         const int poc = pl.poc;
@@ -2006,7 +2008,57 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     auto coin = [&]() { return uni(0, 1) == 1; };
     Params p{cfg->width, cfg->height, cfg->log2_ctb, cfg->sao ? 1 : 0};
     const int ctb = 1 << p.log2_ctb;
-    const int wctb = (p.W + ctb - 1) / ctb, hctb = (p.H + ctb - 1) / ctb;
+    // what depends on the picture size (it changes at an IDR picture with resize): the
+    // tiles (as many as Main's minimum tile size of 256 x 64 luma samples allows), the
+    // cropping window and the tile scan
+    int wctb = 0, hctb = 0;
+    std::vector<int> ts_to_rs, ctb_tile;
+    auto layout = [&](int W, int H) {
+        p.W = W;
+        p.H = H;
+        wctb = (W + ctb - 1) / ctb;
+        hctb = (H + ctb - 1) / ctb;
+        {
+            const int min_w = (256 + ctb - 1) / ctb, min_h = (64 + ctb - 1) / ctb;
+            const int nc = p.wpp ? 1 : std::max(1, std::min(cfg->tile_cols, wctb / min_w));
+            const int nr = p.wpp ? 1 : std::max(1, std::min(cfg->tile_rows, hctb / min_h));
+            p.uniform_tiles = coin() ? 1 : 0;
+            auto bounds = [&](int n, int total, int min_size, std::vector<int>& bd) {
+                bd.assign(1, 0);
+                if (p.uniform_tiles) {
+                    for (int i = 1; i <= n; i++) bd.push_back((i * total) / n);
+                    return;
+                }
+                int left = total;
+                for (int i = 0; i < n - 1; i++) {
+                    const int sz = uni(min_size, left - min_size * (n - 1 - i));
+                    bd.push_back(bd.back() + sz);
+                    left -= sz;
+                }
+                bd.push_back(total);
+            };
+            bounds(nc, wctb, min_w, p.col_bd);
+            bounds(nr, hctb, min_h, p.row_bd);
+            p.lf_across_tiles = coin() ? 1 : 0;
+        }
+        if (cfg->crop) {   // the window keeps at least 16 x 16 luma samples
+            const int mx = std::min(8, (p.W - 16) / 8), my = std::min(8, (p.H - 16) / 8);
+            p.crop[0] = uni(0, std::max(0, mx));
+            p.crop[1] = uni(0, std::max(0, mx));
+            p.crop[2] = uni(0, std::max(0, my));
+            p.crop[3] = uni(0, std::max(0, my));
+        }
+        // tile scan (6.5.1): CtbAddrTsToRs and the TileId of each raster address
+        ts_to_rs.clear();
+        ctb_tile.assign((size_t)wctb * hctb, 0);
+        for (size_t j = 0; j + 1 < p.row_bd.size(); j++)
+            for (size_t i = 0; i + 1 < p.col_bd.size(); i++)
+                for (int y = p.row_bd[j]; y < p.row_bd[j + 1]; y++)
+                    for (int x = p.col_bd[i]; x < p.col_bd[i + 1]; x++) {
+                        ts_to_rs.push_back(y * wctb + x);
+                        ctb_tile[(size_t)y * wctb + x] = (int)(j * (p.col_bd.size() - 1) + i);
+                    }
+    };
     if (cfg->inter) {
         p.inter = 1;
         p.dpb_minus1 = cfg->max_refs;
@@ -2033,30 +2085,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         p.beta_div2 = uni(-6, 6);
         p.tc_div2 = uni(-6, 6);
     }
-    // tiles: as many as Main's minimum tile size (256 x 64 luma samples) allows
-    {
-        const int min_w = (256 + ctb - 1) / ctb, min_h = (64 + ctb - 1) / ctb;
-        const int nc = std::max(1, std::min(cfg->tile_cols, wctb / min_w));
-        const int nr = std::max(1, std::min(cfg->tile_rows, hctb / min_h));
-        p.uniform_tiles = coin() ? 1 : 0;
-        auto bounds = [&](int n, int total, int min_size, std::vector<int>& bd) {
-            bd.assign(1, 0);
-            if (p.uniform_tiles) {
-                for (int i = 1; i <= n; i++) bd.push_back((i * total) / n);
-                return;
-            }
-            int left = total;
-            for (int i = 0; i < n - 1; i++) {
-                const int sz = uni(min_size, left - min_size * (n - 1 - i));
-                bd.push_back(bd.back() + sz);
-                left -= sz;
-            }
-            bd.push_back(total);
-        };
-        bounds(nc, wctb, min_w, p.col_bd);
-        bounds(nr, hctb, min_h, p.row_bd);
-        p.lf_across_tiles = coin() ? 1 : 0;
-    }
+    layout(cfg->width, cfg->height);
     p.wpp = cfg->wpp && p.tiles() == 1 ? 1 : 0;
     p.dependent_slices = cfg->dependent_slices ? 1 : 0;
     p.lf_across_slices = cfg->slices > 1 ? (coin() ? 1 : 0) : 1;
@@ -2072,13 +2101,6 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         p.pcm_lf_disabled = coin() ? 1 : 0;
     }
     p.scaling = cfg->scaling;
-    if (cfg->crop) {   // the window keeps at least 16 x 16 luma samples
-        const int mx = std::min(8, (p.W - 16) / 8), my = std::min(8, (p.H - 16) / 8);
-        p.crop[0] = uni(0, std::max(0, mx));
-        p.crop[1] = uni(0, std::max(0, mx));
-        p.crop[2] = uni(0, std::max(0, my));
-        p.crop[3] = uni(0, std::max(0, my));
-    }
     p.output_flag = cfg->p_no_output > 0 ? 1 : 0;
     p.long_term = cfg->long_term ? 1 : 0;
     p.list_mod = cfg->list_mod ? 1 : 0;
@@ -2087,15 +2109,6 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         while ((1 << need) <= 2 * std::max(1, cfg->ra_gop) + 2) need++;
         p.poc_bits = cfg->poc_lsb_bits ? std::max(need, std::min(16, cfg->poc_lsb_bits)) : 8;
     }
-    // tile scan (6.5.1): CtbAddrTsToRs and the TileId of each raster address
-    std::vector<int> ts_to_rs, ctb_tile((size_t)wctb * hctb);
-    for (size_t j = 0; j + 1 < p.row_bd.size(); j++)
-        for (size_t i = 0; i + 1 < p.col_bd.size(); i++)
-            for (int y = p.row_bd[j]; y < p.row_bd[j + 1]; y++)
-                for (int x = p.col_bd[i]; x < p.col_bd[i + 1]; x++) {
-                    ts_to_rs.push_back(y * wctb + x);
-                    ctb_tile[(size_t)y * wctb + x] = (int)(j * (p.col_bd.size() - 1) + i);
-                }
     const std::vector<PicPlan> plan = plan_sequence(*cfg, rng);
     if (cfg->inter) dpb_sizes(plan, p.num_reorder, p.dpb_minus1);
     if (cfg->inter && cfg->sps_rps) {   // the SPS holds the RPSs of most P/B pictures (the more frequent first)
@@ -2134,8 +2147,17 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     GopState gop;
     gop.decode_idx_of_poc.assign((size_t)cfg->pictures, 0);
     for (int k = 0; k < cfg->pictures; k++) {
-        Picture pic(*cfg, rng, p);
         const PicPlan& pl = plan[(size_t)k];
+        std::vector<uint8_t> param_sets;
+        if (cfg->resize && k > 0 && (pl.nal_type == 19 || pl.nal_type == 20) && coin()) {
+            // a new size (multiples of 8, at least 16 x 16) from this IDR picture on: the SPS
+            // and PPS are sent again before it (same ids; the new SPS is activated there)
+            layout(std::max(16, cfg->width - 8 * uni(0, (cfg->width - 16) / 16)),
+                   std::max(16, cfg->height - 8 * uni(0, (cfg->height - 16) / 16)));
+            nal(param_sets, 33, sps(p, rng));
+            nal(param_sets, 34, pps(p, rng));
+        }
+        Picture pic(*cfg, rng, p);
         gop.decode_idx_of_poc[(size_t)pl.poc] = k;
         pic.wctb = wctb;
         pic.hctb = hctb;
@@ -2147,8 +2169,9 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         pic.qp8.assign((size_t)(p.W / 8) * (p.H / 8), 0);
         pic.mode4.assign((size_t)(p.W / 4) * (p.H / 4), 1);
         pic.coeffs.reserve((size_t)p.W * p.H * 3 / 2);
-        if (p.extra && k > 0 && pl.slice_type == 2 && uni(0, 1)) nal(out, 36, {});   // EOS_NUT before an IDR picture
-        pic.code_picture(pl, gop, out, k > 0);
+        if (p.extra && k > 0 && (pl.nal_type == 19 || pl.nal_type == 20) && uni(0, 1))
+            nal(out, 36, {});   // EOS_NUT before an IDR picture
+        pic.code_picture(pl, gop, out, k > 0, param_sets);
         s->slice_type[k] = pic.slice_type;
         s->poc[k] = pl.poc;
         s->output[k] = pl.output ? 1 : 0;

@@ -100,6 +100,8 @@ typedef struct hevcgen_cfg {
                                  /* and RADL from the middle one on)                      */
     int32_t  poc_lsb_bits;       /* log2_max_pic_order_cnt_lsb (0: 8); raised where the   */
                                  /* GOP needs more; small values make POCs wrap            */
+    int32_t  resize;             /* with idr_period: an IDR picture may bring a new SPS   */
+                                 /* (a smaller picture size) and PPS                      */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an

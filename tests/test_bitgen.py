@@ -79,6 +79,9 @@ CONFIGS = {
         w=72, h=40, seed=43, inter=1, pictures=40, poc_lsb_bits=4, long_term=1, max_refs=3),
     "P/B 72x40, 40 pictures, random access with CRA pictures, POC LSBs of 4 bits": dict(
         w=72, h=40, seed=44, inter=1, pictures=40, poc_lsb_bits=4, ra_gop=4, cra=1),
+    "P/B 200x136, an IDR picture every 4 with a new size (SPS and PPS sent again)": dict(
+        w=200, h=136, seed=45, inter=1, pictures=16, idr_period=4, resize=1, crop=1),
+    "I 200x136, a new size at every picture": dict(w=200, h=136, seed=46, pictures=6, resize=1),
     "P/B 200x136, long-term reference pictures, an IDR picture every 5": dict(
         w=200, h=136, seed=37, inter=1, pictures=12, long_term=1, idr_period=5, max_refs=2, tmvp=1),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
@@ -383,10 +386,9 @@ def test_dropin_host_code_decodes_generated_streams(name):
     assert _md5(got) == _md5(want)
     assert [f.poc for f in got] == [f.poc for f in want] == _output_order(pics)
     c = CONFIGS[name]
-    crop = (0, 0, 0, 0) if not c.get("crop") else None
-    for f in got:   # the conformance window
-        assert (f.width, f.height) == (want[0].width, want[0].height)
-        if crop is not None:
+    for f, g in zip(got, want):   # the conformance window, the size of each picture
+        assert (f.width, f.height) == (g.width, g.height)
+        if not c.get("crop") and not c.get("resize"):
             assert (f.width, f.height) == (c["w"], c["h"])
 
 
