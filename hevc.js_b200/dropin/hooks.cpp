@@ -503,6 +503,22 @@ void Backend::submit(DecodingContext& ctx) {
         fail("picture POC " + std::to_string(ctx.pic->poc) + " is not supported: " + w.unsupported);
         raise();
     }
+    // Every luma sample is predicted once: by the luma TUs of intra CUs (PCM included) and
+    // by the PUs of inter CUs.  More than the picture's area means slices that code some
+    // blocks twice (a damaged stream: the reference keeps whichever came last); the records
+    // cannot say which, so the picture fails here rather than differ silently.
+    {
+        uint64_t area = 0;
+        for (const hevc_tu_t& t : w.tus)
+            if (t.c_idx == 0 && (t.flags & HEVC_TU_INTRA)) area += (uint64_t)1 << (2 * t.log2_size);
+        for (const hevc_pu_t& u : w.pus) area += (uint64_t)u.w * u.h;
+        const uint64_t pic_area = (uint64_t)ctx.sps->pic_width_in_luma_samples * ctx.sps->pic_height_in_luma_samples;
+        if (area > pic_area) {
+            fail("picture POC " + std::to_string(ctx.pic->poc) +
+                 ": its slices code some blocks more than once (a damaged stream)");
+            raise();
+        }
+    }
     if (ensure_gpu(*ctx.sps)) raise();
     const hevc::DPB& d = *ctx.dpb;
     // the shared pointer of the current picture, and the slots whose pictures are gone or

@@ -330,6 +330,47 @@ def test_gpu_decoding_from_a_cra_picture(seed):
     _check_from_a_cra(None, seed)
 
 
+def _with_a_slice_twice():
+    """A generated stream in which the second slice of the first picture is sent again after
+    the picture's last one: those CTUs are coded twice (a damaged stream)."""
+    from hevc_b200 import bitgen
+    data, _ = bitgen.generate(200, 136, 7, inter=1, pictures=3, slices=4, log2_ctb=4)
+    pos = [k for k in range(len(data) - 3) if data[k:k + 4] == b"\x00\x00\x00\x01"]
+    nals = [data[a:b] for a, b in zip(pos, pos[1:] + [len(data)])]
+    vcl = [i for i, n in enumerate(nals) if ((n[4] >> 1) & 63) < 32]
+    starts = [i for i in vcl if nals[i][6] & 0x80]   # first_slice_segment_in_pic_flag
+    pic0 = [i for i in vcl if starts[0] <= i < starts[1]]
+    assert len(pic0) >= 2
+    return b"".join(nals[:pic0[-1] + 1] + [nals[pic0[1]]] + nals[pic0[-1] + 1:])
+
+
+def _check_slice_twice(lib):
+    from hevc_b200 import decoder as D
+    data = _with_a_slice_twice()
+    ref = D.Decoder(REF_LIB)
+    assert ref.decode(data) == 0   # the reference keeps whichever coding came last
+    dec = D.Decoder(lib)
+    assert dec.decode(data) != 0
+    assert "code some blocks more than once" in dec.last_error()
+
+
+def test_a_picture_whose_slices_overlap_fails():
+    """The drop-in refuses a picture whose slices code some blocks twice, with a message,
+    where its records cannot say which coding the reference kept."""
+    _needs_reference()
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    _check_slice_twice(checker)
+
+
+@pytest.mark.gpu
+@pytest.mark.last
+def test_gpu_a_picture_whose_slices_overlap_fails():
+    _needs_reference()
+    _check_slice_twice(None)
+
+
 def test_random_access_streams_are_reordered():
     """A random-access stream codes each mini-GOP's last picture first and the others by
     bisection; every POC appears once."""
