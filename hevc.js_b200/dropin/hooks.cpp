@@ -653,6 +653,38 @@ void Backend::submit(DecodingContext& ctx) {
 
 // ---- the reference's hooks --------------------------------------------------------------
 
+// RefPicList construction (dpb.cpp:245), called for each P and B slice.  A P or B slice
+// needs a current reference picture (NumPicTotalCurr > 0, 7.4.7.2); without one the
+// reference's list construction loops without end (dpb.cpp:259-266, a damaged stream can
+// ask for it), so the drop-in counts NumPicTotalCurr (7-55) from the slice's RPS first and
+// refuses the picture instead.
+extern "C" void __real__ZN4hevc3DPB23construct_ref_pic_listsERKNS_11SliceHeaderERKNS_3SPSERKNS_3PPSE(
+    hevc::DPB*, const hevc::SliceHeader&, const hevc::SPS&, const hevc::PPS&);
+extern "C" void __wrap__ZN4hevc3DPB23construct_ref_pic_listsERKNS_11SliceHeaderERKNS_3SPSERKNS_3PPSE(
+    hevc::DPB* dpb, const hevc::SliceHeader& sh, const hevc::SPS& sps, const hevc::PPS& pps) {
+    if (sh.slice_type != hevc::SliceType::I) {
+        const hevc::ShortTermRefPicSet* rps = &sh.st_rps;
+        if (sh.short_term_ref_pic_set_sps_flag)
+            rps = sh.short_term_ref_pic_set_idx < sps.st_ref_pic_sets.size() ? &sps.st_ref_pic_sets[sh.short_term_ref_pic_set_idx]
+                                                                           : nullptr;
+        int total = 0;
+        if (rps) {
+            for (uint32_t i = 0; i < rps->NumNegativePics && i < 16; i++) total += rps->UsedByCurrPicS0[i];
+            for (uint32_t i = 0; i < rps->NumPositivePics && i < 16; i++) total += rps->UsedByCurrPicS1[i];
+        }
+        const uint32_t n_lt = std::min<uint32_t>(32, sh.num_long_term_sps + sh.num_long_term_pics);
+        for (uint32_t i = 0; i < n_lt; i++)
+            total += i < sh.num_long_term_sps ? sps.used_by_curr_pic_lt_sps_flag[sh.lt_idx_sps[i] % 32]
+                                              : sh.used_by_curr_pic_lt_flag[i];
+        if (total == 0) {
+            dropin::Backend* b = dropin::lookup(dpb);
+            b->fail("a P or B slice without a current reference picture (NumPicTotalCurr 0: a damaged stream)");
+            b->raise();
+        }
+    }
+    __real__ZN4hevc3DPB23construct_ref_pic_listsERKNS_11SliceHeaderERKNS_3SPSERKNS_3PPSE(dpb, sh, sps, pps);
+}
+
 namespace hevc {
 void decode_residual_coding(DecodingContext& ctx, int x0, int y0, int log2TrafoSize, int cIdx, int16_t* coefficients);
 }

@@ -371,6 +371,56 @@ def test_gpu_a_picture_whose_slices_overlap_fails():
     _check_slice_twice(None)
 
 
+def _without_a_current_reference():
+    """A generated P picture whose RPS marks its one reference as not used by it
+    (used_by_curr_pic_s0_flag flipped): NumPicTotalCurr is 0, which 7.4.7.2 forbids in a P
+    slice (a damaged stream)."""
+    from hevc_b200 import bitgen
+    data, _ = bitgen.generate(64, 64, 5, inter=1, pictures=3, max_refs=1, p_b=0.0, sao=0, tmvp=0)
+    pos = [k for k in range(len(data) - 3) if data[k:k + 4] == b"\x00\x00\x00\x01"]
+    nals = [data[a:b] for a, b in zip(pos, pos[1:] + [len(data)])]
+    k = [(n[4] >> 1) & 63 for n in nals].index(1)   # the first P picture (TRAIL_R)
+    n = bytearray(nals[k])
+    bits = "".join(f"{b:08b}" for b in n[6:10])
+    # first_slice_segment_in_pic_flag, pps id, slice_type P, 8 POC LSBs, sps flag 0,
+    # num_negative_pics 1, num_positive_pics 0, delta_poc_s0_minus1 0, then the flag
+    assert bits[:5] == "11010" and bits[13:17] == "0010" and bits[17:19] == "11", bits
+    n[6 + 19 // 8] ^= 0x80 >> (19 % 8)
+    nals[k] = bytes(n)
+    return b"".join(nals)
+
+
+def _check_without_a_current_reference(lib):
+    from hevc_b200 import decoder as D
+    dec = D.Decoder(lib)
+    assert dec.decode(_without_a_current_reference()) != 0
+    assert "without a current reference picture" in dec.last_error()
+
+
+def test_a_slice_without_a_current_reference_fails(tmp_path):
+    """The drop-in refuses a P/B slice with NumPicTotalCurr 0; the reference's list
+    construction does not end on it (dpb.cpp:259-266: checked in a child process with a
+    time limit)."""
+    _needs_reference()
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    _check_without_a_current_reference(checker)
+    stream = tmp_path / "nocurr.265"
+    stream.write_bytes(_without_a_current_reference())
+    code = ("import sys; sys.path.insert(0, %r); import __graft_entry__ as ge; ge.load_package(); "
+            "from hevc_b200 import decoder as D; D.Decoder(%r).decode(open(%r, 'rb').read())"
+            % (os.path.dirname(HERE), REF_LIB, str(stream)))
+    with pytest.raises(subprocess.TimeoutExpired):
+        subprocess.run([sys.executable, "-c", code], capture_output=True, timeout=5)
+
+
+@pytest.mark.gpu
+@pytest.mark.last
+def test_gpu_a_slice_without_a_current_reference_fails():
+    _check_without_a_current_reference(None)
+
+
 def test_random_access_streams_are_reordered():
     """A random-access stream codes each mini-GOP's last picture first and the others by
     bisection; every POC appears once."""
