@@ -34,7 +34,7 @@ class GenCfg(C.Structure):
                 ("idr_period", C.c_int32), ("crop", C.c_int32), ("p_no_output", C.c_double),
                 ("long_term", C.c_int32), ("list_mod", C.c_int32), ("extra_syntax", C.c_int32),
                 ("sps_rps", C.c_int32), ("cra", C.c_int32), ("poc_lsb_bits", C.c_int32),
-                ("resize", C.c_int32)]
+                ("resize", C.c_int32), ("temporal", C.c_int32)]
 
 # ref_quirks bits (csrc/bitgen.h): tools written the way the reference's parser reads them
 QUIRK_TILES_PCM, QUIRK_DEPENDENT = 1, 2
@@ -45,14 +45,14 @@ class GenStream(C.Structure):
                 ("num_tus", C.POINTER(C.c_int32)), ("tus", C.POINTER(C.POINTER(abi.TU))),
                 ("num_coeffs", C.POINTER(C.c_uint64)), ("coeffs", C.POINTER(C.POINTER(C.c_int16))),
                 ("slice_type", C.POINTER(C.c_int32)), ("poc", C.POINTER(C.c_int32)),
-                ("output", C.POINTER(C.c_int32)), ("crop", C.c_int32 * 4),
+                ("output", C.POINTER(C.c_int32)), ("tid", C.POINTER(C.c_int32)), ("crop", C.c_int32 * 4),
                 ("num_pus", C.POINTER(C.c_int32)),
                 ("pus", C.POINTER(C.POINTER(abi.PU)))]
 
 # slice_type values (7.4.7.1)
 SLICE_B, SLICE_P, SLICE_I = 0, 1, 2
 
-GenPicture = collections.namedtuple("GenPicture", "tus levels pus slice_type poc output")
+GenPicture = collections.namedtuple("GenPicture", "tus levels pus slice_type poc output tid")
 
 
 _lib = None
@@ -94,7 +94,8 @@ def generate(width, height, seed, **cfg):
             n = int(s.num_coeffs[k])
             levels = np.ctypeslib.as_array(s.coeffs[k], shape=(n,)).copy() if n else np.zeros(0, np.int16)
             pus = [abi.PU.from_buffer_copy(s.pus[k][i]) for i in range(s.num_pus[k])]
-            pics.append(GenPicture(tus, levels, pus, int(s.slice_type[k]), int(s.poc[k]), bool(s.output[k])))
+            pics.append(GenPicture(tus, levels, pus, int(s.slice_type[k]), int(s.poc[k]), bool(s.output[k]),
+                                   int(s.tid[k])))
         return data, pics
     finally:
         g.hevcgen_stream_free(sp)

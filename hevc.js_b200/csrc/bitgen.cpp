@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <functional>
+#include <map>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -51,12 +52,12 @@ struct Bits {
     }
 };
 
-// Annex B: start code, NAL unit header (nuh_layer_id 0, TemporalId 0), emulation prevention.
-void nal(std::vector<uint8_t>& out, int type, const std::vector<uint8_t>& rbsp) {
+// Annex B: start code, NAL unit header (nuh_layer_id 0, TemporalId tid), emulation prevention.
+void nal(std::vector<uint8_t>& out, int type, const std::vector<uint8_t>& rbsp, int tid = 0) {
     const uint8_t sc[4] = {0, 0, 0, 1};
     out.insert(out.end(), sc, sc + 4);
     out.push_back((uint8_t)(type << 1));
-    out.push_back(1);
+    out.push_back((uint8_t)(tid + 1));   // nuh_temporal_id_plus1
     int zeros = 0;
     for (uint8_t b : rbsp) {
         if (zeros >= 2 && b <= 3) {
@@ -279,7 +280,7 @@ struct Contexts {
 namespace {
 
 // ---- parameter sets (7.3.2) ---------------------------------------------------------------
-void profile_tier_level(Bits& b) {
+void profile_tier_level(Bits& b, int max_sub_layers_minus1) {
     b.put(0, 2);           // general_profile_space
     b.put(0, 1);           // general_tier_flag
     b.put(1, 5);           // general_profile_idc: Main
@@ -291,6 +292,12 @@ void profile_tier_level(Bits& b) {
     b.put(0, 32);          // general_reserved_zero_43bits (and general_inbld_flag / reserved bit)
     b.put(0, 12);
     b.put(120, 8);         // general_level_idc: 4
+    for (int i = 0; i < max_sub_layers_minus1; i++) {
+        b.bit(0);          // sub_layer_profile_present_flag
+        b.bit(0);          // sub_layer_level_present_flag
+    }
+    if (max_sub_layers_minus1 > 0)
+        for (int i = max_sub_layers_minus1; i < 8; i++) b.put(0, 2);   // reserved_zero_2bits
 }
 
 // A short-term RPS as deltas to the current POC: before it (closest first) and after it
@@ -381,6 +388,7 @@ struct Params {
     int long_term = 0;                                          // long_term_ref_pics_present_flag
     int list_mod = 0;                                           // lists_modification_present_flag
     int poc_bits = 8;                                           // log2_max_pic_order_cnt_lsb
+    int max_tid = 0;                                            // sps_max_sub_layers_minus1
     int extra = 0;             // AUD, SEI, filler, EOS/EOB NAL units, VUI, slice_reserved_flag, header extensions
     int extra_bits = 0;                                         // num_extra_slice_header_bits
     std::vector<Rps> rps_sets;                                  // the SPS's st_ref_pic_set()s
@@ -425,14 +433,16 @@ std::vector<uint8_t> vps(const Params& p) {
     b.bit(1);              // vps_base_layer_internal_flag
     b.bit(1);              // vps_base_layer_available_flag
     b.put(0, 6);           // vps_max_layers_minus1
-    b.put(0, 3);           // vps_max_sub_layers_minus1
-    b.bit(1);              // vps_temporal_id_nesting_flag
+    b.put((uint32_t)p.max_tid, 3);           // vps_max_sub_layers_minus1
+    b.bit(p.max_tid == 0 ? 1 : 0);           // vps_temporal_id_nesting_flag
     b.put(0xFFFF, 16);     // vps_reserved_0xffff_16bits
-    profile_tier_level(b);
+    profile_tier_level(b, p.max_tid);
     b.bit(1);              // vps_sub_layer_ordering_info_present_flag
-    b.ue((uint32_t)p.dpb_minus1);            // vps_max_dec_pic_buffering_minus1
-    b.ue((uint32_t)p.num_reorder);           // vps_max_num_reorder_pics
-    b.ue(0);               // vps_max_latency_increase_plus1
+    for (int i = 0; i <= p.max_tid; i++) {   // the same for every sub-layer
+        b.ue((uint32_t)p.dpb_minus1);        // vps_max_dec_pic_buffering_minus1
+        b.ue((uint32_t)p.num_reorder);       // vps_max_num_reorder_pics
+        b.ue(0);                             // vps_max_latency_increase_plus1
+    }
     b.put(0, 6);           // vps_max_layer_id
     b.ue(0);               // vps_num_layer_sets_minus1
     b.bit(0);              // vps_timing_info_present_flag
@@ -512,9 +522,9 @@ void vui_parameters(Bits& b, std::mt19937_64& rng) {
 std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
     Bits b;
     b.put(0, 4);           // sps_video_parameter_set_id
-    b.put(0, 3);           // sps_max_sub_layers_minus1
-    b.bit(1);              // sps_temporal_id_nesting_flag
-    profile_tier_level(b);
+    b.put((uint32_t)p.max_tid, 3);           // sps_max_sub_layers_minus1
+    b.bit(p.max_tid == 0 ? 1 : 0);           // sps_temporal_id_nesting_flag
+    profile_tier_level(b, p.max_tid);
     b.ue(0);               // sps_seq_parameter_set_id
     b.ue(1);               // chroma_format_idc: 4:2:0
     b.ue((uint32_t)p.W);   // pic_width_in_luma_samples
@@ -526,9 +536,11 @@ std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
     b.ue(0);               // bit_depth_chroma_minus8
     b.ue((uint32_t)(p.poc_bits - 4));        // log2_max_pic_order_cnt_lsb_minus4
     b.bit(1);              // sps_sub_layer_ordering_info_present_flag
-    b.ue((uint32_t)p.dpb_minus1);            // sps_max_dec_pic_buffering_minus1
-    b.ue((uint32_t)p.num_reorder);           // sps_max_num_reorder_pics
-    b.ue(0);               // sps_max_latency_increase_plus1
+    for (int i = 0; i <= p.max_tid; i++) {
+        b.ue((uint32_t)p.dpb_minus1);        // sps_max_dec_pic_buffering_minus1
+        b.ue((uint32_t)p.num_reorder);       // sps_max_num_reorder_pics
+        b.ue(0);                             // sps_max_latency_increase_plus1
+    }
     b.ue(0);               // log2_min_luma_coding_block_size_minus3: 8x8
     b.ue((uint32_t)(p.log2_ctb - 3));        // log2_diff_max_min_luma_coding_block_size
     b.ue(0);               // log2_min_luma_transform_block_size_minus2: 4x4
@@ -636,7 +648,7 @@ namespace {
 // decode index, and its short-term RPS (7.4.8): the pictures kept, those before it in output
 // order (closest first) and those after it (closest first), each used by it or not.
 struct PicPlan {
-    int poc = 0, slice_type = 2, decode_idx = 0, nal_type = 19;
+    int poc = 0, slice_type = 2, decode_idx = 0, nal_type = 19, tid = 0;   // tid: TemporalId
     bool output = true, no_output_of_prior = false;   // pic_output_flag, no_output_of_prior_pics_flag
     std::vector<int> neg, pos, lt;   // lt: POCs kept as long-term reference pictures
     std::vector<int> neg_used, pos_used, lt_used, lt_msb;   // lt_msb: delta_poc_msb_present_flag
@@ -1455,10 +1467,10 @@ struct Picture {
     void code_picture(const PicPlan& pl, GopState& gop, std::vector<uint8_t>& out, bool aud,
                       const std::vector<uint8_t>& param_sets) {
         plan = &pl;
-        if (p.extra && aud) nal(out, 35, access_unit_delimiter());
+        if (p.extra && aud) nal(out, 35, access_unit_delimiter(), pl.tid);
         out.insert(out.end(), param_sets.begin(), param_sets.end());   // a new SPS and PPS (after the AUD)
         if (p.extra)
-            for (int i = uni(0, 2); i > 0; i--) nal(out, 39, sei_user_data());   // PREFIX_SEI
+            for (int i = uni(0, 2); i > 0; i--) nal(out, 39, sei_user_data(), pl.tid);   // PREFIX_SEI
         const int poc = pl.poc;
         slice_type = pl.slice_type;
         const bool intra = slice_type == 2;
@@ -1491,7 +1503,7 @@ struct Picture {
                     if (hh.n) hh.trailing();
                     std::vector<uint8_t> rbsp = hh.buf;
                     rbsp.insert(rbsp.end(), d.buf.begin(), d.buf.end());
-                    nal(out, nal_type, rbsp);
+                    nal(out, nal_type, rbsp, pl.tid);
                     break;
                 }
                 if (entry) {
@@ -1518,15 +1530,15 @@ struct Picture {
                 for (size_t k = 0; k + 1 < starts.size(); k++)
                     got.push_back((uint32_t)(pos[hsize + starts[k + 1]] - pos[hsize + starts[k]]));
                 if (got == sizes || iter == 8) {
-                    nal(out, nal_type, rbsp);
+                    nal(out, nal_type, rbsp, pl.tid);
                     break;
                 }
                 sizes = got;
             }
         }
         if (p.extra) {
-            for (int i = uni(0, 1); i > 0; i--) nal(out, 40, sei_user_data());   // SUFFIX_SEI
-            if (uni(0, 2) == 0) nal(out, 38, filler_data());                     // FD_NUT
+            for (int i = uni(0, 1); i > 0; i--) nal(out, 40, sei_user_data(), pl.tid);   // SUFFIX_SEI
+            if (uni(0, 2) == 0) nal(out, 38, filler_data(), pl.tid);                     // FD_NUT
         }
     }
 
@@ -1840,14 +1852,16 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
         // their inner pictures are its leading pictures: RADL from POC radl_from on (they
         // use only the CRA picture and other RADL pictures), RASL below it
         std::vector<int> cra, radl_from;
+        std::map<int, int> tid_of;   // TemporalId: the bisection depth (with temporal)
         if (cfg.inter) {
             const int g = std::max(1, cfg.ra_gop);
-            std::function<void(int, int)> bisect = [&](int lo, int hi) {
+            std::function<void(int, int, int)> bisect = [&](int lo, int hi, int depth) {
                 if (hi - lo < 2) return;
                 const int mid = (lo + hi) / 2;
                 order.push_back(mid);
-                bisect(lo, mid);
-                bisect(mid, hi);
+                tid_of[mid] = cfg.temporal ? std::min(6, depth) : 0;
+                bisect(lo, mid, depth + 1);
+                bisect(mid, hi, depth + 1);
             };
             for (int base = 0; base < n - 1; base += g) {
                 const int anchor = std::min(base + g, n - 1);
@@ -1856,7 +1870,7 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
                     cra.push_back(anchor);
                     radl_from.push_back(anchor - base >= 2 && u01() < 0.5 ? (base + anchor) / 2 : anchor);
                 }
-                bisect(base, anchor);
+                bisect(base, anchor, 1);
             }
         }
         // long-term (low delay only): from the period's third picture on, its IDR picture
@@ -1891,8 +1905,9 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
                     std::sort(future.begin(), future.end());
                     if (!past.empty() && !(floor > poc)) r.push_back(past[0]);
                     if (!future.empty()) r.push_back(future[0]);
-                    if (!(floor > poc) && (int)r.size() < cfg.max_refs && past.size() > 1 && u01() < 0.5)
-                        r.push_back(past[1]);
+                    if (!(floor > poc) && (int)r.size() < cfg.max_refs && past.size() > 1 &&
+                        tid_of[past[1]] <= tid_of[poc] && u01() < 0.5)
+                        r.push_back(past[1]);   // a picture of a higher sub-layer is never a reference
                 }
             }
             refs.push_back(r);
@@ -1901,6 +1916,7 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
             PicPlan pl;
             pl.poc = order[j];
             pl.decode_idx = (int)plan.size();
+            pl.tid = tid_of.count(pl.poc) ? tid_of[pl.poc] : 0;
             const bool is_cra = std::find(cra.begin(), cra.end(), pl.poc) != cra.end();
             pl.slice_type = j == 0 || is_cra ? 2 : (u01() < cfg.p_b ? 0 : 1);
             pl.output = !(cfg.p_no_output > 0 && u01() < cfg.p_no_output);
@@ -2110,6 +2126,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         p.poc_bits = cfg->poc_lsb_bits ? std::max(need, std::min(16, cfg->poc_lsb_bits)) : 8;
     }
     const std::vector<PicPlan> plan = plan_sequence(*cfg, rng);
+    for (const PicPlan& pl : plan) p.max_tid = std::max(p.max_tid, pl.tid);
     if (cfg->inter) dpb_sizes(plan, p.num_reorder, p.dpb_minus1);
     if (cfg->inter && cfg->sps_rps) {   // the SPS holds the RPSs of most P/B pictures (the more frequent first)
         std::vector<std::pair<int, Rps>> count;
@@ -2143,6 +2160,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     s->pus = static_cast<hevc_pu_t**>(std::calloc((size_t)cfg->pictures, sizeof(hevc_pu_t*)));
     s->poc = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
     s->output = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
+    s->tid = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
     for (int k = 0; k < 4; k++) s->crop[k] = p.crop[k];
     GopState gop;
     gop.decode_idx_of_poc.assign((size_t)cfg->pictures, 0);
@@ -2175,6 +2193,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         s->slice_type[k] = pic.slice_type;
         s->poc[k] = pl.poc;
         s->output[k] = pl.output ? 1 : 0;
+        s->tid[k] = pl.tid;
         s->num_pus[k] = (int32_t)pic.pus.size();
         s->pus[k] = static_cast<hevc_pu_t*>(std::malloc(sizeof(hevc_pu_t) * std::max<size_t>(1, pic.pus.size())));
         if (!pic.pus.empty())
@@ -2205,6 +2224,7 @@ void hevcgen_stream_free(hevcgen_stream_t* s) {
     std::free(s->slice_type);
     std::free(s->poc);
     std::free(s->output);
+    std::free(s->tid);
     std::free(s->num_pus);
     std::free(s->pus);
     std::free(s->num_tus);

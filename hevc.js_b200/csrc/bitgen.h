@@ -102,6 +102,8 @@ typedef struct hevcgen_cfg {
                                  /* GOP needs more; small values make POCs wrap            */
     int32_t  resize;             /* with idr_period: an IDR picture may bring a new SPS   */
                                  /* (a smaller picture size) and PPS                      */
+    int32_t  temporal;           /* random access: temporal sub-layers, TemporalId the    */
+                                 /* picture's bisection depth (VPS/SPS sub-layer fields)  */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an
@@ -137,6 +139,7 @@ typedef struct hevcgen_stream {
     int32_t*  slice_type;        /* per picture: 0 B, 1 P, 2 I (slice_type of 7.4.7.1)   */
     int32_t*  poc;               /* per picture: PicOrderCntVal (output order)            */
     int32_t*  output;            /* per picture: pic_output_flag                          */
+    int32_t*  tid;               /* per picture: TemporalId                               */
     int32_t   crop[4];           /* conformance window: left, right, top, bottom, in      */
                                  /* chroma samples (SubWidthC = SubHeightC = 2)           */
     int32_t*  num_pus;           /* per picture                                           */

@@ -82,6 +82,8 @@ CONFIGS = {
     "P/B 200x136, an IDR picture every 4 with a new size (SPS and PPS sent again)": dict(
         w=200, h=136, seed=45, inter=1, pictures=16, idr_period=4, resize=1, crop=1),
     "I 200x136, a new size at every picture": dict(w=200, h=136, seed=46, pictures=6, resize=1),
+    "B 200x136, random access, mini-GOPs of 8, temporal sub-layers, CRA pictures": dict(
+        w=200, h=136, seed=47, inter=1, pictures=17, ra_gop=8, temporal=1, cra=1, p_b=1.0),
     "P/B 200x136, long-term reference pictures, an IDR picture every 5": dict(
         w=200, h=136, seed=37, inter=1, pictures=12, long_term=1, idr_period=5, max_refs=2, tmvp=1),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
@@ -419,6 +421,41 @@ def test_a_slice_without_a_current_reference_fails(tmp_path):
 @pytest.mark.last
 def test_gpu_a_slice_without_a_current_reference_fails():
     _check_without_a_current_reference(None)
+
+
+def _check_sub_layers(lib):
+    """Every temporal sub-bitstream (the NAL units of TemporalId <= T) decodes to the
+    reference's frames: the pictures of those sub-layers, in POC order."""
+    from hevc_b200 import bitgen, decoder as D
+    data, pics = bitgen.generate(200, 136, 48, inter=1, pictures=17, ra_gop=8, temporal=1)
+    pos = [k for k in range(len(data) - 3) if data[k:k + 4] == b"\x00\x00\x00\x01"]
+    nals = [data[a:b] for a, b in zip(pos, pos[1:] + [len(data)])]
+    top = max(g.tid for g in pics)
+    assert top == 3
+    for t in range(top + 1):
+        sub = b"".join(n for n in nals if (n[5] & 7) - 1 <= t)   # nuh_temporal_id_plus1
+        ref = D.Decoder(REF_LIB)
+        assert ref.decode(sub) == 0
+        want = ref.frames()
+        assert [f.poc for f in want] == sorted(g.poc for g in pics if g.tid <= t)
+        dec = D.Decoder(lib)
+        assert dec.decode(sub) == 0, dec.last_error()
+        assert _md5(dec.frames()) == _md5(want), t
+
+
+def test_temporal_sub_bitstreams():
+    _needs_reference()
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    _check_sub_layers(checker)
+
+
+@pytest.mark.gpu
+@pytest.mark.last
+def test_gpu_temporal_sub_bitstreams():
+    _needs_reference()
+    _check_sub_layers(None)
 
 
 def test_random_access_streams_are_reordered():
