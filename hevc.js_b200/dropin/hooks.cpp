@@ -653,6 +653,34 @@ void Backend::submit(DecodingContext& ctx) {
 
 // ---- the reference's hooks --------------------------------------------------------------
 
+// The data of a slice segment (coding_tree.cpp:536).  With WPP the reference decodes the
+// CTU rows on its thread pool (coding_tree.cpp:404-533), each row starting once the row
+// above has finished its second CTU; a picture one CTU wide has no second CTU, and every
+// row would wait for good.  Such a picture's slices take the reference's sequential path
+// (no thread pool), whose contexts at a row start are initialised, as 9.3.1 does when the
+// CTU above and to the right is unavailable.
+extern "C" bool __real__ZN4hevc25decode_slice_segment_dataERNS_15DecodingContextERNS_15BitstreamReaderERKSt6vectorImSaImEEm(
+    DecodingContext&, hevc::BitstreamReader&, const std::vector<size_t>&, size_t);
+extern "C" bool __wrap__ZN4hevc25decode_slice_segment_dataERNS_15DecodingContextERNS_15BitstreamReaderERKSt6vectorImSaImEEm(
+    DecodingContext& ctx, hevc::BitstreamReader& bs, const std::vector<size_t>& epb, size_t header_size) {
+    hevc::ThreadPool* pool = ctx.thread_pool;
+    if (pool && ctx.pps && ctx.pps->entropy_coding_sync_enabled_flag && ctx.sps && ctx.sps->PicWidthInCtbsY == 1) {
+        ctx.thread_pool = nullptr;
+        bool ok;
+        try {
+            ok = __real__ZN4hevc25decode_slice_segment_dataERNS_15DecodingContextERNS_15BitstreamReaderERKSt6vectorImSaImEEm(
+                ctx, bs, epb, header_size);
+        } catch (...) {
+            ctx.thread_pool = pool;
+            throw;
+        }
+        ctx.thread_pool = pool;
+        return ok;
+    }
+    return __real__ZN4hevc25decode_slice_segment_dataERNS_15DecodingContextERNS_15BitstreamReaderERKSt6vectorImSaImEEm(
+        ctx, bs, epb, header_size);
+}
+
 // RefPicList construction (dpb.cpp:245), called for each P and B slice.  A P or B slice
 // needs a current reference picture (NumPicTotalCurr > 0, 7.4.7.2); without one the
 // reference's list construction loops without end (dpb.cpp:259-266, a damaged stream can

@@ -220,6 +220,25 @@ void perform_inter_prediction(DecodingContext& ctx, int xPb, int yPb, int w, int
     R.pu_ref[1].push_back(rp[1]);
 }
 
+// A slice segment's data (coding_tree.cpp:536).  With WPP the reference decodes CTU rows on
+// its thread pool, each row waiting for the second CTU of the row above
+// (coding_tree.cpp:404-533); a picture one CTU wide has none and the rows would wait for
+// good, so its slices take the reference's own sequential path (no thread pool).  The
+// drop-in does the same (dropin/hooks.cpp).
+bool decode_slice_segment_data(DecodingContext& ctx, BitstreamReader& bs, const std::vector<size_t>& epb,
+                               size_t header_size) {
+    static auto f = real<bool (*)(DecodingContext&, BitstreamReader&, const std::vector<size_t>&, size_t)>(
+        "_ZN4hevc25decode_slice_segment_dataERNS_15DecodingContextERNS_15BitstreamReaderERKSt6vectorImSaImEEm");
+    ThreadPool* pool = ctx.thread_pool;
+    if (pool && ctx.pps && ctx.pps->entropy_coding_sync_enabled_flag && ctx.sps && ctx.sps->PicWidthInCtbsY == 1) {
+        ctx.thread_pool = nullptr;
+        const bool ok = f(ctx, bs, epb, header_size);
+        ctx.thread_pool = pool;
+        return ok;
+    }
+    return f(ctx, bs, epb, header_size);
+}
+
 // The picture's records from the context the reference's filters read
 // (decoder.cpp:117-185 fills it; the harness in ref_harness.cpp does the inverse).
 void apply_deblocking(DecodingContext& ctx) {

@@ -458,6 +458,75 @@ def test_gpu_temporal_sub_bitstreams():
     _check_sub_layers(None)
 
 
+def _one_ctu_wide(**kw):
+    """A WPP stream of pictures one CTU wide (64x256, 64x64 CTUs): four CTU rows, each its own
+    substream."""
+    from hevc_b200 import bitgen
+    return bitgen.generate(64, 256, 3, log2_ctb=6, wpp=1, **kw)
+
+
+def test_wpp_pictures_one_ctu_wide(port, tmp_path):
+    """The reference's threaded WPP path starts each CTU row once the row above has finished
+    its second CTU (coding_tree.cpp:404-533); a picture one CTU wide has none, and the
+    unmodified reference does not return (checked in a child process with a time limit).
+    The drop-in (and the recorder) give such pictures the reference's sequential path: the
+    reference then parses the drawn records, and the drop-in's frames are the oracle's
+    reconstruction of them."""
+    _needs_reference()
+    from hevc_b200 import decoder as D
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import real_streams
+    for kw in (dict(pictures=3), dict(inter=1, pictures=6, ra_gop=4)):
+        data, pics = _one_ctu_wide(**kw)
+        summary, rec, log = _record(tmp_path, data)
+        n = len(pics)
+        assert summary == f"pictures {n} matched {n} mismatched 0 unsupported 0 decode_rc 0", log
+        assert _differences(pics, rec) == []
+        outs = real_streams.replay(port.reconstruct_picture, rec)   # decode order, packed I420
+        want, period = [], []   # output order: period by period (an IDR picture starts one), by POC
+        for g, o in zip(pics, outs):
+            if g.slice_type == 2 and g.poc == 0 and period:
+                want += sorted(period, key=lambda e: e[0])
+                period = []
+            period.append((g.poc, o))
+        want += sorted(period, key=lambda e: e[0])
+        dec = D.Decoder(checker)
+        assert dec.decode(data) == 0, dec.last_error()
+        frames = dec.frames()
+        assert [f.poc for f in frames] == [e[0] for e in want]
+        for f, (poc, w) in zip(frames, want):
+            got = np.concatenate([pl.astype(np.uint8).ravel() for pl in f.planes])
+            assert np.array_equal(got, w), poc
+    stream = tmp_path / "wide1.265"
+    stream.write_bytes(_one_ctu_wide(pictures=2)[0])
+    code = ("import sys; sys.path.insert(0, %r); import __graft_entry__ as ge; ge.load_package(); "
+            "from hevc_b200 import decoder as D; D.Decoder(%r).decode(open(%r, 'rb').read())"
+            % (os.path.dirname(HERE), REF_LIB, str(stream)))
+    with pytest.raises(subprocess.TimeoutExpired):
+        subprocess.run([sys.executable, "-c", code], capture_output=True, timeout=5)
+
+
+@pytest.mark.gpu
+@pytest.mark.last
+def test_gpu_wpp_pictures_one_ctu_wide():
+    """The GPU drop-in on the same streams: the CPU checker's frames (the same host code over
+    the oracle)."""
+    from hevc_b200 import decoder as D
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    for kw in (dict(pictures=3), dict(inter=1, pictures=6, ra_gop=4)):
+        data, _ = _one_ctu_wide(**kw)
+        ref = D.Decoder(checker)
+        assert ref.decode(data) == 0
+        dec = D.Decoder()
+        assert dec.decode(data) == 0, dec.last_error()
+        assert _md5(dec.frames()) == _md5(ref.frames())
+
+
 def test_random_access_streams_are_reordered():
     """A random-access stream codes each mini-GOP's last picture first and the others by
     bisection; every POC appears once."""
