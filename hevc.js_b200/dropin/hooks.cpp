@@ -655,16 +655,20 @@ void Backend::submit(DecodingContext& ctx) {
 
 // The data of a slice segment (coding_tree.cpp:536).  With WPP the reference decodes the
 // CTU rows on its thread pool (coding_tree.cpp:404-533), each row starting once the row
-// above has finished its second CTU; a picture one CTU wide has no second CTU, and every
-// row would wait for good.  Such a picture's slices take the reference's sequential path
-// (no thread pool), whose contexts at a row start are initialised, as 9.3.1 does when the
-// CTU above and to the right is unavailable.
+// above has finished its second CTU, from the slice's first row to the picture's last, each
+// from column 0.  A picture one CTU wide has no second CTU, and every row would wait for
+// good; a picture of several slice segments has segments that start inside a row or end
+// before the picture does, which that path decodes from the wrong substreams.  Such
+// pictures take the reference's sequential path (no thread pool), which follows 9.3.1:
+// contexts initialised at a slice and synchronised at a row start within one (initialised
+// there when the CTU above and to the right is unavailable, as in a picture one CTU wide).
 extern "C" bool __real__ZN4hevc25decode_slice_segment_dataERNS_15DecodingContextERNS_15BitstreamReaderERKSt6vectorImSaImEEm(
     DecodingContext&, hevc::BitstreamReader&, const std::vector<size_t>&, size_t);
 extern "C" bool __wrap__ZN4hevc25decode_slice_segment_dataERNS_15DecodingContextERNS_15BitstreamReaderERKSt6vectorImSaImEEm(
     DecodingContext& ctx, hevc::BitstreamReader& bs, const std::vector<size_t>& epb, size_t header_size) {
     hevc::ThreadPool* pool = ctx.thread_pool;
-    if (pool && ctx.pps && ctx.pps->entropy_coding_sync_enabled_flag && ctx.sps && ctx.sps->PicWidthInCtbsY == 1) {
+    if (pool && ctx.pps && ctx.pps->entropy_coding_sync_enabled_flag && ctx.sps &&
+        (ctx.sps->PicWidthInCtbsY == 1 || ctx.num_slices > 1)) {
         ctx.thread_pool = nullptr;
         bool ok;
         try {

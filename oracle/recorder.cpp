@@ -221,16 +221,18 @@ void perform_inter_prediction(DecodingContext& ctx, int xPb, int yPb, int w, int
 }
 
 // A slice segment's data (coding_tree.cpp:536).  With WPP the reference decodes CTU rows on
-// its thread pool, each row waiting for the second CTU of the row above
-// (coding_tree.cpp:404-533); a picture one CTU wide has none and the rows would wait for
-// good, so its slices take the reference's own sequential path (no thread pool).  The
-// drop-in does the same (dropin/hooks.cpp).
+// its thread pool, each row waiting for the second CTU of the row above and every row from
+// column 0 to the picture's end (coding_tree.cpp:404-533); a picture one CTU wide has no
+// second CTU and the rows would wait for good, and a picture of several slice segments is
+// decoded from the wrong substreams.  Such pictures take the reference's own sequential
+// path (no thread pool).  The drop-in does the same (dropin/hooks.cpp).
 bool decode_slice_segment_data(DecodingContext& ctx, BitstreamReader& bs, const std::vector<size_t>& epb,
                                size_t header_size) {
     static auto f = real<bool (*)(DecodingContext&, BitstreamReader&, const std::vector<size_t>&, size_t)>(
         "_ZN4hevc25decode_slice_segment_dataERNS_15DecodingContextERNS_15BitstreamReaderERKSt6vectorImSaImEEm");
     ThreadPool* pool = ctx.thread_pool;
-    if (pool && ctx.pps && ctx.pps->entropy_coding_sync_enabled_flag && ctx.sps && ctx.sps->PicWidthInCtbsY == 1) {
+    if (pool && ctx.pps && ctx.pps->entropy_coding_sync_enabled_flag && ctx.sps &&
+        (ctx.sps->PicWidthInCtbsY == 1 || ctx.num_slices > 1)) {
         ctx.thread_pool = nullptr;
         const bool ok = f(ctx, bs, epb, header_size);
         ctx.thread_pool = pool;

@@ -465,6 +465,78 @@ def _one_ctu_wide(**kw):
     return bitgen.generate(64, 256, 3, log2_ctb=6, wpp=1, **kw)
 
 
+def _check_records_and_frames(port, tmp_path, lib, data, pics):
+    """Where the unmodified reference cannot be the judge: the recorder (the reference's
+    parser, on its sequential WPP path) must parse the drawn records and its oracle replay
+    match, and the drop-in's frames must be the oracle's reconstruction of those records,
+    in output order."""
+    from hevc_b200 import decoder as D
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import real_streams
+    summary, rec, log = _record(tmp_path, data)
+    n = len(pics)
+    assert summary == f"pictures {n} matched {n} mismatched 0 unsupported 0 decode_rc 0", log
+    assert _differences(pics, rec) == []
+    outs = real_streams.replay(port.reconstruct_picture, rec)   # decode order, packed I420
+    want, period = [], []   # output order: period by period (an IDR picture starts one), by POC
+    for g, o in zip(pics, outs):
+        if g.slice_type == 2 and g.poc == 0 and period:
+            want += sorted(period, key=lambda e: e[0])
+            period = []
+        period.append((g.poc, o))
+    want += sorted(period, key=lambda e: e[0])
+    dec = D.Decoder(lib)
+    assert dec.decode(data) == 0, dec.last_error()
+    frames = dec.frames()
+    assert [f.poc for f in frames] == [e[0] for e in want]
+    for f, (poc, w) in zip(frames, want):
+        got = np.concatenate([pl.astype(np.uint8).ravel() for pl in f.planes])
+        assert np.array_equal(got, w), poc
+    return frames
+
+
+def _wpp_slices(**kw):
+    """A WPP stream of several slices per picture (some starting inside a CTU row)."""
+    from hevc_b200 import bitgen
+    return bitgen.generate(200, 136, 20, log2_ctb=5, wpp=1, slices=6, **kw)
+
+
+def test_wpp_pictures_of_several_slices(port, tmp_path):
+    """The reference's threaded WPP path decodes every row of a slice from column 0 to the
+    picture's last row (coding_tree.cpp:404-533), so a picture of several slices is decoded
+    from the wrong substreams.  The drop-in (and the recorder) give such pictures the
+    reference's sequential path, which follows 9.3.1: the drawn records, and the oracle's
+    reconstruction of them.  The unmodified reference's frames differ here (in 29 of 40
+    such streams drawn: where its stray rows are not all coded again by a later slice)."""
+    _needs_reference()
+    from hevc_b200 import decoder as D
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    for kw in (dict(pictures=3), dict(inter=1, pictures=6, ra_gop=4, qp_delta_depth=2)):
+        data, pics = _wpp_slices(**kw)
+        frames = _check_records_and_frames(port, tmp_path, checker, data, pics)
+        ref = D.Decoder(REF_LIB)
+        assert ref.decode(data) == 0
+        assert _md5(ref.frames()) != _md5(frames)
+
+
+@pytest.mark.gpu
+@pytest.mark.last
+def test_gpu_wpp_pictures_of_several_slices():
+    from hevc_b200 import decoder as D
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    for kw in (dict(pictures=3), dict(inter=1, pictures=6, ra_gop=4, qp_delta_depth=2)):
+        data, _ = _wpp_slices(**kw)
+        ref = D.Decoder(checker)
+        assert ref.decode(data) == 0
+        dec = D.Decoder()
+        assert dec.decode(data) == 0, dec.last_error()
+        assert _md5(dec.frames()) == _md5(ref.frames())
+
+
 def test_wpp_pictures_one_ctu_wide(port, tmp_path):
     """The reference's threaded WPP path starts each CTU row once the row above has finished
     its second CTU (coding_tree.cpp:404-533); a picture one CTU wide has none, and the
@@ -473,33 +545,11 @@ def test_wpp_pictures_one_ctu_wide(port, tmp_path):
     reference then parses the drawn records, and the drop-in's frames are the oracle's
     reconstruction of them."""
     _needs_reference()
-    from hevc_b200 import decoder as D
     checker = os.path.join(REF, "libhevcdec_oracle.so")
     if not os.path.exists(checker):
         pytest.skip("the drop-in checker is not built (oracle/Makefile)")
-    sys.path.insert(0, os.path.join(HERE, "golden"))
-    import real_streams
     for kw in (dict(pictures=3), dict(inter=1, pictures=6, ra_gop=4)):
-        data, pics = _one_ctu_wide(**kw)
-        summary, rec, log = _record(tmp_path, data)
-        n = len(pics)
-        assert summary == f"pictures {n} matched {n} mismatched 0 unsupported 0 decode_rc 0", log
-        assert _differences(pics, rec) == []
-        outs = real_streams.replay(port.reconstruct_picture, rec)   # decode order, packed I420
-        want, period = [], []   # output order: period by period (an IDR picture starts one), by POC
-        for g, o in zip(pics, outs):
-            if g.slice_type == 2 and g.poc == 0 and period:
-                want += sorted(period, key=lambda e: e[0])
-                period = []
-            period.append((g.poc, o))
-        want += sorted(period, key=lambda e: e[0])
-        dec = D.Decoder(checker)
-        assert dec.decode(data) == 0, dec.last_error()
-        frames = dec.frames()
-        assert [f.poc for f in frames] == [e[0] for e in want]
-        for f, (poc, w) in zip(frames, want):
-            got = np.concatenate([pl.astype(np.uint8).ravel() for pl in f.planes])
-            assert np.array_equal(got, w), poc
+        _check_records_and_frames(port, tmp_path, checker, *_one_ctu_wide(**kw))
     stream = tmp_path / "wide1.265"
     stream.write_bytes(_one_ctu_wide(pictures=2)[0])
     code = ("import sys; sys.path.insert(0, %r); import __graft_entry__ as ge; ge.load_package(); "
