@@ -39,6 +39,10 @@ pb16       the P/B steady state: 2 groups of 16 streams of P/B pictures whose ba
            batched and plain forms and its own end-to-end rate.
 serving    64 live streams of mixed resolutions with Poisson segment arrivals (4 lanes,
            continuous batching): per-frame latency p50/p99.
+dropin     the drop-in decoder (hevc_decoder_decode, CABAC included) on the reference's 1080p
+           stream, beside the reference's own build of the same API; dropin_generated the
+           same on generated 1080p random-access streams, without and with WPP, in a child
+           process bounded by a timeout.
 --impl reference runs privaloops/hevc.js's own reconstruction functions (oracle/_ref,
            compiled from the reference's sources) on all host cores for the same GOP mix.
 """
@@ -780,12 +784,28 @@ GENERATED_1080P = dict(width=1920, height=1080, seed=4242, inter=1, pictures=32,
 
 
 def dropin_generated_child(reps=3):
-    """The drop-in on a stream of the random-syntax generator (csrc/bitgen.cpp), in this
-    process: the reference's own decode gives the MD5 both are checked against."""
+    """The drop-in on streams of the random-syntax generator (csrc/bitgen.cpp), in this
+    process: GENERATED_1080P, and the same syntax with WPP (entry points per CTU row, which
+    the reference's parser decodes on its thread pool, so both decoders parse on several
+    host threads) under "wpp"."""
+    out = generated_leg(GENERATED_1080P, reps)
+    out["wpp"] = generated_leg(GENERATED_1080P_WPP, reps)
+    out["wpp"]["note"] = ("the same syntax with WPP: one slice per picture, CTU rows parsed on the reference "
+                          "parser's thread pool in both decoders")
+    return out
+
+
+# the WPP form of GENERATED_1080P (another seed)
+GENERATED_1080P_WPP = dict(GENERATED_1080P, seed=4243, wpp=1)
+
+
+def generated_leg(cfg, reps):
+    """One generated stream through time_dropin: the reference's own decode gives the MD5
+    both decoders are checked against."""
     import hashlib
     from hevc_b200 import bitgen, decoder as D
     import oracle
-    c = dict(GENERATED_1080P)
+    c = dict(cfg)
     w, h, seed = c.pop("width"), c.pop("height"), c.pop("seed")
     data, pics = bitgen.generate(w, h, seed, **c)
     ref = D.Decoder(os.path.join(oracle.HERE, "_ref", "libhevcdec.so"))
@@ -794,7 +814,7 @@ def dropin_generated_child(reps=3):
     frames = ref.frames()
     want = hashlib.md5(b"".join(fr.yuv_bytes() for fr in frames)).hexdigest()
     ref.close()
-    out = {"stream": "generated (csrc/bitgen.cpp)", "config": GENERATED_1080P, "frames": len(frames),
+    out = {"stream": "generated (csrc/bitgen.cpp)", "config": cfg, "frames": len(frames),
            "bytes": len(data), "width": w, "height": h}
     out.update(time_dropin(data, len(frames), want, reps))
     out["note"] = ("random-access mini-GOPs of 8 from the seeded generator; both decoders checked against the "
