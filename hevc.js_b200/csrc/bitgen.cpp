@@ -1926,6 +1926,14 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
                 if (j > 0 && pl.poc < cra[c] && pl.poc > cra[c] - std::max(1, cfg.ra_gop) &&
                     std::find(order.begin(), order.begin() + (long)j, cra[c]) != order.begin() + (long)j)
                     pl.nal_type = pl.poc >= radl_from[c] ? 7 : 9;
+            if (cfg.nonref_types && j > 0 && (pl.nal_type == 1 || pl.nal_type == 7 || pl.nal_type == 9)) {
+                // a picture no later one uses: the sub-layer non-reference type (TRAIL_N,
+                // RADL_N, RASL_N), which 8.3.1 leaves out of prevTid0Pic
+                bool used = false;
+                for (size_t m = j + 1; m < order.size() && !used; m++)
+                    used = std::find(refs[m].begin(), refs[m].end(), pl.poc) != refs[m].end();
+                if (!used) pl.nal_type -= 1;
+            }
             if (j > 0) {
                 std::vector<int> keep;   // decoded before j, used by j or by a later picture
                 for (size_t i = 0; i < j; i++) {

@@ -104,6 +104,8 @@ typedef struct hevcgen_cfg {
                                  /* (a smaller picture size) and PPS                      */
     int32_t  temporal;           /* random access: temporal sub-layers, TemporalId the    */
                                  /* picture's bisection depth (VPS/SPS sub-layer fields)  */
+    int32_t  nonref_types;       /* a picture no later one uses gets TRAIL_N, RADL_N or   */
+                                 /* RASL_N (sub-layer non-reference)                      */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an
