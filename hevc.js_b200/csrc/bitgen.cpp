@@ -391,6 +391,7 @@ struct Params {
     int max_tid = 0;                                            // sps_max_sub_layers_minus1
     int extra = 0;             // AUD, SEI, filler, EOS/EOB NAL units, VUI, slice_reserved_flag, header extensions
     int extra_bits = 0;                                         // num_extra_slice_header_bits
+    int pps_id = 0;                                             // pps_pic_parameter_set_id
     std::vector<Rps> rps_sets;                                  // the SPS's st_ref_pic_set()s
     int wpp = 0;                                                // entropy_coding_sync_enabled_flag
     std::vector<int> col_bd, row_bd;                            // tile boundaries in CTBs (one tile: {0, w})
@@ -577,7 +578,7 @@ std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
 
 std::vector<uint8_t> pps(const Params& p, std::mt19937_64& rng) {
     Bits b;
-    b.ue(0);               // pps_pic_parameter_set_id
+    b.ue((uint32_t)p.pps_id);                // pps_pic_parameter_set_id
     b.ue(0);               // pps_seq_parameter_set_id
     b.bit(p.dependent_slices ? 1 : 0);       // dependent_slice_segments_enabled_flag
     b.bit(p.output_flag ? 1 : 0);             // output_flag_present_flag
@@ -1299,7 +1300,7 @@ struct Picture {
         const int nctb = wctb * hctb;
         b.bit(sg.start == 0);   // first_slice_segment_in_pic_flag
         if (irap) b.bit(plan->no_output_of_prior ? 1 : 0);   // no_output_of_prior_pics_flag
-        b.ue(0);                // slice_pic_parameter_set_id
+        b.ue((uint32_t)p.pps_id);   // slice_pic_parameter_set_id
         if (sg.start > 0) {
             if (p.dependent_slices) b.bit(sg.dependent ? 1 : 0);   // dependent_slice_segment_flag
             int bits = 0;
@@ -2156,7 +2157,37 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     if (p.extra) nal(out, 35, Picture::access_unit_delimiter());
     nal(out, 32, vps(p));
     nal(out, 33, sps(p, rng));
-    nal(out, 34, pps(p, rng));
+    // PPS variants (pps_count): the tools the configuration enables, each switched on or off
+    // and drawn again per PPS; each picture refers to one of them
+    std::vector<Params> ppss(1, p);
+    auto vary = [&](Params& q) {
+        q.qp_delta = p.qp_delta && coin() ? 1 : 0;
+        if (q.qp_delta) q.qp_delta_depth = uni(0, p.log2_ctb - 3);
+        if (cfg->chroma_qp_offsets) {
+            q.cb_qp_offset = uni(-12, 12);
+            q.cr_qp_offset = uni(-12, 12);
+            q.slice_chroma_offsets = coin() ? 1 : 0;
+        }
+        if (cfg->deblock_ctl) {
+            q.dbk_override = coin() ? 1 : 0;
+            q.dbk_disabled = uni(0, 3) == 0 ? 1 : 0;
+            q.beta_div2 = uni(-6, 6);
+            q.tc_div2 = uni(-6, 6);
+        }
+        q.bypass = p.bypass && coin() ? 1 : 0;
+        q.tskip = p.tskip && coin() ? 1 : 0;
+        q.sdh = p.sdh && coin() ? 1 : 0;
+        q.wp = p.wp && coin() ? 1 : 0;
+        q.list_mod = p.list_mod && coin() ? 1 : 0;
+        if (cfg->inter) q.log2_pml = uni(2, p.log2_ctb);
+    };
+    for (int i = 1; i < std::min(64, std::max(1, cfg->pps_count)); i++) {
+        Params q = p;
+        q.pps_id = i;
+        vary(q);
+        ppss.push_back(q);
+    }
+    for (const Params& q : ppss) nal(out, 34, pps(q, rng));
     auto* s = static_cast<hevcgen_stream_t*>(std::calloc(1, sizeof(hevcgen_stream_t)));
     s->pictures = cfg->pictures;
     s->num_tus = static_cast<int32_t*>(std::calloc((size_t)cfg->pictures, sizeof(int32_t)));
@@ -2181,9 +2212,18 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
             layout(std::max(16, cfg->width - 8 * uni(0, (cfg->width - 16) / 16)),
                    std::max(16, cfg->height - 8 * uni(0, (cfg->height - 16) / 16)));
             nal(param_sets, 33, sps(p, rng));
-            nal(param_sets, 34, pps(p, rng));
+            for (Params& q : ppss) {   // the new size in every PPS variant
+                q.W = p.W;
+                q.H = p.H;
+                q.col_bd = p.col_bd;
+                q.row_bd = p.row_bd;
+                q.uniform_tiles = p.uniform_tiles;
+                q.lf_across_tiles = p.lf_across_tiles;
+                for (int c = 0; c < 4; c++) q.crop[c] = p.crop[c];
+                nal(param_sets, 34, pps(q, rng));
+            }
         }
-        Picture pic(*cfg, rng, p);
+        Picture pic(*cfg, rng, ppss[(size_t)uni(0, (int)ppss.size() - 1)]);
         gop.decode_idx_of_poc[(size_t)pl.poc] = k;
         pic.wctb = wctb;
         pic.hctb = hctb;

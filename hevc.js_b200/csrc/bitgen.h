@@ -106,6 +106,9 @@ typedef struct hevcgen_cfg {
                                  /* picture's bisection depth (VPS/SPS sub-layer fields)  */
     int32_t  nonref_types;       /* a picture no later one uses gets TRAIL_N, RADL_N or   */
                                  /* RASL_N (sub-layer non-reference)                      */
+    int32_t  pps_count;          /* PPSs in the stream (ids 0..): the enabled tools switched */
+                                 /* on or off and drawn again per PPS; each picture refers */
+                                 /* to one of them                                        */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an

@@ -86,6 +86,9 @@ CONFIGS = {
         w=200, h=136, seed=47, inter=1, pictures=17, ra_gop=8, temporal=1, cra=1, p_b=1.0),
     "P/B 200x136, 40 pictures, CRA pictures, non-reference NAL types, POC LSBs of 4 bits": dict(
         w=200, h=136, seed=49, inter=1, pictures=40, ra_gop=4, cra=1, nonref_types=1, poc_lsb_bits=4),
+    "P/B 200x136, four PPSs (cu_qp_delta, chroma offsets, deblocking, transform skip, WP, lists)": dict(
+        w=200, h=136, seed=50, inter=1, pictures=8, pps_count=4, qp_delta_depth=2, chroma_qp_offsets=1,
+        deblock_ctl=1, p_tskip=0.3, sdh=1, list_mod=1, wp=1),
     "P/B 200x136, long-term reference pictures, an IDR picture every 5": dict(
         w=200, h=136, seed=37, inter=1, pictures=12, long_term=1, idr_period=5, max_refs=2, tmvp=1),
     # written the way the reference reads these tools (HEVCGEN_QUIRK_*): see
