@@ -2223,7 +2223,7 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
                 nal(param_sets, 34, pps(q, rng));
             }
         }
-        Picture pic(*cfg, rng, ppss[(size_t)uni(0, (int)ppss.size() - 1)]);
+        Picture pic(*cfg, rng, ppss[ppss.size() > 1 ? (size_t)uni(0, (int)ppss.size() - 1) : 0]);
         gop.decode_idx_of_poc[(size_t)pl.poc] = k;
         pic.wctb = wctb;
         pic.hctb = hctb;
