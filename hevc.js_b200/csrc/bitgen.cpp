@@ -1927,9 +1927,31 @@ std::vector<PicPlan> plan_sequence(const hevcgen_cfg_t& cfg, std::mt19937_64& rn
                 if (j > 0 && pl.poc < cra[c] && pl.poc > cra[c] - std::max(1, cfg.ra_gop) &&
                     std::find(order.begin(), order.begin() + (long)j, cra[c]) != order.begin() + (long)j)
                     pl.nal_type = pl.poc >= radl_from[c] ? 7 : 9;
-            if (cfg.nonref_types && j > 0 && (pl.nal_type == 1 || pl.nal_type == 7 || pl.nal_type == 9)) {
+            if (cfg.temporal && j > 0 && pl.nal_type == 1 && pl.tid > 0 && u01() < 0.6) {
+                // a sub-layer switching point where the plan allows one (7.4.2.2): TSA when
+                // neither it nor a later picture of its sub-layer or above uses a picture of
+                // those sub-layers decoded before it; else STSA, the same within its sub-layer
+                std::map<int, size_t> at;   // POC -> decode position in the period
+                for (size_t i = 0; i < order.size(); i++) at[order[i]] = i;
+                auto allowed = [&](bool tsa) {
+                    auto hit = [&](int r, int t) { return tsa ? tid_of[r] >= t : tid_of[r] == t; };
+                    for (int r : refs[j])
+                        if (hit(r, pl.tid)) return false;
+                    for (size_t m = j + 1; m < order.size(); m++) {
+                        const int tm = tid_of[order[m]];
+                        if (tsa ? tm < pl.tid : tm != pl.tid) continue;
+                        for (int r : refs[m])
+                            if (at[r] < j && hit(r, pl.tid)) return false;
+                    }
+                    return true;
+                };
+                if (allowed(true)) pl.nal_type = 3;          // TSA_R
+                else if (allowed(false)) pl.nal_type = 5;    // STSA_R
+            }
+            if (cfg.nonref_types && j > 0 &&
+                (pl.nal_type == 1 || pl.nal_type == 3 || pl.nal_type == 5 || pl.nal_type == 7 || pl.nal_type == 9)) {
                 // a picture no later one uses: the sub-layer non-reference type (TRAIL_N,
-                // RADL_N, RASL_N), which 8.3.1 leaves out of prevTid0Pic
+                // TSA_N, STSA_N, RADL_N, RASL_N), which 8.3.1 leaves out of prevTid0Pic
                 bool used = false;
                 for (size_t m = j + 1; m < order.size() && !used; m++)
                     used = std::find(refs[m].begin(), refs[m].end(), pl.poc) != refs[m].end();

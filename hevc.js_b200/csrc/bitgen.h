@@ -103,9 +103,10 @@ typedef struct hevcgen_cfg {
     int32_t  resize;             /* with idr_period: an IDR picture may bring a new SPS   */
                                  /* (a smaller picture size) and PPS                      */
     int32_t  temporal;           /* random access: temporal sub-layers, TemporalId the    */
-                                 /* picture's bisection depth (VPS/SPS sub-layer fields)  */
-    int32_t  nonref_types;       /* a picture no later one uses gets TRAIL_N, RADL_N or   */
-                                 /* RASL_N (sub-layer non-reference)                      */
+                                 /* picture's bisection depth (VPS/SPS sub-layer fields); */
+                                 /* TSA and STSA pictures where the plan allows them      */
+    int32_t  nonref_types;       /* a picture no later one uses gets TRAIL_N, TSA_N,      */
+                                 /* STSA_N, RADL_N or RASL_N (sub-layer non-reference)    */
     int32_t  pps_count;          /* PPSs in the stream (ids 0..): the enabled tools switched */
                                  /* on or off and drawn again per PPS; each picture refers */
                                  /* to one of them                                        */
