@@ -20,6 +20,9 @@ import pytest
 
 import oracle
 
+# every test here imports the package (the generator, the decoder wrapper)
+pytestmark = pytest.mark.usefixtures("hb")
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF = os.path.join(oracle.HERE, "_ref")
 RECORDER = os.path.join(REF, "hevc-record")
@@ -376,6 +379,53 @@ def test_a_picture_whose_slices_overlap_fails():
 def test_gpu_a_picture_whose_slices_overlap_fails():
     _needs_reference()
     _check_slice_twice(None)
+
+
+def _with_a_slice_header_cut():
+    """A generated stream cut two bytes into the header of the last picture's second slice."""
+    from hevc_b200 import bitgen
+    data, _ = bitgen.generate(200, 136, 7, inter=1, pictures=3, slices=4, log2_ctb=4)
+    pos = [k for k in range(len(data) - 3) if data[k:k + 4] == b"\x00\x00\x00\x01"]
+    nals = [data[a:b] for a, b in zip(pos, pos[1:] + [len(data)])]
+    vcl = [i for i, n in enumerate(nals) if ((n[4] >> 1) & 63) < 32]
+    starts = [i for i in vcl if nals[i][6] & 0x80]   # first_slice_segment_in_pic_flag
+    last = [i for i in vcl if i >= starts[-1]]
+    assert len(starts) == 3 and len(last) >= 2
+    return b"".join(nals[:last[1]]) + nals[last[1]][:8]
+
+
+def _check_slice_header_cut(lib):
+    from hevc_b200 import decoder as D
+    data = _with_a_slice_header_cut()
+    ref = D.Decoder(REF_LIB)
+    assert ref.decode(data) == 0
+    want = ref.frames()
+    assert [f.poc for f in want] == [0, 1, 2]   # POC 2's slices were never decoded
+    dec = D.Decoder(lib)
+    assert dec.decode(data) == 0, dec.last_error()
+    got = dec.frames()
+    assert [f.poc for f in got] == [0, 1]
+    assert _md5(got) == _md5(want[:2])
+
+
+def test_a_picture_cut_short_is_not_handed_out():
+    """A picture whose second slice header fails to parse: the reference still outputs it
+    (decoder.cpp:85 marks it for output when it is allocated; decoder.cpp:198-201 returns
+    before any of its slice data is decoded), with whatever samples its reused buffer held.
+    The drop-in hands out no frame for a picture it did not reconstruct, and every other
+    frame is the reference's."""
+    _needs_reference()
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    _check_slice_header_cut(checker)
+
+
+@pytest.mark.gpu
+@pytest.mark.last
+def test_gpu_a_picture_cut_short_is_not_handed_out():
+    _needs_reference()
+    _check_slice_header_cut(None)
 
 
 def _without_a_current_reference():
