@@ -35,7 +35,7 @@ class GenCfg(C.Structure):
                 ("long_term", C.c_int32), ("list_mod", C.c_int32), ("extra_syntax", C.c_int32),
                 ("sps_rps", C.c_int32), ("cra", C.c_int32), ("poc_lsb_bits", C.c_int32),
                 ("resize", C.c_int32), ("temporal", C.c_int32), ("nonref_types", C.c_int32),
-                ("pps_count", C.c_int32)]
+                ("pps_count", C.c_int32), ("bit_depth", C.c_int32)]
 
 # ref_quirks bits (csrc/bitgen.h): tools written the way the reference's parser reads them
 QUIRK_TILES_PCM, QUIRK_DEPENDENT = 1, 2

@@ -388,6 +388,7 @@ struct Params {
     int long_term = 0;                                          // long_term_ref_pics_present_flag
     int list_mod = 0;                                           // lists_modification_present_flag
     int poc_bits = 8;                                           // log2_max_pic_order_cnt_lsb
+    int bit_depth = 8;                                          // BitDepthY = BitDepthC
     int max_tid = 0;                                            // sps_max_sub_layers_minus1
     int extra = 0;             // AUD, SEI, filler, EOS/EOB NAL units, VUI, slice_reserved_flag, header extensions
     int extra_bits = 0;                                         // num_extra_slice_header_bits
@@ -533,8 +534,8 @@ std::vector<uint8_t> sps(const Params& p, std::mt19937_64& rng) {
     b.bit(p.crop[0] | p.crop[1] | p.crop[2] | p.crop[3] ? 1 : 0);   // conformance_window_flag
     if (p.crop[0] | p.crop[1] | p.crop[2] | p.crop[3])
         for (int k = 0; k < 4; k++) b.ue((uint32_t)p.crop[k]);   // conf_win_left/right/top/bottom_offset
-    b.ue(0);               // bit_depth_luma_minus8
-    b.ue(0);               // bit_depth_chroma_minus8
+    b.ue((uint32_t)(p.bit_depth - 8));       // bit_depth_luma_minus8
+    b.ue((uint32_t)(p.bit_depth - 8));       // bit_depth_chroma_minus8
     b.ue((uint32_t)(p.poc_bits - 4));        // log2_max_pic_order_cnt_lsb_minus4
     b.bit(1);              // sps_sub_layer_ordering_info_present_flag
     for (int i = 0; i <= p.max_tid; i++) {
@@ -632,11 +633,12 @@ std::vector<uint8_t> pps(const Params& p, std::mt19937_64& rng) {
     return b.buf;
 }
 
-// chroma QP of 4:2:0 (8.6.1, table 8-10) for the records
-int chroma_qp(int qpi) {
+// chroma Qp' of 4:2:0 (8.6.1, table 8-10) for the records: qPi clipped to
+// -QpBdOffsetC..57, mapped, plus QpBdOffsetC (bd_off)
+int chroma_qp(int qpi, int bd_off) {
     static const int tab[14] = {29, 30, 31, 32, 33, 33, 34, 34, 35, 35, 36, 36, 37, 37};
-    qpi = std::min(57, std::max(0, qpi));
-    return qpi < 30 ? qpi : (qpi > 43 ? qpi - 6 : tab[qpi - 30]);
+    qpi = std::min(57, std::max(-bd_off, qpi));
+    return (qpi < 30 ? qpi : (qpi > 43 ? qpi - 6 : tab[qpi - 30])) + bd_off;
 }
 
 }  // namespace
@@ -1038,7 +1040,11 @@ struct Picture {
     // cu_qp_delta_abs (9.3.3.10: prefix TR cMax 5, first bin context 0, the others context
     // 1; suffix EG0 bypass) and cu_qp_delta_sign_flag; CuQpDeltaVal in -26..25 (7.4.9.14)
     void cu_qp_delta() {
-        const int v = u01() < 0.6 ? uni(-3, 3) : uni(-26, 25), a = std::abs(v);
+        int v = u01() < 0.6 ? uni(-3, 3) : uni(-26, 25);
+        // above 8 bits QpY stays in 0..51, where the wrap of 8.6.1 never applies (the
+        // records' QP is unsigned)
+        if (p.bit_depth > 8) v = std::min(51 - qg_pred, std::max(-qg_pred, v));
+        const int a = std::abs(v);
         for (int k = 0; k < 5; k++) {
             E.decision(C.qp_delta[k ? 1 : 0], k < a);
             if (k >= a) break;
@@ -1066,14 +1072,14 @@ struct Picture {
             t.y = (uint16_t)(c ? y0 / 2 : y0);
             t.log2_size = (uint8_t)l2;
             t.c_idx = (uint8_t)c;
-            t.qp = (uint8_t)cu_qp();
+            t.qp = (uint8_t)(cu_qp() + 6 * (p.bit_depth - 8));
             t.flags = (uint8_t)(HEVC_TU_INTRA | HEVC_TU_CODED | HEVC_TU_PCM | (cu_bypass ? HEVC_TU_BYPASS : 0));
             t.intra_mode = 1;
             t.coeff_offset = (uint32_t)coeffs.size();
             for (int i = 0; i < 1 << (2 * l2); i++) {
                 const int v = uni(0, (1 << bits) - 1);
                 b.put((uint32_t)v, bits);
-                coeffs.push_back((int16_t)(v << (8 - bits)));
+                coeffs.push_back((int16_t)(v << (p.bit_depth - bits)));
             }
             tus.push_back(t);
         }
@@ -1088,8 +1094,8 @@ struct Picture {
         t.y = (uint16_t)y;
         t.log2_size = (uint8_t)log2;
         t.c_idx = (uint8_t)c;
-        const int qpy = cu_qp();
-        t.qp = (uint8_t)(c ? chroma_qp(qpy + (c == 1 ? cb_off : cr_off)) : qpy);
+        const int qpy = cu_qp(), bd_off = 6 * (p.bit_depth - 8);
+        t.qp = (uint8_t)(c ? chroma_qp(qpy + (c == 1 ? cb_off : cr_off), bd_off) : qpy + bd_off);
         t.flags = (uint8_t)((inter ? 0 : HEVC_TU_INTRA) | (coded ? HEVC_TU_CODED : 0) |
                             (coded && cu_bypass ? HEVC_TU_BYPASS : 0));
         t.intra_mode = (uint8_t)(inter ? 0 : mode);
@@ -1815,10 +1821,12 @@ void Picture::sao(int rx, int ry) {
         }
         if (!type) continue;
         int abs_v[4];
-        for (int k = 0; k < 4; k++) {   // sao_offset_abs: TR cMax 7, bypass
-            abs_v[k] = uni(0, 7);
+        // sao_offset_abs: TR cMax (1 << (Min(BitDepth, 10) - 5)) - 1, bypass (7.4.9.3.2)
+        const int sao_max = (1 << (std::min(p.bit_depth, 10) - 5)) - 1;
+        for (int k = 0; k < 4; k++) {
+            abs_v[k] = uni(0, sao_max);
             for (int b = 0; b < abs_v[k]; b++) E.bypass(1);
-            if (abs_v[k] < 7) E.bypass(0);
+            if (abs_v[k] < sao_max) E.bypass(0);
         }
         if (type == 1) {
             for (int k = 0; k < 4; k++)
@@ -2048,7 +2056,8 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
         cfg->max_mvd > 1 << 14 || cfg->max_merge < 0 || cfg->max_merge > 5 || cfg->depth_inter < 0 ||
         cfg->depth_inter > 2 || cfg->slices < 1 || cfg->tile_cols < 1 || cfg->tile_rows < 1 || cfg->scaling < 0 ||
         cfg->scaling > 3 || cfg->qp_delta_depth < 0 ||
-        (cfg->wpp && cfg->dependent_slices && (cfg->ref_quirks & HEVCGEN_QUIRK_DEPENDENT)) || cfg->idr_period < 0)
+        (cfg->wpp && cfg->dependent_slices && (cfg->ref_quirks & HEVCGEN_QUIRK_DEPENDENT)) || cfg->idr_period < 0 ||
+        (cfg->bit_depth != 0 && cfg->bit_depth != 8 && cfg->bit_depth != 10))
         return nullptr;
     std::mt19937_64 rng(cfg->seed);
     auto uni = [&](int lo, int hi) { return std::uniform_int_distribution<int>(lo, hi)(rng); };
@@ -2139,10 +2148,11 @@ hevcgen_stream_t* hevcgen_stream(const hevcgen_cfg_t* cfg) {
     p.bypass = cfg->p_bypass > 0 ? 1 : 0;
     p.tskip = cfg->p_tskip > 0 ? 1 : 0;
     p.sdh = cfg->sdh ? 1 : 0;
+    p.bit_depth = cfg->bit_depth == 10 ? 10 : 8;
     if (cfg->p_pcm > 0) {
         p.pcm = 1;
-        p.pcm_bits_y = uni(1, 8);
-        p.pcm_bits_c = uni(1, 8);
+        p.pcm_bits_y = uni(1, p.bit_depth);
+        p.pcm_bits_c = uni(1, p.bit_depth);
         p.pcm_log2_min = uni(3, std::min(5, p.log2_ctb));
         p.pcm_log2_max = uni(p.pcm_log2_min, std::min(5, p.log2_ctb));
         p.pcm_lf_disabled = coin() ? 1 : 0;

@@ -110,6 +110,9 @@ typedef struct hevcgen_cfg {
     int32_t  pps_count;          /* PPSs in the stream (ids 0..): the enabled tools switched */
                                  /* on or off and drawn again per PPS; each picture refers */
                                  /* to one of them                                        */
+    int32_t  bit_depth;          /* 8 (0 means 8) or 10: BitDepthY = BitDepthC; with 10,  */
+                                 /* CuQpDeltaVal keeps QpY in 0..51, the TU records hold */
+                                 /* Qp' (QpY + QpBdOffset), SAO offsets reach 31         */
 } hevcgen_cfg_t;
 
 /* Tiles and PCM: after end_of_subset_one_bit and after pcm_flag the reference reads an

@@ -229,6 +229,54 @@ def test_reference_parses_the_drawn_syntax(hb, tmp_path, name):
             assert not g.pus
 
 
+TEN_BIT = [name for name in sorted(CONFIGS) if any(k in name for k in (
+    "chroma QP offsets", "PCM", "weighted prediction", "scaling lists in the SPS", "2x2 tiles",
+    "dependent slice segments", "sign hiding", "dense levels"))]
+
+
+@pytest.mark.parametrize("name", TEN_BIT)
+def test_reference_parses_the_drawn_syntax_at_10_bits(tmp_path, name):
+    """Main10 streams (BitDepthY = BitDepthC = 10): the reference parses every picture into
+    the drawn records.  Their QP is Qp' (QpY + QpBdOffset, 8.6.1), SAO offsets reach 31
+    (7.4.9.3.2), PCM samples up to 10 bits.  The oracle and the kernels keep 8-bit
+    samples, so the recorder marks the pictures unsupported and only the records are
+    compared."""
+    _needs_reference()
+    from hevc_b200 import bitgen
+    c = dict(CONFIGS[name], bit_depth=10)
+    data, pics = bitgen.generate(c.pop("w"), c.pop("h"), c.pop("seed"), **c)
+    summary, rec, log = _record(tmp_path, data)
+    n = len(pics)
+    assert summary == f"pictures {n} matched 0 mismatched 0 unsupported {n} decode_rc 0", log
+    assert _differences(pics, rec) == []
+    # luma Qp' = QpY + 12 (QpY >= 0 here); the parsed records carry the same
+    assert all(t.qp >= 12 for g in pics for t in g.tus if t.c_idx == 0)
+
+
+def test_dropin_refuses_10_bit_streams():
+    """The drop-in keeps 8-bit samples: a Main10 stream fails at its first picture with a
+    message, and no frame is handed out."""
+    _needs_reference()
+    checker = os.path.join(REF, "libhevcdec_oracle.so")
+    if not os.path.exists(checker):
+        pytest.skip("the drop-in checker is not built (oracle/Makefile)")
+    from hevc_b200 import bitgen, decoder as D
+    data, _ = bitgen.generate(64, 64, 1, bit_depth=10)
+    dec = D.Decoder(checker)
+    assert dec.decode(data) != 0
+    assert "bit" in dec.last_error()
+    assert dec.frames() == []
+
+
+def test_generator_bit_depths():
+    from hevc_b200 import bitgen
+    a, _ = bitgen.generate(64, 64, 1)
+    b, _ = bitgen.generate(64, 64, 1, bit_depth=8)
+    assert a == b
+    with pytest.raises(Exception):
+        bitgen.generate(64, 64, 1, bit_depth=9)
+
+
 # Where the reference's parser departs from H.265 (each found with these streams): a stream
 # written by the standard is not parsed into what was drawn, the same stream written the
 # way the reference reads it is.  Details at the HEVCGEN_QUIRK_* bits (csrc/bitgen.h).
